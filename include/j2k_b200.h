@@ -1,0 +1,173 @@
+/*
+ * j2k_b200 — C ABI of the B200 (sm_100a) JPEG 2000 encode/decode hot path.
+ *
+ * This header replaces the OpenCL plumbing of knopkem/roger (OCLDeviceManager, OCLQueue,
+ * OCLMemoryManager, OCLKernel; src/ocl_platform.h, src/OCLUtil.h:31-39) with a context that owns
+ * a CUDA stream plus grow-only device scratch, and exposes each stage operator of the reference
+ * as one call.  Conventions:
+ *   - every call returns j2k_status (0 = ok, < 0 = error); j2k_last_error() gives the message.
+ *     The reference logged and swallowed cl_int failures (src/OCLUtil.cpp:60-74); here nothing
+ *     is swallowed.
+ *   - stage operators take DEVICE pointers owned by the caller and are ordered on the context's
+ *     stream (j2k_ctx_set_stream to use your own); j2k_stream_sync replaces clFinish
+ *     (src/OCLEncodeDecode.cpp:33-36).
+ *   - a context is not thread-safe: use one per host thread (as the reference's single in-order
+ *     queue, src/OCLUtil.cpp:505-516).
+ *   - device code never traps: kernels report through an error word that becomes a status.
+ *   - pitches are in ELEMENTS of the buffer's type unless the name says bytes.
+ *   - no C++ exceptions cross this boundary.
+ */
+#ifndef J2K_B200_H
+#define J2K_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int j2k_status;
+#define J2K_OK 0
+#define J2K_ERR_INVALID_ARG (-1)
+#define J2K_ERR_CUDA (-2)
+#define J2K_ERR_OUT_OF_MEMORY (-3)
+#define J2K_ERR_DEVICE (-4)       /* a kernel set its error word (bad descriptor, bound hit) */
+#define J2K_ERR_CAPACITY (-5)     /* an output buffer was too small; nothing past it was written */
+#define J2K_ERR_UNSUPPORTED (-6)
+#define J2K_ERR_TIMEOUT (-7)      /* a bounded device-side wait gave up */
+
+enum { J2K_U8 = 0, J2K_I16 = 1, J2K_I32 = 2, J2K_F32 = 3 };
+enum { J2K_MCT_NONE = 0, J2K_MCT_RCT = 1, J2K_MCT_ICT = 2 };
+/* J2K_ORDER_T800: columns then rows per level (T.800 F.4.2; any conformant decoder inverts it).
+ * J2K_ORDER_REF : rows then columns per level (src/CL/ocldwt53.cl:206-277, the reference). */
+enum { J2K_ORDER_T800 = 0, J2K_ORDER_REF = 1 };
+enum { J2K_W53 = 53, J2K_W97 = 97 };
+enum { J2K_BAND_LL = 0, J2K_BAND_HL = 1, J2K_BAND_LH = 2, J2K_BAND_HH = 3 };
+
+typedef struct j2k_ctx j2k_ctx;
+
+/* ---- context: replaces OCLDeviceManager::init/getInfo + ocl_args_d_t ------------------------ */
+j2k_status j2k_ctx_create(int device, j2k_ctx** out);
+j2k_status j2k_ctx_destroy(j2k_ctx* ctx);
+j2k_status j2k_ctx_set_stream(j2k_ctx* ctx, void* cuda_stream); /* NULL = context's own */
+void* j2k_ctx_stream(j2k_ctx* ctx);
+j2k_status j2k_stream_sync(j2k_ctx* ctx);                          /* replaces clFinish */
+const char* j2k_last_error(const j2k_ctx* ctx);
+const char* j2k_status_string(j2k_status s);
+int j2k_version(void);
+
+/* ---- RGB -> planar (+ level shift + RCT/ICT): replaces OCLRGBtoPlanar<T>::run
+ *      (src/OCLRGBtoPlanar.cpp:36-44) and kernel src/CL/oclplanar.cl:23-40.
+ * in: interleaved uint8, ncomp (1..4) samples per pixel, row pitch in bytes.
+ * planes: out_dtype J2K_I32 (mct NONE/RCT) or J2K_F32 (mct NONE/ICT); plane c starts at
+ * planes + c*plane_stride elements, rows plane_pitch elements apart.  Subtracts 128. */
+j2k_status j2k_rgb_to_planar(j2k_ctx* ctx, const uint8_t* in, size_t in_pitch_bytes, int ncomp,
+                             int mct, int out_dtype, void* planes, size_t plane_pitch,
+                             size_t plane_stride, size_t w, size_t h);
+/* Inverse: planes (+ inverse MCT, + 128, round, clamp) -> interleaved uint8. */
+j2k_status j2k_planar_to_rgb(j2k_ctx* ctx, const void* planes, int in_dtype, size_t plane_pitch,
+                             size_t plane_stride, int ncomp, int mct, uint8_t* out,
+                             size_t out_pitch_bytes, size_t w, size_t h);
+
+/* ---- forward DWT: replaces OCLDWTForward<T>::run (src/OCLDWTForward.cpp:124-137) and kernels
+ * src/CL/ocldwt53.cl:167-292 / src/CL/ocldwt97.cl:196-420,487-716.
+ * Out-of-place, all `levels` levels, Mallat layout in `out` (low half first on both axes,
+ * ceil(n/2) low samples).  kernel 53: in/out int32.  kernel 97: in float32; out float32 when
+ * steps == NULL, else int32 dead-zone indices with steps[b] (host array, 3*levels+1 entries in
+ * T.800 QCD order: LL_L, then HL,LH,HH for level L..1).  `in` is not modified.
+ * Uses context scratch for the intermediate LL bands. */
+j2k_status j2k_dwt_forward(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                           void* out, size_t out_pitch, size_t w, size_t h, int levels,
+                           const float* steps);
+/* ---- inverse DWT: replaces OCLDWTRev<T>::run (src/OCLDWTRev.cpp:39-58), whose kernels
+ * (ocldwt53rev.cl / ocldwt97rev.cl) are forward transforms; this is the true inverse.
+ * kernel 97 with steps != NULL reads int32 indices and dequantises ((|q|+1/2)*step). */
+j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                           void* out, size_t out_pitch, size_t w, size_t h, int levels,
+                           const float* steps);
+
+/* ---- EBCOT tier-1: replaces OCLBPC<T>::run (src/OCLBPC.cpp:38-50) and src/CL/oclbpc.cl:279-746.
+ * Code-blocks partition every subband of a Mallat plane (w x h, `levels`) on a cbw x cbh grid
+ * anchored at the subband origin, subbands in QCD order, blocks in raster order. */
+typedef struct {
+    uint32_t offset;   /* byte offset of this block's codeword in the bytes buffer */
+    int32_t length;    /* codeword bytes (0 for an all-zero block) */
+    uint8_t numbps;    /* magnitude bit-planes coded */
+    uint8_t npasses;   /* coding passes (3*numbps-2, or 0) */
+    uint8_t orient;    /* J2K_BAND_* */
+    uint8_t band;      /* subband index in QCD order */
+    uint16_t x0, y0;   /* top-left sample in the component's Mallat plane */
+    uint16_t cw, ch;   /* block size */
+    uint16_t comp;     /* component index */
+    uint16_t reserved;
+} j2k_cb_desc;
+
+/* Number of code-blocks of the partition above. */
+size_t j2k_codeblock_count(size_t w, size_t h, int levels, int cbw, int cbh);
+/* Encodes every code-block of `coeff` (int32, device).  descs (device, count entries) and
+ * bytes (device, count*cap_per_block bytes) are written; block i's codeword starts at
+ * i*cap_per_block.  J2K_ERR_CAPACITY when a block needs more than cap_per_block bytes.
+ * cbw, cbh: powers of two in 4..64, cbw*cbh <= 4096. */
+j2k_status j2k_bpc_encode(j2k_ctx* ctx, const int32_t* coeff, size_t pitch, size_t w, size_t h,
+                          int levels, int cbw, int cbh, j2k_cb_desc* descs, uint8_t* bytes,
+                          size_t cap_per_block);
+/* Decodes code-blocks (device descs/bytes as produced above) back into an int32 Mallat plane. */
+j2k_status j2k_bpc_decode(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
+                          size_t count, int32_t* coeff, size_t pitch, size_t w, size_t h,
+                          int levels, int cbw, int cbh);
+
+/* ---- whole-image encoder / decoder: replaces OCLEncoder<T>/OCLDecoder<T>
+ * (src/OCLEncoder.cpp:43-52, src/OCLDecoder.cpp:35-38, src/OCLEncodeDecode.h:23-38). */
+typedef struct j2k_encoder j2k_encoder;
+typedef struct {
+    int levels;        /* decomposition levels */
+    int cbw, cbh;      /* code-block size (default 64x64) */
+    int order;         /* J2K_ORDER_* (default T800) */
+    const float* steps;/* lossy: 3*levels+1 steps; NULL = 8*2^-level */
+} j2k_enc_params;
+
+j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_encoder** out);
+j2k_status j2k_encoder_destroy(j2k_encoder* enc);
+/* Reference-shaped entry (OCLEncoder<T>::run(components, w, h, levels, precision)): planar HOST
+ * components, already level-shifted (pixel-128) as src/OCLTest.cpp:80-90 builds them, of type
+ * dtype (J2K_I16, J2K_I32 or J2K_F32).  ncomp >= 3 applies RCT (lossless) / ICT (lossy) to
+ * components 0..2.  precision = bit depth (8). */
+j2k_status j2k_encoder_run(j2k_encoder* enc, const void* const* comps, int ncomp, int dtype,
+                           size_t w, size_t h, size_t levels, size_t precision,
+                           const j2k_enc_params* params);
+/* Fast entry: interleaved uint8 pixels (ncomp 1 or 3), on the host (on_device = 0, copied
+ * through pinned staging) or already on the device. */
+j2k_status j2k_encoder_run_interleaved(j2k_encoder* enc, const uint8_t* pixels, int on_device,
+                                       size_t pitch_bytes, int ncomp, size_t w, size_t h,
+                                       const j2k_enc_params* params);
+/* Host copy of the DWT coefficients (int32 lossless / lossy-quantised, float when
+ * output_dwt_only && lossy), planes back to back, row pitch in bytes returned (the reference's
+ * OCLEncodeDecode::mapDWTOut dropped it).  Valid until unmap. */
+j2k_status j2k_encoder_map_dwt_out(j2k_encoder* enc, void** ptr, size_t* pitch_bytes);
+j2k_status j2k_encoder_unmap_dwt_out(j2k_encoder* enc, void* ptr);
+/* Code-block results of the last run, copied to the host: *count descriptors (component-major)
+ * and their codewords packed back to back (descs[i].offset rewritten to the packed offset).
+ * Pass descs/bytes NULL to query count and total bytes. */
+j2k_status j2k_encoder_get_codeblocks(j2k_encoder* enc, j2k_cb_desc* descs, size_t* count,
+                                      uint8_t* bytes, size_t cap, size_t* used);
+/* T.800 codestream (SOC..EOC, one tile, one layer, LRCP) of the last run.  out NULL: size only. */
+j2k_status j2k_encoder_get_codestream(j2k_encoder* enc, uint8_t* out, size_t cap, size_t* len);
+/* Device-side view of the last run's results (valid until the next run). */
+j2k_status j2k_encoder_device_results(j2k_encoder* enc, const j2k_cb_desc** descs,
+                                      const uint8_t** bytes, size_t* count,
+                                      size_t* cap_per_block);
+
+typedef struct j2k_decoder j2k_decoder;
+j2k_status j2k_decoder_create(j2k_ctx* ctx, int lossy, j2k_decoder** out);
+j2k_status j2k_decoder_destroy(j2k_decoder* dec);
+/* Decodes code-blocks (layout of j2k_encoder_get_codeblocks; host or device memory) to an
+ * interleaved uint8 image (host or device). */
+j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs,
+                                      const uint8_t* bytes, size_t nbytes, int on_device,
+                                      int ncomp, size_t w, size_t h, const j2k_enc_params* params,
+                                      uint8_t* out, int out_on_device, size_t out_pitch_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

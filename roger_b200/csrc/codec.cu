@@ -1,0 +1,511 @@
+// Whole-image encoder / decoder objects and the tier-1 ABI entry points.
+//
+// Reference: OCLEncoder<T>::run (src/OCLEncoder.cpp:43-52: upload -> DWT -> planar -> BPC),
+// OCLDecoder<T>::run (src/OCLDecoder.cpp:35-38), OCLEncodeDecode<T>::mapDWTOut/finish
+// (src/OCLEncodeDecode.cpp:33-49) and OCLMemoryManager<T>::init/mapImage
+// (src/OCLMemoryManager.cpp:56-190).  The B200 pipeline order is upload -> planar+MCT ->
+// DWT (+ quantiser) -> tier-1, all on one stream, with every buffer kept resident and grown
+// only when a larger image arrives.  Code-block codewords are packed on the device (prefix
+// sum of lengths + gather) so a single device->host copy returns them.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "j2k_internal.cuh"
+
+namespace {
+
+size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+bool valid_cb(int v) { return v >= 4 && v <= 64 && (v & (v - 1)) == 0; }
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    j2k_status ensure(j2k_ctx* ctx, size_t bytes) {
+        if (n >= bytes) return J2K_OK;
+        if (p) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(p);
+            p = nullptr;
+            n = 0;
+        }
+        J2K_CUDA(ctx, cudaMalloc(&p, bytes));
+        n = bytes;
+        return J2K_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// gather each block's codeword (at i*cap) into a packed buffer at out_off[i]
+__global__ void pack_kernel(const j2k_cb_desc* __restrict__ descs, const uint32_t* __restrict__ off,
+                            const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int n) {
+    int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (wid >= n) return;
+    int len = descs[wid].length;
+    const uint8_t* s = src + descs[wid].offset;
+    uint8_t* d = dst + off[wid];
+    for (int k = lane; k < len; k += 32) d[k] = s[k];
+}
+
+__global__ void lengths_kernel(const j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ len, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) len[i] = (uint32_t)max(descs[i].length, 0);
+}
+
+std::vector<float> default_steps(size_t w, size_t h, int levels) {
+    std::vector<j2k_band_rect> r(3 * levels + 1);
+    j2k_band_rects(w, h, levels, r.data());
+    std::vector<float> s(r.size());
+    for (size_t b = 0; b < r.size(); ++b) s[b] = 8.0f * std::ldexp(1.0f, -r[b].level);
+    return s;
+}
+
+}  // namespace
+
+struct j2k_encoder {
+    j2k_ctx* ctx = nullptr;
+    int lossy = 0, dwt_only = 0;
+    // geometry of the last run
+    size_t w = 0, h = 0;
+    int ncomp = 0, levels = 0, cbw = 64, cbh = 64, order = J2K_ORDER_T800, mct = 0;
+    std::vector<float> steps;
+    DevBuf in, planes, coef, jobs, descs, bytes, lens, offs, packed, cubtmp;
+    std::vector<j2k_cb_job> hjobs;
+    size_t njobs = 0, cap = 0, sym_cap = 0;
+    size_t job_key[6] = {0, 0, 0, 0, 0, 0};
+    bool have_result = false;
+    void* mapped = nullptr;
+};
+
+struct j2k_decoder {
+    j2k_ctx* ctx = nullptr;
+    int lossy = 0;
+    DevBuf descs, bytes, coef, planes, out, jobs;
+    std::vector<j2k_cb_job> hjobs;
+    size_t job_key[6] = {0, 0, 0, 0, 0, 0};
+};
+
+static j2k_status prepare_jobs(j2k_ctx* ctx, std::vector<j2k_cb_job>& hjobs, DevBuf& djobs,
+                               size_t* key, size_t w, size_t h, int ncomp, int levels, int cbw,
+                               int cbh, size_t* njobs) {
+    size_t k[6] = {w, h, (size_t)ncomp, (size_t)levels, (size_t)cbw, (size_t)cbh};
+    if (std::equal(k, k + 6, key) && !hjobs.empty()) {
+        *njobs = hjobs.size();
+        return J2K_OK;
+    }
+    hjobs.clear();
+    for (int c = 0; c < ncomp; ++c) j2k_build_jobs(w, h, levels, cbw, cbh, &hjobs, c);
+    J2K_TRY(djobs.ensure(ctx, std::max<size_t>(hjobs.size(), 1) * sizeof(j2k_cb_job)));
+    J2K_CUDA(ctx, cudaMemcpyAsync(djobs.p, hjobs.data(), hjobs.size() * sizeof(j2k_cb_job),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    std::copy(k, k + 6, key);
+    *njobs = hjobs.size();
+    return J2K_OK;
+}
+
+static j2k_status check_params(j2k_ctx* ctx, const j2k_enc_params* p, size_t w, size_t h,
+                               int* levels, int* cbw, int* cbh, int* order) {
+    *levels = p ? p->levels : 5;
+    *cbw = p && p->cbw ? p->cbw : 64;
+    *cbh = p && p->cbh ? p->cbh : 64;
+    *order = p ? p->order : J2K_ORDER_T800;
+    if (*levels < 0 || *levels > 32) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "levels must be in 0..32");
+    if (!valid_cb(*cbw) || !valid_cb(*cbh) || *cbw * *cbh > 4096)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "code-block size must be a power of two in 4..64");
+    if (*order != J2K_ORDER_T800 && *order != J2K_ORDER_REF)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bad order");
+    if (w == 0 || h == 0 || w > 65535 || h > 65535)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "image size must be in 1..65535");
+    return J2K_OK;
+}
+
+// DWT of every component + tier-1 of all blocks.  planes: ncomp planes (int32 or float).
+static j2k_status encode_planes(j2k_encoder* e) {
+    j2k_ctx* ctx = e->ctx;
+    const size_t n = e->w * e->h;
+    const bool quant = e->lossy && !e->dwt_only;
+    const size_t csz = 4;
+    J2K_TRY(e->coef.ensure(ctx, n * csz * e->ncomp));
+    size_t w1 = (e->w + 1) / 2, h1 = (e->h + 1) / 2, w2 = (w1 + 1) / 2, h2 = (h1 + 1) / 2;
+    void* ll0 = j2k_scratch(ctx, SCR_LL0, w1 * h1 * 4);
+    void* ll1 = j2k_scratch(ctx, SCR_LL1, w2 * h2 * 4);
+    if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
+    for (int c = 0; c < e->ncomp; ++c) {
+        const char* src = (const char*)e->planes.p + (size_t)c * n * 4;
+        char* dst = (char*)e->coef.p + (size_t)c * n * csz;
+        J2K_TRY(j2k_dwt_fwd_impl(ctx, e->lossy ? J2K_W97 : J2K_W53, e->lossy ? J2K_ORDER_T800 : e->order,
+                                 src, e->w, dst, e->w, e->w, e->h, e->levels,
+                                 quant ? e->steps.data() : nullptr, ll0, ll1, j2k_dwt_tile{64, 64},
+                                 ctx->stream));
+    }
+    e->have_result = true;
+    if (e->dwt_only) return J2K_OK;
+    J2K_TRY(prepare_jobs(ctx, e->hjobs, e->jobs, e->job_key, e->w, e->h, e->ncomp, e->levels, e->cbw,
+                         e->cbh, &e->njobs));
+    const size_t nblk = (size_t)e->cbw * e->cbh;
+    if (e->cap == 0) e->cap = align16(nblk * 2 + 256);
+    if (e->sym_cap == 0) e->sym_cap = align16(nblk * 20 + 256);
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        J2K_TRY(e->descs.ensure(ctx, std::max<size_t>(e->njobs, 1) * sizeof(j2k_cb_desc)));
+        J2K_TRY(e->bytes.ensure(ctx, std::max<size_t>(e->njobs, 1) * e->cap));
+        J2K_TRY(j2k_clear_device_error(ctx));
+        J2K_TRY(j2k_t1_encode_jobs(ctx, (const int32_t*)e->coef.p, e->w, (const j2k_cb_job*)e->jobs.p,
+                                   e->njobs, (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p, e->cap,
+                                   e->sym_cap, ctx->stream));
+        j2k_status s = j2k_read_device_error(ctx);
+        if (s == J2K_OK) return J2K_OK;
+        if (s != J2K_ERR_CAPACITY) return s;
+        // grow whichever capacity overflowed and retry
+        if (ctx->err.find("symbol") != std::string::npos) e->sym_cap = align16(e->sym_cap * 2);
+        else e->cap = align16(e->cap * 2);
+    }
+    return j2k_fail(ctx, J2K_ERR_CAPACITY, "tier-1 capacities kept overflowing");
+}
+
+// pack codewords on the device: descs[i].offset -> packed offsets; returns total bytes
+static j2k_status pack_blocks(j2k_encoder* e, size_t* total) {
+    j2k_ctx* ctx = e->ctx;
+    int n = (int)e->njobs;
+    J2K_TRY(e->lens.ensure(ctx, (size_t)(n + 1) * 4));
+    J2K_TRY(e->offs.ensure(ctx, (size_t)(n + 1) * 4));
+    lengths_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>((const j2k_cb_desc*)e->descs.p, (uint32_t*)e->lens.p, n);
+    J2K_CUDA(ctx, cudaMemsetAsync((uint32_t*)e->lens.p + n, 0, 4, ctx->stream));
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, (uint32_t*)e->lens.p, (uint32_t*)e->offs.p, n + 1, ctx->stream);
+    J2K_TRY(e->cubtmp.ensure(ctx, tmp + 16));
+    J2K_CUDA(ctx, cub::DeviceScan::ExclusiveSum(e->cubtmp.p, tmp, (uint32_t*)e->lens.p,
+                                                (uint32_t*)e->offs.p, n + 1, ctx->stream));
+    uint32_t tot = 0;
+    J2K_CUDA(ctx, cudaMemcpyAsync(&tot, (uint32_t*)e->offs.p + n, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    J2K_TRY(e->packed.ensure(ctx, (size_t)tot + 16));
+    pack_kernel<<<(n * 32 + 255) / 256, 256, 0, ctx->stream>>>((const j2k_cb_desc*)e->descs.p,
+                                                               (const uint32_t*)e->offs.p,
+                                                               (const uint8_t*)e->bytes.p,
+                                                               (uint8_t*)e->packed.p, n);
+    J2K_CUDA(ctx, cudaGetLastError());
+    *total = tot;
+    return J2K_OK;
+}
+
+extern "C" {
+
+j2k_status j2k_bpc_encode(j2k_ctx* ctx, const int32_t* coeff, size_t pitch, size_t w, size_t h,
+                          int levels, int cbw, int cbh, j2k_cb_desc* descs, uint8_t* bytes,
+                          size_t cap_per_block) {
+    if (!ctx) return J2K_ERR_INVALID_ARG;
+    if (!coeff || !descs || !bytes || pitch < w || w == 0 || h == 0 || w > 65535 || h > 65535)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_encode: bad pointer/size/pitch");
+    if (levels < 0 || levels > 32 || !valid_cb(cbw) || !valid_cb(cbh) || cbw * cbh > 4096)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_encode: bad levels or code-block size");
+    if (cap_per_block == 0 || cap_per_block % 16)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_encode: cap_per_block must be a positive multiple of 16");
+    cudaSetDevice(ctx->device);
+    std::vector<j2k_cb_job> jobs;
+    j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, 0);
+    j2k_cb_job* dj = (j2k_cb_job*)j2k_scratch(ctx, SCR_JOBS, jobs.size() * sizeof(j2k_cb_job) + 16);
+    if (!dj) return J2K_ERR_OUT_OF_MEMORY;
+    J2K_CUDA(ctx, cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice, ctx->stream));
+    size_t sym_cap = align16((size_t)cbw * cbh * 20 + 256);
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        J2K_TRY(j2k_clear_device_error(ctx));
+        J2K_TRY(j2k_t1_encode_jobs(ctx, coeff, pitch, dj, jobs.size(), descs, bytes, cap_per_block,
+                                   sym_cap, ctx->stream));
+        j2k_status s = j2k_read_device_error(ctx);
+        if (s == J2K_OK) return J2K_OK;
+        if (s == J2K_ERR_CAPACITY && ctx->err.find("symbol") != std::string::npos) {
+            sym_cap = align16(sym_cap * 2);
+            continue;
+        }
+        return s;
+    }
+    return j2k_fail(ctx, J2K_ERR_CAPACITY, "tier-1 symbol capacity kept overflowing");
+}
+
+j2k_status j2k_bpc_decode(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
+                          size_t count, int32_t* coeff, size_t pitch, size_t w, size_t h,
+                          int levels, int cbw, int cbh) {
+    if (!ctx) return J2K_ERR_INVALID_ARG;
+    if (!coeff || !descs || !bytes || pitch < w || w == 0 || h == 0 || w > 65535 || h > 65535)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_decode: bad pointer/size/pitch");
+    if (levels < 0 || levels > 32 || !valid_cb(cbw) || !valid_cb(cbh) || cbw * cbh > 4096)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_decode: bad levels or code-block size");
+    cudaSetDevice(ctx->device);
+    std::vector<j2k_cb_job> jobs;
+    j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, 0);
+    if (jobs.size() != count)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_decode: count does not match the partition");
+    j2k_cb_job* dj = (j2k_cb_job*)j2k_scratch(ctx, SCR_JOBS, jobs.size() * sizeof(j2k_cb_job) + 16);
+    if (!dj) return J2K_ERR_OUT_OF_MEMORY;
+    J2K_CUDA(ctx, cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice, ctx->stream));
+    J2K_TRY(j2k_clear_device_error(ctx));
+    J2K_TRY(j2k_t1_decode_jobs(ctx, descs, bytes, dj, jobs.size(), coeff, pitch, ctx->stream));
+    return j2k_read_device_error(ctx);
+}
+
+j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_encoder** out) {
+    if (!ctx || !out) return J2K_ERR_INVALID_ARG;
+    j2k_encoder* e = new (std::nothrow) j2k_encoder();
+    if (!e) return J2K_ERR_OUT_OF_MEMORY;
+    e->ctx = ctx;
+    e->lossy = lossy ? 1 : 0;
+    e->dwt_only = output_dwt_only ? 1 : 0;
+    *out = e;
+    return J2K_OK;
+}
+
+j2k_status j2k_encoder_destroy(j2k_encoder* e) {
+    if (!e) return J2K_ERR_INVALID_ARG;
+    cudaSetDevice(e->ctx->device);
+    cudaStreamSynchronize(e->ctx->stream);
+    for (DevBuf* b : {&e->in, &e->planes, &e->coef, &e->jobs, &e->descs, &e->bytes, &e->lens, &e->offs,
+                      &e->packed, &e->cubtmp})
+        b->release();
+    if (e->mapped) cudaFreeHost(e->mapped);
+    delete e;
+    return J2K_OK;
+}
+
+static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const j2k_enc_params* p) {
+    j2k_ctx* ctx = e->ctx;
+    int levels, cbw, cbh, order;
+    J2K_TRY(check_params(ctx, p, w, h, &levels, &cbw, &cbh, &order));
+    if (ncomp != 1 && ncomp != 3)
+        return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "encoder supports 1 or 3 components");
+    e->w = w;
+    e->h = h;
+    e->ncomp = ncomp;
+    e->levels = levels;
+    e->cbw = cbw;
+    e->cbh = cbh;
+    e->order = order;
+    e->mct = ncomp >= 3 ? (e->lossy ? J2K_MCT_ICT : J2K_MCT_RCT) : J2K_MCT_NONE;
+    if (e->lossy) {
+        if (p && p->steps) e->steps.assign(p->steps, p->steps + 3 * levels + 1);
+        else e->steps = default_steps(w, h, levels);
+        for (float s : e->steps)
+            if (!(s > 0.0f)) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "quantiser steps must be > 0");
+    } else {
+        e->steps.clear();
+    }
+    J2K_TRY(e->planes.ensure(ctx, w * h * 4 * (size_t)ncomp));
+    e->have_result = false;
+    return J2K_OK;
+}
+
+j2k_status j2k_encoder_run_interleaved(j2k_encoder* e, const uint8_t* pixels, int on_device,
+                                       size_t pitch, int ncomp, size_t w, size_t h,
+                                       const j2k_enc_params* p) {
+    if (!e) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    if (!pixels) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "pixels is NULL");
+    if (pitch == 0) pitch = w * (size_t)ncomp;
+    if (pitch < w * (size_t)ncomp) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "pitch too small");
+    cudaSetDevice(ctx->device);
+    J2K_TRY(setup_run(e, ncomp, w, h, p));
+    const uint8_t* src = pixels;
+    if (!on_device) {
+        J2K_TRY(e->in.ensure(ctx, pitch * h + 16));
+        J2K_CUDA(ctx, cudaMemcpyAsync(e->in.p, pixels, pitch * h, cudaMemcpyHostToDevice, ctx->stream));
+        src = (const uint8_t*)e->in.p;
+    }
+    J2K_TRY(j2k_launch_planar_fwd(ctx, src, pitch, ncomp, e->mct, e->lossy ? J2K_F32 : J2K_I32, e->planes.p,
+                                  w, w * h, w, h, ctx->stream));
+    return encode_planes(e);
+}
+
+j2k_status j2k_encoder_run(j2k_encoder* e, const void* const* comps, int ncomp, int dtype, size_t w,
+                           size_t h, size_t levels, size_t precision, const j2k_enc_params* p) {
+    if (!e) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    if (!comps) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "components is NULL");
+    if (dtype != J2K_I16 && dtype != J2K_I32 && dtype != J2K_F32)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "component dtype must be I16, I32 or F32");
+    if (precision != 8) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "only 8-bit precision is supported");
+    j2k_enc_params q{};
+    if (p) q = *p;
+    q.levels = (int)levels;
+    cudaSetDevice(ctx->device);
+    J2K_TRY(setup_run(e, ncomp, w, h, &q));
+    const size_t n = w * h, esz = dtype == J2K_I16 ? 2 : 4;
+    J2K_TRY(e->in.ensure(ctx, n * esz * ncomp + 16));
+    int pd = e->lossy ? J2K_F32 : J2K_I32;
+    for (int c = 0; c < ncomp; ++c) {
+        if (!comps[c]) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "component pointer is NULL");
+        char* staged = (char*)e->in.p + (size_t)c * n * esz;
+        J2K_CUDA(ctx, cudaMemcpyAsync(staged, comps[c], n * esz, cudaMemcpyHostToDevice, ctx->stream));
+        J2K_TRY(j2k_launch_cast_planes(ctx, staged, dtype, (char*)e->planes.p + (size_t)c * n * 4, pd, n, ctx->stream));
+    }
+    if (e->mct != J2K_MCT_NONE) J2K_TRY(j2k_launch_mct_planes(ctx, e->planes.p, pd, n, n, e->mct, ctx->stream));
+    return encode_planes(e);
+}
+
+j2k_status j2k_encoder_map_dwt_out(j2k_encoder* e, void** ptr, size_t* pitch_bytes) {
+    if (!e || !ptr) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    if (!e->have_result) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no encoder run yet");
+    size_t bytes = e->w * e->h * 4 * e->ncomp;
+    if (!e->mapped) J2K_CUDA(ctx, cudaMallocHost(&e->mapped, bytes));
+    J2K_CUDA(ctx, cudaMemcpyAsync(e->mapped, e->coef.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *ptr = e->mapped;
+    if (pitch_bytes) *pitch_bytes = e->w * 4;
+    return J2K_OK;
+}
+
+j2k_status j2k_encoder_unmap_dwt_out(j2k_encoder* e, void* ptr) {
+    if (!e) return J2K_ERR_INVALID_ARG;
+    if (ptr && ptr == e->mapped) {
+        cudaFreeHost(e->mapped);
+        e->mapped = nullptr;
+    }
+    return J2K_OK;
+}
+
+j2k_status j2k_encoder_get_codeblocks(j2k_encoder* e, j2k_cb_desc* descs, size_t* count,
+                                      uint8_t* bytes, size_t cap, size_t* used) {
+    if (!e || !count) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    if (!e->have_result || e->dwt_only) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no tier-1 result");
+    cudaSetDevice(ctx->device);
+    size_t total = 0;
+    J2K_TRY(pack_blocks(e, &total));
+    if (used) *used = total;
+    if (!descs && !bytes) {
+        *count = e->njobs;
+        return J2K_OK;
+    }
+    if (descs && *count < e->njobs) return j2k_fail(ctx, J2K_ERR_CAPACITY, "descs array too small");
+    if (bytes && cap < total) return j2k_fail(ctx, J2K_ERR_CAPACITY, "bytes buffer too small");
+    *count = e->njobs;
+    if (bytes) J2K_CUDA(ctx, cudaMemcpyAsync(bytes, e->packed.p, total, cudaMemcpyDeviceToHost, ctx->stream));
+    if (descs) {
+        J2K_CUDA(ctx, cudaMemcpyAsync(descs, e->descs.p, e->njobs * sizeof(j2k_cb_desc), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    }
+    J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (descs) {
+        uint32_t acc = 0;
+        for (size_t i = 0; i < e->njobs; ++i) {
+            descs[i].offset = acc;
+            acc += (uint32_t)std::max(descs[i].length, 0);
+        }
+    }
+    return J2K_OK;
+}
+
+j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, size_t* len) {
+    if (!e || !len) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    size_t count = 0, total = 0;
+    J2K_TRY(j2k_encoder_get_codeblocks(e, nullptr, &count, nullptr, 0, &total));
+    std::vector<j2k_cb_desc> d(count);
+    std::vector<uint8_t> b(total + 1);
+    J2K_TRY(j2k_encoder_get_codeblocks(e, d.data(), &count, b.data(), b.size(), &total));
+    std::vector<j2k_t2_block> blocks(count);
+    for (size_t i = 0; i < count; ++i)
+        blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, b.data() + d[i].offset};
+    std::vector<uint8_t> cs = j2k_t2_write(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
+                                           e->mct != J2K_MCT_NONE, e->steps.data(), blocks);
+    *len = cs.size();
+    if (!out) return J2K_OK;
+    if (cap < cs.size()) return j2k_fail(ctx, J2K_ERR_CAPACITY, "codestream buffer too small");
+    std::memcpy(out, cs.data(), cs.size());
+    return J2K_OK;
+}
+
+j2k_status j2k_encoder_device_results(j2k_encoder* e, const j2k_cb_desc** descs, const uint8_t** bytes,
+                                      size_t* count, size_t* cap_per_block) {
+    if (!e) return J2K_ERR_INVALID_ARG;
+    if (!e->have_result || e->dwt_only) return j2k_fail(e->ctx, J2K_ERR_INVALID_ARG, "no tier-1 result");
+    if (descs) *descs = (const j2k_cb_desc*)e->descs.p;
+    if (bytes) *bytes = (const uint8_t*)e->bytes.p;
+    if (count) *count = e->njobs;
+    if (cap_per_block) *cap_per_block = e->cap;
+    return J2K_OK;
+}
+
+j2k_status j2k_decoder_create(j2k_ctx* ctx, int lossy, j2k_decoder** out) {
+    if (!ctx || !out) return J2K_ERR_INVALID_ARG;
+    j2k_decoder* d = new (std::nothrow) j2k_decoder();
+    if (!d) return J2K_ERR_OUT_OF_MEMORY;
+    d->ctx = ctx;
+    d->lossy = lossy ? 1 : 0;
+    *out = d;
+    return J2K_OK;
+}
+
+j2k_status j2k_decoder_destroy(j2k_decoder* d) {
+    if (!d) return J2K_ERR_INVALID_ARG;
+    cudaSetDevice(d->ctx->device);
+    cudaStreamSynchronize(d->ctx->stream);
+    for (DevBuf* b : {&d->descs, &d->bytes, &d->coef, &d->planes, &d->out, &d->jobs}) b->release();
+    delete d;
+    return J2K_OK;
+}
+
+j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, const uint8_t* bytes,
+                                      size_t nbytes, int on_device, int ncomp, size_t w, size_t h,
+                                      const j2k_enc_params* p, uint8_t* out, int out_on_device,
+                                      size_t out_pitch) {
+    if (!d) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = d->ctx;
+    if (!descs || !bytes || !out) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "NULL pointer");
+    if (ncomp != 1 && ncomp != 3) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "decoder supports 1 or 3 components");
+    int levels, cbw, cbh, order;
+    J2K_TRY(check_params(ctx, p, w, h, &levels, &cbw, &cbh, &order));
+    if (out_pitch == 0) out_pitch = w * (size_t)ncomp;
+    cudaSetDevice(ctx->device);
+    size_t njobs = 0;
+    J2K_TRY(prepare_jobs(ctx, d->hjobs, d->jobs, d->job_key, w, h, ncomp, levels, cbw, cbh, &njobs));
+    const j2k_cb_desc* dd = descs;
+    const uint8_t* db = bytes;
+    if (!on_device) {
+        J2K_TRY(d->descs.ensure(ctx, njobs * sizeof(j2k_cb_desc) + 16));
+        J2K_TRY(d->bytes.ensure(ctx, nbytes + 16));
+        J2K_CUDA(ctx, cudaMemcpyAsync(d->descs.p, descs, njobs * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));
+        J2K_CUDA(ctx, cudaMemcpyAsync(d->bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, ctx->stream));
+        dd = (const j2k_cb_desc*)d->descs.p;
+        db = (const uint8_t*)d->bytes.p;
+    }
+    const size_t n = w * h;
+    J2K_TRY(d->coef.ensure(ctx, n * 4 * ncomp));
+    J2K_TRY(d->planes.ensure(ctx, n * 4 * ncomp));
+    J2K_TRY(j2k_clear_device_error(ctx));
+    J2K_TRY(j2k_t1_decode_jobs(ctx, dd, db, (const j2k_cb_job*)d->jobs.p, njobs, (int32_t*)d->coef.p, w, ctx->stream));
+    std::vector<float> steps;
+    if (d->lossy) {
+        if (p && p->steps) steps.assign(p->steps, p->steps + 3 * levels + 1);
+        else steps = default_steps(w, h, levels);
+    }
+    size_t w1 = (w + 1) / 2, h1 = (h + 1) / 2, w2 = (w1 + 1) / 2, h2 = (h1 + 1) / 2;
+    void* ll0 = j2k_scratch(ctx, SCR_LL0, w1 * h1 * 4);
+    void* ll1 = j2k_scratch(ctx, SCR_LL1, w2 * h2 * 4);
+    if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
+    for (int c = 0; c < ncomp; ++c) {
+        J2K_TRY(j2k_dwt_inv_impl(ctx, d->lossy ? J2K_W97 : J2K_W53, d->lossy ? J2K_ORDER_T800 : order,
+                                 (const char*)d->coef.p + (size_t)c * n * 4, w,
+                                 (char*)d->planes.p + (size_t)c * n * 4, w, w, h, levels,
+                                 d->lossy ? steps.data() : nullptr, ll0, ll1, j2k_dwt_tile{64, 64}, ctx->stream));
+    }
+    int mct = ncomp >= 3 ? (d->lossy ? J2K_MCT_ICT : J2K_MCT_RCT) : J2K_MCT_NONE;
+    uint8_t* dst = out;
+    if (!out_on_device) {
+        J2K_TRY(d->out.ensure(ctx, out_pitch * h + 16));
+        dst = (uint8_t*)d->out.p;
+    }
+    J2K_TRY(j2k_launch_planar_inv(ctx, d->planes.p, d->lossy ? J2K_F32 : J2K_I32, w, n, ncomp, mct, dst,
+                                  out_pitch, w, h, ctx->stream));
+    if (!out_on_device)
+        J2K_CUDA(ctx, cudaMemcpyAsync(out, dst, out_pitch * h, cudaMemcpyDeviceToHost, ctx->stream));
+    return j2k_read_device_error(ctx);
+}
+
+}  // extern "C"

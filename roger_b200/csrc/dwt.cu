@@ -1,0 +1,431 @@
+// Forward and inverse 2-D lifting DWT, reversible 5/3 (int32) and irreversible 9/7 (fp32),
+// one launch per decomposition level, Mallat output.
+//
+// Reference: src/CL/ocldwt53.cl:167-292 (5/3, rows in registers then columns in local memory,
+// whole-sample symmetric extension through a MIRRORED_REPEAT sampler, :86) and
+// src/CL/ocldwt97.cl:196-420 / :487-716 (9/7 with fused "quantisation"), level recursion
+// src/OCLDWTForward.cpp:124-137.  Differences by design:
+//   * each CTA stages a (TW+2H) x (TH+2H) tile (H = 2 for 5/3, 4 for 9/7) in shared memory,
+//     extension is done by mirroring the load coordinates (parity preserving), and every lifting
+//     step of both axes runs in shared memory with the tile shrinking by one sample per step;
+//   * the row/column order is a template parameter: J2K_ORDER_REF (rows first, the reference)
+//     or J2K_ORDER_T800 (columns first, T.800 F.4.2);
+//   * odd sizes follow T.800 (ceil(n/2) low samples; a 1-sample axis is left untransformed);
+//   * 9/7 arithmetic is the reference's horizontal pipeline order (ocldwt97.cl:248-310:
+//     x + c*(left+right), then low*1/K, high*K after each 1-D pass) with every operation
+//     rounded separately, which makes it bit-comparable with the CPU oracle;
+//   * the dead-zone quantiser (T.800 E.1) is fused into the writes of the final subbands; the
+//     inverse fuses the midpoint dequantiser into its loads.
+// HBM roofline per level: read c*n + write c*n bytes (c = 4), n = samples of the level.
+#include "j2k_internal.cuh"
+
+namespace {
+
+constexpr float P1 = -1.586134342f, U1 = -0.05298011854f, P2 = 0.8829110762f, U2 = 0.4435068522f;
+constexpr float KMUL = 1.23017410491400f, KDIV = 0.81289306611596153187273657637352f;
+
+__device__ __forceinline__ int mirror(int i, int n) {
+    if (n == 1) return 0;
+    while (i < 0 || i >= n) {
+        if (i < 0) i = -i;
+        if (i >= n) i = 2 * (n - 1) - i;
+    }
+    return i;
+}
+
+template <int KERN> struct KT;
+template <> struct KT<53> {
+    using T = int32_t;
+    static constexpr int H = 2, NSTEP = 2;
+    __device__ static int par(bool inv, int s) { return inv ? (s & 1) : 1 - (s & 1); }
+    __device__ static T op(bool inv, int s, T x, T a, T b) {
+        if (!inv) return s == 0 ? x - ((a + b) >> 1) : x + ((a + b + 2) >> 2);
+        return s == 0 ? x - ((a + b + 2) >> 2) : x + ((a + b) >> 1);
+    }
+};
+template <> struct KT<97> {
+    using T = float;
+    static constexpr int H = 4, NSTEP = 4;
+    __device__ static int par(bool inv, int s) { return inv ? (s & 1) : 1 - (s & 1); }
+    __device__ static T op(bool inv, int s, T x, T a, T b) {
+        float c;
+        if (!inv) c = s == 0 ? P1 : (s == 1 ? U1 : (s == 2 ? P2 : U2));
+        else c = s == 0 ? -U2 : (s == 1 ? -P2 : (s == 2 ? -U1 : -P1));
+        return __fadd_rn(x, __fmul_rn(c, __fadd_rn(a, b)));
+    }
+};
+
+// Shared tile geometry
+template <int KERN, int TW, int TH>
+struct Tile {
+    static constexpr int H = KT<KERN>::H;
+    static constexpr int NX = TW + 2 * H, NY = TH + 2 * H;
+    static constexpr int S = NX + 1;  // odd stride: column sweeps hit distinct banks
+};
+
+// One lifting step along columns (vertical): rows of the step's parity in
+// [STEP+1, NY-STEP-1), columns [C0, C1).  All bounds are compile-time constants.
+template <int KERN, int TW, int TH, bool INV, int STEP, int C0, int C1>
+__device__ __forceinline__ void vstep(typename KT<KERN>::T* s) {
+    using G = Tile<KERN, TW, TH>;
+    constexpr int PAR = INV ? (STEP & 1) : 1 - (STEP & 1);
+    constexpr int LO = STEP + 1, HI = G::NY - STEP - 1;
+    constexpr int FIRST = LO + ((LO & 1) != PAR);
+    constexpr int NR = FIRST < HI ? (HI - FIRST + 1) / 2 : 0;
+    constexpr int NCOL = C1 - C0;
+    for (int e = threadIdx.x; e < NR * NCOL; e += blockDim.x) {
+        int r = FIRST + 2 * (e / NCOL), c = C0 + e % NCOL;
+        auto* p = s + r * G::S + c;
+        *p = KT<KERN>::op(INV, STEP, *p, p[-G::S], p[G::S]);
+    }
+}
+
+// One lifting step along rows (horizontal): columns of the step's parity, rows [R0, R1).
+template <int KERN, int TW, int TH, bool INV, int STEP, int R0, int R1>
+__device__ __forceinline__ void hstep(typename KT<KERN>::T* s) {
+    using G = Tile<KERN, TW, TH>;
+    constexpr int PAR = INV ? (STEP & 1) : 1 - (STEP & 1);
+    constexpr int LO = STEP + 1, HI = G::NX - STEP - 1;
+    constexpr int FIRST = LO + ((LO & 1) != PAR);
+    constexpr int NC = FIRST < HI ? (HI - FIRST + 1) / 2 : 0;
+    constexpr int NROW = R1 - R0;
+    for (int e = threadIdx.x; e < NROW * NC; e += blockDim.x) {
+        int c = FIRST + 2 * (e % NC), r = R0 + e / NC;
+        auto* p = s + r * G::S + c;
+        *p = KT<KERN>::op(INV, STEP, *p, p[-1], p[1]);
+    }
+}
+
+template <int KERN, int TW, int TH, bool INV, int C0, int C1, int K = 0>
+__device__ __forceinline__ void vsteps(typename KT<KERN>::T* s) {
+    if constexpr (K < KT<KERN>::NSTEP) {
+        vstep<KERN, TW, TH, INV, K, C0, C1>(s);
+        __syncthreads();
+        vsteps<KERN, TW, TH, INV, C0, C1, K + 1>(s);
+    }
+}
+template <int KERN, int TW, int TH, bool INV, int R0, int R1, int K = 0>
+__device__ __forceinline__ void hsteps(typename KT<KERN>::T* s) {
+    if constexpr (K < KT<KERN>::NSTEP) {
+        hstep<KERN, TW, TH, INV, K, R0, R1>(s);
+        __syncthreads();
+        hsteps<KERN, TW, TH, INV, R0, R1, K + 1>(s);
+    }
+}
+
+// 9/7 scaling sweeps (forward: low*KDIV, high*KMUL; inverse: low*KMUL, high*KDIV).
+// VERT: factor by row parity, else by column parity.  Region [C0,C1) x [R0,R1).
+template <int KERN, int TW, int TH, bool INV, bool VERT, int C0, int C1, int R0, int R1>
+__device__ __forceinline__ void scale97(typename KT<KERN>::T* s) {
+    if constexpr (KERN == 97) {
+        using G = Tile<KERN, TW, TH>;
+        constexpr int NCOL = C1 - C0, N = (R1 - R0) * NCOL;
+        for (int e = threadIdx.x; e < N; e += blockDim.x) {
+            int r = R0 + e / NCOL, c = C0 + e % NCOL;
+            int odd = VERT ? (r & 1) : (c & 1);
+            float f = odd ? (INV ? KDIV : KMUL) : (INV ? KMUL : KDIV);
+            s[r * G::S + c] = __fmul_rn(s[r * G::S + c], f);
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int32_t quantize(float v, float step) {
+    int32_t m = (int32_t)floorf(__fdiv_rn(fabsf(v), step));
+    return v < 0.0f ? -m : m;
+}
+__device__ __forceinline__ float dequantize(int32_t q, float step) {
+    int32_t m = q < 0 ? -q : q;
+    float r = m ? __fmul_rn(__fadd_rn((float)m, 0.5f), step) : 0.0f;
+    return q < 0 ? -r : r;
+}
+
+struct Steps4 { float ll, hl, lh, hh; };
+
+// ---- forward level ----------------------------------------------------------------------------
+// src: level input (w x h).  Detail subbands go to dst at Mallat positions (dst is the full
+// output plane); LL goes to ll_dst (T) unless QLL, in which case it is quantised into dst.
+template <int KERN, int ORDER, int TW, int TH, typename TD, bool QUANT, bool QLL>
+__global__ void __launch_bounds__(256)
+dwt_fwd_level(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
+              typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst,
+              size_t dpitch, Steps4 st) {
+    using T = typename KT<KERN>::T;
+    using G = Tile<KERN, TW, TH>;
+    constexpr int H = G::H;
+    __shared__ T s[G::NY * G::S];
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    for (int e = threadIdx.x; e < G::NX * G::NY; e += blockDim.x) {
+        int r = e / G::NX, c = e % G::NX;
+        int gy = mirror(y0 - H + r, h), gx = mirror(x0 - H + c, w);
+        s[r * G::S + c] = src[(size_t)gy * spitch + gx];
+    }
+    __syncthreads();
+    const bool dov = h > 1, doh = w > 1;
+    if (ORDER == J2K_ORDER_T800) {
+        if (dov) {
+            vsteps<KERN, TW, TH, false, 0, G::NX>(s);
+            scale97<KERN, TW, TH, false, true, 0, G::NX, H, H + TH>(s);
+        }
+        if (doh) hsteps<KERN, TW, TH, false, H, H + TH>(s);
+    } else {
+        if (doh) {
+            hsteps<KERN, TW, TH, false, 0, G::NY>(s);
+            scale97<KERN, TW, TH, false, false, H, H + TW, 0, G::NY>(s);
+        }
+        if (dov) vsteps<KERN, TW, TH, false, H, H + TW>(s);
+    }
+    // write the four subbands; the second pass's scaling is applied here
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    constexpr int SW = TW / 2, SH = TH / 2;
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        const int qx = q & 1, qy = q >> 1;
+        float f = 1.0f;
+        if (KERN == 97) {
+            if (ORDER == J2K_ORDER_T800) f = doh ? (qx ? KMUL : KDIV) : 1.0f;
+            else f = dov ? (qy ? KMUL : KDIV) : 1.0f;
+        }
+        const float step = q == 0 ? st.ll : (q == 1 ? st.hl : (q == 2 ? st.lh : st.hh));
+        for (int e = threadIdx.x; e < SW * SH; e += blockDim.x) {
+            int i = e % SW, j = e / SW;
+            int x = x0 + 2 * i + qx, y = y0 + 2 * j + qy;
+            if (x >= w || y >= h) continue;
+            T v = s[(H + 2 * j + qy) * G::S + H + 2 * i + qx];
+            if (KERN == 97) v = (T)__fmul_rn((float)v, f);
+            int sx = (x >> 1) + (qx ? wl : 0), sy = (y >> 1) + (qy ? hl : 0);
+            if (q == 0 && !QLL) {
+                ll_dst[(size_t)sy * llpitch + sx] = v;
+            } else if (QUANT) {
+                dst[(size_t)sy * dpitch + sx] = (TD)quantize((float)v, step);
+            } else {
+                dst[(size_t)sy * dpitch + sx] = (TD)v;
+            }
+        }
+    }
+}
+
+// ---- inverse level ----------------------------------------------------------------------------
+// Reconstructs the w x h region of level k-1 from the detail subbands of `src` (Mallat plane,
+// optionally int32 indices when DEQ) and the LL band (ll_src, or src itself when DEQLL).
+template <int KERN, int ORDER, int TW, int TH, typename TS, bool DEQ, bool DEQLL>
+__global__ void __launch_bounds__(256)
+dwt_inv_level(const TS* __restrict__ src, size_t spitch,
+              const typename KT<KERN>::T* __restrict__ ll_src, size_t llpitch, int w, int h,
+              typename KT<KERN>::T* __restrict__ out, size_t opitch, Steps4 st) {
+    using T = typename KT<KERN>::T;
+    using G = Tile<KERN, TW, TH>;
+    constexpr int H = G::H;
+    __shared__ T s[G::NY * G::S];
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    for (int e = threadIdx.x; e < G::NX * G::NY; e += blockDim.x) {
+        int r = e / G::NX, c = e % G::NX;
+        int gy = mirror(y0 - H + r, h), gx = mirror(x0 - H + c, w);
+        int qx = gx & 1, qy = gy & 1;
+        int sx = (gx >> 1) + (qx ? wl : 0), sy = (gy >> 1) + (qy ? hl : 0);
+        T v;
+        if (!qx && !qy) {
+            if (DEQLL) v = (T)dequantize((int32_t)src[(size_t)sy * spitch + sx], st.ll);
+            else v = ll_src[(size_t)sy * llpitch + sx];
+        } else {
+            TS raw = src[(size_t)sy * spitch + sx];
+            if (DEQ) v = (T)dequantize((int32_t)raw, qx && qy ? st.hh : (qx ? st.hl : st.lh));
+            else v = (T)raw;
+        }
+        s[r * G::S + c] = v;
+    }
+    __syncthreads();
+    const bool dov = h > 1, doh = w > 1;
+    if (ORDER == J2K_ORDER_T800) {
+        // undo rows first (all rows of the tile are needed by the column pass)
+        if (doh) {
+            scale97<KERN, TW, TH, true, false, 0, G::NX, 0, G::NY>(s);
+            hsteps<KERN, TW, TH, true, 0, G::NY>(s);
+        }
+        if (dov) {
+            scale97<KERN, TW, TH, true, true, H, H + TW, 0, G::NY>(s);
+            vsteps<KERN, TW, TH, true, H, H + TW>(s);
+        }
+    } else {
+        if (dov) {
+            scale97<KERN, TW, TH, true, true, 0, G::NX, 0, G::NY>(s);
+            vsteps<KERN, TW, TH, true, 0, G::NX>(s);
+        }
+        if (doh) {
+            scale97<KERN, TW, TH, true, false, 0, G::NX, H, H + TH>(s);
+            hsteps<KERN, TW, TH, true, H, H + TH>(s);
+        }
+    }
+    for (int e = threadIdx.x; e < TW * TH; e += blockDim.x) {
+        int i = e % TW, j = e / TW;
+        int x = x0 + i, y = y0 + j;
+        if (x < w && y < h) out[(size_t)y * opitch + x] = s[(H + j) * G::S + H + i];
+    }
+}
+
+// levels == 0: plain copy, or quantisation of the single LL band
+template <typename TI, typename TO, bool Q>
+__global__ void copy_plane(const TI* __restrict__ in, size_t ip, TO* __restrict__ out, size_t op,
+                           int w, int h, float step) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    TI v = in[(size_t)y * ip + x];
+    if (Q) out[(size_t)y * op + x] = (TO)quantize((float)v, step);
+    else out[(size_t)y * op + x] = (TO)v;
+}
+template <typename TI, typename TO, bool DQ>
+__global__ void copy_plane_deq(const TI* __restrict__ in, size_t ip, TO* __restrict__ out,
+                               size_t op, int w, int h, float step) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    TI v = in[(size_t)y * ip + x];
+    if (DQ) out[(size_t)y * op + x] = (TO)dequantize((int32_t)v, step);
+    else out[(size_t)y * op + x] = (TO)v;
+}
+
+template <int KERN, int ORDER, int TW, int TH>
+j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, size_t out_pitch,
+                      int w, int h, int levels, const float* steps, void* ll0, void* ll1,
+                      cudaStream_t stream) {
+    using T = typename KT<KERN>::T;
+    const bool quant = (KERN == 97) && steps != nullptr;
+    if (levels == 0) {
+        dim3 g((w + 255) / 256, h);
+        if (quant)
+            copy_plane<float, int32_t, true><<<g, 256, 0, stream>>>((const float*)in, in_pitch, (int32_t*)out, out_pitch, w, h, steps[0]);
+        else
+            copy_plane<T, T, false><<<g, 256, 0, stream>>>((const T*)in, in_pitch, (T*)out, out_pitch, w, h, 1.0f);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    int cw = w, chh = h;
+    const T* src = (const T*)in;
+    size_t spitch = in_pitch;
+    for (int k = 0; k < levels; ++k) {
+        bool last = (k == levels - 1);
+        dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH);
+        T* lld;
+        size_t llp;
+        if (last) {
+            lld = (T*)out;
+            llp = out_pitch;
+        } else {
+            int nw = (cw + 1) / 2;
+            lld = (T*)((k % 2 == 0) ? ll0 : ll1);
+            llp = (size_t)nw;
+        }
+        // subband indices of this level in QCD order: level L-k's triple
+        int dl = k + 1;  // decomposition level produced
+        int bt = 1 + 3 * (levels - dl);
+        Steps4 st{1.f, 1.f, 1.f, 1.f};
+        if (quant) st = Steps4{steps[0], steps[bt], steps[bt + 1], steps[bt + 2]};
+        if (quant) {
+            if (last)
+                dwt_fwd_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st);
+            else
+                dwt_fwd_level<KERN, ORDER, TW, TH, int32_t, true, false><<<grid, 256, 0, stream>>>(
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st);
+        } else {
+            dwt_fwd_level<KERN, ORDER, TW, TH, T, false, false><<<grid, 256, 0, stream>>>(
+                src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st);
+        }
+        J2K_CUDA(ctx, cudaGetLastError());
+        src = lld;
+        spitch = llp;
+        cw = (cw + 1) / 2;
+        chh = (chh + 1) / 2;
+    }
+    return J2K_OK;
+}
+
+template <int KERN, int ORDER, int TW, int TH>
+j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, size_t out_pitch,
+                      int w, int h, int levels, const float* steps, void* ll0, void* ll1,
+                      cudaStream_t stream) {
+    using T = typename KT<KERN>::T;
+    const bool deq = (KERN == 97) && steps != nullptr;
+    if (levels == 0) {
+        dim3 g((w + 255) / 256, h);
+        if (deq)
+            copy_plane_deq<int32_t, float, true><<<g, 256, 0, stream>>>((const int32_t*)in, in_pitch, (float*)out, out_pitch, w, h, steps[0]);
+        else
+            copy_plane_deq<T, T, false><<<g, 256, 0, stream>>>((const T*)in, in_pitch, (T*)out, out_pitch, w, h, 1.0f);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    int ws[40], hs[40];
+    ws[0] = w;
+    hs[0] = h;
+    for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
+    for (int k = levels - 1; k >= 0; --k) {
+        int cw = ws[k], chh = hs[k];
+        dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH);
+        T* o = (k == 0) ? (T*)out : (T*)((k % 2 == 1) ? ll0 : ll1);
+        size_t op = (k == 0) ? out_pitch : (size_t)cw;
+        const T* lls = (k == levels - 1) ? (const T*)in : (const T*)((k % 2 == 1) ? ll1 : ll0);
+        size_t llp = (k == levels - 1) ? in_pitch : (size_t)ws[k + 1];
+        int bt = 1 + 3 * (levels - (k + 1));
+        Steps4 st{1.f, 1.f, 1.f, 1.f};
+        if (deq) st = Steps4{steps[0], steps[bt], steps[bt + 1], steps[bt + 2]};
+        if (deq) {
+            if (k == levels - 1)
+                dwt_inv_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(
+                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st);
+            else
+                dwt_inv_level<KERN, ORDER, TW, TH, int32_t, true, false><<<grid, 256, 0, stream>>>(
+                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st);
+        } else {
+            dwt_inv_level<KERN, ORDER, TW, TH, T, false, false><<<grid, 256, 0, stream>>>(
+                (const T*)in, in_pitch, lls, llp, cw, chh, o, op, st);
+        }
+        J2K_CUDA(ctx, cudaGetLastError());
+    }
+    return J2K_OK;
+}
+
+template <int KERN, int TW, int TH>
+j2k_status fwd_dispatch_order(j2k_ctx* ctx, int order, const void* in, size_t ip, void* out,
+                              size_t op, int w, int h, int levels, const float* steps, void* a,
+                              void* b, cudaStream_t st) {
+    if (order == J2K_ORDER_REF) return fwd_levels<KERN, J2K_ORDER_REF, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
+    return fwd_levels<KERN, J2K_ORDER_T800, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
+}
+template <int KERN, int TW, int TH>
+j2k_status inv_dispatch_order(j2k_ctx* ctx, int order, const void* in, size_t ip, void* out,
+                              size_t op, int w, int h, int levels, const float* steps, void* a,
+                              void* b, cudaStream_t st) {
+    if (order == J2K_ORDER_REF) return inv_levels<KERN, J2K_ORDER_REF, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
+    return inv_levels<KERN, J2K_ORDER_T800, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
+}
+
+}  // namespace
+
+// Tile shapes offered to callers (and the autotuner): 64x64, 128x32, 32x128 (input samples).
+#define J2K_TILE_DISPATCH(FN, KERN, ...)                                                      \
+    (tile.tw == 128 && tile.th == 32)   ? FN<KERN, 128, 32>(__VA_ARGS__)                      \
+    : (tile.tw == 32 && tile.th == 128) ? FN<KERN, 32, 128>(__VA_ARGS__)                      \
+                                        : FN<KERN, 64, 64>(__VA_ARGS__)
+
+j2k_status j2k_dwt_fwd_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
+                            const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
+                            cudaStream_t st) {
+    if (kernel == J2K_W53)
+        return J2K_TILE_DISPATCH(fwd_dispatch_order, 53, ctx, order, in, in_pitch, out, out_pitch,
+                                 (int)w, (int)h, levels, steps, ll0, ll1, st);
+    return J2K_TILE_DISPATCH(fwd_dispatch_order, 97, ctx, order, in, in_pitch, out, out_pitch,
+                             (int)w, (int)h, levels, steps, ll0, ll1, st);
+}
+
+j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
+                            const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
+                            cudaStream_t st) {
+    if (kernel == J2K_W53)
+        return J2K_TILE_DISPATCH(inv_dispatch_order, 53, ctx, order, in, in_pitch, out, out_pitch,
+                                 (int)w, (int)h, levels, steps, ll0, ll1, st);
+    return J2K_TILE_DISPATCH(inv_dispatch_order, 97, ctx, order, in, in_pitch, out, out_pitch,
+                             (int)w, (int)h, levels, steps, ll0, ll1, st);
+}

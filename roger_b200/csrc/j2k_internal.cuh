@@ -1,0 +1,110 @@
+// Internal declarations shared by the CUDA translation units of libj2kb200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "j2k_b200.h"
+
+// Device error word values (written by kernels, read back by the host; kernels never trap).
+enum : uint32_t {
+    J2K_DEVERR_NONE = 0,
+    J2K_DEVERR_SYM_CAPACITY = 1,  // symbol buffer of a code-block full
+    J2K_DEVERR_OUT_CAPACITY = 2,  // codeword buffer of a code-block full
+    J2K_DEVERR_BAD_JOB = 3,       // malformed code-block descriptor
+    J2K_DEVERR_TIMEOUT = 4,       // bounded wait expired
+    J2K_DEVERR_PLANES = 5,        // more magnitude bit-planes than the coder supports
+};
+
+struct j2k_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // grow-only device scratch slots (each independently sized)
+    void* scratch[8] = {};
+    size_t scratch_size[8] = {};
+    uint32_t* d_err = nullptr;   // device error word
+    void* h_pinned = nullptr;    // pinned staging
+    size_t h_pinned_size = 0;
+    int sm_count = 148;
+};
+
+// scratch slot ids
+enum { SCR_LL0 = 0, SCR_LL1 = 1, SCR_JOBS = 2, SCR_SYMS = 3, SCR_T1STATE = 4, SCR_MISC = 5,
+       SCR_PLANES = 6, SCR_MISC2 = 7 };
+
+j2k_status j2k_fail(j2k_ctx* ctx, j2k_status s, const std::string& msg);
+j2k_status j2k_cuda_check(j2k_ctx* ctx, cudaError_t e, const char* what);
+void* j2k_scratch(j2k_ctx* ctx, int slot, size_t bytes);  // nullptr on failure (error set)
+void* j2k_pinned(j2k_ctx* ctx, size_t bytes);
+j2k_status j2k_read_device_error(j2k_ctx* ctx);             // syncs the stream
+j2k_status j2k_clear_device_error(j2k_ctx* ctx);
+
+#define J2K_TRY(x)                              \
+    do {                                        \
+        j2k_status _s = (x);                    \
+        if (_s != J2K_OK) return _s;            \
+    } while (0)
+#define J2K_CUDA(ctx, call) J2K_TRY(j2k_cuda_check((ctx), (call), #call))
+
+// ---- geometry -------------------------------------------------------------------------------
+struct j2k_band_rect {
+    size_t x0, y0, w, h;
+    int orient, level;
+};
+int j2k_band_rects(size_t w, size_t h, int levels, j2k_band_rect* out);  // returns 3L+1
+
+// code-block job for the tier-1 kernels (device side)
+struct j2k_cb_job {
+    uint32_t x0, y0;   // position in the (component-stacked) coefficient plane
+    uint16_t cw, ch;
+    uint8_t orient, band;
+    uint16_t comp;
+    uint16_t px0, py0; // position within the component's Mallat plane
+};
+// Appends the jobs of one component plane (rows comp*h.. of a stacked plane) to *jobs.
+size_t j2k_build_jobs(size_t w, size_t h, int levels, int cbw, int cbh, std::vector<j2k_cb_job>* jobs,
+                      int comp = 0);
+
+// ---- launchers (defined in the .cu files) ---------------------------------------------------
+j2k_status j2k_launch_planar_fwd(j2k_ctx* ctx, const uint8_t* in, size_t in_pitch, int ncomp,
+                                 int mct, int out_dtype, void* planes, size_t plane_pitch,
+                                 size_t plane_stride, size_t w, size_t h, cudaStream_t st);
+j2k_status j2k_launch_planar_inv(j2k_ctx* ctx, const void* planes, int in_dtype,
+                                 size_t plane_pitch, size_t plane_stride, int ncomp, int mct,
+                                 uint8_t* out, size_t out_pitch, size_t w, size_t h,
+                                 cudaStream_t st);
+j2k_status j2k_launch_cast_planes(j2k_ctx* ctx, const void* src, int src_dtype, void* dst,
+                                  int dst_dtype, size_t n, cudaStream_t st);
+j2k_status j2k_launch_mct_planes(j2k_ctx* ctx, void* planes, int dtype, size_t plane_stride,
+                                 size_t n, int mct, cudaStream_t st);
+
+struct j2k_dwt_tile { int tw, th; };
+j2k_status j2k_dwt_fwd_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
+                            const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
+                            cudaStream_t st);
+j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
+                            const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
+                            cudaStream_t st);
+
+j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
+                              const j2k_cb_job* d_jobs, size_t njobs, j2k_cb_desc* descs,
+                              uint8_t* bytes, size_t cap_per_block, size_t sym_cap_per_block,
+                              cudaStream_t st);
+j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
+                              const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
+                              size_t pitch, cudaStream_t st);
+
+// host tier-2 writer
+struct j2k_t2_block {
+    int numbps, npasses, length;
+    const uint8_t* data;
+};
+std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
+                                  int lossless, int mct, const float* steps,
+                                  const std::vector<j2k_t2_block>& blocks);

@@ -1,0 +1,272 @@
+// EBCOT tier-1 decoder (T.800 Annex D context modelling + Annex C.3 MQ decoder).
+//
+// The reference has no decoder for this stage (src/OCLDecoder.cpp:35-38 runs only the "reverse"
+// DWT).  Decoding is serial per code-block (every context depends on the bits decoded before
+// it), so one warp takes one block: lane 0 runs the MQ decoder and the context logic on 64-bit
+// row masks of significance / sign / refined / visited in shared memory, the whole warp clears
+// the output region first and applies the signs at the end.  Magnitude bits are accumulated in
+// the output plane itself (each block owns its region).
+#include "j2k_internal.cuh"
+
+namespace {
+
+constexpr int kWarps = 4;
+
+__constant__ uint16_t d_qe[47] = {
+    0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801, 0x3001, 0x2401,
+    0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401, 0x3001, 0x2801, 0x2401, 0x2201,
+    0x1C01, 0x1801, 0x1601, 0x1401, 0x1201, 0x1101, 0x0AC1, 0x09C1, 0x08A1, 0x0521, 0x0441, 0x02A1,
+    0x0221, 0x0141, 0x0111, 0x0085, 0x0049, 0x0025, 0x0015, 0x0009, 0x0005, 0x0001, 0x5601};
+__constant__ uint8_t d_nmps[47] = {1,  2,  3,  4,  5,  38, 7,  8,  9,  10, 11, 12, 13, 29, 15, 16,
+                                   17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32,
+                                   33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 44, 45, 45, 46};
+__constant__ uint8_t d_nlps[47] = {1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 18, 20, 21, 14, 14,
+                                   15, 16, 17, 18, 19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29,
+                                   30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
+
+__device__ __forceinline__ int zc_label_calc(int orient, int h, int v, int d) {
+    if (orient == J2K_BAND_HH) {
+        int hv = h + v;
+        if (d >= 3) return 8;
+        if (d == 2) return hv >= 1 ? 7 : 6;
+        if (d == 1) return hv >= 2 ? 5 : (hv == 1 ? 4 : 3);
+        return hv >= 2 ? 2 : (hv == 1 ? 1 : 0);
+    }
+    if (orient == J2K_BAND_HL) { int t = h; h = v; v = t; }
+    if (h == 2) return 8;
+    if (h == 1) return v >= 1 ? 7 : (d >= 1 ? 6 : 5);
+    if (v == 2) return 4;
+    if (v == 1) return 3;
+    return d >= 2 ? 2 : d;
+}
+
+struct DecSmem {
+    uint64_t sig[66], neg[66], ref[66], vis[66];
+    uint8_t st[19];
+};
+
+struct Mqd {
+    const uint8_t* data;
+    int len, bp, CT;
+    uint32_t A, C;
+    __device__ uint32_t byte(int i) const { return i < len ? data[i] : 0xFFu; }
+    __device__ void bytein() {
+        if (byte(bp) == 0xFF) {
+            if (byte(bp + 1) > 0x8F) {
+                C += 0xFF00;
+                CT = 8;
+            } else {
+                ++bp;
+                C += byte(bp) << 9;
+                CT = 7;
+            }
+        } else {
+            ++bp;
+            C += byte(bp) << 8;
+            CT = 8;
+        }
+    }
+    __device__ void init(const uint8_t* d, int n) {
+        data = d;
+        len = n;
+        bp = 0;
+        C = byte(0) << 16;
+        bytein();
+        C <<= 7;
+        CT -= 7;
+        A = 0x8000;
+    }
+    __device__ int decode(uint8_t* st, int cx) {
+        int sv = st[cx], idx = sv >> 1, mps = sv & 1;
+        uint32_t qe = d_qe[idx];
+        int D;
+        A -= qe;
+        if ((C >> 16) < qe) {
+            if (A < qe) {
+                A = qe;
+                D = mps;
+                idx = d_nmps[idx];
+            } else {
+                A = qe;
+                D = 1 - mps;
+                if (idx == 0 || idx == 6 || idx == 14) mps ^= 1;
+                idx = d_nlps[idx];
+            }
+            st[cx] = (uint8_t)((idx << 1) | mps);
+            do {
+                if (CT == 0) bytein();
+                A <<= 1;
+                C <<= 1;
+                --CT;
+            } while (!(A & 0x8000));
+        } else {
+            C -= qe << 16;
+            if (!(A & 0x8000)) {
+                if (A < qe) {
+                    D = 1 - mps;
+                    if (idx == 0 || idx == 6 || idx == 14) mps ^= 1;
+                    idx = d_nlps[idx];
+                } else {
+                    D = mps;
+                    idx = d_nmps[idx];
+                }
+                st[cx] = (uint8_t)((idx << 1) | mps);
+                do {
+                    if (CT == 0) bytein();
+                    A <<= 1;
+                    C <<= 1;
+                    --CT;
+                } while (!(A & 0x8000));
+            } else {
+                D = mps;
+            }
+        }
+        return D;
+    }
+};
+
+__device__ __forceinline__ uint32_t nb3(uint64_t m, int x) { return (uint32_t)(((m << 1) >> x) & 7); }
+
+__global__ void __launch_bounds__(kWarps * 32)
+t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
+                 const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
+                 size_t pitch, uint32_t* __restrict__ err) {
+    __shared__ DecSmem smem[kWarps];
+    __shared__ uint8_t zc_lut[4][3][3][5];
+    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) {
+        int o = i / 45, r = i % 45;
+        zc_lut[o][r / 15][(r / 5) % 3][r % 5] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int jid = blockIdx.x * kWarps + wid;
+    if (jid >= njobs) return;
+    DecSmem& S = smem[wid];
+    const j2k_cb_job J = jobs[jid];
+    const j2k_cb_desc D = descs[jid];
+    const int cw = J.cw, ch = J.ch, orient = J.orient;
+    if (cw == 0 || ch == 0 || cw > 64 || ch > 64 || orient > 3 || D.numbps > 31 ||
+        D.npasses > 3 * D.numbps || D.length < 0) {
+        if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+        return;
+    }
+    int32_t* blk = coeff + (size_t)J.y0 * pitch + J.x0;
+    for (int r = 0; r < ch; ++r)
+        for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
+    for (int r = lane; r < 66; r += 32) { S.sig[r] = 0; S.neg[r] = 0; S.ref[r] = 0; S.vis[r] = 0; }
+    if (lane < 19) S.st[lane] = 0;
+    __syncwarp();
+    if (lane == 0 && D.numbps > 0 && D.npasses > 0) {
+        S.st[0] = 4 << 1;
+        S.st[17] = 3 << 1;
+        S.st[18] = 46 << 1;
+        Mqd m;
+        m.init(bytes + D.offset, D.length);
+        int pass = 0;
+        const int nb = D.numbps, np = D.npasses;
+        auto sigbit = [&](int x, int y) -> int { return (int)((S.sig[y + 1] >> x) & 1); };
+        auto zc = [&](int x, int y) -> int {
+            uint32_t a = nb3(S.sig[y], x), b = nb3(S.sig[y + 1], x), c = nb3(S.sig[y + 2], x);
+            int h = (b & 1) + (b >> 2), v = ((a >> 1) & 1) + ((c >> 1) & 1);
+            int d = (a & 1) + (a >> 2) + (c & 1) + (c >> 2);
+            return (h + v + d) ? (int)zc_lut[orient][h][v][d] | 0x100 : zc_lut[orient][0][0][0];
+        };
+        auto sc = [&](int x, int y) -> int {
+            auto contrib = [&](int xx, int yy) -> int {
+                if (xx < 0 || xx >= 64) return 0;
+                if (!((S.sig[yy + 1] >> xx) & 1)) return 0;
+                return ((S.neg[yy + 1] >> xx) & 1) ? -1 : 1;
+            };
+            int hc = contrib(x - 1, y) + contrib(x + 1, y);
+            int vc = contrib(x, y - 1) + contrib(x, y + 1);
+            hc = max(-1, min(1, hc));
+            vc = max(-1, min(1, vc));
+            int xr = 0;
+            if (hc < 0 || (hc == 0 && vc < 0)) { hc = -hc; vc = -vc; xr = 1; }
+            int lab = hc == 0 ? (vc ? 10 : 9) : 12 + vc;
+            return lab | (xr << 7);
+        };
+        auto set_sig = [&](int x, int y, int neg, int p) {
+            S.sig[y + 1] |= 1ull << x;
+            if (neg) S.neg[y + 1] |= 1ull << x;
+            blk[(size_t)y * pitch + x] |= 1 << p;
+        };
+        for (int p = nb - 1; p >= 0 && pass < np; --p) {
+            if (p != nb - 1) {
+                for (int y0 = 0; y0 < ch; y0 += 4)
+                    for (int x = 0; x < cw; ++x)
+                        for (int y = y0; y < y0 + 4 && y < ch; ++y) {
+                            if (sigbit(x, y)) continue;
+                            int z = zc(x, y);
+                            if (!(z & 0x100)) continue;
+                            int bit = m.decode(S.st, z & 31);
+                            S.vis[y + 1] |= 1ull << x;
+                            if (bit) {
+                                int s = sc(x, y);
+                                int sg = m.decode(S.st, s & 31) ^ (s >> 7);
+                                set_sig(x, y, sg, p);
+                            }
+                        }
+                if (++pass >= np) break;
+                for (int y0 = 0; y0 < ch; y0 += 4)
+                    for (int x = 0; x < cw; ++x)
+                        for (int y = y0; y < y0 + 4 && y < ch; ++y) {
+                            if (!sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
+                            int lab;
+                            if ((S.ref[y + 1] >> x) & 1) lab = 16;
+                            else lab = (zc(x, y) & 0x100) ? 15 : 14;
+                            if (m.decode(S.st, lab)) blk[(size_t)y * pitch + x] |= 1 << p;
+                            S.ref[y + 1] |= 1ull << x;
+                        }
+                if (++pass >= np) break;
+            }
+            for (int y0 = 0; y0 < ch; y0 += 4)
+                for (int x = 0; x < cw; ++x) {
+                    int start = y0;
+                    if (y0 + 3 < ch) {
+                        bool rl = true;
+                        for (int y = y0; y < y0 + 4 && rl; ++y)
+                            if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1) || (zc(x, y) & 0x100)) rl = false;
+                        if (rl) {
+                            if (!m.decode(S.st, 17)) continue;
+                            int idx = m.decode(S.st, 18) << 1;
+                            idx |= m.decode(S.st, 18);
+                            int y = y0 + idx;
+                            int s = sc(x, y);
+                            int sg = m.decode(S.st, s & 31) ^ (s >> 7);
+                            set_sig(x, y, sg, p);
+                            start = y + 1;
+                        }
+                    }
+                    for (int y = start; y < y0 + 4 && y < ch; ++y) {
+                        if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
+                        int z = zc(x, y);
+                        int bit = m.decode(S.st, z & 31);
+                        if (bit) {
+                            int s = sc(x, y);
+                            int sg = m.decode(S.st, s & 31) ^ (s >> 7);
+                            set_sig(x, y, sg, p);
+                        }
+                    }
+                }
+            ++pass;
+            for (int r = 0; r < 66; ++r) S.vis[r] = 0;
+        }
+    }
+    __syncwarp();
+    for (int r = 0; r < ch; ++r)
+        for (int x = lane; x < cw; x += 32)
+            if ((S.neg[r + 1] >> x) & 1) blk[(size_t)r * pitch + x] = -blk[(size_t)r * pitch + x];
+}
+
+}  // namespace
+
+j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
+                              const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff, size_t pitch,
+                              cudaStream_t st) {
+    if (njobs == 0) return J2K_OK;
+    unsigned g = (unsigned)((njobs + kWarps - 1) / kWarps);
+    t1_decode_kernel<<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, pitch, ctx->d_err);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
+}
