@@ -49,7 +49,10 @@ typedef struct j2k_ctx j2k_ctx;
 /* ---- context: replaces OCLDeviceManager::init/getInfo + ocl_args_d_t ------------------------ */
 j2k_status j2k_ctx_create(int device, j2k_ctx** out);
 j2k_status j2k_ctx_destroy(j2k_ctx* ctx);
-j2k_status j2k_ctx_set_stream(j2k_ctx* ctx, void* cuda_stream); /* NULL = context's own */
+/* Launch on `cuda_stream` from now on (NULL = the CUDA legacy default stream).  A new context
+ * uses a non-blocking stream of its own; j2k_ctx_use_own_stream switches back to it. */
+j2k_status j2k_ctx_set_stream(j2k_ctx* ctx, void* cuda_stream);
+j2k_status j2k_ctx_use_own_stream(j2k_ctx* ctx);
 void* j2k_ctx_stream(j2k_ctx* ctx);
 j2k_status j2k_stream_sync(j2k_ctx* ctx);                          /* replaces clFinish */
 const char* j2k_last_error(const j2k_ctx* ctx);

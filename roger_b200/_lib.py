@@ -46,6 +46,7 @@ SIGS = {
     "j2k_ctx_create": (I, [I, C.POINTER(P)]),
     "j2k_ctx_destroy": (I, [P]),
     "j2k_ctx_set_stream": (I, [P, P]),
+    "j2k_ctx_use_own_stream": (I, [P]),
     "j2k_ctx_stream": (P, [P]),
     "j2k_stream_sync": (I, [P]),
     "j2k_last_error": (C.c_char_p, [P]),

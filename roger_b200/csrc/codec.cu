@@ -468,6 +468,14 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
     const j2k_cb_desc* dd = descs;
     const uint8_t* db = bytes;
     if (!on_device) {
+        // host descriptors are validated before any kernel reads through them
+        for (size_t i = 0; i < njobs; ++i) {
+            const j2k_cb_desc& q = descs[i];
+            if (q.length < 0 || (size_t)q.offset + (size_t)q.length > nbytes || q.numbps > 31 ||
+                q.npasses > 3 * q.numbps)
+                return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "code-block descriptor " + std::to_string(i) +
+                                                              " is out of range");
+        }
         J2K_TRY(d->descs.ensure(ctx, njobs * sizeof(j2k_cb_desc) + 16));
         J2K_TRY(d->bytes.ensure(ctx, nbytes + 16));
         J2K_CUDA(ctx, cudaMemcpyAsync(d->descs.p, descs, njobs * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));

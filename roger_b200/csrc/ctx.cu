@@ -189,7 +189,13 @@ j2k_status j2k_ctx_destroy(j2k_ctx* ctx) {
 
 j2k_status j2k_ctx_set_stream(j2k_ctx* ctx, void* s) {
     if (!ctx) return J2K_ERR_INVALID_ARG;
-    ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+    ctx->stream = (cudaStream_t)s;  // NULL is the CUDA legacy default stream
+    return J2K_OK;
+}
+
+j2k_status j2k_ctx_use_own_stream(j2k_ctx* ctx) {
+    if (!ctx) return J2K_ERR_INVALID_ARG;
+    ctx->stream = ctx->own_stream;
     return J2K_OK;
 }
 

@@ -24,13 +24,14 @@ namespace {
 constexpr float P1 = -1.586134342f, U1 = -0.05298011854f, P2 = 0.8829110762f, U2 = 0.4435068522f;
 constexpr float KMUL = 1.23017410491400f, KDIV = 0.81289306611596153187273657637352f;
 
+// whole-sample symmetric extension (period 2(n-1)), parity preserving
 __device__ __forceinline__ int mirror(int i, int n) {
+    if (i >= 0 && i < n) return i;
     if (n == 1) return 0;
-    while (i < 0 || i >= n) {
-        if (i < 0) i = -i;
-        if (i >= n) i = 2 * (n - 1) - i;
-    }
-    return i;
+    const int p = 2 * (n - 1);
+    i %= p;
+    if (i < 0) i += p;
+    return i >= n ? p - i : i;
 }
 
 template <int KERN> struct KT;

@@ -12,19 +12,40 @@ namespace {
 
 constexpr int kWarps = 4;
 
+// T.800 Table C.2 (probability estimation), device and host copies
 __constant__ uint16_t d_qe[47] = {
     0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801, 0x3001, 0x2401,
     0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401, 0x3001, 0x2801, 0x2401, 0x2201,
     0x1C01, 0x1801, 0x1601, 0x1401, 0x1201, 0x1101, 0x0AC1, 0x09C1, 0x08A1, 0x0521, 0x0441, 0x02A1,
     0x0221, 0x0141, 0x0111, 0x0085, 0x0049, 0x0025, 0x0015, 0x0009, 0x0005, 0x0001, 0x5601};
-__constant__ uint8_t d_nmps[47] = {1,  2,  3,  4,  5,  38, 7,  8,  9,  10, 11, 12, 13, 29, 15, 16,
-                                   17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32,
-                                   33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 44, 45, 45, 46};
-__constant__ uint8_t d_nlps[47] = {1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 18, 20, 21, 14, 14,
-                                   15, 16, 17, 18, 19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29,
-                                   30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
+__constant__ uint8_t d_nmps[47] = {
+    1,  2,  3,  4,  5,  38, 7,  8,  9,  10, 11, 12, 13, 29, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24,
+    25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 44, 45, 45, 46};
+__constant__ uint8_t d_nlps[47] = {
+    1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 18, 20, 21, 14, 14, 15, 16, 17, 18, 19, 19, 20, 21,
+    22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
+static const uint16_t h_qe[47] = {
+    0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801, 0x3001, 0x2401,
+    0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401, 0x3001, 0x2801, 0x2401, 0x2201,
+    0x1C01, 0x1801, 0x1601, 0x1401, 0x1201, 0x1101, 0x0AC1, 0x09C1, 0x08A1, 0x0521, 0x0441, 0x02A1,
+    0x0221, 0x0141, 0x0111, 0x0085, 0x0049, 0x0025, 0x0015, 0x0009, 0x0005, 0x0001, 0x5601};
+static const uint8_t h_nmps[47] = {
+    1,  2,  3,  4,  5,  38, 7,  8,  9,  10, 11, 12, 13, 29, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24,
+    25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 44, 45, 45, 46};
+static const uint8_t h_nlps[47] = {
+    1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 18, 20, 21, 14, 14, 15, 16, 17, 18, 19, 19, 20, 21,
+    22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
+#ifdef __CUDA_ARCH__
+#define QE(i) d_qe[i]
+#define NMPS(i) d_nmps[i]
+#define NLPS(i) d_nlps[i]
+#else
+#define QE(i) h_qe[i]
+#define NMPS(i) h_nmps[i]
+#define NLPS(i) h_nlps[i]
+#endif
 
-__device__ __forceinline__ int zc_label_calc(int orient, int h, int v, int d) {
+__host__ __device__ __forceinline__ int zc_label_calc(int orient, int h, int v, int d) {
     if (orient == J2K_BAND_HH) {
         int hv = h + v;
         if (d >= 3) return 8;
@@ -49,8 +70,8 @@ struct Mqd {
     const uint8_t* data;
     int len, bp, CT;
     uint32_t A, C;
-    __device__ uint32_t byte(int i) const { return i < len ? data[i] : 0xFFu; }
-    __device__ void bytein() {
+    __host__ __device__ uint32_t byte(int i) const { return i < len ? data[i] : 0xFFu; }
+    __host__ __device__ void bytein() {
         if (byte(bp) == 0xFF) {
             if (byte(bp + 1) > 0x8F) {
                 C += 0xFF00;
@@ -66,7 +87,7 @@ struct Mqd {
             CT = 8;
         }
     }
-    __device__ void init(const uint8_t* d, int n) {
+    __host__ __device__ void init(const uint8_t* d, int n) {
         data = d;
         len = n;
         bp = 0;
@@ -76,21 +97,21 @@ struct Mqd {
         CT -= 7;
         A = 0x8000;
     }
-    __device__ int decode(uint8_t* st, int cx) {
+    __host__ __device__ int decode(uint8_t* st, int cx) {
         int sv = st[cx], idx = sv >> 1, mps = sv & 1;
-        uint32_t qe = d_qe[idx];
+        uint32_t qe = QE(idx);
         int D;
         A -= qe;
         if ((C >> 16) < qe) {
             if (A < qe) {
                 A = qe;
                 D = mps;
-                idx = d_nmps[idx];
+                idx = NMPS(idx);
             } else {
                 A = qe;
                 D = 1 - mps;
                 if (idx == 0 || idx == 6 || idx == 14) mps ^= 1;
-                idx = d_nlps[idx];
+                idx = NLPS(idx);
             }
             st[cx] = (uint8_t)((idx << 1) | mps);
             do {
@@ -105,10 +126,10 @@ struct Mqd {
                 if (A < qe) {
                     D = 1 - mps;
                     if (idx == 0 || idx == 6 || idx == 14) mps ^= 1;
-                    idx = d_nlps[idx];
+                    idx = NLPS(idx);
                 } else {
                     D = mps;
-                    idx = d_nmps[idx];
+                    idx = NMPS(idx);
                 }
                 st[cx] = (uint8_t)((idx << 1) | mps);
                 do {
@@ -125,51 +146,30 @@ struct Mqd {
     }
 };
 
-__device__ __forceinline__ uint32_t nb3(uint64_t m, int x) { return (uint32_t)(((m << 1) >> x) & 7); }
+// bits x-1, x, x+1 of a row mask (bit 0 = column x-1); columns outside 0..63 read as 0
+__host__ __device__ __forceinline__ uint32_t nb3(uint64_t m, int x) {
+    return (uint32_t)(x > 0 ? (m >> (x - 1)) & 7 : (m << 1) & 7);
+}
 
-__global__ void __launch_bounds__(kWarps * 32)
-t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
-                 const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
-                 size_t pitch, uint32_t* __restrict__ err) {
-    __shared__ DecSmem smem[kWarps];
-    __shared__ uint8_t zc_lut[4][3][3][5];
-    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) {
-        int o = i / 45, r = i % 45;
-        zc_lut[o][r / 15][(r / 5) % 3][r % 5] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int jid = blockIdx.x * kWarps + wid;
-    if (jid >= njobs) return;
-    DecSmem& S = smem[wid];
-    const j2k_cb_job J = jobs[jid];
-    const j2k_cb_desc D = descs[jid];
-    const int cw = J.cw, ch = J.ch, orient = J.orient;
-    if (cw == 0 || ch == 0 || cw > 64 || ch > 64 || orient > 3 || D.numbps > 31 ||
-        D.npasses > 3 * D.numbps || D.length < 0) {
-        if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
-        return;
-    }
-    int32_t* blk = coeff + (size_t)J.y0 * pitch + J.x0;
-    for (int r = 0; r < ch; ++r)
-        for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
-    for (int r = lane; r < 66; r += 32) { S.sig[r] = 0; S.neg[r] = 0; S.ref[r] = 0; S.vis[r] = 0; }
-    if (lane < 19) S.st[lane] = 0;
-    __syncwarp();
-    if (lane == 0 && D.numbps > 0 && D.npasses > 0) {
+// Serial decode of one code-block into magnitudes (blk, pre-zeroed) and sign/state masks in S.
+// Host-callable so that the exact device logic can be checked on the CPU.
+__host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint8_t* data, int len, int numbps,
+                                      int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch) {
+#define zc_lut_at(o, h, v, d) lut[(((o) * 3 + (h)) * 3 + (v)) * 5 + (d)]
+
         S.st[0] = 4 << 1;
         S.st[17] = 3 << 1;
         S.st[18] = 46 << 1;
         Mqd m;
-        m.init(bytes + D.offset, D.length);
+        m.init(data, len);
         int pass = 0;
-        const int nb = D.numbps, np = D.npasses;
+        const int nb = numbps, np = npasses;
         auto sigbit = [&](int x, int y) -> int { return (int)((S.sig[y + 1] >> x) & 1); };
         auto zc = [&](int x, int y) -> int {
             uint32_t a = nb3(S.sig[y], x), b = nb3(S.sig[y + 1], x), c = nb3(S.sig[y + 2], x);
             int h = (b & 1) + (b >> 2), v = ((a >> 1) & 1) + ((c >> 1) & 1);
             int d = (a & 1) + (a >> 2) + (c & 1) + (c >> 2);
-            return (h + v + d) ? (int)zc_lut[orient][h][v][d] | 0x100 : zc_lut[orient][0][0][0];
+            return (h + v + d) ? (int)zc_lut_at(orient, h, v, d) | 0x100 : zc_lut_at(orient, 0, 0, 0);
         };
         auto sc = [&](int x, int y) -> int {
             auto contrib = [&](int xx, int yy) -> int {
@@ -252,7 +252,41 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
             ++pass;
             for (int r = 0; r < 66; ++r) S.vis[r] = 0;
         }
+    #undef zc_lut_at
+}
+
+__global__ void __launch_bounds__(kWarps * 32)
+t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
+                 const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
+                 size_t pitch, uint32_t* __restrict__ err) {
+    __shared__ DecSmem smem[kWarps];
+    __shared__ uint8_t zc_lut[4][3][3][5];
+    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) {
+        int o = i / 45, r = i % 45;
+        zc_lut[o][r / 15][(r / 5) % 3][r % 5] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
     }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int jid = blockIdx.x * kWarps + wid;
+    if (jid >= njobs) return;
+    DecSmem& S = smem[wid];
+    const j2k_cb_job J = jobs[jid];
+    const j2k_cb_desc D = descs[jid];
+    const int cw = J.cw, ch = J.ch, orient = J.orient;
+    if (cw == 0 || ch == 0 || cw > 64 || ch > 64 || orient > 3 || D.numbps > 31 ||
+        D.npasses > 3 * D.numbps || D.length < 0) {
+        if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+        return;
+    }
+    int32_t* blk = coeff + (size_t)J.y0 * pitch + J.x0;
+    for (int r = 0; r < ch; ++r)
+        for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
+    for (int r = lane; r < 66; r += 32) { S.sig[r] = 0; S.neg[r] = 0; S.ref[r] = 0; S.vis[r] = 0; }
+    if (lane < 19) S.st[lane] = 0;
+    __syncwarp();
+    if (lane == 0 && D.numbps > 0 && D.npasses > 0)
+        decode_block(S, &zc_lut[0][0][0][0], bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch,
+                     blk, pitch);
     __syncwarp();
     for (int r = 0; r < ch; ++r)
         for (int x = lane; x < cw; x += 32)
@@ -260,6 +294,27 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
 }
 
 }  // namespace
+
+// Host execution of the device decoder logic for one block (used by the test suite).
+extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
+                                        int cw, int ch, int32_t* out, size_t pitch) {
+    if (cw < 1 || ch < 1 || cw > 64 || ch > 64 || orient < 0 || orient > 3 || numbps > 31) return -1;
+    DecSmem S;
+    for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
+    for (int k = 0; k < 19; ++k) S.st[k] = 0;
+    uint8_t lut[4 * 45];
+    for (int i = 0; i < 4 * 45; ++i) {
+        int o = i / 45, r = i % 45;
+        lut[i] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
+    }
+    for (int y = 0; y < ch; ++y)
+        for (int x = 0; x < cw; ++x) out[(size_t)y * pitch + x] = 0;
+    if (numbps > 0 && npasses > 0) decode_block(S, lut, data, len, numbps, npasses, orient, cw, ch, out, pitch);
+    for (int y = 0; y < ch; ++y)
+        for (int x = 0; x < cw; ++x)
+            if ((S.neg[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
+    return 0;
+}
 
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff, size_t pitch,

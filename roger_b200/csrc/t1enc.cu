@@ -127,7 +127,10 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
     WarpSmem& S = smem[wid];
     const j2k_cb_job J = jobs[jid];
     if (J.cw == 0 || J.ch == 0 || J.cw > 64 || J.ch > 64 || J.orient > 3) {
-        if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+        if (lane == 0) {
+            atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+            nsyms[jid] = 0;
+        }
         return;
     }
     Ctx c{coeff + (size_t)J.y0 * pitch + J.x0, pitch, J.cw, J.ch};
@@ -176,7 +179,11 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
     d.comp = J.comp;
     d.reserved = 0;
     if (numbps > 31) {
-        if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_PLANES);
+        if (lane == 0) {
+            atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_PLANES);
+            nsyms[jid] = 0;
+            descs[jid] = d;
+        }
         return;
     }
     uint8_t* out = syms + (size_t)jid * sym_cap;
@@ -429,7 +436,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
     cst[0 * kMqThreads + t] = 4 << 1;
     cst[17 * kMqThreads + t] = 3 << 1;
     cst[18 * kMqThreads + t] = 46 << 1;
-    const int n = (int)nsyms[jid];
+    const int n = (int)min((size_t)nsyms[jid], sym_cap);
     const uint8_t* sp = syms + (size_t)jid * sym_cap;
     MqOut o{reinterpret_cast<uint32_t*>(bytes + (size_t)jid * cap_per_block), (int)cap_per_block,
             0u, 0, 0, false};
@@ -469,7 +476,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
         int m = min(16, n - i0);
         for (int k = 0; k < m; ++k) {
             uint32_t sym = (wv[k >> 2] >> (8 * (k & 3))) & 0xFF;
-            int cx = sym & 31, dbit = sym >> 7;
+            int cx = min((int)(sym & 31), 18), dbit = sym >> 7;
             uint32_t sv = cst[cx * kMqThreads + t];
             int idx = sv >> 1, mps = sv & 1;
             uint32_t te = tab[idx];

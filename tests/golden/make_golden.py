@@ -67,7 +67,7 @@ def main():
     coef = O.dwt53_fwd(planes[0], 5)
     for (x0, y0, cw, ch, orient, tag) in [(0, 0, 16, 16, O.LL, "LL5"), (256, 0, 64, 64, O.HL, "HL1"),
                                           (0, 256, 64, 64, O.LH, "LH1"), (256, 256, 64, 64, O.HH, "HH1"),
-                                          (128, 64, 64, 64, O.HH, "HH2"), (16, 0, 16, 16, O.HL, "HL5")]:
+                                          (128, 128, 64, 64, O.HH, "HH2"), (16, 0, 16, 16, O.HL, "HL5")]:
         blk = np.ascontiguousarray(coef[y0:y0 + ch, x0:x0 + cw])
         data, info, syms = O.t1_encode(blk, orient, want_symbols=True)
         out["t1"].append(dict(tag=tag, x0=x0, y0=y0, cw=cw, ch=ch, orient=orient,

@@ -64,3 +64,22 @@ def test_python_mirror_subbands_match_oracle():
     for (w, h, L) in [(512, 512, 5), (33, 17, 2), (1, 1, 3), (2047, 65, 5)]:
         assert subband_rects(w, h, L) == [tuple(s) for s in O.subbands(w, h, L)]
         assert np.array_equal(default_steps(w, h, L), O.default_steps(w, h, L))
+
+
+@pytest.mark.parametrize("cw,ch,orient", [(64, 64, 0), (64, 64, 1), (64, 64, 2), (64, 64, 3), (64, 4, 0),
+                                          (64, 1, 3), (33, 17, 1), (8, 64, 2), (1, 1, 0)])
+def test_device_decoder_logic_runs_on_host(cw, ch, orient):
+    """The tier-1 decoder's per-block routine is __host__ __device__; run it on the CPU against
+    oracle-encoded blocks (no kernel launch)."""
+    import ctypes as C
+    from oracle import oracle as O
+    from roger_b200 import _lib
+    f = C.CDLL(_lib.LIB_PATH).j2k_t1_decode_block_host
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
+    rng = np.random.default_rng(cw * 7 + ch + orient)
+    blk = rng.laplace(0, 25, (ch, cw)).astype(np.int32)
+    data, info = O.t1_encode(blk, orient)
+    buf = np.frombuffer(data + b"\0", np.uint8).copy()
+    out = np.zeros_like(blk)
+    assert f(buf.ctypes.data, len(data), info["numbps"], info["npasses"], orient, cw, ch, out.ctypes.data, cw) == 0
+    assert np.array_equal(out, blk)
