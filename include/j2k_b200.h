@@ -56,6 +56,10 @@ j2k_status j2k_ctx_use_own_stream(j2k_ctx* ctx);
 void* j2k_ctx_stream(j2k_ctx* ctx);
 j2k_status j2k_stream_sync(j2k_ctx* ctx);                          /* replaces clFinish */
 const char* j2k_last_error(const j2k_ctx* ctx);
+/* Launch-shape knobs (set by the autotuner; defaults are sensible).  No reference counterpart:
+ * the reference fixed its OpenCL work-group shapes in -D build strings (src/OCLEncoder.cpp:27-29). */
+enum { J2K_TUNE_MQ_LANES = 1 };
+j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value);
 const char* j2k_status_string(j2k_status s);
 int j2k_version(void);
 

@@ -50,6 +50,7 @@ SIGS = {
     "j2k_ctx_stream": (P, [P]),
     "j2k_stream_sync": (I, [P]),
     "j2k_last_error": (C.c_char_p, [P]),
+    "j2k_ctx_set_tuning": (I, [P, I, I]),
     "j2k_status_string": (C.c_char_p, [I]),
     "j2k_version": (I, []),
     "j2k_rgb_to_planar": (I, [P, P, S, I, I, I, P, S, S, S, S]),

@@ -207,6 +207,17 @@ j2k_status j2k_stream_sync(j2k_ctx* ctx) {
     return J2K_OK;
 }
 
+j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
+    if (!ctx) return J2K_ERR_INVALID_ARG;
+    if (key == J2K_TUNE_MQ_LANES) {
+        if (value != 8 && value != 16 && value != 32)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "MQ lanes per warp must be 8, 16 or 32");
+        ctx->mq_lanes = value;
+        return J2K_OK;
+    }
+    return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown tuning key");
+}
+
 const char* j2k_last_error(const j2k_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 size_t j2k_codeblock_count(size_t w, size_t h, int levels, int cbw, int cbh) {

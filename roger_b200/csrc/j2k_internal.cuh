@@ -30,6 +30,7 @@ struct j2k_ctx {
     void* h_pinned = nullptr;    // pinned staging
     size_t h_pinned_size = 0;
     int sm_count = 148;
+    int mq_lanes = 32;           // tier-1 MQ: code-blocks per warp (tuning knob)
 };
 
 // scratch slot ids

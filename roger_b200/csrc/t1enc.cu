@@ -21,6 +21,8 @@
 //
 // Phase B — one lane per code-block runs the MQ encoder over its symbol stream (T.800 C.2,
 // FLUSH of C.2.9, trailing 0xFF dropped); codeword bytes are written as aligned 32-bit words.
+#include <cub/cub.cuh>
+
 #include "j2k_internal.cuh"
 
 namespace {
@@ -387,6 +389,14 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
 }
 
 // ---- phase B: MQ encoder, one lane per code-block ------------------------------------------------
+//
+// The coder is serial per block, so the kernel time is (longest block's symbol count) x
+// (latency per symbol).  Blocks are ordered longest-first (a radix sort of the symbol counts)
+// so the lanes of a warp finish together and the biggest blocks start first.  Per context the
+// state is one packed word in shared memory: Qe (bits 0-15), next-MPS index (16-21), next-LPS
+// index (22-27), switch flag (28), MPS (31).  The MPS-without-renormalisation case, the most
+// frequent, touches no memory but the state load; the next symbol's state is loaded before the
+// current one finishes, and forwarded when both use the same context.
 
 __constant__ uint16_t c_qe[47] = {
     0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801, 0x3001, 0x2401,
@@ -400,136 +410,175 @@ __constant__ uint8_t c_nlps[47] = {1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 1
                                    15, 16, 17, 18, 19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29,
                                    30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
 
-constexpr int kMqThreads = 128;
+constexpr int kMqThreads = 64;
 
-struct MqOut {
-    uint32_t* base;   // word-aligned output
-    int cap;          // bytes
-    uint32_t wacc;
+// Branch-light MQ encoder state.  The exchange and state transition are predicated so the
+// lanes of a warp (each coding a different block) stay converged; only the byte output, about
+// one symbol in sixteen, branches.
+struct MqEnc {
+    uint32_t A, C, B;   // B: pending output byte (may still receive a carry)
+    int CT, bp;         // bp: index of B (-1 before the first byte)
+    uint32_t* out;      // word-aligned codeword buffer
+    int cap;            // bytes
+    uint32_t wacc;      // completed bytes waiting for a 32-bit store
     int wn, wbase;
     bool ovf;
-    __device__ void push(uint32_t byte) {
+    __device__ __forceinline__ void push(uint32_t byte) {
         wacc |= byte << (8 * wn);
         if (++wn == 4) {
-            if (wbase + 4 <= cap) base[wbase >> 2] = wacc; else ovf = true;
+            if (wbase + 4 <= cap) out[wbase >> 2] = wacc; else ovf = true;
             wbase += 4;
             wn = 0;
             wacc = 0;
         }
     }
+    // T.800 C.2 BYTEOUT in one straight-line form: a carry (C >= 2^27 after a non-0xFF byte)
+    // increments the pending byte; a 0xFF byte (before or after the carry) is followed by 7 bits.
+    __device__ __forceinline__ void byteout() {
+        if (B != 0xFF && C >= 0x8000000u) {
+            if (bp >= 0) B += 1;
+            C &= 0x7FFFFFF;
+        }
+        const bool ff = (B == 0xFF);
+        const uint32_t v = ff ? (C >> 20) : (C >> 19);
+        C &= ff ? 0xFFFFFu : 0x7FFFFu;
+        CT = ff ? 7 : 8;
+        if (bp >= 0) push(B);
+        ++bp;
+        B = v & 0xFF;
+    }
+    // shift by sh (0..15) with at most two byte outputs
+    __device__ __forceinline__ void renorm(int sh) {
+        int k = min(sh, CT);
+        A <<= k;
+        C <<= k;
+        CT -= k;
+        sh -= k;
+        if (CT == 0) {
+            byteout();
+            k = min(sh, CT);
+            A <<= k;
+            C <<= k;
+            CT -= k;
+            sh -= k;
+            if (CT == 0) {
+                byteout();
+                A <<= sh;
+                C <<= sh;
+                CT -= sh;
+            }
+        }
+    }
 };
 
+template <int LANES>
 __global__ void __launch_bounds__(kMqThreads)
 t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* __restrict__ nsyms,
-             int njobs, uint8_t* __restrict__ bytes, size_t cap_per_block,
-             j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+             const uint32_t* __restrict__ order, int njobs, uint8_t* __restrict__ bytes,
+             size_t cap_per_block, j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
     __shared__ uint32_t tab[47];
-    __shared__ uint8_t cst[19 * kMqThreads];
+    __shared__ uint32_t cst[19 * kMqThreads];
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
         tab[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
     __syncthreads();
-    const int jid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (jid >= njobs) return;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane >= LANES) return;
+    const int gid = (blockIdx.x * (kMqThreads / 32) + wid) * LANES + lane;
+    if (gid >= njobs) return;
+    const int jid = order ? (int)order[gid] : gid;
     const int t = threadIdx.x;
-    for (int k = 0; k < 19; ++k) cst[k * kMqThreads + t] = 0;
-    cst[0 * kMqThreads + t] = 4 << 1;
-    cst[17 * kMqThreads + t] = 3 << 1;
-    cst[18 * kMqThreads + t] = 46 << 1;
+    uint32_t* st = cst + t;  // context k at st[k * kMqThreads]
+    for (int k = 0; k < 19; ++k) st[k * kMqThreads] = tab[0];
+    st[0] = tab[4];
+    st[17 * kMqThreads] = tab[3];
+    st[18 * kMqThreads] = tab[46];
     const int n = (int)min((size_t)nsyms[jid], sym_cap);
-    const uint8_t* sp = syms + (size_t)jid * sym_cap;
-    MqOut o{reinterpret_cast<uint32_t*>(bytes + (size_t)jid * cap_per_block), (int)cap_per_block,
-            0u, 0, 0, false};
-    uint32_t A = 0x8000, C = 0, B = 0;
-    int CT = 12, bp = -1;
-    auto emit = [&](uint32_t v) {
-        if (bp >= 0) o.push(B);
-        ++bp;
-        B = v & 0xFF;
-    };
-    auto byteout = [&]() {
-        if (B == 0xFF) {
-            emit(C >> 20);
-            C &= 0xFFFFF;
-            CT = 7;
-        } else if (C < 0x8000000u) {
-            emit(C >> 19);
-            C &= 0x7FFFF;
-            CT = 8;
-        } else {
-            if (bp >= 0) B += 1; // carry into the pending byte
-            if (bp >= 0 && B == 0xFF) {
-                C &= 0x7FFFFFF;
-                emit(C >> 20);
-                C &= 0xFFFFF;
-                CT = 7;
-            } else {
-                emit(C >> 19);
-                C &= 0x7FFFF;
-                CT = 8;
-            }
-        }
-    };
-    for (int i0 = 0; i0 < n; i0 += 16) {
-        uint4 q = *reinterpret_cast<const uint4*>(sp + i0);
-        uint32_t wv[4] = {q.x, q.y, q.z, q.w};
-        int m = min(16, n - i0);
-        for (int k = 0; k < m; ++k) {
-            uint32_t sym = (wv[k >> 2] >> (8 * (k & 3))) & 0xFF;
-            int cx = min((int)(sym & 31), 18), dbit = sym >> 7;
-            uint32_t sv = cst[cx * kMqThreads + t];
-            int idx = sv >> 1, mps = sv & 1;
-            uint32_t te = tab[idx];
-            uint32_t qe = te & 0xFFFF;
-            A -= qe;
-            if (dbit == mps) {
-                if (A & 0x8000) {
-                    C += qe;
-                    continue;
+    MqEnc e;
+    e.A = 0x8000;
+    e.C = 0;
+    e.B = 0;
+    e.CT = 12;
+    e.bp = -1;
+    e.out = reinterpret_cast<uint32_t*>(bytes + (size_t)jid * cap_per_block);
+    e.cap = (int)cap_per_block;
+    e.wacc = 0;
+    e.wn = 0;
+    e.wbase = 0;
+    e.ovf = false;
+    // Symbols stream in 16-byte chunks with two chunks in flight per lane; the next symbol's
+    // context state is loaded one step ahead and forwarded when the current symbol updates it.
+    const uint4* sp4 = reinterpret_cast<const uint4*>(syms + (size_t)jid * sym_cap);
+    const int nchunks = (n + 15) >> 4;
+    const uint4 z4 = make_uint4(0, 0, 0, 0);
+    uint4 c0 = nchunks > 0 ? __ldcs(sp4) : z4;
+    uint4 c1 = nchunks > 1 ? __ldcs(sp4 + 1) : z4;
+    int cx = min((int)(c0.x & 31), 18);
+    uint32_t ent = st[cx * kMqThreads];
+    for (int k = 0; k < nchunks; ++k) {
+        const uint4 cur = c0;
+        c0 = c1;
+        c1 = (k + 2 < nchunks) ? __ldcs(sp4 + k + 2) : z4;
+        const int m = min(16, n - 16 * k);
+        const uint32_t w[5] = {cur.x, cur.y, cur.z, cur.w, c0.x};
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (j < m) {
+                const uint32_t sym = (w[j >> 2] >> (8 * (j & 3))) & 0xFF;
+                const uint32_t nsym = (w[(j + 1) >> 2] >> (8 * ((j + 1) & 3))) & 0xFF;
+                const int d = sym >> 7;
+                const int ncx = min((int)(nsym & 31), 18);
+                uint32_t nent = st[ncx * kMqThreads];
+                const uint32_t qe = ent & 0xFFFF;
+                const int mps = ent >> 31;
+                const bool is_mps = d == mps;
+                const uint32_t a1 = e.A - qe;
+                const bool fast = is_mps && (a1 & 0x8000);
+                const bool addc = fast || (is_mps != (a1 < qe));
+                e.C += addc ? qe : 0u;
+                e.A = addc ? a1 : qe;
+                // state transition (not taken on the fast path)
+                const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
+                const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
+                const uint32_t upd = tab[nidx] | (nmps << 31);
+                if (!fast) {
+                    st[cx * kMqThreads] = upd;
+                    if (ncx == cx) nent = upd;
                 }
-                if (A < qe) A = qe; else C += qe;
-                idx = (te >> 16) & 63;
-            } else {
-                if (A < qe) C += qe; else A = qe;
-                mps ^= (te >> 28) & 1;
-                idx = (te >> 22) & 63;
-            }
-            cst[cx * kMqThreads + t] = (uint8_t)((idx << 1) | mps);
-            int sh = __clz(A) - 16;
-            while (sh > 0) {
-                int kk = min(sh, CT);
-                A <<= kk;
-                C <<= kk;
-                CT -= kk;
-                sh -= kk;
-                if (CT == 0) byteout();
+                e.renorm(__clz(e.A) - 16);
+                cx = ncx;
+                ent = nent;
             }
         }
     }
     int len = 0;
     if (n > 0) {
-        uint32_t tempc = C + A;
-        C |= 0xFFFF;
-        if (C >= tempc) C -= 0x8000;
-        C <<= CT;
-        byteout();
-        C <<= CT;
-        byteout();
-        len = bp + 1;
-        if (B == 0xFF) len--;
-        o.push(B);
-        // drain the partial word with byte stores
+        uint32_t tempc = e.C + e.A;
+        e.C |= 0xFFFF;
+        if (e.C >= tempc) e.C -= 0x8000;
+        e.C <<= e.CT;
+        e.byteout();
+        e.C <<= e.CT;
+        e.byteout();
+        len = e.bp + 1;
+        if (e.B == 0xFF) len--;
+        e.push(e.B);
         uint8_t* bb = bytes + (size_t)jid * cap_per_block;
-        for (int k = 0; k < o.wn; ++k) {
-            if (o.wbase + k < o.cap) bb[o.wbase + k] = (uint8_t)(o.wacc >> (8 * k));
-            else o.ovf = true;
+        for (int k = 0; k < e.wn; ++k) {
+            if (e.wbase + k < e.cap) bb[e.wbase + k] = (uint8_t)(e.wacc >> (8 * k));
+            else e.ovf = true;
         }
     }
-    if (o.ovf || len > (int)cap_per_block) {
+    if (e.ovf || len > (int)cap_per_block) {
         atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_OUT_CAPACITY);
         len = 0;
     }
     descs[jid].length = len;
+}
+
+__global__ void iota_kernel(uint32_t* v, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (uint32_t)i;
 }
 
 }  // namespace
@@ -544,17 +593,36 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
     if (((uintptr_t)bytes & 15) != 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "t1: bytes buffer must be 16-byte aligned");
     uint8_t* syms = (uint8_t*)j2k_scratch(ctx, SCR_SYMS, njobs * sym_cap + 64);
-    uint32_t* meta = (uint32_t*)j2k_scratch(ctx, SCR_T1STATE, njobs * 4 * (92 + 1) + 64);
+    // meta: nsyms | pass ends (92 per job) | sort keys/values (4 arrays of njobs)
+    size_t meta_words = njobs * (1 + 92 + 4) + 64;
+    uint32_t* meta = (uint32_t*)j2k_scratch(ctx, SCR_T1STATE, meta_words * 4);
     if (!syms || !meta) return J2K_ERR_OUT_OF_MEMORY;
     uint32_t* nsyms = meta;
     uint32_t* pend = meta + njobs;
+    uint32_t* keys_out = pend + njobs * 92;
+    uint32_t* idx_in = keys_out + njobs;
+    uint32_t* idx_out = idx_in + njobs;
     unsigned ga = (unsigned)((njobs + kWarpsPerCta - 1) / kWarpsPerCta);
     t1_symbols_kernel<<<ga, kWarpsPerCta * 32, 0, st>>>(coeff, pitch, d_jobs, (int)njobs, syms, sym_cap,
                                                         nsyms, pend, descs, cap_per_block, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
-    unsigned gb = (unsigned)((njobs + kMqThreads - 1) / kMqThreads);
-    t1_mq_kernel<<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, (int)njobs, bytes, cap_per_block,
-                                            descs, ctx->d_err);
+    // longest-first order for the MQ lanes
+    iota_kernel<<<(unsigned)((njobs + 255) / 256), 256, 0, st>>>(idx_in, (int)njobs);
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, nsyms, keys_out, idx_in, idx_out, (int)njobs, 0, 32, st);
+    void* tbuf = j2k_scratch(ctx, SCR_MISC, tmp + 16);
+    if (!tbuf) return J2K_ERR_OUT_OF_MEMORY;
+    J2K_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, nsyms, keys_out, idx_in, idx_out,
+                                                            (int)njobs, 0, 32, st));
+    const int lanes = ctx->mq_lanes;  // active lanes (blocks) per warp: 32, 16 or 8
+    const size_t per_cta = (size_t)lanes * (kMqThreads / 32);
+    unsigned gb = (unsigned)((njobs + per_cta - 1) / per_cta);
+    if (lanes == 8)
+        t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block, descs, ctx->d_err);
+    else if (lanes == 16)
+        t1_mq_kernel<16><<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block, descs, ctx->d_err);
+    else
+        t1_mq_kernel<32><<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block, descs, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }
