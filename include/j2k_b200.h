@@ -93,6 +93,24 @@ j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, 
                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
                            const float* steps);
 
+/* ---- allocation-free forward DWT.  No counterpart in the reference (its OCLMemoryManager
+ * allocated every image itself).  For callers that cannot allocate device memory — a plugin
+ * inside a framework that owns the device heap, or a latency-critical pipeline that must never
+ * reach cudaMalloc — this variant of j2k_dwt_forward needs no context and allocates nothing:
+ * its intermediate LL bands live in a 5 MiB array reserved in the library's device image,
+ * which every GPU that loads the library holds until the process exits.  Limit: the LL bands
+ * of the image must fit, i.e. ceil(w/2)*ceil(h/2) + ceil(w/4)*ceil(h/4) <= 1,310,720 samples
+ * (2048x2048 at most for square images); larger images return J2K_ERR_CAPACITY.  Arguments
+ * and output are those of j2k_dwt_forward, launched on `cuda_stream` (NULL = legacy default
+ * stream).  The first call on a device looks up the array's device address; make that first
+ * call before any stream capture.  All calls share the one array (its contents persist from
+ * the previous call and nothing needs clearing), so calls whose execution overlaps on the GPU
+ * race: order them on one stream or synchronise between them.  Errors are returned as
+ * statuses only (there is no context to hold a message). */
+j2k_status j2k_dwt_forward_noalloc(void* cuda_stream, int kernel, int order, const void* in,
+                                   size_t in_pitch, void* out, size_t out_pitch, size_t w, size_t h,
+                                   int levels, const float* steps);
+
 /* ---- EBCOT tier-1: replaces OCLBPC<T>::run (src/OCLBPC.cpp:38-50) and src/CL/oclbpc.cl:279-746.
  * Code-blocks partition every subband of a Mallat plane (w x h, `levels`) on a cbw x cbh grid
  * anchored at the subband origin, subbands in QCD order, blocks in raster order. */

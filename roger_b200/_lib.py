@@ -57,6 +57,7 @@ SIGS = {
     "j2k_planar_to_rgb": (I, [P, P, I, S, S, I, I, P, S, S, S]),
     "j2k_dwt_forward": (I, [P, I, I, P, S, P, S, S, S, I, P]),
     "j2k_dwt_inverse": (I, [P, I, I, P, S, P, S, S, S, I, P]),
+    "j2k_dwt_forward_noalloc": (I, [P, I, I, P, S, P, S, S, S, I, P]),
     "j2k_codeblock_count": (S, [S, S, I, I, I]),
     "j2k_bpc_encode": (I, [P, P, S, S, S, I, I, I, P, P, S]),
     "j2k_bpc_decode": (I, [P, P, P, S, P, S, S, S, I, I, I]),
