@@ -27,18 +27,16 @@
 
 namespace {
 
-constexpr int kWarpsPerCta = 4;
-constexpr int kPlanesShared = 16;   // magnitude planes kept in shared memory; more are sliced from global
+constexpr int kWarpsPerCta = 8;
 constexpr int kRows = 64;
-constexpr int kMaxStage = 20;       // symbols per lane per stripe pass (2 columns x 10)
+constexpr int kPlaneWords = 32 * kRows;  // per-block bit-plane scratch: 64 rows x 32 planes
 
 struct WarpSmem {
-    uint64_t planes[kPlanesShared][kRows];
-    uint64_t sig[kRows + 2], vis[kRows + 2], ref[kRows + 2], neg[kRows + 2];
-    uint8_t stage[32][kMaxStage];
+    uint64_t sig[kRows + 2], vis[kRows + 2], ref[kRows + 2], neg[kRows + 2];  // index r+1
+    uint64_t bits[kRows];                                                      // current plane
 };
 
-// T.800 Table D.1 zero-coding labels, index [orient][h][v][d]
+// T.800 Table D.1 zero-coding label from (h, v, d) counts
 __device__ __forceinline__ int zc_label_calc(int orient, int h, int v, int d) {
     if (orient == J2K_BAND_HH) {
         int hv = h + v;
@@ -55,10 +53,7 @@ __device__ __forceinline__ int zc_label_calc(int orient, int h, int v, int d) {
     return d >= 2 ? 2 : d;
 }
 
-__device__ __forceinline__ uint64_t dil(uint64_t m) { return m | (m << 1) | (m >> 1); }
-__device__ __forceinline__ int bitat(uint64_t m, int c) { return (c < 0 || c > 63) ? 0 : (int)((m >> c) & 1); }
-
-// (label | xor<<7) for the sign context of a sample, T.800 Tables D.2/D.3
+// (label | xor<<7) of T.800 Tables D.2/D.3 from the horizontal / vertical contributions
 __device__ __forceinline__ int sc_code(int hc, int vc) {
     hc = max(-1, min(1, hc));
     vc = max(-1, min(1, vc));
@@ -68,59 +63,52 @@ __device__ __forceinline__ int sc_code(int hc, int vc) {
     return lab | (x << 7);
 }
 
-struct Ctx {
-    const int32_t* blk;   // block origin in the coefficient plane
-    size_t pitch;
-    int cw, ch;
-};
+__device__ __forceinline__ uint64_t dil(uint64_t m) { return m | (m << 1) | (m >> 1); }
 
-// bit-plane row mask for plane p >= kPlanesShared, sliced from global memory
-__device__ uint64_t plane_row_global(const Ctx& c, int p, int r, int lane) {
-    uint32_t lo = 0, hi = 0;
-    int32_t v0 = (lane < c.cw) ? c.blk[(size_t)r * c.pitch + lane] : 0;
-    int32_t v1 = (lane + 32 < c.cw) ? c.blk[(size_t)r * c.pitch + lane + 32] : 0;
-    uint32_t m0 = v0 < 0 ? (uint32_t)(-(int64_t)v0) : (uint32_t)v0;
-    uint32_t m1 = v1 < 0 ? (uint32_t)(-(int64_t)v1) : (uint32_t)v1;
-    lo = __ballot_sync(0xffffffffu, (m0 >> p) & 1);
-    hi = __ballot_sync(0xffffffffu, (m1 >> p) & 1);
-    return (uint64_t)lo | ((uint64_t)hi << 32);
+// 4-bit window of a row mask around this lane's column pair: bit 0 = column c0-1 ...
+// bit 3 = column c0+2 (columns outside 0..63 read as 0)
+__device__ __forceinline__ uint32_t win4(uint64_t m, int c0) {
+    return (uint32_t)(c0 ? (m >> (c0 - 1)) : (m << 1)) & 0xF;
 }
 
-__device__ __forceinline__ uint64_t plane_row(const WarpSmem& S, const Ctx& c, int p, int r, int lane) {
-    if (r >= c.ch || r < 0) return 0;
-    if (p < kPlanesShared) return S.planes[p][r];
-    return plane_row_global(c, p, r, lane);
-}
-
-// emit staged symbols of all lanes in lane order; returns the warp total
-__device__ __forceinline__ int flush_stage(WarpSmem& S, int lane, int cnt, uint8_t* out, int pos,
-                                           int cap, bool& ovf) {
-    int inc = cnt;
+// warp exclusive prefix sum; returns the total in *tot
+__device__ __forceinline__ int warp_excl(int v, int lane, int* tot) {
+    int inc = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         int t = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= o) inc += t;
     }
-    int total = __shfl_sync(0xffffffffu, inc, 31);
-    int off = pos + inc - cnt;
-    if (pos + total > cap) {
-        ovf = true;
-        return total;
-    }
-    for (int k = 0; k < cnt; ++k) out[off + k] = S.stage[lane][k];
-    return total;
+    *tot = __shfl_sync(0xffffffffu, inc, 31);
+    return inc - v;
 }
+
+// Context/decision emission for one coded sample: ZC (or SC) from 3-bit neighbour windows.
+// zlut: 256-entry zero-coding table of this orientation indexed by the 8 neighbour bits
+// (W E N S NW NE SW SE); slut: sign table indexed by (sig W E N S) | (neg W E N S) << 4.
+struct Lut {
+    const uint8_t* z;
+    const uint8_t* s;
+};
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_job* __restrict__ jobs,
                   int njobs, uint8_t* __restrict__ syms, size_t sym_cap, uint32_t* __restrict__ nsyms,
-                  uint32_t* __restrict__ pass_end, j2k_cb_desc* __restrict__ descs,
-                  size_t cap_per_block, uint32_t* __restrict__ err) {
+                  uint32_t* __restrict__ pass_end, uint64_t* __restrict__ plane_scratch,
+                  j2k_cb_desc* __restrict__ descs, size_t cap_per_block, uint32_t* __restrict__ err) {
     __shared__ WarpSmem smem[kWarpsPerCta];
-    __shared__ uint8_t zc_lut[4][3][3][5];
-    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) {
-        int o = i / 45, r = i % 45;
-        zc_lut[o][r / 15][(r / 5) % 3][r % 5] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
+    __shared__ uint8_t zlut[4][256];
+    __shared__ uint8_t slut[256];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+        int o = i >> 8, b = i & 255;
+        int W = b & 1, E = (b >> 1) & 1, N = (b >> 2) & 1, S = (b >> 3) & 1;
+        int d = ((b >> 4) & 1) + ((b >> 5) & 1) + ((b >> 6) & 1) + ((b >> 7) & 1);
+        zlut[o][b] = (uint8_t)zc_label_calc(o, W + E, N + S, d);
+    }
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        int sg = i & 15, ng = i >> 4;
+        auto ct = [&](int k) { return ((sg >> k) & 1) ? (((ng >> k) & 1) ? -1 : 1) : 0; };
+        slut[i] = (uint8_t)sc_code(ct(0) + ct(1), ct(2) + ct(3));
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -135,38 +123,40 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
         }
         return;
     }
-    Ctx c{coeff + (size_t)J.y0 * pitch + J.x0, pitch, J.cw, J.ch};
-    const int orient = J.orient;
-    const uint64_t colmask = c.cw == 64 ? ~0ull : ((1ull << c.cw) - 1);
+    const int cw = J.cw, ch = J.ch;
+    const int32_t* blk = coeff + (size_t)J.y0 * pitch + J.x0;
+    const uint8_t* zl = zlut[J.orient];
+    const uint64_t colmask = cw == 64 ? ~0ull : ((1ull << cw) - 1);
+    uint64_t* planes = plane_scratch + (size_t)jid * kPlaneWords;
 
-    // ---- slice magnitudes into bit-plane masks; signs; numbps
+    // ---- bit-plane slicing: lane p ends up holding plane p of each row and stores it
     uint32_t mor = 0;
-    for (int r = 0; r < c.ch; ++r) {
-        int32_t v0 = (lane < c.cw) ? c.blk[(size_t)r * pitch + lane] : 0;
-        int32_t v1 = (lane + 32 < c.cw) ? c.blk[(size_t)r * pitch + lane + 32] : 0;
+    for (int r = 0; r < ch; ++r) {
+        int32_t v0 = (lane < cw) ? blk[(size_t)r * pitch + lane] : 0;
+        int32_t v1 = (lane + 32 < cw) ? blk[(size_t)r * pitch + lane + 32] : 0;
         uint32_t m0 = v0 < 0 ? (uint32_t)(-(int64_t)v0) : (uint32_t)v0;
         uint32_t m1 = v1 < 0 ? (uint32_t)(-(int64_t)v1) : (uint32_t)v1;
         mor |= m0 | m1;
         uint64_t ng = (uint64_t)__ballot_sync(0xffffffffu, v0 < 0) |
                       ((uint64_t)__ballot_sync(0xffffffffu, v1 < 0) << 32);
-        if (lane == 0) S.neg[r + 1] = ng;
-#pragma unroll 4
-        for (int p = 0; p < kPlanesShared; ++p) {
+        uint32_t any = __reduce_or_sync(0xffffffffu, m0 | m1);
+        uint64_t mine = 0;
+        for (int p = 0; p < 32 && (any >> p); ++p) {
             uint64_t pm = (uint64_t)__ballot_sync(0xffffffffu, (m0 >> p) & 1) |
                           ((uint64_t)__ballot_sync(0xffffffffu, (m1 >> p) & 1) << 32);
-            if (lane == 0) S.planes[p][r] = pm;
+            if (lane == p) mine = pm;
         }
+        planes[r * 32 + lane] = mine;  // row-major [row][plane]: one coalesced 256-byte store
+        if (lane == 0) S.neg[r + 1] = ng;
     }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) mor |= __shfl_xor_sync(0xffffffffu, mor, o);
+    mor = __reduce_or_sync(0xffffffffu, mor);
     const int numbps = mor ? 32 - __clz(mor) : 0;
     for (int r = lane; r < kRows + 2; r += 32) {
         S.sig[r] = 0;
         S.vis[r] = 0;
         S.ref[r] = 0;
-        if (r == 0 || r > c.ch) S.neg[r] = 0;
+        if (r == 0 || r > ch) S.neg[r] = 0;
     }
-    __syncwarp();
     j2k_cb_desc d;
     d.offset = (uint32_t)((size_t)jid * cap_per_block);
     d.length = 0;
@@ -188,77 +178,108 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
         }
         return;
     }
+    __syncwarp();
     uint8_t* out = syms + (size_t)jid * sym_cap;
     uint32_t* pend = pass_end + (size_t)jid * 92;
     const int cap = (int)sym_cap;
     int pos = 0, npass = 0;
     bool ovf = false;
-    const int nstripes = (c.ch + 3) >> 2;
-    const int c0 = 2 * lane, c1 = 2 * lane + 1;
+    const int nstripes = (ch + 3) >> 2;
+    const int c0 = 2 * lane;
+    const bool active = c0 < cw;
+    const uint32_t ownmask = active ? (c0 + 1 < cw ? 3u : 1u) : 0u;  // columns c0, c0+1 present
 
     for (int p = numbps - 1; p >= 0 && !ovf; --p) {
+        // current plane into shared (rows beyond ch are zero)
+        S.bits[lane] = lane < ch ? planes[lane * 32 + p] : 0;
+        S.bits[lane + 32] = lane + 32 < ch ? planes[(lane + 32) * 32 + p] : 0;
+        __syncwarp();
         if (p != numbps - 1) {
             // ------------------------- significance propagation pass
             for (int s = 0; s < nstripes && !ovf; ++s) {
                 const int r0 = 4 * s;
-                uint64_t O[6], A[6], B[4], C[4], M[4], E[4], N[6], K[4];
-                for (int j = -1; j <= 4; ++j) O[j + 1] = S.sig[r0 + j + 1];
+                uint64_t O[6], N[6], C[4], M[4], E[4], K[4], B[4];
+#pragma unroll
+                for (int j = 0; j < 6; ++j) O[j] = S.sig[r0 + j];
+                bool anyk = false;
+#pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    uint64_t V = (r0 + j < c.ch) ? colmask : 0;
-                    B[j] = plane_row(S, c, p, r0 + j, lane);
+                    const uint64_t V = (r0 + j < ch) ? colmask : 0;
+                    B[j] = S.bits[(r0 + j) & 63];
                     C[j] = ~O[j + 1] & V;
                     M[j] = C[j] & B[j];
-                    E[j] = dil(O[j]) | dil(O[j + 1]) | dil(O[j + 2]);
+                    E[j] = C[j] & (dil(O[j]) | dil(O[j + 1]) | dil(O[j + 2]));
+                    anyk |= E[j] != 0;
                 }
-                N[0] = N[1] = N[2] = N[3] = N[4] = N[5] = 0;
-                bool changed = true;
-                while (changed) {
+                if (!anyk) continue;  // no candidate has a significant neighbour: nothing coded
+                N[0] = N[5] = 0;
+                N[1] = N[2] = N[3] = N[4] = 0;
+                for (bool changed = true; changed;) {
                     changed = false;
+#pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         uint64_t seeds = M[j] & (E[j] | ((N[j] | N[j + 2]) << 1) | N[j]);
                         uint64_t nn = M[j] & (~(M[j] + seeds) | seeds);
-                        if (nn != N[j + 1]) { N[j + 1] = nn; changed = true; }
+                        changed |= nn != N[j + 1];
+                        N[j + 1] = nn;
                     }
                 }
-                for (int j = 0; j < 4; ++j)
-                    K[j] = C[j] & (E[j] | ((N[j] | N[j + 1] | N[j + 2]) << 1) | N[j]);
-                A[0] = O[0];
-                A[5] = O[5];
-                for (int j = 0; j < 4; ++j) A[j + 1] = O[j + 1] | N[j + 1];
-                uint64_t NG[6];
-                for (int j = -1; j <= 4; ++j) NG[j + 1] = S.neg[r0 + j + 1];
-                // contexts for this lane's two columns
-                int cnt = 0;
-                for (int cc = c0; cc <= c1; ++cc) {
-                    if (cc >= c.cw) break;
-                    for (int j = 0; j < 4; ++j) {
-                        if (!((K[j] >> cc) & 1)) continue;
-                        int w_ = bitat(A[j + 1], cc - 1), e_ = bitat(O[j + 1], cc + 1);
-                        int n_ = bitat(A[j], cc), s_ = bitat(O[j + 2], cc);
-                        int dd = bitat(A[j], cc - 1) + bitat(O[j], cc + 1) + bitat(A[j + 2], cc - 1) +
-                                 bitat(O[j + 2], cc + 1);
-                        int lab = zc_lut[orient][w_ + e_][n_ + s_][dd];
-                        int bit = (int)((B[j] >> cc) & 1);
-                        S.stage[lane][cnt++] = (uint8_t)(lab | (bit << 7));
-                        if (bit) {
-                            int hc = (w_ ? (bitat(NG[j + 1], cc - 1) ? -1 : 1) : 0) +
-                                     (e_ ? (bitat(NG[j + 1], cc + 1) ? -1 : 1) : 0);
-                            int vc = (n_ ? (bitat(NG[j], cc) ? -1 : 1) : 0) +
-                                     (s_ ? (bitat(NG[j + 2], cc) ? -1 : 1) : 0);
-                            int sc = sc_code(hc, vc);
-                            int sgn = bitat(NG[j + 1], cc);
-                            S.stage[lane][cnt++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+#pragma unroll
+                for (int j = 0; j < 4; ++j) K[j] = C[j] & (E[j] | ((N[j] | N[j + 1] | N[j + 2]) << 1) | N[j]);
+                // per-lane windows
+                uint32_t a[6], o[6], ng[6], kk = 0, nn4 = 0, bb = 0;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    o[j] = win4(O[j], c0);
+                    a[j] = win4(O[j] | N[j], c0);
+                    ng[j] = win4(S.neg[r0 + j], c0);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    kk |= ((win4(K[j], c0) >> 1) & ownmask) << (2 * j);
+                    nn4 |= ((win4(N[j + 1], c0) >> 1) & ownmask) << (2 * j);
+                    bb |= ((win4(B[j], c0) >> 1) & 3u) << (2 * j);
+                }
+                int cnt = __popc(kk) + __popc(nn4);
+                int tot;
+                int off = pos + warp_excl(cnt, lane, &tot);
+                if (pos + tot > cap) {
+                    ovf = true;
+                    break;
+                }
+                if (cnt) {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int bitpos = 2 * j + k;
+                            if (!((kk >> bitpos) & 1)) continue;
+                            const uint32_t up = ((a[j] >> k) & 3) | ((o[j] >> k) & 4);
+                            const uint32_t md = ((a[j + 1] >> k) & 1) | ((o[j + 1] >> k) & 4);
+                            const uint32_t dn = ((a[j + 2] >> k) & 1) | ((o[j + 2] >> k) & 6);
+                            // index: W E N S NW NE SW SE
+                            const uint32_t zi = (md & 1) | ((md >> 1) & 2) | ((up & 2) << 1) | ((dn & 2) << 2) |
+                                                ((up & 1) << 4) | ((up & 4) << 3) | ((dn & 1) << 6) | ((dn & 4) << 5);
+                            const int bit = (bb >> bitpos) & 1;
+                            out[off++] = (uint8_t)(zl[zi] | (bit << 7));
+                            if (bit) {
+                                const uint32_t sg4 = (zi & 15);
+                                const uint32_t nw = ng[j + 1] >> k, nu = ng[j] >> k, nd = ng[j + 2] >> k;
+                                const uint32_t ng4 = (nw & 1) | ((nw >> 1) & 2) | ((nu & 2) << 1) | ((nd & 2) << 2);
+                                const int sc = slut[sg4 | (ng4 << 4)];
+                                const int sgn = (ng[j + 1] >> (k + 1)) & 1;
+                                out[off++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                            }
                         }
-                    }
                 }
-                __syncwarp();
-                pos += flush_stage(S, lane, cnt, out, pos, cap, ovf);
-                __syncwarp();
-                if (lane == 0)
+                pos += tot;
+                if (lane == 0) {
+#pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        S.sig[r0 + j + 1] = A[j + 1];
+                        S.sig[r0 + j + 1] = O[j + 1] | N[j + 1];
                         S.vis[r0 + j + 1] = K[j];
                     }
+                }
                 __syncwarp();
             }
             if (lane == 0) pend[npass] = (uint32_t)pos;
@@ -266,32 +287,48 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
             // ------------------------- magnitude refinement pass
             for (int s = 0; s < nstripes && !ovf; ++s) {
                 const int r0 = 4 * s;
-                uint64_t SG[6], R[4], B[4], RF[4];
-                for (int j = -1; j <= 4; ++j) SG[j + 1] = S.sig[r0 + j + 1];
+                uint64_t SG[6], R[4];
+                bool anyr = false;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) SG[j] = S.sig[r0 + j];
+#pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     R[j] = SG[j + 1] & ~S.vis[r0 + j + 1];
-                    B[j] = plane_row(S, c, p, r0 + j, lane);
-                    RF[j] = S.ref[r0 + j + 1];
+                    anyr |= R[j] != 0;
                 }
-                int cnt = 0;
-                for (int cc = c0; cc <= c1; ++cc) {
-                    if (cc >= c.cw) break;
-                    for (int j = 0; j < 4; ++j) {
-                        if (!((R[j] >> cc) & 1)) continue;
-                        int lab;
-                        if ((RF[j] >> cc) & 1) lab = 16;
-                        else {
-                            uint64_t nb = dil(SG[j]) | dil(SG[j + 2]) | (SG[j + 1] << 1) | (SG[j + 1] >> 1);
-                            lab = ((nb >> cc) & 1) ? 15 : 14;
+                if (!anyr) continue;
+                uint32_t rr = 0, rf = 0, nb = 0, bb = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint64_t nbm = dil(SG[j]) | dil(SG[j + 2]) | (SG[j + 1] << 1) | (SG[j + 1] >> 1);
+                    rr |= ((win4(R[j], c0) >> 1) & ownmask) << (2 * j);
+                    rf |= ((win4(S.ref[r0 + j + 1], c0) >> 1) & 3u) << (2 * j);
+                    nb |= ((win4(nbm, c0) >> 1) & 3u) << (2 * j);
+                    bb |= ((win4(S.bits[(r0 + j) & 63], c0) >> 1) & 3u) << (2 * j);
+                }
+                const int cnt = __popc(rr);
+                int tot;
+                int off = pos + warp_excl(cnt, lane, &tot);
+                if (pos + tot > cap) {
+                    ovf = true;
+                    break;
+                }
+                if (cnt) {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int bitpos = 2 * j + k;
+                            if (!((rr >> bitpos) & 1)) continue;
+                            const int lab = ((rf >> bitpos) & 1) ? 16 : (((nb >> bitpos) & 1) ? 15 : 14);
+                            out[off++] = (uint8_t)(lab | (((bb >> bitpos) & 1) << 7));
                         }
-                        S.stage[lane][cnt++] = (uint8_t)(lab | (int)(((B[j] >> cc) & 1) << 7));
-                    }
                 }
-                __syncwarp();
-                pos += flush_stage(S, lane, cnt, out, pos, cap, ovf);
-                __syncwarp();
-                if (lane == 0)
-                    for (int j = 0; j < 4; ++j) S.ref[r0 + j + 1] = RF[j] | R[j];
+                pos += tot;
+                if (lane == 0) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) S.ref[r0 + j + 1] |= R[j];
+                }
                 __syncwarp();
             }
             if (lane == 0) pend[npass] = (uint32_t)pos;
@@ -300,77 +337,110 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
         // ------------------------- cleanup pass
         for (int s = 0; s < nstripes && !ovf; ++s) {
             const int r0 = 4 * s;
-            const bool full = r0 + 3 < c.ch;
-            uint64_t O[6], A[6], B[4], C[4], N[4], NG[6];
-            for (int j = -1; j <= 4; ++j) {
-                O[j + 1] = S.sig[r0 + j + 1];
-                NG[j + 1] = S.neg[r0 + j + 1];
-            }
+            const bool full = r0 + 3 < ch;
+            uint64_t O[6], C[4], N[4];
+            bool anyc = false;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) O[j] = S.sig[r0 + j];
+#pragma unroll
             for (int j = 0; j < 4; ++j) {
-                uint64_t V = (r0 + j < c.ch) ? colmask : 0;
-                B[j] = plane_row(S, c, p, r0 + j, lane);
+                const uint64_t V = (r0 + j < ch) ? colmask : 0;
                 C[j] = V & ~O[j + 1] & ~S.vis[r0 + j + 1];
-                N[j] = C[j] & B[j];
+                N[j] = C[j] & S.bits[(r0 + j) & 63];
+                anyc |= C[j] != 0;
             }
-            A[0] = O[0];
-            A[5] = O[5];
-            for (int j = 0; j < 4; ++j) A[j + 1] = O[j + 1] | N[j];
+            if (!anyc) continue;
+            uint32_t a[6], o[6], ng[6], cc = 0, nn4 = 0;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                o[j] = win4(O[j], c0);
+                a[j] = win4((j >= 1 && j <= 4) ? (O[j] | N[j - 1]) : O[j], c0);
+                ng[j] = win4(S.neg[r0 + j], c0);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                cc |= ((win4(C[j], c0) >> 1) & ownmask) << (2 * j);
+                nn4 |= ((win4(N[j], c0) >> 1) & ownmask) << (2 * j);
+            }
+            // per column: run-length mode?  (full stripe, 4 candidates, no significant neighbour)
+            uint32_t rlmask = 0;  // bit k: column c0+k codes in run-length mode
             int cnt = 0;
-            for (int cc = c0; cc <= c1; ++cc) {
-                if (cc >= c.cw) break;
-                int start = 0;
-                if (full && ((C[0] & C[1] & C[2] & C[3]) >> cc) & 1) {
-                    uint64_t lm = (cc > 0) ? (1ull << (cc - 1)) : 0;
-                    uint64_t rm = (cc + 1 < 64) ? (1ull << (cc + 1)) : 0;
-                    uint64_t cm = 1ull << cc;
-                    bool quiet = !((A[1] | A[2] | A[3] | A[4]) & lm) && !((O[1] | O[2] | O[3] | O[4]) & rm) &&
-                                 !((O[0] | O[5]) & (lm | cm | rm));
-                    if (quiet) {
-                        int first = -1;
-                        for (int j = 0; j < 4; ++j)
-                            if (first < 0 && ((N[j] >> cc) & 1)) first = j;
-                        S.stage[lane][cnt++] = (uint8_t)(17 | ((first >= 0) << 7));
-                        if (first < 0) continue;
-                        S.stage[lane][cnt++] = (uint8_t)(18 | (((first >> 1) & 1) << 7));
-                        S.stage[lane][cnt++] = (uint8_t)(18 | ((first & 1) << 7));
-                        int j = first;
-                        int w_ = bitat(A[j + 1], cc - 1), e_ = bitat(O[j + 1], cc + 1);
-                        int n_ = bitat(A[j], cc), s_ = bitat(O[j + 2], cc);
-                        int hc = (w_ ? (bitat(NG[j + 1], cc - 1) ? -1 : 1) : 0) +
-                                 (e_ ? (bitat(NG[j + 1], cc + 1) ? -1 : 1) : 0);
-                        int vc = (n_ ? (bitat(NG[j], cc) ? -1 : 1) : 0) +
-                                 (s_ ? (bitat(NG[j + 2], cc) ? -1 : 1) : 0);
-                        int sc = sc_code(hc, vc);
-                        int sgn = bitat(NG[j + 1], cc);
-                        S.stage[lane][cnt++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
-                        start = first + 1;
-                    }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t colc = (cc >> k) & 0x55;  // bits 0,2,4,6: rows 0..3
+                const uint32_t coln = (nn4 >> k) & 0x55;
+                bool rl = false;
+                if (full && colc == 0x55) {
+                    uint32_t q = 0;
+#pragma unroll
+                    for (int j = 1; j <= 4; ++j) q |= ((a[j] >> k) & 1) | ((o[j] >> k) & 4);
+                    q |= ((o[0] >> k) & 7) | ((o[5] >> k) & 7);
+                    rl = q == 0;
                 }
-                for (int j = start; j < 4; ++j) {
-                    if (!((C[j] >> cc) & 1)) continue;
-                    int w_ = bitat(A[j + 1], cc - 1), e_ = bitat(O[j + 1], cc + 1);
-                    int n_ = bitat(A[j], cc), s_ = bitat(O[j + 2], cc);
-                    int dd = bitat(A[j], cc - 1) + bitat(O[j], cc + 1) + bitat(A[j + 2], cc - 1) +
-                             bitat(O[j + 2], cc + 1);
-                    int lab = zc_lut[orient][w_ + e_][n_ + s_][dd];
-                    int bit = (int)((B[j] >> cc) & 1);
-                    S.stage[lane][cnt++] = (uint8_t)(lab | (bit << 7));
-                    if (bit) {
-                        int hc = (w_ ? (bitat(NG[j + 1], cc - 1) ? -1 : 1) : 0) +
-                                 (e_ ? (bitat(NG[j + 1], cc + 1) ? -1 : 1) : 0);
-                        int vc = (n_ ? (bitat(NG[j], cc) ? -1 : 1) : 0) +
-                                 (s_ ? (bitat(NG[j + 2], cc) ? -1 : 1) : 0);
-                        int sc = sc_code(hc, vc);
-                        int sgn = bitat(NG[j + 1], cc);
-                        S.stage[lane][cnt++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                if (rl) {
+                    rlmask |= 1u << k;
+                    if (coln) {
+                        const int first = (__ffs(coln) - 1) >> 1;  // row of the first 1
+                        int rest = 0;
+                        for (int j = first + 1; j < 4; ++j) rest += 1 + ((coln >> (2 * j)) & 1);
+                        cnt += 1 + 2 + 1 + rest;
+                    } else {
+                        cnt += 1;
+                    }
+                } else {
+                    cnt += __popc(colc) + __popc(coln);
+                }
+            }
+            int tot;
+            int off = pos + warp_excl(cnt, lane, &tot);
+            if (pos + tot > cap) {
+                ovf = true;
+                break;
+            }
+            if (cnt) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const uint32_t colc = (cc >> k) & 0x55;
+                    const uint32_t coln = (nn4 >> k) & 0x55;
+                    if (!colc) continue;
+                    int jstart = 0;
+                    if ((rlmask >> k) & 1) {
+                        out[off++] = (uint8_t)(17 | ((coln != 0) << 7));
+                        if (!coln) continue;
+                        const int first = (__ffs(coln) - 1) >> 1;
+                        out[off++] = (uint8_t)(18 | (((first >> 1) & 1) << 7));
+                        out[off++] = (uint8_t)(18 | ((first & 1) << 7));
+                        // sign of the first significant sample: its four neighbours are insignificant
+                        const int sgn = (ng[first + 1] >> (k + 1)) & 1;
+                        const int sc = slut[0];
+                        out[off++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                        jstart = first + 1;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (j < jstart || !((colc >> (2 * j)) & 1)) continue;
+                        const uint32_t up = ((a[j] >> k) & 3) | ((o[j] >> k) & 4);
+                        const uint32_t md = ((a[j + 1] >> k) & 1) | ((o[j + 1] >> k) & 4);
+                        const uint32_t dn = ((a[j + 2] >> k) & 1) | ((o[j + 2] >> k) & 6);
+                        const uint32_t zi = (md & 1) | ((md >> 1) & 2) | ((up & 2) << 1) | ((dn & 2) << 2) |
+                                            ((up & 1) << 4) | ((up & 4) << 3) | ((dn & 1) << 6) | ((dn & 4) << 5);
+                        const int bit = (coln >> (2 * j)) & 1;
+                        out[off++] = (uint8_t)(zl[zi] | (bit << 7));
+                        if (bit) {
+                            const uint32_t nw = ng[j + 1] >> k, nu = ng[j] >> k, nd = ng[j + 2] >> k;
+                            const uint32_t ng4 = (nw & 1) | ((nw >> 1) & 2) | ((nu & 2) << 1) | ((nd & 2) << 2);
+                            const int sc = slut[(zi & 15) | (ng4 << 4)];
+                            const int sgn = (ng[j + 1] >> (k + 1)) & 1;
+                            out[off++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                        }
                     }
                 }
             }
-            __syncwarp();
-            pos += flush_stage(S, lane, cnt, out, pos, cap, ovf);
-            __syncwarp();
-            if (lane == 0)
-                for (int j = 0; j < 4; ++j) S.sig[r0 + j + 1] = A[j + 1];
+            pos += tot;
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) S.sig[r0 + j + 1] = O[j + 1] | N[j];
+            }
             __syncwarp();
         }
         if (lane == 0) pend[npass] = (uint32_t)pos;
@@ -593,6 +663,8 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
     if (((uintptr_t)bytes & 15) != 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "t1: bytes buffer must be 16-byte aligned");
     uint8_t* syms = (uint8_t*)j2k_scratch(ctx, SCR_SYMS, njobs * sym_cap + 64);
+    uint64_t* planes = (uint64_t*)j2k_scratch(ctx, SCR_PLANES, njobs * kPlaneWords * 8 + 64);
+    if (!planes) return J2K_ERR_OUT_OF_MEMORY;
     // meta: nsyms | pass ends (92 per job) | sort keys/values (4 arrays of njobs)
     size_t meta_words = njobs * (1 + 92 + 4) + 64;
     uint32_t* meta = (uint32_t*)j2k_scratch(ctx, SCR_T1STATE, meta_words * 4);
@@ -604,7 +676,7 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
     uint32_t* idx_out = idx_in + njobs;
     unsigned ga = (unsigned)((njobs + kWarpsPerCta - 1) / kWarpsPerCta);
     t1_symbols_kernel<<<ga, kWarpsPerCta * 32, 0, st>>>(coeff, pitch, d_jobs, (int)njobs, syms, sym_cap,
-                                                        nsyms, pend, descs, cap_per_block, ctx->d_err);
+                                                        nsyms, pend, planes, descs, cap_per_block, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     // longest-first order for the MQ lanes
     iota_kernel<<<(unsigned)((njobs + 255) / 256), 256, 0, st>>>(idx_in, (int)njobs);
