@@ -58,7 +58,10 @@ j2k_status j2k_stream_sync(j2k_ctx* ctx);                          /* replaces c
 const char* j2k_last_error(const j2k_ctx* ctx);
 /* Launch-shape knobs (set by the autotuner; defaults are sensible).  No reference counterpart:
  * the reference fixed its OpenCL work-group shapes in -D build strings (src/OCLEncoder.cpp:27-29). */
-enum { J2K_TUNE_MQ_LANES = 1 };
+enum {
+    J2K_TUNE_MQ_LANES = 1,   /* one-lane-per-block MQ kernel: blocks per warp (8, 16, 32) */
+    J2K_TUNE_MQ_VARIANT = 2  /* 0: one lane per block (default); 1: state warp + code-register warp */
+};
 j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value);
 const char* j2k_status_string(j2k_status s);
 int j2k_version(void);

@@ -215,6 +215,11 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->mq_lanes = value;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_MQ_VARIANT) {
+        if (value != 0 && value != 1) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "MQ variant must be 0 or 1");
+        ctx->mq_variant = value;
+        return J2K_OK;
+    }
     return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown tuning key");
 }
 

@@ -30,7 +30,8 @@ struct j2k_ctx {
     void* h_pinned = nullptr;    // pinned staging
     size_t h_pinned_size = 0;
     int sm_count = 148;
-    int mq_lanes = 32;           // tier-1 MQ: code-blocks per warp (tuning knob)
+    int mq_lanes = 8;            // tier-1 MQ: code-blocks per warp (tuning knob)
+    int mq_variant = 0;          // 0: one lane per block, 1: state warp + code warp pair
 };
 
 // scratch slot ids

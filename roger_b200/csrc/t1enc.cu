@@ -646,6 +646,162 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
     descs[jid].length = len;
 }
 
+// ---- decoupled MQ coder: probability-state warp + code-register warp ---------------------------
+//
+// The MQ recurrences split cleanly: the interval register A and the 19 context states never
+// read the code register C, and C (with its byte output) only needs, per symbol, the value
+// Qe, whether Qe is added to C, and the renormalisation shift.  Warp 0 of each CTA runs the
+// A/state recurrence for 32 blocks (one per lane, branch-free) and writes one packed entry
+// per symbol (Qe | add<<16 | shift<<17) into a double-buffered shared ring; warp 1 runs the C
+// recurrence and the T.800 C.2 byte output one 32-symbol chunk behind.  Each warp carries
+// half of the serial chain and the two halves overlap.
+constexpr int kPairChunk = 32;
+
+__global__ void __launch_bounds__(64)
+t1_mq_pair_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* __restrict__ nsyms,
+                  const uint32_t* __restrict__ order, int njobs, uint8_t* __restrict__ bytes,
+                  size_t cap_per_block, j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+    __shared__ uint32_t tab[47];
+    __shared__ uint32_t cst[20 * 32];
+    __shared__ uint32_t ring[2][kPairChunk][32];
+    __shared__ uint32_t finalA[32];
+    for (int i = threadIdx.x; i < 47; i += blockDim.x)
+        tab[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
+                 ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gid = blockIdx.x * 32 + lane;
+    const bool live = gid < njobs;
+    const int jid = live ? (order ? (int)order[gid] : gid) : 0;
+    const int n = live ? (int)min((size_t)nsyms[jid], sym_cap) : 0;
+    int nmax = n;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    const int nchunks = (nmax + kPairChunk - 1) / kPairChunk;
+    if (warp == 0) {
+        // ------------------------------------------------ probability-state warp
+        uint32_t* st = cst + lane;  // context k at st[32*k]
+        for (int k = 0; k < 19; ++k) st[32 * k] = tab[0];
+        st[0] = tab[4];
+        st[32 * 17] = tab[3];
+        st[32 * 18] = tab[46];
+        uint32_t A = 0x8000;
+        const uint4* sp4 = reinterpret_cast<const uint4*>(syms + (size_t)jid * sym_cap);
+        const int nq = (n + 15) >> 4;  // 16-symbol chunks of this lane
+        const uint4 z4 = make_uint4(0, 0, 0, 0);
+        uint4 q0 = nq > 0 ? __ldcs(sp4) : z4, q1 = nq > 1 ? __ldcs(sp4 + 1) : z4;
+        uint4 q2 = nq > 2 ? __ldcs(sp4 + 2) : z4, q3 = nq > 3 ? __ldcs(sp4 + 3) : z4;
+        int cx = min((int)(q0.x & 31), 18);
+        uint32_t ent = st[32 * cx];
+        for (int k = 0; k <= nchunks; ++k) {
+            if (k < nchunks) {
+                const uint32_t w[9] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x};
+                const int base = k * kPairChunk;
+                uint32_t* rb = &ring[k & 1][0][lane];
+#pragma unroll
+                for (int j = 0; j < kPairChunk; ++j) {
+                    const bool valid = base + j < n;
+                    const uint32_t sym = (w[j >> 2] >> (8 * (j & 3))) & 0xFF;
+                    const uint32_t nsym = (w[(j + 1) >> 2] >> (8 * ((j + 1) & 3))) & 0xFF;
+                    const int ncx = min((int)(nsym & 31), 18);
+                    uint32_t nent = st[32 * ncx];
+                    const uint32_t qe = valid ? (ent & 0xFFFF) : 0u;
+                    const int mps = ent >> 31;
+                    const bool is_mps = !valid || ((int)(sym >> 7) == mps);
+                    const uint32_t a1 = A - qe;
+                    const bool fast = is_mps && (a1 & 0x8000);
+                    const bool addc = fast || (is_mps != (a1 < qe));
+                    const uint32_t a2 = addc ? a1 : qe;
+                    const int sh = __clz(a2) - 16;
+                    A = a2 << sh;
+                    const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
+                    const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
+                    const uint32_t upd = tab[nidx] | (nmps << 31);
+                    if (!fast) {
+                        st[32 * cx] = upd;
+                        if (ncx == cx) nent = upd;
+                    }
+                    rb[32 * j] = qe | ((uint32_t)addc << 16) | ((uint32_t)sh << 17);
+                    cx = ncx;
+                    ent = nent;
+                }
+                // advance the symbol window by two 16-symbol chunks, keeping two in flight
+                const int nextq = 2 * (k + 1);
+                q0 = q2;
+                q1 = q3;
+                q2 = nextq + 2 < nq ? __ldcs(sp4 + nextq + 2) : z4;
+                q3 = nextq + 3 < nq ? __ldcs(sp4 + nextq + 3) : z4;
+            } else {
+                finalA[lane] = A;
+            }
+            __syncthreads();
+        }
+    } else {
+        // ------------------------------------------------ code-register warp
+        MqEnc e;
+        e.A = 0;
+        e.C = 0;
+        e.B = 0;
+        e.CT = 12;
+        e.bp = -1;
+        e.out = reinterpret_cast<uint32_t*>(bytes + (size_t)jid * cap_per_block);
+        e.cap = (int)cap_per_block;
+        e.wacc = 0;
+        e.wn = 0;
+        e.wbase = 0;
+        e.ovf = false;
+        for (int k = 0; k <= nchunks; ++k) {
+            if (k > 0) {
+                const uint32_t* rb = &ring[(k - 1) & 1][0][lane];
+#pragma unroll 8
+                for (int j = 0; j < kPairChunk; ++j) {
+                    const uint32_t en = rb[32 * j];
+                    e.C += (en & 0xFFFF) & (0u - ((en >> 16) & 1));
+                    int sh = (int)(en >> 17);
+                    if (sh < e.CT) {
+                        e.C <<= sh;
+                        e.CT -= sh;
+                    } else {
+                        while (sh > 0) {
+                            const int kk = min(sh, e.CT);
+                            e.C <<= kk;
+                            e.CT -= kk;
+                            sh -= kk;
+                            if (e.CT == 0) e.byteout();
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (!live) return;
+        int len = 0;
+        if (n > 0) {
+            e.A = finalA[lane];
+            uint32_t tempc = e.C + e.A;
+            e.C |= 0xFFFF;
+            if (e.C >= tempc) e.C -= 0x8000;
+            e.C <<= e.CT;
+            e.byteout();
+            e.C <<= e.CT;
+            e.byteout();
+            len = e.bp + 1;
+            if (e.B == 0xFF) len--;
+            e.push(e.B);
+            uint8_t* bb = bytes + (size_t)jid * cap_per_block;
+            for (int k = 0; k < e.wn; ++k) {
+                if (e.wbase + k < e.cap) bb[e.wbase + k] = (uint8_t)(e.wacc >> (8 * k));
+                else e.ovf = true;
+            }
+        }
+        if (e.ovf || len > (int)cap_per_block) {
+            atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_OUT_CAPACITY);
+            len = 0;
+        }
+        descs[jid].length = len;
+    }
+}
+
 __global__ void iota_kernel(uint32_t* v, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = (uint32_t)i;
@@ -686,6 +842,13 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
     if (!tbuf) return J2K_ERR_OUT_OF_MEMORY;
     J2K_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, nsyms, keys_out, idx_in, idx_out,
                                                             (int)njobs, 0, 32, st));
+    if (ctx->mq_variant == 1) {
+        unsigned gp = (unsigned)((njobs + 31) / 32);
+        t1_mq_pair_kernel<<<gp, 64, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block,
+                                             descs, ctx->d_err);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
     const int lanes = ctx->mq_lanes;  // active lanes (blocks) per warp: 32, 16 or 8
     const size_t per_cta = (size_t)lanes * (kMqThreads / 32);
     unsigned gb = (unsigned)((njobs + per_cta - 1) / per_cta);
