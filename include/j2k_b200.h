@@ -195,6 +195,47 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs
                                       int ncomp, size_t w, size_t h, const j2k_enc_params* params,
                                       uint8_t* out, int out_on_device, size_t out_pitch_bytes);
 
+/* ---- batched encoder.  No counterpart in the reference, which encodes one image per
+ * OCLEncoder<T>::run call (src/OCLEncoder.cpp:43-52).  Many images of uneven size, mixed 5/3 and
+ * 9/7, are encoded by one fixed launch sequence (batched planar split, one DWT launch per level
+ * and filter, one persistent tier-1 pass over a device-side queue of all code-blocks, one MQ
+ * launch), captured once in a CUDA graph and replayed. */
+typedef struct {
+    uint32_t w, h;
+    int ncomp;           /* 1 or 3 */
+    int kernel;          /* J2K_W53: lossless (RCT); J2K_W97: ICT + dead-zone quantiser */
+    int levels;          /* 1..32 */
+    int cb;              /* square code-block side: power of two in 4..64 */
+    const float* steps;  /* 9/7: 3*levels+1 steps (copied); NULL = 8*2^-level */
+} j2k_batch_image;
+typedef struct j2k_batch j2k_batch;
+enum {
+    J2K_BATCH_USE_GRAPH = 1,     /* 1 (default): capture the launch sequence once, replay it */
+    J2K_BATCH_TILE53 = 2,        /* DWT tile shape of 5/3 images: 0 64x64, 1 128x32, 2 32x128 */
+    J2K_BATCH_TILE97 = 3,        /* same for 9/7 images */
+    J2K_BATCH_PHASE_A_ORDER = 4, /* 1: context modelling takes the largest code-blocks first */
+    J2K_BATCH_MQ_VARIANT = 5,    /* read-only here; set with j2k_ctx_set_tuning */
+    J2K_BATCH_MQ_LANES = 6
+};
+j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, j2k_batch** out);
+j2k_status j2k_batch_destroy(j2k_batch* b);
+/* The batch's packed device input buffer and each image's byte offset in it (n+1 entries,
+ * the last is the total): interleaved uint8 pixels, rows packed (pitch = w*ncomp). */
+j2k_status j2k_batch_input(j2k_batch* b, uint8_t** device_buffer, size_t* offsets);
+/* Encodes the batch.  pixels: per-image pointers (host or device) copied into the input buffer
+ * first, or NULL when the caller filled the input buffer itself. */
+j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_device);
+j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value);
+j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value);
+/* Times the tile shapes and code-block-to-warp schedules on this batch and keeps the fastest;
+ * report (optional, 5 ints): tile53, tile97, phase-A order, MQ variant, MQ blocks per warp. */
+j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report);
+/* Per-image results of the last encode: code-blocks (layout of j2k_encoder_get_codeblocks) and
+ * the T.800 codestream. */
+j2k_status j2k_batch_get_codeblocks(j2k_batch* b, int image, j2k_cb_desc* descs, size_t* count,
+                                    uint8_t* bytes, size_t cap, size_t* used);
+j2k_status j2k_batch_get_codestream(j2k_batch* b, int image, uint8_t* out, size_t cap, size_t* len);
+
 #ifdef __cplusplus
 }
 #endif

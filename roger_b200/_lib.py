@@ -73,7 +73,21 @@ SIGS = {
     "j2k_decoder_create": (I, [P, I, C.POINTER(P)]),
     "j2k_decoder_destroy": (I, [P]),
     "j2k_decoder_run_codeblocks": (I, [P, P, P, S, I, I, S, S, P, P, I, S]),
+    "j2k_batch_create": (I, [P, P, I, C.POINTER(P)]),
+    "j2k_batch_destroy": (I, [P]),
+    "j2k_batch_input": (I, [P, C.POINTER(P), P]),
+    "j2k_batch_encode": (I, [P, P, I]),
+    "j2k_batch_set_option": (I, [P, I, I]),
+    "j2k_batch_get_option": (I, [P, I, C.POINTER(I)]),
+    "j2k_batch_autotune": (I, [P, I, P]),
+    "j2k_batch_get_codeblocks": (I, [P, I, P, C.POINTER(S), P, S, C.POINTER(S)]),
+    "j2k_batch_get_codestream": (I, [P, I, P, S, C.POINTER(S)]),
 }
+
+
+class BatchImage(C.Structure):
+    _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("ncomp", C.c_int), ("kernel", C.c_int),
+                ("levels", C.c_int), ("cb", C.c_int), ("steps", C.c_void_p)]
 
 
 def exported_symbols():

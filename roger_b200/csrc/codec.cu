@@ -101,7 +101,7 @@ static j2k_status prepare_jobs(j2k_ctx* ctx, std::vector<j2k_cb_job>& hjobs, Dev
         return J2K_OK;
     }
     hjobs.clear();
-    for (int c = 0; c < ncomp; ++c) j2k_build_jobs(w, h, levels, cbw, cbh, &hjobs, c);
+    for (int c = 0; c < ncomp; ++c) j2k_build_jobs(w, h, levels, cbw, cbh, &hjobs, c, (uint64_t)c * w * h, w);
     J2K_TRY(djobs.ensure(ctx, std::max<size_t>(hjobs.size(), 1) * sizeof(j2k_cb_job)));
     J2K_CUDA(ctx, cudaMemcpyAsync(djobs.p, hjobs.data(), hjobs.size() * sizeof(j2k_cb_job),
                                   cudaMemcpyHostToDevice, ctx->stream));
@@ -153,12 +153,17 @@ static j2k_status encode_planes(j2k_encoder* e) {
     if (e->cap == 0) e->cap = align16(nblk * 2 + 256);
     if (e->sym_cap == 0) e->sym_cap = align16(nblk * 20 + 256);
     for (int attempt = 0; attempt < 6; ++attempt) {
+        if (e->hjobs.empty() || e->hjobs[0].out_cap != e->cap || e->hjobs[0].sym_cap != e->sym_cap) {
+            j2k_assign_capacities(e->hjobs, 0, e->cap, e->sym_cap, nullptr, nullptr);
+            J2K_CUDA(ctx, cudaMemcpyAsync(e->jobs.p, e->hjobs.data(), e->hjobs.size() * sizeof(j2k_cb_job),
+                                          cudaMemcpyHostToDevice, ctx->stream));
+        }
         J2K_TRY(e->descs.ensure(ctx, std::max<size_t>(e->njobs, 1) * sizeof(j2k_cb_desc)));
         J2K_TRY(e->bytes.ensure(ctx, std::max<size_t>(e->njobs, 1) * e->cap));
         J2K_TRY(j2k_clear_device_error(ctx));
-        J2K_TRY(j2k_t1_encode_jobs(ctx, (const int32_t*)e->coef.p, e->w, (const j2k_cb_job*)e->jobs.p,
-                                   e->njobs, (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p, e->cap,
-                                   e->sym_cap, ctx->stream));
+        J2K_TRY(j2k_t1_encode_jobs(ctx, (const int32_t*)e->coef.p, (const j2k_cb_job*)e->jobs.p,
+                                   e->njobs, (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p,
+                                   e->njobs * e->sym_cap, nullptr, ctx->stream));
         j2k_status s = j2k_read_device_error(ctx);
         if (s == J2K_OK) return J2K_OK;
         if (s != J2K_ERR_CAPACITY) return s;
@@ -209,15 +214,16 @@ j2k_status j2k_bpc_encode(j2k_ctx* ctx, const int32_t* coeff, size_t pitch, size
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_encode: cap_per_block must be a positive multiple of 16");
     cudaSetDevice(ctx->device);
     std::vector<j2k_cb_job> jobs;
-    j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, 0);
+    j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, 0, 0, pitch);
     j2k_cb_job* dj = (j2k_cb_job*)j2k_scratch(ctx, SCR_JOBS, jobs.size() * sizeof(j2k_cb_job) + 16);
     if (!dj) return J2K_ERR_OUT_OF_MEMORY;
-    J2K_CUDA(ctx, cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice, ctx->stream));
     size_t sym_cap = align16((size_t)cbw * cbh * 20 + 256);
     for (int attempt = 0; attempt < 6; ++attempt) {
+        j2k_assign_capacities(jobs, 0, cap_per_block, sym_cap, nullptr, nullptr);
+        J2K_CUDA(ctx, cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice, ctx->stream));
         J2K_TRY(j2k_clear_device_error(ctx));
-        J2K_TRY(j2k_t1_encode_jobs(ctx, coeff, pitch, dj, jobs.size(), descs, bytes, cap_per_block,
-                                   sym_cap, ctx->stream));
+        J2K_TRY(j2k_t1_encode_jobs(ctx, coeff, dj, jobs.size(), descs, bytes, jobs.size() * sym_cap, nullptr,
+                                   ctx->stream));
         j2k_status s = j2k_read_device_error(ctx);
         if (s == J2K_OK) return J2K_OK;
         if (s == J2K_ERR_CAPACITY && ctx->err.find("symbol") != std::string::npos) {
@@ -239,14 +245,14 @@ j2k_status j2k_bpc_decode(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t*
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_decode: bad levels or code-block size");
     cudaSetDevice(ctx->device);
     std::vector<j2k_cb_job> jobs;
-    j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, 0);
+    j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, 0, 0, pitch);
     if (jobs.size() != count)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_decode: count does not match the partition");
     j2k_cb_job* dj = (j2k_cb_job*)j2k_scratch(ctx, SCR_JOBS, jobs.size() * sizeof(j2k_cb_job) + 16);
     if (!dj) return J2K_ERR_OUT_OF_MEMORY;
     J2K_CUDA(ctx, cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice, ctx->stream));
     J2K_TRY(j2k_clear_device_error(ctx));
-    J2K_TRY(j2k_t1_decode_jobs(ctx, descs, bytes, dj, jobs.size(), coeff, pitch, ctx->stream));
+    J2K_TRY(j2k_t1_decode_jobs(ctx, descs, bytes, dj, jobs.size(), coeff, ctx->stream));
     return j2k_read_device_error(ctx);
 }
 
@@ -487,7 +493,7 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
     J2K_TRY(d->coef.ensure(ctx, n * 4 * ncomp));
     J2K_TRY(d->planes.ensure(ctx, n * 4 * ncomp));
     J2K_TRY(j2k_clear_device_error(ctx));
-    J2K_TRY(j2k_t1_decode_jobs(ctx, dd, db, (const j2k_cb_job*)d->jobs.p, njobs, (int32_t*)d->coef.p, w, ctx->stream));
+    J2K_TRY(j2k_t1_decode_jobs(ctx, dd, db, (const j2k_cb_job*)d->jobs.p, njobs, (int32_t*)d->coef.p, ctx->stream));
     std::vector<float> steps;
     if (d->lossy) {
         if (p && p->steps) steps.assign(p->steps, p->steps + 3 * levels + 1);

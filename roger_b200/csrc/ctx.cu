@@ -105,9 +105,10 @@ int j2k_band_rects(size_t w, size_t h, int levels, j2k_band_rect* out) {
 }
 
 size_t j2k_build_jobs(size_t w, size_t h, int levels, int cbw, int cbh,
-                      std::vector<j2k_cb_job>* jobs, int comp) {
+                      std::vector<j2k_cb_job>* jobs, int comp, uint64_t base, size_t pitch, uint32_t image) {
     j2k_band_rect r[3 * 32 + 1];
     int nb = j2k_band_rects(w, h, levels, r);
+    if (pitch == 0) pitch = w;
     size_t n = 0;
     for (int b = 0; b < nb; ++b) {
         if (!r[b].w || !r[b].h) continue;
@@ -115,11 +116,13 @@ size_t j2k_build_jobs(size_t w, size_t h, int levels, int cbw, int cbh,
             for (size_t x = 0; x < r[b].w; x += (size_t)cbw) {
                 if (jobs) {
                     j2k_cb_job j;
-                    j.x0 = (uint32_t)(r[b].x0 + x);
-                    j.y0 = (uint32_t)(r[b].y0 + y + (size_t)comp * h);
-                    j.px0 = (uint16_t)(r[b].x0 + x);
-                    j.py0 = (uint16_t)(r[b].y0 + y);
+                    const size_t px = r[b].x0 + x, py = r[b].y0 + y;
+                    j.off = base + (uint64_t)py * pitch + px;
+                    j.pitch = (uint32_t)pitch;
+                    j.px0 = (uint16_t)px;
+                    j.py0 = (uint16_t)py;
                     j.comp = (uint16_t)comp;
+                    j.image = image;
                     j.cw = (uint16_t)(r[b].w - x < (size_t)cbw ? r[b].w - x : (size_t)cbw);
                     j.ch = (uint16_t)(r[b].h - y < (size_t)cbh ? r[b].h - y : (size_t)cbh);
                     j.orient = (uint8_t)r[b].orient;
@@ -130,6 +133,22 @@ size_t j2k_build_jobs(size_t w, size_t h, int levels, int cbw, int cbh,
             }
     }
     return n;
+}
+
+void j2k_assign_capacities(std::vector<j2k_cb_job>& jobs, size_t first, size_t out_cap, size_t sym_cap,
+                           size_t* out_total, size_t* sym_total) {
+    uint64_t o = 0, y = 0;
+    for (size_t i = first; i < jobs.size(); ++i) {
+        j2k_cb_job& j = jobs[i];
+        j.out_cap = (uint32_t)out_cap;
+        j.sym_cap = (uint32_t)sym_cap;
+        j.out_off = o;
+        j.sym_off = y;
+        o += out_cap;
+        y += sym_cap;
+    }
+    if (out_total) *out_total = o;
+    if (sym_total) *sym_total = y;
 }
 
 static bool valid_cb(int v) { return v >= 4 && v <= 64 && (v & (v - 1)) == 0; }

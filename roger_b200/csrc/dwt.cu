@@ -147,15 +147,13 @@ struct Steps4 { float ll, hl, lh, hh; };
 // src: level input (w x h).  Detail subbands go to dst at Mallat positions (dst is the full
 // output plane); LL goes to ll_dst (T) unless QLL, in which case it is quantised into dst.
 template <int KERN, int ORDER, int TW, int TH, typename TD, bool QUANT, bool QLL>
-__global__ void __launch_bounds__(256)
-dwt_fwd_level(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
-              typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst,
-              size_t dpitch, Steps4 st) {
+__device__ __forceinline__ void fwd_tile(typename KT<KERN>::T* s, const typename KT<KERN>::T* __restrict__ src,
+                                         size_t spitch, int w, int h, typename KT<KERN>::T* __restrict__ ll_dst,
+                                         size_t llpitch, TD* __restrict__ dst, size_t dpitch, Steps4 st, int x0,
+                                         int y0) {
     using T = typename KT<KERN>::T;
     using G = Tile<KERN, TW, TH>;
     constexpr int H = G::H;
-    __shared__ T s[G::NY * G::S];
-    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     for (int e = threadIdx.x; e < G::NX * G::NY; e += blockDim.x) {
         int r = e / G::NX, c = e % G::NX;
         int gy = mirror(y0 - H + r, h), gx = mirror(x0 - H + c, w);
@@ -203,6 +201,42 @@ dwt_fwd_level(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w
                 dst[(size_t)sy * dpitch + sx] = (TD)v;
             }
         }
+    }
+}
+
+template <int KERN, int ORDER, int TW, int TH, typename TD, bool QUANT, bool QLL>
+__global__ void __launch_bounds__(256)
+dwt_fwd_level(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
+              typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst,
+              size_t dpitch, Steps4 st) {
+    using G = Tile<KERN, TW, TH>;
+    __shared__ typename KT<KERN>::T s[G::NY * G::S];
+    fwd_tile<KERN, ORDER, TW, TH, TD, QUANT, QLL>(s, src, spitch, w, h, ll_dst, llpitch, dst, dpitch, st,
+                                                 blockIdx.x * TW, blockIdx.y * TH);
+}
+
+// Batched forward level: CTA b takes tile b of a flattened tile list covering many images
+// (owner[b] = image slot, tiles numbered row-major within each image from d.tile0).
+template <int KERN, int ORDER, int TW, int TH>
+__global__ void __launch_bounds__(256)
+dwt_fwd_batched(const j2k_dwt_level_desc* __restrict__ descs, const uint32_t* __restrict__ owner) {
+    using T = typename KT<KERN>::T;
+    using G = Tile<KERN, TW, TH>;
+    __shared__ T s[G::NY * G::S];
+    const j2k_dwt_level_desc d = descs[owner[blockIdx.x]];
+    const int t = (int)(blockIdx.x - d.tile0);
+    const int x0 = (t % d.tiles_x) * TW, y0 = (t / d.tiles_x) * TH;
+    const Steps4 st{d.s_ll, d.s_hl, d.s_lh, d.s_hh};
+    if (KERN == 97 && (d.flags & 1)) {
+        if (d.flags & 2)
+            fwd_tile<KERN, ORDER, TW, TH, int32_t, true, true>(s, (const T*)d.src, d.spitch, d.w, d.h, (T*)d.ll_dst,
+                                                                d.llpitch, (int32_t*)d.dst, d.dpitch, st, x0, y0);
+        else
+            fwd_tile<KERN, ORDER, TW, TH, int32_t, true, false>(s, (const T*)d.src, d.spitch, d.w, d.h, (T*)d.ll_dst,
+                                                                 d.llpitch, (int32_t*)d.dst, d.dpitch, st, x0, y0);
+    } else {
+        fwd_tile<KERN, ORDER, TW, TH, T, false, false>(s, (const T*)d.src, d.spitch, d.w, d.h, (T*)d.ll_dst,
+                                                        d.llpitch, (T*)d.dst, d.dpitch, st, x0, y0);
     }
 }
 
@@ -429,4 +463,29 @@ j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in,
                                  (int)w, (int)h, levels, steps, ll0, ll1, st);
     return J2K_TILE_DISPATCH(inv_dispatch_order, 97, ctx, order, in, in_pitch, out, out_pitch,
                              (int)w, (int)h, levels, steps, ll0, ll1, st);
+}
+
+j2k_status j2k_dwt_fwd_batched_launch(j2k_ctx* ctx, int kernel, int order, j2k_dwt_tile tile,
+                                      const j2k_dwt_level_desc* d_descs, const uint32_t* d_owner,
+                                      unsigned ntiles, cudaStream_t st) {
+    if (ntiles == 0) return J2K_OK;
+#define BL(K, O, TW_, TH_) dwt_fwd_batched<K, O, TW_, TH_><<<ntiles, 256, 0, st>>>(d_descs, d_owner)
+#define BL_ORDER(K, TW_, TH_)                          \
+    do {                                               \
+        if (order == J2K_ORDER_REF) BL(K, J2K_ORDER_REF, TW_, TH_); \
+        else BL(K, J2K_ORDER_T800, TW_, TH_);          \
+    } while (0)
+#define BL_TILE(K)                                                          \
+    do {                                                                    \
+        if (tile.tw == 128 && tile.th == 32) BL_ORDER(K, 128, 32);          \
+        else if (tile.tw == 32 && tile.th == 128) BL_ORDER(K, 32, 128);     \
+        else BL_ORDER(K, 64, 64);                                           \
+    } while (0)
+    if (kernel == J2K_W53) BL_TILE(53);
+    else BL_TILE(97);
+#undef BL_TILE
+#undef BL_ORDER
+#undef BL
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
 }

@@ -61,15 +61,26 @@ int j2k_band_rects(size_t w, size_t h, int levels, j2k_band_rect* out);  // retu
 
 // code-block job for the tier-1 kernels (device side)
 struct j2k_cb_job {
-    uint32_t x0, y0;   // position in the (component-stacked) coefficient plane
+    uint64_t off;      // element offset of the block's first sample from the coefficient base
+    uint32_t pitch;    // row pitch of its plane (elements)
     uint16_t cw, ch;
     uint8_t orient, band;
     uint16_t comp;
     uint16_t px0, py0; // position within the component's Mallat plane
+    uint32_t image;    // image index (batched encoder), 0 otherwise
+    uint32_t out_cap;  // codeword capacity (bytes, multiple of 16)
+    uint32_t sym_cap;  // symbol-stream capacity (bytes, multiple of 16)
+    uint64_t out_off;  // codeword byte offset in the output buffer (16-aligned)
+    uint64_t sym_off;  // symbol-stream byte offset in the scratch buffer (16-aligned)
 };
-// Appends the jobs of one component plane (rows comp*h.. of a stacked plane) to *jobs.
+// Fills out/sym offsets of jobs[first..] uniformly (block i at i*cap) or, when per_sample
+// factors are given, proportionally to block area.  Returns total (out, sym) bytes.
+void j2k_assign_capacities(std::vector<j2k_cb_job>& jobs, size_t first, size_t out_cap, size_t sym_cap,
+                           size_t* out_total, size_t* sym_total);
+// Appends the jobs of one component plane, whose sample (0,0) sits at element `base` of the
+// coefficient buffer with row pitch `pitch`, to *jobs.
 size_t j2k_build_jobs(size_t w, size_t h, int levels, int cbw, int cbh, std::vector<j2k_cb_job>* jobs,
-                      int comp = 0);
+                      int comp = 0, uint64_t base = 0, size_t pitch = 0, uint32_t image = 0);
 
 // ---- launchers (defined in the .cu files) ---------------------------------------------------
 j2k_status j2k_launch_planar_fwd(j2k_ctx* ctx, const uint8_t* in, size_t in_pitch, int ncomp,
@@ -84,7 +95,34 @@ j2k_status j2k_launch_cast_planes(j2k_ctx* ctx, const void* src, int src_dtype, 
 j2k_status j2k_launch_mct_planes(j2k_ctx* ctx, void* planes, int dtype, size_t plane_stride,
                                  size_t n, int mct, cudaStream_t st);
 
+// one image of a batched planar split
+struct j2k_batch_planar_desc {
+    uint64_t in_off;     // byte offset of the interleaved pixels in the input buffer
+    uint64_t plane_off;  // element offset of plane 0 in the plane buffer
+    uint64_t stride;     // elements between planes (16-aligned)
+    uint64_t n;          // pixels
+    int ncomp, mct;
+};
+j2k_status j2k_launch_planar_batched(j2k_ctx* ctx, const j2k_batch_planar_desc* d_descs, const uint2* d_work,
+                                     unsigned nwork, const uint8_t* in_base, void* plane_base, int float_out,
+                                     cudaStream_t st);
+
 struct j2k_dwt_tile { int tw, th; };
+// one image at one decomposition level, for the batched forward DWT
+struct j2k_dwt_level_desc {
+    const void* src;    // level input (w x h)
+    void* ll_dst;       // LL output (unless flags & 2)
+    void* dst;          // full coefficient plane (Mallat positions)
+    size_t spitch, llpitch, dpitch;
+    int w, h;
+    float s_ll, s_hl, s_lh, s_hh;  // quantiser steps (9/7)
+    int flags;          // 1: quantise details (9/7), 2: this is the last level (LL quantised into dst)
+    int tiles_x;
+    uint32_t tile0;     // first flattened tile index of this image
+};
+j2k_status j2k_dwt_fwd_batched_launch(j2k_ctx* ctx, int kernel, int order, j2k_dwt_tile tile,
+                                      const j2k_dwt_level_desc* d_descs, const uint32_t* d_owner,
+                                      unsigned ntiles, cudaStream_t st);
 j2k_status j2k_dwt_fwd_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
@@ -94,13 +132,14 @@ j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
                             cudaStream_t st);
 
-j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
-                              const j2k_cb_job* d_jobs, size_t njobs, j2k_cb_desc* descs,
-                              uint8_t* bytes, size_t cap_per_block, size_t sym_cap_per_block,
-                              cudaStream_t st);
+// Tier-1 encode of njobs blocks.  order (device, optional): phase-A processing order (largest
+// first); sym_bytes: size of the symbol scratch the jobs' sym_off/sym_cap address.
+j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_job* d_jobs, size_t njobs,
+                              j2k_cb_desc* descs, uint8_t* bytes, size_t sym_bytes,
+                              const uint32_t* d_order, cudaStream_t st);
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
-                              size_t pitch, cudaStream_t st);
+                              cudaStream_t st);
 
 // host tier-2 writer
 struct j2k_t2_block {

@@ -258,7 +258,7 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
 __global__ void __launch_bounds__(kWarps * 32)
 t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
                  const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
-                 size_t pitch, uint32_t* __restrict__ err) {
+                 uint32_t* __restrict__ err) {
     __shared__ DecSmem smem[kWarps];
     __shared__ uint8_t zc_lut[4][3][3][5];
     for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) {
@@ -278,7 +278,8 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
         if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
         return;
     }
-    int32_t* blk = coeff + (size_t)J.y0 * pitch + J.x0;
+    const size_t pitch = J.pitch;
+    int32_t* blk = coeff + J.off;
     for (int r = 0; r < ch; ++r)
         for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
     for (int r = lane; r < 66; r += 32) { S.sig[r] = 0; S.neg[r] = 0; S.ref[r] = 0; S.vis[r] = 0; }
@@ -317,11 +318,11 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
 }
 
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
-                              const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff, size_t pitch,
+                              const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
                               cudaStream_t st) {
     if (njobs == 0) return J2K_OK;
     unsigned g = (unsigned)((njobs + kWarps - 1) / kWarps);
-    t1_decode_kernel<<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, pitch, ctx->d_err);
+    t1_decode_kernel<<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }

@@ -23,6 +23,8 @@
 // FLUSH of C.2.9, trailing 0xFF dropped); codeword bytes are written as aligned 32-bit words.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "j2k_internal.cuh"
 
 namespace {
@@ -92,10 +94,11 @@ struct Lut {
 };
 
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
-t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_job* __restrict__ jobs,
-                  int njobs, uint8_t* __restrict__ syms, size_t sym_cap, uint32_t* __restrict__ nsyms,
+t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__ jobs,
+                  int njobs, const uint32_t* __restrict__ order, uint32_t* __restrict__ queue,
+                  uint8_t* __restrict__ syms, uint32_t* __restrict__ nsyms,
                   uint32_t* __restrict__ pass_end, uint64_t* __restrict__ plane_scratch,
-                  j2k_cb_desc* __restrict__ descs, size_t cap_per_block, uint32_t* __restrict__ err) {
+                  j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
     __shared__ WarpSmem smem[kWarpsPerCta];
     __shared__ uint8_t zlut[4][256];
     __shared__ uint8_t slut[256];
@@ -112,22 +115,29 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int jid = blockIdx.x * kWarpsPerCta + wid;
-    if (jid >= njobs) return;
     WarpSmem& S = smem[wid];
+    // persistent: each warp pulls code-blocks from the device-side queue until it is empty;
+    // its bit-plane scratch slot is reused from block to block
+    uint64_t* planes = plane_scratch + (size_t)(blockIdx.x * kWarpsPerCta + wid) * kPlaneWords;
+    for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = (int)atomicAdd(queue, 1u);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= njobs) break;
+    const int jid = order ? (int)order[qi] : qi;
     const j2k_cb_job J = jobs[jid];
-    if (J.cw == 0 || J.ch == 0 || J.cw > 64 || J.ch > 64 || J.orient > 3) {
+    if (J.cw == 0 || J.ch == 0 || J.cw > 64 || J.ch > 64 || J.orient > 3 || J.sym_cap % 16 != 0) {
         if (lane == 0) {
             atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
             nsyms[jid] = 0;
         }
-        return;
+        continue;
     }
     const int cw = J.cw, ch = J.ch;
-    const int32_t* blk = coeff + (size_t)J.y0 * pitch + J.x0;
+    const size_t pitch = J.pitch;
+    const int32_t* blk = coeff + J.off;
     const uint8_t* zl = zlut[J.orient];
     const uint64_t colmask = cw == 64 ? ~0ull : ((1ull << cw) - 1);
-    uint64_t* planes = plane_scratch + (size_t)jid * kPlaneWords;
 
     // ---- bit-plane slicing: lane p ends up holding plane p of each row and stores it
     uint32_t mor = 0;
@@ -158,7 +168,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
         if (r == 0 || r > ch) S.neg[r] = 0;
     }
     j2k_cb_desc d;
-    d.offset = (uint32_t)((size_t)jid * cap_per_block);
+    d.offset = (uint32_t)J.out_off;
     d.length = 0;
     d.numbps = (uint8_t)numbps;
     d.npasses = (uint8_t)(numbps ? 3 * numbps - 2 : 0);
@@ -176,12 +186,13 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
             nsyms[jid] = 0;
             descs[jid] = d;
         }
-        return;
+        __syncwarp();
+        continue;
     }
     __syncwarp();
-    uint8_t* out = syms + (size_t)jid * sym_cap;
+    uint8_t* out = syms + J.sym_off;
     uint32_t* pend = pass_end + (size_t)jid * 92;
-    const int cap = (int)sym_cap;
+    const int cap = (int)J.sym_cap;
     int pos = 0, npass = 0;
     bool ovf = false;
     const int nstripes = (ch + 3) >> 2;
@@ -456,6 +467,8 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, size_t pitch, const j2k_cb_
         nsyms[jid] = (uint32_t)pos;
         descs[jid] = d;
     }
+    __syncwarp();
+    }  // queue loop
 }
 
 // ---- phase B: MQ encoder, one lane per code-block ------------------------------------------------
@@ -543,9 +556,9 @@ struct MqEnc {
 
 template <int LANES>
 __global__ void __launch_bounds__(kMqThreads)
-t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* __restrict__ nsyms,
+t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jobs, const uint32_t* __restrict__ nsyms,
              const uint32_t* __restrict__ order, int njobs, uint8_t* __restrict__ bytes,
-             size_t cap_per_block, j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+              j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
     __shared__ uint32_t tab[47];
     __shared__ uint32_t cst[19 * kMqThreads];
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
@@ -563,6 +576,8 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
     st[0] = tab[4];
     st[17 * kMqThreads] = tab[3];
     st[18 * kMqThreads] = tab[46];
+    const j2k_cb_job J = jobs[jid];
+    const size_t sym_cap = J.sym_cap, cap_per_block = J.out_cap;
     const int n = (int)min((size_t)nsyms[jid], sym_cap);
     MqEnc e;
     e.A = 0x8000;
@@ -570,7 +585,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
     e.B = 0;
     e.CT = 12;
     e.bp = -1;
-    e.out = reinterpret_cast<uint32_t*>(bytes + (size_t)jid * cap_per_block);
+    e.out = reinterpret_cast<uint32_t*>(bytes + J.out_off);
     e.cap = (int)cap_per_block;
     e.wacc = 0;
     e.wn = 0;
@@ -578,7 +593,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
     e.ovf = false;
     // Symbols stream in 16-byte chunks with two chunks in flight per lane; the next symbol's
     // context state is loaded one step ahead and forwarded when the current symbol updates it.
-    const uint4* sp4 = reinterpret_cast<const uint4*>(syms + (size_t)jid * sym_cap);
+    const uint4* sp4 = reinterpret_cast<const uint4*>(syms + J.sym_off);
     const int nchunks = (n + 15) >> 4;
     const uint4 z4 = make_uint4(0, 0, 0, 0);
     uint4 c0 = nchunks > 0 ? __ldcs(sp4) : z4;
@@ -633,7 +648,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
         len = e.bp + 1;
         if (e.B == 0xFF) len--;
         e.push(e.B);
-        uint8_t* bb = bytes + (size_t)jid * cap_per_block;
+        uint8_t* bb = bytes + J.out_off;
         for (int k = 0; k < e.wn; ++k) {
             if (e.wbase + k < e.cap) bb[e.wbase + k] = (uint8_t)(e.wacc >> (8 * k));
             else e.ovf = true;
@@ -658,9 +673,9 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* _
 constexpr int kPairChunk = 32;
 
 __global__ void __launch_bounds__(64)
-t1_mq_pair_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32_t* __restrict__ nsyms,
+t1_mq_pair_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jobs, const uint32_t* __restrict__ nsyms,
                   const uint32_t* __restrict__ order, int njobs, uint8_t* __restrict__ bytes,
-                  size_t cap_per_block, j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+                   j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
     __shared__ uint32_t tab[47];
     __shared__ uint32_t cst[20 * 32];
     __shared__ uint32_t ring[2][kPairChunk][32];
@@ -673,6 +688,8 @@ t1_mq_pair_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32
     const int gid = blockIdx.x * 32 + lane;
     const bool live = gid < njobs;
     const int jid = live ? (order ? (int)order[gid] : gid) : 0;
+    const j2k_cb_job J = jobs[jid];
+    const size_t sym_cap = J.sym_cap, cap_per_block = J.out_cap;
     const int n = live ? (int)min((size_t)nsyms[jid], sym_cap) : 0;
     int nmax = n;
 #pragma unroll
@@ -686,7 +703,7 @@ t1_mq_pair_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32
         st[32 * 17] = tab[3];
         st[32 * 18] = tab[46];
         uint32_t A = 0x8000;
-        const uint4* sp4 = reinterpret_cast<const uint4*>(syms + (size_t)jid * sym_cap);
+        const uint4* sp4 = reinterpret_cast<const uint4*>(syms + J.sym_off);
         const int nq = (n + 15) >> 4;  // 16-symbol chunks of this lane
         const uint4 z4 = make_uint4(0, 0, 0, 0);
         uint4 q0 = nq > 0 ? __ldcs(sp4) : z4, q1 = nq > 1 ? __ldcs(sp4 + 1) : z4;
@@ -744,7 +761,7 @@ t1_mq_pair_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32
         e.B = 0;
         e.CT = 12;
         e.bp = -1;
-        e.out = reinterpret_cast<uint32_t*>(bytes + (size_t)jid * cap_per_block);
+        e.out = reinterpret_cast<uint32_t*>(bytes + J.out_off);
         e.cap = (int)cap_per_block;
         e.wacc = 0;
         e.wn = 0;
@@ -788,7 +805,7 @@ t1_mq_pair_kernel(const uint8_t* __restrict__ syms, size_t sym_cap, const uint32
             len = e.bp + 1;
             if (e.B == 0xFF) len--;
             e.push(e.B);
-            uint8_t* bb = bytes + (size_t)jid * cap_per_block;
+            uint8_t* bb = bytes + J.out_off;
             for (int k = 0; k < e.wn; ++k) {
                 if (e.wbase + k < e.cap) bb[e.wbase + k] = (uint8_t)(e.wacc >> (8 * k));
                 else e.ovf = true;
@@ -809,30 +826,32 @@ __global__ void iota_kernel(uint32_t* v, int n) {
 
 }  // namespace
 
-j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
-                              const j2k_cb_job* d_jobs, size_t njobs, j2k_cb_desc* descs,
-                              uint8_t* bytes, size_t cap_per_block, size_t sym_cap,
-                              cudaStream_t st) {
+j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_job* d_jobs, size_t njobs,
+                              j2k_cb_desc* descs, uint8_t* bytes, size_t sym_bytes,
+                              const uint32_t* d_order, cudaStream_t st) {
     if (njobs == 0) return J2K_OK;
-    if (cap_per_block % 16 != 0 || sym_cap % 16 != 0)
-        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "t1: capacities must be multiples of 16");
     if (((uintptr_t)bytes & 15) != 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "t1: bytes buffer must be 16-byte aligned");
-    uint8_t* syms = (uint8_t*)j2k_scratch(ctx, SCR_SYMS, njobs * sym_cap + 64);
-    uint64_t* planes = (uint64_t*)j2k_scratch(ctx, SCR_PLANES, njobs * kPlaneWords * 8 + 64);
-    if (!planes) return J2K_ERR_OUT_OF_MEMORY;
-    // meta: nsyms | pass ends (92 per job) | sort keys/values (4 arrays of njobs)
-    size_t meta_words = njobs * (1 + 92 + 4) + 64;
+    uint8_t* syms = (uint8_t*)j2k_scratch(ctx, SCR_SYMS, sym_bytes + 64);
+    // persistent phase A: one bit-plane slot per resident warp
+    int per_sm = 0;
+    J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_symbols_kernel, kWarpsPerCta * 32, 0));
+    per_sm = std::max(per_sm, 1);
+    const size_t ctas = std::min<size_t>((njobs + kWarpsPerCta - 1) / kWarpsPerCta, (size_t)per_sm * ctx->sm_count);
+    uint64_t* planes = (uint64_t*)j2k_scratch(ctx, SCR_PLANES, ctas * kWarpsPerCta * kPlaneWords * 8 + 64);
+    // meta: queue head | nsyms | pass ends (92 per job) | sort keys/values (3 arrays of njobs)
+    size_t meta_words = 16 + njobs * (1 + 92 + 3) + 64;
     uint32_t* meta = (uint32_t*)j2k_scratch(ctx, SCR_T1STATE, meta_words * 4);
-    if (!syms || !meta) return J2K_ERR_OUT_OF_MEMORY;
-    uint32_t* nsyms = meta;
-    uint32_t* pend = meta + njobs;
+    if (!syms || !meta || !planes) return J2K_ERR_OUT_OF_MEMORY;
+    uint32_t* queue = meta;
+    uint32_t* nsyms = meta + 16;
+    uint32_t* pend = nsyms + njobs;
     uint32_t* keys_out = pend + njobs * 92;
     uint32_t* idx_in = keys_out + njobs;
     uint32_t* idx_out = idx_in + njobs;
-    unsigned ga = (unsigned)((njobs + kWarpsPerCta - 1) / kWarpsPerCta);
-    t1_symbols_kernel<<<ga, kWarpsPerCta * 32, 0, st>>>(coeff, pitch, d_jobs, (int)njobs, syms, sym_cap,
-                                                        nsyms, pend, planes, descs, cap_per_block, ctx->d_err);
+    J2K_CUDA(ctx, cudaMemsetAsync(queue, 0, 4, st));
+    t1_symbols_kernel<<<(unsigned)ctas, kWarpsPerCta * 32, 0, st>>>(coeff, d_jobs, (int)njobs, d_order, queue, syms,
+                                                                   nsyms, pend, planes, descs, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     // longest-first order for the MQ lanes
     iota_kernel<<<(unsigned)((njobs + 255) / 256), 256, 0, st>>>(idx_in, (int)njobs);
@@ -844,8 +863,7 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
                                                             (int)njobs, 0, 32, st));
     if (ctx->mq_variant == 1) {
         unsigned gp = (unsigned)((njobs + 31) / 32);
-        t1_mq_pair_kernel<<<gp, 64, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block,
-                                             descs, ctx->d_err);
+        t1_mq_pair_kernel<<<gp, 64, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
         J2K_CUDA(ctx, cudaGetLastError());
         return J2K_OK;
     }
@@ -853,11 +871,11 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, size_t pitch,
     const size_t per_cta = (size_t)lanes * (kMqThreads / 32);
     unsigned gb = (unsigned)((njobs + per_cta - 1) / per_cta);
     if (lanes == 8)
-        t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block, descs, ctx->d_err);
+        t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
     else if (lanes == 16)
-        t1_mq_kernel<16><<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block, descs, ctx->d_err);
+        t1_mq_kernel<16><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
     else
-        t1_mq_kernel<32><<<gb, kMqThreads, 0, st>>>(syms, sym_cap, nsyms, idx_out, (int)njobs, bytes, cap_per_block, descs, ctx->d_err);
+        t1_mq_kernel<32><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }
