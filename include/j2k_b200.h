@@ -60,7 +60,9 @@ const char* j2k_last_error(const j2k_ctx* ctx);
  * the reference fixed its OpenCL work-group shapes in -D build strings (src/OCLEncoder.cpp:27-29). */
 enum {
     J2K_TUNE_MQ_LANES = 1,   /* one-lane-per-block MQ kernel: blocks per warp (8, 16, 32) */
-    J2K_TUNE_MQ_VARIANT = 2  /* 0: one lane per block (default); 1: state warp + code-register warp */
+    J2K_TUNE_MQ_VARIANT = 2, /* 0: one lane per block (default); 1: state warp + code-register warp */
+    J2K_TUNE_DWT_FAST_TH = 3, /* register-lifting forward DWT tile height: 16 (default), 32, 0 = off */
+    J2K_TUNE_DWT_PIPE = 4     /* 1: that kernel streams bands with cp.async double buffering (default 0) */
 };
 j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value);
 const char* j2k_status_string(j2k_status s);

@@ -239,6 +239,16 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->mq_variant = value;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_DWT_FAST_TH) {
+        if (value != 0 && value != 16 && value != 32)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "fast DWT tile height must be 0, 16 or 32");
+        ctx->dwt_fast_th = value;
+        return J2K_OK;
+    }
+    if (key == J2K_TUNE_DWT_PIPE) {
+        ctx->dwt_pipe = value != 0;
+        return J2K_OK;
+    }
     return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown tuning key");
 }
 

@@ -17,6 +17,8 @@
 //   * the dead-zone quantiser (T.800 E.1) is fused into the writes of the final subbands; the
 //     inverse fuses the midpoint dequantiser into its loads.
 // HBM roofline per level: read c*n + write c*n bytes (c = 4), n = samples of the level.
+#include <algorithm>
+
 #include "j2k_internal.cuh"
 
 namespace {
@@ -240,6 +242,302 @@ dwt_fwd_batched(const j2k_dwt_level_desc* __restrict__ descs, const uint32_t* __
     }
 }
 
+// ---- fast forward level (T.800 order) ------------------------------------------------------------
+// One CTA produces a 248 x 32 tile of level outputs from a 256-column x (32 + 2*HV)-row strip:
+//   * rows are loaded with 16-byte vectors (mirrored scalar loads only where the strip leaves
+//     the image), columns x0-4 .. x0+251;
+//   * the vertical lifting runs in registers, one thread per column, the whole column unrolled;
+//   * the horizontal lifting runs in registers, 8 samples per lane, neighbours exchanged with
+//     warp shuffles (the 4-column halo absorbs the missing neighbours at the warp ends);
+//   * subbands are written straight from registers (8-byte vectors when aligned).
+// Same arithmetic, operation order and rounding as dwt_fwd_level, so the outputs are identical.
+constexpr int FTW = 248, FNX = 256;
+
+template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
+__global__ void __launch_bounds__(256, (KERN == 53 && FTH == 16) ? 8 : 6)
+dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
+             typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
+             Steps4 st, int vec_out) {
+    using T = typename KT<KERN>::T;
+    constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
+    __shared__ __align__(16) T s[NY][FNX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
+    const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * FTH;
+    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
+    // 1. load the strip
+    for (int r = warp; r < NY; r += 8) {
+        const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
+#pragma unroll
+        for (int q2 = 0; q2 < 2; ++q2) {
+            const int q = lane + 32 * q2;
+            const int gx = x0 - 4 + 4 * q;
+            uint4 v;
+            if (inner_x) {
+                v = __ldg(reinterpret_cast<const uint4*>(row + gx));
+            } else {
+                T e[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) e[k] = row[mirror(gx + k, w)];
+                v = *reinterpret_cast<uint4*>(e);
+            }
+            *reinterpret_cast<uint4*>(&s[r][4 * q]) = v;
+        }
+    }
+    __syncthreads();
+    // 2. vertical lifting of column t in registers
+    if (h > 1) {
+        T c[NY];
+#pragma unroll
+        for (int r = 0; r < NY; ++r) c[r] = s[r][t];
+#pragma unroll
+        for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+            const int par = 1 - (k & 1);
+#pragma unroll
+            for (int r = k + 1; r < NY - k - 1; ++r)
+                if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
+        }
+#pragma unroll
+        for (int r = HV; r < HV + FTH; ++r) {
+            T v = c[r];
+            if (KERN == 97) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
+            s[r][t] = v;
+        }
+    }
+    __syncthreads();
+    // 3. horizontal lifting per row, 8 samples per lane (tile columns 8*lane .. 8*lane+7)
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    const bool doh = w > 1;
+#pragma unroll
+    for (int i = 0; i < FTH / 8; ++i) {
+        const int r = HV + warp + 8 * i;
+        const int y = y0 + r - HV;
+        if (y >= h) break;
+        T v[8];
+        *reinterpret_cast<uint4*>(&v[0]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane]);
+        *reinterpret_cast<uint4*>(&v[4]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane + 4]);
+        if (doh) {
+#pragma unroll
+            for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+                if ((k & 1) == 0) {  // odd samples from their even neighbours
+                    const T nx = __shfl_down_sync(0xffffffffu, v[0], 1);
+                    v[1] = KT<KERN>::op(false, k, v[1], v[0], v[2]);
+                    v[3] = KT<KERN>::op(false, k, v[3], v[2], v[4]);
+                    v[5] = KT<KERN>::op(false, k, v[5], v[4], v[6]);
+                    v[7] = KT<KERN>::op(false, k, v[7], v[6], nx);
+                } else {             // even samples from their odd neighbours
+                    const T pv = __shfl_up_sync(0xffffffffu, v[7], 1);
+                    v[0] = KT<KERN>::op(false, k, v[0], pv, v[1]);
+                    v[2] = KT<KERN>::op(false, k, v[2], v[1], v[3]);
+                    v[4] = KT<KERN>::op(false, k, v[4], v[3], v[5]);
+                    v[6] = KT<KERN>::op(false, k, v[6], v[5], v[7]);
+                }
+            }
+            if (KERN == 97) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) v[j] = (T)__fmul_rn((float)v[j], (j & 1) ? KMUL : KDIV);
+            }
+        }
+        // subband rows: even y -> LL / HL, odd y -> LH / HH
+        const int qy = y & 1;
+        const int sy = (y >> 1) + (qy ? hl : 0);
+        const int xs = x0 - 4 + 8 * lane;  // absolute x of v[0] (even)
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {  // samples v[4*half .. 4*half+3]
+            const int e0 = 8 * lane + 4 * half;  // tile column of the first sample
+            const int xa = xs + 4 * half;
+            if (e0 + 4 <= 4 || e0 >= 252) continue;  // halo columns
+            for (int qx = 0; qx < 2; ++qx) {
+                const bool isll = (qx == 0 && qy == 0);
+                T a = v[4 * half + qx], b = v[4 * half + 2 + qx];
+                const int sx = (xa >> 1) + (qx ? wl : 0);  // band index of a (b is sx+1)
+                const bool va = xa + qx < w, vb = xa + 2 + qx < w;
+                if (isll && !QLL) {
+                    T* p = ll_dst + (size_t)sy * llpitch + sx;
+                    if (vec_out && va && vb) {
+                        T pr[2] = {a, b};
+                        *reinterpret_cast<uint2*>(p) = *reinterpret_cast<uint2*>(pr);
+                    } else {
+                        if (va) p[0] = a;
+                        if (vb) p[1] = b;
+                    }
+                } else {
+                    const float step = isll ? st.ll : (qx && qy ? st.hh : (qx ? st.hl : st.lh));
+                    TD oa, ob;
+                    if (QUANT) {
+                        oa = (TD)quantize((float)a, step);
+                        ob = (TD)quantize((float)b, step);
+                    } else {
+                        oa = (TD)a;
+                        ob = (TD)b;
+                    }
+                    TD* p = dst + (size_t)sy * dpitch + sx;
+                    if (vec_out && va && vb && ((sx & 1) == 0)) {
+                        TD pr[2] = {oa, ob};
+                        *reinterpret_cast<uint2*>(p) = *reinterpret_cast<uint2*>(pr);
+                    } else {
+                        if (va) p[0] = oa;
+                        if (vb) p[1] = ob;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---- pipelined fast forward level ------------------------------------------------------------
+// Same tile computation as dwt_fwd_fast, but each CTA walks a column strip band by band
+// (bands blockIdx.y, blockIdx.y + gridDim.y, ...) with two shared strips: while band i is
+// lifted, band i+1 streams into the other strip with cp.async (16-byte copies in the interior,
+// 4-byte mirrored copies at the image border), so loads are always in flight.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
+__global__ void __launch_bounds__(256)
+dwt_fwd_pipe(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
+             typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
+             Steps4 st, int vec_out, int nbands) {
+    using T = typename KT<KERN>::T;
+    constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
+    __shared__ __align__(16) T sb[2][NY][FNX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
+    const int x0 = blockIdx.x * FTW;
+    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    auto issue = [&](int band, int buf) {
+        const int y0 = band * FTH;
+        for (int e = t; e < NY * 64; e += 256) {
+            const int r = e >> 6, q = e & 63;
+            const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
+            const int gx = x0 - 4 + 4 * q;
+            T* d = &sb[buf][r][4 * q];
+            if (inner_x) {
+                cp_async16(d, row + gx);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) cp_async4(d + k, row + mirror(gx + k, w));
+            }
+        }
+    };
+    int band = blockIdx.y;
+    if (band < nbands) issue(band, 0);
+    cp_async_commit();
+    for (int it = 0; band < nbands; ++it, band += gridDim.y) {
+        const int buf = it & 1;
+        const int next = band + gridDim.y;
+        if (next < nbands) issue(next, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        auto& s = sb[buf];
+        const int y0 = band * FTH;
+        if (h > 1) {
+            T c[NY];
+#pragma unroll
+            for (int r = 0; r < NY; ++r) c[r] = s[r][t];
+#pragma unroll
+            for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+                const int par = 1 - (k & 1);
+#pragma unroll
+                for (int r = k + 1; r < NY - k - 1; ++r)
+                    if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
+            }
+#pragma unroll
+            for (int r = HV; r < HV + FTH; ++r) {
+                T v = c[r];
+                if (KERN == 97) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
+                s[r][t] = v;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < FTH / 8; ++i) {
+            const int r = HV + warp + 8 * i;
+            const int y = y0 + r - HV;
+            if (y >= h) break;
+            T v[8];
+            *reinterpret_cast<uint4*>(&v[0]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane]);
+            *reinterpret_cast<uint4*>(&v[4]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane + 4]);
+            if (w > 1) {
+#pragma unroll
+                for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+                    if ((k & 1) == 0) {
+                        const T nx = __shfl_down_sync(0xffffffffu, v[0], 1);
+                        v[1] = KT<KERN>::op(false, k, v[1], v[0], v[2]);
+                        v[3] = KT<KERN>::op(false, k, v[3], v[2], v[4]);
+                        v[5] = KT<KERN>::op(false, k, v[5], v[4], v[6]);
+                        v[7] = KT<KERN>::op(false, k, v[7], v[6], nx);
+                    } else {
+                        const T pv = __shfl_up_sync(0xffffffffu, v[7], 1);
+                        v[0] = KT<KERN>::op(false, k, v[0], pv, v[1]);
+                        v[2] = KT<KERN>::op(false, k, v[2], v[1], v[3]);
+                        v[4] = KT<KERN>::op(false, k, v[4], v[3], v[5]);
+                        v[6] = KT<KERN>::op(false, k, v[6], v[5], v[7]);
+                    }
+                }
+                if (KERN == 97) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) v[j] = (T)__fmul_rn((float)v[j], (j & 1) ? KMUL : KDIV);
+                }
+            }
+            const int qy = y & 1;
+            const int sy = (y >> 1) + (qy ? hl : 0);
+            const int xs = x0 - 4 + 8 * lane;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const int e0 = 8 * lane + 4 * half;
+                const int xa = xs + 4 * half;
+                if (e0 + 4 <= 4 || e0 >= 252) continue;
+#pragma unroll
+                for (int qx = 0; qx < 2; ++qx) {
+                    const bool isll = (qx == 0 && qy == 0);
+                    T a = v[4 * half + qx], b = v[4 * half + 2 + qx];
+                    const int sx = (xa >> 1) + (qx ? wl : 0);
+                    const bool va = xa + qx < w, vb = xa + 2 + qx < w;
+                    if (isll && !QLL) {
+                        T* p = ll_dst + (size_t)sy * llpitch + sx;
+                        if (vec_out && va && vb) {
+                            T pr[2] = {a, b};
+                            *reinterpret_cast<uint2*>(p) = *reinterpret_cast<uint2*>(pr);
+                        } else {
+                            if (va) p[0] = a;
+                            if (vb) p[1] = b;
+                        }
+                    } else {
+                        const float stp = isll ? st.ll : (qx && qy ? st.hh : (qx ? st.hl : st.lh));
+                        TD oa, ob;
+                        if (QUANT) {
+                            oa = (TD)quantize((float)a, stp);
+                            ob = (TD)quantize((float)b, stp);
+                        } else {
+                            oa = (TD)a;
+                            ob = (TD)b;
+                        }
+                        TD* p = dst + (size_t)sy * dpitch + sx;
+                        if (vec_out && va && vb && ((sx & 1) == 0)) {
+                            TD pr[2] = {oa, ob};
+                            *reinterpret_cast<uint2*>(p) = *reinterpret_cast<uint2*>(pr);
+                        } else {
+                            if (va) p[0] = oa;
+                            if (vb) p[1] = ob;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();  // strip `buf` is refilled two bands later
+    }
+    cp_async_wait1();
+}
+
 // ---- inverse level ----------------------------------------------------------------------------
 // Reconstructs the w x h region of level k-1 from the detail subbands of `src` (Mallat plane,
 // optionally int32 indices when DEQ) and the LL band (ll_src, or src itself when DEQLL).
@@ -348,14 +646,54 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
         } else {
             int nw = (cw + 1) / 2;
             lld = (T*)((k % 2 == 0) ? ll0 : ll1);
-            llp = (size_t)nw;
+            llp = (size_t)nw;  // the next level's input pitch
         }
         // subband indices of this level in QCD order: level L-k's triple
         int dl = k + 1;  // decomposition level produced
         int bt = 1 + 3 * (levels - dl);
         Steps4 st{1.f, 1.f, 1.f, 1.f};
         if (quant) st = Steps4{steps[0], steps[bt], steps[bt + 1], steps[bt + 2]};
-        if (quant) {
+        const bool fast_ok = ORDER == J2K_ORDER_T800 && ((uintptr_t)src & 15) == 0 && (spitch & 3) == 0 &&
+                             cw >= 8 && chh >= 2 && (!ctx || ctx->dwt_fast_th != 0);
+        if (fast_ok) {
+            const int fth = ctx ? ctx->dwt_fast_th : 32;
+            dim3 fg((cw + FTW - 1) / FTW, (chh + fth - 1) / fth);
+            const int vec = (((uintptr_t)out & 7) == 0) && ((out_pitch & 1) == 0) &&
+                            (((uintptr_t)lld & 7) == 0) && ((llp & 1) == 0);
+#define FAST(TH_)                                                                                        \
+    do {                                                                                                 \
+        if (quant) {                                                                                     \
+            if (last)                                                                                    \
+                dwt_fwd_fast<KERN, int32_t, true, true, TH_><<<fg, 256, 0, stream>>>(                    \
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec);                 \
+            else                                                                                         \
+                dwt_fwd_fast<KERN, int32_t, true, false, TH_><<<fg, 256, 0, stream>>>(                   \
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec);                 \
+        } else {                                                                                         \
+            dwt_fwd_fast<KERN, T, false, false, TH_><<<fg, 256, 0, stream>>>(src, spitch, cw, chh, lld, \
+                                                                              llp, (T*)out, out_pitch,   \
+                                                                              st, vec);                  \
+        }                                                                                                \
+    } while (0)
+            if (ctx && ctx->dwt_pipe) {
+                const int bands = (chh + 16 - 1) / 16;
+                const int tx = (cw + FTW - 1) / FTW;
+                const int want = std::max(1, (ctx->sm_count * 4 + tx - 1) / tx);
+                dim3 pg(tx, std::min(bands, want));
+                if (quant) {
+                    if (last)
+                        dwt_fwd_pipe<KERN, int32_t, true, true, 16><<<pg, 256, 0, stream>>>(
+                            src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, bands);
+                    else
+                        dwt_fwd_pipe<KERN, int32_t, true, false, 16><<<pg, 256, 0, stream>>>(
+                            src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, bands);
+                } else {
+                    dwt_fwd_pipe<KERN, T, false, false, 16><<<pg, 256, 0, stream>>>(
+                        src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, vec, bands);
+                }
+            } else if (fth == 16) FAST(16); else FAST(32);
+#undef FAST
+        } else if (quant) {
             if (last)
                 dwt_fwd_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(
                     src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st);

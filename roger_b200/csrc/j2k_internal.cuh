@@ -32,6 +32,8 @@ struct j2k_ctx {
     int sm_count = 148;
     int mq_lanes = 8;            // tier-1 MQ: code-blocks per warp (tuning knob)
     int mq_variant = 0;          // 0: one lane per block, 1: state warp + code warp pair
+    int dwt_fast_th = 16;        // fast level-0 DWT tile height (16, 32; 0 = off)
+    int dwt_pipe = 0;            // fast level-0 DWT: persistent cp.async double-buffered variant
 };
 
 // scratch slot ids

@@ -199,3 +199,24 @@ def test_capacity_errors_are_reported_not_trapped(C):
     # the context stays usable afterwards
     descs, data = C.bpc_encode(dev(coef), 2, 64, 64)
     assert (descs["length"] > 0).all()
+
+
+FAST_CASES = [(8, 9, 1), (248, 64, 2), (252, 35, 3), (300, 77, 4), (496, 33, 2), (1000, 130, 5), (4096, 40, 1),
+              (744, 2, 1), (16, 300, 4)]
+
+
+@pytest.mark.parametrize("w,h,L", FAST_CASES)
+@pytest.mark.parametrize("kern", [53, 97])
+def test_fast_level0_path_bit_exact(C, w, h, L, kern):
+    """Widths divisible by 4 take the register-lifting level-0 kernel; it must reproduce the
+    oracle exactly (5/3, 9/7 and quantised 9/7)."""
+    rng = np.random.default_rng(w * 13 + h)
+    if kern == 53:
+        x = rng.integers(-255, 256, (h, w)).astype(np.int32)
+        assert np.array_equal(C.dwt_forward(dev(x), L, 53, 0).cpu().numpy(), O.dwt53_fwd(x, L))
+    else:
+        x = rng.uniform(-128, 128, (h, w)).astype(np.float32)
+        assert np.array_equal(C.dwt_forward(dev(x), L, 97, 0).cpu().numpy(), O.dwt97_fwd(x, L))
+        st = O.default_steps(w, h, L)
+        assert np.array_equal(C.dwt_forward(dev(x), L, 97, 0, steps=st).cpu().numpy(),
+                              O.quantize(O.dwt97_fwd(x, L), L, st))
