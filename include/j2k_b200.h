@@ -197,6 +197,30 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs
                                       int ncomp, size_t w, size_t h, const j2k_enc_params* params,
                                       uint8_t* out, int out_on_device, size_t out_pitch_bytes);
 
+/* ---- differentiable 9/7 (no counterpart in the reference).  n images of w x h float32,
+ * planes back to back (pitch w, plane stride w*h), device pointers, T.800 order.  Used with
+ * j2k_dwt_forward / j2k_dwt_inverse (kernel 97, steps NULL) as the forward operators.
+ * j2k_dwt97_forward_adjoint: transpose of the forward DWT (Mallat gradient -> image gradient).
+ * j2k_dwt97_inverse_adjoint: transpose of the inverse DWT (image gradient -> Mallat gradient).
+ * The relaxed quantiser replaces rounding by additive noise of one step: for a coefficient y of
+ * subband b (step = exp(log_steps[b]), log_steps a device array of 3L+1 floats),
+ *   t = y/step + u, u ~ U[-1/2,1/2) (Philox4x32-10 keyed by seed+image, counter = y*w+x),
+ *   y_hat = t*step, rate = log2(1+|t|).
+ * Forward writes y_hat and, per (image, band, part), a partial rate sum (parts_per_band
+ * partials per band, to be summed by the caller in a fixed order).  Backward, for a loss
+ * L(y_hat) + lam * sum(rate), writes dL/dy and per-(image, band, part) partials of dL/dlog_step.
+ * levels <= 16. */
+j2k_status j2k_dwt97_forward_adjoint(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, size_t w,
+                                     size_t h, int levels);
+j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_coef, int n, size_t w,
+                                     size_t h, int levels);
+j2k_status j2k_relaxed_quant_forward(j2k_ctx* ctx, const float* y, float* y_hat, int n, size_t w, size_t h,
+                                     int levels, const float* log_steps, uint64_t seed, float* rate_partials,
+                                     int parts_per_band);
+j2k_status j2k_relaxed_quant_backward(j2k_ctx* ctx, const float* y, const float* g_yhat, float* g_y, int n,
+                                      size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
+                                      float lam, float* g_logstep_partials, int parts_per_band);
+
 /* ---- batched encoder.  No counterpart in the reference, which encodes one image per
  * OCLEncoder<T>::run call (src/OCLEncoder.cpp:43-52).  Many images of uneven size, mixed 5/3 and
  * 9/7, are encoded by one fixed launch sequence (batched planar split, one DWT launch per level

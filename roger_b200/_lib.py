@@ -73,6 +73,10 @@ SIGS = {
     "j2k_decoder_create": (I, [P, I, C.POINTER(P)]),
     "j2k_decoder_destroy": (I, [P]),
     "j2k_decoder_run_codeblocks": (I, [P, P, P, S, I, I, S, S, P, P, I, S]),
+    "j2k_dwt97_forward_adjoint": (I, [P, P, P, I, S, S, I]),
+    "j2k_dwt97_inverse_adjoint": (I, [P, P, P, I, S, S, I]),
+    "j2k_relaxed_quant_forward": (I, [P, P, P, I, S, S, I, P, C.c_uint64, P, I]),
+    "j2k_relaxed_quant_backward": (I, [P, P, P, P, I, S, S, I, P, C.c_uint64, C.c_float, P, I]),
     "j2k_batch_create": (I, [P, P, I, C.POINTER(P)]),
     "j2k_batch_destroy": (I, [P]),
     "j2k_batch_input": (I, [P, C.POINTER(P), P]),
