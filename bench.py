@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=W, help="image side (default 4096)")
+    ap.add_argument("--diff", type=int, default=1, help="time the differentiable 9/7 step (1) or not (0)")
     ap.add_argument("--batch-images", type=int, default=256,
                     help="images of the uneven mixed batch timed batched vs per-image (0 = skip)")
     return ap.parse_args()
@@ -318,6 +319,8 @@ def main():
     )
     if args.batch_images and world == 1:
         line["batched"] = bench_batched(args.batch_images, flush)
+    if args.diff and world == 1:
+        line["diff97"] = bench_diff97(flush, hbm)
     if cpu_line:
         line["cpu_baseline"] = cpu_line
     if rank == 0:
@@ -326,6 +329,50 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
+    """One rate-distortion training step of the differentiable 9/7 path on 16 x 1024^2 float32
+    images (seeds 200..215, /255): forward DWT, relaxed quantiser, inverse DWT, MSE + 0.01 *
+    rate, and the backward through the adjoint kernels, for pixels and 16 log-steps.
+    Compulsory traffic: 4 transforms of N*8*sum_k 4^-k bytes, quantiser forward 8N, loss and
+    its gradient 12N, quantiser backward 12N (N = samples)."""
+    import math
+    import numpy as np
+    import torch
+    from roger_b200 import diff97 as D
+    from roger_b200 import synth
+    x = torch.from_numpy(synth.float_batch(n, size, size, 200)).cuda().requires_grad_(True)
+    ls = torch.full((3 * levels + 1,), math.log(1 / 64.0), device="cuda", requires_grad=True)
+
+    def step():
+        x.grad = None
+        ls.grad = None
+        loss = D.rd_loss(x, ls, levels, 0.01, 200)
+        loss.backward()
+        return loss
+
+    for _ in range(3):
+        step()
+    tt = []
+    for _ in range(5):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        step()
+        e.record()
+        e.synchronize()
+        tt.append(s.elapsed_time(e))
+    ms = statistics.median(tt)
+    N = n * size * size
+    tr = N * 8 * sum(4.0 ** -k for k in range(levels))
+    algo = 4 * tr + 8 * N + 12 * N + 12 * N
+    return {"workload": f"{n} x {size}x{size} float32, 9/7 L={levels}, relaxed quantiser, loss = MSE + 0.01*rate, "
+                        "grads wrt pixels and 16 log-steps",
+            "ms_per_step": round(ms, 3), "algorithmic_bytes": int(algo),
+            "achieved_gbs": round(algo / (ms * 1e-3) / 1e9, 1), "hbm_frac": round(algo / (ms * 1e-3) / 1e9 / hbm, 4),
+            "mpix_s": round(N / 1e6 / (ms * 1e-3), 1)}
 
 
 def bench_batched(n, flush):

@@ -116,6 +116,15 @@ j2k_status j2k_dwt_forward_noalloc(void* cuda_stream, int kernel, int order, con
                                    size_t in_pitch, void* out, size_t out_pitch, size_t w, size_t h,
                                    int levels, const float* steps);
 
+/* Batched forms: n images, image i at in + i*in_stride / out + i*out_stride elements, one
+ * launch per level for the whole batch (the reference transforms one image per call). */
+j2k_status j2k_dwt_forward_batch(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                                 size_t in_stride, void* out, size_t out_pitch, size_t out_stride, int n,
+                                 size_t w, size_t h, int levels, const float* steps);
+j2k_status j2k_dwt_inverse_batch(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                                 size_t in_stride, void* out, size_t out_pitch, size_t out_stride, int n,
+                                 size_t w, size_t h, int levels, const float* steps);
+
 /* ---- EBCOT tier-1: replaces OCLBPC<T>::run (src/OCLBPC.cpp:38-50) and src/CL/oclbpc.cl:279-746.
  * Code-blocks partition every subband of a Mallat plane (w x h, `levels`) on a cbw x cbh grid
  * anchored at the subband origin, subbands in QCD order, blocks in raster order. */

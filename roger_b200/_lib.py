@@ -58,6 +58,8 @@ SIGS = {
     "j2k_dwt_forward": (I, [P, I, I, P, S, P, S, S, S, I, P]),
     "j2k_dwt_inverse": (I, [P, I, I, P, S, P, S, S, S, I, P]),
     "j2k_dwt_forward_noalloc": (I, [P, I, I, P, S, P, S, S, S, I, P]),
+    "j2k_dwt_forward_batch": (I, [P, I, I, P, S, S, P, S, S, I, S, S, I, P]),
+    "j2k_dwt_inverse_batch": (I, [P, I, I, P, S, S, P, S, S, I, S, S, I, P]),
     "j2k_codeblock_count": (S, [S, S, I, I, I]),
     "j2k_bpc_encode": (I, [P, P, S, S, S, I, I, I, P, P, S]),
     "j2k_bpc_decode": (I, [P, P, P, S, P, S, S, S, I, I, I]),

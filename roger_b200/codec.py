@@ -135,36 +135,48 @@ def _steps_arg(steps, levels):
 
 
 def dwt_forward(plane, levels, kernel=None, order=L.ORDER_T800, steps=None, ctx=None, out=None):
-    """Forward DWT of one (H, W) plane (int32 -> 5/3, float32 -> 9/7), Mallat output.
-    With steps (9/7 only) the output is int32 dead-zone indices."""
+    """Forward DWT of one (H, W) plane or a batch (N, H, W) of planes (int32 -> 5/3,
+    float32 -> 9/7), Mallat output.  With steps (9/7 only) the output is int32 dead-zone
+    indices.  A batch is transformed with one launch per level."""
     ctx = ctx or default_context(plane.device.index or 0)
     _need_cuda(plane, "plane")
     if kernel is None:
         kernel = L.W53 if plane.dtype == torch.int32 else L.W97
-    h, w = plane.shape
+    h, w = plane.shape[-2:]
     odt = torch.int32 if (kernel == L.W53 or steps is not None) else torch.float32
     if out is None:
-        out = torch.empty((h, w), dtype=odt, device=plane.device)
+        out = torch.empty(plane.shape, dtype=odt, device=plane.device)
     keep, sp = _steps_arg(steps, levels)
     hh = ctx._bind()
-    check(lib().j2k_dwt_forward(hh, kernel, order, _ptr(plane), plane.stride(0), _ptr(out),
-                                out.stride(0), w, h, levels, sp), hh)
+    if plane.dim() == 3:
+        check(lib().j2k_dwt_forward_batch(hh, kernel, order, _ptr(plane), plane.stride(1), plane.stride(0),
+                                          _ptr(out), out.stride(1), out.stride(0), plane.shape[0], w, h,
+                                          levels, sp), hh)
+    else:
+        check(lib().j2k_dwt_forward(hh, kernel, order, _ptr(plane), plane.stride(0), _ptr(out),
+                                    out.stride(0), w, h, levels, sp), hh)
     return out
 
 
 def dwt_inverse(coef, levels, kernel=None, order=L.ORDER_T800, steps=None, ctx=None, out=None):
+    """Inverse DWT of one (H, W) Mallat plane or a batch (N, H, W)."""
     ctx = ctx or default_context(coef.device.index or 0)
     _need_cuda(coef, "coef")
     if kernel is None:
         kernel = L.W53 if (coef.dtype == torch.int32 and steps is None) else L.W97
-    h, w = coef.shape
+    h, w = coef.shape[-2:]
     odt = torch.int32 if kernel == L.W53 else torch.float32
     if out is None:
-        out = torch.empty((h, w), dtype=odt, device=coef.device)
+        out = torch.empty(coef.shape, dtype=odt, device=coef.device)
     keep, sp = _steps_arg(steps, levels)
     hh = ctx._bind()
-    check(lib().j2k_dwt_inverse(hh, kernel, order, _ptr(coef), coef.stride(0), _ptr(out),
-                                out.stride(0), w, h, levels, sp), hh)
+    if coef.dim() == 3:
+        check(lib().j2k_dwt_inverse_batch(hh, kernel, order, _ptr(coef), coef.stride(1), coef.stride(0),
+                                          _ptr(out), out.stride(1), out.stride(0), coef.shape[0], w, h,
+                                          levels, sp), hh)
+    else:
+        check(lib().j2k_dwt_inverse(hh, kernel, order, _ptr(coef), coef.stride(0), _ptr(out),
+                                    out.stride(0), w, h, levels, sp), hh)
     return out
 
 

@@ -343,3 +343,39 @@ j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, 
 }
 
 }  // extern "C"
+
+extern "C" j2k_status j2k_dwt_forward_batch(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                                            size_t in_stride, void* out, size_t out_pitch, size_t out_stride,
+                                            int n, size_t w, size_t h, int levels, const float* steps) {
+    if (!ctx) return J2K_ERR_INVALID_ARG;
+    J2K_TRY(check_dwt_args(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels));
+    if (n <= 0 || n > 65535 || in_stride < in_pitch * h || out_stride < out_pitch * h)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "dwt batch: bad image count or plane stride");
+    if (kernel == J2K_W53 && steps)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "dwt: the 5/3 path is not quantised");
+    cudaSetDevice(ctx->device);
+    size_t w1 = (w + 1) / 2, h1 = (h + 1) / 2, w2 = (w1 + 1) / 2, h2 = (h1 + 1) / 2;
+    void* ll0 = j2k_scratch(ctx, SCR_LL0, w1 * h1 * 4 * (size_t)n);
+    void* ll1 = j2k_scratch(ctx, SCR_LL1, w2 * h2 * 4 * (size_t)n);
+    if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
+    return j2k_dwt_fwd_impl(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps, ll0, ll1,
+                            j2k_dwt_tile{64, 64}, ctx->stream, n, in_stride, out_stride);
+}
+
+extern "C" j2k_status j2k_dwt_inverse_batch(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
+                                            size_t in_stride, void* out, size_t out_pitch, size_t out_stride,
+                                            int n, size_t w, size_t h, int levels, const float* steps) {
+    if (!ctx) return J2K_ERR_INVALID_ARG;
+    J2K_TRY(check_dwt_args(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels));
+    if (n <= 0 || n > 65535 || in_stride < in_pitch * h || out_stride < out_pitch * h)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "dwt batch: bad image count or plane stride");
+    if (kernel == J2K_W53 && steps)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "dwt: the 5/3 path is not quantised");
+    cudaSetDevice(ctx->device);
+    size_t w1 = (w + 1) / 2, h1 = (h + 1) / 2, w2 = (w1 + 1) / 2, h2 = (h1 + 1) / 2;
+    void* ll0 = j2k_scratch(ctx, SCR_LL0, w1 * h1 * 4 * (size_t)n);
+    void* ll1 = j2k_scratch(ctx, SCR_LL1, w2 * h2 * 4 * (size_t)n);
+    if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
+    return j2k_dwt_inv_impl(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps, ll0, ll1,
+                            j2k_dwt_tile{64, 64}, ctx->stream, n, in_stride, out_stride);
+}

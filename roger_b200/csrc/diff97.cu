@@ -29,49 +29,62 @@ constexpr float P1 = -1.586134342f, U1 = -0.05298011854f, P2 = 0.8829110762f, U2
 constexpr float KMUL = 1.23017410491400f, KDIV = 0.81289306611596153187273657637352f;
 constexpr int TW = 64, TH = 64, HALO = 4, NX = TW + 2 * HALO, NY = TH + 2 * HALO, SS = NX + 1;
 
-// transposed step k of a sequence: parity updated and coefficient
-struct AdjStep {
-    int par;
-    float c;
-};
-// forward-adjoint (after the forward scaling): L3^T, L2^T, L1^T, L0^T
-__device__ __constant__ AdjStep kFwdAdj[4] = {{1, U2}, {0, P2}, {1, U1}, {0, P1}};
-// inverse-adjoint (before the inverse scaling): L3'^T (odd -P1 -> even), L2'^T, L1'^T, L0'^T
-__device__ __constant__ AdjStep kInvAdj[4] = {{0, -P1}, {1, -U1}, {0, -P2}, {1, -U2}};
+// Transposed step sequences (parity updated, coefficient):
+//   forward adjoint (after the forward scaling): (odd, U2), (even, P2), (odd, U1), (even, P1)
+//   inverse adjoint (before the inverse scaling): (even, -P1), (odd, -U1), (even, -P2), (odd, -U2)
 
-// One transposed step along columns (VERT) or rows of the shared tile.  Absolute coordinates of
-// tile row/col 0 are (ay0, ax0); n is the line length along the step's axis.
-template <bool VERT>
-__device__ __forceinline__ void adj_step(float* s, int k, const AdjStep* seq, int ay0, int ax0, int n, int lo, int hi,
-                                         int olo, int ohi) {
-    const int par = seq[k].par;   // parity updated
-    const float c = seq[k].c;
-    const int len = VERT ? NY : NX;
-    (void)len;
-    const int span = ohi - olo;
-    for (int e = threadIdx.x; e < (hi - lo) * span; e += blockDim.x) {
-        const int a = lo + e / span, o = olo + e % span;  // a: along the step axis, o: across
-        const int r = VERT ? a : o, cc = VERT ? o : a;
-        const int abs_a = (VERT ? ay0 : ax0) + a;
-        if ((abs_a & 1) != par || abs_a < 0 || abs_a >= n) continue;
-        float* p = s + r * SS + cc;
-        const int st = VERT ? SS : 1;
+// One transposed step along columns (VERT) or rows of the shared tile: positions along the
+// step axis in [LO, HI) (tile coordinates), across it in [OLO, OHI).  Absolute coordinate of
+// tile index 0 along the axis: a0; n: line length.  EDGE: the tile touches the image boundary
+// along this axis (only then are the zero-extension and boundary doubling applied).
+template <bool VERT, bool FWD, int K, int LO, int HI, int OLO, int OHI, bool EDGE>
+__device__ __forceinline__ void adj_step(float* s, int a0, int n) {
+    constexpr int span = OHI - OLO, cnt = (HI - LO) * span;
+    const int par = FWD ? (K == 0 || K == 2 ? 1 : 0) : (K == 0 || K == 2 ? 0 : 1);
+    const float c = FWD ? (K == 0 ? U2 : K == 1 ? P2 : K == 2 ? U1 : P1)
+                        : (K == 0 ? -P1 : K == 1 ? -U1 : K == 2 ? -P2 : -U2);
+    constexpr int st = VERT ? SS : 1;
+    const int first = LO + (((a0 + LO) & 1) != par);  // first position of the updated parity
+    const int na = first < HI ? (HI - first + 1) / 2 : 0;
+    for (int e = threadIdx.x; e < na * span; e += blockDim.x) {
+        const int a = first + 2 * (e / span), o = OLO + e % span;
+        float* p = s + (VERT ? a * SS + o : o * SS + a);
         float left = p[-st], right = p[st];
-        const int src = 1 - par;  // parity of the neighbours
-        if (abs_a - 1 == 0 && (0 & 1) == src) left *= 2.0f;
-        if (abs_a + 1 == n - 1 && ((n - 1) & 1) == src) right *= 2.0f;
-        if (abs_a - 1 < 0) left = 0.0f;
-        if (abs_a + 1 >= n) right = 0.0f;
+        if (EDGE) {
+            const int abs_a = a0 + a;
+            if (abs_a < 0 || abs_a >= n) continue;
+            if (abs_a - 1 < 0) left = 0.0f;
+            else if (abs_a - 1 == 0) left *= 2.0f;        // sample 0 has the source parity here
+            if (abs_a + 1 >= n) right = 0.0f;
+            else if (abs_a + 1 == n - 1) right *= 2.0f;   // so does sample n-1
+        }
         *p = __fadd_rn(*p, __fmul_rn(c, __fadd_rn(left, right)));
     }
+    (void)cnt;
+}
+
+template <bool VERT, bool FWD, int OLO, int OHI, bool EDGE>
+__device__ __forceinline__ void adj_steps(float* s, int a0, int n) {
+    constexpr int L = VERT ? NY : NX;
+    adj_step<VERT, FWD, 0, 1, L - 1, OLO, OHI, EDGE>(s, a0, n);
+    __syncthreads();
+    adj_step<VERT, FWD, 1, 2, L - 2, OLO, OHI, EDGE>(s, a0, n);
+    __syncthreads();
+    adj_step<VERT, FWD, 2, 3, L - 3, OLO, OHI, EDGE>(s, a0, n);
+    __syncthreads();
+    adj_step<VERT, FWD, 3, 4, L - 4, OLO, OHI, EDGE>(s, a0, n);
+    __syncthreads();
 }
 
 // Adjoint of one forward level: subband gradients (Mallat positions of `gsrc`, LL from `gll`
 // with pitch llpitch) -> gradient of the level input (w x h) in `gout`.
 __global__ void __launch_bounds__(256)
 fwd_adj_level(const float* __restrict__ gsrc, size_t spitch, const float* __restrict__ gll, size_t llpitch,
-              int w, int h, float* __restrict__ gout, size_t opitch) {
+              int w, int h, float* __restrict__ gout, size_t opitch, size_t zs, size_t zll, size_t zo) {
     __shared__ float s[NY * SS];
+    gsrc += blockIdx.z * zs;
+    gll += blockIdx.z * zll;
+    gout += blockIdx.z * zo;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     const int ax0 = x0 - HALO, ay0 = y0 - HALO;
     const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
@@ -87,17 +100,16 @@ fwd_adj_level(const float* __restrict__ gsrc, size_t spitch, const float* __rest
         s[r * SS + c] = v;
     }
     __syncthreads();
-    // rows (the forward applied them last): scale by the forward factors, then L^T steps
+    const bool edge_x = ax0 <= 0 || ax0 + NX >= w, edge_y = ay0 <= 0 || ay0 + NY >= h;
+    // rows (the forward applied them last): scale by the forward factors, then the L^T steps
     if (w > 1) {
         for (int e = threadIdx.x; e < NX * NY; e += blockDim.x) {
             const int r = e / NX, c = e % NX;
             s[r * SS + c] = __fmul_rn(s[r * SS + c], ((ax0 + c) & 1) ? KMUL : KDIV);
         }
         __syncthreads();
-        for (int k = 0; k < 4; ++k) {
-            adj_step<false>(s, k, kFwdAdj, ay0, ax0, w, k + 1, NX - k - 1, 0, NY);
-            __syncthreads();
-        }
+        if (edge_x) adj_steps<false, true, 0, NY, true>(s, ax0, w);
+        else adj_steps<false, true, 0, NY, false>(s, ax0, w);
     }
     if (h > 1) {
         for (int e = threadIdx.x; e < NX * NY; e += blockDim.x) {
@@ -105,10 +117,8 @@ fwd_adj_level(const float* __restrict__ gsrc, size_t spitch, const float* __rest
             s[r * SS + c] = __fmul_rn(s[r * SS + c], ((ay0 + r) & 1) ? KMUL : KDIV);
         }
         __syncthreads();
-        for (int k = 0; k < 4; ++k) {
-            adj_step<true>(s, k, kFwdAdj, ay0, ax0, h, k + 1, NY - k - 1, HALO, HALO + TW);
-            __syncthreads();
-        }
+        if (edge_y) adj_steps<true, true, HALO, HALO + TW, true>(s, ay0, h);
+        else adj_steps<true, true, HALO, HALO + TW, false>(s, ay0, h);
     }
     for (int e = threadIdx.x; e < TW * TH; e += blockDim.x) {
         const int i = e % TW, j = e / TW;
@@ -121,8 +131,11 @@ fwd_adj_level(const float* __restrict__ gsrc, size_t spitch, const float* __rest
 // `gin`) -> subband gradients (details into the Mallat plane `gdst`, LL into `gll`).
 __global__ void __launch_bounds__(256)
 inv_adj_level(const float* __restrict__ gin, size_t ipitch, int w, int h, float* __restrict__ gdst, size_t dpitch,
-              float* __restrict__ gll, size_t llpitch) {
+              float* __restrict__ gll, size_t llpitch, size_t zi, size_t zd, size_t zll) {
     __shared__ float s[NY * SS];
+    gin += blockIdx.z * zi;
+    gdst += blockIdx.z * zd;
+    gll += blockIdx.z * zll;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     const int ax0 = x0 - HALO, ay0 = y0 - HALO;
     for (int e = threadIdx.x; e < NX * NY; e += blockDim.x) {
@@ -131,12 +144,11 @@ inv_adj_level(const float* __restrict__ gin, size_t ipitch, int w, int h, float*
         s[r * SS + c] = (gx >= 0 && gx < w && gy >= 0 && gy < h) ? gin[(size_t)gy * ipitch + gx] : 0.0f;
     }
     __syncthreads();
+    const bool edge_x = ax0 <= 0 || ax0 + NX >= w, edge_y = ay0 <= 0 || ay0 + NY >= h;
     // columns first (the inverse applied them last)
     if (h > 1) {
-        for (int k = 0; k < 4; ++k) {
-            adj_step<true>(s, k, kInvAdj, ay0, ax0, h, k + 1, NY - k - 1, 0, NX);
-            __syncthreads();
-        }
+        if (edge_y) adj_steps<true, false, 0, NX, true>(s, ay0, h);
+        else adj_steps<true, false, 0, NX, false>(s, ay0, h);
         for (int e = threadIdx.x; e < NX * NY; e += blockDim.x) {
             const int r = e / NX, c = e % NX;
             s[r * SS + c] = __fmul_rn(s[r * SS + c], ((ay0 + r) & 1) ? KDIV : KMUL);
@@ -144,10 +156,8 @@ inv_adj_level(const float* __restrict__ gin, size_t ipitch, int w, int h, float*
         __syncthreads();
     }
     if (w > 1) {
-        for (int k = 0; k < 4; ++k) {
-            adj_step<false>(s, k, kInvAdj, ay0, ax0, w, k + 1, NX - k - 1, HALO, HALO + TH);
-            __syncthreads();
-        }
+        if (edge_x) adj_steps<false, false, HALO, HALO + TH, true>(s, ax0, w);
+        else adj_steps<false, false, HALO, HALO + TH, false>(s, ax0, w);
     }
     const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
     for (int e = threadIdx.x; e < TW * TH; e += blockDim.x) {
@@ -286,29 +296,30 @@ j2k_status j2k_dwt97_forward_adjoint(j2k_ctx* ctx, const float* g_coef, float* g
     ws[0] = (int)w;
     hs[0] = (int)h;
     for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
-    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, (size_t)ws[1] * hs[1] * 4 + 64);
-    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, (size_t)ws[1] * hs[1] * 4 + 64);
+    const size_t plane = w * h, zlev = (size_t)ws[1] * hs[1];
+    if (levels == 0) {
+        for (int img = 0; img < n; ++img)
+            copy_f<<<dim3((unsigned)((w + 255) / 256), (unsigned)h), 256, 0, st>>>(g_coef + img * plane, w,
+                                                                                  g_img + img * plane, w, (int)w,
+                                                                                  (int)h);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, zlev * n * 4 + 64);
+    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, zlev * n * 4 + 64);
     if (!s0 || !s1) return J2K_ERR_OUT_OF_MEMORY;
-    const size_t plane = w * h;
-    for (int img = 0; img < n; ++img) {
-        const float* gc = g_coef + (size_t)img * plane;
-        float* gi = g_img + (size_t)img * plane;
-        if (levels == 0) {
-            copy_f<<<dim3((unsigned)((w + 255) / 256), (unsigned)h), 256, 0, st>>>(gc, w, gi, w, (int)w, (int)h);
-            continue;
-        }
-        // deepest level first; level k's LL gradient comes from level k+1's output
-        const float* ll = gc;  // LL_L lives in the top-left of the Mallat plane
-        size_t llp = w;
-        for (int k = levels - 1; k >= 0; --k) {
-            float* out = k == 0 ? gi : ((levels - 1 - k) % 2 == 0 ? s0 : s1);
-            size_t op = k == 0 ? w : (size_t)ws[k];
-            dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH);
-            fwd_adj_level<<<g, 256, 0, st>>>(gc, w, ll, llp, ws[k], hs[k], out, op);
-            J2K_CUDA(ctx, cudaGetLastError());
-            ll = out;
-            llp = op;
-        }
+    // deepest level first; level k's LL gradient is level k+1's output
+    const float* ll = g_coef;  // LL_L lives in the top-left of each Mallat plane
+    size_t llp = w, llz = plane;
+    for (int k = levels - 1; k >= 0; --k) {
+        float* out = k == 0 ? g_img : ((levels - 1 - k) % 2 == 0 ? s0 : s1);
+        const size_t op = k == 0 ? w : (size_t)ws[k], oz = k == 0 ? plane : zlev;
+        dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
+        fwd_adj_level<<<g, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k], out, op, plane, llz, oz);
+        J2K_CUDA(ctx, cudaGetLastError());
+        ll = out;
+        llp = op;
+        llz = oz;
     }
     return J2K_OK;
 }
@@ -322,29 +333,30 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
     ws[0] = (int)w;
     hs[0] = (int)h;
     for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
-    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, (size_t)ws[1] * hs[1] * 4 + 64);
-    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, (size_t)ws[1] * hs[1] * 4 + 64);
+    const size_t plane = w * h, zlev = (size_t)ws[1] * hs[1];
+    if (levels == 0) {
+        for (int img = 0; img < n; ++img)
+            copy_f<<<dim3((unsigned)((w + 255) / 256), (unsigned)h), 256, 0, st>>>(g_img + img * plane, w,
+                                                                                  g_coef + img * plane, w, (int)w,
+                                                                                  (int)h);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, zlev * n * 4 + 64);
+    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, zlev * n * 4 + 64);
     if (!s0 || !s1) return J2K_ERR_OUT_OF_MEMORY;
-    const size_t plane = w * h;
-    for (int img = 0; img < n; ++img) {
-        const float* gi = g_img + (size_t)img * plane;
-        float* gc = g_coef + (size_t)img * plane;
-        if (levels == 0) {
-            copy_f<<<dim3((unsigned)((w + 255) / 256), (unsigned)h), 256, 0, st>>>(gi, w, gc, w, (int)w, (int)h);
-            continue;
-        }
-        const float* in = gi;
-        size_t ip = w;
-        for (int k = 0; k < levels; ++k) {
-            const bool last = k == levels - 1;
-            float* ll = last ? gc : (k % 2 == 0 ? s0 : s1);
-            size_t llp = last ? w : (size_t)ws[k + 1];
-            dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH);
-            inv_adj_level<<<g, 256, 0, st>>>(in, ip, ws[k], hs[k], gc, w, ll, llp);
-            J2K_CUDA(ctx, cudaGetLastError());
-            in = ll;
-            ip = llp;
-        }
+    const float* in = g_img;
+    size_t ip = w, iz = plane;
+    for (int k = 0; k < levels; ++k) {
+        const bool last = k == levels - 1;
+        float* ll = last ? g_coef : (k % 2 == 0 ? s0 : s1);
+        const size_t llp = last ? w : (size_t)ws[k + 1], llz = last ? plane : zlev;
+        dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
+        inv_adj_level<<<g, 256, 0, st>>>(in, ip, ws[k], hs[k], g_coef, w, ll, llp, iz, plane, llz);
+        J2K_CUDA(ctx, cudaGetLastError());
+        in = ll;
+        ip = llp;
+        iz = llz;
     }
     return J2K_OK;
 }

@@ -144,6 +144,8 @@ __device__ __forceinline__ float dequantize(int32_t q, float step) {
 }
 
 struct Steps4 { float ll, hl, lh, hh; };
+// element strides between consecutive images of a batch (blockIdx.z selects the image)
+struct ZStride { size_t src, dst, ll; };
 
 // ---- forward level ----------------------------------------------------------------------------
 // src: level input (w x h).  Detail subbands go to dst at Mallat positions (dst is the full
@@ -210,9 +212,12 @@ template <int KERN, int ORDER, int TW, int TH, typename TD, bool QUANT, bool QLL
 __global__ void __launch_bounds__(256)
 dwt_fwd_level(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
               typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst,
-              size_t dpitch, Steps4 st) {
+              size_t dpitch, Steps4 st, ZStride z) {
     using G = Tile<KERN, TW, TH>;
     __shared__ typename KT<KERN>::T s[G::NY * G::S];
+    src += blockIdx.z * z.src;
+    dst += blockIdx.z * z.dst;
+    ll_dst += blockIdx.z * z.ll;
     fwd_tile<KERN, ORDER, TW, TH, TD, QUANT, QLL>(s, src, spitch, w, h, ll_dst, llpitch, dst, dpitch, st,
                                                  blockIdx.x * TW, blockIdx.y * TH);
 }
@@ -257,8 +262,11 @@ template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
 __global__ void __launch_bounds__(256, (KERN == 53 && FTH == 16) ? 8 : 6)
 dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
              typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
-             Steps4 st, int vec_out) {
+             Steps4 st, int vec_out, ZStride z) {
     using T = typename KT<KERN>::T;
+    src += blockIdx.z * z.src;
+    dst += blockIdx.z * z.dst;
+    ll_dst += blockIdx.z * z.ll;
     constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
     __shared__ __align__(16) T s[NY][FNX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
@@ -545,7 +553,10 @@ template <int KERN, int ORDER, int TW, int TH, typename TS, bool DEQ, bool DEQLL
 __global__ void __launch_bounds__(256)
 dwt_inv_level(const TS* __restrict__ src, size_t spitch,
               const typename KT<KERN>::T* __restrict__ ll_src, size_t llpitch, int w, int h,
-              typename KT<KERN>::T* __restrict__ out, size_t opitch, Steps4 st) {
+              typename KT<KERN>::T* __restrict__ out, size_t opitch, Steps4 st, ZStride z) {
+    src += blockIdx.z * z.src;
+    ll_src += blockIdx.z * z.ll;
+    out += blockIdx.z * z.dst;
     using T = typename KT<KERN>::T;
     using G = Tile<KERN, TW, TH>;
     constexpr int H = G::H;
@@ -600,7 +611,9 @@ dwt_inv_level(const TS* __restrict__ src, size_t spitch,
 // levels == 0: plain copy, or quantisation of the single LL band
 template <typename TI, typename TO, bool Q>
 __global__ void copy_plane(const TI* __restrict__ in, size_t ip, TO* __restrict__ out, size_t op,
-                           int w, int h, float step) {
+                           int w, int h, float step, ZStride z) {
+    in += blockIdx.z * z.src;
+    out += blockIdx.z * z.dst;
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= w || y >= h) return;
     TI v = in[(size_t)y * ip + x];
@@ -609,7 +622,9 @@ __global__ void copy_plane(const TI* __restrict__ in, size_t ip, TO* __restrict_
 }
 template <typename TI, typename TO, bool DQ>
 __global__ void copy_plane_deq(const TI* __restrict__ in, size_t ip, TO* __restrict__ out,
-                               size_t op, int w, int h, float step) {
+                               size_t op, int w, int h, float step, ZStride z) {
+    in += blockIdx.z * z.src;
+    out += blockIdx.z * z.dst;
     int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= w || y >= h) return;
     TI v = in[(size_t)y * ip + x];
@@ -620,34 +635,42 @@ __global__ void copy_plane_deq(const TI* __restrict__ in, size_t ip, TO* __restr
 template <int KERN, int ORDER, int TW, int TH>
 j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, size_t out_pitch,
                       int w, int h, int levels, const float* steps, void* ll0, void* ll1,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, int n, size_t in_z, size_t out_z) {
     using T = typename KT<KERN>::T;
     const bool quant = (KERN == 97) && steps != nullptr;
     if (levels == 0) {
-        dim3 g((w + 255) / 256, h);
+        dim3 g((w + 255) / 256, h, n);
+        const ZStride zc{in_z, out_z, 0};
         if (quant)
-            copy_plane<float, int32_t, true><<<g, 256, 0, stream>>>((const float*)in, in_pitch, (int32_t*)out, out_pitch, w, h, steps[0]);
+            copy_plane<float, int32_t, true><<<g, 256, 0, stream>>>((const float*)in, in_pitch, (int32_t*)out, out_pitch, w, h, steps[0], zc);
         else
-            copy_plane<T, T, false><<<g, 256, 0, stream>>>((const T*)in, in_pitch, (T*)out, out_pitch, w, h, 1.0f);
+            copy_plane<T, T, false><<<g, 256, 0, stream>>>((const T*)in, in_pitch, (T*)out, out_pitch, w, h, 1.0f, zc);
         J2K_CUDA(ctx, cudaGetLastError());
         return J2K_OK;
     }
     int cw = w, chh = h;
     const T* src = (const T*)in;
     size_t spitch = in_pitch;
+    // per-image strides of the two LL scratch buffers (sized for level 0 / level 1 outputs)
+    const size_t z0 = (size_t)((w + 1) / 2) * ((h + 1) / 2);
+    const size_t z1 = (size_t)(((w + 1) / 2 + 1) / 2) * (((h + 1) / 2 + 1) / 2);
+    size_t src_z = in_z;
     for (int k = 0; k < levels; ++k) {
         bool last = (k == levels - 1);
-        dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH);
+        dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH, n);
         T* lld;
-        size_t llp;
+        size_t llp, ll_z;
         if (last) {
             lld = (T*)out;
             llp = out_pitch;
+            ll_z = out_z;
         } else {
             int nw = (cw + 1) / 2;
             lld = (T*)((k % 2 == 0) ? ll0 : ll1);
             llp = (size_t)nw;  // the next level's input pitch
+            ll_z = (k % 2 == 0) ? z0 : z1;
         }
+        const ZStride zs{src_z, out_z, ll_z};
         // subband indices of this level in QCD order: level L-k's triple
         int dl = k + 1;  // decomposition level produced
         int bt = 1 + 3 * (levels - dl);
@@ -657,7 +680,7 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
                              cw >= 8 && chh >= 2 && (!ctx || ctx->dwt_fast_th != 0);
         if (fast_ok) {
             const int fth = ctx ? ctx->dwt_fast_th : 32;
-            dim3 fg((cw + FTW - 1) / FTW, (chh + fth - 1) / fth);
+            dim3 fg((cw + FTW - 1) / FTW, (chh + fth - 1) / fth, n);
             const int vec = (((uintptr_t)out & 7) == 0) && ((out_pitch & 1) == 0) &&
                             (((uintptr_t)lld & 7) == 0) && ((llp & 1) == 0);
 #define FAST(TH_)                                                                                        \
@@ -665,17 +688,17 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
         if (quant) {                                                                                     \
             if (last)                                                                                    \
                 dwt_fwd_fast<KERN, int32_t, true, true, TH_><<<fg, 256, 0, stream>>>(                    \
-                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec);                 \
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs);             \
             else                                                                                         \
                 dwt_fwd_fast<KERN, int32_t, true, false, TH_><<<fg, 256, 0, stream>>>(                   \
-                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec);                 \
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs);             \
         } else {                                                                                         \
             dwt_fwd_fast<KERN, T, false, false, TH_><<<fg, 256, 0, stream>>>(src, spitch, cw, chh, lld, \
                                                                               llp, (T*)out, out_pitch,   \
-                                                                              st, vec);                  \
+                                                                              st, vec, zs);              \
         }                                                                                                \
     } while (0)
-            if (ctx && ctx->dwt_pipe) {
+            if (ctx && ctx->dwt_pipe && n == 1) {
                 const int bands = (chh + 16 - 1) / 16;
                 const int tx = (cw + FTW - 1) / FTW;
                 const int want = std::max(1, (ctx->sm_count * 4 + tx - 1) / tx);
@@ -696,17 +719,18 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
         } else if (quant) {
             if (last)
                 dwt_fwd_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(
-                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st);
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, zs);
             else
                 dwt_fwd_level<KERN, ORDER, TW, TH, int32_t, true, false><<<grid, 256, 0, stream>>>(
-                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st);
+                    src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, zs);
         } else {
             dwt_fwd_level<KERN, ORDER, TW, TH, T, false, false><<<grid, 256, 0, stream>>>(
-                src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st);
+                src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, zs);
         }
         J2K_CUDA(ctx, cudaGetLastError());
         src = lld;
         spitch = llp;
+        src_z = ll_z;
         cw = (cw + 1) / 2;
         chh = (chh + 1) / 2;
     }
@@ -716,15 +740,16 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
 template <int KERN, int ORDER, int TW, int TH>
 j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, size_t out_pitch,
                       int w, int h, int levels, const float* steps, void* ll0, void* ll1,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, int n, size_t in_z, size_t out_z) {
     using T = typename KT<KERN>::T;
     const bool deq = (KERN == 97) && steps != nullptr;
     if (levels == 0) {
-        dim3 g((w + 255) / 256, h);
+        dim3 g((w + 255) / 256, h, n);
+        const ZStride zc{in_z, out_z, 0};
         if (deq)
-            copy_plane_deq<int32_t, float, true><<<g, 256, 0, stream>>>((const int32_t*)in, in_pitch, (float*)out, out_pitch, w, h, steps[0]);
+            copy_plane_deq<int32_t, float, true><<<g, 256, 0, stream>>>((const int32_t*)in, in_pitch, (float*)out, out_pitch, w, h, steps[0], zc);
         else
-            copy_plane_deq<T, T, false><<<g, 256, 0, stream>>>((const T*)in, in_pitch, (T*)out, out_pitch, w, h, 1.0f);
+            copy_plane_deq<T, T, false><<<g, 256, 0, stream>>>((const T*)in, in_pitch, (T*)out, out_pitch, w, h, 1.0f, zc);
         J2K_CUDA(ctx, cudaGetLastError());
         return J2K_OK;
     }
@@ -732,26 +757,33 @@ j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
     ws[0] = w;
     hs[0] = h;
     for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
+    // per-image strides of the two LL scratch buffers: odd levels use ll0 (level-1 size),
+    // even levels >= 2 use ll1 (level-2 size)
+    const size_t z0 = (size_t)ws[1] * hs[1];
+    const size_t z1 = levels >= 2 ? (size_t)ws[2] * hs[2] : 0;
     for (int k = levels - 1; k >= 0; --k) {
         int cw = ws[k], chh = hs[k];
-        dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH);
+        dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH, n);
         T* o = (k == 0) ? (T*)out : (T*)((k % 2 == 1) ? ll0 : ll1);
         size_t op = (k == 0) ? out_pitch : (size_t)cw;
+        const size_t o_z = (k == 0) ? out_z : ((k % 2 == 1) ? z0 : z1);
         const T* lls = (k == levels - 1) ? (const T*)in : (const T*)((k % 2 == 1) ? ll1 : ll0);
         size_t llp = (k == levels - 1) ? in_pitch : (size_t)ws[k + 1];
+        const size_t l_z = (k == levels - 1) ? in_z : ((k % 2 == 1) ? z1 : z0);
+        const ZStride zs{in_z, o_z, l_z};
         int bt = 1 + 3 * (levels - (k + 1));
         Steps4 st{1.f, 1.f, 1.f, 1.f};
         if (deq) st = Steps4{steps[0], steps[bt], steps[bt + 1], steps[bt + 2]};
         if (deq) {
             if (k == levels - 1)
                 dwt_inv_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(
-                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st);
+                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs);
             else
                 dwt_inv_level<KERN, ORDER, TW, TH, int32_t, true, false><<<grid, 256, 0, stream>>>(
-                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st);
+                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs);
         } else {
             dwt_inv_level<KERN, ORDER, TW, TH, T, false, false><<<grid, 256, 0, stream>>>(
-                (const T*)in, in_pitch, lls, llp, cw, chh, o, op, st);
+                (const T*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs);
         }
         J2K_CUDA(ctx, cudaGetLastError());
     }
@@ -761,16 +793,16 @@ j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
 template <int KERN, int TW, int TH>
 j2k_status fwd_dispatch_order(j2k_ctx* ctx, int order, const void* in, size_t ip, void* out,
                               size_t op, int w, int h, int levels, const float* steps, void* a,
-                              void* b, cudaStream_t st) {
-    if (order == J2K_ORDER_REF) return fwd_levels<KERN, J2K_ORDER_REF, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
-    return fwd_levels<KERN, J2K_ORDER_T800, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
+                              void* b, cudaStream_t st, int n, size_t iz, size_t oz) {
+    if (order == J2K_ORDER_REF) return fwd_levels<KERN, J2K_ORDER_REF, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st, n, iz, oz);
+    return fwd_levels<KERN, J2K_ORDER_T800, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st, n, iz, oz);
 }
 template <int KERN, int TW, int TH>
 j2k_status inv_dispatch_order(j2k_ctx* ctx, int order, const void* in, size_t ip, void* out,
                               size_t op, int w, int h, int levels, const float* steps, void* a,
-                              void* b, cudaStream_t st) {
-    if (order == J2K_ORDER_REF) return inv_levels<KERN, J2K_ORDER_REF, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
-    return inv_levels<KERN, J2K_ORDER_T800, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st);
+                              void* b, cudaStream_t st, int n, size_t iz, size_t oz) {
+    if (order == J2K_ORDER_REF) return inv_levels<KERN, J2K_ORDER_REF, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st, n, iz, oz);
+    return inv_levels<KERN, J2K_ORDER_T800, TW, TH>(ctx, in, ip, out, op, w, h, levels, steps, a, b, st, n, iz, oz);
 }
 
 }  // namespace
@@ -784,23 +816,23 @@ j2k_status inv_dispatch_order(j2k_ctx* ctx, int order, const void* in, size_t ip
 j2k_status j2k_dwt_fwd_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
-                            cudaStream_t st) {
+                            cudaStream_t st, int n, size_t in_z, size_t out_z) {
     if (kernel == J2K_W53)
         return J2K_TILE_DISPATCH(fwd_dispatch_order, 53, ctx, order, in, in_pitch, out, out_pitch,
-                                 (int)w, (int)h, levels, steps, ll0, ll1, st);
+                                 (int)w, (int)h, levels, steps, ll0, ll1, st, n, in_z, out_z);
     return J2K_TILE_DISPATCH(fwd_dispatch_order, 97, ctx, order, in, in_pitch, out, out_pitch,
-                             (int)w, (int)h, levels, steps, ll0, ll1, st);
+                             (int)w, (int)h, levels, steps, ll0, ll1, st, n, in_z, out_z);
 }
 
 j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
-                            cudaStream_t st) {
+                            cudaStream_t st, int n, size_t in_z, size_t out_z) {
     if (kernel == J2K_W53)
         return J2K_TILE_DISPATCH(inv_dispatch_order, 53, ctx, order, in, in_pitch, out, out_pitch,
-                                 (int)w, (int)h, levels, steps, ll0, ll1, st);
+                                 (int)w, (int)h, levels, steps, ll0, ll1, st, n, in_z, out_z);
     return J2K_TILE_DISPATCH(inv_dispatch_order, 97, ctx, order, in, in_pitch, out, out_pitch,
-                             (int)w, (int)h, levels, steps, ll0, ll1, st);
+                             (int)w, (int)h, levels, steps, ll0, ll1, st, n, in_z, out_z);
 }
 
 j2k_status j2k_dwt_fwd_batched_launch(j2k_ctx* ctx, int kernel, int order, j2k_dwt_tile tile,

@@ -125,14 +125,16 @@ struct j2k_dwt_level_desc {
 j2k_status j2k_dwt_fwd_batched_launch(j2k_ctx* ctx, int kernel, int order, j2k_dwt_tile tile,
                                       const j2k_dwt_level_desc* d_descs, const uint32_t* d_owner,
                                       unsigned ntiles, cudaStream_t st);
+// n images at element strides in_z / out_z (blockIdx.z); the LL scratch holds n images at
+// strides ceil(w/2)*ceil(h/2) (ll0) and ceil(w/4)*ceil(h/4) (ll1).
 j2k_status j2k_dwt_fwd_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
-                            cudaStream_t st);
+                            cudaStream_t st, int n = 1, size_t in_z = 0, size_t out_z = 0);
 j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
-                            cudaStream_t st);
+                            cudaStream_t st, int n = 1, size_t in_z = 0, size_t out_z = 0);
 
 // Tier-1 encode of njobs blocks.  order (device, optional): phase-A processing order (largest
 // first); sym_bytes: size of the symbol scratch the jobs' sym_off/sym_cap address.

@@ -37,8 +37,8 @@ def dwt97(x, levels):
     x = x.contiguous()
     n, hh, ww = x.shape
     y = torch.empty_like(x)
-    for i in range(n):
-        check(lib().j2k_dwt_forward(h, L.W97, L.ORDER_T800, _p(x[i]), ww, _p(y[i]), ww, ww, hh, levels, None), h)
+    check(lib().j2k_dwt_forward_batch(h, L.W97, L.ORDER_T800, _p(x), ww, ww * hh, _p(y), ww, ww * hh, n, ww, hh,
+                                      levels, None), h)
     return y
 
 
@@ -47,8 +47,8 @@ def idwt97(y, levels):
     y = y.contiguous()
     n, hh, ww = y.shape
     x = torch.empty_like(y)
-    for i in range(n):
-        check(lib().j2k_dwt_inverse(h, L.W97, L.ORDER_T800, _p(y[i]), ww, _p(x[i]), ww, ww, hh, levels, None), h)
+    check(lib().j2k_dwt_inverse_batch(h, L.W97, L.ORDER_T800, _p(y), ww, ww * hh, _p(x), ww, ww * hh, n, ww, hh,
+                                      levels, None), h)
     return x
 
 

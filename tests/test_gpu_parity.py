@@ -220,3 +220,31 @@ def test_fast_level0_path_bit_exact(C, w, h, L, kern):
         st = O.default_steps(w, h, L)
         assert np.array_equal(C.dwt_forward(dev(x), L, 97, 0, steps=st).cpu().numpy(),
                               O.quantize(O.dwt97_fwd(x, L), L, st))
+
+
+BATCH_CASES = [(33, 17, 3), (248, 64, 2), (127, 131, 5), (64, 64, 6), (1, 9, 2), (300, 77, 4)]
+
+
+@pytest.mark.parametrize("w,h,L", BATCH_CASES)
+@pytest.mark.parametrize("order", [0, 1])
+def test_batched_dwt_matches_per_image(C, w, h, L, order):
+    """One launch per level over a batch of planes (image index in the grid's z) must give each
+    plane exactly what the single-plane transform and the oracle give."""
+    n = 3
+    rng = np.random.default_rng(w * 7 + h + L)
+    xi = rng.integers(-255, 256, (n, h, w)).astype(np.int32)
+    xf = rng.uniform(-128, 128, (n, h, w)).astype(np.float32)
+    yi = C.dwt_forward(dev(xi), L, 53, order).cpu().numpy()
+    yf = C.dwt_forward(dev(xf), L, 97, order).cpu().numpy()
+    for i in range(n):
+        assert np.array_equal(yi[i], O.dwt53_fwd(xi[i], L, order))
+        assert np.array_equal(yf[i], O.dwt97_fwd(xf[i], L, order))
+    assert np.array_equal(C.dwt_inverse(dev(yi), L, 53, order).cpu().numpy(), xi)
+    bf = C.dwt_inverse(dev(yf), L, 97, order).cpu().numpy()
+    for i in range(n):
+        assert np.array_equal(bf[i], O.dwt97_inv(yf[i], L, order))
+    if order == 0:
+        st = O.default_steps(w, h, L)
+        q = C.dwt_forward(dev(xf), L, 97, 0, steps=st).cpu().numpy()
+        for i in range(n):
+            assert np.array_equal(q[i], O.quantize(O.dwt97_fwd(xf[i], L), L, st))
