@@ -213,12 +213,13 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs
  * j2k_dwt97_inverse_adjoint: transpose of the inverse DWT (image gradient -> Mallat gradient).
  * The relaxed quantiser replaces rounding by additive noise of one step: for a coefficient y of
  * subband b (step = exp(log_steps[b]), log_steps a device array of 3L+1 floats),
- *   t = y/step + u, u ~ U[-1/2,1/2) (Philox4x32-10 keyed by seed+image, counter = y*w+x),
- *   y_hat = t*step, rate = log2(1+|t|).
- * Forward writes y_hat and, per (image, band, part), a partial rate sum (parts_per_band
- * partials per band, to be summed by the caller in a fixed order).  Backward, for a loss
- * L(y_hat) + lam * sum(rate), writes dL/dy and per-(image, band, part) partials of dL/dlog_step.
- * levels <= 16. */
+ *   t = y/step + u, y_hat = t*step, rate = log2(1+|t|), u ~ U[-1/2,1/2): Philox4x32-10 keyed
+ *   by seed+image, counter y*ceil(w/4) + x/4 for the Mallat sample (x, y), output word x%4,
+ *   u = (word >> 8) * 2^-24 - 1/2.
+ * Forward writes y_hat and, per (image, band, part), a partial rate sum: the plane's rows are
+ * split into parts_per_band row ranges, partial[(image*(3L+1) + band)*parts_per_band + part],
+ * to be summed by the caller in a fixed order.  Backward, for a loss L(y_hat) + lam*sum(rate),
+ * writes dL/dy and the same layout of partials of dL/dlog_step.  levels <= 16. */
 j2k_status j2k_dwt97_forward_adjoint(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, size_t w,
                                      size_t h, int levels);
 j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_coef, int n, size_t w,
@@ -229,6 +230,24 @@ j2k_status j2k_relaxed_quant_forward(j2k_ctx* ctx, const float* y, float* y_hat,
 j2k_status j2k_relaxed_quant_backward(j2k_ctx* ctx, const float* y, const float* g_yhat, float* g_y, int n,
                                       size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
                                       float lam, float* g_logstep_partials, int parts_per_band);
+/* Same, with the incoming gradient scaled on the device: g_yhat = (*scale) * alpha * g_in and the
+ * rate weight (*scale) * lam (scale: device pointer to one float, NULL = 1), so that an autograd
+ * backward can pass its output gradient without reading it on the host. */
+j2k_status j2k_relaxed_quant_backward_scaled(j2k_ctx* ctx, const float* y, const float* g_in, float* g_y, int n,
+                                             size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
+                                             float lam, const float* scale, float alpha, float* g_logstep_partials,
+                                             int parts_per_band);
+/* Fused residual forms for a distortion term mean((IDWT(y) - x)^2):
+ * j2k_dwt97_inverse_residual writes d = IDWT(y) - x (the reconstruction itself is never stored)
+ * and one partial sum of d^2 per 248 x 16 tile of the finest level, j2k_dwt97_residual_partials
+ * of them, image-major; j2k_dwt97_forward_adjoint_residual writes
+ * g_img = DWT^T(g_coef) - (*scale) * alpha * sub (scale: device pointer or NULL = 1). */
+size_t j2k_dwt97_residual_partials(size_t w, size_t h, int n);
+j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float* x, float* d, int n, size_t w,
+                                      size_t h, int levels, float* sq_partials);
+j2k_status j2k_dwt97_forward_adjoint_residual(j2k_ctx* ctx, const float* g_coef, const float* sub,
+                                              const float* scale, float alpha, float* g_img, int n, size_t w,
+                                              size_t h, int levels);
 
 /* ---- batched encoder.  No counterpart in the reference, which encodes one image per
  * OCLEncoder<T>::run call (src/OCLEncoder.cpp:43-52).  Many images of uneven size, mixed 5/3 and

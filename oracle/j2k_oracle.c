@@ -1285,6 +1285,15 @@ double or_philox_uniform(uint64_t seed, uint64_t i) {
     return (double)(o[0] >> 8) * (1.0 / 16777216.0) - 0.5;
 }
 
+double or_rd_noise(uint64_t seed, size_t w, size_t x, size_t y) {
+    /* one Philox block per 4 consecutive samples of a plane row: counter y*ceil(w/4) + x/4,
+     * output word x%4 */
+    uint64_t c = (uint64_t)y * ((w + 3) / 4) + x / 4;
+    uint32_t ctr[4] = {(uint32_t)c, (uint32_t)(c >> 32), 0, 0}, o[4];
+    or_philox4x32((uint32_t)seed, (uint32_t)(seed >> 32), ctr, o);
+    return (double)(o[x & 3] >> 8) * (1.0 / 16777216.0) - 0.5;
+}
+
 double or_rd_loss_f64(const double* x, size_t w, size_t h, int levels, const double* log_steps,
                       double lam, uint64_t seed, double* grad_x, double* grad_ls) {
     size_t N = w * h;
@@ -1305,7 +1314,7 @@ double or_rd_loss_f64(const double* x, size_t w, size_t h, int levels, const dou
         for (size_t yy = y0; yy < y0 + sh; ++yy)
             for (size_t xx = x0; xx < x0 + sw; ++xx) {
                 size_t i = yy * w + xx;
-                double u = or_philox_uniform(seed, i);
+                double u = or_rd_noise(seed, w, xx, yy);
                 double t = y[i] / st + u;
                 yh[i] = t * st;
                 rate += log(1.0 + fabs(t)) * inv_ln2;
@@ -1330,7 +1339,7 @@ double or_rd_loss_f64(const double* x, size_t w, size_t h, int levels, const dou
             for (size_t yy = y0; yy < y0 + sh; ++yy)
                 for (size_t xx = x0; xx < x0 + sw; ++xx) {
                     size_t i = yy * w + xx;
-                    double u = or_philox_uniform(seed, i);
+                    double u = or_rd_noise(seed, w, xx, yy);
                     double t = y[i] / st + u;
                     double sg = t > 0 ? 1.0 : (t < 0 ? -1.0 : 0.0);
                     double dr_dt = lam * inv_ln2 * sg / (1.0 + fabs(t));

@@ -125,6 +125,7 @@ long or_encode_image(const uint8_t* img, size_t w, size_t h, int ncomp, const or
 /* ---- differentiable 9/7 (FP64) ------------------------------------------------------------- */
 /* Philox4x32-10 (Salmon et al., SC'11) uniform in [-0.5, 0.5) for element index i. */
 double or_philox_uniform(uint64_t seed, uint64_t i);
+double or_rd_noise(uint64_t seed, size_t w, size_t x, size_t y);
 void or_philox4x32(uint32_t key0, uint32_t key1, const uint32_t ctr[4], uint32_t out[4]);
 /* loss = mean((x_hat - x)^2) + lam * sum log2(1 + |y + u*step|/step) over all coefficients,
  * x_hat = IDWT(y + u*step), y = DWT(x); steps = exp(log_steps[b]).  Returns the loss; when

@@ -50,6 +50,7 @@ def lib():
             "or_t1_decode": [P, I, I, I, I, P, S, I, I],
             "or_encode_image": [P, S, S, I, P, P, C.c_long],
             "or_philox_uniform": [C.c_uint64, C.c_uint64],
+            "or_rd_noise": [C.c_uint64, S, S, S],
             "or_rd_loss_f64": [P, S, S, I, P, D, C.c_uint64, P, P],
         }
         for name, args in sig.items():
@@ -60,6 +61,7 @@ def lib():
         L.or_subband_rect.restype = I
         L.or_encode_image.restype = C.c_long
         L.or_philox_uniform.restype = D
+        L.or_rd_noise.restype = D
         L.or_rd_loss_f64.restype = D
         _LIB = L
     return _LIB
@@ -219,6 +221,11 @@ def encode_image(img, levels, cbw=64, cbh=64, lossless=True, order=ORDER_T800, s
 
 def philox_uniform(seed, i):
     return lib().or_philox_uniform(seed, i)
+
+
+def rd_noise(seed, w, x, y):
+    """Noise sample of the relaxed quantiser at Mallat position (x, y) of a w-wide plane."""
+    return lib().or_rd_noise(seed, w, x, y)
 
 
 def rd_loss(x, levels, log_steps, lam, seed, grads=True):

@@ -197,7 +197,7 @@ j2k_status j2k_ctx_destroy(j2k_ctx* ctx) {
     if (!ctx) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < J2K_SCRATCH_SLOTS; ++i)
         if (ctx->scratch[i]) cudaFree(ctx->scratch[i]);
     if (ctx->d_err) cudaFree(ctx->d_err);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);

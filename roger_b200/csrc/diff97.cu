@@ -21,12 +21,10 @@
 // position in its Mallat plane (the oracle draws the same stream).
 #include <cmath>
 
-#include "j2k_internal.cuh"
+#include "lift.cuh"
 
 namespace {
 
-constexpr float P1 = -1.586134342f, U1 = -0.05298011854f, P2 = 0.8829110762f, U2 = 0.4435068522f;
-constexpr float KMUL = 1.23017410491400f, KDIV = 0.81289306611596153187273657637352f;
 constexpr int TW = 64, TH = 64, HALO = 4, NX = TW + 2 * HALO, NY = TH + 2 * HALO, SS = NX + 1;
 
 // Transposed step sequences (parity updated, coefficient):
@@ -177,10 +175,44 @@ __global__ void copy_f(const float* __restrict__ a, size_t ap, float* __restrict
     if (x < w && y < h) b[(size_t)y * bp + x] = a[(size_t)y * ap + x];
 }
 
+// out = a - (*scale) * alpha * b (natural order, n planes back to back); the small-level
+// fallback of the fused residual forms below
+__global__ void axpy_f(const float* a, const float* b, const float* scale, float alpha, float* out, size_t count) {
+    const float sc = __fmul_rn(scale ? *scale : 1.0f, alpha);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __fsub_rn(a[i], __fmul_rn(sc, b[i]));
+}
+
+// d = xh - x over the same 248 x 16 tiles as the strip kernel, one partial sum of d^2 per tile
+__global__ void residual_tiles(const float* xh, const float* x, float* d, int w, int h, float* part) {
+    const size_t plane = (size_t)w * h;
+    xh += blockIdx.z * plane;
+    x += blockIdx.z * plane;
+    d += blockIdx.z * plane;
+    float sq = 0.0f;
+    for (int e = threadIdx.x; e < FTW * STH; e += blockDim.x) {
+        const int xx = blockIdx.x * FTW + e % FTW, yy = blockIdx.y * STH + e / FTW;
+        if (xx < w && yy < h) {
+            const size_t i = (size_t)yy * w + xx;
+            const float v = __fsub_rn(xh[i], x[i]);
+            d[i] = v;
+            sq = __fmaf_rn(v, v, sq);
+        }
+    }
+    __shared__ float red[256];
+    red[threadIdx.x] = sq;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = red[0];
+}
+
 // ---- Philox4x32-10 (Salmon et al., SC'11) -------------------------------------------------------
-__device__ __forceinline__ float philox_uniform(uint64_t seed, uint64_t i) {
-    uint32_t c0 = (uint32_t)i, c1 = (uint32_t)(i >> 32), c2 = 0, c3 = 0;
-    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+__device__ __forceinline__ void philox4(uint64_t key, uint64_t ctr, uint32_t (&o)[4]) {
+    uint32_t c0 = (uint32_t)ctr, c1 = (uint32_t)(ctr >> 32), c2 = 0, c3 = 0;
+    uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
         const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
@@ -193,93 +225,234 @@ __device__ __forceinline__ float philox_uniform(uint64_t seed, uint64_t i) {
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
     }
-    return __fmul_rn((float)(c0 >> 8), 1.0f / 16777216.0f) - 0.5f;
+    o[0] = c0;
+    o[1] = c1;
+    o[2] = c2;
+    o[3] = c3;
+}
+__device__ __forceinline__ float noise_of(uint32_t word) {
+    return __fmul_rn((float)(word >> 8), 1.0f / 16777216.0f) - 0.5f;
 }
 
-// band geometry of one Mallat plane, in QCD order
-struct Bands {
-    int nb;
-    int x0[3 * 16 + 1], y0[3 * 16 + 1], bw[3 * 16 + 1], bh[3 * 16 + 1];
+// Level widths/heights of one Mallat plane: W[0] = w, W[k] = ceil(W[k-1]/2).
+struct Levels {
+    int L;
+    int W[17], H[17];
 };
-
-// grid: (tiles of 256 samples within the band, band, image).  Each CTA writes one partial sum
-// per output (rate) so that the host-side reduction is in a fixed order.
-__global__ void __launch_bounds__(256)
-relaxed_quant_fwd(const float* __restrict__ y, float* __restrict__ yhat, int w, int h, size_t plane,
-                  Bands B, const float* __restrict__ log_steps, uint64_t seed, float* __restrict__ rate_part,
-                  int parts_per_band) {
-    const int b = blockIdx.y, img = blockIdx.z;
-    const int n = B.bw[b] * B.bh[b];
-    const float step = expf(log_steps[b]);
-    const float inv_ln2 = 1.4426950408889634f;
-    float acc = 0.0f;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int xx = B.x0[b] + e % B.bw[b], yy = B.y0[b] + e / B.bw[b];
-        const size_t idx = (size_t)img * plane + (size_t)yy * w + xx;
-        const float u = philox_uniform(seed + (uint64_t)img, (uint64_t)yy * w + xx);
-        const float t = __fadd_rn(__fdiv_rn(y[idx], step), u);
-        yhat[idx] = __fmul_rn(t, step);
-        acc += log1pf(fabsf(t)) * inv_ln2;
-    }
-    __shared__ float red[256];
-    red[threadIdx.x] = acc;
-    __syncthreads();
-    for (int o = 128; o; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) rate_part[((size_t)img * B.nb + b) * parts_per_band + blockIdx.x] = red[0];
+// depth of a coordinate: how many of the levels keep it in their low half
+__device__ __forceinline__ int depth_of(int v, const int* lim, int L) {
+    int d = 0;
+#pragma unroll
+    for (int k = 1; k <= 16; ++k)
+        if (k <= L) d += v < lim[k];
+    return d;
+}
+// QCD band index of the Mallat sample with depths (dx, dy): LL = 0, level d's HL/LH/HH at
+// 1 + 3(L - d) + {0, 1, 2}
+__device__ __forceinline__ int band_of(int dx, int dy, int L) {
+    const int m = min(dx, dy);
+    if (m == L) return 0;
+    const int o = (dx == m && dy == m) ? 2 : (dx == m ? 0 : 1);
+    return 1 + 3 * (L - (m + 1)) + o;
 }
 
-// g_y = g_yhat + lam * dr/dt / step;  g_logstep[b] += g_yhat * u * step + lam * dr/dt * (-y/step)
+// Relaxed quantiser over whole Mallat planes.  grid (parts, images); CTA p takes rows
+// [p*rows, (p+1)*rows) of its image, thread i the 4-sample groups i, i+256, ... of each row.
+// Noise: one Philox4x32-10 call per group (key seed + image, counter y*ceil(w/4) + x/4), word
+// x%4 for sample x.  Per-band sums are kept per thread in shared memory and reduced in a
+// fixed order, so the partials are deterministic.
+template <bool BWD>
 __global__ void __launch_bounds__(256)
-relaxed_quant_bwd(const float* __restrict__ y, const float* __restrict__ gyhat, float* __restrict__ gy, int w, int h,
-                  size_t plane, Bands B, const float* __restrict__ log_steps, uint64_t seed, float lam,
-                  float* __restrict__ gls_part, int parts_per_band) {
-    const int b = blockIdx.y, img = blockIdx.z;
-    const int n = B.bw[b] * B.bh[b];
-    const float step = expf(log_steps[b]);
-    const float inv_ln2 = 1.4426950408889634f;
-    float acc = 0.0f;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const int xx = B.x0[b] + e % B.bw[b], yy = B.y0[b] + e / B.bw[b];
-        const size_t idx = (size_t)img * plane + (size_t)yy * w + xx;
-        const float u = philox_uniform(seed + (uint64_t)img, (uint64_t)yy * w + xx);
-        const float yv = y[idx];
-        const float t = __fadd_rn(__fdiv_rn(yv, step), u);
-        const float sg = t > 0.0f ? 1.0f : (t < 0.0f ? -1.0f : 0.0f);
-        const float drdt = lam * inv_ln2 * sg / (1.0f + fabsf(t));
-        const float g = gyhat[idx];
-        gy[idx] = g + drdt / step;
-        acc += g * u * step - drdt * yv / step;
+relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, float* __restrict__ out, int w, int h,
+                size_t plane, Levels lv, const float* __restrict__ log_steps, uint64_t seed, float lam,
+                const float* __restrict__ gscale, float alpha, float* __restrict__ part, int rows, int vec) {
+    extern __shared__ float acc[];  // [band][256]
+    __shared__ float stp[49], rstp[49];
+    __shared__ int wlim[17], hlim[17];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, img = blockIdx.y;
+    const int L = lv.L, nb = 3 * L + 1;
+    for (int b = 0; b < nb; ++b) acc[b * 256 + t] = 0.0f;
+    if (t < nb) {
+        stp[t] = expf(log_steps[t]);
+        rstp[t] = __frcp_rn(stp[t]);
     }
-    __shared__ float red[256];
-    red[threadIdx.x] = acc;
+    if (t <= L) {
+        wlim[t] = lv.W[t];
+        hlim[t] = lv.H[t];
+    }
     __syncthreads();
-    for (int o = 128; o; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
+    const float inv_ln2 = 1.4426950408889634f;
+    float G = 1.0f, lamG = lam;
+    if (BWD) {
+        const float s = gscale ? *gscale : 1.0f;
+        G = __fmul_rn(s, alpha);
+        lamG = __fmul_rn(s, lam);
     }
-    if (threadIdx.x == 0) gls_part[((size_t)img * B.nb + b) * parts_per_band + blockIdx.x] = red[0];
+    const int groups = (w + 3) >> 2;
+    const uint64_t key = seed + (uint64_t)img;
+    const int r0 = blockIdx.x * rows, r1 = min(h, r0 + rows);
+    for (int yy = r0; yy < r1; ++yy) {
+        const int dy = depth_of(yy, hlim, L);
+        const size_t rb = (size_t)img * plane + (size_t)yy * w;
+        for (int g = t; g < groups; g += 256) {
+            const int x = 4 * g;
+            uint32_t o[4];
+            philox4(key, (uint64_t)yy * groups + g, o);
+            float v[4], gi[4] = {0.f, 0.f, 0.f, 0.f}, r[4];
+            if (vec && x + 4 <= w) {
+                *reinterpret_cast<float4*>(v) = __ldg(reinterpret_cast<const float4*>(y + rb + x));
+                if (BWD) *reinterpret_cast<float4*>(gi) = __ldg(reinterpret_cast<const float4*>(gin + rb + x));
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    v[k] = x + k < w ? y[rb + x + k] : 0.0f;
+                    if (BWD) gi[k] = x + k < w ? gin[rb + x + k] : 0.0f;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (x + k >= w) break;
+                const int b = band_of(depth_of(x + k, wlim, L), dy, L);
+                const float step = stp[b], rs = rstp[b], u = noise_of(o[k]);
+                const float tt = __fadd_rn(__fmul_rn(v[k], rs), u);
+                if (!BWD) {
+                    r[k] = __fmul_rn(tt, step);
+                    acc[b * 256 + t] += log1pf(fabsf(tt)) * inv_ln2;
+                } else {
+                    const float sg = tt > 0.0f ? 1.0f : (tt < 0.0f ? -1.0f : 0.0f);
+                    const float drdt = __fdividef(lamG * inv_ln2 * sg, 1.0f + fabsf(tt));
+                    const float g = __fmul_rn(G, gi[k]);
+                    r[k] = __fadd_rn(g, __fmul_rn(drdt, rs));
+                    acc[b * 256 + t] += g * u * step - drdt * v[k] * rs;
+                }
+            }
+            if (vec && x + 4 <= w) {
+                *reinterpret_cast<float4*>(out + rb + x) = *reinterpret_cast<float4*>(r);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (x + k < w) out[rb + x + k] = r[k];
+            }
+        }
+    }
+    __syncthreads();
+    for (int b = warp; b < nb; b += 8) {
+        float a = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a += acc[b * 256 + lane + 32 * i];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (lane == 0) part[((size_t)img * nb + b) * gridDim.x + blockIdx.x] = a;
+    }
 }
 
-Bands make_bands(int w, int h, int levels) {
-    Bands B{};
-    j2k_band_rect r[3 * 16 + 1];
-    B.nb = j2k_band_rects(w, h, levels, r);
-    for (int b = 0; b < B.nb; ++b) {
-        B.x0[b] = (int)r[b].x0;
-        B.y0[b] = (int)r[b].y0;
-        B.bw[b] = (int)r[b].w;
-        B.bh[b] = (int)r[b].h;
+Levels make_levels(int w, int h, int levels) {
+    Levels lv{};
+    lv.L = levels;
+    lv.W[0] = w;
+    lv.H[0] = h;
+    for (int k = 1; k <= levels; ++k) {
+        lv.W[k] = (lv.W[k - 1] + 1) / 2;
+        lv.H[k] = (lv.H[k - 1] + 1) / 2;
     }
-    return B;
+    return lv;
 }
 
 j2k_status check_common(j2k_ctx* ctx, const void* a, const void* b, int n, size_t w, size_t h, int levels) {
     if (!ctx) return J2K_ERR_INVALID_ARG;
-    if (!a || !b || n <= 0 || w == 0 || h == 0 || w > 65535 || h > 65535 || levels < 0 || levels > 16)
+    if (!a || !b || n <= 0 || n > 65535 || w == 0 || h == 0 || w > 65535 || h > 65535 || levels < 0 ||
+        levels > 16)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "differentiable 9/7: bad pointer, size or levels (0..16)");
+    return J2K_OK;
+}
+
+// Transpose of the forward DWT, deepest level first.  With `ex` (EXTRA 2) the level-0 output
+// is g_img = DWT^T(g_coef) - (*scale) * alpha * sub.
+j2k_status fwd_adj_run(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, size_t w, size_t h, int levels,
+                       const SynExtra* ex) {
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    int ws[20], hs[20];
+    ws[0] = (int)w;
+    hs[0] = (int)h;
+    for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
+    const size_t plane = w * h, zlev = (size_t)ws[1] * hs[1];
+    if (levels == 0) {
+        if (ex) {
+            axpy_f<<<ctx->sm_count * 4, 256, 0, st>>>(g_coef, ex->sub, ex->scale, ex->alpha, g_img, plane * n);
+        } else {
+            for (int img = 0; img < n; ++img)
+                copy_f<<<dim3((unsigned)((w + 255) / 256), (unsigned)h), 256, 0, st>>>(
+                    g_coef + img * plane, w, g_img + img * plane, w, (int)w, (int)h);
+        }
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, zlev * n * 4 + 64);
+    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, zlev * n * 4 + 64);
+    if (!s0 || !s1) return J2K_ERR_OUT_OF_MEMORY;
+    const float* ll = g_coef;  // LL_L lives in the top-left of each Mallat plane
+    size_t llp = w, llz = plane;
+    for (int k = levels - 1; k >= 0; --k) {
+        float* out = k == 0 ? g_img : ((levels - 1 - k) % 2 == 0 ? s0 : s1);
+        const size_t op = k == 0 ? w : (size_t)ws[k], oz = k == 0 ? plane : zlev;
+        const bool fused = k == 0 && ex;
+        if (ws[k] >= 8 && hs[k] >= 2) {
+            const int wl = (ws[k] + 1) / 2;
+            const int vec = (((uintptr_t)g_coef & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) &&
+                            (((uintptr_t)ll & 7) == 0) && ((llp & 1) == 0) && ((llz & 1) == 0) && ((wl & 1) == 0);
+            const dim3 fg((ws[k] + FTW - 1) / FTW, (hs[k] + STH - 1) / STH, n);
+            const ZStride zs{plane, oz, llz};
+            if (fused)
+                dwt_syn_fast<97, 1, float, false, false, 2><<<fg, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k],
+                                                                                 out, op, Steps4{}, zs, vec, *ex);
+            else
+                dwt_syn_fast<97, 1, float, false, false, 0><<<fg, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k],
+                                                                                 out, op, Steps4{}, zs, vec,
+                                                                                 SynExtra{});
+        } else {
+            dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
+            fwd_adj_level<<<g, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k], out, op, plane, llz, oz);
+            if (fused)
+                axpy_f<<<ctx->sm_count * 4, 256, 0, st>>>(g_img, ex->sub, ex->scale, ex->alpha, g_img, plane * n);
+        }
+        J2K_CUDA(ctx, cudaGetLastError());
+        ll = out;
+        llp = op;
+        llz = oz;
+    }
+    return J2K_OK;
+}
+
+j2k_status quant_run(j2k_ctx* ctx, bool bwd, const float* y, const float* gin, float* out, int n, size_t w,
+                     size_t h, int levels, const float* log_steps, uint64_t seed, float lam, const float* gscale,
+                     float alpha, float* partials, int parts) {
+    J2K_TRY(check_common(ctx, y, out, n, w, h, levels));
+    if (!log_steps || !partials || parts <= 0 || parts > 65535 || (bwd && !gin))
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "relaxed quantiser: bad log_steps, partials or parts");
+    cudaSetDevice(ctx->device);
+    const int nb = 3 * levels + 1;
+    const size_t smem = (size_t)nb * 256 * 4;
+    const int rows = (int)((h + parts - 1) / parts);
+    const size_t plane = w * h;
+    const int vec = (((uintptr_t)y & 15) == 0) && (((uintptr_t)out & 15) == 0) && (!bwd || ((uintptr_t)gin & 15) == 0) &&
+                    ((w & 3) == 0);
+    const dim3 g((unsigned)parts, (unsigned)n);
+    const Levels lv = make_levels((int)w, (int)h, levels);
+    if (bwd) {
+        if (smem > 48 * 1024)
+            J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem));
+        relaxed_quant_k<true><<<g, 256, smem, ctx->stream>>>(y, gin, out, (int)w, (int)h, plane, lv, log_steps, seed,
+                                                             lam, gscale, alpha, partials, rows, vec);
+    } else {
+        if (smem > 48 * 1024)
+            J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem));
+        relaxed_quant_k<false><<<g, 256, smem, ctx->stream>>>(y, nullptr, out, (int)w, (int)h, plane, lv, log_steps,
+                                                              seed, 0.0f, nullptr, 1.0f, partials, rows, vec);
+    }
+    J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }
 
@@ -290,38 +463,16 @@ extern "C" {
 j2k_status j2k_dwt97_forward_adjoint(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, size_t w, size_t h,
                                      int levels) {
     J2K_TRY(check_common(ctx, g_coef, g_img, n, w, h, levels));
-    cudaSetDevice(ctx->device);
-    cudaStream_t st = ctx->stream;
-    int ws[20], hs[20];
-    ws[0] = (int)w;
-    hs[0] = (int)h;
-    for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
-    const size_t plane = w * h, zlev = (size_t)ws[1] * hs[1];
-    if (levels == 0) {
-        for (int img = 0; img < n; ++img)
-            copy_f<<<dim3((unsigned)((w + 255) / 256), (unsigned)h), 256, 0, st>>>(g_coef + img * plane, w,
-                                                                                  g_img + img * plane, w, (int)w,
-                                                                                  (int)h);
-        J2K_CUDA(ctx, cudaGetLastError());
-        return J2K_OK;
-    }
-    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, zlev * n * 4 + 64);
-    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, zlev * n * 4 + 64);
-    if (!s0 || !s1) return J2K_ERR_OUT_OF_MEMORY;
-    // deepest level first; level k's LL gradient is level k+1's output
-    const float* ll = g_coef;  // LL_L lives in the top-left of each Mallat plane
-    size_t llp = w, llz = plane;
-    for (int k = levels - 1; k >= 0; --k) {
-        float* out = k == 0 ? g_img : ((levels - 1 - k) % 2 == 0 ? s0 : s1);
-        const size_t op = k == 0 ? w : (size_t)ws[k], oz = k == 0 ? plane : zlev;
-        dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
-        fwd_adj_level<<<g, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k], out, op, plane, llz, oz);
-        J2K_CUDA(ctx, cudaGetLastError());
-        ll = out;
-        llp = op;
-        llz = oz;
-    }
-    return J2K_OK;
+    return fwd_adj_run(ctx, g_coef, g_img, n, w, h, levels, nullptr);
+}
+
+j2k_status j2k_dwt97_forward_adjoint_residual(j2k_ctx* ctx, const float* g_coef, const float* sub,
+                                              const float* scale, float alpha, float* g_img, int n, size_t w,
+                                              size_t h, int levels) {
+    J2K_TRY(check_common(ctx, g_coef, g_img, n, w, h, levels));
+    if (!sub) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "forward adjoint residual: sub is NULL");
+    const SynExtra ex{sub, w, w * h, scale, alpha, nullptr};
+    return fwd_adj_run(ctx, g_coef, g_img, n, w, h, levels, &ex);
 }
 
 j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_coef, int n, size_t w, size_t h,
@@ -351,8 +502,17 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
         const bool last = k == levels - 1;
         float* ll = last ? g_coef : (k % 2 == 0 ? s0 : s1);
         const size_t llp = last ? w : (size_t)ws[k + 1], llz = last ? plane : zlev;
-        dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
-        inv_adj_level<<<g, 256, 0, st>>>(in, ip, ws[k], hs[k], g_coef, w, ll, llp, iz, plane, llz);
+        if (ws[k] >= 8 && hs[k] >= 2) {
+            const int vin = (((uintptr_t)in & 15) == 0) && ((ip & 3) == 0) && ((iz & 3) == 0);
+            const int vout = (((uintptr_t)g_coef & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) &&
+                             (((uintptr_t)ll & 7) == 0) && ((llp & 1) == 0) && ((llz & 1) == 0);
+            const dim3 fg((ws[k] + FTW - 1) / FTW, (hs[k] + STH - 1) / STH, n);
+            iadj_ana_fast<<<fg, 256, 0, st>>>(in, ip, ws[k], hs[k], g_coef, w, ll, llp, ZStride{iz, plane, llz}, vin,
+                                              vout);
+        } else {
+            dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
+            inv_adj_level<<<g, 256, 0, st>>>(in, ip, ws[k], hs[k], g_coef, w, ll, llp, iz, plane, llz);
+        }
         J2K_CUDA(ctx, cudaGetLastError());
         in = ll;
         ip = llp;
@@ -361,34 +521,74 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
     return J2K_OK;
 }
 
+size_t j2k_dwt97_residual_partials(size_t w, size_t h, int n) {
+    return ((w + FTW - 1) / FTW) * ((h + STH - 1) / STH) * (size_t)(n > 0 ? n : 0);
+}
+
+j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float* x, float* d, int n, size_t w,
+                                      size_t h, int levels, float* sq_partials) {
+    J2K_TRY(check_common(ctx, y, d, n, w, h, levels));
+    if (!x || !sq_partials) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "inverse residual: NULL x or partials");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t plane = w * h;
+    const dim3 fg((unsigned)((w + FTW - 1) / FTW), (unsigned)((h + STH - 1) / STH), (unsigned)n);
+    if (levels == 0 || w < 8 || h < 2) {
+        // small planes: plain inverse into d, then the residual pass over the same tiles
+        J2K_TRY(j2k_dwt_inverse_batch(ctx, J2K_W97, J2K_ORDER_T800, y, w, plane, d, w, plane, n, w, h, levels,
+                                      nullptr));
+        residual_tiles<<<fg, 256, 0, st>>>(d, x, d, (int)w, (int)h, sq_partials);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    // levels L..2 reconstruct LL_1 (the top-left ceil(w/2) x ceil(h/2) of each Mallat plane is
+    // itself the Mallat plane of LL_1's (L-1)-level transform) into scratch; level 1 runs fused
+    const size_t w1 = (w + 1) / 2, h1 = (h + 1) / 2;
+    const float* ll = y;
+    size_t llp = w, llz = plane;
+    if (levels > 1) {
+        float* buf = (float*)j2k_scratch(ctx, SCR_RES, w1 * h1 * (size_t)n * 4 + 64);
+        if (!buf) return J2K_ERR_OUT_OF_MEMORY;
+        size_t w2 = (w1 + 1) / 2, h2 = (h1 + 1) / 2;
+        void* a = j2k_scratch(ctx, SCR_LL0, w2 * h2 * (size_t)n * 4 + 64);
+        void* b = j2k_scratch(ctx, SCR_LL1, ((w2 + 1) / 2) * ((h2 + 1) / 2) * (size_t)n * 4 + 64);
+        if (!a || !b) return J2K_ERR_OUT_OF_MEMORY;
+        J2K_TRY(j2k_dwt_inv_impl(ctx, J2K_W97, J2K_ORDER_T800, y, w, buf, w1, w1, h1, levels - 1, nullptr, a, b,
+                                 j2k_dwt_tile{64, 64}, st, n, plane, w1 * h1));
+        ll = buf;
+        llp = w1;
+        llz = w1 * h1;
+    }
+    const int wl = (int)w1;
+    const int vec = (((uintptr_t)y & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) && (((uintptr_t)ll & 7) == 0) &&
+                    ((llp & 1) == 0) && ((llz & 1) == 0) && ((wl & 1) == 0);
+    const SynExtra ex{x, w, plane, nullptr, 1.0f, sq_partials};
+    dwt_syn_fast<97, 0, float, false, false, 1><<<fg, 256, 0, st>>>(y, w, ll, llp, (int)w, (int)h, d, w, Steps4{},
+                                                                     ZStride{plane, plane, llz}, vec, ex);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
+}
+
 j2k_status j2k_relaxed_quant_forward(j2k_ctx* ctx, const float* y, float* y_hat, int n, size_t w, size_t h,
                                      int levels, const float* log_steps, uint64_t seed, float* rate_partials,
                                      int parts_per_band) {
-    J2K_TRY(check_common(ctx, y, y_hat, n, w, h, levels));
-    if (!log_steps || !rate_partials || parts_per_band <= 0 || parts_per_band > 65535)
-        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "relaxed quantiser: bad log_steps/partials");
-    cudaSetDevice(ctx->device);
-    Bands B = make_bands((int)w, (int)h, levels);
-    dim3 g((unsigned)parts_per_band, (unsigned)B.nb, (unsigned)n);
-    relaxed_quant_fwd<<<g, 256, 0, ctx->stream>>>(y, y_hat, (int)w, (int)h, w * h, B, log_steps, seed, rate_partials,
-                                                  parts_per_band);
-    J2K_CUDA(ctx, cudaGetLastError());
-    return J2K_OK;
+    return quant_run(ctx, false, y, nullptr, y_hat, n, w, h, levels, log_steps, seed, 0.0f, nullptr, 1.0f,
+                     rate_partials, parts_per_band);
 }
 
 j2k_status j2k_relaxed_quant_backward(j2k_ctx* ctx, const float* y, const float* g_yhat, float* g_y, int n,
                                       size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
                                       float lam, float* g_logstep_partials, int parts_per_band) {
-    J2K_TRY(check_common(ctx, y, g_y, n, w, h, levels));
-    if (!g_yhat || !log_steps || !g_logstep_partials || parts_per_band <= 0 || parts_per_band > 65535)
-        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "relaxed quantiser backward: bad arguments");
-    cudaSetDevice(ctx->device);
-    Bands B = make_bands((int)w, (int)h, levels);
-    dim3 g((unsigned)parts_per_band, (unsigned)B.nb, (unsigned)n);
-    relaxed_quant_bwd<<<g, 256, 0, ctx->stream>>>(y, g_yhat, g_y, (int)w, (int)h, w * h, B, log_steps, seed, lam,
-                                                  g_logstep_partials, parts_per_band);
-    J2K_CUDA(ctx, cudaGetLastError());
-    return J2K_OK;
+    return quant_run(ctx, true, y, g_yhat, g_y, n, w, h, levels, log_steps, seed, lam, nullptr, 1.0f,
+                     g_logstep_partials, parts_per_band);
+}
+
+j2k_status j2k_relaxed_quant_backward_scaled(j2k_ctx* ctx, const float* y, const float* g_in, float* g_y, int n,
+                                             size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
+                                             float lam, const float* scale, float alpha, float* g_logstep_partials,
+                                             int parts_per_band) {
+    return quant_run(ctx, true, y, g_in, g_y, n, w, h, levels, log_steps, seed, lam, scale, alpha,
+                     g_logstep_partials, parts_per_band);
 }
 
 }  // extern "C"

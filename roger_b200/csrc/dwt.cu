@@ -19,44 +19,9 @@
 // HBM roofline per level: read c*n + write c*n bytes (c = 4), n = samples of the level.
 #include <algorithm>
 
-#include "j2k_internal.cuh"
+#include "lift.cuh"
 
 namespace {
-
-constexpr float P1 = -1.586134342f, U1 = -0.05298011854f, P2 = 0.8829110762f, U2 = 0.4435068522f;
-constexpr float KMUL = 1.23017410491400f, KDIV = 0.81289306611596153187273657637352f;
-
-// whole-sample symmetric extension (period 2(n-1)), parity preserving
-__device__ __forceinline__ int mirror(int i, int n) {
-    if (i >= 0 && i < n) return i;
-    if (n == 1) return 0;
-    const int p = 2 * (n - 1);
-    i %= p;
-    if (i < 0) i += p;
-    return i >= n ? p - i : i;
-}
-
-template <int KERN> struct KT;
-template <> struct KT<53> {
-    using T = int32_t;
-    static constexpr int H = 2, NSTEP = 2;
-    __device__ static int par(bool inv, int s) { return inv ? (s & 1) : 1 - (s & 1); }
-    __device__ static T op(bool inv, int s, T x, T a, T b) {
-        if (!inv) return s == 0 ? x - ((a + b) >> 1) : x + ((a + b + 2) >> 2);
-        return s == 0 ? x - ((a + b + 2) >> 2) : x + ((a + b) >> 1);
-    }
-};
-template <> struct KT<97> {
-    using T = float;
-    static constexpr int H = 4, NSTEP = 4;
-    __device__ static int par(bool inv, int s) { return inv ? (s & 1) : 1 - (s & 1); }
-    __device__ static T op(bool inv, int s, T x, T a, T b) {
-        float c;
-        if (!inv) c = s == 0 ? P1 : (s == 1 ? U1 : (s == 2 ? P2 : U2));
-        else c = s == 0 ? -U2 : (s == 1 ? -P2 : (s == 2 ? -U1 : -P1));
-        return __fadd_rn(x, __fmul_rn(c, __fadd_rn(a, b)));
-    }
-};
 
 // Shared tile geometry
 template <int KERN, int TW, int TH>
@@ -132,20 +97,6 @@ __device__ __forceinline__ void scale97(typename KT<KERN>::T* s) {
         __syncthreads();
     }
 }
-
-__device__ __forceinline__ int32_t quantize(float v, float step) {
-    int32_t m = (int32_t)floorf(__fdiv_rn(fabsf(v), step));
-    return v < 0.0f ? -m : m;
-}
-__device__ __forceinline__ float dequantize(int32_t q, float step) {
-    int32_t m = q < 0 ? -q : q;
-    float r = m ? __fmul_rn(__fadd_rn((float)m, 0.5f), step) : 0.0f;
-    return q < 0 ? -r : r;
-}
-
-struct Steps4 { float ll, hl, lh, hh; };
-// element strides between consecutive images of a batch (blockIdx.z selects the image)
-struct ZStride { size_t src, dst, ll; };
 
 // ---- forward level ----------------------------------------------------------------------------
 // src: level input (w x h).  Detail subbands go to dst at Mallat positions (dst is the full
@@ -256,7 +207,6 @@ dwt_fwd_batched(const j2k_dwt_level_desc* __restrict__ descs, const uint32_t* __
 //     warp shuffles (the 4-column halo absorbs the missing neighbours at the warp ends);
 //   * subbands are written straight from registers (8-byte vectors when aligned).
 // Same arithmetic, operation order and rounding as dwt_fwd_level, so the outputs are identical.
-constexpr int FTW = 248, FNX = 256;
 
 template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
 __global__ void __launch_bounds__(256, (KERN == 53 && FTH == 16) ? 8 : 6)
@@ -774,7 +724,27 @@ j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
         int bt = 1 + 3 * (levels - (k + 1));
         Steps4 st{1.f, 1.f, 1.f, 1.f};
         if (deq) st = Steps4{steps[0], steps[bt], steps[bt + 1], steps[bt + 2]};
-        if (deq) {
+        const bool fast_ok = ORDER == J2K_ORDER_T800 && cw >= 8 && chh >= 2 && (!ctx || ctx->dwt_fast_th != 0);
+        if (fast_ok) {
+            // register-lifting strip kernel; 8-byte band loads when every row start is aligned
+            const int wl = (cw + 1) / 2;
+            const int vec = (((uintptr_t)in & 7) == 0) && ((in_pitch & 1) == 0) && ((in_z & 1) == 0) &&
+                            (((uintptr_t)lls & 7) == 0) && ((llp & 1) == 0) && ((l_z & 1) == 0) &&
+                            ((wl & 1) == 0);
+            const dim3 fg((cw + FTW - 1) / FTW, (chh + STH - 1) / STH, n);
+            const SynExtra ex{};
+            if (deq) {
+                if (k == levels - 1)
+                    dwt_syn_fast<KERN, 0, int32_t, true, true, 0><<<fg, 256, 0, stream>>>(
+                        (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
+                else
+                    dwt_syn_fast<KERN, 0, int32_t, true, false, 0><<<fg, 256, 0, stream>>>(
+                        (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
+            } else {
+                dwt_syn_fast<KERN, 0, T, false, false, 0><<<fg, 256, 0, stream>>>(
+                    (const T*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
+            }
+        } else if (deq) {
             if (k == levels - 1)
                 dwt_inv_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(
                     (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs);

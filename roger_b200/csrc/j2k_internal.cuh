@@ -18,14 +18,16 @@ enum : uint32_t {
     J2K_DEVERR_PLANES = 5,        // more magnitude bit-planes than the coder supports
 };
 
+constexpr int J2K_SCRATCH_SLOTS = 9;
+
 struct j2k_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     std::string err;
     // grow-only device scratch slots (each independently sized)
-    void* scratch[8] = {};
-    size_t scratch_size[8] = {};
+    void* scratch[J2K_SCRATCH_SLOTS] = {};
+    size_t scratch_size[J2K_SCRATCH_SLOTS] = {};
     uint32_t* d_err = nullptr;   // device error word
     void* h_pinned = nullptr;    // pinned staging
     size_t h_pinned_size = 0;
@@ -38,7 +40,7 @@ struct j2k_ctx {
 
 // scratch slot ids
 enum { SCR_LL0 = 0, SCR_LL1 = 1, SCR_JOBS = 2, SCR_SYMS = 3, SCR_T1STATE = 4, SCR_MISC = 5,
-       SCR_PLANES = 6, SCR_MISC2 = 7 };
+       SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8 };
 
 j2k_status j2k_fail(j2k_ctx* ctx, j2k_status s, const std::string& msg);
 j2k_status j2k_cuda_check(j2k_ctx* ctx, cudaError_t e, const char* what);

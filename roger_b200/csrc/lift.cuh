@@ -1,0 +1,452 @@
+// Shared pieces of the lifting kernels: 9/7 constants, whole-sample symmetric extension, the
+// 5/3 and 9/7 step traits, the dead-zone (de)quantiser, and the register-lifting strip kernels
+// that run the synthesis shape (Mallat bands in, natural order out: the inverse DWT and the
+// transpose of the forward DWT) and the analysis shape of the transpose of the inverse DWT.
+//
+// Strip geometry (all register kernels): a CTA of 256 threads owns a 248-column x 16-row tile
+// of the level's output and stages a 256-column x (16 + 2*HV)-row strip in shared memory
+// (4 columns of halo on each side, HV = 2 rows for 5/3, 4 for 9/7).  Horizontal lifting runs
+// with 8 samples per lane and warp shuffles for the neighbours; vertical lifting runs with one
+// thread per column and the whole column in registers.  Each lifting step consumes one sample
+// of halo per side, so 4 columns / HV rows suffice for the 2 (5/3) or 4 (9/7) steps.
+#pragma once
+
+#include "j2k_internal.cuh"
+
+namespace {
+
+constexpr float P1 = -1.586134342f, U1 = -0.05298011854f, P2 = 0.8829110762f, U2 = 0.4435068522f;
+constexpr float KMUL = 1.23017410491400f, KDIV = 0.81289306611596153187273657637352f;
+
+// whole-sample symmetric extension (period 2(n-1)), parity preserving
+__device__ __forceinline__ int mirror(int i, int n) {
+    if (i >= 0 && i < n) return i;
+    if (n == 1) return 0;
+    const int p = 2 * (n - 1);
+    i %= p;
+    if (i < 0) i += p;
+    return i >= n ? p - i : i;
+}
+
+template <int KERN> struct KT;
+template <> struct KT<53> {
+    using T = int32_t;
+    static constexpr int H = 2, NSTEP = 2;
+    __device__ static int par(bool inv, int s) { return inv ? (s & 1) : 1 - (s & 1); }
+    __device__ static T op(bool inv, int s, T x, T a, T b) {
+        if (!inv) return s == 0 ? x - ((a + b) >> 1) : x + ((a + b + 2) >> 2);
+        return s == 0 ? x - ((a + b + 2) >> 2) : x + ((a + b) >> 1);
+    }
+};
+template <> struct KT<97> {
+    using T = float;
+    static constexpr int H = 4, NSTEP = 4;
+    __device__ static int par(bool inv, int s) { return inv ? (s & 1) : 1 - (s & 1); }
+    __device__ static T op(bool inv, int s, T x, T a, T b) {
+        float c;
+        if (!inv) c = s == 0 ? P1 : (s == 1 ? U1 : (s == 2 ? P2 : U2));
+        else c = s == 0 ? -U2 : (s == 1 ? -P2 : (s == 2 ? -U1 : -P1));
+        return __fadd_rn(x, __fmul_rn(c, __fadd_rn(a, b)));
+    }
+};
+
+__device__ __forceinline__ int32_t quantize(float v, float step) {
+    int32_t m = (int32_t)floorf(__fdiv_rn(fabsf(v), step));
+    return v < 0.0f ? -m : m;
+}
+__device__ __forceinline__ float dequantize(int32_t q, float step) {
+    int32_t m = q < 0 ? -q : q;
+    float r = m ? __fmul_rn(__fadd_rn((float)m, 0.5f), step) : 0.0f;
+    return q < 0 ? -r : r;
+}
+
+struct Steps4 { float ll, hl, lh, hh; };
+// element strides between consecutive images of a batch (blockIdx.z selects the image)
+struct ZStride { size_t src, dst, ll; };
+
+constexpr int FTW = 248, FNX = 256, STH = 16;
+
+// ---- transposed 9/7 steps -----------------------------------------------------------------------
+// A forward step updates parity p: x_i += c (x_m(i-1) + x_m(i+1)), m = symmetric mirror.  Its
+// transpose updates the other parity with the same coefficient from the neighbours weighted by
+// adj_w: 0 outside [0, n), 2 for the boundary samples 0 and n-1 (the mirrored references fold
+// back onto them), 1 elsewhere.  Sequences (step k: parity updated, coefficient):
+//   transpose of the forward (after the forward scaling): odd U2, even P2, odd U1, even P1
+//   transpose of the inverse (then the inverse scaling):  even -P1, odd -U1, even -P2, odd -U2
+__device__ __forceinline__ float adj_w(int k, int n) {
+    return (k < 0 || k >= n) ? 0.0f : ((k == 0 || k == n - 1) ? 2.0f : 1.0f);
+}
+template <bool FADJ>
+__device__ __forceinline__ constexpr float adj_coef(int k) {
+    return FADJ ? (k == 0 ? U2 : k == 1 ? P2 : k == 2 ? U1 : P1) : (k == 0 ? -P1 : k == 1 ? -U1 : k == 2 ? -P2 : -U2);
+}
+template <bool FADJ>
+__device__ __forceinline__ constexpr int adj_par(int k) {  // parity updated by step k
+    return FADJ ? ((k & 1) ? 0 : 1) : (k & 1);
+}
+__device__ __forceinline__ float adj_op(float c, float x, float a, float b) {
+    return __fadd_rn(x, __fmul_rn(c, __fadd_rn(a, b)));
+}
+
+// Horizontal steps of one strip row held as 8 consecutive samples per lane (v[j] at absolute
+// x = xs + j, xs even).  MODE 0: inverse 5/3 or 9/7 (scaling first); 1: transpose of the
+// forward 9/7 (forward scaling first); 2: transpose of the inverse 9/7 (inverse scaling last).
+// EDGE: apply the adjoint boundary weights (only tiles touching the image edge need them).
+template <int KERN, int MODE, bool EDGE>
+__device__ __forceinline__ void hlift8(typename KT<KERN>::T (&v)[8], int xs, int n) {
+    using T = typename KT<KERN>::T;
+    if constexpr (MODE == 0) {
+        if constexpr (KERN == 97) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = __fmul_rn(v[j], (j & 1) ? KDIV : KMUL);
+        }
+#pragma unroll
+        for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+            if ((k & 1) == 0) {  // even samples from their odd neighbours
+                const T pv = __shfl_up_sync(0xffffffffu, v[7], 1);
+                v[0] = KT<KERN>::op(true, k, v[0], pv, v[1]);
+                v[2] = KT<KERN>::op(true, k, v[2], v[1], v[3]);
+                v[4] = KT<KERN>::op(true, k, v[4], v[3], v[5]);
+                v[6] = KT<KERN>::op(true, k, v[6], v[5], v[7]);
+            } else {             // odd samples from their even neighbours
+                const T nx = __shfl_down_sync(0xffffffffu, v[0], 1);
+                v[1] = KT<KERN>::op(true, k, v[1], v[0], v[2]);
+                v[3] = KT<KERN>::op(true, k, v[3], v[2], v[4]);
+                v[5] = KT<KERN>::op(true, k, v[5], v[4], v[6]);
+                v[7] = KT<KERN>::op(true, k, v[7], v[6], nx);
+            }
+        }
+    } else {
+        constexpr bool FADJ = MODE == 1;
+        if constexpr (FADJ) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = __fmul_rn(v[j], (j & 1) ? KMUL : KDIV);
+        }
+        float wt[10];  // weights of absolute positions xs-1 .. xs+8
+        if constexpr (EDGE) {
+#pragma unroll
+            for (int j = 0; j < 10; ++j) wt[j] = adj_w(xs - 1 + j, n);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float c = adj_coef<FADJ>(k);
+            if (adj_par<FADJ>(k) == 0) {
+                float pv = __shfl_up_sync(0xffffffffu, v[7], 1);
+                if constexpr (EDGE) {
+#pragma unroll
+                    for (int j = 0; j < 8; j += 2) {
+                        const float a = __fmul_rn(j ? v[j - 1] : pv, wt[j]), b = __fmul_rn(v[j + 1], wt[j + 2]);
+                        v[j] = adj_op(c, v[j], a, b);
+                    }
+                } else {
+                    v[0] = adj_op(c, v[0], pv, v[1]);
+                    v[2] = adj_op(c, v[2], v[1], v[3]);
+                    v[4] = adj_op(c, v[4], v[3], v[5]);
+                    v[6] = adj_op(c, v[6], v[5], v[7]);
+                }
+            } else {
+                float nx = __shfl_down_sync(0xffffffffu, v[0], 1);
+                if constexpr (EDGE) {
+#pragma unroll
+                    for (int j = 1; j < 8; j += 2) {
+                        const float a = __fmul_rn(v[j - 1], wt[j]), b = __fmul_rn(j < 7 ? v[j + 1] : nx, wt[j + 2]);
+                        v[j] = adj_op(c, v[j], a, b);
+                    }
+                } else {
+                    v[1] = adj_op(c, v[1], v[0], v[2]);
+                    v[3] = adj_op(c, v[3], v[2], v[4]);
+                    v[5] = adj_op(c, v[5], v[4], v[6]);
+                    v[7] = adj_op(c, v[7], v[6], nx);
+                }
+            }
+        }
+        if constexpr (!FADJ) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = __fmul_rn(v[j], (j & 1) ? KDIV : KMUL);
+        }
+    }
+}
+
+// Vertical steps of one column held in registers (c[r] at absolute row ys + r, ys even).
+template <int KERN, int MODE, bool EDGE, int NY>
+__device__ __forceinline__ void vlift(typename KT<KERN>::T (&c)[NY], int ys, int n) {
+    if constexpr (MODE == 0) {
+        if constexpr (KERN == 97) {
+#pragma unroll
+            for (int r = 0; r < NY; ++r) c[r] = __fmul_rn(c[r], (r & 1) ? KDIV : KMUL);
+        }
+#pragma unroll
+        for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+#pragma unroll
+            for (int r = k + 1; r < NY - k - 1; ++r)
+                if ((r & 1) == (k & 1)) c[r] = KT<KERN>::op(true, k, c[r], c[r - 1], c[r + 1]);
+        }
+    } else {
+        constexpr bool FADJ = MODE == 1;
+        if constexpr (FADJ) {
+#pragma unroll
+            for (int r = 0; r < NY; ++r) c[r] = __fmul_rn(c[r], (r & 1) ? KMUL : KDIV);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float cf = adj_coef<FADJ>(k);
+#pragma unroll
+            for (int r = k + 1; r < NY - k - 1; ++r) {
+                if ((r & 1) != adj_par<FADJ>(k)) continue;
+                float a = c[r - 1], b = c[r + 1];
+                if constexpr (EDGE) {
+                    a = __fmul_rn(a, adj_w(ys + r - 1, n));
+                    b = __fmul_rn(b, adj_w(ys + r + 1, n));
+                }
+                c[r] = adj_op(cf, c[r], a, b);
+            }
+        }
+        if constexpr (!FADJ) {
+#pragma unroll
+            for (int r = 0; r < NY; ++r) c[r] = __fmul_rn(c[r], (r & 1) ? KDIV : KMUL);
+        }
+    }
+}
+
+// ---- synthesis strip kernel ---------------------------------------------------------------------
+// Reconstructs (MODE 0) or back-propagates through (MODE 1, 9/7 only) one level: the level's
+// detail bands sit at their Mallat positions in `src` (pitch spitch), its LL band in `ll_src`
+// (or in `src` itself when DEQLL), and the w x h natural-order result goes to `out`.
+//   MODE 0: symmetric extension by mirrored loads, inverse steps, bit-identical to dwt_inv_level;
+//           DEQ / DEQLL: the detail / LL samples are int32 dead-zone indices, dequantised on load.
+//   MODE 1: zero extension and adjoint boundary weights.
+// EXTRA 1 (MODE 0, float): out = result - sub, and the CTA's sum of out^2 goes to part[cta].
+// EXTRA 2 (MODE 1):        out = result - (*scale) * alpha * sub.
+struct SynExtra {
+    const float* sub;
+    size_t sub_pitch, sub_z;
+    const float* scale;
+    float alpha;
+    float* part;
+};
+
+template <int KERN, int MODE, typename TS, bool DEQ, bool DEQLL, int EXTRA>
+__global__ void __launch_bounds__(256)
+dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>::T* __restrict__ ll_src,
+             size_t llpitch, int w, int h, typename KT<KERN>::T* __restrict__ out, size_t opitch, Steps4 st,
+             ZStride z, int vec_in, SynExtra ex) {
+    using T = typename KT<KERN>::T;
+    constexpr int HV = KT<KERN>::H, NY = STH + 2 * HV;
+    __shared__ __align__(16) T s[NY][FNX];
+    src += blockIdx.z * z.src;
+    ll_src += blockIdx.z * z.ll;
+    out += blockIdx.z * z.dst;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
+    const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * STH;
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
+    // 1. natural-order strip: s[r][c] = level sample (y0 - HV + r, x0 - 4 + c)
+    for (int r = warp; r < NY; r += 8) {
+        int gy = y0 - HV + r;
+        if (MODE == 0) {
+            gy = mirror(gy, h);
+        } else if (gy < 0 || gy >= h) {
+#pragma unroll
+            for (int q2 = 0; q2 < 2; ++q2) *reinterpret_cast<uint4*>(&s[r][4 * (lane + 32 * q2)]) = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        const int qy = gy & 1;
+        const TS* srow = src + (size_t)((gy >> 1) + (qy ? hl : 0)) * spitch;
+        const T* lrow = ll_src + (size_t)(gy >> 1) * llpitch;
+        const bool low_ll = (qy == 0) && !DEQLL;  // low half from the separate LL buffer
+        const float sl = qy ? st.lh : st.ll, sh = qy ? st.hh : st.hl;
+        auto deq = [&](TS raw, float step) -> T {
+            if constexpr (DEQ) return (T)dequantize((int32_t)raw, step);
+            else return (T)raw;
+        };
+#pragma unroll
+        for (int q2 = 0; q2 < 2; ++q2) {
+            const int q = lane + 32 * q2;
+            const int gx = x0 - 4 + 4 * q;
+            T e[4];
+            if (inner_x && vec_in) {
+                const int lx = gx >> 1;
+                T lo[2];
+                if (low_ll) {
+                    *reinterpret_cast<uint2*>(lo) = __ldg(reinterpret_cast<const uint2*>(lrow + lx));
+                } else {
+                    TS raw[2];
+                    *reinterpret_cast<uint2*>(raw) = __ldg(reinterpret_cast<const uint2*>(srow + lx));
+                    lo[0] = deq(raw[0], sl);
+                    lo[1] = deq(raw[1], sl);
+                }
+                TS rh[2];
+                *reinterpret_cast<uint2*>(rh) = __ldg(reinterpret_cast<const uint2*>(srow + wl + lx));
+                e[0] = lo[0];
+                e[1] = deq(rh[0], sh);
+                e[2] = lo[1];
+                e[3] = deq(rh[1], sh);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    int gk = gx + k;
+                    if (MODE == 0) {
+                        gk = mirror(gk, w);
+                    } else if (gk < 0 || gk >= w) {
+                        e[k] = (T)0;
+                        continue;
+                    }
+                    const int i = gk >> 1;
+                    if (gk & 1) e[k] = deq(srow[wl + i], sh);
+                    else e[k] = low_ll ? lrow[i] : deq(srow[i], sl);
+                }
+            }
+            *reinterpret_cast<uint4*>(&s[r][4 * q]) = *reinterpret_cast<uint4*>(e);
+        }
+    }
+    __syncthreads();
+    // 2. horizontal steps on every strip row (the vertical pass needs the halo rows too)
+    if (w > 1) {
+        const int xs = x0 - 4 + 8 * lane;
+        const bool edge_x = !(x0 - 4 > 0 && x0 + 252 < w);
+        for (int r = warp; r < NY; r += 8) {
+            T v[8];
+            *reinterpret_cast<uint4*>(&v[0]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane]);
+            *reinterpret_cast<uint4*>(&v[4]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane + 4]);
+            if (MODE == 1 && edge_x) hlift8<KERN, MODE, true>(v, xs, w);
+            else hlift8<KERN, MODE, false>(v, xs, w);
+            *reinterpret_cast<uint4*>(&s[r][8 * lane]) = *reinterpret_cast<uint4*>(&v[0]);
+            *reinterpret_cast<uint4*>(&s[r][8 * lane + 4]) = *reinterpret_cast<uint4*>(&v[4]);
+        }
+    }
+    __syncthreads();
+    // 3. vertical steps, one column per thread, and the natural-order writes
+    T c[NY];
+#pragma unroll
+    for (int r = 0; r < NY; ++r) c[r] = s[r][t];
+    if (h > 1) {
+        const int ys = y0 - HV;
+        const bool edge_y = !(ys > 0 && y0 + STH + HV - 1 < h - 1);
+        if (MODE == 1 && edge_y) vlift<KERN, MODE, true, NY>(c, ys, h);
+        else vlift<KERN, MODE, false, NY>(c, ys, h);
+    }
+    const int x = x0 - 4 + t;
+    const bool colok = t >= 4 && t < 252 && x < w;
+    float sq = 0.0f;
+    float sc = 0.0f;
+    if constexpr (EXTRA == 2) sc = __fmul_rn(ex.scale ? *ex.scale : 1.0f, ex.alpha);
+    const float* sub = nullptr;
+    if constexpr (EXTRA != 0) sub = ex.sub + blockIdx.z * ex.sub_z;
+#pragma unroll
+    for (int j = 0; j < STH; ++j) {
+        const int y = y0 + j;
+        if (colok && y < h) {
+            T v = c[HV + j];
+            if constexpr (EXTRA == 1) {
+                v = __fsub_rn(v, sub[(size_t)y * ex.sub_pitch + x]);
+                sq = __fmaf_rn(v, v, sq);
+            } else if constexpr (EXTRA == 2) {
+                v = __fsub_rn(v, __fmul_rn(sc, sub[(size_t)y * ex.sub_pitch + x]));
+            }
+            out[(size_t)y * opitch + x] = v;
+        }
+    }
+    if constexpr (EXTRA == 1) {
+        __shared__ float red[8];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+        if (lane == 0) red[warp] = sq;
+        __syncthreads();
+        if (t == 0) {
+            float a = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a += red[i];
+            ex.part[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = a;
+        }
+    }
+}
+
+// ---- analysis strip kernel for the transpose of the inverse 9/7 ---------------------------------
+// Gradient of a reconstructed level (w x h natural order, `gin`) -> gradients of its subbands:
+// details at their Mallat positions in `gdst`, LL into `gll`.  Zero extension, adjoint
+// boundary weights; columns first, then rows (the inverse ran rows, then columns).
+__global__ void __launch_bounds__(256)
+iadj_ana_fast(const float* __restrict__ gin, size_t ipitch, int w, int h, float* __restrict__ gdst, size_t dpitch,
+              float* __restrict__ gll, size_t llpitch, ZStride z, int vec_in, int vec_out) {
+    constexpr int HV = 4, NY = STH + 2 * HV;
+    __shared__ __align__(16) float s[NY][FNX];
+    gin += blockIdx.z * z.src;
+    gdst += blockIdx.z * z.dst;
+    gll += blockIdx.z * z.ll;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
+    const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * STH;
+    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
+    for (int r = warp; r < NY; r += 8) {
+        const int gy = y0 - HV + r;
+        const bool rowok = gy >= 0 && gy < h;
+        const float* row = gin + (size_t)(rowok ? gy : 0) * ipitch;
+#pragma unroll
+        for (int q2 = 0; q2 < 2; ++q2) {
+            const int q = lane + 32 * q2;
+            const int gx = x0 - 4 + 4 * q;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (rowok) {
+                if (inner_x && vec_in) {
+                    v = __ldg(reinterpret_cast<const float4*>(row + gx));
+                } else {
+                    float e[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) e[k] = (gx + k >= 0 && gx + k < w) ? row[gx + k] : 0.0f;
+                    v = make_float4(e[0], e[1], e[2], e[3]);
+                }
+            }
+            *reinterpret_cast<float4*>(&s[r][4 * q]) = v;
+        }
+    }
+    __syncthreads();
+    if (h > 1) {
+        float c[NY];
+#pragma unroll
+        for (int r = 0; r < NY; ++r) c[r] = s[r][t];
+        const int ys = y0 - HV;
+        if (!(ys > 0 && y0 + STH + HV - 1 < h - 1)) vlift<97, 2, true, NY>(c, ys, h);
+        else vlift<97, 2, false, NY>(c, ys, h);
+#pragma unroll
+        for (int r = HV; r < HV + STH; ++r) s[r][t] = c[r];
+    }
+    __syncthreads();
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    const int xs = x0 - 4 + 8 * lane;
+    const bool edge_x = !(x0 - 4 > 0 && x0 + 252 < w);
+#pragma unroll
+    for (int i = 0; i < STH / 8; ++i) {
+        const int r = HV + warp + 8 * i;
+        const int y = y0 + r - HV;
+        if (y >= h) break;
+        float v[8];
+        *reinterpret_cast<float4*>(&v[0]) = *reinterpret_cast<const float4*>(&s[r][8 * lane]);
+        *reinterpret_cast<float4*>(&v[4]) = *reinterpret_cast<const float4*>(&s[r][8 * lane + 4]);
+        if (w > 1) {
+            if (edge_x) hlift8<97, 2, true>(v, xs, w);
+            else hlift8<97, 2, false>(v, xs, w);
+        }
+        const int qy = y & 1;
+        const int sy = (y >> 1) + (qy ? hl : 0);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int e0 = 8 * lane + 4 * half;
+            const int xa = xs + 4 * half;
+            if (e0 + 4 <= 4 || e0 >= 252) continue;  // halo columns
+#pragma unroll
+            for (int qx = 0; qx < 2; ++qx) {
+                const float a = v[4 * half + qx], b = v[4 * half + 2 + qx];
+                const int sx = (xa >> 1) + (qx ? wl : 0);
+                const bool va = xa + qx < w, vb = xa + 2 + qx < w;
+                float* p = (qx == 0 && qy == 0) ? gll + (size_t)sy * llpitch + sx : gdst + (size_t)sy * dpitch + sx;
+                if (vec_out && va && vb && ((sx & 1) == 0)) {
+                    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+                } else {
+                    if (va) p[0] = a;
+                    if (vb) p[1] = b;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace

@@ -1,14 +1,15 @@
 """Differentiable 9/7 for rate-distortion training (no counterpart in the reference).
 
-Three torch.autograd.Function bindings over the C ABI — the forward and inverse 9/7 DWT with
-their hand-written adjoints as backward, and the relaxed dead-zone quantiser (additive uniform
-noise of one step per subband) with its backward — and the loss they compose:
+torch.autograd.Function bindings over the C ABI — the forward and inverse 9/7 DWT with their
+hand-written adjoints as backward, the relaxed dead-zone quantiser (additive uniform noise of
+one step per subband) with its backward, and the fused rate-distortion loss
     loss = mean((IDWT(Q(DWT(x))) - x)^2) + lam * sum_b sum log2(1 + |y_hat|/step_b)
 differentiable with respect to the pixels x and the per-subband log steps.  torch provides the
-device memory, the stream and the elementwise MSE; the transforms, adjoints and quantiser run
-in libj2kb200's kernels.  No lifting intermediate is kept: the DWT is linear, so its backward
-needs only the incoming gradient; the quantiser keeps its input y (or recomputes it from x in
-the chunked form, which bounds memory when the batch does not fit in HBM).
+device memory and the stream; every pass runs in libj2kb200's kernels.  The fused loss keeps two
+planes per image for its backward: the quantiser input y and the residual d = IDWT(y_hat) - x
+(the reconstruction itself is never stored; the residual pass is fused into the last inverse
+level, and the "- 2/N d" term of the pixel gradient into the last forward-adjoint level).  The
+backward reads its output gradient on the device, so a step never synchronises with the host.
 """
 import ctypes as C
 
@@ -19,7 +20,10 @@ from . import _lib as L
 from ._lib import check, lib
 from .codec import default_context, subband_rects
 
-PARTS = 64  # partial sums per (image, band)
+
+def _parts(h):
+    """Row ranges per image of the quantiser kernels (one partial sum per band and range)."""
+    return max(1, min(int(h), 64))
 
 
 def _p(t):
@@ -70,8 +74,8 @@ def idwt97_adjoint(g, levels):
     return out
 
 
-def _band_sum(parts, n, nb):
-    return parts.view(n, nb, PARTS).sum(dim=2)
+def _band_sum(parts, n, nb, k):
+    return parts.view(n, nb, k).sum(dim=2)
 
 
 def relaxed_quant(y, log_steps, levels, seed):
@@ -79,24 +83,51 @@ def relaxed_quant(y, log_steps, levels, seed):
     ctx, h = _ctx(y)
     y = y.contiguous()
     n, hh, ww = y.shape
-    nb = 3 * levels + 1
+    nb, k = 3 * levels + 1, _parts(hh)
     ls = log_steps.detach().float().contiguous()
     yh = torch.empty_like(y)
-    parts = torch.empty(n * nb * PARTS, device=y.device, dtype=torch.float32)
-    check(lib().j2k_relaxed_quant_forward(h, _p(y), _p(yh), n, ww, hh, levels, _p(ls), seed, _p(parts), PARTS), h)
-    return yh, _band_sum(parts, n, nb)
+    parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+    check(lib().j2k_relaxed_quant_forward(h, _p(y), _p(yh), n, ww, hh, levels, _p(ls), seed, _p(parts), k), h)
+    return yh, _band_sum(parts, n, nb, k)
 
 
-def relaxed_quant_backward(y, g_yhat, log_steps, levels, seed, lam):
+def relaxed_quant_backward(y, g_yhat, log_steps, levels, seed, lam, scale=None, alpha=1.0):
+    """-> (dL/dy, dL/dlog_steps) for L = <g, y_hat> + lam * sum(rate), g = scale * alpha * g_yhat
+    (scale: optional 0-dim CUDA tensor, read on the device)."""
     ctx, h = _ctx(y)
     n, hh, ww = y.shape
-    nb = 3 * levels + 1
+    nb, k = 3 * levels + 1, _parts(hh)
     ls = log_steps.detach().float().contiguous()
     gy = torch.empty_like(y)
-    parts = torch.empty(n * nb * PARTS, device=y.device, dtype=torch.float32)
-    check(lib().j2k_relaxed_quant_backward(h, _p(y.contiguous()), _p(g_yhat.contiguous()), _p(gy), n, ww, hh,
-                                           levels, _p(ls), seed, float(lam), _p(parts), PARTS), h)
-    return gy, _band_sum(parts, n, nb).sum(dim=0)
+    parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+    sp = None if scale is None else _p(scale)
+    check(lib().j2k_relaxed_quant_backward_scaled(h, _p(y.contiguous()), _p(g_yhat.contiguous()), _p(gy), n, ww, hh,
+                                                  levels, _p(ls), seed, float(lam), sp, float(alpha), _p(parts), k),
+          h)
+    return gy, _band_sum(parts, n, nb, k).sum(dim=0)
+
+
+def inverse_residual(y, x, levels):
+    """-> (d = IDWT(y) - x, sum of d^2 as a 0-dim tensor), fused into the last inverse level."""
+    ctx, h = _ctx(y)
+    y, x = y.contiguous(), x.contiguous()
+    n, hh, ww = y.shape
+    d = torch.empty_like(y)
+    parts = torch.empty(lib().j2k_dwt97_residual_partials(ww, hh, n), device=y.device, dtype=torch.float32)
+    check(lib().j2k_dwt97_inverse_residual(h, _p(y), _p(x), _p(d), n, ww, hh, levels, _p(parts)), h)
+    return d, parts.sum()
+
+
+def forward_adjoint_residual(g, sub, levels, scale=None, alpha=1.0):
+    """-> DWT^T(g) - scale * alpha * sub, fused into the last adjoint level."""
+    ctx, h = _ctx(g)
+    g, sub = g.contiguous(), sub.contiguous()
+    n, hh, ww = g.shape
+    out = torch.empty_like(g)
+    sp = None if scale is None else _p(scale)
+    check(lib().j2k_dwt97_forward_adjoint_residual(h, _p(g), _p(sub), sp, float(alpha), _p(out), n, ww, hh, levels),
+          h)
+    return out
 
 
 class DWT97(torch.autograd.Function):
@@ -151,8 +182,43 @@ class RelaxedQuant(torch.autograd.Function):
         return gy, gls.to(log_steps.dtype), None, None
 
 
+class RDLoss(torch.autograd.Function):
+    """Fused rate-distortion loss of a (N, H, W) float32 batch (one 0-dim CUDA tensor).
+    Forward: DWT, quantiser, inverse with the residual fused in.  Backward: inverse adjoint of
+    the residual, quantiser backward (scaled by 2/N and the output gradient on the device),
+    forward adjoint with the -2/N residual fused in."""
+
+    @staticmethod
+    def forward(ctx, x, log_steps, levels, lam, seed):
+        x = x.detach().contiguous()
+        y = dwt97(x, levels)
+        yh, rate = relaxed_quant(y, log_steps, levels, seed)
+        d, sq = inverse_residual(yh, x, levels)
+        del yh
+        ctx.save_for_backward(y, d, log_steps)
+        ctx.levels, ctx.lam, ctx.seed = levels, lam, seed
+        return sq / x.numel() + lam * rate.sum()
+
+    @staticmethod
+    def backward(ctx, g):
+        y, d, log_steps = ctx.saved_tensors
+        g = g.detach().float().contiguous()
+        alpha = 2.0 / d.numel()
+        g_res = idwt97_adjoint(d, ctx.levels)
+        g_y, g_ls = relaxed_quant_backward(y, g_res, log_steps, ctx.levels, ctx.seed, ctx.lam, scale=g, alpha=alpha)
+        del g_res
+        gx = forward_adjoint_residual(g_y, d, ctx.levels, scale=g, alpha=alpha)
+        return gx, g_ls.to(log_steps.dtype), None, None, None
+
+
 def rd_loss(x, log_steps, levels=5, lam=0.01, seed=0):
     """Rate-distortion loss of a (N, H, W) float32 batch; differentiable in x and log_steps."""
+    return RDLoss.apply(x, log_steps, levels, lam, seed)
+
+
+def rd_loss_composed(x, log_steps, levels=5, lam=0.01, seed=0):
+    """The same loss composed from the separate autograd pieces (DWT97, RelaxedQuant, IDWT97
+    and torch's MSE); kept to check the fused form against."""
     y = DWT97.apply(x, levels)
     yh, rate = RelaxedQuant.apply(y, log_steps, levels, seed)
     xh = IDWT97.apply(yh, levels)
@@ -161,29 +227,25 @@ def rd_loss(x, log_steps, levels=5, lam=0.01, seed=0):
 
 def rd_loss_and_grads(x, log_steps, levels=5, lam=0.01, seed=0, chunk=None):
     """Loss and gradients computed chunk by chunk (images [i, i+chunk) at a time), so the peak
-    device memory is that of one chunk: the quantiser input is recomputed from the chunk's
-    pixels in the backward instead of being kept for the whole batch."""
+    device memory is that of one chunk (its coefficients and residual) when the whole batch
+    does not fit in HBM.  Returns (loss as a 0-dim tensor, dL/dx, dL/dlog_steps)."""
     n = x.shape[0]
     chunk = chunk or n
     total = float(x.numel())
+    alpha = 2.0 / total
     gx = torch.empty_like(x)
     gls = torch.zeros_like(log_steps, dtype=torch.float32)
-    loss = 0.0
+    loss = torch.zeros((), device=x.device, dtype=torch.float32)
     for i in range(0, n, chunk):
         xc = x[i:i + chunk].contiguous()
-        # forward
         y = dwt97(xc, levels)
         yh, rate = relaxed_quant(y, log_steps, levels, seed + i)
-        del y
-        xh = idwt97(yh, levels)
+        d, sq = inverse_residual(yh, xc, levels)
         del yh
-        d = xh - xc
-        loss += float((d * d).sum()) / total + lam * float(rate.sum())
-        # backward (recompute y from the chunk's pixels)
-        g_xh = (2.0 / total) * d
-        g_yh = idwt97_adjoint(g_xh, levels)
-        y = dwt97(xc, levels)
-        g_y, g_ls = relaxed_quant_backward(y, g_yh, log_steps, levels, seed + i, lam)
-        gx[i:i + chunk] = dwt97_adjoint(g_y, levels) - g_xh
+        loss += sq / total + lam * rate.sum()
+        g_res = idwt97_adjoint(d, levels)
+        g_y, g_ls = relaxed_quant_backward(y, g_res, log_steps, levels, seed + i, lam, alpha=alpha)
+        del g_res, y
+        gx[i:i + chunk] = forward_adjoint_residual(g_y, d, levels, alpha=alpha)
         gls += g_ls
     return loss, gx, gls

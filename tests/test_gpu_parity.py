@@ -222,6 +222,26 @@ def test_fast_level0_path_bit_exact(C, w, h, L, kern):
                               O.quantize(O.dwt97_fwd(x, L), L, st))
 
 
+@pytest.mark.parametrize("w,h,L", FAST_CASES + [(1024, 1024, 5), (517, 35, 4), (8, 2, 1)])
+@pytest.mark.parametrize("kern", [53, 97])
+def test_fast_inverse_path_bit_exact(C, w, h, L, kern):
+    """Levels at least 8 wide take the register-lifting synthesis kernel (T.800 order); it must
+    reproduce the oracle's inverse exactly, dequantising inverse included."""
+    rng = np.random.default_rng(w * 17 + h + kern)
+    if kern == 53:
+        x = rng.integers(-255, 256, (h, w)).astype(np.int32)
+        y = O.dwt53_fwd(x, L)
+        assert np.array_equal(C.dwt_inverse(dev(y), L, 53, 0).cpu().numpy(), O.dwt53_inv(y, L))
+    else:
+        x = rng.uniform(-128, 128, (h, w)).astype(np.float32)
+        y = O.dwt97_fwd(x, L)
+        assert np.array_equal(C.dwt_inverse(dev(y), L, 97, 0).cpu().numpy(), O.dwt97_inv(y, L))
+        st = O.default_steps(w, h, L)
+        q = O.quantize(y, L, st)
+        assert np.array_equal(C.dwt_inverse(dev(q), L, 97, 0, steps=st).cpu().numpy(),
+                              O.dwt97_inv(O.dequantize(q, L, st), L))
+
+
 BATCH_CASES = [(33, 17, 3), (248, 64, 2), (127, 131, 5), (64, 64, 6), (1, 9, 2), (300, 77, 4)]
 
 

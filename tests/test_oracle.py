@@ -164,3 +164,25 @@ def test_rct_ict_round_trip():
     assert np.array_equal(O.planar_inv(O.planar_fwd(img, O.MCT_RCT), O.MCT_RCT), img)
     back = O.planar_inv(O.planar_fwd(img, O.MCT_ICT, as_float=True), O.MCT_ICT)
     assert np.abs(back.astype(int) - img).max() <= 1
+
+
+def test_philox_known_answers_and_noise_layout():
+    """Philox4x32-10 against the published known-answer vectors of its authors (Random123), and
+    the relaxed quantiser's layout: one block per 4 samples of a row, word x % 4."""
+    import ctypes as C
+    L = O.lib()
+    L.or_philox4x32.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    kat = [((0, 0), (0, 0, 0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+           ((0xffffffff, 0xffffffff), (0xffffffff,) * 4, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+           ((0xa4093822, 0x299f31d0), (0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344),
+            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for key, ctr, want in kat:
+        c, o = (C.c_uint32 * 4)(*ctr), (C.c_uint32 * 4)()
+        L.or_philox4x32(key[0], key[1], c, o)
+        assert tuple(o) == want
+    seed, w = 12345, 10
+    for x, y in [(0, 0), (3, 0), (4, 0), (9, 2), (7, 5)]:
+        ctr = y * ((w + 3) // 4) + x // 4
+        c, o = (C.c_uint32 * 4)(ctr & 0xffffffff, ctr >> 32, 0, 0), (C.c_uint32 * 4)()
+        L.or_philox4x32(seed & 0xffffffff, seed >> 32, c, o)
+        assert O.rd_noise(seed, w, x, y) == (o[x % 4] >> 8) / 16777216.0 - 0.5
