@@ -89,6 +89,19 @@ def cpu_baseline(tile=1024, tiles=None):
                        f"tier-1+tier-2 with the C oracle, one process per core, wall {wall:.1f}s")
 
 
+def profiled_traffic(size):
+    """DRAM bytes (read + write) of one launch of the level-0 5/3 kernel as captured by ncu on
+    the same 4096x4096 plane (kept as a text summary under profiles/); None when absent or
+    for another size."""
+    path = os.path.join(ROOT, "profiles", "dwt_fwd_fast_53_level0_4096.txt")
+    if size != 4096 or not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return int(line.split(":")[1])
+    return None
+
+
 class L2Flush:
     """Writes a 256 MiB buffer (larger than the 126 MB L2) and then reads another one, so the
     next timed kernel starts with a cold L2 that holds no dirty lines of the flush itself."""
@@ -301,9 +314,9 @@ def main():
              "ms_per_step": round(ms_e2e, 4),
              "path": "OCLEncoder.run_rgb (j2k_encoder_run_interleaved, pinned host input) + "
                      "get_codeblocks (device pack + D2H)"},
-        roofline={"bound": "hbm", "kernel": "dwt_fwd_level<53,T800> level 0 (4096x4096 int32 plane)",
+        roofline={"bound": "hbm", "kernel": f"dwt_fwd_fast<53> level 0 ({size}x{size} int32 plane)",
                   "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                  "frac": round(achieved / hbm, 4), "traffic": None,
+                  "frac": round(achieved / hbm, 4), "traffic": profiled_traffic(size),
                   "algorithmic_bytes_per_launch": l0_bytes,
                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
         stages_ms={"planar_rct": round(t_planar, 4), "dwt_all_levels_3comp": round(t_dwt, 4),
@@ -317,6 +330,9 @@ def main():
         clocks=clocks,
         gpu_launches=int(args.steps * (1 + 3 * LEVELS + 2)),
     )
+    if world == 1 and size == W:
+        line["lossless_decode"] = bench_lossless_decode(img_h, res)
+        line["lossy"] = bench_lossy(img_h, img_d, flush)
     if args.batch_images and world == 1:
         line["batched"] = bench_batched(args.batch_images, flush)
     if args.diff and world == 1:
@@ -329,6 +345,65 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def bench_lossless_decode(img_h, res, reps=3):
+    """Config 1's round trip: decode the code-blocks of the timed lossless encode (host bytes in,
+    host pixels out, through OCLDecoder) and require the exact input back."""
+    import numpy as np
+    from roger_b200 import codec as C
+    descs, data = res[0], res[1].cpu().numpy() if hasattr(res[1], "cpu") else res[1]
+    h, w, nc = img_h.shape
+    dec = C.OCLDecoder(lossy=False)
+    out = dec.run(descs, data, w, h, nc, levels=LEVELS, cbw=CB, cbh=CB)
+    tt = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        dec.run(descs, data, w, h, nc, levels=LEVELS, cbw=CB, cbh=CB)
+        tt.append(time.perf_counter() - t0)
+    t = statistics.median(tt)
+    return {"workload": "decode of the lossless 4096x4096 RGB encode: tier-1 decode, inverse 5/3 (6 levels), "
+                        "inverse RCT, interleave; host code-block bytes in, host pixels out",
+            "bit_exact": bool(np.array_equal(out.reshape(img_h.shape), img_h)),
+            "ms": round(t * 1e3, 2), "mpix_s": round(w * h / 1e6 / t, 1)}
+
+
+def bench_lossy(img_h, img_d, flush, levels=6):
+    """Config 2: 4096x4096 RGB, ICT + 9/7 FP32 (6 levels) + dead-zone quantiser (step 8*2^-k at
+    level k) + tier-1; encode Mpix/s with the image resident, then decode and reconstruction
+    PSNR (the per-subband FP32-vs-FP64 coefficient error is a test: test_c2_fp64_error_per_subband)."""
+    import numpy as np
+    import torch
+    from roger_b200 import codec as C
+    h, w, nc = img_h.shape
+    enc = C.OCLEncoder(lossy=True)
+
+    def step():
+        enc.run_rgb(img_d, levels=levels, cbw=CB, cbh=CB)
+    for _ in range(2):
+        step()
+    tt = []
+    for _ in range(5):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        step()
+        e.record()
+        e.synchronize()
+        tt.append(s.elapsed_time(e))
+    ms = statistics.median(tt)
+    descs, data = enc.get_codeblocks()
+    data = data.cpu().numpy() if hasattr(data, "cpu") else data
+    rec = C.OCLDecoder(lossy=True).run(descs, data, w, h, nc, levels=levels, cbw=CB, cbh=CB)
+    err = rec.reshape(img_h.shape).astype(np.float64) - img_h.astype(np.float64)
+    mse = float((err * err).mean())
+    psnr = 10 * math.log10(255.0 ** 2 / mse) if mse > 0 else float("inf")
+    return {"workload": f"lossy encode {w}x{h} RGB: ICT + 9/7 FP32 L={levels} + dead-zone steps 8*2^-k + tier-1, "
+                        f"{CB}x{CB} code-blocks",
+            "ms_per_step": round(ms, 3), "mpix_s": round(w * h / 1e6 / (ms * 1e-3), 1),
+            "codeword_bytes": int(data.size if hasattr(data, "size") else len(data)),
+            "psnr_db": round(psnr, 3)}
 
 
 def bench_diff97(flush, hbm, n=16, size=1024, levels=5):

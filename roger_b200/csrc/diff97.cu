@@ -262,7 +262,7 @@ __device__ __forceinline__ int band_of(int dx, int dy, int L) {
 // x%4 for sample x.  Per-band sums are kept per thread in shared memory and reduced in a
 // fixed order, so the partials are deterministic.
 template <bool BWD>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, float* __restrict__ out, int w, int h,
                 size_t plane, Levels lv, const float* __restrict__ log_steps, uint64_t seed, float lam,
                 const float* __restrict__ gscale, float alpha, float* __restrict__ part, int rows, int vec) {
@@ -291,47 +291,65 @@ relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, floa
     const int groups = (w + 3) >> 2;
     const uint64_t key = seed + (uint64_t)img;
     const int r0 = blockIdx.x * rows, r1 = min(h, r0 + rows);
-    for (int yy = r0; yy < r1; ++yy) {
-        const int dy = depth_of(yy, hlim, L);
-        const size_t rb = (size_t)img * plane + (size_t)yy * w;
-        for (int g = t; g < groups; g += 256) {
-            const int x = 4 * g;
-            uint32_t o[4];
-            philox4(key, (uint64_t)yy * groups + g, o);
-            float v[4], gi[4] = {0.f, 0.f, 0.f, 0.f}, r[4];
-            if (vec && x + 4 <= w) {
-                *reinterpret_cast<float4*>(v) = __ldg(reinterpret_cast<const float4*>(y + rb + x));
-                if (BWD) *reinterpret_cast<float4*>(gi) = __ldg(reinterpret_cast<const float4*>(gin + rb + x));
-            } else {
+    const size_t ib = (size_t)img * plane;
+    constexpr int RB = BWD ? 2 : 4;  // rows per batch: all their loads are issued before any use
+    for (int g = t; g < groups; g += 256) {
+        const int x = 4 * g;
+        const bool full = vec && x + 4 <= w;
+        int dx[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dx[k] = depth_of(x + k, wlim, L);
+        for (int y0 = r0; y0 < r1; y0 += RB) {
+            float v[RB][4], gi[RB][4];
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+                const size_t rb = ib + (size_t)(y0 + i) * w + x;
+                if (y0 + i >= r1) break;
+                if (full) {
+                    *reinterpret_cast<float4*>(v[i]) = __ldg(reinterpret_cast<const float4*>(y + rb));
+                    if (BWD) *reinterpret_cast<float4*>(gi[i]) = __ldg(reinterpret_cast<const float4*>(gin + rb));
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        v[i][k] = x + k < w ? y[rb + k] : 0.0f;
+                        if (BWD) gi[i][k] = x + k < w ? gin[rb + k] : 0.0f;
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+                const int yy = y0 + i;
+                if (yy >= r1) break;
+                const int dy = depth_of(yy, hlim, L);
+                uint32_t o[4];
+                philox4(key, (uint64_t)yy * groups + g, o);
+                float r[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    v[k] = x + k < w ? y[rb + x + k] : 0.0f;
-                    if (BWD) gi[k] = x + k < w ? gin[rb + x + k] : 0.0f;
+                    r[k] = 0.0f;
+                    if (x + k >= w) continue;
+                    const int b = band_of(dx[k], dy, L);
+                    const float step = stp[b], rs = rstp[b], u = noise_of(o[k]);
+                    const float tt = __fadd_rn(__fmul_rn(v[i][k], rs), u);
+                    if (!BWD) {
+                        r[k] = __fmul_rn(tt, step);
+                        acc[b * 256 + t] += log1pf(fabsf(tt)) * inv_ln2;
+                    } else {
+                        const float sg = tt > 0.0f ? 1.0f : (tt < 0.0f ? -1.0f : 0.0f);
+                        const float drdt = __fdividef(lamG * inv_ln2 * sg, 1.0f + fabsf(tt));
+                        const float gg = __fmul_rn(G, gi[i][k]);
+                        r[k] = __fadd_rn(gg, __fmul_rn(drdt, rs));
+                        acc[b * 256 + t] += gg * u * step - drdt * v[i][k] * rs;
+                    }
                 }
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (x + k >= w) break;
-                const int b = band_of(depth_of(x + k, wlim, L), dy, L);
-                const float step = stp[b], rs = rstp[b], u = noise_of(o[k]);
-                const float tt = __fadd_rn(__fmul_rn(v[k], rs), u);
-                if (!BWD) {
-                    r[k] = __fmul_rn(tt, step);
-                    acc[b * 256 + t] += log1pf(fabsf(tt)) * inv_ln2;
+                const size_t rb = ib + (size_t)yy * w + x;
+                if (full) {
+                    *reinterpret_cast<float4*>(out + rb) = *reinterpret_cast<float4*>(r);
                 } else {
-                    const float sg = tt > 0.0f ? 1.0f : (tt < 0.0f ? -1.0f : 0.0f);
-                    const float drdt = __fdividef(lamG * inv_ln2 * sg, 1.0f + fabsf(tt));
-                    const float g = __fmul_rn(G, gi[k]);
-                    r[k] = __fadd_rn(g, __fmul_rn(drdt, rs));
-                    acc[b * 256 + t] += g * u * step - drdt * v[k] * rs;
-                }
-            }
-            if (vec && x + 4 <= w) {
-                *reinterpret_cast<float4*>(out + rb + x) = *reinterpret_cast<float4*>(r);
-            } else {
 #pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (x + k < w) out[rb + x + k] = r[k];
+                    for (int k = 0; k < 4; ++k)
+                        if (x + k < w) out[rb + k] = r[k];
+                }
             }
         }
     }

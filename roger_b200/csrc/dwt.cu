@@ -222,25 +222,22 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
     const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * FTH;
     const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
-    // 1. load the strip
+    // 1. load the strip: every copy of the CTA in flight at once (cp.async, no register staging)
     for (int r = warp; r < NY; r += 8) {
         const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
 #pragma unroll
         for (int q2 = 0; q2 < 2; ++q2) {
             const int q = lane + 32 * q2;
             const int gx = x0 - 4 + 4 * q;
-            uint4 v;
             if (inner_x) {
-                v = __ldg(reinterpret_cast<const uint4*>(row + gx));
+                cp_async16(&s[r][4 * q], row + gx);
             } else {
-                T e[4];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) e[k] = row[mirror(gx + k, w)];
-                v = *reinterpret_cast<uint4*>(e);
+                for (int k = 0; k < 4; ++k) cp_async4(&s[r][4 * q + k], row + mirror(gx + k, w));
             }
-            *reinterpret_cast<uint4*>(&s[r][4 * q]) = v;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
     // 2. vertical lifting of column t in registers
     if (h > 1) {
@@ -347,17 +344,6 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
 // (bands blockIdx.y, blockIdx.y + gridDim.y, ...) with two shared strips: while band i is
 // lifted, band i+1 streams into the other strip with cp.async (16-byte copies in the interior,
 // 4-byte mirrored copies at the image border), so loads are always in flight.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-
 template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
 __global__ void __launch_bounds__(256)
 dwt_fwd_pipe(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,

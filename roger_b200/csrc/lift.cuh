@@ -66,6 +66,23 @@ struct ZStride { size_t src, dst, ll; };
 
 constexpr int FTW = 248, FNX = 256, STH = 16;
 
+// asynchronous global -> shared copies (sm_80+ cp.async), waited for with cp_async_wait_all
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ---- transposed 9/7 steps -----------------------------------------------------------------------
 // A forward step updates parity p: x_i += c (x_m(i-1) + x_m(i+1)), m = symmetric mirror.  Its
 // transpose updates the other parity with the same coefficient from the neighbours weighted by
@@ -240,7 +257,9 @@ dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>:
     const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * STH;
     const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
     const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
-    // 1. natural-order strip: s[r][c] = level sample (y0 - HV + r, x0 - 4 + c)
+    // 1. stage the strip deinterleaved: row r holds the level's row y0 - HV + r (mirrored, or
+    //    zero outside the level for MODE 1) as s[r][j] = even sample x0 - 4 + 2j (low band) and
+    //    s[r][128 + j] = odd sample x0 - 3 + 2j (high band), j < 128, raw (not dequantised)
     for (int r = warp; r < NY; r += 8) {
         int gy = y0 - HV + r;
         if (MODE == 0) {
@@ -252,64 +271,76 @@ dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>:
         }
         const int qy = gy & 1;
         const TS* srow = src + (size_t)((gy >> 1) + (qy ? hl : 0)) * spitch;
-        const T* lrow = ll_src + (size_t)(gy >> 1) * llpitch;
-        const bool low_ll = (qy == 0) && !DEQLL;  // low half from the separate LL buffer
-        const float sl = qy ? st.lh : st.ll, sh = qy ? st.hh : st.hl;
-        auto deq = [&](TS raw, float step) -> T {
-            if constexpr (DEQ) return (T)dequantize((int32_t)raw, step);
-            else return (T)raw;
-        };
+        const void* lsrc = (qy == 0 && !DEQLL) ? (const void*)(ll_src + (size_t)(gy >> 1) * llpitch)
+                                               : (const void*)srow;  // low half: LL or LH row
+        const int lx0 = (x0 - 4) >> 1;
+        if (inner_x && vec_in) {
 #pragma unroll
-        for (int q2 = 0; q2 < 2; ++q2) {
-            const int q = lane + 32 * q2;
-            const int gx = x0 - 4 + 4 * q;
-            T e[4];
-            if (inner_x && vec_in) {
-                const int lx = gx >> 1;
-                T lo[2];
-                if (low_ll) {
-                    *reinterpret_cast<uint2*>(lo) = __ldg(reinterpret_cast<const uint2*>(lrow + lx));
-                } else {
-                    TS raw[2];
-                    *reinterpret_cast<uint2*>(raw) = __ldg(reinterpret_cast<const uint2*>(srow + lx));
-                    lo[0] = deq(raw[0], sl);
-                    lo[1] = deq(raw[1], sl);
-                }
-                TS rh[2];
-                *reinterpret_cast<uint2*>(rh) = __ldg(reinterpret_cast<const uint2*>(srow + wl + lx));
-                e[0] = lo[0];
-                e[1] = deq(rh[0], sh);
-                e[2] = lo[1];
-                e[3] = deq(rh[1], sh);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    int gk = gx + k;
-                    if (MODE == 0) {
-                        gk = mirror(gk, w);
-                    } else if (gk < 0 || gk >= w) {
-                        e[k] = (T)0;
-                        continue;
-                    }
-                    const int i = gk >> 1;
-                    if (gk & 1) e[k] = deq(srow[wl + i], sh);
-                    else e[k] = low_ll ? lrow[i] : deq(srow[i], sl);
-                }
+            for (int q2 = 0; q2 < 2; ++q2) {
+                const int j = 2 * (lane + 32 * q2);  // pairs of band samples, 8-byte copies
+                cp_async8(&s[r][j], (const uint32_t*)lsrc + lx0 + j);
+                cp_async8(&s[r][128 + j], srow + wl + lx0 + j);
             }
-            *reinterpret_cast<uint4*>(&s[r][4 * q]) = *reinterpret_cast<uint4*>(e);
+        } else {
+            for (int j = lane; j < 128; j += 32) {
+                int ge = x0 - 4 + 2 * j, go = ge + 1;
+                bool ze = false, zo = false;
+                if (MODE == 0) {
+                    ge = mirror(ge, w);
+                    go = mirror(go, w);
+                } else {
+                    ze = ge < 0 || ge >= w;
+                    zo = go < 0 || go >= w;
+                }
+                if (ze) s[r][j] = (T)0;
+                else cp_async4(&s[r][j], (const uint32_t*)lsrc + (ge >> 1));
+                if (zo) s[r][128 + j] = (T)0;
+                else cp_async4(&s[r][128 + j], srow + wl + (go >> 1));
+            }
         }
     }
+    // the residual operand of this thread's output column, fetched now so that its latency
+    // hides behind the lifting
+    float sb[EXTRA != 0 ? STH : 1];
+    if constexpr (EXTRA != 0) {
+        const float* sub = ex.sub + blockIdx.z * ex.sub_z;
+        const int x = x0 - 4 + t;
+        const bool colok = t >= 4 && t < 252 && x < w;
+#pragma unroll
+        for (int j = 0; j < STH; ++j)
+            sb[j] = (colok && y0 + j < h) ? __ldg(sub + (size_t)(y0 + j) * ex.sub_pitch + x) : 0.0f;
+    }
+    cp_async_wait_all();
     __syncthreads();
-    // 2. horizontal steps on every strip row (the vertical pass needs the halo rows too)
-    if (w > 1) {
+    // 2. horizontal steps on every strip row (the vertical pass needs the halo rows too), written
+    //    back in natural order: s[r][c] = sample x0 - 4 + c
+    {
         const int xs = x0 - 4 + 8 * lane;
         const bool edge_x = !(x0 - 4 > 0 && x0 + 252 < w);
         for (int r = warp; r < NY; r += 8) {
-            T v[8];
-            *reinterpret_cast<uint4*>(&v[0]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane]);
-            *reinterpret_cast<uint4*>(&v[4]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane + 4]);
-            if (MODE == 1 && edge_x) hlift8<KERN, MODE, true>(v, xs, w);
-            else hlift8<KERN, MODE, false>(v, xs, w);
+            T lo[4], hi[4], v[8];
+            *reinterpret_cast<uint4*>(lo) = *reinterpret_cast<const uint4*>(&s[r][4 * lane]);
+            *reinterpret_cast<uint4*>(hi) = *reinterpret_cast<const uint4*>(&s[r][128 + 4 * lane]);
+            if constexpr (DEQ) {
+                const int qy = r & 1;  // mirroring keeps the parity of y0 - HV + r
+                const float sl = qy ? st.lh : st.ll, sh = qy ? st.hh : st.hl;
+                const bool lo_raw = qy == 1 || DEQLL;  // LL rows hold floats unless DEQLL
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (lo_raw) lo[k] = (T)dequantize(__float_as_int(lo[k]), sl);
+                    hi[k] = (T)dequantize(__float_as_int(hi[k]), sh);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[2 * k] = lo[k];
+                v[2 * k + 1] = hi[k];
+            }
+            if (w > 1) {
+                if (MODE == 1 && edge_x) hlift8<KERN, MODE, true>(v, xs, w);
+                else hlift8<KERN, MODE, false>(v, xs, w);
+            }
+            __syncwarp();
             *reinterpret_cast<uint4*>(&s[r][8 * lane]) = *reinterpret_cast<uint4*>(&v[0]);
             *reinterpret_cast<uint4*>(&s[r][8 * lane + 4]) = *reinterpret_cast<uint4*>(&v[4]);
         }
@@ -330,18 +361,16 @@ dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>:
     float sq = 0.0f;
     float sc = 0.0f;
     if constexpr (EXTRA == 2) sc = __fmul_rn(ex.scale ? *ex.scale : 1.0f, ex.alpha);
-    const float* sub = nullptr;
-    if constexpr (EXTRA != 0) sub = ex.sub + blockIdx.z * ex.sub_z;
 #pragma unroll
     for (int j = 0; j < STH; ++j) {
         const int y = y0 + j;
         if (colok && y < h) {
             T v = c[HV + j];
             if constexpr (EXTRA == 1) {
-                v = __fsub_rn(v, sub[(size_t)y * ex.sub_pitch + x]);
+                v = __fsub_rn(v, sb[j]);
                 sq = __fmaf_rn(v, v, sq);
             } else if constexpr (EXTRA == 2) {
-                v = __fsub_rn(v, __fmul_rn(sc, sub[(size_t)y * ex.sub_pitch + x]));
+                v = __fsub_rn(v, __fmul_rn(sc, sb[j]));
             }
             out[(size_t)y * opitch + x] = v;
         }
@@ -384,20 +413,18 @@ iadj_ana_fast(const float* __restrict__ gin, size_t ipitch, int w, int h, float*
         for (int q2 = 0; q2 < 2; ++q2) {
             const int q = lane + 32 * q2;
             const int gx = x0 - 4 + 4 * q;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (rowok) {
-                if (inner_x && vec_in) {
-                    v = __ldg(reinterpret_cast<const float4*>(row + gx));
-                } else {
-                    float e[4];
+            if (rowok && inner_x && vec_in) {
+                cp_async16(&s[r][4 * q], row + gx);
+            } else {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) e[k] = (gx + k >= 0 && gx + k < w) ? row[gx + k] : 0.0f;
-                    v = make_float4(e[0], e[1], e[2], e[3]);
+                for (int k = 0; k < 4; ++k) {
+                    if (rowok && gx + k >= 0 && gx + k < w) cp_async4(&s[r][4 * q + k], row + gx + k);
+                    else s[r][4 * q + k] = 0.0f;
                 }
             }
-            *reinterpret_cast<float4*>(&s[r][4 * q]) = v;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
     if (h > 1) {
         float c[NY];

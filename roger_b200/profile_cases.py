@@ -1,0 +1,114 @@
+"""Small, self-contained GPU cases for profiling one kernel (or one step) under a profiler.
+
+    python -m roger_b200.profile_cases <case>
+
+Each case builds its inputs, runs the operation once untimed (so that allocations, scratch
+buffers and first-launch costs happen before the launch of interest) and then once more;
+profile the second run, e.g. ``ncu -k regex:dwt_fwd_fast -s 3 -c 1 ...``.  Sizes follow the
+benchmark workloads but stay within a few hundred MB of device memory:
+
+  planar       4096x4096 RGB uint8 -> 3 int32 planes with RCT (1 launch)
+  dwt53        level-0 5/3 forward of a 4096x4096 int32 plane (1 launch per run)
+  dwt53-all    6-level 5/3 forward of the same plane
+  idwt53       level-0 5/3 inverse of the same plane
+  tier1        EBCOT tier-1 of one 4096x4096 RCT component (6 levels, 4096 64x64 blocks)
+  encode       one whole lossless 4096x4096 RGB encode (planar, 3 x 6 DWT levels, tier-1)
+  diff-kernels one level-0 launch of every kernel of the differentiable 9/7 step on
+               16 x 1024x1024 float32 (forward, quantiser, inverse+residual, inverse adjoint,
+               quantiser backward, forward adjoint+residual)
+  diff-step    one fused rate-distortion step (5 levels, forward + backward)
+"""
+import math
+import sys
+
+import torch
+
+from . import codec as C
+from . import synth
+
+
+def _rgb(size=4096):
+    return torch.from_numpy(synth.rgb(size, size, (100, 101, 102, 103))).cuda()
+
+
+def case_planar():
+    img = _rgb()
+    return lambda: C.rgb_to_planar(img, 1)
+
+
+def case_dwt53(levels=1):
+    planes = C.rgb_to_planar(_rgb(), 1)
+    out = torch.empty_like(planes[0])
+    return lambda: C.dwt_forward(planes[0], levels, out=out)
+
+
+def case_idwt53():
+    planes = C.rgb_to_planar(_rgb(), 1)
+    coef = C.dwt_forward(planes[0], 1)
+    out = torch.empty_like(coef)
+    return lambda: C.dwt_inverse(coef, 1, out=out)
+
+
+def case_tier1():
+    planes = C.rgb_to_planar(_rgb(), 1)
+    coef = C.dwt_forward(planes[0], 6)
+    bpc = C.OCLBPC()
+    return lambda: bpc.run(coef, 6, 64, 64)
+
+
+def case_encode():
+    img = _rgb()
+    enc = C.OCLEncoder(lossy=False)
+    return lambda: enc.run_rgb(img, levels=6, cbw=64, cbh=64)
+
+
+def case_diff_kernels():
+    from . import diff97 as D
+    x = torch.from_numpy(synth.float_batch(16, 1024, 1024, 200)).cuda()
+    L = 1
+    ls = torch.full((3 * L + 1,), math.log(1 / 64.0), device="cuda")
+
+    def run():
+        y = D.dwt97(x, L)
+        yh, _ = D.relaxed_quant(y, ls, L, 200)
+        d, _ = D.inverse_residual(yh, x, L)
+        g = D.idwt97_adjoint(d, L)
+        gy, _ = D.relaxed_quant_backward(y, g, ls, L, 200, 0.01)
+        return D.forward_adjoint_residual(gy, d, L, alpha=1e-3)
+    return run
+
+
+def case_diff_step():
+    from . import diff97 as D
+    x = torch.from_numpy(synth.float_batch(16, 1024, 1024, 200)).cuda().requires_grad_(True)
+    L = 5
+    ls = torch.full((3 * L + 1,), math.log(1 / 64.0), device="cuda", requires_grad=True)
+
+    def run():
+        x.grad = None
+        ls.grad = None
+        D.rd_loss(x, ls, L, 0.01, 200).backward()
+    return run
+
+
+CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_dwt53(6),
+         "idwt53": case_idwt53, "tier1": case_tier1, "encode": case_encode,
+         "diff-kernels": case_diff_kernels, "diff-step": case_diff_step}
+
+
+def main(argv):
+    if len(argv) != 1 or argv[0] not in CASES:
+        print(__doc__)
+        print("cases:", ", ".join(CASES))
+        return 2
+    run = CASES[argv[0]]()
+    run()
+    torch.cuda.synchronize()
+    run()
+    torch.cuda.synchronize()
+    print("ok", argv[0])
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

@@ -268,3 +268,27 @@ def test_batched_dwt_matches_per_image(C, w, h, L, order):
         q = C.dwt_forward(dev(xf), L, 97, 0, steps=st).cpu().numpy()
         for i in range(n):
             assert np.array_equal(q[i], O.quantize(O.dwt97_fwd(xf[i], L), L, st))
+
+
+def test_c2_fp64_error_per_subband(C, capsys):
+    """Config 2 (4096x4096 RGB, ICT, 9/7 FP32, 6 levels): each subband's coefficient error
+    against the FP64 lifting oracle, relative to the subband's peak magnitude, for the three
+    components.  Bar: 1e-4; the table is printed (run with -s to see it)."""
+    img = synth.rgb(4096, 4096, (100, 101, 102, 103))
+    planes = C.rgb_to_planar(dev(img), 2, out_dtype=torch.float32)
+    L = 6
+    rows = []
+    worst = 0.0
+    for c in range(3):
+        got = C.dwt_forward(planes[c].contiguous(), L, 97, 0).cpu().numpy().astype(np.float64)
+        ref = O.dwt97_fwd(planes[c].cpu().numpy().astype(np.float64), L, f64=True)
+        for (x0, y0, sw, sh, o, lv) in O.subbands(4096, 4096, L):
+            a, b = got[y0:y0 + sh, x0:x0 + sw], ref[y0:y0 + sh, x0:x0 + sw]
+            e = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-12))
+            rows.append((c, lv, "LL HL LH HH".split()[o], e))
+            worst = max(worst, e)
+    with capsys.disabled():
+        print("\nC2 9/7 FP32 vs FP64, max |err| / max |coef| per subband (component, level, band):")
+        for c, lv, o, e in rows:
+            print(f"  c{c} L{lv} {o}: {e:.3e}")
+    assert worst <= 1e-4
