@@ -62,7 +62,9 @@ enum {
     J2K_TUNE_MQ_LANES = 1,   /* one-lane-per-block MQ kernel: blocks per warp (8, 16, 32) */
     J2K_TUNE_MQ_VARIANT = 2, /* 0: one lane per block (default); 1: state warp + code-register warp */
     J2K_TUNE_DWT_FAST_TH = 3, /* register-lifting forward DWT tile height: 16 (default), 32, 0 = off */
-    J2K_TUNE_DWT_PIPE = 4     /* 1: that kernel streams bands with cp.async double buffering (default 0) */
+    J2K_TUNE_DWT_PIPE = 4,    /* 1: that kernel streams bands with cp.async double buffering (default 0) */
+    J2K_TUNE_DWT_REG = 5      /* 1 (default): that kernel loads its columns straight into registers;
+                                 0: it stages the strip in shared memory with cp.async */
 };
 j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value);
 const char* j2k_status_string(j2k_status s);

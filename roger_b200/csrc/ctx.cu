@@ -249,6 +249,10 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->dwt_pipe = value != 0;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_DWT_REG) {
+        ctx->dwt_reg = value != 0;
+        return J2K_OK;
+    }
     return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown tuning key");
 }
 

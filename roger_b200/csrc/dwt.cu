@@ -208,8 +208,11 @@ dwt_fwd_batched(const j2k_dwt_level_desc* __restrict__ descs, const uint32_t* __
 //   * subbands are written straight from registers (8-byte vectors when aligned).
 // Same arithmetic, operation order and rounding as dwt_fwd_level, so the outputs are identical.
 
-template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
-__global__ void __launch_bounds__(256, (KERN == 53 && FTH == 16) ? 8 : 6)
+// REG: each thread loads its column of the strip straight from global memory into registers
+// (coalesced 4-byte loads, all NY in flight at once), so the strip is never staged in shared
+// memory; only the FTH vertically lifted rows go through shared memory to the horizontal pass.
+template <int KERN, typename TD, bool QUANT, bool QLL, int FTH, bool REG>
+__global__ void __launch_bounds__(256, REG ? (FTH == 16 ? 6 : 4) : ((KERN == 53 && FTH == 16) ? 8 : 6))
 dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
              typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
              Steps4 st, int vec_out, ZStride z) {
@@ -218,32 +221,46 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
     dst += blockIdx.z * z.dst;
     ll_dst += blockIdx.z * z.ll;
     constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
-    __shared__ __align__(16) T s[NY][FNX];
+    constexpr int SR = REG ? FTH : NY, RO = REG ? HV : 0;  // shared rows; strip row r at s[r - RO]
+    __shared__ __align__(16) T s[SR][FNX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
     const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * FTH;
     const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
-    // 1. load the strip: every copy of the CTA in flight at once (cp.async, no register staging)
-    for (int r = warp; r < NY; r += 8) {
-        const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
+    T c[NY];
+    if constexpr (REG) {
+        // 1. column t of the strip, rows y0-HV .. y0+FTH+HV-1 (mirrored at the image edges)
+        const bool inner_y = (y0 - HV >= 0) && (y0 + FTH + HV <= h);
+        const int gx = x0 - 4 + t;
+        const T* colp = src + (inner_x ? gx : mirror(gx, w));
 #pragma unroll
-        for (int q2 = 0; q2 < 2; ++q2) {
-            const int q = lane + 32 * q2;
-            const int gx = x0 - 4 + 4 * q;
-            if (inner_x) {
-                cp_async16(&s[r][4 * q], row + gx);
-            } else {
+        for (int r = 0; r < NY; ++r) {
+            const int gy = inner_y ? y0 - HV + r : mirror(y0 - HV + r, h);
+            c[r] = __ldg(colp + (size_t)gy * spitch);
+        }
+    } else {
+        // 1. load the strip: every copy of the CTA in flight at once (cp.async, no register staging)
+        for (int r = warp; r < NY; r += 8) {
+            const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) cp_async4(&s[r][4 * q + k], row + mirror(gx + k, w));
+            for (int q2 = 0; q2 < 2; ++q2) {
+                const int q = lane + 32 * q2;
+                const int gx = x0 - 4 + 4 * q;
+                if (inner_x) {
+                    cp_async16(&s[r][4 * q], row + gx);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) cp_async4(&s[r][4 * q + k], row + mirror(gx + k, w));
+                }
             }
         }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    // 2. vertical lifting of column t in registers
-    if (h > 1) {
-        T c[NY];
+        cp_async_wait_all();
+        __syncthreads();
 #pragma unroll
         for (int r = 0; r < NY; ++r) c[r] = s[r][t];
+        __syncthreads();
+    }
+    // 2. vertical lifting of column t in registers
+    if (h > 1) {
 #pragma unroll
         for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
             const int par = 1 - (k & 1);
@@ -251,12 +268,12 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
             for (int r = k + 1; r < NY - k - 1; ++r)
                 if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
         }
+    }
 #pragma unroll
-        for (int r = HV; r < HV + FTH; ++r) {
-            T v = c[r];
-            if (KERN == 97) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
-            s[r][t] = v;
-        }
+    for (int r = HV; r < HV + FTH; ++r) {
+        T v = c[r];
+        if (KERN == 97 && h > 1) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
+        s[r - RO][t] = v;
     }
     __syncthreads();
     // 3. horizontal lifting per row, 8 samples per lane (tile columns 8*lane .. 8*lane+7)
@@ -268,8 +285,8 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
         const int y = y0 + r - HV;
         if (y >= h) break;
         T v[8];
-        *reinterpret_cast<uint4*>(&v[0]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane]);
-        *reinterpret_cast<uint4*>(&v[4]) = *reinterpret_cast<const uint4*>(&s[r][8 * lane + 4]);
+        *reinterpret_cast<uint4*>(&v[0]) = *reinterpret_cast<const uint4*>(&s[r - RO][8 * lane]);
+        *reinterpret_cast<uint4*>(&v[4]) = *reinterpret_cast<const uint4*>(&s[r - RO][8 * lane + 4]);
         if (doh) {
 #pragma unroll
             for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
@@ -619,19 +636,18 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
             dim3 fg((cw + FTW - 1) / FTW, (chh + fth - 1) / fth, n);
             const int vec = (((uintptr_t)out & 7) == 0) && ((out_pitch & 1) == 0) &&
                             (((uintptr_t)lld & 7) == 0) && ((llp & 1) == 0);
-#define FAST(TH_)                                                                                        \
+#define FAST(TH_, REG_)                                                                                  \
     do {                                                                                                 \
         if (quant) {                                                                                     \
             if (last)                                                                                    \
-                dwt_fwd_fast<KERN, int32_t, true, true, TH_><<<fg, 256, 0, stream>>>(                    \
+                dwt_fwd_fast<KERN, int32_t, true, true, TH_, REG_><<<fg, 256, 0, stream>>>(              \
                     src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs);             \
             else                                                                                         \
-                dwt_fwd_fast<KERN, int32_t, true, false, TH_><<<fg, 256, 0, stream>>>(                   \
+                dwt_fwd_fast<KERN, int32_t, true, false, TH_, REG_><<<fg, 256, 0, stream>>>(             \
                     src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs);             \
         } else {                                                                                         \
-            dwt_fwd_fast<KERN, T, false, false, TH_><<<fg, 256, 0, stream>>>(src, spitch, cw, chh, lld, \
-                                                                              llp, (T*)out, out_pitch,   \
-                                                                              st, vec, zs);              \
+            dwt_fwd_fast<KERN, T, false, false, TH_, REG_><<<fg, 256, 0, stream>>>(                      \
+                src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, vec, zs);                        \
         }                                                                                                \
     } while (0)
             if (ctx && ctx->dwt_pipe && n == 1) {
@@ -650,7 +666,11 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
                     dwt_fwd_pipe<KERN, T, false, false, 16><<<pg, 256, 0, stream>>>(
                         src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, vec, bands);
                 }
-            } else if (fth == 16) FAST(16); else FAST(32);
+            } else if (ctx && !ctx->dwt_reg) {
+                if (fth == 16) FAST(16, false); else FAST(32, false);
+            } else {
+                if (fth == 16) FAST(16, true); else FAST(32, true);
+            }
 #undef FAST
         } else if (quant) {
             if (last)

@@ -36,6 +36,7 @@ struct j2k_ctx {
     int mq_variant = 0;          // 0: one lane per block, 1: state warp + code warp pair
     int dwt_fast_th = 16;        // fast level-0 DWT tile height (16, 32; 0 = off)
     int dwt_pipe = 0;            // fast level-0 DWT: persistent cp.async double-buffered variant
+    int dwt_reg = 1;             // fast forward DWT: columns loaded straight into registers (0: cp.async strip)
 };
 
 // scratch slot ids

@@ -60,6 +60,12 @@ __device__ __forceinline__ float dequantize(int32_t q, float step) {
     return q < 0 ? -r : r;
 }
 
+template <typename T>
+__device__ __forceinline__ T bits_as(uint32_t u) {
+    if constexpr (sizeof(T) == 4 && T(0.5f) != T(0)) return __uint_as_float(u);
+    else return (T)(int32_t)u;
+}
+
 struct Steps4 { float ll, hl, lh, hh; };
 // element strides between consecutive images of a batch (blockIdx.z selects the image)
 struct ZStride { size_t src, dst, ll; };
@@ -257,49 +263,7 @@ dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>:
     const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * STH;
     const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
     const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
-    // 1. stage the strip deinterleaved: row r holds the level's row y0 - HV + r (mirrored, or
-    //    zero outside the level for MODE 1) as s[r][j] = even sample x0 - 4 + 2j (low band) and
-    //    s[r][128 + j] = odd sample x0 - 3 + 2j (high band), j < 128, raw (not dequantised)
-    for (int r = warp; r < NY; r += 8) {
-        int gy = y0 - HV + r;
-        if (MODE == 0) {
-            gy = mirror(gy, h);
-        } else if (gy < 0 || gy >= h) {
-#pragma unroll
-            for (int q2 = 0; q2 < 2; ++q2) *reinterpret_cast<uint4*>(&s[r][4 * (lane + 32 * q2)]) = make_uint4(0, 0, 0, 0);
-            continue;
-        }
-        const int qy = gy & 1;
-        const TS* srow = src + (size_t)((gy >> 1) + (qy ? hl : 0)) * spitch;
-        const void* lsrc = (qy == 0 && !DEQLL) ? (const void*)(ll_src + (size_t)(gy >> 1) * llpitch)
-                                               : (const void*)srow;  // low half: LL or LH row
-        const int lx0 = (x0 - 4) >> 1;
-        if (inner_x && vec_in) {
-#pragma unroll
-            for (int q2 = 0; q2 < 2; ++q2) {
-                const int j = 2 * (lane + 32 * q2);  // pairs of band samples, 8-byte copies
-                cp_async8(&s[r][j], (const uint32_t*)lsrc + lx0 + j);
-                cp_async8(&s[r][128 + j], srow + wl + lx0 + j);
-            }
-        } else {
-            for (int j = lane; j < 128; j += 32) {
-                int ge = x0 - 4 + 2 * j, go = ge + 1;
-                bool ze = false, zo = false;
-                if (MODE == 0) {
-                    ge = mirror(ge, w);
-                    go = mirror(go, w);
-                } else {
-                    ze = ge < 0 || ge >= w;
-                    zo = go < 0 || go >= w;
-                }
-                if (ze) s[r][j] = (T)0;
-                else cp_async4(&s[r][j], (const uint32_t*)lsrc + (ge >> 1));
-                if (zo) s[r][128 + j] = (T)0;
-                else cp_async4(&s[r][128 + j], srow + wl + (go >> 1));
-            }
-        }
-    }
-    // the residual operand of this thread's output column, fetched now so that its latency
+    // the residual operand of this thread's output column, fetched first so that its latency
     // hides behind the lifting
     float sb[EXTRA != 0 ? STH : 1];
     if constexpr (EXTRA != 0) {
@@ -310,37 +274,74 @@ dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>:
         for (int j = 0; j < STH; ++j)
             sb[j] = (colok && y0 + j < h) ? __ldg(sub + (size_t)(y0 + j) * ex.sub_pitch + x) : 0.0f;
     }
-    cp_async_wait_all();
-    __syncthreads();
+    // 1. the strip's rows y0 - HV + r (mirrored, or zero outside the level for MODE 1), warp w
+    //    taking rows w, w + 8, ...: lane l loads the band samples of natural columns
+    //    x0 - 4 + 8l .. + 7 straight into registers (low band: LL or LH row, high band: HL or
+    //    HH row), raw; all rows' loads are issued before any is used
+    constexpr int RI = (NY + 7) / 8;
+    uint32_t rl[RI][4], rh[RI][4];
+    const int lx = ((x0 - 4) >> 1) + 4 * lane;  // band index of this lane's first low sample
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+        const int r = warp + 8 * i;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) rl[i][k] = rh[i][k] = 0u;
+        if (r >= NY) continue;
+        int gy = y0 - HV + r;
+        if (MODE == 0) gy = mirror(gy, h);
+        else if (gy < 0 || gy >= h) continue;
+        const int qy = gy & 1;
+        const uint32_t* srow = reinterpret_cast<const uint32_t*>(src + (size_t)((gy >> 1) + (qy ? hl : 0)) * spitch);
+        const uint32_t* lsrc = (qy == 0 && !DEQLL)
+                                   ? reinterpret_cast<const uint32_t*>(ll_src + (size_t)(gy >> 1) * llpitch)
+                                   : srow;
+        if (inner_x && vec_in) {
+            const uint2 l0 = __ldg(reinterpret_cast<const uint2*>(lsrc + lx));
+            const uint2 l1 = __ldg(reinterpret_cast<const uint2*>(lsrc + lx + 2));
+            const uint2 h0 = __ldg(reinterpret_cast<const uint2*>(srow + wl + lx));
+            const uint2 h1 = __ldg(reinterpret_cast<const uint2*>(srow + wl + lx + 2));
+            rl[i][0] = l0.x; rl[i][1] = l0.y; rl[i][2] = l1.x; rl[i][3] = l1.y;
+            rh[i][0] = h0.x; rh[i][1] = h0.y; rh[i][2] = h1.x; rh[i][3] = h1.y;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                int ge = x0 - 4 + 8 * lane + 2 * k, go = ge + 1;
+                if (MODE == 0) {
+                    ge = mirror(ge, w);
+                    go = mirror(go, w);
+                }
+                if (ge >= 0 && ge < w) rl[i][k] = __ldg(lsrc + (ge >> 1));
+                if (go >= 0 && go < w) rh[i][k] = __ldg(srow + wl + (go >> 1));
+            }
+        }
+    }
     // 2. horizontal steps on every strip row (the vertical pass needs the halo rows too), written
-    //    back in natural order: s[r][c] = sample x0 - 4 + c
+    //    in natural order: s[r][c] = sample x0 - 4 + c
     {
         const int xs = x0 - 4 + 8 * lane;
         const bool edge_x = !(x0 - 4 > 0 && x0 + 252 < w);
-        for (int r = warp; r < NY; r += 8) {
-            T lo[4], hi[4], v[8];
-            *reinterpret_cast<uint4*>(lo) = *reinterpret_cast<const uint4*>(&s[r][4 * lane]);
-            *reinterpret_cast<uint4*>(hi) = *reinterpret_cast<const uint4*>(&s[r][128 + 4 * lane]);
-            if constexpr (DEQ) {
-                const int qy = r & 1;  // mirroring keeps the parity of y0 - HV + r
-                const float sl = qy ? st.lh : st.ll, sh = qy ? st.hh : st.hl;
-                const bool lo_raw = qy == 1 || DEQLL;  // LL rows hold floats unless DEQLL
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (lo_raw) lo[k] = (T)dequantize(__float_as_int(lo[k]), sl);
-                    hi[k] = (T)dequantize(__float_as_int(hi[k]), sh);
-                }
-            }
+        for (int i = 0; i < RI; ++i) {
+            const int r = warp + 8 * i;
+            if (r >= NY) break;
+            T v[8];
+            const int qy = r & 1;  // mirroring keeps the parity of y0 - HV + r
+            const float sl = qy ? st.lh : st.ll, sh = qy ? st.hh : st.hl;
+            const bool lo_raw = qy == 1 || DEQLL;  // LL rows hold values unless DEQLL
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                v[2 * k] = lo[k];
-                v[2 * k + 1] = hi[k];
+                if constexpr (DEQ) {
+                    v[2 * k] = lo_raw ? (T)dequantize((int32_t)rl[i][k], sl) : bits_as<T>(rl[i][k]);
+                    v[2 * k + 1] = (T)dequantize((int32_t)rh[i][k], sh);
+                } else {
+                    v[2 * k] = bits_as<T>(rl[i][k]);
+                    v[2 * k + 1] = bits_as<T>(rh[i][k]);
+                }
             }
             if (w > 1) {
                 if (MODE == 1 && edge_x) hlift8<KERN, MODE, true>(v, xs, w);
                 else hlift8<KERN, MODE, false>(v, xs, w);
             }
-            __syncwarp();
             *reinterpret_cast<uint4*>(&s[r][8 * lane]) = *reinterpret_cast<uint4*>(&v[0]);
             *reinterpret_cast<uint4*>(&s[r][8 * lane + 4]) = *reinterpret_cast<uint4*>(&v[4]);
         }
@@ -398,44 +399,32 @@ __global__ void __launch_bounds__(256)
 iadj_ana_fast(const float* __restrict__ gin, size_t ipitch, int w, int h, float* __restrict__ gdst, size_t dpitch,
               float* __restrict__ gll, size_t llpitch, ZStride z, int vec_in, int vec_out) {
     constexpr int HV = 4, NY = STH + 2 * HV;
-    __shared__ __align__(16) float s[NY][FNX];
+    __shared__ __align__(16) float s[STH][FNX];  // the vertically lifted rows y0 .. y0+STH-1
     gin += blockIdx.z * z.src;
     gdst += blockIdx.z * z.dst;
     gll += blockIdx.z * z.ll;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
     const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * STH;
-    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
-    for (int r = warp; r < NY; r += 8) {
-        const int gy = y0 - HV + r;
-        const bool rowok = gy >= 0 && gy < h;
-        const float* row = gin + (size_t)(rowok ? gy : 0) * ipitch;
+    (void)vec_in;
+    // column t of the strip straight into registers (zero outside the level)
+    float c[NY];
+    {
+        const int gx = x0 - 4 + t;
+        const bool colok = gx >= 0 && gx < w;
+        const float* colp = gin + (colok ? gx : 0);
 #pragma unroll
-        for (int q2 = 0; q2 < 2; ++q2) {
-            const int q = lane + 32 * q2;
-            const int gx = x0 - 4 + 4 * q;
-            if (rowok && inner_x && vec_in) {
-                cp_async16(&s[r][4 * q], row + gx);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (rowok && gx + k >= 0 && gx + k < w) cp_async4(&s[r][4 * q + k], row + gx + k);
-                    else s[r][4 * q + k] = 0.0f;
-                }
-            }
+        for (int r = 0; r < NY; ++r) {
+            const int gy = y0 - HV + r;
+            c[r] = (colok && gy >= 0 && gy < h) ? __ldg(colp + (size_t)gy * ipitch) : 0.0f;
         }
     }
-    cp_async_wait_all();
-    __syncthreads();
     if (h > 1) {
-        float c[NY];
-#pragma unroll
-        for (int r = 0; r < NY; ++r) c[r] = s[r][t];
         const int ys = y0 - HV;
         if (!(ys > 0 && y0 + STH + HV - 1 < h - 1)) vlift<97, 2, true, NY>(c, ys, h);
         else vlift<97, 2, false, NY>(c, ys, h);
-#pragma unroll
-        for (int r = HV; r < HV + STH; ++r) s[r][t] = c[r];
     }
+#pragma unroll
+    for (int r = HV; r < HV + STH; ++r) s[r - HV][t] = c[r];
     __syncthreads();
     const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
     const int xs = x0 - 4 + 8 * lane;
@@ -446,8 +435,8 @@ iadj_ana_fast(const float* __restrict__ gin, size_t ipitch, int w, int h, float*
         const int y = y0 + r - HV;
         if (y >= h) break;
         float v[8];
-        *reinterpret_cast<float4*>(&v[0]) = *reinterpret_cast<const float4*>(&s[r][8 * lane]);
-        *reinterpret_cast<float4*>(&v[4]) = *reinterpret_cast<const float4*>(&s[r][8 * lane + 4]);
+        *reinterpret_cast<float4*>(&v[0]) = *reinterpret_cast<const float4*>(&s[r - HV][8 * lane]);
+        *reinterpret_cast<float4*>(&v[4]) = *reinterpret_cast<const float4*>(&s[r - HV][8 * lane + 4]);
         if (w > 1) {
             if (edge_x) hlift8<97, 2, true>(v, xs, w);
             else hlift8<97, 2, false>(v, xs, w);
