@@ -232,13 +232,19 @@ j2k_status j2k_relaxed_quant_forward(j2k_ctx* ctx, const float* y, float* y_hat,
 j2k_status j2k_relaxed_quant_backward(j2k_ctx* ctx, const float* y, const float* g_yhat, float* g_y, int n,
                                       size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
                                       float lam, float* g_logstep_partials, int parts_per_band);
-/* Same, with the incoming gradient scaled on the device: g_yhat = (*scale) * alpha * g_in and the
+/* Forward that also writes every sample's noise u to `noise` (n*w*h floats), for a backward that
+ * then reads it instead of regenerating it. */
+j2k_status j2k_relaxed_quant_forward_noise(j2k_ctx* ctx, const float* y, float* y_hat, float* noise, int n, size_t w,
+                                           size_t h, int levels, const float* log_steps, uint64_t seed,
+                                           float* rate_partials, int parts_per_band);
+/* Backward with the incoming gradient scaled on the device: g_yhat = (*scale) * alpha * g_in and the
  * rate weight (*scale) * lam (scale: device pointer to one float, NULL = 1), so that an autograd
- * backward can pass its output gradient without reading it on the host. */
+ * backward can pass its output gradient without reading it on the host.  noise: the forward's
+ * noise (j2k_relaxed_quant_forward_noise), or NULL to regenerate it from seed. */
 j2k_status j2k_relaxed_quant_backward_scaled(j2k_ctx* ctx, const float* y, const float* g_in, float* g_y, int n,
                                              size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
-                                             float lam, const float* scale, float alpha, float* g_logstep_partials,
-                                             int parts_per_band);
+                                             const float* noise, float lam, const float* scale, float alpha,
+                                             float* g_logstep_partials, int parts_per_band);
 /* Fused residual forms for a distortion term mean((IDWT(y) - x)^2):
  * j2k_dwt97_inverse_residual writes d = IDWT(y) - x (the reconstruction itself is never stored)
  * and one partial sum of d^2 per 248 x 16 tile of the finest level, j2k_dwt97_residual_partials

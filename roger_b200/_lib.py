@@ -79,7 +79,8 @@ SIGS = {
     "j2k_dwt97_inverse_adjoint": (I, [P, P, P, I, S, S, I]),
     "j2k_relaxed_quant_forward": (I, [P, P, P, I, S, S, I, P, C.c_uint64, P, I]),
     "j2k_relaxed_quant_backward": (I, [P, P, P, P, I, S, S, I, P, C.c_uint64, C.c_float, P, I]),
-    "j2k_relaxed_quant_backward_scaled": (I, [P, P, P, P, I, S, S, I, P, C.c_uint64, C.c_float, P, C.c_float,
+    "j2k_relaxed_quant_forward_noise": (I, [P, P, P, P, I, S, S, I, P, C.c_uint64, P, I]),
+    "j2k_relaxed_quant_backward_scaled": (I, [P, P, P, P, I, S, S, I, P, C.c_uint64, P, C.c_float, P, C.c_float,
                                               P, I]),
     "j2k_dwt97_residual_partials": (S, [S, S, I]),
     "j2k_dwt97_inverse_residual": (I, [P, P, P, P, I, S, S, I, P]),

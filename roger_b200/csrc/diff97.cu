@@ -261,11 +261,14 @@ __device__ __forceinline__ int band_of(int dx, int dy, int L) {
 // Noise: one Philox4x32-10 call per group (key seed + image, counter y*ceil(w/4) + x/4), word
 // x%4 for sample x.  Per-band sums are kept per thread in shared memory and reduced in a
 // fixed order, so the partials are deterministic.
-template <bool BWD>
+// NZ: the forward also writes the noise u of every sample to nz, and the backward reads it from
+// there instead of regenerating it.
+template <bool BWD, bool NZ>
 __global__ void __launch_bounds__(256, 3)
 relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, float* __restrict__ out, int w, int h,
                 size_t plane, Levels lv, const float* __restrict__ log_steps, uint64_t seed, float lam,
-                const float* __restrict__ gscale, float alpha, float* __restrict__ part, int rows, int vec) {
+                const float* __restrict__ gscale, float alpha, float* __restrict__ part, int rows, int vec,
+                float* __restrict__ nz) {
     extern __shared__ float acc[];  // [band][256]
     __shared__ float stp[49], rstp[49];
     __shared__ int wlim[17], hlim[17];
@@ -300,7 +303,7 @@ relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, floa
 #pragma unroll
         for (int k = 0; k < 4; ++k) dx[k] = depth_of(x + k, wlim, L);
         for (int y0 = r0; y0 < r1; y0 += RB) {
-            float v[RB][4], gi[RB][4];
+            float v[RB][4], gi[RB][4], un[RB][4];
 #pragma unroll
             for (int i = 0; i < RB; ++i) {
                 const size_t rb = ib + (size_t)(y0 + i) * w + x;
@@ -308,11 +311,13 @@ relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, floa
                 if (full) {
                     *reinterpret_cast<float4*>(v[i]) = __ldg(reinterpret_cast<const float4*>(y + rb));
                     if (BWD) *reinterpret_cast<float4*>(gi[i]) = __ldg(reinterpret_cast<const float4*>(gin + rb));
+                    if (BWD && NZ) *reinterpret_cast<float4*>(un[i]) = __ldg(reinterpret_cast<const float4*>(nz + rb));
                 } else {
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         v[i][k] = x + k < w ? y[rb + k] : 0.0f;
                         if (BWD) gi[i][k] = x + k < w ? gin[rb + k] : 0.0f;
+                        if (BWD && NZ) un[i][k] = x + k < w ? nz[rb + k] : 0.0f;
                     }
                 }
             }
@@ -321,19 +326,20 @@ relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, floa
                 const int yy = y0 + i;
                 if (yy >= r1) break;
                 const int dy = depth_of(yy, hlim, L);
-                uint32_t o[4];
-                philox4(key, (uint64_t)yy * groups + g, o);
-                float r[4];
+                uint32_t o[4] = {0u, 0u, 0u, 0u};
+                if (!(BWD && NZ)) philox4(key, (uint64_t)yy * groups + g, o);
+                float r[4], uo[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     r[k] = 0.0f;
                     if (x + k >= w) continue;
                     const int b = band_of(dx[k], dy, L);
-                    const float step = stp[b], rs = rstp[b], u = noise_of(o[k]);
+                    const float step = stp[b], rs = rstp[b], u = (BWD && NZ) ? un[i][k] : noise_of(o[k]);
+                    uo[k] = u;
                     const float tt = __fadd_rn(__fmul_rn(v[i][k], rs), u);
                     if (!BWD) {
                         r[k] = __fmul_rn(tt, step);
-                        acc[b * 256 + t] += log1pf(fabsf(tt)) * inv_ln2;
+                        acc[b * 256 + t] += __log2f(__fadd_rn(1.0f, fabsf(tt)));
                     } else {
                         const float sg = tt > 0.0f ? 1.0f : (tt < 0.0f ? -1.0f : 0.0f);
                         const float drdt = __fdividef(lamG * inv_ln2 * sg, 1.0f + fabsf(tt));
@@ -345,10 +351,14 @@ relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, floa
                 const size_t rb = ib + (size_t)yy * w + x;
                 if (full) {
                     *reinterpret_cast<float4*>(out + rb) = *reinterpret_cast<float4*>(r);
+                    if (!BWD && NZ) *reinterpret_cast<float4*>(nz + rb) = *reinterpret_cast<float4*>(uo);
                 } else {
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
-                        if (x + k < w) out[rb + k] = r[k];
+                        if (x + k < w) {
+                            out[rb + k] = r[k];
+                            if (!BWD && NZ) nz[rb + k] = uo[k];
+                        }
                 }
             }
         }
@@ -444,7 +454,7 @@ j2k_status fwd_adj_run(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, s
 
 j2k_status quant_run(j2k_ctx* ctx, bool bwd, const float* y, const float* gin, float* out, int n, size_t w,
                      size_t h, int levels, const float* log_steps, uint64_t seed, float lam, const float* gscale,
-                     float alpha, float* partials, int parts) {
+                     float alpha, float* partials, int parts, float* noise) {
     J2K_TRY(check_common(ctx, y, out, n, w, h, levels));
     if (!log_steps || !partials || parts <= 0 || parts > 65535 || (bwd && !gin))
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "relaxed quantiser: bad log_steps, partials or parts");
@@ -454,22 +464,26 @@ j2k_status quant_run(j2k_ctx* ctx, bool bwd, const float* y, const float* gin, f
     const int rows = (int)((h + parts - 1) / parts);
     const size_t plane = w * h;
     const int vec = (((uintptr_t)y & 15) == 0) && (((uintptr_t)out & 15) == 0) && (!bwd || ((uintptr_t)gin & 15) == 0) &&
-                    ((w & 3) == 0);
+                    (!noise || ((uintptr_t)noise & 15) == 0) && ((w & 3) == 0);
     const dim3 g((unsigned)parts, (unsigned)n);
     const Levels lv = make_levels((int)w, (int)h, levels);
+#define RQ_LAUNCH(B_, N_)                                                                                     \
+    do {                                                                                                       \
+        if (smem > 48 * 1024)                                                                                  \
+            J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<B_, N_>,                                        \
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));       \
+        relaxed_quant_k<B_, N_><<<g, 256, smem, ctx->stream>>>(y, gin, out, (int)w, (int)h, plane, lv,         \
+                                                              log_steps, seed, lam, gscale, alpha, partials,   \
+                                                              rows, vec, noise);                               \
+    } while (0)
     if (bwd) {
-        if (smem > 48 * 1024)
-            J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem));
-        relaxed_quant_k<true><<<g, 256, smem, ctx->stream>>>(y, gin, out, (int)w, (int)h, plane, lv, log_steps, seed,
-                                                             lam, gscale, alpha, partials, rows, vec);
+        if (noise) RQ_LAUNCH(true, true);
+        else RQ_LAUNCH(true, false);
     } else {
-        if (smem > 48 * 1024)
-            J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)smem));
-        relaxed_quant_k<false><<<g, 256, smem, ctx->stream>>>(y, nullptr, out, (int)w, (int)h, plane, lv, log_steps,
-                                                              seed, 0.0f, nullptr, 1.0f, partials, rows, vec);
+        if (noise) RQ_LAUNCH(false, true);
+        else RQ_LAUNCH(false, false);
     }
+#undef RQ_LAUNCH
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }
@@ -591,22 +605,30 @@ j2k_status j2k_relaxed_quant_forward(j2k_ctx* ctx, const float* y, float* y_hat,
                                      int levels, const float* log_steps, uint64_t seed, float* rate_partials,
                                      int parts_per_band) {
     return quant_run(ctx, false, y, nullptr, y_hat, n, w, h, levels, log_steps, seed, 0.0f, nullptr, 1.0f,
-                     rate_partials, parts_per_band);
+                     rate_partials, parts_per_band, nullptr);
+}
+
+j2k_status j2k_relaxed_quant_forward_noise(j2k_ctx* ctx, const float* y, float* y_hat, float* noise, int n, size_t w,
+                                           size_t h, int levels, const float* log_steps, uint64_t seed,
+                                           float* rate_partials, int parts_per_band) {
+    if (!noise) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "relaxed quantiser: noise buffer is NULL");
+    return quant_run(ctx, false, y, nullptr, y_hat, n, w, h, levels, log_steps, seed, 0.0f, nullptr, 1.0f,
+                     rate_partials, parts_per_band, noise);
 }
 
 j2k_status j2k_relaxed_quant_backward(j2k_ctx* ctx, const float* y, const float* g_yhat, float* g_y, int n,
                                       size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
                                       float lam, float* g_logstep_partials, int parts_per_band) {
     return quant_run(ctx, true, y, g_yhat, g_y, n, w, h, levels, log_steps, seed, lam, nullptr, 1.0f,
-                     g_logstep_partials, parts_per_band);
+                     g_logstep_partials, parts_per_band, nullptr);
 }
 
 j2k_status j2k_relaxed_quant_backward_scaled(j2k_ctx* ctx, const float* y, const float* g_in, float* g_y, int n,
                                              size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
-                                             float lam, const float* scale, float alpha, float* g_logstep_partials,
-                                             int parts_per_band) {
+                                             const float* noise, float lam, const float* scale, float alpha,
+                                             float* g_logstep_partials, int parts_per_band) {
     return quant_run(ctx, true, y, g_in, g_y, n, w, h, levels, log_steps, seed, lam, scale, alpha,
-                     g_logstep_partials, parts_per_band);
+                     g_logstep_partials, parts_per_band, const_cast<float*>(noise));
 }
 
 }  // extern "C"

@@ -5,11 +5,12 @@ hand-written adjoints as backward, the relaxed dead-zone quantiser (additive uni
 one step per subband) with its backward, and the fused rate-distortion loss
     loss = mean((IDWT(Q(DWT(x))) - x)^2) + lam * sum_b sum log2(1 + |y_hat|/step_b)
 differentiable with respect to the pixels x and the per-subband log steps.  torch provides the
-device memory and the stream; every pass runs in libj2kb200's kernels.  The fused loss keeps two
-planes per image for its backward: the quantiser input y and the residual d = IDWT(y_hat) - x
-(the reconstruction itself is never stored; the residual pass is fused into the last inverse
-level, and the "- 2/N d" term of the pixel gradient into the last forward-adjoint level).  The
-backward reads its output gradient on the device, so a step never synchronises with the host.
+device memory and the stream; every pass runs in libj2kb200's kernels.  The fused loss keeps three
+planes per image for its backward: the quantiser input y, its noise u (so the backward does not
+regenerate it) and the residual d = IDWT(y_hat) - x (the reconstruction itself is never stored;
+the residual pass is fused into the last inverse level, and the "- 2/N d" term of the pixel
+gradient into the last forward-adjoint level).  The backward reads its output gradient on the
+device, so a step never synchronises with the host.
 """
 import ctypes as C
 
@@ -78,8 +79,8 @@ def _band_sum(parts, n, nb, k):
     return parts.view(n, nb, k).sum(dim=2)
 
 
-def relaxed_quant(y, log_steps, levels, seed):
-    """-> (y_hat, rate per image and band (N, 3L+1))."""
+def relaxed_quant(y, log_steps, levels, seed, keep_noise=False):
+    """-> (y_hat, rate per image and band (N, 3L+1)), plus the noise u when keep_noise."""
     ctx, h = _ctx(y)
     y = y.contiguous()
     n, hh, ww = y.shape
@@ -87,13 +88,19 @@ def relaxed_quant(y, log_steps, levels, seed):
     ls = log_steps.detach().float().contiguous()
     yh = torch.empty_like(y)
     parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+    if keep_noise:
+        u = torch.empty_like(y)
+        check(lib().j2k_relaxed_quant_forward_noise(h, _p(y), _p(yh), _p(u), n, ww, hh, levels, _p(ls), seed,
+                                                    _p(parts), k), h)
+        return yh, _band_sum(parts, n, nb, k), u
     check(lib().j2k_relaxed_quant_forward(h, _p(y), _p(yh), n, ww, hh, levels, _p(ls), seed, _p(parts), k), h)
     return yh, _band_sum(parts, n, nb, k)
 
 
-def relaxed_quant_backward(y, g_yhat, log_steps, levels, seed, lam, scale=None, alpha=1.0):
+def relaxed_quant_backward(y, g_yhat, log_steps, levels, seed, lam, scale=None, alpha=1.0, noise=None):
     """-> (dL/dy, dL/dlog_steps) for L = <g, y_hat> + lam * sum(rate), g = scale * alpha * g_yhat
-    (scale: optional 0-dim CUDA tensor, read on the device)."""
+    (scale: optional 0-dim CUDA tensor, read on the device; noise: the forward's kept noise, else
+    it is regenerated from seed)."""
     ctx, h = _ctx(y)
     n, hh, ww = y.shape
     nb, k = 3 * levels + 1, _parts(hh)
@@ -101,9 +108,10 @@ def relaxed_quant_backward(y, g_yhat, log_steps, levels, seed, lam, scale=None, 
     gy = torch.empty_like(y)
     parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
     sp = None if scale is None else _p(scale)
+    npt = None if noise is None else _p(noise.contiguous())
     check(lib().j2k_relaxed_quant_backward_scaled(h, _p(y.contiguous()), _p(g_yhat.contiguous()), _p(gy), n, ww, hh,
-                                                  levels, _p(ls), seed, float(lam), sp, float(alpha), _p(parts), k),
-          h)
+                                                  levels, _p(ls), seed, npt, float(lam), sp, float(alpha), _p(parts),
+                                                  k), h)
     return gy, _band_sum(parts, n, nb, k).sum(dim=0)
 
 
@@ -192,20 +200,21 @@ class RDLoss(torch.autograd.Function):
     def forward(ctx, x, log_steps, levels, lam, seed):
         x = x.detach().contiguous()
         y = dwt97(x, levels)
-        yh, rate = relaxed_quant(y, log_steps, levels, seed)
+        yh, rate, u = relaxed_quant(y, log_steps, levels, seed, keep_noise=True)
         d, sq = inverse_residual(yh, x, levels)
         del yh
-        ctx.save_for_backward(y, d, log_steps)
+        ctx.save_for_backward(y, d, u, log_steps)
         ctx.levels, ctx.lam, ctx.seed = levels, lam, seed
         return sq / x.numel() + lam * rate.sum()
 
     @staticmethod
     def backward(ctx, g):
-        y, d, log_steps = ctx.saved_tensors
+        y, d, u, log_steps = ctx.saved_tensors
         g = g.detach().float().contiguous()
         alpha = 2.0 / d.numel()
         g_res = idwt97_adjoint(d, ctx.levels)
-        g_y, g_ls = relaxed_quant_backward(y, g_res, log_steps, ctx.levels, ctx.seed, ctx.lam, scale=g, alpha=alpha)
+        g_y, g_ls = relaxed_quant_backward(y, g_res, log_steps, ctx.levels, ctx.seed, ctx.lam, scale=g, alpha=alpha,
+                                           noise=u)
         del g_res
         gx = forward_adjoint_residual(g_y, d, ctx.levels, scale=g, alpha=alpha)
         return gx, g_ls.to(log_steps.dtype), None, None, None

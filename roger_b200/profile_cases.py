@@ -70,10 +70,10 @@ def case_diff_kernels():
 
     def run():
         y = D.dwt97(x, L)
-        yh, _ = D.relaxed_quant(y, ls, L, 200)
+        yh, _, u = D.relaxed_quant(y, ls, L, 200, keep_noise=True)
         d, _ = D.inverse_residual(yh, x, L)
         g = D.idwt97_adjoint(d, L)
-        gy, _ = D.relaxed_quant_backward(y, g, ls, L, 200, 0.01)
+        gy, _ = D.relaxed_quant_backward(y, g, ls, L, 200, 0.01, noise=u)
         return D.forward_adjoint_residual(gy, d, L, alpha=1e-3)
     return run
 

@@ -143,3 +143,23 @@ def test_fused_rd_loss_matches_composed_form(D, n, w, h, L):
     assert abs(a.item() - b.item()) <= 1e-5 * abs(b.item())
     assert torch.allclose(x1.grad, x2.grad, rtol=1e-3, atol=1e-7 * x2.grad.abs().max().item())
     assert torch.allclose(l1.grad, l2.grad, rtol=1e-4, atol=1e-6)
+
+
+def test_kept_noise_matches_regenerated_noise(D):
+    """The forward that keeps its noise writes exactly the oracle's noise, and the backward that
+    reads it gives the same gradients as the backward that regenerates it."""
+    n, w, h, L, seed = 2, 70, 37, 3, 5
+    rng = np.random.default_rng(3)
+    y = torch.from_numpy(rng.normal(scale=10.0, size=(n, h, w)).astype(np.float32)).cuda()
+    ls = torch.linspace(-1.0, 1.0, 3 * L + 1, device="cuda")
+    yh, rate, u = D.relaxed_quant(y, ls, L, seed, keep_noise=True)
+    yh2, rate2 = D.relaxed_quant(y, ls, L, seed)
+    assert torch.equal(yh, yh2) and torch.equal(rate, rate2)
+    un = u.cpu().numpy()
+    for i in range(n):
+        for yy, xx in [(0, 0), (5, 3), (36, 69), (17, 40)]:
+            assert un[i, yy, xx] == np.float32(O.rd_noise(seed + i, w, xx, yy))
+    g = torch.from_numpy(rng.normal(size=(n, h, w)).astype(np.float32)).cuda()
+    a = D.relaxed_quant_backward(y, g, ls, L, seed, 0.01, noise=u)
+    b = D.relaxed_quant_backward(y, g, ls, L, seed, 0.01)
+    assert torch.equal(a[0], b[0]) and torch.allclose(a[1], b[1], rtol=1e-6, atol=0)
