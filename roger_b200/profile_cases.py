@@ -8,8 +8,8 @@ profile the second run, e.g. ``ncu -k regex:dwt_fwd_fast -s 3 -c 1 ...``.  Sizes
 benchmark workloads but stay within a few hundred MB of device memory:
 
   planar       4096x4096 RGB uint8 -> 3 int32 planes with RCT (1 launch)
-  dwt53        level-0 5/3 forward of a 4096x4096 int32 plane (1 launch per run)
-  dwt53-all    6-level 5/3 forward of the same plane
+  dwt53        level-0 5/3 forward of the three 4096x4096 int32 RCT planes (1 launch per run)
+  dwt53-all    6-level 5/3 forward of the same planes
   idwt53       level-0 5/3 inverse of the same plane
   tier1        EBCOT tier-1 of one 4096x4096 RCT component (6 levels, 4096 64x64 blocks)
   encode       one whole lossless 4096x4096 RGB encode (planar, 3 x 6 DWT levels, tier-1)
@@ -38,8 +38,8 @@ def case_planar():
 
 def case_dwt53(levels=1):
     planes = C.rgb_to_planar(_rgb(), 1)
-    out = torch.empty_like(planes[0])
-    return lambda: C.dwt_forward(planes[0], levels, out=out)
+    out = torch.empty_like(planes)
+    return lambda: C.dwt_forward(planes, levels, out=out)
 
 
 def case_idwt53():
