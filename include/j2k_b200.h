@@ -208,6 +208,32 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs
                                       int ncomp, size_t w, size_t h, const j2k_enc_params* params,
                                       uint8_t* out, int out_on_device, size_t out_pitch_bytes);
 
+/* ---- codestream reading (tier-2 decoding).  No counterpart in the reference, which writes and
+ * reads no codestream.  Parses a T.800 codestream of one tile (tile-parts allowed), one quality
+ * layer, LRCP or RLCP progression, one precinct per resolution, the default code-block style,
+ * reversible (5/3) or irreversible (9/7) transform with no, derived or expounded quantisation,
+ * 1 or 3 (with colour transform) 8-bit components: the subset this library writes and the one
+ * OpenJPEG writes by default.  SOP/EPH markers are skipped.  Other streams return
+ * J2K_ERR_UNSUPPORTED with the reason in `err`.  Call with descs = bytes = NULL for the stream
+ * info, the code-block count and the codeword bytes needed; then with buffers of that size:
+ * descs (job order, as j2k_encoder_get_codeblocks) and the codewords packed back to back.  The
+ * result feeds j2k_decoder_run_codeblocks (lossy = !info->lossless, steps = info->steps).
+ * Host memory only; needs no context. */
+#define J2K_MAX_BANDS 97
+typedef struct {
+    uint32_t w, h;
+    int ncomp, levels, cbw, cbh;
+    int lossless;      /* 1: reversible 5/3; 0: irreversible 9/7 */
+    int mct;           /* colour transform (RCT with 5/3, ICT with 9/7) */
+    int guard;         /* guard bits */
+    int precision;     /* bits per component sample */
+    int layers, progression;
+    float steps[J2K_MAX_BANDS];  /* per-subband quantiser steps in QCD order (1 when lossless) */
+} j2k_stream_info;
+j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
+                               size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
+                               size_t errlen);
+
 /* ---- differentiable 9/7 (no counterpart in the reference).  n images of w x h float32,
  * planes back to back (pitch w, plane stride w*h), device pointers, T.800 order.  Used with
  * j2k_dwt_forward / j2k_dwt_inverse (kernel 97, steps NULL) as the forward operators.

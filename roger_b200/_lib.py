@@ -32,6 +32,16 @@ class EncParams(C.Structure):
                 ("steps", C.c_void_p)]
 
 
+J2K_MAX_BANDS = 97
+
+
+class StreamInfo(C.Structure):
+    _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("ncomp", C.c_int), ("levels", C.c_int), ("cbw", C.c_int),
+                ("cbh", C.c_int), ("lossless", C.c_int), ("mct", C.c_int), ("guard", C.c_int),
+                ("precision", C.c_int), ("layers", C.c_int), ("progression", C.c_int),
+                ("steps", C.c_float * J2K_MAX_BANDS)]
+
+
 class J2KError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{STATUS.get(status, status)} ({status}): {msg}")
@@ -61,6 +71,7 @@ SIGS = {
     "j2k_dwt_forward_batch": (I, [P, I, I, P, S, S, P, S, S, I, S, S, I, P]),
     "j2k_dwt_inverse_batch": (I, [P, I, I, P, S, S, P, S, S, I, S, S, I, P]),
     "j2k_codeblock_count": (S, [S, S, I, I, I]),
+    "j2k_codestream_read": (I, [P, S, P, P, P, P, S, P, P, S]),
     "j2k_bpc_encode": (I, [P, P, S, S, S, I, I, I, P, P, S]),
     "j2k_bpc_decode": (I, [P, P, P, S, P, S, S, S, I, I, I]),
     "j2k_encoder_create": (I, [P, I, I, C.POINTER(P)]),

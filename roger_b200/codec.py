@@ -16,7 +16,8 @@ from ._lib import J2KError, check, lib
 
 __all__ = ["Context", "rgb_to_planar", "planar_to_rgb", "dwt_forward", "dwt_inverse",
            "codeblock_count", "bpc_encode", "bpc_decode", "OCLEncoder", "OCLDecoder",
-           "OCLDWTForward", "OCLDWTRev", "OCLRGBtoPlanar", "OCLBPC", "default_steps",
+           "OCLDWTForward", "OCLDWTRev", "OCLRGBtoPlanar", "OCLBPC", "default_steps", "read_codestream",
+           "decode_codestream",
            "subband_rects", "J2KError"]
 
 
@@ -361,6 +362,43 @@ class OCLDecoder(OCLEncodeDecode):
                                                w, h, C.byref(p), out.ctypes.data_as(C.c_void_p), 0,
                                                w * ncomp), hh)
         return out
+
+
+def read_codestream(cs):
+    """Tier-2 decoding of a codestream (bytes): -> (info dict, descs structured array, codeword
+    bytes), ready for OCLDecoder.run.  Raises J2KError(J2K_ERR_UNSUPPORTED) with the reason for
+    streams outside the supported subset (one tile, one layer, LRCP/RLCP, default code-block
+    style, 1 or 3 colour-transformed 8-bit components)."""
+    buf = np.frombuffer(bytes(cs), np.uint8)
+    info = L.StreamInfo()
+    cnt, used = C.c_size_t(), C.c_size_t()
+    err = C.create_string_buffer(256)
+    s = lib().j2k_codestream_read(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(info), None, C.byref(cnt),
+                                  None, 0, C.byref(used), err, 256)
+    if s != 0:
+        raise L.J2KError(s, err.value.decode())
+    descs = np.zeros(cnt.value, L.CB_DESC)
+    data = np.zeros(max(used.value, 1), np.uint8)
+    s = lib().j2k_codestream_read(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(info),
+                                  descs.ctypes.data_as(C.c_void_p), C.byref(cnt), data.ctypes.data_as(C.c_void_p),
+                                  data.size, C.byref(used), err, 256)
+    if s != 0:
+        raise L.J2KError(s, err.value.decode())
+    nb = 3 * info.levels + 1
+    d = dict(w=info.w, h=info.h, ncomp=info.ncomp, levels=info.levels, cbw=info.cbw, cbh=info.cbh,
+             lossless=bool(info.lossless), mct=info.mct, guard=info.guard, precision=info.precision,
+             layers=info.layers, progression=info.progression,
+             steps=np.array(info.steps[:nb], np.float32))
+    return d, descs, data[:used.value]
+
+
+def decode_codestream(cs, ctx=None):
+    """Decodes a codestream on the GPU: tier-2 on the host, then tier-1, inverse DWT and inverse
+    colour transform on the device.  Returns (H, W, C) uint8."""
+    info, descs, data = read_codestream(cs)
+    dec = OCLDecoder(ctx=ctx, lossy=not info["lossless"])
+    return dec.run(descs, data, info["w"], info["h"], info["ncomp"], levels=info["levels"], cbw=info["cbw"],
+                   cbh=info["cbh"], steps=None if info["lossless"] else info["steps"])
 
 
 class OCLDWTForward:

@@ -3,6 +3,7 @@
 // one codeword segment each (all passes included).  The reference has no tier-2 at all.
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "j2k_internal.cuh"
@@ -270,4 +271,379 @@ std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int
     o.v[sot + 9] = (uint8_t)psot;
     o.u16(0xFFD9);  // EOC
     return o.v;
+}
+
+// ---- tier-2 reading (codestream parser) -----------------------------------------------------
+namespace {
+
+struct ReadErr {
+    j2k_status s;
+    const char* msg;
+};
+
+struct Cursor {
+    const uint8_t* p;
+    size_t n, i = 0;
+    uint32_t u8() {
+        if (i >= n) throw ReadErr{J2K_ERR_INVALID_ARG, "codestream truncated"};
+        return p[i++];
+    }
+    uint32_t u16() { uint32_t a = u8(); return (a << 8) | u8(); }
+    uint32_t u32() { uint32_t a = u16(); return (a << 16) | u16(); }
+};
+
+// packet-header bit reader: after a 0xFF byte the next byte carries 7 bits (B.10.1)
+struct BitReader {
+    const uint8_t* p;
+    size_t n, i;
+    uint32_t cur = 0;
+    int left = 0;
+    bool last_ff = false;
+    BitReader(const uint8_t* d, size_t len, size_t start) : p(d), n(len), i(start) {}
+    int bit() {
+        if (left == 0) {
+            if (i >= n) throw ReadErr{J2K_ERR_INVALID_ARG, "packet header truncated"};
+            cur = p[i++];
+            left = last_ff ? 7 : 8;
+            last_ff = (cur == 0xFF);
+        }
+        --left;
+        return (int)((cur >> left) & 1);
+    }
+    uint32_t bits(int k) {
+        uint32_t v = 0;
+        while (k--) v = (v << 1) | (uint32_t)bit();
+        return v;
+    }
+    // end of header: byte aligned; a header whose last byte is 0xFF is followed by one more
+    size_t end() {
+        if (last_ff) {
+            if (i >= n) throw ReadErr{J2K_ERR_INVALID_ARG, "packet header truncated"};
+            ++i;
+        }
+        return i;
+    }
+};
+
+// B.10.2 tag tree, decoding side
+struct TagTreeDec {
+    std::vector<int> lw, lh, off, low, val;
+    std::vector<uint8_t> known;
+    int nlev = 0;
+    TagTreeDec(int nw, int nh) {
+        int w = nw, h = nh, total = 0;
+        for (;;) {
+            lw.push_back(w);
+            lh.push_back(h);
+            off.push_back(total);
+            total += w * h;
+            ++nlev;
+            if (w == 1 && h == 1) break;
+            w = (w + 1) / 2;
+            h = (h + 1) / 2;
+        }
+        low.assign(total, 0);
+        val.assign(total, 0);
+        known.assign(total, 0);
+    }
+    // value of leaf (x, y) if it is below `threshold`, else `threshold`
+    int decode(BitReader& br, int x, int y, int threshold) {
+        int path[40];
+        for (int l = 0; l < nlev; ++l) {
+            path[l] = off[l] + y * lw[l] + x;
+            x >>= 1;
+            y >>= 1;
+        }
+        int lo = 0;
+        for (int l = nlev - 1; l >= 0; --l) {
+            const int q = path[l];
+            if (low[q] < lo) low[q] = lo;
+            while (!known[q] && low[q] < threshold) {
+                if (br.bit()) {
+                    known[q] = 1;
+                    val[q] = low[q];
+                } else {
+                    ++low[q];
+                }
+            }
+            lo = low[q];
+        }
+        const int leaf = path[0];
+        return (known[leaf] && val[leaf] < threshold) ? val[leaf] : threshold;
+    }
+};
+
+int get_npasses(BitReader& br) {  // Table B.4
+    if (!br.bit()) return 1;
+    if (!br.bit()) return 2;
+    uint32_t v = br.bits(2);
+    if (v < 3) return 3 + (int)v;
+    v = br.bits(5);
+    if (v < 31) return 6 + (int)v;
+    return 37 + (int)br.bits(7);
+}
+
+}  // namespace
+
+namespace {
+
+// Parses a codestream into stream parameters, one descriptor per code-block (job order:
+// component, subband in QCD order, raster) and the packet bytes of the tile (tile-parts
+// concatenated); src_off[i] is block i's codeword offset within tile_bytes.
+j2k_status t2_read(const uint8_t* cs, size_t n, j2k_stream_info* info, std::vector<j2k_cb_desc>* descs,
+                   std::vector<uint32_t>* src_off, std::vector<uint8_t>* tile_bytes, std::string* err) {
+    try {
+        Cursor c{cs, n};
+        if (c.u16() != 0xFF4F) throw ReadErr{J2K_ERR_INVALID_ARG, "no SOC marker"};
+        j2k_stream_info I{};
+        int ncomp = 0, levels = -1, prog = 0, layers = 0, mct = 0, cbw = 0, cbh = 0, sty = 0, xform = 0, scod = 0;
+        int qstyle = -1, guard = 0;
+        std::vector<int> eps, mant;
+        uint32_t tw = 0, th = 0;
+        std::vector<uint8_t> data;  // packet bytes of tile 0, tile-parts concatenated
+        bool in_tile = false;
+        for (;;) {
+            const uint32_t m = c.u16();
+            if (m == 0xFFD9) break;  // EOC
+            if (m == 0xFF93) {       // SOD: read to the end of the tile-part
+                throw ReadErr{J2K_ERR_INVALID_ARG, "SOD outside a tile-part"};
+            }
+            const size_t seg_start = c.i;
+            const uint32_t L = c.u16();
+            if (L < 2 || seg_start + L > n) throw ReadErr{J2K_ERR_INVALID_ARG, "bad marker segment length"};
+            const size_t seg_end = seg_start + L;
+            if (m == 0xFF51) {  // SIZ
+                c.u16();
+                const uint32_t xs = c.u32(), ys = c.u32(), x0 = c.u32(), y0 = c.u32();
+                tw = c.u32();
+                th = c.u32();
+                const uint32_t tx0 = c.u32(), ty0 = c.u32();
+                ncomp = (int)c.u16();
+                if (x0 || y0 || tx0 || ty0) throw ReadErr{J2K_ERR_UNSUPPORTED, "image or tile offsets"};
+                if (tw < xs || th < ys) throw ReadErr{J2K_ERR_UNSUPPORTED, "more than one tile"};
+                if (ncomp != 1 && ncomp != 3) throw ReadErr{J2K_ERR_UNSUPPORTED, "component count other than 1 or 3"};
+                for (int k = 0; k < ncomp; ++k) {
+                    const uint32_t ssiz = c.u8(), dx = c.u8(), dy = c.u8();
+                    if (ssiz != 7 || dx != 1 || dy != 1)
+                        throw ReadErr{J2K_ERR_UNSUPPORTED, "components other than 8-bit unsigned, unsubsampled"};
+                }
+                I.w = xs;
+                I.h = ys;
+                I.ncomp = ncomp;
+                I.precision = 8;
+            } else if (m == 0xFF52) {  // COD
+                scod = (int)c.u8();
+                prog = (int)c.u8();
+                layers = (int)c.u16();
+                mct = (int)c.u8();
+                levels = (int)c.u8();
+                cbw = 1 << ((int)c.u8() + 2);
+                cbh = 1 << ((int)c.u8() + 2);
+                sty = (int)c.u8();
+                xform = (int)c.u8();
+                if (scod & 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "user-defined precincts"};
+                if (layers != 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "more than one quality layer"};
+                if (prog != 0 && prog != 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "progression other than LRCP/RLCP"};
+                if (sty != 0) throw ReadErr{J2K_ERR_UNSUPPORTED, "code-block style options (bypass, reset, ...)"};
+                if (levels > 32 || cbw > 64 || cbh > 64 || cbw * cbh > 4096)
+                    throw ReadErr{J2K_ERR_UNSUPPORTED, "code-block size or decomposition levels"};
+            } else if (m == 0xFF5C) {  // QCD
+                const uint32_t sq = c.u8();
+                guard = (int)(sq >> 5);
+                qstyle = (int)(sq & 31);
+                const size_t nbytes = seg_end - c.i;
+                if (qstyle == 0) {
+                    for (size_t k = 0; k < nbytes; ++k) {
+                        eps.push_back((int)(c.u8() >> 3));
+                        mant.push_back(0);
+                    }
+                } else if (qstyle == 1 || qstyle == 2) {
+                    for (size_t k = 0; k + 1 < nbytes; k += 2) {
+                        const uint32_t v = c.u16();
+                        eps.push_back((int)(v >> 11));
+                        mant.push_back((int)(v & 0x7FF));
+                    }
+                } else {
+                    throw ReadErr{J2K_ERR_UNSUPPORTED, "quantisation style"};
+                }
+            } else if (m == 0xFF53 || m == 0xFF5D || m == 0xFF5E || m == 0xFF60 || m == 0xFF61) {
+                throw ReadErr{J2K_ERR_UNSUPPORTED, "COC, QCC, RGN, PPM or PPT marker"};
+            } else if (m == 0xFF90) {  // SOT
+                const uint32_t isot = c.u16(), psot = c.u32();
+                c.u8();
+                c.u8();
+                if (isot != 0) throw ReadErr{J2K_ERR_UNSUPPORTED, "more than one tile"};
+                // tile-part header markers up to SOD
+                size_t end = psot ? seg_start - 2 + psot : n - 2;
+                if (end > n) throw ReadErr{J2K_ERR_INVALID_ARG, "bad Psot"};
+                c.i = seg_end;
+                for (;;) {
+                    const uint32_t mm = c.u16();
+                    if (mm == 0xFF93) break;
+                    const size_t s2 = c.i;
+                    const uint32_t L2 = c.u16();
+                    if (mm == 0xFF52 || mm == 0xFF5C || mm == 0xFF53 || mm == 0xFF5D || mm == 0xFF61)
+                        throw ReadErr{J2K_ERR_UNSUPPORTED, "coding or quantisation markers in a tile-part header"};
+                    c.i = s2 + L2;
+                }
+                if (c.i > end) throw ReadErr{J2K_ERR_INVALID_ARG, "bad tile-part"};
+                data.insert(data.end(), cs + c.i, cs + end);
+                c.i = end;
+                in_tile = true;
+                continue;
+            }
+            c.i = seg_end;
+        }
+        (void)in_tile;
+        if (!ncomp || levels < 0 || qstyle < 0) throw ReadErr{J2K_ERR_INVALID_ARG, "missing SIZ, COD or QCD"};
+        if (ncomp == 3 && !mct) throw ReadErr{J2K_ERR_UNSUPPORTED, "three components without a colour transform"};
+        if (ncomp == 1 && mct) throw ReadErr{J2K_ERR_INVALID_ARG, "colour transform on one component"};
+        const int nb = 3 * levels + 1;
+        if (qstyle == 1) {  // derived: every band from the LL exponent (E.1.1.1)
+            if (eps.empty()) throw ReadErr{J2K_ERR_INVALID_ARG, "empty QCD"};
+            const int e0 = eps[0], m0 = mant[0];
+            eps.assign(nb, 0);
+            mant.assign(nb, m0);
+            for (int b = 0; b < nb; ++b) {
+                const int lev = b == 0 ? levels : levels - (b - 1) / 3;  // decomposition level of band b
+                eps[b] = e0 - (levels - lev);
+            }
+        }
+        if ((int)eps.size() < nb) throw ReadErr{J2K_ERR_INVALID_ARG, "QCD lists fewer bands than the transform has"};
+        I.levels = levels;
+        I.cbw = cbw;
+        I.cbh = cbh;
+        I.lossless = xform == 1;
+        I.mct = mct;
+        I.guard = guard;
+        I.layers = layers;
+        I.progression = prog;
+        std::vector<j2k_band_rect> rects(nb);
+        j2k_band_rects(I.w, I.h, levels, rects.data());
+        for (int b = 0; b < nb && b < J2K_MAX_BANDS; ++b) {
+            const int o = rects[b].orient;
+            const int gain = o == J2K_BAND_LL ? 0 : (o == J2K_BAND_HH ? 2 : 1);
+            I.steps[b] = I.lossless ? 1.0f : std::ldexp(1.0f + mant[b] / 2048.0f, 8 + gain - eps[b]);
+        }
+        // code-blocks in job order (component, band, raster) and the packets of the tile
+        std::vector<size_t> first((size_t)ncomp * nb + 1);
+        std::vector<int> ncbx(nb), ncby(nb);
+        size_t k = 0;
+        for (int cc = 0; cc < ncomp; ++cc)
+            for (int b = 0; b < nb; ++b) {
+                first[(size_t)cc * nb + b] = k;
+                ncbx[b] = (rects[b].w && rects[b].h) ? (int)((rects[b].w + cbw - 1) / cbw) : 0;
+                ncby[b] = (rects[b].w && rects[b].h) ? (int)((rects[b].h + cbh - 1) / cbh) : 0;
+                k += (size_t)ncbx[b] * ncby[b];
+            }
+        first[(size_t)ncomp * nb] = k;
+        descs->assign(k, j2k_cb_desc{});
+        src_off->assign(k, 0);
+        for (int cc = 0; cc < ncomp; ++cc)
+            for (int b = 0; b < nb; ++b)
+                for (int j = 0; j < ncby[b]; ++j)
+                    for (int i = 0; i < ncbx[b]; ++i) {
+                        j2k_cb_desc& d = (*descs)[first[(size_t)cc * nb + b] + (size_t)j * ncbx[b] + i];
+                        d.orient = (uint8_t)rects[b].orient;
+                        d.band = (uint8_t)b;
+                        d.x0 = (uint16_t)(rects[b].x0 + (size_t)i * cbw);
+                        d.y0 = (uint16_t)(rects[b].y0 + (size_t)j * cbh);
+                        d.cw = (uint16_t)std::min<size_t>(cbw, rects[b].w - (size_t)i * cbw);
+                        d.ch = (uint16_t)std::min<size_t>(cbh, rects[b].h - (size_t)j * cbh);
+                        d.comp = (uint16_t)cc;
+                    }
+        size_t pos = 0;
+        const uint8_t* pd = data.data();
+        const size_t pn = data.size();
+        for (int r = 0; r <= levels; ++r)
+            for (int cc = 0; cc < ncomp; ++cc) {
+                if (scod & 2) {  // SOP marker segment before the packet
+                    if (pos + 6 <= pn && pd[pos] == 0xFF && pd[pos + 1] == 0x91) pos += 6;
+                }
+                const int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
+                const int bcount = r == 0 ? 1 : 3;
+                BitReader br(pd, pn, pos);
+                std::vector<std::pair<size_t, int>> body;  // (block index, length) in packet order
+                if (br.bit()) {
+                    for (int q = 0; q < bcount; ++q) {
+                        const int b = b0 + q;
+                        const int nbx = ncbx[b], nby = ncby[b];
+                        if (!nbx || !nby) continue;
+                        TagTreeDec ti(nbx, nby), tz(nbx, nby);
+                        const int Mb = guard + eps[b] - 1;
+                        for (int j = 0; j < nby; ++j)
+                            for (int i = 0; i < nbx; ++i) {
+                                const size_t idx = first[(size_t)cc * nb + b] + (size_t)j * nbx + i;
+                                if (ti.decode(br, i, j, 1) >= 1) continue;  // not included
+                                int z = 0;
+                                while ((z = tz.decode(br, i, j, 1 << 30)) == (1 << 30)) {
+                                }
+                                const int np = get_npasses(br);
+                                int lblock = 3;
+                                while (br.bit()) ++lblock;
+                                const int lbits = lblock + floorlog2(np);
+                                if (lbits > 31) throw ReadErr{J2K_ERR_INVALID_ARG, "code-block length field too long"};
+                                const int len = (int)br.bits(lbits);
+                                j2k_cb_desc& d = (*descs)[idx];
+                                const int nbps = Mb - z;
+                                if (nbps < 1 || nbps > 31 || np > 3 * nbps - 2)
+                                    throw ReadErr{J2K_ERR_INVALID_ARG, "inconsistent bit-planes or passes"};
+                                d.numbps = (uint8_t)nbps;
+                                d.npasses = (uint8_t)np;
+                                d.length = len;
+                                body.push_back({idx, len});
+                            }
+                    }
+                }
+                pos = br.end();
+                if (scod & 4) {  // EPH
+                    if (pos + 2 <= pn && pd[pos] == 0xFF && pd[pos + 1] == 0x92) pos += 2;
+                }
+                for (auto& e : body) {
+                    if (pos + (size_t)e.second > pn) throw ReadErr{J2K_ERR_INVALID_ARG, "packet body truncated"};
+                    (*src_off)[e.first] = (uint32_t)pos;
+                    pos += (size_t)e.second;
+                }
+            }
+        *info = I;
+        tile_bytes->swap(data);
+        return J2K_OK;
+    } catch (const ReadErr& e) {
+        if (err) *err = e.msg;
+        return e.s;
+    }
+}
+
+}  // namespace
+
+extern "C" j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
+                                          size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
+                                          size_t errlen) {
+    if (!cs || !info || !count || !used) return J2K_ERR_INVALID_ARG;
+    std::vector<j2k_cb_desc> d;
+    std::vector<uint32_t> off;
+    std::vector<uint8_t> tile;
+    std::string msg;
+    j2k_status s = t2_read(cs, n, info, &d, &off, &tile, &msg);
+    if (s != J2K_OK) {
+        if (err && errlen) {
+            std::strncpy(err, msg.c_str(), errlen - 1);
+            err[errlen - 1] = 0;
+        }
+        return s;
+    }
+    size_t total = 0;
+    for (const auto& x : d) total += (size_t)x.length;
+    *count = d.size();
+    *used = total;
+    if (!descs && !bytes) return J2K_OK;
+    if (!descs || !bytes || cap < total) return J2K_ERR_CAPACITY;
+    size_t o = 0;
+    for (size_t i = 0; i < d.size(); ++i) {
+        d[i].offset = (uint32_t)o;
+        if (d[i].length > 0) std::memcpy(bytes + o, tile.data() + off[i], (size_t)d[i].length);
+        o += (size_t)d[i].length;
+        descs[i] = d[i];
+    }
+    return J2K_OK;
 }

@@ -1,0 +1,95 @@
+"""Tier-2 reading: codestreams written by this library (the oracle's, byte-identical to the GPU
+encoder's) and by OpenJPEG (through Pillow, a black box) are parsed by j2k_codestream_read;
+the code-blocks are then decoded (tier-1, inverse DWT, inverse colour transform) by the oracle
+on the CPU here and by the GPU decoder in the -m gpu test, and must give the input back exactly
+(lossless) or what OpenJPEG itself decodes to within rounding (lossy)."""
+import io
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from roger_b200 import codec as C
+from roger_b200 import synth
+from roger_b200._lib import J2KError
+
+PIL = pytest.importorskip("PIL.Image")
+
+
+def _openjpeg(img, levels, lossless=True, cb=64):
+    buf = io.BytesIO()
+    kw = dict(irreversible=not lossless, num_resolutions=levels + 1, codeblock_size=(cb, cb), progression="LRCP",
+              no_jp2=True)
+    if img.ndim == 3:
+        kw["mct"] = 1
+    PIL.fromarray(img).save(buf, "JPEG2000", **kw)
+    return buf.getvalue()
+
+
+def _cpu_decode(cs):
+    info, descs, data = C.read_codestream(cs)
+    w, h, nc, L = info["w"], info["h"], info["ncomp"], info["levels"]
+    planes = np.zeros((nc, h, w), np.int32)
+    for d in descs:
+        if d["length"] <= 0 and d["npasses"] == 0:
+            continue
+        blk = O.t1_decode(bytes(data[d["offset"]:d["offset"] + d["length"]]), int(d["numbps"]), int(d["npasses"]),
+                          int(d["orient"]), int(d["cw"]), int(d["ch"]))
+        planes[d["comp"], d["y0"]:d["y0"] + d["ch"], d["x0"]:d["x0"] + d["cw"]] = blk
+    if info["lossless"]:
+        rec = np.stack([O.dwt53_inv(p, L) for p in planes])
+        return O.planar_inv(rec, 1 if nc == 3 else 0).reshape(h, w, nc) if nc == 3 else \
+            O.planar_inv(rec, 0).reshape(h, w)
+    st = info["steps"]
+    rec = np.stack([O.dwt97_inv(O.dequantize(p, L, st), L) for p in planes])
+    out = O.planar_inv(rec, 2 if nc == 3 else 0)
+    return out.reshape(h, w, nc) if nc == 3 else out.reshape(h, w)
+
+
+CASES = [(131, 97, 1, 4, 64), (200, 64, 3, 5, 64), (77, 301, 3, 3, 32), (64, 64, 1, 2, 32)]
+
+
+@pytest.mark.parametrize("w,h,nc,L,cb", CASES)
+def test_own_codestream_parses_and_round_trips(w, h, nc, L, cb):
+    img = synth.gray(w, h, 5) if nc == 1 else synth.rgb(w, h, (5, 6, 7, 8))
+    cs = bytes(O.encode_image(img, L, cb, cb, True))
+    info, descs, data = C.read_codestream(cs)
+    assert (info["w"], info["h"], info["ncomp"], info["levels"], info["cbw"]) == (w, h, nc, L, cb)
+    assert info["lossless"] and info["mct"] == (1 if nc == 3 else 0)
+    assert np.array_equal(_cpu_decode(cs).reshape(img.shape), img)
+
+
+@pytest.mark.parametrize("w,h,nc,L,cb", CASES)
+def test_openjpeg_lossless_codestream_decodes_exactly(w, h, nc, L, cb):
+    img = synth.gray(w, h, 9) if nc == 1 else synth.rgb(w, h, (9, 10, 11, 12))
+    cs = _openjpeg(img, L, True, cb)
+    assert np.array_equal(_cpu_decode(cs).reshape(img.shape), img)
+
+
+def test_openjpeg_lossy_codestream_matches_openjpeg_decode():
+    img = synth.rgb(160, 120, (21, 22, 23, 24))
+    cs = _openjpeg(img, 4, lossless=False)
+    ours = _cpu_decode(cs).reshape(img.shape).astype(np.int32)
+    theirs = np.asarray(PIL.open(io.BytesIO(cs))).astype(np.int32)
+    assert np.abs(ours - theirs).max() <= 2
+
+
+def test_unsupported_streams_are_rejected_with_a_reason():
+    img = synth.rgb(64, 64, (1, 2, 3, 4))
+    buf = io.BytesIO()
+    PIL.fromarray(img).save(buf, "JPEG2000", num_resolutions=3, quality_mode="rates", quality_layers=[40, 20, 10],
+                            no_jp2=True)
+    with pytest.raises(J2KError, match="layer"):
+        C.read_codestream(buf.getvalue())
+    with pytest.raises(J2KError):
+        C.read_codestream(b"\\x00\\x01\\x02")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h,nc,L,cb", CASES)
+def test_gpu_decodes_openjpeg_and_own_codestreams(w, h, nc, L, cb):
+    img = synth.gray(w, h, 13) if nc == 1 else synth.rgb(w, h, (13, 14, 15, 16))
+    for cs in (_openjpeg(img, L, True, cb), bytes(O.encode_image(img, L, cb, cb, True))):
+        out = C.decode_codestream(cs)
+        assert np.array_equal(out.reshape(img.shape), img)
