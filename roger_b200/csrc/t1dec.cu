@@ -147,6 +147,13 @@ struct Mqd {
 };
 
 // bits x-1, x, x+1 of a row mask (bit 0 = column x-1); columns outside 0..63 read as 0
+__host__ __device__ __forceinline__ int ctz64(uint64_t v) {
+#ifdef __CUDA_ARCH__
+    return __ffsll((long long)v) - 1;
+#else
+    return __builtin_ctzll(v);
+#endif
+}
 __host__ __device__ __forceinline__ uint32_t nb3(uint64_t m, int x) {
     return (uint32_t)(x > 0 ? (m >> (x - 1)) & 7 : (m << 1) & 7);
 }
@@ -191,11 +198,24 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
             if (neg) S.neg[y + 1] |= 1ull << x;
             blk[(size_t)y * pitch + x] |= 1 << p;
         };
+        const uint64_t cols = cw >= 64 ? ~0ull : ((1ull << cw) - 1);
         for (int p = nb - 1; p >= 0 && pass < np; --p) {
             if (p != nb - 1) {
-                for (int y0 = 0; y0 < ch; y0 += 4)
-                    for (int x = 0; x < cw; ++x)
-                        for (int y = y0; y < y0 + 4 && y < ch; ++y) {
+                // significance propagation: only columns next to a significant sample can hold a
+                // decision; a column joins when its left neighbour gains a significant sample
+                for (int y0 = 0; y0 < ch; y0 += 4) {
+                    const int y1 = min(y0 + 4, ch);
+                    uint64_t cm = 0;
+                    for (int y = y0; y < y1; ++y) {
+                        uint64_t nbm = S.sig[y] | S.sig[y + 1] | S.sig[y + 2];
+                        nbm |= (nbm << 1) | (nbm >> 1);
+                        cm |= ~S.sig[y + 1] & nbm;
+                    }
+                    cm &= cols;
+                    while (cm) {
+                        const int x = ctz64(cm);
+                        cm &= cm - 1;
+                        for (int y = y0; y < y1; ++y) {
                             if (sigbit(x, y)) continue;
                             int z = zc(x, y);
                             if (!(z & 0x100)) continue;
@@ -205,12 +225,22 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                                 int s = sc(x, y);
                                 int sg = m.decode(S.st, s & 31) ^ (s >> 7);
                                 set_sig(x, y, sg, p);
+                                cm |= (2ull << x) & cols;
                             }
                         }
+                    }
+                }
                 if (++pass >= np) break;
-                for (int y0 = 0; y0 < ch; y0 += 4)
-                    for (int x = 0; x < cw; ++x)
-                        for (int y = y0; y < y0 + 4 && y < ch; ++y) {
+                // magnitude refinement: significant samples not visited in this plane
+                for (int y0 = 0; y0 < ch; y0 += 4) {
+                    const int y1 = min(y0 + 4, ch);
+                    uint64_t rm = 0;
+                    for (int y = y0; y < y1; ++y) rm |= S.sig[y + 1] & ~S.vis[y + 1];
+                    rm &= cols;
+                    while (rm) {
+                        const int x = ctz64(rm);
+                        rm &= rm - 1;
+                        for (int y = y0; y < y1; ++y) {
                             if (!sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
                             int lab;
                             if ((S.ref[y + 1] >> x) & 1) lab = 16;
@@ -218,10 +248,19 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                             if (m.decode(S.st, lab)) blk[(size_t)y * pitch + x] |= 1 << p;
                             S.ref[y + 1] |= 1ull << x;
                         }
+                    }
+                }
                 if (++pass >= np) break;
             }
-            for (int y0 = 0; y0 < ch; y0 += 4)
-                for (int x = 0; x < cw; ++x) {
+            // cleanup: every insignificant sample not visited in this plane
+            for (int y0 = 0; y0 < ch; y0 += 4) {
+                const int y1 = min(y0 + 4, ch);
+                uint64_t um = 0;
+                for (int y = y0; y < y1; ++y) um |= ~S.sig[y + 1] & ~S.vis[y + 1];
+                um &= cols;
+                while (um) {
+                    const int x = ctz64(um);
+                    um &= um - 1;
                     int start = y0;
                     if (y0 + 3 < ch) {
                         bool rl = true;
@@ -238,7 +277,7 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                             start = y + 1;
                         }
                     }
-                    for (int y = start; y < y0 + 4 && y < ch; ++y) {
+                    for (int y = start; y < y1; ++y) {
                         if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
                         int z = zc(x, y);
                         int bit = m.decode(S.st, z & 31);
@@ -249,6 +288,7 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                         }
                     }
                 }
+            }
             ++pass;
             for (int r = 0; r < 66; ++r) S.vis[r] = 0;
         }
