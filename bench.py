@@ -233,7 +233,7 @@ def main():
 
     def step_e2e():
         enc.run_rgb(img_pinned.numpy(), levels=LEVELS, cbw=CB, cbh=CB)
-        return enc.get_codeblocks()
+        return enc.get_codeblocks(pinned=True)
 
     def barrier():
         if world > 1:
@@ -326,7 +326,7 @@ def main():
              "h2d_bytes_per_step": int(img_h.nbytes), "d2h_bytes_per_step": d2h,
              "ms_per_step": round(ms_e2e, 4),
              "path": "OCLEncoder.run_rgb (j2k_encoder_run_interleaved, pinned host input) + "
-                     "get_codeblocks (device pack + D2H)"},
+                     "get_codeblocks(pinned=True) (device pack + D2H into page-locked buffers)"},
         roofline={"bound": "hbm", "kernel": f"dwt_fwd_fast<53> level 0 (3 x {size}x{size} int32 planes, one launch)",
                   "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                   "frac": round(achieved / hbm, 4), "traffic": profiled_traffic(size),
@@ -341,7 +341,8 @@ def main():
                "gsample_passes_per_s": round(samples / ((ms - t_planar - t_dwt) * 1e-3) / 1e9, 3),
                "codeword_bytes": int(res[1].size)},
         clocks=clocks,
-        gpu_launches=int(args.steps * (1 + 3 * LEVELS + 2)),
+        # per encode: planar, 3 x 6 DWT levels, tier-1 phase A, the sort's index fill, MQ coder
+        gpu_launches=int(args.steps * (1 + 3 * LEVELS + 3)),
     )
     if world == 1 and size == W and args.extras:
         line["lossless_decode"] = bench_lossless_decode(img_h, res)

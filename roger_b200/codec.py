@@ -306,13 +306,25 @@ class OCLEncoder(OCLEncodeDecode):
         check(lib().j2k_encoder_unmap_dwt_out(self.h, ptr), self.ctx.h)
         return out
 
-    def get_codeblocks(self):
-        """(descs structured array, packed codeword bytes) copied to the host."""
+    def get_codeblocks(self, pinned=False):
+        """(descs structured array, packed codeword bytes) copied to the host.  With pinned=True
+        the copies land in page-locked buffers owned by the encoder (a faster transfer) and the
+        returned arrays are views of them, valid until the next get_codeblocks call."""
         cnt, used = C.c_size_t(), C.c_size_t()
         check(lib().j2k_encoder_get_codeblocks(self.h, None, C.byref(cnt), None, 0, C.byref(used)),
               self.ctx.h)
-        d = np.zeros(cnt.value, L.CB_DESC)
-        b = np.zeros(max(used.value, 1), np.uint8)
+        nd, nb = cnt.value * L.CB_DESC.itemsize, max(used.value, 1)
+        if pinned:
+            pd, pb = getattr(self, "_pin_d", None), getattr(self, "_pin_b", None)
+            if pd is None or pd.numel() < nd:
+                self._pin_d = pd = torch.empty(nd, dtype=torch.uint8, pin_memory=True)
+            if pb is None or pb.numel() < nb:
+                self._pin_b = pb = torch.empty(nb + nb // 4, dtype=torch.uint8, pin_memory=True)
+            d = pd.numpy()[:nd].view(L.CB_DESC)
+            b = pb.numpy()
+        else:
+            d = np.zeros(cnt.value, L.CB_DESC)
+            b = np.zeros(nb, np.uint8)
         check(lib().j2k_encoder_get_codeblocks(self.h, d.ctypes.data_as(C.c_void_p), C.byref(cnt),
                                                b.ctypes.data_as(C.c_void_p), b.size, C.byref(used)),
               self.ctx.h)

@@ -81,6 +81,8 @@ struct j2k_encoder {
     size_t njobs = 0, cap = 0, sym_cap = 0;
     size_t job_key[6] = {0, 0, 0, 0, 0, 0};
     bool have_result = false;
+    bool packed_ok = false;  // the packed codewords of the current result are on the device
+    size_t packed_total = 0;
     void* mapped = nullptr;
 };
 
@@ -177,6 +179,10 @@ static j2k_status encode_planes(j2k_encoder* e) {
 // pack codewords on the device: descs[i].offset -> packed offsets; returns total bytes
 static j2k_status pack_blocks(j2k_encoder* e, size_t* total) {
     j2k_ctx* ctx = e->ctx;
+    if (e->packed_ok) {  // already packed for this result (size query, then copy)
+        *total = e->packed_total;
+        return J2K_OK;
+    }
     int n = (int)e->njobs;
     J2K_TRY(e->lens.ensure(ctx, (size_t)(n + 1) * 4));
     J2K_TRY(e->offs.ensure(ctx, (size_t)(n + 1) * 4));
@@ -197,6 +203,8 @@ static j2k_status pack_blocks(j2k_encoder* e, size_t* total) {
                                                                (uint8_t*)e->packed.p, n);
     J2K_CUDA(ctx, cudaGetLastError());
     *total = tot;
+    e->packed_total = tot;
+    e->packed_ok = true;
     return J2K_OK;
 }
 
@@ -303,6 +311,7 @@ static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const
     }
     J2K_TRY(e->planes.ensure(ctx, w * h * 4 * (size_t)ncomp));
     e->have_result = false;
+    e->packed_ok = false;
     return J2K_OK;
 }
 
