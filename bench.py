@@ -454,6 +454,21 @@ def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
         e.synchronize()
         tt.append(s.elapsed_time(e))
     ms = statistics.median(tt)
+    # the same step captured once in a CUDA graph and replayed (no per-kernel host work)
+    gstep = D.GraphedRDStep(x, ls, levels, 0.01, 200)
+    for _ in range(3):
+        gstep()
+    tg = []
+    for _ in range(5):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        gstep()
+        e.record()
+        e.synchronize()
+        tg.append(s.elapsed_time(e))
+    ms_graph = statistics.median(tg)
     N = n * size * size
     tr = N * 8 * sum(4.0 ** -k for k in range(levels))
     algo = 4 * tr + 8 * N + 12 * N + 12 * N
@@ -461,7 +476,11 @@ def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
                         "grads wrt pixels and 16 log-steps",
             "ms_per_step": round(ms, 3), "algorithmic_bytes": int(algo),
             "achieved_gbs": round(algo / (ms * 1e-3) / 1e9, 1), "hbm_frac": round(algo / (ms * 1e-3) / 1e9 / hbm, 4),
-            "mpix_s": round(N / 1e6 / (ms * 1e-3), 1)}
+            "mpix_s": round(N / 1e6 / (ms * 1e-3), 1),
+            "graphed": {"path": "diff97.GraphedRDStep (the same step captured in one CUDA graph)",
+                        "ms_per_step": round(ms_graph, 3),
+                        "achieved_gbs": round(algo / (ms_graph * 1e-3) / 1e9, 1),
+                        "hbm_frac": round(algo / (ms_graph * 1e-3) / 1e9 / hbm, 4)}}
 
 
 def bench_batched(n, flush):

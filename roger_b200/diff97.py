@@ -258,3 +258,36 @@ def rd_loss_and_grads(x, log_steps, levels=5, lam=0.01, seed=0, chunk=None):
         gx[i:i + chunk] = forward_adjoint_residual(g_y, d, levels, alpha=alpha)
         gls += g_ls
     return loss, gx, gls
+
+
+class GraphedRDStep:
+    """One rate-distortion step (loss, its gradient with respect to the pixels and the log-steps)
+    captured once in a CUDA graph and replayed: a step is then one graph launch, with no
+    per-kernel host work.  The inputs are static: write new pixels or log-steps into `x` and
+    `log_steps` (in place) before calling; the results are the tensors `loss`, `x.grad` and
+    `log_steps.grad`, overwritten by every call.  Capture warms up first (library scratch,
+    autograd) on a side stream, as CUDA-graph capture requires."""
+
+    def __init__(self, x, log_steps, levels=5, lam=0.01, seed=0, warmup=3):
+        if not (x.is_cuda and x.requires_grad and log_steps.requires_grad):
+            raise ValueError("GraphedRDStep: x and log_steps must be CUDA tensors that require grad")
+        self.x, self.log_steps = x, log_steps
+        args = (levels, lam, seed)
+        side = torch.cuda.Stream(device=x.device)
+        side.wait_stream(torch.cuda.current_stream(x.device))
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                x.grad = None
+                log_steps.grad = None
+                rd_loss(x, log_steps, *args).backward()
+        torch.cuda.current_stream(x.device).wait_stream(side)
+        x.grad = None
+        log_steps.grad = None
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.loss = rd_loss(x, log_steps, *args)
+            self.loss.backward()
+
+    def __call__(self):
+        self.graph.replay()
+        return self.loss

@@ -163,3 +163,22 @@ def test_kept_noise_matches_regenerated_noise(D):
     a = D.relaxed_quant_backward(y, g, ls, L, seed, 0.01, noise=u)
     b = D.relaxed_quant_backward(y, g, ls, L, seed, 0.01)
     assert torch.equal(a[0], b[0]) and torch.allclose(a[1], b[1], rtol=1e-6, atol=0)
+
+
+def test_graphed_step_matches_eager_step(D):
+    """The CUDA-graph replay of a step gives the eager step's loss and gradients exactly, and
+    follows new inputs written into its static tensors."""
+    L = 3
+    x = torch.from_numpy(synth.float_batch(2, 96, 80, 60)).cuda().requires_grad_(True)
+    ls = torch.full((3 * L + 1,), -4.0, device="cuda", requires_grad=True)
+    step = D.GraphedRDStep(x, ls, L, 0.01, 7)
+    for k in range(2):
+        with torch.no_grad():
+            x.mul_(0.5 + 0.25 * k)
+        loss = step().item()
+        xe = x.detach().clone().requires_grad_(True)
+        le = ls.detach().clone().requires_grad_(True)
+        ref = D.rd_loss(xe, le, L, 0.01, 7)
+        ref.backward()
+        assert loss == ref.item()
+        assert torch.equal(x.grad, xe.grad) and torch.equal(ls.grad, le.grad)
