@@ -165,6 +165,10 @@ typedef struct {
     int cbw, cbh;      /* code-block size (default 64x64) */
     int order;         /* J2K_ORDER_* (default T800) */
     const float* steps;/* lossy: 3*levels+1 steps; NULL = 8*2^-level */
+    size_t target_bytes; /* 0: every coding pass kept; else the codestream is cut to at most this many
+                            bytes by rate-distortion optimised truncation of the code-blocks (PCRD-opt:
+                            bit-plane truncation points, one quality layer).  No counterpart in the
+                            reference, which writes no codestream. */
 } j2k_enc_params;
 
 j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_encoder** out);

@@ -807,6 +807,7 @@ int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient,
                 }
             }
         npasses += 1;
+        if (info && nbps - 1 - p < 32) info->plane_bytes[nbps - 1 - p] = e.bp + 1;
         for (int y = 0; y < ch; ++y)
             for (int x = 0; x < cw; ++x) FLAG(&t, x, y) &= (uint8_t)~F_VIS;
     }
@@ -909,9 +910,17 @@ int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orie
         for (int y = 0; y < ch; ++y)
             for (int x = 0; x < cw; ++x) FLAG(&t, x, y) &= (uint8_t)~F_VIS;
     }
+    /* a block cut at the end of a bit-plane above the last one: significant magnitudes are
+     * reconstructed at the middle of the interval their undecoded low bits leave */
+    uint32_t half = 0;
+    if (npasses < 3 * numbps - 2 && (npasses - 1) % 3 == 0) {
+        const int plast = numbps - 1 - (npasses - 1) / 3;
+        half = plast > 0 ? 1u << (plast - 1) : 0u;
+    }
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x) {
             int32_t m = (int32_t)mag[y * cw + x];
+            if (FLAG(&t, x, y) & F_SIG) m += (int32_t)half;
             coeff[(size_t)y * pitch + x] = (FLAG(&t, x, y) & F_NEG) ? -m : m;
         }
     free(mag);
@@ -1362,4 +1371,21 @@ double or_rd_loss_f64(const double* x, size_t w, size_t h, int levels, const dou
     free(xh);
     free(gy);
     return loss;
+}
+
+void or_t1_plane_distortion(const int32_t* coeff, size_t pitch, int cw, int ch, int numbps, double dist[33]) {
+    for (int k = 0; k < 33; ++k) dist[k] = 0.0;
+    for (int y = 0; y < ch; ++y)
+        for (int x = 0; x < cw; ++x) {
+            const int32_t v = coeff[(size_t)y * pitch + x];
+            const uint64_t m = v < 0 ? (uint64_t)(-(int64_t)v) : (uint64_t)v;
+            dist[32] += (double)m * (double)m;
+            for (int k = 0; k < numbps && k < 32; ++k) {
+                const int p = numbps - 1 - k;
+                const uint64_t hi = (m >> p) << p;
+                const uint64_t rec = hi ? hi + ((1ull << p) >> 1) : 0;
+                const double e = (double)m - (double)rec;
+                dist[k] += e * e;
+            }
+        }
 }

@@ -98,7 +98,18 @@ typedef struct {
     int npasses;  /* 3*numbps-2, or 0 */
     int length;   /* codeword bytes */
     int nsyms;    /* number of MQ symbols coded */
+    /* bytes the coder had produced (bytes 0..bp, the last one still open to a carry) when the
+     * cleanup pass of bit-plane k (k = 0 for the most significant) ended */
+    int plane_bytes[32];
 } or_t1_info;
+/* Bytes kept when a code-block is truncated after the cleanup pass of bit-plane k (npasses =
+ * 3k+1): the bytes produced so far plus OR_TRUNC_EXTRA more of the finished codeword (what the MQ
+ * decoder reads ahead of the encoder), never more than the whole codeword. */
+#define OR_TRUNC_EXTRA 4
+/* Squared reconstruction error of one code-block when it is decoded down to bit-plane k only
+ * (dist[k], k = 0 .. numbps-1, k = 0 the most significant; magnitudes below the last decoded
+ * plane reconstructed at the middle of their interval), and with nothing decoded (dist[32]). */
+void or_t1_plane_distortion(const int32_t* coeff, size_t pitch, int cw, int ch, int numbps, double dist[33]);
 /* Encodes one code-block.  coeff: cw x ch int32 values (two's complement) at row pitch `pitch`.
  * out: capacity `cap` bytes.  syms (optional, capacity sym_cap): one byte per MQ symbol,
  * context label in bits 0-4 and the decision in bit 7, in coding order.  Returns the codeword

@@ -51,6 +51,7 @@ def lib():
             "or_encode_image": [P, S, S, I, P, P, C.c_long],
             "or_philox_uniform": [C.c_uint64, C.c_uint64],
             "or_rd_noise": [C.c_uint64, S, S, S],
+            "or_t1_plane_distortion": [P, S, I, I, I, P],
             "or_rd_loss_f64": [P, S, S, I, P, D, C.c_uint64, P, P],
         }
         for name, args in sig.items():
@@ -72,7 +73,8 @@ def _p(a):
 
 
 class T1Info(C.Structure):
-    _fields_ = [("numbps", C.c_int), ("npasses", C.c_int), ("length", C.c_int), ("nsyms", C.c_int)]
+    _fields_ = [("numbps", C.c_int), ("npasses", C.c_int), ("length", C.c_int), ("nsyms", C.c_int),
+                ("plane_bytes", C.c_int * 32)]
 
 
 class EncParams(C.Structure):
@@ -188,7 +190,8 @@ def t1_encode(block, orient, want_symbols=False):
                            C.byref(info))
     if n < 0:
         raise RuntimeError("oracle t1 encode overflow")
-    d = dict(numbps=info.numbps, npasses=info.npasses, length=info.length, nsyms=info.nsyms)
+    d = dict(numbps=info.numbps, npasses=info.npasses, length=info.length, nsyms=info.nsyms,
+             plane_bytes=list(info.plane_bytes[:info.numbps]))
     if want_symbols:
         return out[:n].tobytes(), d, syms[:info.nsyms].copy()
     return out[:n].tobytes(), d
@@ -236,3 +239,21 @@ def rd_loss(x, levels, log_steps, lam, seed, grads=True):
     gl = np.empty_like(ls) if grads else None
     loss = lib().or_rd_loss_f64(_p(x), w, h, levels, _p(ls), lam, seed, _p(gx), _p(gl))
     return (loss, gx, gl) if grads else loss
+
+
+TRUNC_EXTRA = 4
+
+
+def truncation_length(info, k):
+    """Codeword bytes kept when the block is cut after bit-plane k (npasses = 3k+1)."""
+    if k >= info["numbps"] - 1:
+        return info["length"]
+    return min(info["length"], info["plane_bytes"][k] + TRUNC_EXTRA)
+
+
+def plane_distortion(block, numbps):
+    block = np.ascontiguousarray(block, np.int32)
+    ch, cw = block.shape
+    out = np.zeros(33, np.float64)
+    lib().or_t1_plane_distortion(_p(block), cw, cw, ch, numbps, _p(out))
+    return out

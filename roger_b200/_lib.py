@@ -29,7 +29,7 @@ assert CB_DESC.itemsize == 24
 
 class EncParams(C.Structure):
     _fields_ = [("levels", C.c_int), ("cbw", C.c_int), ("cbh", C.c_int), ("order", C.c_int),
-                ("steps", C.c_void_p)]
+                ("steps", C.c_void_p), ("target_bytes", C.c_size_t)]
 
 
 J2K_MAX_BANDS = 97

@@ -222,9 +222,9 @@ def bpc_decode(descs, data, w, h, levels, cbw=64, cbh=64, ctx=None, out=None):
 # Reference-shaped classes
 # ---------------------------------------------------------------------------------------------
 
-def _params(levels, cbw, cbh, order, steps):
+def _params(levels, cbw, cbh, order, steps, target_bytes=0):
     keep, sp = _steps_arg(steps, levels) if steps is not None else (None, None)
-    p = L.EncParams(levels, cbw, cbh, order, sp)
+    p = L.EncParams(levels, cbw, cbh, order, sp, int(target_bytes))
     return p, keep
 
 
@@ -261,20 +261,23 @@ class OCLEncoder(OCLEncodeDecode):
             pass
 
     def run(self, components, w, h, levels, precision=8, cbw=64, cbh=64, order=L.ORDER_T800,
-            steps=None):
+            steps=None, target_bytes=0):
         """Reference signature: planar host components (numpy int16/int32/float32, already
-        level-shifted by -128, as src/OCLTest.cpp:80-90 builds them)."""
+        level-shifted by -128, as src/OCLTest.cpp:80-90 builds them).  target_bytes > 0 cuts the
+        codestream to at most that many bytes (PCRD-opt rate control)."""
         comps = [np.ascontiguousarray(c) for c in components]
         dt = {np.dtype(np.int16): L.I16, np.dtype(np.int32): L.I32, np.dtype(np.float32): L.F32}[comps[0].dtype]
         arr = (C.c_void_p * len(comps))(*[c.ctypes.data for c in comps])
-        p, keep = _params(levels, cbw, cbh, order, steps)
+        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes)
         hh = self.ctx._bind()
         check(lib().j2k_encoder_run(self.h, arr, len(comps), dt, w, h, levels, precision, C.byref(p)), hh)
         self.w, self.h_, self.ncomp, self.levels = w, h, len(comps), levels
         return self
 
-    def run_rgb(self, img, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None):
-        """Interleaved uint8 image, (H, W, C) or (H, W); numpy (host) or CUDA tensor."""
+    def run_rgb(self, img, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None, target_bytes=0):
+        """Interleaved uint8 image, (H, W, C) or (H, W); numpy (host) or CUDA tensor.
+        target_bytes > 0 cuts the codestream to at most that many bytes (PCRD-opt rate control:
+        bit-plane truncation points of every code-block chosen on their rate-distortion hulls)."""
         if isinstance(img, torch.Tensor) and img.is_cuda:
             t = img.contiguous()
             ptr, on_dev = t.data_ptr(), 1
@@ -287,7 +290,7 @@ class OCLEncoder(OCLEncodeDecode):
             hgt, wid = a.shape[0], a.shape[1]
             nc = 1 if a.ndim == 2 else a.shape[2]
             keep_img = a
-        p, keep = _params(levels, cbw, cbh, order, steps)
+        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes)
         hh = self.ctx._bind()
         check(lib().j2k_encoder_run_interleaved(self.h, C.c_void_p(ptr), on_dev, wid * nc, nc, wid, hgt,
                                                 C.byref(p)), hh)

@@ -83,6 +83,8 @@ struct j2k_encoder {
     bool have_result = false;
     bool packed_ok = false;  // the packed codewords of the current result are on the device
     size_t packed_total = 0;
+    size_t target_bytes = 0;  // rate control: codestream budget (0 = keep every pass)
+    DevBuf rate_pb, rate_dist;
     void* mapped = nullptr;
 };
 
@@ -129,6 +131,55 @@ static j2k_status check_params(j2k_ctx* ctx, const j2k_enc_params* p, size_t w, 
 }
 
 // DWT of every component + tier-1 of all blocks.  planes: ncomp planes (int32 or float).
+// PCRD-opt truncation of the current tier-1 result to the encoder's byte budget: per-block
+// bit-plane byte positions and distortions come from the tier-1 rate path; the chosen passes
+// and lengths are written back into the device descriptors, which the packing and the
+// codestream writer then follow.  The codestream size (headers included) is checked by writing
+// its headers, and the codeword budget lowered by any excess.
+static j2k_status rate_control(j2k_encoder* e) {
+    j2k_ctx* ctx = e->ctx;
+    const size_t n = e->njobs;
+    std::vector<j2k_cb_desc> d(n);
+    std::vector<uint32_t> pb(n * 32);
+    std::vector<double> dist(n * 33);
+    J2K_CUDA(ctx, cudaMemcpyAsync(d.data(), e->descs.p, n * sizeof(j2k_cb_desc), cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaMemcpyAsync(pb.data(), e->rate_pb.p, n * 32 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaMemcpyAsync(dist.data(), e->rate_dist.p, n * 33 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const int kernel = e->lossy ? J2K_W97 : J2K_W53;
+    const int nb = 3 * e->levels + 1;
+    std::vector<double> gain(nb), w(n);
+    for (int b = 0; b < nb; ++b) {
+        gain[b] = j2k_band_gain(kernel, e->levels, b);
+        if (e->lossy) gain[b] *= (double)e->steps[b] * e->steps[b];
+    }
+    for (size_t i = 0; i < n; ++i) w[i] = gain[e->hjobs[i].band];
+    const std::vector<j2k_cb_desc> full = d;
+    size_t maxlen = 0;
+    for (const auto& x : full) maxlen = std::max(maxlen, (size_t)std::max(x.length, 0));
+    std::vector<uint8_t> zeros(maxlen + 1, 0);
+    size_t budget = e->target_bytes;
+    for (int it = 0; it < 6; ++it) {
+        d = full;
+        j2k_pcrd_truncate(d.data(), n, pb.data(), dist.data(), w.data(), budget);
+        std::vector<j2k_t2_block> blocks(n);
+        for (size_t i = 0; i < n; ++i) blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, zeros.data()};
+        const size_t size = j2k_t2_write(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
+                                         e->mct != J2K_MCT_NONE, e->steps.data(), blocks).size();
+        if (size <= e->target_bytes) break;
+        const size_t excess = size - e->target_bytes + 16;
+        if (budget <= excess) {
+            budget = 0;
+            if (it > 0) break;
+        } else {
+            budget -= excess;
+        }
+    }
+    J2K_CUDA(ctx, cudaMemcpyAsync(e->descs.p, d.data(), n * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));
+    J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return J2K_OK;
+}
+
 static j2k_status encode_planes(j2k_encoder* e) {
     j2k_ctx* ctx = e->ctx;
     const size_t n = e->w * e->h;
@@ -163,11 +214,19 @@ static j2k_status encode_planes(j2k_encoder* e) {
         J2K_TRY(e->descs.ensure(ctx, std::max<size_t>(e->njobs, 1) * sizeof(j2k_cb_desc)));
         J2K_TRY(e->bytes.ensure(ctx, std::max<size_t>(e->njobs, 1) * e->cap));
         J2K_TRY(j2k_clear_device_error(ctx));
+        uint32_t* pb = nullptr;
+        double* dist = nullptr;
+        if (e->target_bytes) {
+            J2K_TRY(e->rate_pb.ensure(ctx, e->njobs * 32 * 4 + 16));
+            J2K_TRY(e->rate_dist.ensure(ctx, e->njobs * 33 * 8 + 16));
+            pb = (uint32_t*)e->rate_pb.p;
+            dist = (double*)e->rate_dist.p;
+        }
         J2K_TRY(j2k_t1_encode_jobs(ctx, (const int32_t*)e->coef.p, (const j2k_cb_job*)e->jobs.p,
                                    e->njobs, (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p,
-                                   e->njobs * e->sym_cap, nullptr, ctx->stream));
+                                   e->njobs * e->sym_cap, nullptr, ctx->stream, pb, dist));
         j2k_status s = j2k_read_device_error(ctx);
-        if (s == J2K_OK) return J2K_OK;
+        if (s == J2K_OK) return e->target_bytes ? rate_control(e) : J2K_OK;
         if (s != J2K_ERR_CAPACITY) return s;
         // grow whichever capacity overflowed and retry
         if (ctx->err.find("symbol") != std::string::npos) e->sym_cap = align16(e->sym_cap * 2);
@@ -293,6 +352,7 @@ static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const
     J2K_TRY(check_params(ctx, p, w, h, &levels, &cbw, &cbh, &order));
     if (ncomp != 1 && ncomp != 3)
         return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "encoder supports 1 or 3 components");
+    e->target_bytes = p ? p->target_bytes : 0;
     e->w = w;
     e->h = h;
     e->ncomp = ncomp;

@@ -141,9 +141,26 @@ j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in,
 
 // Tier-1 encode of njobs blocks.  order (device, optional): phase-A processing order (largest
 // first); sym_bytes: size of the symbol scratch the jobs' sym_off/sym_cap address.
+// plane_bytes (njobs x 32) and dist (njobs x 33), both device, optional: when given, the MQ coder
+// records the bytes produced at every bit-plane end and the distortion of every truncation point
+// is computed (rate control).
 j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_job* d_jobs, size_t njobs,
                               j2k_cb_desc* descs, uint8_t* bytes, size_t sym_bytes,
-                              const uint32_t* d_order, cudaStream_t st);
+                              const uint32_t* d_order, cudaStream_t st, uint32_t* plane_bytes = nullptr,
+                              double* dist = nullptr);
+
+// ---- rate control (PCRD-opt, rate.cpp) -----------------------------------------------------
+// Squared-norm gain of the synthesis basis of subband b (QCD order) for the 5/3 or 9/7 inverse
+// with `levels` levels: an error e in that band's coefficients costs gain * e^2 in the image.
+double j2k_band_gain(int kernel, int levels, int band);
+// Truncation choice per code-block for a codeword budget: for block i (numbps nb, codeword
+// length len, bit-plane byte positions pb[32], distortions d[33] as from the tier-1 rate path,
+// weight w = band gain (* step^2 when lossy)), picks npasses in {0, 1, 4, ..., 3nb-2} and the
+// kept length so that the total kept bytes stay within budget and the weighted distortion is
+// as low as the convex hulls allow.  Writes descs[i].npasses and descs[i].length.
+void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
+                       const double* weight, size_t budget);
+constexpr int J2K_TRUNC_EXTRA = 4;  // bytes kept beyond those produced at a plane end
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
                               cudaStream_t st);

@@ -329,9 +329,20 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
         decode_block(S, &zc_lut[0][0][0][0], bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch,
                      blk, pitch);
     __syncwarp();
+    // a block cut at the end of a bit-plane above the last one (rate control): significant
+    // magnitudes are reconstructed at the middle of the interval their undecoded bits leave
+    int32_t half = 0;
+    if (D.npasses < 3 * D.numbps - 2 && (D.npasses - 1) % 3 == 0) {
+        const int plast = D.numbps - 1 - (D.npasses - 1) / 3;
+        half = plast > 0 ? 1 << (plast - 1) : 0;
+    }
     for (int r = 0; r < ch; ++r)
-        for (int x = lane; x < cw; x += 32)
-            if ((S.neg[r + 1] >> x) & 1) blk[(size_t)r * pitch + x] = -blk[(size_t)r * pitch + x];
+        for (int x = lane; x < cw; x += 32) {
+            int32_t v = blk[(size_t)r * pitch + x];
+            if ((S.sig[r + 1] >> x) & 1) v += half;
+            if ((S.neg[r + 1] >> x) & 1) v = -v;
+            blk[(size_t)r * pitch + x] = v;
+        }
 }
 
 }  // namespace

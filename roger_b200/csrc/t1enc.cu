@@ -554,11 +554,14 @@ struct MqEnc {
     }
 };
 
-template <int LANES>
+// RATE: also record, for every bit-plane k, the bytes produced (bp + 1) when its cleanup pass
+// ends (pass 3k; pass ends in symbols from phase A) into plane_bytes[job * 32 + k].
+template <int LANES, bool RATE = false>
 __global__ void __launch_bounds__(kMqThreads)
 t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jobs, const uint32_t* __restrict__ nsyms,
              const uint32_t* __restrict__ order, int njobs, uint8_t* __restrict__ bytes,
-              j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+              j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err,
+              const uint32_t* __restrict__ pend = nullptr, uint32_t* __restrict__ plane_bytes = nullptr) {
     __shared__ uint32_t tab[47];
     __shared__ uint32_t cst[19 * kMqThreads];
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
@@ -600,6 +603,20 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
     uint4 c1 = nchunks > 1 ? __ldcs(sp4 + 1) : z4;
     int cx = min((int)(c0.x & 31), 18);
     uint32_t ent = st[cx * kMqThreads];
+    // RATE bookkeeping: next cleanup pass (3 * kp) and the symbol count at which it ends
+    int kp = 0, npass = 0;
+    uint32_t next_end = 0xFFFFFFFFu;
+    const uint32_t* pe = nullptr;
+    if (RATE) {
+        npass = descs[jid].npasses;
+        pe = pend + (size_t)jid * 92;
+        next_end = npass > 0 ? pe[0] : 0xFFFFFFFFu;
+        while (next_end == 0u) {  // passes with no symbols at all
+            plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);
+            ++kp;
+            next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
+        }
+    }
     for (int k = 0; k < nchunks; ++k) {
         const uint4 cur = c0;
         c0 = c1;
@@ -633,6 +650,14 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
                 e.renorm(__clz(e.A) - 16);
                 cx = ncx;
                 ent = nent;
+                if (RATE) {
+                    const uint32_t done = (uint32_t)(16 * k + j + 1);
+                    while (done == next_end) {
+                        if (kp < 32) plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);
+                        ++kp;
+                        next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
+                    }
+                }
             }
         }
     }
@@ -824,11 +849,67 @@ __global__ void iota_kernel(uint32_t* v, int n) {
     if (i < n) v[i] = (uint32_t)i;
 }
 
+// Squared reconstruction error of every code-block when decoded down to bit-plane k only
+// (dist[job * 33 + k]; magnitudes below the last decoded plane at the middle of their interval)
+// and with nothing decoded (dist[job * 33 + 32]).  One warp per block; exact 64-bit integer sums
+// in a fixed order, so the truncation choices built on them are deterministic.  A sample of
+// magnitude m with top bit b contributes m^2 to every plane above b (bucketed, prefix-summed at
+// the end) and its exact midpoint error to the planes at and below b.
+__global__ void __launch_bounds__(64)
+t1_dist_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__ jobs,
+               const j2k_cb_desc* __restrict__ descs, int njobs, double* __restrict__ dist) {
+    __shared__ unsigned long long acc[2][32][33], bucket[2][32][33];  // [warp][plane or bit][lane]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int jid = blockIdx.x * 2 + w;
+    if (jid >= njobs) return;
+    const j2k_cb_job J = jobs[jid];
+    const int nb = min((int)descs[jid].numbps, 31);
+    for (int k = 0; k < 32; ++k) acc[w][k][lane] = bucket[w][k][lane] = 0ull;
+    if (J.cw <= 64 && J.ch <= 64) {
+        for (int y = 0; y < J.ch; ++y) {
+            const int32_t* row = coeff + J.off + (size_t)y * J.pitch;
+            for (int x = lane; x < J.cw; x += 32) {
+                const int32_t v = row[x];
+                const uint32_t m = v < 0 ? (uint32_t)(-(int64_t)v) : (uint32_t)v;
+                if (!m) continue;
+                const int b = 31 - __clz(m);
+                bucket[w][b][lane] += (unsigned long long)m * m;
+                for (int p = min(b, nb - 1); p >= 0; --p) {
+                    const uint32_t hi = (m >> p) << p;
+                    const int64_t e = (int64_t)m - (int64_t)(hi + ((1u << p) >> 1));
+                    acc[w][nb - 1 - p][lane] += (unsigned long long)(e * e);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        unsigned long long bsum[32], total = 0;
+        for (int b = 0; b < 32; ++b) {
+            unsigned long long s2 = 0;
+            for (int l = 0; l < 32; ++l) s2 += bucket[w][b][l];
+            bsum[b] = s2;
+            total += s2;
+        }
+        double* d = dist + (size_t)jid * 33;
+        for (int k = 0; k < 32; ++k) {
+            unsigned long long s2 = 0;
+            if (k < nb) {
+                for (int l = 0; l < 32; ++l) s2 += acc[w][k][l];
+                const int p = nb - 1 - k;
+                for (int b = 0; b < p && b < 32; ++b) s2 += bsum[b];  // samples still below plane p
+            }
+            d[k] = (double)s2;
+        }
+        d[32] = (double)total;
+    }
+}
+
 }  // namespace
 
 j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_job* d_jobs, size_t njobs,
                               j2k_cb_desc* descs, uint8_t* bytes, size_t sym_bytes,
-                              const uint32_t* d_order, cudaStream_t st) {
+                              const uint32_t* d_order, cudaStream_t st, uint32_t* plane_bytes, double* dist) {
     if (njobs == 0) return J2K_OK;
     if (((uintptr_t)bytes & 15) != 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "t1: bytes buffer must be 16-byte aligned");
@@ -870,6 +951,16 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     const int lanes = ctx->mq_lanes;  // active lanes (blocks) per warp: 32, 16 or 8
     const size_t per_cta = (size_t)lanes * (kMqThreads / 32);
     unsigned gb = (unsigned)((njobs + per_cta - 1) / per_cta);
+    if (plane_bytes && dist) {
+        // rate control: byte positions at every bit-plane end, and the distortion of each
+        // truncation point (the coefficients are still in place)
+        t1_mq_kernel<8, true><<<(unsigned)((njobs + 15) / 16), kMqThreads, 0, st>>>(
+            syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err, pend, plane_bytes);
+        J2K_CUDA(ctx, cudaGetLastError());
+        t1_dist_kernel<<<(unsigned)((njobs + 1) / 2), 64, 0, st>>>(coeff, d_jobs, descs, (int)njobs, dist);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
     if (lanes == 8)
         t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
     else if (lanes == 16)

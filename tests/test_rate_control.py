@@ -1,0 +1,94 @@
+"""Rate control (PCRD-opt truncation of the code-blocks to a byte budget, one quality layer).
+
+CPU: the truncation rule (bytes produced at the end of a bit-plane + 4) decodes every kept pass
+exactly as the whole codeword does, and the per-plane distortions behave.  GPU: codestreams cut
+to a target are within it, decode through OpenJPEG and through this library's GPU decoder,
+whose output is identical to the oracle's decode of the same codestream, and quality rises with
+the budget up to lossless."""
+import io
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from roger_b200 import synth
+
+
+def _blocks(img, L, cb):
+    co = O.dwt53_fwd(img.astype(np.int32) - 128, L)
+    h, w = img.shape
+    for (x0, y0, sw, sh, o, lv) in O.subbands(w, h, L):
+        for by in range(y0, y0 + sh, cb):
+            for bx in range(x0, x0 + sw, cb):
+                yield o, co[by:min(by + cb, y0 + sh), bx:min(bx + cb, x0 + sw)]
+
+
+def test_truncated_codewords_decode_like_whole_ones():
+    img = synth.gray(192, 160, 7)
+    n = 0
+    for o, blk in _blocks(img, 4, 32):
+        data, info = O.t1_encode(blk, o)
+        nb = info["numbps"]
+        for k in range(nb):
+            L = O.truncation_length(info, k)
+            assert L <= info["length"]
+            a = O.t1_decode(data[:L], nb, 3 * k + 1, o, blk.shape[1], blk.shape[0])
+            b = O.t1_decode(data, nb, 3 * k + 1, o, blk.shape[1], blk.shape[0])
+            assert np.array_equal(a, b)
+            n += 1
+    assert n > 100
+
+
+def test_plane_distortion_decreases_to_zero():
+    img = synth.gray(128, 128, 8)
+    for o, blk in _blocks(img, 3, 32):
+        data, info = O.t1_encode(blk, o)
+        nb = info["numbps"]
+        d = O.plane_distortion(blk, nb)
+        assert d[32] == float((blk.astype(np.float64) ** 2).sum())
+        if nb:
+            assert all(d[k + 1] <= d[k] for k in range(nb - 1))
+            assert d[0] <= d[32] and d[nb - 1] == 0.0
+
+
+def _psnr(a, b):
+    e = a.astype(np.float64) - b.astype(np.float64)
+    mse = float((e * e).mean())
+    return float("inf") if mse == 0 else 10 * np.log10(255.0 ** 2 / mse)
+
+
+def _oracle_decode(cs):
+    from roger_b200 import codec as C
+    info, descs, data = C.read_codestream(cs)
+    w, h, nc, L = info["w"], info["h"], info["ncomp"], info["levels"]
+    planes = np.zeros((nc, h, w), np.int32)
+    for d in descs:
+        if d["npasses"] == 0:
+            continue
+        blk = O.t1_decode(bytes(data[d["offset"]:d["offset"] + d["length"]]), int(d["numbps"]),
+                          int(d["npasses"]), int(d["orient"]), int(d["cw"]), int(d["ch"]))
+        planes[d["comp"], d["y0"]:d["y0"] + d["ch"], d["x0"]:d["x0"] + d["cw"]] = blk
+    rec = np.stack([O.dwt53_inv(p, L) for p in planes])
+    return O.planar_inv(rec, 1 if nc == 3 else 0).reshape(h, w, nc)
+
+
+@pytest.mark.gpu
+def test_rate_controlled_codestreams():
+    from PIL import Image
+    from roger_b200 import codec as C
+    img = synth.rgb(384, 256, (31, 32, 33, 34))
+    enc = C.OCLEncoder(lossy=False)
+    full = len(enc.run_rgb(img, levels=5, cbw=32, cbh=32).codestream())
+    last = -1.0
+    for frac in (0.03, 0.1, 0.3, 0.6):
+        target = int(full * frac)
+        cs = bytes(enc.run_rgb(img, levels=5, cbw=32, cbh=32, target_bytes=target).codestream())
+        assert 0.8 * target <= len(cs) <= target
+        ours = C.decode_codestream(cs).reshape(img.shape)
+        assert np.array_equal(ours, _oracle_decode(cs).reshape(img.shape))
+        theirs = np.asarray(Image.open(io.BytesIO(cs))).reshape(img.shape)
+        p_ours, p_theirs = _psnr(ours, img), _psnr(theirs, img)
+        assert p_ours > last and abs(p_ours - p_theirs) < 1.0
+        last = p_ours
+    cs = bytes(enc.run_rgb(img, levels=5, cbw=32, cbh=32, target_bytes=10 * full).codestream())
+    assert np.array_equal(C.decode_codestream(cs).reshape(img.shape), img)
