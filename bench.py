@@ -347,6 +347,7 @@ def main():
     if world == 1 and size == W and args.extras:
         line["lossless_decode"] = bench_lossless_decode(img_h, res)
         line["lossy"] = bench_lossy(img_h, img_d, flush)
+        line["rate_control"] = bench_rate_control(img_d, img_h, flush)
     if args.batch_images and world == 1:
         line["batched"] = bench_batched(args.batch_images, flush)
     if args.diff and world == 1:
@@ -418,6 +419,42 @@ def bench_lossy(img_h, img_d, flush, levels=6):
             "ms_per_step": round(ms, 3), "mpix_s": round(w * h / 1e6 / (ms * 1e-3), 1),
             "codeword_bytes": int(data.size if hasattr(data, "size") else len(data)),
             "psnr_db": round(psnr, 3)}
+
+
+def bench_rate_control(img_d, img_h, flush, bpp=1.0):
+    """Rate control on config 1's image: lossless pipeline (RCT + 5/3 L=6 + tier-1) with the
+    codestream cut to `bpp` bits per pixel by PCRD-opt; encode time with the image resident
+    (tier-1 rate path, distortion pass, host PCRD and the descriptor update included), size and
+    reconstruction PSNR of the GPU decode."""
+    import numpy as np
+    import torch
+    from roger_b200 import codec as C
+    h, w, nc = img_h.shape
+    target = int(w * h * bpp / 8)
+    enc = C.OCLEncoder(lossy=False)
+
+    def step():
+        enc.run_rgb(img_d, levels=LEVELS, cbw=CB, cbh=CB, target_bytes=target)
+    for _ in range(2):
+        step()
+    tt = []
+    for _ in range(5):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        step()
+        e.record()
+        e.synchronize()
+        tt.append(s.elapsed_time(e))
+    ms = statistics.median(tt)
+    cs = bytes(enc.codestream())
+    rec = C.decode_codestream(cs).reshape(img_h.shape)
+    err = rec.astype(np.float64) - img_h.astype(np.float64)
+    mse = float((err * err).mean())
+    return {"workload": f"config-1 image, lossless pipeline cut to {bpp} bpp ({target} bytes) by PCRD-opt",
+            "ms_per_step": round(ms, 3), "mpix_s": round(w * h / 1e6 / (ms * 1e-3), 1),
+            "codestream_bytes": len(cs), "psnr_db": round(10 * math.log10(255.0 ** 2 / mse), 3)}
 
 
 def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
