@@ -317,6 +317,11 @@ j2k_status j2k_batch_input(j2k_batch* b, uint8_t** device_buffer, size_t* offset
 /* Encodes the batch.  pixels: per-image pointers (host or device) copied into the input buffer
  * first, or NULL when the caller filled the input buffer itself. */
 j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_device);
+/* Same, without waiting: the copies and the launch sequence are queued on the context's stream
+ * and the device error word is read (and a tier-1 capacity overflow re-run) by the next call
+ * that needs the result (j2k_batch_pack, j2k_batch_get_codeblocks, ...).  Host pixels must stay
+ * valid until the stream has consumed them (page-locked memory makes the copies asynchronous). */
+j2k_status j2k_batch_encode_async(j2k_batch* b, const uint8_t* const* pixels, int on_device);
 j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value);
 j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value);
 /* Times the tile shapes and code-block-to-warp schedules on this batch and keeps the fastest;
@@ -327,6 +332,16 @@ j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report);
 j2k_status j2k_batch_get_codeblocks(j2k_batch* b, int image, j2k_cb_desc* descs, size_t* count,
                                     uint8_t* bytes, size_t cap, size_t* used);
 j2k_status j2k_batch_get_codestream(j2k_batch* b, int image, uint8_t* out, size_t cap, size_t* len);
+/* Bulk readback, for hosts that move whole batches: j2k_batch_pack packs every code-block of the
+ * last result back to back on the device (job order: image by image, each in the layout of
+ * j2k_encoder_get_codeblocks) and returns the total bytes (it waits for the packing sizes);
+ * j2k_batch_read_packed then queues the copies of the descriptors (offsets into the packed
+ * bytes) and the bytes to host buffers on the context's stream, without waiting, so that with
+ * page-locked buffers they overlap other work; j2k_batch_image_jobs gives each image's first
+ * job (n+1 entries, the last = the total count). */
+j2k_status j2k_batch_pack(j2k_batch* b, size_t* total);
+j2k_status j2k_batch_read_packed(j2k_batch* b, j2k_cb_desc* descs, uint8_t* bytes, size_t cap);
+j2k_status j2k_batch_image_jobs(j2k_batch* b, size_t* first);
 
 #ifdef __cplusplus
 }

@@ -98,8 +98,12 @@ SIGS = {
     "j2k_dwt97_forward_adjoint_residual": (I, [P, P, P, P, C.c_float, P, I, S, S, I]),
     "j2k_batch_create": (I, [P, P, I, C.POINTER(P)]),
     "j2k_batch_destroy": (I, [P]),
+    "j2k_batch_pack": (I, [P, C.POINTER(S)]),
+    "j2k_batch_read_packed": (I, [P, P, P, S]),
+    "j2k_batch_image_jobs": (I, [P, C.POINTER(S)]),
     "j2k_batch_input": (I, [P, C.POINTER(P), P]),
     "j2k_batch_encode": (I, [P, P, I]),
+    "j2k_batch_encode_async": (I, [P, P, I]),
     "j2k_batch_set_option": (I, [P, I, I]),
     "j2k_batch_get_option": (I, [P, I, C.POINTER(I)]),
     "j2k_batch_autotune": (I, [P, I, P]),

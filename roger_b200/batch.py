@@ -72,14 +72,19 @@ class BatchEncoder:
                 raise ValueError("images must be all on the host or all on the device")
         return ptrs, on_dev, keep
 
-    def encode(self, images=None):
-        """Encodes the batch; images=None re-encodes what is already in the input buffer."""
+    def encode(self, images=None, wait=True):
+        """Encodes the batch; images=None re-encodes what is already in the input buffer.
+        wait=False queues the work on the current stream and returns at once (the device error
+        word is read by the next call that needs the result); host images must then stay alive
+        until the stream has copied them."""
         hh = self.ctx._bind()
+        fn = lib().j2k_batch_encode if wait else lib().j2k_batch_encode_async
         if images is None:
-            check(lib().j2k_batch_encode(self.h, None, 0), hh)
+            check(fn(self.h, None, 0), hh)
         else:
             ptrs, on_dev, keep = self.load(images)
-            check(lib().j2k_batch_encode(self.h, ptrs, on_dev), hh)
+            self._keep = keep
+            check(fn(self.h, ptrs, on_dev), hh)
         return self
 
     def set_option(self, key, value):
@@ -92,6 +97,50 @@ class BatchEncoder:
         return {"tile53": TILE_NAMES[rep[0]], "tile97": TILE_NAMES[rep[1]],
                 "phase_a_order": "largest-first" if rep[2] else "natural",
                 "mq": ("state+code warp pair" if rep[3] else f"one lane per block, {rep[4]} per warp")}
+
+    def results(self, pinned=True):
+        """Every image's (descs, codeword bytes), read back in one packing pass and two copies
+        (into reused page-locked buffers when pinned; views valid until the next call)."""
+        self.read_async(pinned)
+        torch.cuda.current_stream().synchronize()
+        return self.split()
+
+    def read_async(self, pinned=True):
+        """Packs the results on the device and queues their copy to the host on the current
+        stream without waiting (split() after the stream has finished gives the per-image
+        views).  Waits only for the packed size."""
+        hh = self.ctx._bind()
+        total = C.c_size_t()
+        check(lib().j2k_batch_pack(self.h, C.byref(total)), hh)
+        first = (C.c_size_t * (len(self.desc) + 1))()
+        check(lib().j2k_batch_image_jobs(self.h, first), hh)
+        self._first = [first[i] for i in range(len(self.desc) + 1)]
+        nd, nb = self._first[-1] * L.CB_DESC.itemsize, max(total.value, 1)
+        if pinned:
+            pd, pb = getattr(self, "_pin_d", None), getattr(self, "_pin_b", None)
+            if pd is None or pd.numel() < nd:
+                self._pin_d = pd = torch.empty(nd, dtype=torch.uint8, pin_memory=True)
+            if pb is None or pb.numel() < nb:
+                self._pin_b = pb = torch.empty(nb + nb // 4, dtype=torch.uint8, pin_memory=True)
+            self._d = pd.numpy()[:nd].view(L.CB_DESC)
+            self._b = pb.numpy()
+        else:
+            self._d = np.zeros(self._first[-1], L.CB_DESC)
+            self._b = np.zeros(nb, np.uint8)
+        self._total = total.value
+        check(lib().j2k_batch_read_packed(self.h, self._d.ctypes.data_as(C.c_void_p),
+                                          self._b.ctypes.data_as(C.c_void_p), self._b.size), hh)
+
+    def split(self):
+        out = []
+        for i in range(len(self.desc)):
+            a, b = self._first[i], self._first[i + 1]
+            d = self._d[a:b].copy()
+            base = int(d["offset"][0]) if b > a else 0
+            end = int(d["offset"][-1] + max(int(d["length"][-1]), 0)) if b > a else 0
+            d["offset"] -= base
+            out.append((d, self._b[base:end]))
+        return out
 
     def codeblocks(self, i):
         cnt, used = C.c_size_t(), C.c_size_t()
@@ -109,3 +158,55 @@ class BatchEncoder:
         check(lib().j2k_batch_get_codestream(self.h, i, out.ctypes.data_as(C.c_void_p), out.size, C.byref(n)),
               self.ctx.h)
         return out.tobytes()
+
+
+class PipelinedBatchEncoder:
+    """A batch split into `parts` consecutive groups, each with its own context, batched encoder
+    and CUDA stream, so that one group's host-to-device copies and result read-back overlap the
+    other groups' encoding.  Images come from host memory (page-locked for the copies to be
+    asynchronous: `pin` makes such copies once); results come back in one packed read per group."""
+
+    def __init__(self, images, parts=2, device=0):
+        from .codec import Context
+        self.desc = list(images)
+        self.groups = self.split_groups(self.desc, parts)
+        self.ctxs = [Context(device) for _ in self.groups]
+        self.encs = [BatchEncoder(self.desc[a:b], ctx=c) for (a, b), c in zip(self.groups, self.ctxs)]
+        self.streams = [torch.cuda.Stream(device=device) for _ in self.groups]
+
+    @staticmethod
+    def split_groups(descs, parts):
+        """Consecutive [a, b) index ranges, at most `parts`, none empty, of about equal samples."""
+        n = len(descs)
+        if n == 0:
+            return []
+        parts = max(1, min(parts, n))
+        px = np.cumsum([d["w"] * d["h"] * d["ncomp"] for d in descs])
+        cuts = [0] + [int(np.searchsorted(px, px[-1] * k / parts)) + 1 for k in range(1, parts)] + [n]
+        cuts = sorted(set(min(max(c, 0), n) for c in cuts))
+        return [(cuts[k], cuts[k + 1]) for k in range(len(cuts) - 1) if cuts[k + 1] > cuts[k]]
+
+    @staticmethod
+    def pin(images):
+        """Page-locked host copies of numpy images (made once, outside any timed region)."""
+        out = []
+        for im in images:
+            t = torch.from_numpy(np.ascontiguousarray(im)).pin_memory()
+            out.append(t.numpy())
+        return out
+
+    def encode(self, images):
+        """images: host arrays in batch order (page-locked for overlap).  Returns every image's
+        (descs, codeword bytes)."""
+        for (a, b), enc, s in zip(self.groups, self.encs, self.streams):
+            with torch.cuda.stream(s):
+                enc.encode(images[a:b], wait=False)
+        for enc, s in zip(self.encs, self.streams):
+            with torch.cuda.stream(s):
+                enc.read_async(pinned=True)
+        for s in self.streams:
+            s.synchronize()
+        out = []
+        for enc in self.encs:
+            out.extend(enc.split())
+        return out

@@ -17,6 +17,8 @@
 #include <new>
 #include <numeric>
 
+#include <cub/cub.cuh>
+
 #include "j2k_internal.cuh"
 
 namespace {
@@ -85,8 +87,35 @@ struct j2k_batch {
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;  // capture stream (the caller's may be the legacy stream)
     bool have_result = false;
+    bool pending = false;  // enqueued by j2k_batch_encode_async, device error word not read yet
     std::string err;
+    // packed results (j2k_batch_pack): every block's codeword back to back, in job order
+    Buf plens, poffs, ptmp, packed, pdescs;
+    size_t packed_total = 0;
 };
+
+namespace {
+__global__ void batch_lengths_kernel(const j2k_cb_desc* __restrict__ d, uint32_t* __restrict__ len, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) len[i] = (uint32_t)max(d[i].length, 0);
+}
+// one warp per block: codeword to its packed offset, descriptor with the packed offset
+__global__ void batch_pack_kernel(const j2k_cb_desc* __restrict__ d, const uint32_t* __restrict__ off,
+                                  const uint8_t* __restrict__ src, uint8_t* __restrict__ dst,
+                                  j2k_cb_desc* __restrict__ out, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const int len = max(d[w].length, 0);
+    const uint8_t* a = src + d[w].offset;
+    uint8_t* b = dst + off[w];
+    for (int k = lane; k < len; k += 32) b[k] = a[k];
+    if (lane == 0) {
+        j2k_cb_desc x = d[w];
+        x.offset = off[w];
+        out[w] = x;
+    }
+}
+}  // namespace
 
 static void drop_graph(j2k_batch* b) {
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -419,10 +448,12 @@ j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
     return J2K_OK;
 }
 
-j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
+j2k_status j2k_batch_encode_async(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
     if (!b) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
+    b->have_result = false;
+    b->pending = false;
     if (pixels) {
         for (size_t i = 0; i < b->img.size(); ++i) {
             const ImgPlan& im = b->img[i];
@@ -431,9 +462,21 @@ j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_d
                                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
         }
     }
+    J2K_TRY(j2k_clear_device_error(ctx));
+    J2K_TRY(run_once(b));
+    b->pending = true;
+    return J2K_OK;
+}
+
+}  // extern "C"
+
+// Reads the device error word of a pending run (one stream synchronisation); a capacity
+// overflow grows the tier-1 buffers and re-runs from the input still on the device.
+static j2k_status batch_finish(j2k_batch* b) {
+    if (!b->pending) return J2K_OK;
+    j2k_ctx* ctx = b->ctx;
+    b->pending = false;
     for (int attempt = 0; attempt < 6; ++attempt) {
-        J2K_TRY(j2k_clear_device_error(ctx));
-        J2K_TRY(run_once(b));
         j2k_status s = j2k_read_device_error(ctx);
         if (s == J2K_OK) {
             b->have_result = true;
@@ -443,8 +486,17 @@ j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_d
         if (ctx->err.find("symbol") != std::string::npos) b->sym_factor *= 2; else b->out_factor *= 2;
         drop_graph(b);
         J2K_TRY(layout_t1(b));
+        J2K_TRY(j2k_clear_device_error(ctx));
+        J2K_TRY(run_once(b));
     }
     return j2k_fail(ctx, J2K_ERR_CAPACITY, "tier-1 capacities kept overflowing");
+}
+
+extern "C" {
+
+j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
+    J2K_TRY(j2k_batch_encode_async(b, pixels, on_device));
+    return batch_finish(b);
 }
 
 // Times each candidate on this batch (CUDA events around the stage it affects) and keeps the
@@ -454,6 +506,7 @@ j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report) {
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
     reps = std::max(reps, 1);
+    J2K_TRY(batch_finish(b));
     const bool graph = b->use_graph;
     b->use_graph = false;
     drop_graph(b);
@@ -521,6 +574,7 @@ j2k_status j2k_batch_get_codeblocks(j2k_batch* b, int image, j2k_cb_desc* descs,
                                     uint8_t* bytes, size_t cap, size_t* used) {
     if (!b || !count || image < 0 || image >= (int)b->img.size()) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
+    J2K_TRY(batch_finish(b));
     if (!b->have_result) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no batch result yet");
     const ImgPlan& im = b->img[image];
     std::vector<j2k_cb_desc> d(im.njobs);
@@ -565,6 +619,61 @@ j2k_status j2k_batch_get_codestream(j2k_batch* b, int image, uint8_t* out, size_
     if (!out) return J2K_OK;
     if (cap < cs.size()) return j2k_fail(b->ctx, J2K_ERR_CAPACITY, "codestream buffer too small");
     std::memcpy(out, cs.data(), cs.size());
+    return J2K_OK;
+}
+
+}  // extern "C"
+
+
+extern "C" {
+
+j2k_status j2k_batch_pack(j2k_batch* b, size_t* total) {
+    if (!b || !total) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    J2K_TRY(batch_finish(b));
+    if (!b->have_result) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no batch result yet");
+    const int n = (int)b->hjobs.size();
+    cudaStream_t st = ctx->stream;
+    J2K_TRY(b->plens.ensure(ctx, (size_t)(n + 1) * 4));
+    J2K_TRY(b->poffs.ensure(ctx, (size_t)(n + 1) * 4));
+    J2K_TRY(b->pdescs.ensure(ctx, (size_t)std::max(n, 1) * sizeof(j2k_cb_desc)));
+    batch_lengths_kernel<<<(n + 255) / 256, 256, 0, st>>>((const j2k_cb_desc*)b->descs.p, (uint32_t*)b->plens.p, n);
+    J2K_CUDA(ctx, cudaMemsetAsync((uint32_t*)b->plens.p + n, 0, 4, st));
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, (uint32_t*)b->plens.p, (uint32_t*)b->poffs.p, n + 1, st);
+    J2K_TRY(b->ptmp.ensure(ctx, tmp + 16));
+    J2K_CUDA(ctx, cub::DeviceScan::ExclusiveSum(b->ptmp.p, tmp, (uint32_t*)b->plens.p, (uint32_t*)b->poffs.p,
+                                                n + 1, st));
+    uint32_t tot = 0;
+    J2K_CUDA(ctx, cudaMemcpyAsync(&tot, (uint32_t*)b->poffs.p + n, 4, cudaMemcpyDeviceToHost, st));
+    J2K_CUDA(ctx, cudaStreamSynchronize(st));
+    J2K_TRY(b->packed.ensure(ctx, (size_t)tot + 16));
+    batch_pack_kernel<<<(unsigned)(((size_t)n * 32 + 255) / 256), 256, 0, st>>>(
+        (const j2k_cb_desc*)b->descs.p, (const uint32_t*)b->poffs.p, (const uint8_t*)b->bytes.p,
+        (uint8_t*)b->packed.p, (j2k_cb_desc*)b->pdescs.p, n);
+    J2K_CUDA(ctx, cudaGetLastError());
+    b->packed_total = tot;
+    *total = tot;
+    return J2K_OK;
+}
+
+j2k_status j2k_batch_read_packed(j2k_batch* b, j2k_cb_desc* descs, uint8_t* bytes, size_t cap) {
+    if (!b || !descs || !bytes) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = b->ctx;
+    if (cap < b->packed_total) return j2k_fail(ctx, J2K_ERR_CAPACITY, "bytes buffer smaller than the packed total");
+    cudaSetDevice(ctx->device);
+    J2K_CUDA(ctx, cudaMemcpyAsync(descs, b->pdescs.p, b->hjobs.size() * sizeof(j2k_cb_desc), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    if (b->packed_total)
+        J2K_CUDA(ctx, cudaMemcpyAsync(bytes, b->packed.p, b->packed_total, cudaMemcpyDeviceToHost, ctx->stream));
+    return J2K_OK;
+}
+
+j2k_status j2k_batch_image_jobs(j2k_batch* b, size_t* first) {
+    if (!b || !first) return J2K_ERR_INVALID_ARG;
+    for (size_t i = 0; i < b->img.size(); ++i) first[i] = b->img[i].job0;
+    first[b->img.size()] = b->hjobs.size();
     return J2K_OK;
 }
 

@@ -96,3 +96,40 @@ def test_bad_descriptor_is_rejected():
         BatchEncoder([dict(w=64, h=64, ncomp=2, kernel=53, levels=3, cb=64)])
     with pytest.raises(J2KError):
         BatchEncoder([dict(w=64, h=64, ncomp=1, kernel=53, levels=3, cb=48)])
+
+
+def _same_blocks(got, be):
+    assert len(got) == len(be.desc)
+    for i, (d, b) in enumerate(got):
+        rd, rb = be.codeblocks(i)
+        assert np.array_equal(d, rd), f"image {i}: descriptors differ"
+        assert np.array_equal(np.asarray(b), rb), f"image {i}: codeword bytes differ"
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_bulk_results_match_per_image_codeblocks(batch_and_images, pinned):
+    be, descs, imgs = batch_and_images
+    be.encode(imgs)
+    _same_blocks(be.results(pinned=pinned), be)
+
+
+def test_async_encode_is_read_by_the_pack(batch_and_images):
+    be, descs, imgs = batch_and_images
+    be.encode(imgs)
+    ref = [(d.copy(), np.array(b)) for d, b in be.results()]
+    be.encode(imgs, wait=False)
+    got = be.results()
+    for (d, b), (rd, rb) in zip(got, ref):
+        assert np.array_equal(d, rd) and np.array_equal(np.asarray(b), rb)
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3])
+def test_pipelined_encoder_matches_the_single_batch(batch_and_images, parts):
+    from roger_b200.batch import PipelinedBatchEncoder
+    be, descs, imgs = batch_and_images
+    be.encode(imgs)
+    pe = PipelinedBatchEncoder(descs, parts=parts)
+    assert [a for a, _ in pe.groups][0] == 0 and pe.groups[-1][1] == len(descs)
+    pinned = PipelinedBatchEncoder.pin(imgs)
+    for _ in range(2):  # the second call replays every group's graph
+        _same_blocks(pe.encode(pinned), be)
