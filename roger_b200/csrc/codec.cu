@@ -139,12 +139,16 @@ static j2k_status check_params(j2k_ctx* ctx, const j2k_enc_params* p, size_t w, 
 static j2k_status rate_control(j2k_encoder* e) {
     j2k_ctx* ctx = e->ctx;
     const size_t n = e->njobs;
-    std::vector<j2k_cb_desc> d(n);
-    std::vector<uint32_t> pb(n * 32);
-    std::vector<double> dist(n * 33);
-    J2K_CUDA(ctx, cudaMemcpyAsync(d.data(), e->descs.p, n * sizeof(j2k_cb_desc), cudaMemcpyDeviceToHost, ctx->stream));
-    J2K_CUDA(ctx, cudaMemcpyAsync(pb.data(), e->rate_pb.p, n * 32 * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    J2K_CUDA(ctx, cudaMemcpyAsync(dist.data(), e->rate_dist.p, n * 33 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    // descriptors, plane-end byte counts and distortions through the context's page-locked
+    // staging buffer (the input copy it held is complete: the error word was read after it)
+    uint8_t* hp = (uint8_t*)j2k_pinned(ctx, n * (33 * 8 + 32 * 4 + sizeof(j2k_cb_desc)) + 64);
+    if (!hp) return J2K_ERR_OUT_OF_MEMORY;
+    double* dist = (double*)hp;
+    uint32_t* pb = (uint32_t*)(dist + n * 33);
+    j2k_cb_desc* dh = (j2k_cb_desc*)(pb + n * 32);
+    J2K_CUDA(ctx, cudaMemcpyAsync(dh, e->descs.p, n * sizeof(j2k_cb_desc), cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaMemcpyAsync(pb, e->rate_pb.p, n * 32 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaMemcpyAsync(dist, e->rate_dist.p, n * 33 * 8, cudaMemcpyDeviceToHost, ctx->stream));
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     const int kernel = e->lossy ? J2K_W97 : J2K_W53;
     const int nb = 3 * e->levels + 1;
@@ -154,18 +158,15 @@ static j2k_status rate_control(j2k_encoder* e) {
         if (e->lossy) gain[b] *= (double)e->steps[b] * e->steps[b];
     }
     for (size_t i = 0; i < n; ++i) w[i] = gain[e->hjobs[i].band];
-    const std::vector<j2k_cb_desc> full = d;
-    size_t maxlen = 0;
-    for (const auto& x : full) maxlen = std::max(maxlen, (size_t)std::max(x.length, 0));
-    std::vector<uint8_t> zeros(maxlen + 1, 0);
+    std::vector<j2k_cb_desc> d(n);
+    std::vector<j2k_t2_block> blocks(n);
     size_t budget = e->target_bytes;
     for (int it = 0; it < 6; ++it) {
-        d = full;
-        j2k_pcrd_truncate(d.data(), n, pb.data(), dist.data(), w.data(), budget);
-        std::vector<j2k_t2_block> blocks(n);
-        for (size_t i = 0; i < n; ++i) blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, zeros.data()};
-        const size_t size = j2k_t2_write(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
-                                         e->mct != J2K_MCT_NONE, e->steps.data(), blocks).size();
+        std::memcpy(d.data(), dh, n * sizeof(j2k_cb_desc));
+        j2k_pcrd_truncate(d.data(), n, pb, dist, w.data(), budget);
+        for (size_t i = 0; i < n; ++i) blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, nullptr};
+        const size_t size = j2k_t2_size(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
+                                        e->mct != J2K_MCT_NONE, e->steps.data(), blocks);
         if (size <= e->target_bytes) break;
         const size_t excess = size - e->target_bytes + 16;
         if (budget <= excess) {
@@ -175,7 +176,8 @@ static j2k_status rate_control(j2k_encoder* e) {
             budget -= excess;
         }
     }
-    J2K_CUDA(ctx, cudaMemcpyAsync(e->descs.p, d.data(), n * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));
+    std::memcpy(dh, d.data(), n * sizeof(j2k_cb_desc));
+    J2K_CUDA(ctx, cudaMemcpyAsync(e->descs.p, dh, n * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return J2K_OK;
 }

@@ -158,8 +158,8 @@ double j2k_band_gain(int kernel, int levels, int band);
 // weight w = band gain (* step^2 when lossy)), picks npasses in {0, 1, 4, ..., 3nb-2} and the
 // kept length so that the total kept bytes stay within budget and the weighted distortion is
 // as low as the convex hulls allow.  Writes descs[i].npasses and descs[i].length.
-void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
-                       const double* weight, size_t budget);
+extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
+                                  const double* weight, size_t budget);
 constexpr int J2K_TRUNC_EXTRA = 4;  // bytes kept beyond those produced at a plane end
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
@@ -173,3 +173,6 @@ struct j2k_t2_block {
 std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
                                   int lossless, int mct, const float* steps,
                                   const std::vector<j2k_t2_block>& blocks);
+// Size in bytes of the codestream j2k_t2_write would produce (block data is not read).
+size_t j2k_t2_size(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
+                   const float* steps, const std::vector<j2k_t2_block>& blocks);

@@ -9,10 +9,13 @@
 // interval.  Distortions are squared errors in coefficient units, weighted by the squared norm
 // of the subband's synthesis basis (and the step squared for quantised coefficients), so that
 // blocks of different bands compare in image units.  Each block's points are reduced to their
-// lower convex hull; a bisection on the slope lambda keeps, in every block, the last hull point
-// whose rate-distortion slope is at least lambda.
+// lower convex hull; over all hull segments in order of decreasing slope, those before the first
+// one that no longer fits the budget are kept (a threshold on the slope, found by a weighted
+// selection), so that every block keeps a prefix of its hull.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <limits>
 #include <vector>
 
 #include "j2k_internal.cuh"
@@ -83,73 +86,103 @@ double j2k_band_gain(int kernel, int levels, int band) {
     return o == 0 ? gh * gl : (o == 1 ? gl * gh : gh * gh);
 }
 
-void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
-                       const double* weight, size_t budget) {
-    struct Pt {
-        double L, D;
-        int np;
-    };
-    std::vector<std::vector<Pt>> hull(n);
+extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
+                                  const double* weight, size_t budget) {
+    // hull points of every block, flat: block i owns [first[i], first[i+1]) (scratch kept per
+    // thread between calls)
+    static thread_local std::vector<double> HL, HD;
+    static thread_local std::vector<uint8_t> HN;
+    static thread_local std::vector<size_t> first;
+    HL.clear();
+    HD.clear();
+    HN.clear();
+    first.assign(n + 1, 0);
+    double base = 0.0;  // bytes of every hull's first point (L = 0)
     for (size_t i = 0; i < n; ++i) {
         const j2k_cb_desc& d = descs[i];
         const int nb = d.numbps;
         const double w = weight[i];
-        std::vector<Pt> pts;
-        pts.push_back({0.0, dist[i * 33 + 32] * w, 0});
+        double pl[33], pd[33];
+        int pn[33], m = 0;
+        pl[m] = 0.0, pd[m] = dist[i * 33 + 32] * w, pn[m++] = 0;
         for (int k = 0; k < nb && k < 31; ++k) {
             const int np = 3 * k + 1;
             if (np > d.npasses) break;
-            double L = k == nb - 1 ? (double)d.length
-                                   : std::min<double>(d.length, (double)plane_bytes[i * 32 + k] + J2K_TRUNC_EXTRA);
-            pts.push_back({L, dist[i * 33 + k] * w, np});
+            pl[m] = k == nb - 1 ? (double)d.length
+                                : std::min<double>(d.length, (double)plane_bytes[i * 32 + k] + J2K_TRUNC_EXTRA);
+            pd[m] = dist[i * 33 + k] * w;
+            pn[m++] = np;
         }
         // lower convex hull in (L, D): slopes (D drop per byte) strictly decreasing
-        std::vector<Pt> h;
-        for (const Pt& p : pts) {
-            if (!h.empty() && p.L <= h.back().L) {  // no extra bytes: keep the better point
-                if (p.D < h.back().D) h.back() = p;
+        double hl[33], hd[33];
+        int hn[33], h = 0;
+        for (int q = 0; q < m; ++q) {
+            if (h && pl[q] <= hl[h - 1]) {  // no extra bytes: keep the better point
+                if (pd[q] < hd[h - 1]) hl[h - 1] = pl[q], hd[h - 1] = pd[q], hn[h - 1] = pn[q];
                 continue;
             }
-            if (!h.empty() && p.D >= h.back().D) continue;  // no improvement
-            while (h.size() >= 2) {
-                const Pt& a = h[h.size() - 2];
-                const Pt& b = h.back();
-                const double s1 = (a.D - b.D) / (b.L - a.L), s2 = (b.D - p.D) / (p.L - b.L);
-                if (s2 >= s1) h.pop_back();
-                else break;
-            }
-            h.push_back(p);
+            if (h && pd[q] >= hd[h - 1]) continue;  // no improvement
+            // drop the last hull point while the new point's slope is not below its slope
+            // (cross-multiplied: both byte differences are positive)
+            while (h >= 2 && (hd[h - 1] - pd[q]) * (hl[h - 1] - hl[h - 2]) >=
+                                 (hd[h - 2] - hd[h - 1]) * (pl[q] - hl[h - 1]))
+                --h;
+            hl[h] = pl[q], hd[h] = pd[q], hn[h++] = pn[q];
         }
-        hull[i].swap(h);
+        first[i] = HL.size();
+        base += hl[0];
+        for (int q = 0; q < h; ++q) HL.push_back(hl[q]), HD.push_back(hd[q]), HN.push_back((uint8_t)hn[q]);
     }
-    auto choose = [&](double lam, std::vector<int>* pick) {
-        double total = 0.0;
-        for (size_t i = 0; i < n; ++i) {
-            const std::vector<Pt>& h = hull[i];
-            size_t j = 0;
-            while (j + 1 < h.size() && (h[j].D - h[j + 1].D) / (h[j + 1].L - h[j].L) >= lam) ++j;
-            if (pick) (*pick)[i] = (int)j;
-            total += h[j].L;
-        }
-        return total;
+    first[n] = HL.size();
+    // every hull segment (slope, extra bytes); a block's segments have decreasing slopes, so
+    // keeping the segments of slope above a threshold keeps a prefix of every hull
+    struct Seg {
+        double s, dl;
     };
-    std::vector<int> pick(n, 0);
-    double lo = 0.0, hi = 1.0;
-    if (choose(0.0, nullptr) <= (double)budget) {
-        choose(0.0, &pick);
-    } else {
-        while (choose(hi, nullptr) > (double)budget && hi < 1e300) hi *= 16.0;
-        for (int it = 0; it < 200; ++it) {
-            const double mid = 0.5 * (lo + hi);
-            if (choose(mid, nullptr) > (double)budget) lo = mid;
-            else hi = mid;
+    static thread_local std::vector<Seg> seg;
+    seg.clear();
+    double all = base;
+    for (size_t i = 0; i < n; ++i)
+        for (size_t q = first[i] + 1; q < first[i + 1]; ++q) {
+            const double dl = HL[q] - HL[q - 1];
+            seg.push_back({(HD[q - 1] - HD[q]) / dl, dl});
+            all += dl;
         }
-        choose(hi, &pick);
+    // Threshold: in the order of decreasing slope, the slope of the first segment that no longer
+    // fits the budget; segments of that slope or less are dropped (ties together).  Found by a
+    // weighted quickselect, linear in the number of segments on average.
+    double thr = -1.0;  // keep everything
+    if (all > (double)budget) {
+        double room = (double)budget - base;
+        size_t a = 0, b = seg.size();
+        uint64_t rng = 0x9E3779B97F4A7C15ull;
+        thr = std::numeric_limits<double>::infinity();
+        while (a < b) {
+            rng ^= rng << 13, rng ^= rng >> 7, rng ^= rng << 17;
+            const double piv = seg[a + rng % (b - a)].s;
+            // [a, g): slope > piv, [g, e): slope == piv, [e, b): slope < piv
+            auto g = std::partition(seg.begin() + a, seg.begin() + b, [piv](const Seg& x) { return x.s > piv; });
+            auto e = std::partition(g, seg.begin() + b, [piv](const Seg& x) { return x.s == piv; });
+            double sg = 0.0, se = 0.0;
+            for (auto it = seg.begin() + a; it != g; ++it) sg += it->dl;
+            if (sg > room) {
+                b = (size_t)(g - seg.begin());
+                continue;
+            }
+            room -= sg;
+            for (auto it = g; it != e; ++it) se += it->dl;
+            if (se > room) {
+                thr = piv;
+                break;
+            }
+            room -= se;
+            a = (size_t)(e - seg.begin());
+        }
     }
     for (size_t i = 0; i < n; ++i) {
-        const Pt& p = hull[i][pick[i]];
-        descs[i].npasses = (uint8_t)p.np;
-        descs[i].length = (int32_t)p.L;
-        if (p.np == 0) descs[i].length = 0;
+        size_t q = first[i];
+        while (q + 1 < first[i + 1] && (HD[q] - HD[q + 1]) / (HL[q + 1] - HL[q]) > thr) ++q;
+        descs[i].npasses = HN[q];
+        descs[i].length = HN[q] ? (int32_t)HL[q] : 0;
     }
 }

@@ -131,11 +131,12 @@ void put_npasses(BitWriter& bw, int n) {  // Table B.4
 
 }  // namespace
 
-// blocks: component-major, then subbands in QCD order, then raster order within each subband
-// (exactly the order of j2k_build_jobs).
-std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
-                                  int lossless, int mct, const float* steps,
-                                  const std::vector<j2k_t2_block>& blocks) {
+namespace {
+
+// Writes the codestream into `o`; without bodies only the markers and packet headers are
+// written and the returned size still counts every block's codeword bytes.
+size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
+               const float* steps, const std::vector<j2k_t2_block>& blocks, bool bodies) {
     const int nb = 3 * levels + 1;
     std::vector<j2k_band_rect> rects(nb);
     j2k_band_rects(w, h, levels, rects.data());
@@ -175,7 +176,9 @@ std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int
         G = std::max(G, maxbps[b] - eps[b] + 1);
     }
     G = std::min(G, 7);
-    Bytes o;
+    size_t body = 0;
+    for (const auto& b : blocks) body += (size_t)std::max(b.length, 0);
+    o.v.reserve(256 + (size_t)nb * 4 + blocks.size() * 10 + (bodies ? body : 0));
     o.u16(0xFF4F);  // SOC
     o.u16(0xFF51);  // SIZ
     o.u16((uint32_t)(38 + 3 * ncomp));
@@ -260,17 +263,38 @@ std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int
             bw.flush();
             // the header of the NEXT packet needs the band's Lblock state only within this
             // packet: with one layer every block appears at most once, so no state is kept.
-            for (int q = 0; q < bcount; ++q)
-                for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
-                    o.v.insert(o.v.end(), blocks[i].data, blocks[i].data + blocks[i].length);
+            if (bodies)
+                for (int q = 0; q < bcount; ++q)
+                    for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
+                        o.v.insert(o.v.end(), blocks[i].data, blocks[i].data + blocks[i].length);
         }
-    uint32_t psot = (uint32_t)(o.v.size() - sot);
+    const size_t extra = bodies ? 0 : body;
+    uint32_t psot = (uint32_t)(o.v.size() + extra - sot);
     o.v[sot + 6] = (uint8_t)(psot >> 24);
     o.v[sot + 7] = (uint8_t)(psot >> 16);
     o.v[sot + 8] = (uint8_t)(psot >> 8);
     o.v[sot + 9] = (uint8_t)psot;
     o.u16(0xFFD9);  // EOC
-    return o.v;
+    return o.v.size() + extra;
+}
+
+}  // namespace
+
+// blocks: component-major, then subbands in QCD order, then raster order within each subband
+// (exactly the order of j2k_build_jobs).
+std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
+                                  int lossless, int mct, const float* steps,
+                                  const std::vector<j2k_t2_block>& blocks) {
+    Bytes o;
+    t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, true);
+    return std::move(o.v);
+}
+
+size_t j2k_t2_size(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
+                   const float* steps, const std::vector<j2k_t2_block>& blocks) {
+    static thread_local Bytes o;
+    o.v.clear();
+    return t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, false);
 }
 
 // ---- tier-2 reading (codestream parser) -----------------------------------------------------

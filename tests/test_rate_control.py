@@ -92,3 +92,88 @@ def test_rate_controlled_codestreams():
         last = p_ours
     cs = bytes(enc.run_rgb(img, levels=5, cbw=32, cbh=32, target_bytes=10 * full).codestream())
     assert np.array_equal(C.decode_codestream(cs).reshape(img.shape), img)
+
+
+def _pcrd_reference(desc, pb, dist, w, budget, extra=4):
+    """Plain restatement of the truncation choice: convex hulls, then the hull segments in order
+    of decreasing slope are kept until the first that does not fit; that slope and lower go."""
+    hulls = []
+    for i, d in enumerate(desc):
+        nb, npas, ln = int(d["numbps"]), int(d["npasses"]), int(d["length"])
+        pts = [(0.0, dist[i, 32] * w[i], 0)]
+        for k in range(min(nb, 31)):
+            np_ = 3 * k + 1
+            if np_ > npas:
+                break
+            L = float(ln) if k == nb - 1 else min(float(ln), float(pb[i, k]) + extra)
+            pts.append((L, dist[i, k] * w[i], np_))
+        h = []
+        for p in pts:
+            if h and p[0] <= h[-1][0]:
+                if p[1] < h[-1][1]:
+                    h[-1] = p
+                continue
+            if h and p[1] >= h[-1][1]:
+                continue
+            while len(h) >= 2:
+                a, b = h[-2], h[-1]
+                if (b[1] - p[1]) * (b[0] - a[0]) >= (a[1] - b[1]) * (p[0] - b[0]):
+                    h.pop()
+                else:
+                    break
+            h.append(p)
+        hulls.append(h)
+    segs = sorted(((h[q - 1][1] - h[q][1]) / (h[q][0] - h[q - 1][0]), h[q][0] - h[q - 1][0])
+                  for h in hulls for q in range(1, len(h)))[::-1]
+    thr, room = -1.0, float(budget)
+    if sum(s[1] for s in segs) > budget:
+        for s, dl in segs:
+            if dl > room:
+                thr = s
+                break
+            room -= dl
+    out = []
+    for h in hulls:
+        q = 0
+        while q + 1 < len(h) and (h[q][1] - h[q + 1][1]) / (h[q + 1][0] - h[q][0]) > thr:
+            q += 1
+        out.append((h[q][2], int(h[q][0]) if h[q][2] else 0))
+    return out
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_pcrd_selection_matches_sorted_threshold(seed):
+    import ctypes as C
+    from roger_b200 import _lib
+    f = C.CDLL(_lib.LIB_PATH).j2k_pcrd_truncate
+    f.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
+    f.restype = None
+    rng = np.random.default_rng(seed)
+    n = 700
+    desc = np.zeros(n, _lib.CB_DESC)
+    pb = np.zeros((n, 32), np.uint32)
+    dist = np.zeros((n, 33))
+    for i in range(n):
+        nb = int(rng.integers(0, 14))
+        desc[i]["numbps"] = nb
+        desc[i]["npasses"] = max(3 * nb - 2, 0)
+        steps = rng.integers(0, 400, nb)
+        cum = np.cumsum(steps)
+        pb[i, :nb] = cum
+        desc[i]["length"] = int(cum[-1]) + 3 if nb else 0
+        d = np.sort(rng.exponential(1e6, nb + 1))[::-1]
+        d[-1] = 0.0
+        dist[i, 32] = d[0] if nb else 0.0
+        dist[i, :nb] = d[1:]
+        if nb and rng.random() < 0.1:  # a plane that adds bytes but lowers nothing
+            k = int(rng.integers(0, nb))
+            dist[i, k] = dist[i, 32] if k == 0 else dist[i, k - 1]
+    w = rng.uniform(0.1, 3.0, n)
+    full = int(desc["length"].sum())
+    for frac in (0.0, 0.05, 0.3, 0.8, 1.2):
+        budget = int(full * frac)
+        d2 = desc.copy()
+        f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget)
+        ref = _pcrd_reference(desc, pb, dist, w, budget)
+        assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == ref
+        assert int(d2["length"].sum()) <= min(budget, full)
