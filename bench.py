@@ -579,33 +579,50 @@ def bench_batched(n, flush):
         else:
             same97 &= ok
     # host to host: page-locked host images in, every code-block's codeword back in page-locked
-    # host memory (one packing pass per group); one group, then groups on their own streams so
-    # that copies overlap the other groups' encoding
-    from roger_b200.batch import PipelinedBatchEncoder
-    host = PipelinedBatchEncoder.pin([im.cpu().numpy() for im in imgs])
+    # host memory (one packing pass per batch).  One batch at a time (copies, encode, copies),
+    # then a stream of batches with the next batch's upload and the previous batch's read-back
+    # overlapping the current encode (steady-state time per batch).
+    from roger_b200.batch import StreamingBatchEncoder
+    host = StreamingBatchEncoder.pin([im.cpu().numpy() for im in imgs])
     in_bytes = sum(h.nbytes for h in host)
-    h2h = {}
-    ref_bulk = None
-    for parts in (1, 2, 4):
-        pe = PipelinedBatchEncoder(be.desc, parts=parts)
-        for (a, b), g in zip(pe.groups, pe.encs):
-            g.encode(host[a:b])
-            g.autotune(reps=1)
-        for _ in range(3):
-            res = pe.encode(host)
-        t = ev(lambda: pe.encode(host), 5)
-        out_bytes = sum(int(np.asarray(b).size) + d.nbytes for d, b in res)
-        if ref_bulk is None:
-            ref_bulk = [(d.copy(), np.array(b)) for d, b in res]
-            same = all(np.array_equal(d, be.codeblocks(i)[0]) and np.array_equal(np.asarray(b), be.codeblocks(i)[1])
-                       for i, (d, b) in enumerate(res))
-        else:
-            same = all(np.array_equal(d, rd) and np.array_equal(np.asarray(b), rb)
-                       for (d, b), (rd, rb) in zip(res, ref_bulk))
-        h2h[f"groups_{len(pe.groups)}"] = {"ms": round(t, 3), "mpix_s": round(mpix / (t * 1e-3), 1),
-                                          "h2d_bytes": in_bytes, "d2h_bytes": out_bytes,
-                                          "identical_to_batched": bool(same)}
-        del pe
+    se = StreamingBatchEncoder(be.desc, depth=2)
+    se.autotune(host)
+
+    def one_batch():
+        be.encode(host)
+        return be.results(pinned=True)
+
+    for _ in range(3):
+        res = one_batch()
+    t_seq = ev(one_batch, 5)
+    out_bytes = sum(int(np.asarray(b).size) + d.nbytes for d, b in res)
+    same_seq = all(np.array_equal(d, be.codeblocks(i)[0]) and np.array_equal(np.asarray(b), be.codeblocks(i)[1])
+                   for i, (d, b) in enumerate(res))
+    nstream = 8
+    for _ in se.run([host] * 3):
+        pass
+    tt = []
+    same_stream = True
+    for _ in range(3):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for k, r in enumerate(se.run([host] * nstream)):
+            if k == nstream - 1:
+                last = r
+        s1.record()
+        s1.synchronize()
+        tt.append(s0.elapsed_time(s1) / nstream)
+    for i, (d, b) in enumerate(last):
+        rd, rb = be.codeblocks(i)
+        same_stream &= np.array_equal(d, rd) and np.array_equal(np.asarray(b), rb)
+    t_stream = statistics.median(tt)
+    h2h = {"h2d_bytes_per_batch": in_bytes, "d2h_bytes_per_batch": out_bytes,
+           "one_batch": {"ms": round(t_seq, 3), "mpix_s": round(mpix / (t_seq * 1e-3), 1),
+                         "identical_to_batched": bool(same_seq)},
+           "streamed": {"batches": nstream, "ms_per_batch": round(t_stream, 3),
+                        "mpix_s": round(mpix / (t_stream * 1e-3), 1), "identical_to_batched": bool(same_stream)}}
     return {"workload": f"{n} images, w,h log-uniform [64,2048], 50% RGB, 5/3 even / 9/7 odd, L=3..5, "
                         "32x32|64x64 code-blocks (seed 300)",
             "host_to_host": h2h,

@@ -322,6 +322,9 @@ j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_d
  * that needs the result (j2k_batch_pack, j2k_batch_get_codeblocks, ...).  Host pixels must stay
  * valid until the stream has consumed them (page-locked memory makes the copies asynchronous). */
 j2k_status j2k_batch_encode_async(j2k_batch* b, const uint8_t* const* pixels, int on_device);
+/* Only the copies of j2k_batch_encode (queued on the context's stream), for callers that upload
+ * on a copy stream and encode with pixels = NULL on another. */
+j2k_status j2k_batch_upload(j2k_batch* b, const uint8_t* const* pixels, int on_device);
 j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value);
 j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value);
 /* Times the tile shapes and code-block-to-warp schedules on this batch and keeps the fastest;

@@ -104,6 +104,7 @@ SIGS = {
     "j2k_batch_input": (I, [P, C.POINTER(P), P]),
     "j2k_batch_encode": (I, [P, P, I]),
     "j2k_batch_encode_async": (I, [P, P, I]),
+    "j2k_batch_upload": (I, [P, P, I]),
     "j2k_batch_set_option": (I, [P, I, I]),
     "j2k_batch_get_option": (I, [P, I, C.POINTER(I)]),
     "j2k_batch_autotune": (I, [P, I, P]),

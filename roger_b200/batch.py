@@ -87,6 +87,14 @@ class BatchEncoder:
             check(fn(self.h, ptrs, on_dev), hh)
         return self
 
+    def upload(self, images):
+        """Queues only the copies of the images into the input buffer on the current stream."""
+        hh = self.ctx._bind()
+        ptrs, on_dev, keep = self.load(images)
+        self._keep = keep
+        check(lib().j2k_batch_upload(self.h, ptrs, on_dev), hh)
+        return self
+
     def set_option(self, key, value):
         check(lib().j2k_batch_set_option(self.h, key, value), self.ctx.h)
 
@@ -160,53 +168,72 @@ class BatchEncoder:
         return out.tobytes()
 
 
-class PipelinedBatchEncoder:
-    """A batch split into `parts` consecutive groups, each with its own context, batched encoder
-    and CUDA stream, so that one group's host-to-device copies and result read-back overlap the
-    other groups' encoding.  Images come from host memory (page-locked for the copies to be
-    asynchronous: `pin` makes such copies once); results come back in one packed read per group."""
+class StreamingBatchEncoder:
+    """Encodes a stream of batches of one layout (same image shapes and settings) from host
+    memory to host memory, with the copies overlapped: while batch k is encoded (one batched
+    graph on the compute stream), batch k+1's pixels go up on a copy stream and batch k-1's
+    packed code-blocks come back on their own stream.  `depth` batched encoders (each with its
+    own context and device buffers) take turns; in steady state a batch costs the larger of its
+    encode and its copies instead of their sum.  Splitting one batch into groups that take
+    turns does not pay: tier-1 time is set by the longest code-blocks of each launch, so every
+    extra launch adds its own tail.
 
-    def __init__(self, images, parts=2, device=0):
+    Host images should be page-locked (`pin`) for the copies to be asynchronous.  The results
+    of a batch are views into page-locked buffers of its encoder, valid until that encoder's
+    turn comes again (`depth` batches later)."""
+
+    def __init__(self, images, depth=2, device=0):
         from .codec import Context
         self.desc = list(images)
-        self.groups = self.split_groups(self.desc, parts)
-        self.ctxs = [Context(device) for _ in self.groups]
-        self.encs = [BatchEncoder(self.desc[a:b], ctx=c) for (a, b), c in zip(self.groups, self.ctxs)]
-        self.streams = [torch.cuda.Stream(device=device) for _ in self.groups]
-
-    @staticmethod
-    def split_groups(descs, parts):
-        """Consecutive [a, b) index ranges, at most `parts`, none empty, of about equal samples."""
-        n = len(descs)
-        if n == 0:
-            return []
-        parts = max(1, min(parts, n))
-        px = np.cumsum([d["w"] * d["h"] * d["ncomp"] for d in descs])
-        cuts = [0] + [int(np.searchsorted(px, px[-1] * k / parts)) + 1 for k in range(1, parts)] + [n]
-        cuts = sorted(set(min(max(c, 0), n) for c in cuts))
-        return [(cuts[k], cuts[k + 1]) for k in range(len(cuts) - 1) if cuts[k + 1] > cuts[k]]
+        self.depth = max(2, depth)
+        self.encs = [BatchEncoder(self.desc, ctx=Context(device)) for _ in range(self.depth)]
+        self.compute = torch.cuda.Stream(device=device)
+        self.copy = torch.cuda.Stream(device=device)
+        self.out = [torch.cuda.Stream(device=device) for _ in range(self.depth)]
+        self.computed = [None] * self.depth
 
     @staticmethod
     def pin(images):
         """Page-locked host copies of numpy images (made once, outside any timed region)."""
-        out = []
-        for im in images:
-            t = torch.from_numpy(np.ascontiguousarray(im)).pin_memory()
-            out.append(t.numpy())
-        return out
+        return [torch.from_numpy(np.ascontiguousarray(im)).pin_memory().numpy() for im in images]
 
-    def encode(self, images):
-        """images: host arrays in batch order (page-locked for overlap).  Returns every image's
-        (descs, codeword bytes)."""
-        for (a, b), enc, s in zip(self.groups, self.encs, self.streams):
-            with torch.cuda.stream(s):
-                enc.encode(images[a:b], wait=False)
-        for enc, s in zip(self.encs, self.streams):
-            with torch.cuda.stream(s):
-                enc.read_async(pinned=True)
-        for s in self.streams:
-            s.synchronize()
-        out = []
-        for enc in self.encs:
-            out.extend(enc.split())
-        return out
+    def autotune(self, images, reps=1):
+        for e in self.encs:
+            e.encode(images)
+            e.autotune(reps=reps)
+
+    def _start(self, k, images):
+        i = k % self.depth
+        enc = self.encs[i]
+        if self.computed[i] is not None:  # the input buffer is free once its last encode ran
+            self.copy.wait_event(self.computed[i])
+        with torch.cuda.stream(self.copy):
+            enc.upload(images)
+            up = torch.cuda.Event()
+            up.record(self.copy)
+        self.compute.wait_event(up)
+        with torch.cuda.stream(self.compute):
+            enc.encode(None, wait=False)
+            ev = torch.cuda.Event()
+            ev.record(self.compute)
+        self.computed[i] = ev
+
+    def _finish(self, k):
+        i = k % self.depth
+        s = self.out[i]
+        s.wait_event(self.computed[i])
+        with torch.cuda.stream(s):
+            self.encs[i].read_async(pinned=True)
+        s.synchronize()
+        return self.encs[i].split()
+
+    def run(self, batches):
+        """batches: iterable of lists of host images (batch order).  Yields, per batch in order,
+        every image's (descs, codeword bytes)."""
+        k = -1
+        for k, images in enumerate(batches):
+            self._start(k, images)
+            if k >= 1:
+                yield self._finish(k - 1)
+        if k >= 0:
+            yield self._finish(k)

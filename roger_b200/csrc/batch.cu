@@ -448,20 +448,27 @@ j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
     return J2K_OK;
 }
 
+j2k_status j2k_batch_upload(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
+    if (!b || !pixels) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    for (size_t i = 0; i < b->img.size(); ++i)
+        if (!pixels[i]) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "pixel pointer is NULL");
+    for (size_t i = 0; i < b->img.size(); ++i) {
+        const ImgPlan& im = b->img[i];
+        J2K_CUDA(ctx, cudaMemcpyAsync((uint8_t*)b->in.p + im.in_off, pixels[i], im.n * im.d.ncomp,
+                                      on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return J2K_OK;
+}
+
 j2k_status j2k_batch_encode_async(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
     if (!b) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
     b->have_result = false;
     b->pending = false;
-    if (pixels) {
-        for (size_t i = 0; i < b->img.size(); ++i) {
-            const ImgPlan& im = b->img[i];
-            if (!pixels[i]) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "pixel pointer is NULL");
-            J2K_CUDA(ctx, cudaMemcpyAsync((uint8_t*)b->in.p + im.in_off, pixels[i], im.n * im.d.ncomp,
-                                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
-        }
-    }
+    if (pixels) J2K_TRY(j2k_batch_upload(b, pixels, on_device));
     J2K_TRY(j2k_clear_device_error(ctx));
     J2K_TRY(run_once(b));
     b->pending = true;

@@ -123,13 +123,26 @@ def test_async_encode_is_read_by_the_pack(batch_and_images):
         assert np.array_equal(d, rd) and np.array_equal(np.asarray(b), rb)
 
 
-@pytest.mark.parametrize("parts", [1, 2, 3])
-def test_pipelined_encoder_matches_the_single_batch(batch_and_images, parts):
-    from roger_b200.batch import PipelinedBatchEncoder
+@pytest.mark.parametrize("depth", [2, 3])
+def test_streaming_encoder_matches_the_single_batch(batch_and_images, depth):
+    from roger_b200.batch import StreamingBatchEncoder
     be, descs, imgs = batch_and_images
     be.encode(imgs)
-    pe = PipelinedBatchEncoder(descs, parts=parts)
-    assert [a for a, _ in pe.groups][0] == 0 and pe.groups[-1][1] == len(descs)
-    pinned = PipelinedBatchEncoder.pin(imgs)
-    for _ in range(2):  # the second call replays every group's graph
-        _same_blocks(pe.encode(pinned), be)
+    se = StreamingBatchEncoder(descs, depth=depth)
+    pinned = StreamingBatchEncoder.pin(imgs)
+    flipped = StreamingBatchEncoder.pin([np.ascontiguousarray(im[::-1]) for im in imgs])
+    ref_flip = BatchEncoderRef(descs, flipped)
+    seq = [pinned, flipped, pinned, pinned, flipped]
+    n = 0
+    for k, res in enumerate(se.run(seq)):
+        want = be if seq[k] is pinned else ref_flip
+        _same_blocks(res, want)
+        n += 1
+    assert n == len(seq)
+
+
+def BatchEncoderRef(descs, imgs):
+    from roger_b200.batch import BatchEncoder
+    b = BatchEncoder(descs)
+    b.encode(imgs)
+    return b
