@@ -169,6 +169,10 @@ typedef struct {
                             bytes by rate-distortion optimised truncation of the code-blocks (PCRD-opt:
                             bit-plane truncation points, one quality layer).  No counterpart in the
                             reference, which writes no codestream. */
+    int layers;          /* > 1: that many quality layers, cut by PCRD-opt to layer_bytes[l] bytes of
+                            codestream for layers 0..l (non-decreasing; 0 in the last place keeps
+                            every pass: a lossless final layer); target_bytes is then unused */
+    const size_t* layer_bytes;
 } j2k_enc_params;
 
 j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_encoder** out);
@@ -213,8 +217,8 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs
                                       uint8_t* out, int out_on_device, size_t out_pitch_bytes);
 
 /* ---- codestream reading (tier-2 decoding).  No counterpart in the reference, which writes and
- * reads no codestream.  Parses a T.800 codestream of one tile (tile-parts allowed), one quality
- * layer, LRCP or RLCP progression, one precinct per resolution, the default code-block style,
+ * reads no codestream.  Parses a T.800 codestream of one tile (tile-parts allowed), any number of
+ * quality layers, LRCP or RLCP progression, one precinct per resolution, the default code-block style,
  * reversible (5/3) or irreversible (9/7) transform with no, derived or expounded quantisation,
  * 1 or 3 (with colour transform) 8-bit components: the subset this library writes and the one
  * OpenJPEG writes by default.  SOP/EPH markers are skipped.  Other streams return
@@ -237,6 +241,12 @@ typedef struct {
 j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
                                size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
                                size_t errlen);
+/* Same, keeping only the first max_layers quality layers (0: all): each block's codeword is the
+ * concatenation of its segments from those layers and npasses counts their passes, so the
+ * result decodes to the image at that layer's quality. */
+j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
+                                      j2k_cb_desc* descs, size_t* count, uint8_t* bytes, size_t cap,
+                                      size_t* used, char* err, size_t errlen);
 
 /* ---- differentiable 9/7 (no counterpart in the reference).  n images of w x h float32,
  * planes back to back (pitch w, plane stride w*h), device pointers, T.800 order.  Used with

@@ -29,7 +29,8 @@ assert CB_DESC.itemsize == 24
 
 class EncParams(C.Structure):
     _fields_ = [("levels", C.c_int), ("cbw", C.c_int), ("cbh", C.c_int), ("order", C.c_int),
-                ("steps", C.c_void_p), ("target_bytes", C.c_size_t)]
+                ("steps", C.c_void_p), ("target_bytes", C.c_size_t), ("layers", C.c_int),
+                ("layer_bytes", C.c_void_p)]
 
 
 J2K_MAX_BANDS = 97
@@ -72,6 +73,7 @@ SIGS = {
     "j2k_dwt_inverse_batch": (I, [P, I, I, P, S, S, P, S, S, I, S, S, I, P]),
     "j2k_codeblock_count": (S, [S, S, I, I, I]),
     "j2k_codestream_read": (I, [P, S, P, P, P, P, S, P, P, S]),
+    "j2k_codestream_read_layers": (I, [P, S, I, P, P, P, P, S, P, P, S]),
     "j2k_bpc_encode": (I, [P, P, S, S, S, I, I, I, P, P, S]),
     "j2k_bpc_decode": (I, [P, P, P, S, P, S, S, S, I, I, I]),
     "j2k_encoder_create": (I, [P, I, I, C.POINTER(P)]),

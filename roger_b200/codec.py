@@ -222,9 +222,14 @@ def bpc_decode(descs, data, w, h, levels, cbw=64, cbh=64, ctx=None, out=None):
 # Reference-shaped classes
 # ---------------------------------------------------------------------------------------------
 
-def _params(levels, cbw, cbh, order, steps, target_bytes=0):
+def _params(levels, cbw, cbh, order, steps, target_bytes=0, layers=None):
     keep, sp = _steps_arg(steps, levels) if steps is not None else (None, None)
-    p = L.EncParams(levels, cbw, cbh, order, sp, int(target_bytes))
+    nl, lp = 0, None
+    if layers is not None and len(layers) > 1:
+        lb = np.ascontiguousarray(np.asarray(layers, np.uint64))
+        keep = (keep, lb)
+        nl, lp = len(lb), lb.ctypes.data
+    p = L.EncParams(levels, cbw, cbh, order, sp, int(target_bytes), nl, lp)
     return p, keep
 
 
@@ -261,23 +266,27 @@ class OCLEncoder(OCLEncodeDecode):
             pass
 
     def run(self, components, w, h, levels, precision=8, cbw=64, cbh=64, order=L.ORDER_T800,
-            steps=None, target_bytes=0):
+            steps=None, target_bytes=0, layers=None):
         """Reference signature: planar host components (numpy int16/int32/float32, already
         level-shifted by -128, as src/OCLTest.cpp:80-90 builds them).  target_bytes > 0 cuts the
-        codestream to at most that many bytes (PCRD-opt rate control)."""
+        codestream to at most that many bytes (PCRD-opt rate control); layers = cumulative byte
+        budgets of several quality layers (see run_rgb)."""
         comps = [np.ascontiguousarray(c) for c in components]
         dt = {np.dtype(np.int16): L.I16, np.dtype(np.int32): L.I32, np.dtype(np.float32): L.F32}[comps[0].dtype]
         arr = (C.c_void_p * len(comps))(*[c.ctypes.data for c in comps])
-        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes)
+        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes, layers)
         hh = self.ctx._bind()
         check(lib().j2k_encoder_run(self.h, arr, len(comps), dt, w, h, levels, precision, C.byref(p)), hh)
         self.w, self.h_, self.ncomp, self.levels = w, h, len(comps), levels
         return self
 
-    def run_rgb(self, img, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None, target_bytes=0):
+    def run_rgb(self, img, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None, target_bytes=0,
+                layers=None):
         """Interleaved uint8 image, (H, W, C) or (H, W); numpy (host) or CUDA tensor.
         target_bytes > 0 cuts the codestream to at most that many bytes (PCRD-opt rate control:
-        bit-plane truncation points of every code-block chosen on their rate-distortion hulls)."""
+        bit-plane truncation points of every code-block chosen on their rate-distortion hulls).
+        layers: cumulative codestream byte budgets of quality layers 0, 1, ... (non-decreasing;
+        a last entry of 0 keeps every pass, a lossless final layer for 5/3)."""
         if isinstance(img, torch.Tensor) and img.is_cuda:
             t = img.contiguous()
             ptr, on_dev = t.data_ptr(), 1
@@ -290,7 +299,7 @@ class OCLEncoder(OCLEncodeDecode):
             hgt, wid = a.shape[0], a.shape[1]
             nc = 1 if a.ndim == 2 else a.shape[2]
             keep_img = a
-        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes)
+        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes, layers)
         hh = self.ctx._bind()
         check(lib().j2k_encoder_run_interleaved(self.h, C.c_void_p(ptr), on_dev, wid * nc, nc, wid, hgt,
                                                 C.byref(p)), hh)
@@ -379,24 +388,26 @@ class OCLDecoder(OCLEncodeDecode):
         return out
 
 
-def read_codestream(cs):
+def read_codestream(cs, max_layers=0):
     """Tier-2 decoding of a codestream (bytes): -> (info dict, descs structured array, codeword
-    bytes), ready for OCLDecoder.run.  Raises J2KError(J2K_ERR_UNSUPPORTED) with the reason for
-    streams outside the supported subset (one tile, one layer, LRCP/RLCP, default code-block
+    bytes), ready for OCLDecoder.run.  Every quality layer is parsed; a block's codeword is the
+    concatenation of its segments from the first `max_layers` layers (0: all), so a prefix of the
+    layers decodes to the image at that quality.  Raises J2KError(J2K_ERR_UNSUPPORTED) with the
+    reason for streams outside the supported subset (one tile, LRCP/RLCP, default code-block
     style, 1 or 3 colour-transformed 8-bit components)."""
     buf = np.frombuffer(bytes(cs), np.uint8)
     info = L.StreamInfo()
     cnt, used = C.c_size_t(), C.c_size_t()
     err = C.create_string_buffer(256)
-    s = lib().j2k_codestream_read(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(info), None, C.byref(cnt),
-                                  None, 0, C.byref(used), err, 256)
+    s = lib().j2k_codestream_read_layers(buf.ctypes.data_as(C.c_void_p), buf.size, int(max_layers), C.byref(info),
+                                         None, C.byref(cnt), None, 0, C.byref(used), err, 256)
     if s != 0:
         raise L.J2KError(s, err.value.decode())
     descs = np.zeros(cnt.value, L.CB_DESC)
     data = np.zeros(max(used.value, 1), np.uint8)
-    s = lib().j2k_codestream_read(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(info),
-                                  descs.ctypes.data_as(C.c_void_p), C.byref(cnt), data.ctypes.data_as(C.c_void_p),
-                                  data.size, C.byref(used), err, 256)
+    s = lib().j2k_codestream_read_layers(buf.ctypes.data_as(C.c_void_p), buf.size, int(max_layers), C.byref(info),
+                                         descs.ctypes.data_as(C.c_void_p), C.byref(cnt),
+                                         data.ctypes.data_as(C.c_void_p), data.size, C.byref(used), err, 256)
     if s != 0:
         raise L.J2KError(s, err.value.decode())
     nb = 3 * info.levels + 1
@@ -407,10 +418,11 @@ def read_codestream(cs):
     return d, descs, data[:used.value]
 
 
-def decode_codestream(cs, ctx=None):
+def decode_codestream(cs, ctx=None, max_layers=0):
     """Decodes a codestream on the GPU: tier-2 on the host, then tier-1, inverse DWT and inverse
-    colour transform on the device.  Returns (H, W, C) uint8."""
-    info, descs, data = read_codestream(cs)
+    colour transform on the device.  max_layers > 0 decodes only the first quality layers.
+    Returns (H, W, C) uint8."""
+    info, descs, data = read_codestream(cs, max_layers)
     dec = OCLDecoder(ctx=ctx, lossy=not info["lossless"])
     return dec.run(descs, data, info["w"], info["h"], info["ncomp"], levels=info["levels"], cbw=info["cbw"],
                    cbh=info["cbh"], steps=None if info["lossless"] else info["steps"])

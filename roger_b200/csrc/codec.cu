@@ -84,6 +84,10 @@ struct j2k_encoder {
     bool packed_ok = false;  // the packed codewords of the current result are on the device
     size_t packed_total = 0;
     size_t target_bytes = 0;  // rate control: codestream budget (0 = keep every pass)
+    // quality layers: cumulative codestream budgets (0 in the last place: every pass), and per
+    // layer l and block i the passes / codeword bytes kept after that layer (lay_*[l * n + i])
+    std::vector<size_t> layer_budget;
+    std::vector<int32_t> lay_np, lay_len;
     DevBuf rate_pb, rate_dist;
     void* mapped = nullptr;
 };
@@ -160,22 +164,54 @@ static j2k_status rate_control(j2k_encoder* e) {
     for (size_t i = 0; i < n; ++i) w[i] = gain[e->hjobs[i].band];
     std::vector<j2k_cb_desc> d(n);
     std::vector<j2k_t2_block> blocks(n);
-    size_t budget = e->target_bytes;
-    for (int it = 0; it < 6; ++it) {
-        std::memcpy(d.data(), dh, n * sizeof(j2k_cb_desc));
-        j2k_pcrd_truncate(d.data(), n, pb, dist, w.data(), budget);
-        for (size_t i = 0; i < n; ++i) blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, nullptr};
-        const size_t size = j2k_t2_size(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
-                                        e->mct != J2K_MCT_NONE, e->steps.data(), blocks);
-        if (size <= e->target_bytes) break;
-        const size_t excess = size - e->target_bytes + 16;
-        if (budget <= excess) {
-            budget = 0;
-            if (it > 0) break;
-        } else {
-            budget -= excess;
+    for (size_t i = 0; i < n; ++i) blocks[i] = j2k_t2_block{dh[i].numbps, 0, 0, nullptr};
+    // one layer per budget (a single target_bytes is one layer); each layer keeps at least what
+    // the layer before it kept, and its budget is lowered until the codestream of the layers so
+    // far (headers included) fits it
+    std::vector<size_t> budgets = e->layer_budget;
+    if (budgets.empty()) budgets.push_back(e->target_bytes);
+    const int L = (int)budgets.size();
+    e->lay_np.assign((size_t)L * n, 0);
+    e->lay_len.assign((size_t)L * n, 0);
+    for (int l = 0; l < L; ++l) {
+        int32_t* np = e->lay_np.data() + (size_t)l * n;
+        int32_t* ln = e->lay_len.data() + (size_t)l * n;
+        const int32_t* pnp = l ? np - n : nullptr;
+        const int32_t* pln = l ? ln - n : nullptr;
+        if (budgets[l] == 0) {  // the last layer may keep every pass
+            for (size_t i = 0; i < n; ++i) np[i] = dh[i].npasses, ln[i] = std::max(dh[i].length, 0);
+            continue;
+        }
+        size_t budget = budgets[l];
+        for (int it = 0; it < 6; ++it) {
+            std::memcpy(d.data(), dh, n * sizeof(j2k_cb_desc));
+            j2k_pcrd_truncate(d.data(), n, pb, dist, w.data(), budget);
+            for (size_t i = 0; i < n; ++i) {
+                np[i] = d[i].npasses;
+                ln[i] = d[i].length;
+                if (pnp && np[i] < pnp[i]) np[i] = pnp[i], ln[i] = pln[i];
+            }
+            const size_t size = j2k_t2_size(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
+                                            e->mct != J2K_MCT_NONE, e->steps.data(), blocks, l + 1,
+                                            e->lay_np.data(), e->lay_len.data());
+            if (size <= budgets[l]) break;
+            const size_t excess = size - budgets[l] + 16;
+            if (budget <= excess) {
+                budget = 0;
+                if (it > 0) break;
+            } else {
+                budget -= excess;
+            }
         }
     }
+    const int32_t* fnp = e->lay_np.data() + (size_t)(L - 1) * n;
+    const int32_t* fln = e->lay_len.data() + (size_t)(L - 1) * n;
+    for (size_t i = 0; i < n; ++i) {
+        d[i] = dh[i];
+        d[i].npasses = (uint8_t)fnp[i];
+        d[i].length = fnp[i] ? fln[i] : 0;
+    }
+    if (L == 1) e->lay_np.clear(), e->lay_len.clear();
     std::memcpy(dh, d.data(), n * sizeof(j2k_cb_desc));
     J2K_CUDA(ctx, cudaMemcpyAsync(e->descs.p, dh, n * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -218,7 +254,7 @@ static j2k_status encode_planes(j2k_encoder* e) {
         J2K_TRY(j2k_clear_device_error(ctx));
         uint32_t* pb = nullptr;
         double* dist = nullptr;
-        if (e->target_bytes) {
+        if (e->target_bytes || !e->layer_budget.empty()) {
             J2K_TRY(e->rate_pb.ensure(ctx, e->njobs * 32 * 4 + 16));
             J2K_TRY(e->rate_dist.ensure(ctx, e->njobs * 33 * 8 + 16));
             pb = (uint32_t*)e->rate_pb.p;
@@ -228,7 +264,7 @@ static j2k_status encode_planes(j2k_encoder* e) {
                                    e->njobs, (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p,
                                    e->njobs * e->sym_cap, nullptr, ctx->stream, pb, dist));
         j2k_status s = j2k_read_device_error(ctx);
-        if (s == J2K_OK) return e->target_bytes ? rate_control(e) : J2K_OK;
+        if (s == J2K_OK) return (e->target_bytes || !e->layer_budget.empty()) ? rate_control(e) : J2K_OK;
         if (s != J2K_ERR_CAPACITY) return s;
         // grow whichever capacity overflowed and retry
         if (ctx->err.find("symbol") != std::string::npos) e->sym_cap = align16(e->sym_cap * 2);
@@ -355,6 +391,21 @@ static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const
     if (ncomp != 1 && ncomp != 3)
         return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "encoder supports 1 or 3 components");
     e->target_bytes = p ? p->target_bytes : 0;
+    e->layer_budget.clear();
+    e->lay_np.clear();
+    e->lay_len.clear();
+    if (p && p->layers > 1) {
+        if (!p->layer_bytes || p->layers > 64)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "layers > 1 needs layer_bytes (at most 64 layers)");
+        for (int l = 0; l < p->layers; ++l) {
+            const size_t b = p->layer_bytes[l];
+            if (b == 0 && l != p->layers - 1)
+                return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "only the last layer budget may be 0 (every pass)");
+            if (l && b && b < p->layer_bytes[l - 1])
+                return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "layer budgets must not decrease");
+            e->layer_budget.push_back(b);
+        }
+    }
     e->w = w;
     e->h = h;
     e->ncomp = ncomp;
@@ -489,8 +540,14 @@ j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, 
     std::vector<j2k_t2_block> blocks(count);
     for (size_t i = 0; i < count; ++i)
         blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, b.data() + d[i].offset};
-    std::vector<uint8_t> cs = j2k_t2_write(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
-                                           e->mct != J2K_MCT_NONE, e->steps.data(), blocks);
+    const int L = (int)(e->lay_np.size() / std::max<size_t>(count, 1));
+    std::vector<uint8_t> cs =
+        L > 1 && e->lay_np.size() == (size_t)L * count
+            ? j2k_t2_write_layers(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
+                                  e->mct != J2K_MCT_NONE, e->steps.data(), blocks, L, e->lay_np.data(),
+                                  e->lay_len.data())
+            : j2k_t2_write(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy, e->mct != J2K_MCT_NONE,
+                           e->steps.data(), blocks);
     *len = cs.size();
     if (!out) return J2K_OK;
     if (cap < cs.size()) return j2k_fail(ctx, J2K_ERR_CAPACITY, "codestream buffer too small");

@@ -175,4 +175,11 @@ std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int
                                   const std::vector<j2k_t2_block>& blocks);
 // Size in bytes of the codestream j2k_t2_write would produce (block data is not read).
 size_t j2k_t2_size(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
-                   const float* steps, const std::vector<j2k_t2_block>& blocks);
+                   const float* steps, const std::vector<j2k_t2_block>& blocks, int nlayers = 1,
+                   const int32_t* cum_np = nullptr, const int32_t* cum_len = nullptr);
+// Quality layers: after layer l block i holds cum_np[l * n + i] passes and the first
+// cum_len[l * n + i] bytes of blocks[i].data (both non-decreasing in l).
+std::vector<uint8_t> j2k_t2_write_layers(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
+                                         int lossless, int mct, const float* steps,
+                                         const std::vector<j2k_t2_block>& blocks, int nlayers,
+                                         const int32_t* cum_np, const int32_t* cum_len);

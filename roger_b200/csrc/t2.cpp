@@ -134,9 +134,24 @@ void put_npasses(BitWriter& bw, int n) {  // Table B.4
 namespace {
 
 // Writes the codestream into `o`; without bodies only the markers and packet headers are
-// written and the returned size still counts every block's codeword bytes.
+// written and the returned size still counts every block's codeword bytes.  nlayers quality
+// layers: after layer l block i has cum_np[l * n + i] passes and cum_len[l * n + i] bytes of its
+// codeword (non-decreasing in l); cum_np / cum_len NULL means one layer holding what
+// blocks[i] says.
 size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
-               const float* steps, const std::vector<j2k_t2_block>& blocks, bool bodies) {
+               const float* steps, const std::vector<j2k_t2_block>& blocks, bool bodies, int nlayers = 1,
+               const int32_t* cum_np = nullptr, const int32_t* cum_len = nullptr) {
+    const size_t nblk = blocks.size();
+    if (!cum_np || !cum_len) nlayers = 1;
+    // passes / bytes of block i after layer l (l = -1: nothing)
+    auto NP = [&](int l, size_t i) -> int {
+        if (l < 0) return 0;
+        return cum_np ? cum_np[(size_t)l * nblk + i] : blocks[i].npasses;
+    };
+    auto LEN = [&](int l, size_t i) -> int {
+        if (l < 0) return 0;
+        return cum_len ? cum_len[(size_t)l * nblk + i] : std::max(blocks[i].length, 0);
+    };
     const int nb = 3 * levels + 1;
     std::vector<j2k_band_rect> rects(nb);
     j2k_band_rects(w, h, levels, rects.data());
@@ -177,7 +192,7 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
     }
     G = std::min(G, 7);
     size_t body = 0;
-    for (const auto& b : blocks) body += (size_t)std::max(b.length, 0);
+    for (size_t i = 0; i < nblk; ++i) body += (size_t)LEN(nlayers - 1, i);
     o.v.reserve(256 + (size_t)nb * 4 + blocks.size() * 10 + (bodies ? body : 0));
     o.u16(0xFF4F);  // SOC
     o.u16(0xFF51);  // SIZ
@@ -191,7 +206,7 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
     o.u16(12);
     o.u8(0);
     o.u8(0);        // LRCP
-    o.u16(1);       // one layer
+    o.u16((uint32_t)nlayers);
     o.u8(mct ? 1 : 0);
     o.u8((uint32_t)levels);
     o.u8((uint32_t)(floorlog2(cbw) - 2));
@@ -216,58 +231,82 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
     o.u8(0);
     o.u8(1);
     o.u16(0xFF93);  // SOD
-    for (int r = 0; r <= levels; ++r)
-        for (int c = 0; c < ncomp; ++c) {
-            int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
-            int bcount = r == 0 ? 1 : 3;
-            bool any = false;
-            for (int q = 0; q < bcount; ++q)
-                for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
-                    any |= blocks[i].npasses > 0;
-            BitWriter bw(o);
-            if (!any) {
-                bw.bit(0);
-                bw.flush();
-                continue;
-            }
-            bw.bit(1);
-            for (int q = 0; q < bcount; ++q) {
-                int b = b0 + q;
-                int n = ncbx[b] * ncby[b];
-                if (!n) continue;
-                size_t f = first[(size_t)c * nb + b];
-                int Mb = G + eps[b] - 1;
-                std::vector<int> incl(n), zbp(n);
-                for (int i = 0; i < n; ++i) {
-                    incl[i] = blocks[f + i].npasses > 0 ? 0 : 1;
-                    zbp[i] = Mb - blocks[f + i].numbps;
-                }
-                TagTree ti(ncbx[b], ncby[b], incl), tz(ncbx[b], ncby[b], zbp);
-                for (int j = 0; j < ncby[b]; ++j)
-                    for (int i = 0; i < ncbx[b]; ++i) {
-                        const j2k_t2_block& cb = blocks[f + (size_t)j * ncbx[b] + i];
-                        ti.encode(bw, i, j, 1);
-                        if (cb.npasses == 0) continue;
-                        tz.encode(bw, i, j, 0x7FFFFFF);
-                        put_npasses(bw, cb.npasses);
-                        int lblock = 3;
-                        int bits = floorlog2(cb.length) + 1;
-                        int avail = lblock + floorlog2(cb.npasses);
-                        int inc = bits > avail ? bits - avail : 0;
-                        for (int t = 0; t < inc; ++t) bw.bit(1);
-                        bw.bit(0);
-                        lblock += inc;
-                        bw.bits((uint32_t)cb.length, lblock + floorlog2(cb.npasses));
+    // tag trees (inclusion: first layer holding a pass of the block; zero bit-planes) and the
+    // Lblock state of every block persist from layer to layer
+    std::vector<TagTree> incl, zbp;
+    incl.reserve((size_t)ncomp * nb);
+    zbp.reserve((size_t)ncomp * nb);
+    for (int c = 0; c < ncomp; ++c)
+        for (int b = 0; b < nb; ++b) {
+            const int n = ncbx[b] * ncby[b];
+            const size_t f = first[(size_t)c * nb + b];
+            const int Mb = G + eps[b] - 1;
+            std::vector<int> li(std::max(n, 1), nlayers), lz(std::max(n, 1), 0);
+            for (int i = 0; i < n; ++i) {
+                for (int l = 0; l < nlayers; ++l)
+                    if (NP(l, f + i) > 0) {
+                        li[i] = l;
+                        break;
                     }
+                lz[i] = Mb - blocks[f + i].numbps;
             }
-            bw.flush();
-            // the header of the NEXT packet needs the band's Lblock state only within this
-            // packet: with one layer every block appears at most once, so no state is kept.
-            if (bodies)
+            incl.emplace_back(std::max(ncbx[b], 1), std::max(ncby[b], 1), li);
+            zbp.emplace_back(std::max(ncbx[b], 1), std::max(ncby[b], 1), lz);
+        }
+    std::vector<int> lblock(nblk, 3);
+    for (int l = 0; l < nlayers; ++l)
+        for (int r = 0; r <= levels; ++r)
+            for (int c = 0; c < ncomp; ++c) {
+                int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
+                int bcount = r == 0 ? 1 : 3;
+                bool any = false;
                 for (int q = 0; q < bcount; ++q)
                     for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
-                        o.v.insert(o.v.end(), blocks[i].data, blocks[i].data + blocks[i].length);
-        }
+                        any |= NP(l, i) > NP(l - 1, i);
+                BitWriter bw(o);
+                if (!any) {
+                    bw.bit(0);
+                    bw.flush();
+                    continue;
+                }
+                bw.bit(1);
+                for (int q = 0; q < bcount; ++q) {
+                    int b = b0 + q;
+                    if (!(ncbx[b] * ncby[b])) continue;
+                    size_t f = first[(size_t)c * nb + b];
+                    TagTree& ti = incl[(size_t)c * nb + b];
+                    TagTree& tz = zbp[(size_t)c * nb + b];
+                    for (int j = 0; j < ncby[b]; ++j)
+                        for (int i = 0; i < ncbx[b]; ++i) {
+                            const size_t k = f + (size_t)j * ncbx[b] + i;
+                            const int prev = NP(l - 1, k), cur = NP(l, k);
+                            if (prev == 0) {  // not included before: inclusion tag tree up to layer l
+                                ti.encode(bw, i, j, l + 1);
+                                if (cur == 0) continue;
+                                tz.encode(bw, i, j, 0x7FFFFFF);
+                            } else {
+                                bw.bit(cur > prev);
+                                if (cur == prev) continue;
+                            }
+                            const int newp = cur - prev;
+                            const int seg = LEN(l, k) - LEN(l - 1, k);
+                            put_npasses(bw, newp);
+                            int bits = floorlog2(seg) + 1;
+                            int avail = lblock[k] + floorlog2(newp);
+                            int inc = bits > avail ? bits - avail : 0;
+                            for (int t = 0; t < inc; ++t) bw.bit(1);
+                            bw.bit(0);
+                            lblock[k] += inc;
+                            bw.bits((uint32_t)seg, lblock[k] + floorlog2(newp));
+                        }
+                }
+                bw.flush();
+                if (bodies)
+                    for (int q = 0; q < bcount; ++q)
+                        for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
+                            if (NP(l, i) > NP(l - 1, i))
+                                o.v.insert(o.v.end(), blocks[i].data + LEN(l - 1, i), blocks[i].data + LEN(l, i));
+            }
     const size_t extra = bodies ? 0 : body;
     uint32_t psot = (uint32_t)(o.v.size() + extra - sot);
     o.v[sot + 6] = (uint8_t)(psot >> 24);
@@ -291,10 +330,20 @@ std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int
 }
 
 size_t j2k_t2_size(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
-                   const float* steps, const std::vector<j2k_t2_block>& blocks) {
+                   const float* steps, const std::vector<j2k_t2_block>& blocks, int nlayers,
+                   const int32_t* cum_np, const int32_t* cum_len) {
     static thread_local Bytes o;
     o.v.clear();
-    return t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, false);
+    return t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, false, nlayers, cum_np, cum_len);
+}
+
+std::vector<uint8_t> j2k_t2_write_layers(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
+                                         int lossless, int mct, const float* steps,
+                                         const std::vector<j2k_t2_block>& blocks, int nlayers,
+                                         const int32_t* cum_np, const int32_t* cum_len) {
+    Bytes o;
+    t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, true, nlayers, cum_np, cum_len);
+    return std::move(o.v);
 }
 
 // ---- tier-2 reading (codestream parser) -----------------------------------------------------
@@ -414,8 +463,12 @@ namespace {
 // Parses a codestream into stream parameters, one descriptor per code-block (job order:
 // component, subband in QCD order, raster) and the packet bytes of the tile (tile-parts
 // concatenated); src_off[i] is block i's codeword offset within tile_bytes.
-j2k_status t2_read(const uint8_t* cs, size_t n, j2k_stream_info* info, std::vector<j2k_cb_desc>* descs,
-                   std::vector<uint32_t>* src_off, std::vector<uint8_t>* tile_bytes, std::string* err) {
+// Quality layers: the packets of every layer are parsed (the tag-tree, Lblock and inclusion state
+// carries from layer to layer); a block's codeword is the concatenation of its segments from
+// the first `max_layers` layers (0: all), segs[i] listing (offset in tile_bytes, length).
+j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
+                   std::vector<j2k_cb_desc>* descs, std::vector<std::vector<std::pair<uint32_t, int>>>* segs,
+                   std::vector<uint8_t>* tile_bytes, std::string* err) {
     try {
         Cursor c{cs, n};
         if (c.u16() != 0xFF4F) throw ReadErr{J2K_ERR_INVALID_ARG, "no SOC marker"};
@@ -466,7 +519,7 @@ j2k_status t2_read(const uint8_t* cs, size_t n, j2k_stream_info* info, std::vect
                 sty = (int)c.u8();
                 xform = (int)c.u8();
                 if (scod & 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "user-defined precincts"};
-                if (layers != 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "more than one quality layer"};
+                if (layers < 1) throw ReadErr{J2K_ERR_INVALID_ARG, "no quality layer"};
                 if (prog != 0 && prog != 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "progression other than LRCP/RLCP"};
                 if (sty != 0) throw ReadErr{J2K_ERR_UNSUPPORTED, "code-block style options (bypass, reset, ...)"};
                 if (levels > 32 || cbw > 64 || cbh > 64 || cbw * cbh > 4096)
@@ -562,7 +615,7 @@ j2k_status t2_read(const uint8_t* cs, size_t n, j2k_stream_info* info, std::vect
             }
         first[(size_t)ncomp * nb] = k;
         descs->assign(k, j2k_cb_desc{});
-        src_off->assign(k, 0);
+        segs->assign(k, {});
         for (int cc = 0; cc < ncomp; ++cc)
             for (int b = 0; b < nb; ++b)
                 for (int j = 0; j < ncby[b]; ++j)
@@ -576,59 +629,91 @@ j2k_status t2_read(const uint8_t* cs, size_t n, j2k_stream_info* info, std::vect
                         d.ch = (uint16_t)std::min<size_t>(cbh, rects[b].h - (size_t)j * cbh);
                         d.comp = (uint16_t)cc;
                     }
+        // per (component, band) tag trees and per block Lblock / inclusion state, kept across layers
+        std::vector<TagTreeDec> incl, zbp;
+        incl.reserve((size_t)ncomp * nb);
+        zbp.reserve((size_t)ncomp * nb);
+        for (int cc = 0; cc < ncomp; ++cc)
+            for (int b = 0; b < nb; ++b) {
+                incl.emplace_back(std::max(ncbx[b], 1), std::max(ncby[b], 1));
+                zbp.emplace_back(std::max(ncbx[b], 1), std::max(ncby[b], 1));
+            }
+        std::vector<int> lblock(k, 3), tot_np(k, 0);
+        std::vector<uint8_t> included(k, 0);  // 0, or the block's bit-plane count once included
+        const int keep = max_layers > 0 ? std::min(max_layers, layers) : layers;
         size_t pos = 0;
         const uint8_t* pd = data.data();
         const size_t pn = data.size();
-        for (int r = 0; r <= levels; ++r)
-            for (int cc = 0; cc < ncomp; ++cc) {
-                if (scod & 2) {  // SOP marker segment before the packet
-                    if (pos + 6 <= pn && pd[pos] == 0xFF && pd[pos + 1] == 0x91) pos += 6;
-                }
-                const int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
-                const int bcount = r == 0 ? 1 : 3;
-                BitReader br(pd, pn, pos);
-                std::vector<std::pair<size_t, int>> body;  // (block index, length) in packet order
-                if (br.bit()) {
-                    for (int q = 0; q < bcount; ++q) {
-                        const int b = b0 + q;
-                        const int nbx = ncbx[b], nby = ncby[b];
-                        if (!nbx || !nby) continue;
-                        TagTreeDec ti(nbx, nby), tz(nbx, nby);
-                        const int Mb = guard + eps[b] - 1;
-                        for (int j = 0; j < nby; ++j)
-                            for (int i = 0; i < nbx; ++i) {
-                                const size_t idx = first[(size_t)cc * nb + b] + (size_t)j * nbx + i;
-                                if (ti.decode(br, i, j, 1) >= 1) continue;  // not included
+        auto packet = [&](int l, int r, int cc) {
+            if (scod & 2) {  // SOP marker segment before the packet
+                if (pos + 6 <= pn && pd[pos] == 0xFF && pd[pos + 1] == 0x91) pos += 6;
+            }
+            const int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
+            const int bcount = r == 0 ? 1 : 3;
+            BitReader br(pd, pn, pos);
+            std::vector<std::pair<size_t, int>> body;  // (block index, length) in packet order
+            if (br.bit()) {
+                for (int q = 0; q < bcount; ++q) {
+                    const int b = b0 + q;
+                    const int nbx = ncbx[b], nby = ncby[b];
+                    if (!nbx || !nby) continue;
+                    TagTreeDec& ti = incl[(size_t)cc * nb + b];
+                    TagTreeDec& tz = zbp[(size_t)cc * nb + b];
+                    const int Mb = guard + eps[b] - 1;
+                    for (int j = 0; j < nby; ++j)
+                        for (int i = 0; i < nbx; ++i) {
+                            const size_t idx = first[(size_t)cc * nb + b] + (size_t)j * nbx + i;
+                            j2k_cb_desc& d = (*descs)[idx];
+                            if (!included[idx]) {
+                                if (ti.decode(br, i, j, l + 1) >= l + 1) continue;  // not included yet
                                 int z = 0;
                                 while ((z = tz.decode(br, i, j, 1 << 30)) == (1 << 30)) {
                                 }
-                                const int np = get_npasses(br);
-                                int lblock = 3;
-                                while (br.bit()) ++lblock;
-                                const int lbits = lblock + floorlog2(np);
-                                if (lbits > 31) throw ReadErr{J2K_ERR_INVALID_ARG, "code-block length field too long"};
-                                const int len = (int)br.bits(lbits);
-                                j2k_cb_desc& d = (*descs)[idx];
                                 const int nbps = Mb - z;
-                                if (nbps < 1 || nbps > 31 || np > 3 * nbps - 2)
-                                    throw ReadErr{J2K_ERR_INVALID_ARG, "inconsistent bit-planes or passes"};
-                                d.numbps = (uint8_t)nbps;
-                                d.npasses = (uint8_t)np;
-                                d.length = len;
-                                body.push_back({idx, len});
+                                if (nbps < 1 || nbps > 31)
+                                    throw ReadErr{J2K_ERR_INVALID_ARG, "inconsistent bit-planes"};
+                                included[idx] = (uint8_t)nbps;
+                            } else if (!br.bit()) {
+                                continue;  // no new passes in this layer
                             }
-                    }
-                }
-                pos = br.end();
-                if (scod & 4) {  // EPH
-                    if (pos + 2 <= pn && pd[pos] == 0xFF && pd[pos + 1] == 0x92) pos += 2;
-                }
-                for (auto& e : body) {
-                    if (pos + (size_t)e.second > pn) throw ReadErr{J2K_ERR_INVALID_ARG, "packet body truncated"};
-                    (*src_off)[e.first] = (uint32_t)pos;
-                    pos += (size_t)e.second;
+                            const int np = get_npasses(br);
+                            while (br.bit()) ++lblock[idx];
+                            const int lbits = lblock[idx] + floorlog2(np);
+                            if (lbits > 31) throw ReadErr{J2K_ERR_INVALID_ARG, "code-block length field too long"};
+                            const int len = (int)br.bits(lbits);
+                            tot_np[idx] += np;
+                            if (tot_np[idx] > 3 * included[idx] - 2)
+                                throw ReadErr{J2K_ERR_INVALID_ARG, "more passes than bit-planes allow"};
+                            if (l < keep) {
+                                d.numbps = included[idx];
+                                d.npasses = (uint8_t)(d.npasses + np);
+                                d.length += len;
+                                body.push_back({idx, len});
+                            } else {
+                                body.push_back({(size_t)-1, len});
+                            }
+                        }
                 }
             }
+            pos = br.end();
+            if (scod & 4) {  // EPH
+                if (pos + 2 <= pn && pd[pos] == 0xFF && pd[pos + 1] == 0x92) pos += 2;
+            }
+            for (auto& e : body) {
+                if (pos + (size_t)e.second > pn) throw ReadErr{J2K_ERR_INVALID_ARG, "packet body truncated"};
+                if (e.first != (size_t)-1 && e.second > 0) (*segs)[e.first].push_back({(uint32_t)pos, e.second});
+                pos += (size_t)e.second;
+            }
+        };
+        if (prog == 0) {
+            for (int l = 0; l < layers && l < keep; ++l)
+                for (int r = 0; r <= levels; ++r)
+                    for (int cc = 0; cc < ncomp; ++cc) packet(l, r, cc);
+        } else {
+            for (int r = 0; r <= levels; ++r)
+                for (int l = 0; l < layers; ++l)
+                    for (int cc = 0; cc < ncomp; ++cc) packet(l, r, cc);
+        }
         *info = I;
         tile_bytes->swap(data);
         return J2K_OK;
@@ -640,15 +725,15 @@ j2k_status t2_read(const uint8_t* cs, size_t n, j2k_stream_info* info, std::vect
 
 }  // namespace
 
-extern "C" j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
-                                          size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
-                                          size_t errlen) {
-    if (!cs || !info || !count || !used) return J2K_ERR_INVALID_ARG;
+extern "C" j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
+                                                 j2k_cb_desc* descs, size_t* count, uint8_t* bytes, size_t cap,
+                                                 size_t* used, char* err, size_t errlen) {
+    if (!cs || !info || !count || !used || max_layers < 0) return J2K_ERR_INVALID_ARG;
     std::vector<j2k_cb_desc> d;
-    std::vector<uint32_t> off;
+    std::vector<std::vector<std::pair<uint32_t, int>>> segs;
     std::vector<uint8_t> tile;
     std::string msg;
-    j2k_status s = t2_read(cs, n, info, &d, &off, &tile, &msg);
+    j2k_status s = t2_read(cs, n, max_layers, info, &d, &segs, &tile, &msg);
     if (s != J2K_OK) {
         if (err && errlen) {
             std::strncpy(err, msg.c_str(), errlen - 1);
@@ -665,9 +750,17 @@ extern "C" j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_strea
     size_t o = 0;
     for (size_t i = 0; i < d.size(); ++i) {
         d[i].offset = (uint32_t)o;
-        if (d[i].length > 0) std::memcpy(bytes + o, tile.data() + off[i], (size_t)d[i].length);
-        o += (size_t)d[i].length;
+        for (const auto& sg : segs[i]) {
+            std::memcpy(bytes + o, tile.data() + sg.first, (size_t)sg.second);
+            o += (size_t)sg.second;
+        }
         descs[i] = d[i];
     }
     return J2K_OK;
+}
+
+extern "C" j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
+                                          size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
+                                          size_t errlen) {
+    return j2k_codestream_read_layers(cs, n, 0, info, descs, count, bytes, cap, used, err, errlen);
 }

@@ -78,12 +78,48 @@ def test_openjpeg_lossy_codestream_matches_openjpeg_decode():
 def test_unsupported_streams_are_rejected_with_a_reason():
     img = synth.rgb(64, 64, (1, 2, 3, 4))
     buf = io.BytesIO()
-    PIL.fromarray(img).save(buf, "JPEG2000", num_resolutions=3, quality_mode="rates", quality_layers=[40, 20, 10],
+    PIL.fromarray(img).save(buf, "JPEG2000", num_resolutions=3, tile_size=(32, 32), irreversible=False, mct=1,
                             no_jp2=True)
-    with pytest.raises(J2KError, match="layer"):
+    with pytest.raises(J2KError, match="tile"):
+        C.read_codestream(buf.getvalue())
+    buf = io.BytesIO()
+    PIL.fromarray(img).save(buf, "JPEG2000", num_resolutions=3, irreversible=False, mct=0, no_jp2=True)
+    with pytest.raises(J2KError, match="colour transform"):
         C.read_codestream(buf.getvalue())
     with pytest.raises(J2KError):
-        C.read_codestream(b"\\x00\\x01\\x02")
+        C.read_codestream(b"\x00\x01\x02")
+
+
+def _openjpeg_layers(img, levels, rates, prog="LRCP", cb=64):
+    buf = io.BytesIO()
+    kw = dict(irreversible=False, num_resolutions=levels + 1, codeblock_size=(cb, cb), progression=prog,
+              quality_mode="rates", quality_layers=rates, no_jp2=True)
+    if img.ndim == 3:
+        kw["mct"] = 1
+    PIL.fromarray(img).save(buf, "JPEG2000", **kw)
+    return buf.getvalue()
+
+
+@pytest.mark.parametrize("prog", ["LRCP", "RLCP"])
+@pytest.mark.parametrize("w,h,nc,L,cb", CASES[:3])
+def test_openjpeg_multilayer_lossless_decodes_exactly(w, h, nc, L, cb, prog):
+    img = synth.gray(w, h, 41) if nc == 1 else synth.rgb(w, h, (41, 42, 43, 44))
+    cs = _openjpeg_layers(img, L, [30, 8, 0], prog, cb)
+    info, descs, data = C.read_codestream(cs)
+    assert info["layers"] == 3
+    assert np.array_equal(_cpu_decode(cs).reshape(img.shape), img)
+    # the first layers give each block a prefix of its full codeword and fewer passes
+    prev = None
+    for keep in (1, 2, 3):
+        _, d, b = C.read_codestream(cs, max_layers=keep)
+        assert np.all(d["npasses"] <= descs["npasses"]) and np.all(d["length"] <= descs["length"])
+        for k in np.flatnonzero(d["length"] > 0)[:200]:
+            full = data[descs["offset"][k]:descs["offset"][k] + d["length"][k]]
+            assert np.array_equal(b[d["offset"][k]:d["offset"][k] + d["length"][k]], full)
+        if prev is not None:
+            assert np.all(d["npasses"] >= prev)
+        prev = d["npasses"].copy()
+    assert np.array_equal(prev, descs["npasses"])
 
 
 @pytest.mark.gpu

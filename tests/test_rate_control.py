@@ -177,3 +177,40 @@ def test_pcrd_selection_matches_sorted_threshold(seed):
         ref = _pcrd_reference(desc, pb, dist, w, budget)
         assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == ref
         assert int(d2["length"].sum()) <= min(budget, full)
+
+
+@pytest.mark.gpu
+def test_quality_layers():
+    from PIL import Image
+    from roger_b200 import codec as C
+    img = synth.rgb(384, 256, (51, 52, 53, 54))
+    enc = C.OCLEncoder(lossy=False)
+    full = len(enc.run_rgb(img, levels=5, cbw=32, cbh=32).codestream())
+    budgets = [int(full * 0.04), int(full * 0.15), int(full * 0.4), 0]
+    single = bytes(enc.run_rgb(img, levels=5, cbw=32, cbh=32, target_bytes=budgets[0]).codestream())
+    cs = bytes(enc.run_rgb(img, levels=5, cbw=32, cbh=32, layers=budgets).codestream())
+    info, descs, _ = C.read_codestream(cs)
+    assert info["layers"] == 4
+    # the last layer keeps every pass: lossless for us and for OpenJPEG
+    assert np.array_equal(C.decode_codestream(cs).reshape(img.shape), img)
+    assert np.array_equal(np.asarray(Image.open(io.BytesIO(cs))).reshape(img.shape), img)
+    # layer 0 is the single-layer cut at the same budget, block by block
+    _, d1, b1 = C.read_codestream(single)
+    _, d0, b0 = C.read_codestream(cs, max_layers=1)
+    assert np.array_equal(d0["npasses"], d1["npasses"]) and np.array_equal(d0["length"], d1["length"])
+    assert np.array_equal(b0, b1)
+    # every prefix of layers: codeword bytes within its budget, quality rising, GPU decode equal
+    # to the oracle's and close to OpenJPEG's decode of the same layers
+    last = -1.0
+    for k in (1, 2, 3):
+        _, dk, _ = C.read_codestream(cs, max_layers=k)
+        assert int(dk["length"].sum()) <= budgets[k - 1]
+        ours = C.decode_codestream(cs, max_layers=k).reshape(img.shape)
+        p = _psnr(ours, img)
+        assert p > last
+        last = p
+        im = Image.open(io.BytesIO(cs))
+        t = im.tile[0]
+        im.tile = [type(t)(t[0], t[1], t[2], (t[3][0], 0, k) + tuple(t[3][3:]))]
+        theirs = np.asarray(im).reshape(img.shape)
+        assert abs(_psnr(theirs, img) - p) < 1.0
