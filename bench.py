@@ -618,6 +618,25 @@ def bench_batched(n, flush):
         rd, rb = be.codeblocks(i)
         same_stream &= np.array_equal(d, rd) and np.array_equal(np.asarray(b), rb)
     t_stream = statistics.median(tt)
+    # batched decode of the same 256 codestreams (host bytes in, host pixels out, tier-2 parse
+    # included) against a loop of per-image decodes
+    streams = [be.codestream(i) for i in range(len(descs))]
+    dec = C.OCLDecoder()
+    outs = C.decode_codestreams(streams, decoder=dec)
+    t_dec_b = ev(lambda: C.decode_codestreams(streams, decoder=dec), 3)
+
+    def dec_loop():
+        return [C.decode_codestream(cs) for cs in streams]
+    outs1 = dec_loop()
+    t_dec_1 = ev(dec_loop, 2)
+    dec_same = all(np.array_equal(a.reshape(-1), b.reshape(-1)) for a, b in zip(outs, outs1))
+    exact53 = all(np.array_equal(o.reshape(-1), im.cpu().numpy().reshape(-1))
+                  for d, o, im in zip(descs, outs, imgs) if d["kernel"] == 53)
+    decode = {"path": "decode_codestreams (tier-2 per stream on the host, one upload, one tier-1 launch, "
+                      "per-image inverse DWT + colour transform, one read-back) vs decode_codestream per image",
+              "batched_ms": round(t_dec_b, 3), "batched_mpix_s": round(mpix / (t_dec_b * 1e-3), 1),
+              "per_image_ms": round(t_dec_1, 3), "per_image_mpix_s": round(mpix / (t_dec_1 * 1e-3), 1),
+              "speedup": round(t_dec_1 / t_dec_b, 2), "identical": bool(dec_same), "lossless_exact_53": bool(exact53)}
     h2h = {"h2d_bytes_per_batch": in_bytes, "d2h_bytes_per_batch": out_bytes,
            "one_batch": {"ms": round(t_seq, 3), "mpix_s": round(mpix / (t_seq * 1e-3), 1),
                          "identical_to_batched": bool(same_seq)},
@@ -625,7 +644,7 @@ def bench_batched(n, flush):
                         "mpix_s": round(mpix / (t_stream * 1e-3), 1), "identical_to_batched": bool(same_stream)}}
     return {"workload": f"{n} images, w,h log-uniform [64,2048], 50% RGB, 5/3 even / 9/7 odd, L=3..5, "
                         "32x32|64x64 code-blocks (seed 300)",
-            "host_to_host": h2h,
+            "host_to_host": h2h, "decode": decode,
             "mpix": round(mpix, 3), "batched_ms": round(t_batch, 3), "per_image_ms": round(t_single, 3),
             "batched_mpix_s": round(mpix / (t_batch * 1e-3), 1),
             "per_image_mpix_s": round(mpix / (t_single * 1e-3), 1),

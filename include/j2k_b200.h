@@ -216,6 +216,25 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* dec, const j2k_cb_desc* descs
                                       int ncomp, size_t w, size_t h, const j2k_enc_params* params,
                                       uint8_t* out, int out_on_device, size_t out_pitch_bytes);
 
+/* Batched decode: the code-blocks of n images (each as j2k_codestream_read returns them, host
+ * memory) are uploaded in one copy and tier-1 decoded in one launch; each image then runs its
+ * inverse DWT and inverse colour transform, and every image's pixels come back in one copy into
+ * its `out` (interleaved uint8, pitch w*ncomp).  The reference decodes nothing
+ * (src/OCLDecoder.cpp:35-38). */
+typedef struct {
+    uint32_t w, h;
+    int ncomp;                 /* 1 or 3 (colour transform) */
+    int lossless;              /* 1: 5/3 (RCT); 0: 9/7 (ICT) */
+    int levels, cbw, cbh;
+    const float* steps;        /* lossy: 3*levels+1 steps (QCD order); NULL = 8*2^-level */
+    const j2k_cb_desc* descs;  /* job order, count entries */
+    size_t count;
+    const uint8_t* bytes;      /* codewords, descs[i].offset into it */
+    size_t nbytes;
+    uint8_t* out;              /* host output */
+} j2k_decode_item;
+j2k_status j2k_decoder_run_batch(j2k_decoder* dec, const j2k_decode_item* items, int n);
+
 /* ---- codestream reading (tier-2 decoding).  No counterpart in the reference, which writes and
  * reads no codestream.  Parses a T.800 codestream of one tile (tile-parts allowed), any number of
  * quality layers, LRCP or RLCP progression, one precinct per resolution, the default code-block style,

@@ -88,6 +88,7 @@ SIGS = {
     "j2k_decoder_create": (I, [P, I, C.POINTER(P)]),
     "j2k_decoder_destroy": (I, [P]),
     "j2k_decoder_run_codeblocks": (I, [P, P, P, S, I, I, S, S, P, P, I, S]),
+    "j2k_decoder_run_batch": (I, [P, P, I]),
     "j2k_dwt97_forward_adjoint": (I, [P, P, P, I, S, S, I]),
     "j2k_dwt97_inverse_adjoint": (I, [P, P, P, I, S, S, I]),
     "j2k_relaxed_quant_forward": (I, [P, P, P, I, S, S, I, P, C.c_uint64, P, I]),
@@ -118,6 +119,13 @@ SIGS = {
 class BatchImage(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("ncomp", C.c_int), ("kernel", C.c_int),
                 ("levels", C.c_int), ("cb", C.c_int), ("steps", C.c_void_p)]
+
+
+class DecodeItem(C.Structure):
+    _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("ncomp", C.c_int), ("lossless", C.c_int),
+                ("levels", C.c_int), ("cbw", C.c_int), ("cbh", C.c_int), ("steps", C.c_void_p),
+                ("descs", C.c_void_p), ("count", C.c_size_t), ("bytes", C.c_void_p), ("nbytes", C.c_size_t),
+                ("out", C.c_void_p)]
 
 
 def exported_symbols():

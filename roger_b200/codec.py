@@ -428,6 +428,29 @@ def decode_codestream(cs, ctx=None, max_layers=0):
                    cbh=info["cbh"], steps=None if info["lossless"] else info["steps"])
 
 
+def decode_codestreams(streams, ctx=None, max_layers=0, decoder=None):
+    """Batched GPU decode of many codestreams: tier-2 of each on the host, then one upload of all
+    code-blocks, one tier-1 launch over every block of every image, the inverse DWT and colour
+    transform per image, and one read-back.  Returns a list of (H, W[, C]) uint8 arrays."""
+    ctx = ctx or default_context(0)
+    parsed = [read_codestream(cs, max_layers) for cs in streams]
+    items = (L.DecodeItem * len(parsed))()
+    keep, outs = [], []
+    for k, (info, descs, data) in enumerate(parsed):
+        nc = info["ncomp"]
+        out = np.empty((info["h"], info["w"], nc) if nc > 1 else (info["h"], info["w"]), np.uint8)
+        st = np.ascontiguousarray(info["steps"], np.float32)
+        keep += [descs, data, st]
+        outs.append(out)
+        items[k] = L.DecodeItem(info["w"], info["h"], nc, int(info["lossless"]), info["levels"], info["cbw"],
+                                info["cbh"], None if info["lossless"] else st.ctypes.data, descs.ctypes.data,
+                                descs.size, data.ctypes.data, int(data.size), out.ctypes.data)
+    dec = decoder or OCLDecoder(ctx=ctx)  # a kept decoder reuses its device buffers
+    hh = dec.ctx._bind()
+    check(lib().j2k_decoder_run_batch(dec.h, items, len(parsed)), hh)
+    return outs
+
+
 class OCLDWTForward:
     """OCLDWTForward<T>::run(lossy, w, h, windowX, windowY, level, levels) (src/OCLDWTForward.h:31).
     The window arguments of the OpenCL launch geometry have no meaning here and are ignored."""

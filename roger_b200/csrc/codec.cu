@@ -585,6 +585,114 @@ j2k_status j2k_decoder_destroy(j2k_decoder* d) {
     return J2K_OK;
 }
 
+j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, int n) {
+    if (!d || (!items && n > 0) || n < 0) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = d->ctx;
+    if (n == 0) return J2K_OK;
+    cudaSetDevice(ctx->device);
+    // jobs of every image into one coefficient buffer; descriptors rebased into one byte buffer
+    std::vector<j2k_cb_job> jobs;
+    std::vector<size_t> coef_off(n), out_off(n + 1, 0), job0(n + 1, 0), byte0(n + 1, 0);
+    std::vector<int> lv(n), cbw(n), cbh(n);
+    size_t coef_total = 0, desc_total = 0, max_ll0 = 16, max_ll1 = 16;
+    for (int k = 0; k < n; ++k) {
+        const j2k_decode_item& it = items[k];
+        if (!it.descs || (!it.bytes && it.nbytes) || !it.out)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "NULL pointer in item " + std::to_string(k));
+        if (it.ncomp != 1 && it.ncomp != 3)
+            return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "decoder supports 1 or 3 components");
+        j2k_enc_params p{};
+        p.levels = it.levels;
+        p.cbw = it.cbw;
+        p.cbh = it.cbh;
+        int order;
+        J2K_TRY(check_params(ctx, &p, it.w, it.h, &lv[k], &cbw[k], &cbh[k], &order));
+        coef_off[k] = coef_total;
+        job0[k] = jobs.size();
+        for (int c = 0; c < it.ncomp; ++c)
+            j2k_build_jobs(it.w, it.h, lv[k], cbw[k], cbh[k], &jobs, c, coef_total + (uint64_t)c * it.w * it.h,
+                           it.w, (uint32_t)k);
+        job0[k + 1] = jobs.size();
+        if (it.count != job0[k + 1] - job0[k])
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "item " + std::to_string(k) + ": descriptor count does not "
+                                                      "match the image's code-blocks");
+        for (size_t i = 0; i < it.count; ++i) {
+            const j2k_cb_desc& q = it.descs[i];
+            if (q.length < 0 || (size_t)q.offset + (size_t)q.length > it.nbytes || q.numbps > 31 ||
+                q.npasses > 3 * q.numbps)
+                return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "item " + std::to_string(k) + ": code-block descriptor " +
+                                                              std::to_string(i) + " is out of range");
+        }
+        coef_total += (size_t)it.w * it.h * it.ncomp;
+        byte0[k + 1] = byte0[k] + it.nbytes;
+        out_off[k + 1] = out_off[k] + (size_t)it.w * it.h * it.ncomp;
+        const size_t w1 = (it.w + 1) / 2, h1 = (it.h + 1) / 2;
+        max_ll0 = std::max(max_ll0, w1 * h1 * 4);
+        max_ll1 = std::max(max_ll1, ((w1 + 1) / 2) * ((h1 + 1) / 2) * 4);
+        desc_total += it.count;
+    }
+    // one upload: descriptors and codewords through the page-locked staging buffer
+    const size_t nbytes = byte0[n], dbytes = desc_total * sizeof(j2k_cb_desc);
+    const size_t stage = std::max(align16(dbytes) + nbytes, out_off[n]) + 16;
+    uint8_t* hs = (uint8_t*)j2k_pinned(ctx, stage);
+    if (!hs) return J2K_ERR_OUT_OF_MEMORY;
+    j2k_cb_desc* hd = (j2k_cb_desc*)hs;
+    uint8_t* hb = hs + align16(dbytes);
+    for (int k = 0; k < n; ++k) {
+        const j2k_decode_item& it = items[k];
+        for (size_t i = 0; i < it.count; ++i) {
+            j2k_cb_desc q = it.descs[i];
+            q.offset = (uint32_t)(byte0[k] + q.offset);
+            hd[job0[k] + i] = q;
+        }
+        if (it.nbytes) std::memcpy(hb + byte0[k], it.bytes, it.nbytes);
+    }
+    if (nbytes + 16 > 0xFFFFFFFFull) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "more than 4 GiB of codewords");
+    J2K_TRY(d->descs.ensure(ctx, dbytes + 16));
+    J2K_TRY(d->bytes.ensure(ctx, nbytes + 16));
+    J2K_TRY(d->jobs.ensure(ctx, jobs.size() * sizeof(j2k_cb_job) + 16));
+    J2K_TRY(d->coef.ensure(ctx, coef_total * 4 + 16));
+    J2K_TRY(d->planes.ensure(ctx, coef_total * 4 + 16));
+    J2K_TRY(d->out.ensure(ctx, out_off[n] + 16));
+    d->job_key[0] = 0;  // the per-image job cache no longer describes d->jobs
+    d->hjobs.clear();
+    J2K_CUDA(ctx, cudaMemcpyAsync(d->descs.p, hd, dbytes, cudaMemcpyHostToDevice, ctx->stream));
+    J2K_CUDA(ctx, cudaMemcpyAsync(d->bytes.p, hb, nbytes, cudaMemcpyHostToDevice, ctx->stream));
+    J2K_CUDA(ctx, cudaMemcpyAsync(d->jobs.p, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    J2K_TRY(j2k_clear_device_error(ctx));
+    // tier-1 of every block of every image in one launch
+    J2K_TRY(j2k_t1_decode_jobs(ctx, (const j2k_cb_desc*)d->descs.p, (const uint8_t*)d->bytes.p,
+                               (const j2k_cb_job*)d->jobs.p, jobs.size(), (int32_t*)d->coef.p, ctx->stream));
+    void* ll0 = j2k_scratch(ctx, SCR_LL0, max_ll0);
+    void* ll1 = j2k_scratch(ctx, SCR_LL1, max_ll1);
+    if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
+    for (int k = 0; k < n; ++k) {
+        const j2k_decode_item& it = items[k];
+        const bool lossy = !it.lossless;
+        const size_t w = it.w, h = it.h, px = w * h;
+        std::vector<float> steps;
+        if (lossy) {
+            if (it.steps) steps.assign(it.steps, it.steps + 3 * lv[k] + 1);
+            else steps = default_steps(w, h, lv[k]);
+        }
+        for (int c = 0; c < it.ncomp; ++c)
+            J2K_TRY(j2k_dwt_inv_impl(ctx, lossy ? J2K_W97 : J2K_W53, J2K_ORDER_T800,
+                                     (const char*)d->coef.p + (coef_off[k] + (size_t)c * px) * 4, w,
+                                     (char*)d->planes.p + (coef_off[k] + (size_t)c * px) * 4, w, w, h, lv[k],
+                                     lossy ? steps.data() : nullptr, ll0, ll1, j2k_dwt_tile{64, 64}, ctx->stream));
+        const int mct = it.ncomp >= 3 ? (lossy ? J2K_MCT_ICT : J2K_MCT_RCT) : J2K_MCT_NONE;
+        J2K_TRY(j2k_launch_planar_inv(ctx, (const char*)d->planes.p + coef_off[k] * 4, lossy ? J2K_F32 : J2K_I32, w,
+                                      px, it.ncomp, mct, (uint8_t*)d->out.p + out_off[k], w * it.ncomp, w, h,
+                                      ctx->stream));
+    }
+    // one read-back of every image's pixels
+    J2K_CUDA(ctx, cudaMemcpyAsync(hs, d->out.p, out_off[n], cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_TRY(j2k_read_device_error(ctx));
+    for (int k = 0; k < n; ++k) std::memcpy(items[k].out, hs + out_off[k], out_off[k + 1] - out_off[k]);
+    return J2K_OK;
+}
+
 j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, const uint8_t* bytes,
                                       size_t nbytes, int on_device, int ncomp, size_t w, size_t h,
                                       const j2k_enc_params* p, uint8_t* out, int out_on_device,

@@ -129,3 +129,26 @@ def test_gpu_decodes_openjpeg_and_own_codestreams(w, h, nc, L, cb):
     for cs in (_openjpeg(img, L, True, cb), bytes(O.encode_image(img, L, cb, cb, True))):
         out = C.decode_codestream(cs)
         assert np.array_equal(out.reshape(img.shape), img)
+
+
+@pytest.mark.gpu
+def test_batched_decode_matches_per_image():
+    streams = []
+    for w, h, nc, L, cb in CASES:
+        img = synth.gray(w, h, 61) if nc == 1 else synth.rgb(w, h, (61, 62, 63, 64))
+        streams += [_openjpeg(img, L, True, cb), bytes(O.encode_image(img, L, cb, cb, True)),
+                    _openjpeg_layers(img, L, [30, 8, 0], "RLCP", cb)]
+    img = synth.rgb(160, 120, (65, 66, 67, 68))
+    streams.append(_openjpeg(img, 4, lossless=False))
+    enc = C.OCLEncoder(lossy=True)
+    streams.append(bytes(enc.run_rgb(img, levels=4).codestream()))
+    enc = C.OCLEncoder(lossy=False)
+    streams.append(bytes(enc.run_rgb(img, levels=4, cbw=32, cbh=32, target_bytes=4000).codestream()))
+    outs = C.decode_codestreams(streams)
+    assert len(outs) == len(streams)
+    for k, (cs, out) in enumerate(zip(streams, outs)):
+        ref = C.decode_codestream(cs)
+        assert np.array_equal(out.reshape(-1), ref.reshape(-1)), f"stream {k}"
+    # only the first layer of the layered streams
+    first = C.decode_codestreams(streams[2:3], max_layers=1)[0]
+    assert np.array_equal(first.reshape(-1), C.decode_codestream(streams[2], max_layers=1).reshape(-1))
