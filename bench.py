@@ -107,6 +107,38 @@ def profiled_traffic(size):
     return None
 
 
+def tier1_issue(size, ms, clocks):
+    """Issue roofline of tier-1, the dominant stage: its profiled warp instructions over the live
+    tier-1 time, against the SM issue peak (148 SMs x 4 schedulers x 1 instruction per cycle at
+    the SM clock sampled during the timed region)."""
+    ins = profiled_tier1_instructions(size)
+    if not ins:
+        return None
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = 148 * 4 * mhz * 1e6 / 1e9
+    total = ins["t1_symbols_instructions"] + ins["t1_mq_instructions"]
+    achieved = total / (ms * 1e-3) / 1e9
+    return {"bound": "issue", "kernels": "t1_symbols_kernel + t1_mq_kernel<8>", "achieved": round(achieved, 1),
+            "peak": round(peak, 1), "unit": "G warp-instructions/s", "frac": round(achieved / peak, 4),
+            "instructions_per_encode": total, "tier1_ms": round(ms, 4),
+            "source": "profiles/tier1_instructions_lossless_4096.txt (ncu smsp__inst_executed.sum)"}
+
+
+def profiled_tier1_instructions(size):
+    """Warp instructions of the two tier-1 kernels of one encode of the benchmark image (ncu
+    smsp__inst_executed.sum, deterministic for this input; kept as a text summary under
+    profiles/); None when absent or for another size."""
+    path = os.path.join(ROOT, "profiles", "tier1_instructions_lossless_4096.txt")
+    if size != 4096 or not os.path.exists(path):
+        return None
+    got = {}
+    for line in open(path):
+        for key in ("t1_symbols_instructions", "t1_mq_instructions"):
+            if line.startswith(key + ":"):
+                got[key] = int(line.split(":")[1])
+    return got if len(got) == 2 else None
+
+
 class L2Flush:
     """Writes a 256 MiB buffer (larger than the 126 MB L2) and then reads another one, so the
     next timed kernel starts with a cold L2 that holds no dirty lines of the flush itself."""
@@ -337,6 +369,7 @@ def main():
                    "tier1_all_blocks_derived": round(ms - t_planar - t_dwt, 4)},
         dwt_all_levels_gbs=round(lvl_bytes / (t_dwt * 1e-3) / 1e9, 1),
         planar_gbs=round(n * 15 / (t_planar * 1e-3) / 1e9, 1),
+        tier1_issue=tier1_issue(size, ms - t_planar - t_dwt, clocks),
         tier1={"codeblocks": int(len(descs)), "sample_passes": samples,
                "gsample_passes_per_s": round(samples / ((ms - t_planar - t_dwt) * 1e-3) / 1e9, 3),
                "codeword_bytes": int(res[1].size)},

@@ -61,6 +61,45 @@ __host__ __device__ __forceinline__ int zc_label_calc(int orient, int h, int v, 
     return d >= 2 ? 2 : d;
 }
 
+// Lookup tables shared by the warps of a CTA (the host path builds its own copy).
+//   zc[o][n9]: zero-coding label for orientation o and the 9-bit significance neighbourhood n9
+//              (bits 0-2: row above, columns x-1..x+1; 3-5: own row; 6-8: row below; the
+//              sample's own bit 4 is ignored; a significant neighbour is n9 & 0x1EF != 0)
+//   sc[n8]:    sign-coding label | xor bit << 7 for n8 = sigL negL sigR negR sigU negU sigD negD
+//   mq[i]:     Qe | NMPS << 16 | NLPS << 22 | SWITCH << 28 of probability state i (Table C.2)
+struct DecTables {
+    uint8_t zc[4][512];
+    uint8_t sc[256];
+    uint32_t mq[47];
+};
+
+__host__ __device__ inline void fill_tables_entry(DecTables& T, int i) {
+    if (i < 4 * 512) {
+        const int o = i >> 9, n = i & 511;
+        const int h = ((n >> 3) & 1) + ((n >> 5) & 1), v = ((n >> 1) & 1) + ((n >> 7) & 1);
+        const int d = (n & 1) + ((n >> 2) & 1) + ((n >> 6) & 1) + ((n >> 8) & 1);
+        T.zc[o][n] = (uint8_t)zc_label_calc(o, h, v, d);
+    }
+    if (i < 256) {
+        auto c = [&](int sh) { return ((i >> sh) & 1) ? (((i >> (sh + 1)) & 1) ? -1 : 1) : 0; };
+        int hc = max(-1, min(1, c(0) + c(2))), vc = max(-1, min(1, c(4) + c(6)));
+        int xr = 0;
+        if (hc < 0 || (hc == 0 && vc < 0)) { hc = -hc; vc = -vc; xr = 1; }
+        T.sc[i] = (uint8_t)((hc == 0 ? (vc ? 10 : 9) : 12 + vc) | (xr << 7));
+    }
+    if (i < 47)
+        T.mq[i] = (uint32_t)QE(i) | ((uint32_t)NMPS(i) << 16) | ((uint32_t)NLPS(i) << 22) |
+                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
+}
+
+__host__ __device__ __forceinline__ int clz32(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return __clz(v);
+#else
+    return v ? __builtin_clz(v) : 32;
+#endif
+}
+
 struct DecSmem {
     uint64_t sig[66], neg[66], ref[66], vis[66];
     uint8_t st[19];
@@ -97,51 +136,51 @@ struct Mqd {
         CT -= 7;
         A = 0x8000;
     }
-    __host__ __device__ int decode(uint8_t* st, int cx) {
-        int sv = st[cx], idx = sv >> 1, mps = sv & 1;
-        uint32_t qe = QE(idx);
-        int D;
-        A -= qe;
-        if ((C >> 16) < qe) {
-            if (A < qe) {
-                A = qe;
-                D = mps;
-                idx = NMPS(idx);
-            } else {
-                A = qe;
-                D = 1 - mps;
-                if (idx == 0 || idx == 6 || idx == 14) mps ^= 1;
-                idx = NLPS(idx);
-            }
-            st[cx] = (uint8_t)((idx << 1) | mps);
-            do {
-                if (CT == 0) bytein();
-                A <<= 1;
-                C <<= 1;
-                --CT;
-            } while (!(A & 0x8000));
-        } else {
-            C -= qe << 16;
-            if (!(A & 0x8000)) {
-                if (A < qe) {
-                    D = 1 - mps;
-                    if (idx == 0 || idx == 6 || idx == 14) mps ^= 1;
-                    idx = NLPS(idx);
-                } else {
-                    D = mps;
-                    idx = NMPS(idx);
-                }
-                st[cx] = (uint8_t)((idx << 1) | mps);
-                do {
-                    if (CT == 0) bytein();
-                    A <<= 1;
-                    C <<= 1;
-                    --CT;
-                } while (!(A & 0x8000));
-            } else {
-                D = mps;
-            }
+    // renormalisation by the leading-zero count at once, stopping for a byte-in whenever CT
+    // runs out (the same steps as the bit-by-bit loop of C.3.3)
+    __host__ __device__ __forceinline__ void renorm() {
+        int sh = clz32(A) - 16;
+        while (sh > 0) {
+            if (CT == 0) bytein();
+            const int k = min(sh, CT);
+            A <<= k;
+            C <<= k;
+            CT -= k;
+            sh -= k;
         }
+    }
+    __host__ __device__ int decode(uint8_t* st, const uint32_t* mq, int cx) {
+        const uint32_t sv = st[cx];
+        const uint32_t e = mq[sv >> 1];
+        const uint32_t qe = e & 0xFFFF;
+        const int mps = sv & 1;
+        A -= qe;
+        int D, nm = mps;
+        uint32_t nidx;
+        if ((C >> 16) >= qe) {
+            C -= qe << 16;
+            if (A & 0x8000) return mps;  // MPS, no renormalisation
+            if (A < qe) {                // conditional exchange: LPS
+                D = 1 - mps;
+                nm ^= (int)(e >> 28);
+                nidx = (e >> 22) & 63;
+            } else {
+                D = mps;
+                nidx = (e >> 16) & 63;
+            }
+        } else {
+            if (A < qe) {  // conditional exchange: MPS
+                D = mps;
+                nidx = (e >> 16) & 63;
+            } else {
+                D = 1 - mps;
+                nm ^= (int)(e >> 28);
+                nidx = (e >> 22) & 63;
+            }
+            A = qe;
+        }
+        st[cx] = (uint8_t)((nidx << 1) | nm);
+        renorm();
         return D;
     }
 };
@@ -160,9 +199,10 @@ __host__ __device__ __forceinline__ uint32_t nb3(uint64_t m, int x) {
 
 // Serial decode of one code-block into magnitudes (blk, pre-zeroed) and sign/state masks in S.
 // Host-callable so that the exact device logic can be checked on the CPU.
-__host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint8_t* data, int len, int numbps,
+__host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint8_t* data, int len, int numbps,
                                       int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch) {
-#define zc_lut_at(o, h, v, d) lut[(((o) * 3 + (h)) * 3 + (v)) * 5 + (d)]
+        const uint8_t* zct = T.zc[orient];
+        const uint32_t* mq = T.mq;
 
         S.st[0] = 4 << 1;
         S.st[17] = 3 << 1;
@@ -172,26 +212,20 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
         int pass = 0;
         const int nb = numbps, np = npasses;
         auto sigbit = [&](int x, int y) -> int { return (int)((S.sig[y + 1] >> x) & 1); };
+        // zero-coding label | 0x100 when a neighbour is significant
         auto zc = [&](int x, int y) -> int {
-            uint32_t a = nb3(S.sig[y], x), b = nb3(S.sig[y + 1], x), c = nb3(S.sig[y + 2], x);
-            int h = (b & 1) + (b >> 2), v = ((a >> 1) & 1) + ((c >> 1) & 1);
-            int d = (a & 1) + (a >> 2) + (c & 1) + (c >> 2);
-            return (h + v + d) ? (int)zc_lut_at(orient, h, v, d) | 0x100 : zc_lut_at(orient, 0, 0, 0);
+            const uint32_t n9 = nb3(S.sig[y], x) | (nb3(S.sig[y + 1], x) << 3) | (nb3(S.sig[y + 2], x) << 6);
+            return (int)zct[n9] | ((n9 & 0x1EF) ? 0x100 : 0);
         };
+        // sign-coding label | xor bit << 7
         auto sc = [&](int x, int y) -> int {
-            auto contrib = [&](int xx, int yy) -> int {
-                if (xx < 0 || xx >= 64) return 0;
-                if (!((S.sig[yy + 1] >> xx) & 1)) return 0;
-                return ((S.neg[yy + 1] >> xx) & 1) ? -1 : 1;
-            };
-            int hc = contrib(x - 1, y) + contrib(x + 1, y);
-            int vc = contrib(x, y - 1) + contrib(x, y + 1);
-            hc = max(-1, min(1, hc));
-            vc = max(-1, min(1, vc));
-            int xr = 0;
-            if (hc < 0 || (hc == 0 && vc < 0)) { hc = -hc; vc = -vc; xr = 1; }
-            int lab = hc == 0 ? (vc ? 10 : 9) : 12 + vc;
-            return lab | (xr << 7);
+            const uint64_t r = S.sig[y + 1], rn = S.neg[y + 1];
+            uint32_t n8 = 0;
+            if (x > 0) n8 |= (uint32_t)((r >> (x - 1)) & 1) | ((uint32_t)((rn >> (x - 1)) & 1) << 1);
+            if (x < 63) n8 |= ((uint32_t)((r >> (x + 1)) & 1) << 2) | ((uint32_t)((rn >> (x + 1)) & 1) << 3);
+            n8 |= ((uint32_t)((S.sig[y] >> x) & 1) << 4) | ((uint32_t)((S.neg[y] >> x) & 1) << 5);
+            n8 |= ((uint32_t)((S.sig[y + 2] >> x) & 1) << 6) | ((uint32_t)((S.neg[y + 2] >> x) & 1) << 7);
+            return T.sc[n8];
         };
         auto set_sig = [&](int x, int y, int neg, int p) {
             S.sig[y + 1] |= 1ull << x;
@@ -219,11 +253,11 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                             if (sigbit(x, y)) continue;
                             int z = zc(x, y);
                             if (!(z & 0x100)) continue;
-                            int bit = m.decode(S.st, z & 31);
+                            int bit = m.decode(S.st, mq, z & 31);
                             S.vis[y + 1] |= 1ull << x;
                             if (bit) {
                                 int s = sc(x, y);
-                                int sg = m.decode(S.st, s & 31) ^ (s >> 7);
+                                int sg = m.decode(S.st, mq, s & 31) ^ (s >> 7);
                                 set_sig(x, y, sg, p);
                                 cm |= (2ull << x) & cols;
                             }
@@ -245,7 +279,7 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                             int lab;
                             if ((S.ref[y + 1] >> x) & 1) lab = 16;
                             else lab = (zc(x, y) & 0x100) ? 15 : 14;
-                            if (m.decode(S.st, lab)) blk[(size_t)y * pitch + x] |= 1 << p;
+                            if (m.decode(S.st, mq, lab)) blk[(size_t)y * pitch + x] |= 1 << p;
                             S.ref[y + 1] |= 1ull << x;
                         }
                     }
@@ -267,12 +301,12 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                         for (int y = y0; y < y0 + 4 && rl; ++y)
                             if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1) || (zc(x, y) & 0x100)) rl = false;
                         if (rl) {
-                            if (!m.decode(S.st, 17)) continue;
-                            int idx = m.decode(S.st, 18) << 1;
-                            idx |= m.decode(S.st, 18);
+                            if (!m.decode(S.st, mq, 17)) continue;
+                            int idx = m.decode(S.st, mq, 18) << 1;
+                            idx |= m.decode(S.st, mq, 18);
                             int y = y0 + idx;
                             int s = sc(x, y);
-                            int sg = m.decode(S.st, s & 31) ^ (s >> 7);
+                            int sg = m.decode(S.st, mq, s & 31) ^ (s >> 7);
                             set_sig(x, y, sg, p);
                             start = y + 1;
                         }
@@ -280,10 +314,10 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
                     for (int y = start; y < y1; ++y) {
                         if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
                         int z = zc(x, y);
-                        int bit = m.decode(S.st, z & 31);
+                        int bit = m.decode(S.st, mq, z & 31);
                         if (bit) {
                             int s = sc(x, y);
-                            int sg = m.decode(S.st, s & 31) ^ (s >> 7);
+                            int sg = m.decode(S.st, mq, s & 31) ^ (s >> 7);
                             set_sig(x, y, sg, p);
                         }
                     }
@@ -292,7 +326,6 @@ __host__ __device__ void decode_block(DecSmem& S, const uint8_t* lut, const uint
             ++pass;
             for (int r = 0; r < 66; ++r) S.vis[r] = 0;
         }
-    #undef zc_lut_at
 }
 
 __global__ void __launch_bounds__(kWarps * 32)
@@ -300,11 +333,8 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
                  const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
                  uint32_t* __restrict__ err) {
     __shared__ DecSmem smem[kWarps];
-    __shared__ uint8_t zc_lut[4][3][3][5];
-    for (int i = threadIdx.x; i < 4 * 45; i += blockDim.x) {
-        int o = i / 45, r = i % 45;
-        zc_lut[o][r / 15][(r / 5) % 3][r % 5] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
-    }
+    __shared__ DecTables tabs;
+    for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int jid = blockIdx.x * kWarps + wid;
@@ -326,7 +356,7 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
     if (lane < 19) S.st[lane] = 0;
     __syncwarp();
     if (lane == 0 && D.numbps > 0 && D.npasses > 0)
-        decode_block(S, &zc_lut[0][0][0][0], bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch,
+        decode_block(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch,
                      blk, pitch);
     __syncwarp();
     // a block cut at the end of a bit-plane above the last one (rate control): significant
@@ -354,14 +384,15 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
     DecSmem S;
     for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
     for (int k = 0; k < 19; ++k) S.st[k] = 0;
-    uint8_t lut[4 * 45];
-    for (int i = 0; i < 4 * 45; ++i) {
-        int o = i / 45, r = i % 45;
-        lut[i] = (uint8_t)zc_label_calc(o, r / 15, (r / 5) % 3, r % 5);
+    static DecTables T;
+    static bool built = false;
+    if (!built) {
+        for (int i = 0; i < 4 * 512; ++i) fill_tables_entry(T, i);
+        built = true;
     }
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x) out[(size_t)y * pitch + x] = 0;
-    if (numbps > 0 && npasses > 0) decode_block(S, lut, data, len, numbps, npasses, orient, cw, ch, out, pitch);
+    if (numbps > 0 && npasses > 0) decode_block(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x)
             if ((S.neg[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
