@@ -59,12 +59,19 @@ const char* j2k_last_error(const j2k_ctx* ctx);
 /* Launch-shape knobs (set by the autotuner; defaults are sensible).  No reference counterpart:
  * the reference fixed its OpenCL work-group shapes in -D build strings (src/OCLEncoder.cpp:27-29). */
 enum {
-    J2K_TUNE_MQ_LANES = 1,   /* one-lane-per-block MQ kernel: blocks per warp (8, 16, 32) */
+    J2K_TUNE_MQ_LANES = 1,   /* one-lane-per-block MQ kernel: blocks per warp (8, 16 default, 32) after
+                                the tiers of J2K_TUNE_MQ_TIER */
     J2K_TUNE_MQ_VARIANT = 2, /* 0: one lane per block (default); 1: state warp + code-register warp */
     J2K_TUNE_DWT_FAST_TH = 3, /* register-lifting forward DWT tile height: 16 (default), 32, 0 = off */
     J2K_TUNE_DWT_PIPE = 4,    /* 1: that kernel streams bands with cp.async double buffering (default 0) */
-    J2K_TUNE_DWT_REG = 5      /* 1 (default): that kernel loads its columns straight into registers;
+    J2K_TUNE_DWT_REG = 5,     /* 1 (default): that kernel loads its columns straight into registers;
                                  0: it stages the strip in shared memory with cp.async */
+    J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
+                                 blocks, longest first, go to up to 4 tiers of `warps` warps with
+                                 `lanes` blocks each (lanes 0 ends the list), then to warps of
+                                 J2K_TUNE_MQ_LANES blocks, so that the longest serial chains share
+                                 their warp with fewer others.  Default: SM-count warps x 1 block,
+                                 2 x SM-count warps x 4 blocks */
 };
 j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value);
 const char* j2k_status_string(j2k_status s);

@@ -189,6 +189,13 @@ j2k_status j2k_ctx_create(int device, j2k_ctx** out) {
         return J2K_ERR_CUDA;
     }
     c->stream = c->own_stream;
+    // MQ schedule (longest blocks first): one warp per SM with one block each, two warps per SM
+    // with four blocks each, then 16 blocks per warp
+    c->mq_tier_warps[0] = c->sm_count;
+    c->mq_tier_lanes[0] = 1;
+    c->mq_tier_warps[1] = 2 * c->sm_count;
+    c->mq_tier_lanes[1] = 4;
+    c->mq_lanes = 16;
     *out = c;
     return J2K_OK;
 }
@@ -251,6 +258,14 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
     }
     if (key == J2K_TUNE_DWT_REG) {
         ctx->dwt_reg = value != 0;
+        return J2K_OK;
+    }
+    if (key == J2K_TUNE_MQ_TIER) {
+        const int tier = (value >> 24) & 0x7F, lanes = (value >> 20) & 15, warps = value & 0xFFFFF;
+        if (tier >= J2K_MQ_TIERS || lanes > 8 || value < 0)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "MQ tier: tier 0..3, lanes 0..8");
+        ctx->mq_tier_warps[tier] = lanes ? warps : 0;
+        ctx->mq_tier_lanes[tier] = lanes;
         return J2K_OK;
     }
     return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown tuning key");

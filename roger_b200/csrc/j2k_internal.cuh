@@ -20,6 +20,8 @@ enum : uint32_t {
 
 constexpr int J2K_SCRATCH_SLOTS = 9;
 
+constexpr int J2K_MQ_TIERS = 4;
+
 struct j2k_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -32,10 +34,12 @@ struct j2k_ctx {
     void* h_pinned = nullptr;    // pinned staging
     size_t h_pinned_size = 0;
     int sm_count = 148;
-    int mq_lanes = 8;            // tier-1 MQ: code-blocks per warp (tuning knob)
+    int mq_lanes = 8;            // tier-1 MQ: code-blocks per warp after the schedule's tiers (16 from creation)
     int mq_variant = 0;          // 0: one lane per block, 1: state warp + code warp pair
     int dwt_fast_th = 16;        // fast level-0 DWT tile height (16, 32; 0 = off)
     int dwt_pipe = 0;            // fast level-0 DWT: persistent cp.async double-buffered variant
+    // MQ schedule: tiers of warps with fewer blocks each for the longest blocks (lanes 0 ends)
+    int mq_tier_warps[4] = {0, 0, 0, 0}, mq_tier_lanes[4] = {1, 0, 0, 0};  // tier 0: sm_count warps
     int dwt_reg = 1;             // fast forward DWT: columns loaded straight into registers (0: cp.async strip)
 };
 

@@ -554,6 +554,12 @@ struct MqEnc {
     }
 };
 
+// Warp schedule of the MQ kernel: tier k has warps[k] warps of lanes[k] blocks each.
+struct MqSchedule {
+    int warps[4] = {0, 0, 0, 0};
+    int lanes[4] = {0, 0, 0, 0};
+};
+
 // RATE: also record, for every bit-plane k, the bytes produced (bp + 1) when its cleanup pass
 // ends (pass 3k; pass ends in symbols from phase A) into plane_bytes[job * 32 + k].
 template <int LANES, bool RATE = false>
@@ -561,7 +567,8 @@ __global__ void __launch_bounds__(kMqThreads)
 t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jobs, const uint32_t* __restrict__ nsyms,
              const uint32_t* __restrict__ order, int njobs, uint8_t* __restrict__ bytes,
               j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err,
-              const uint32_t* __restrict__ pend = nullptr, uint32_t* __restrict__ plane_bytes = nullptr) {
+              const uint32_t* __restrict__ pend = nullptr, uint32_t* __restrict__ plane_bytes = nullptr,
+              MqSchedule sched = MqSchedule{}) {
     __shared__ uint32_t tab[47];
     __shared__ uint32_t cst[19 * kMqThreads];
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
@@ -569,8 +576,23 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane >= LANES) return;
-    const int gid = (blockIdx.x * (kMqThreads / 32) + wid) * LANES + lane;
+    // warp w takes blocks in longest-first order: the schedule's tiers first (warps with fewer
+    // blocks each), then LANES blocks per warp
+    const int w = blockIdx.x * (kMqThreads / 32) + wid;
+    int gid = -1, wbase = 0, gbase = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (gid < 0 && w < wbase + sched.warps[k]) {
+            if (lane >= sched.lanes[k]) return;
+            gid = gbase + (w - wbase) * sched.lanes[k] + lane;
+        }
+        wbase += sched.warps[k];
+        gbase += sched.warps[k] * sched.lanes[k];
+    }
+    if (gid < 0) {
+        if (lane >= LANES) return;
+        gid = gbase + (w - wbase) * LANES + lane;
+    }
     if (gid >= njobs) return;
     const int jid = order ? (int)order[gid] : gid;
     const int t = threadIdx.x;
@@ -949,8 +971,19 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
         return J2K_OK;
     }
     const int lanes = ctx->mq_lanes;  // active lanes (blocks) per warp: 32, 16 or 8
-    const size_t per_cta = (size_t)lanes * (kMqThreads / 32);
-    unsigned gb = (unsigned)((njobs + per_cta - 1) / per_cta);
+    // tiers of the schedule, cut to the blocks there are
+    MqSchedule sc{};
+    size_t left = njobs, warps = 0;
+    for (int k = 0; k < J2K_MQ_TIERS && ctx->mq_tier_lanes[k] > 0 && left > 0; ++k) {
+        const size_t l = (size_t)ctx->mq_tier_lanes[k];
+        const size_t wk = std::min<size_t>((size_t)ctx->mq_tier_warps[k], (left + l - 1) / l);
+        sc.warps[k] = (int)wk;
+        sc.lanes[k] = (int)l;
+        left -= std::min(left, wk * l);
+        warps += wk;
+    }
+    warps += (left + lanes - 1) / lanes;
+    unsigned gb = (unsigned)((warps + kMqThreads / 32 - 1) / (kMqThreads / 32));
     if (plane_bytes && dist) {
         // rate control: byte positions at every bit-plane end, and the distortion of each
         // truncation point (the coefficients are still in place)
@@ -962,11 +995,14 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
         return J2K_OK;
     }
     if (lanes == 8)
-        t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
+        t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err,
+                                                   nullptr, nullptr, sc);
     else if (lanes == 16)
-        t1_mq_kernel<16><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
+        t1_mq_kernel<16><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs,
+                                                    ctx->d_err, nullptr, nullptr, sc);
     else
-        t1_mq_kernel<32><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
+        t1_mq_kernel<32><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs,
+                                                    ctx->d_err, nullptr, nullptr, sc);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }
