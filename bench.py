@@ -118,7 +118,7 @@ def tier1_issue(size, ms, clocks):
     peak = 148 * 4 * mhz * 1e6 / 1e9
     total = ins["t1_symbols_instructions"] + ins["t1_mq_instructions"]
     achieved = total / (ms * 1e-3) / 1e9
-    return {"bound": "issue", "kernels": "t1_symbols_kernel + t1_mq_kernel<8>", "achieved": round(achieved, 1),
+    return {"bound": "issue", "kernels": "t1_symbols_kernel + t1_mq_kernel<16> (tiered warp schedule)", "achieved": round(achieved, 1),
             "peak": round(peak, 1), "unit": "G warp-instructions/s", "frac": round(achieved / peak, 4),
             "instructions_per_encode": total, "tier1_ms": round(ms, 4),
             "source": "profiles/tier1_instructions_lossless_4096.txt (ncu smsp__inst_executed.sum)"}
