@@ -343,7 +343,8 @@ enum {
     J2K_BATCH_TILE97 = 3,        /* same for 9/7 images */
     J2K_BATCH_PHASE_A_ORDER = 4, /* 1: context modelling takes the largest code-blocks first */
     J2K_BATCH_MQ_VARIANT = 5,    /* read-only here; set with j2k_ctx_set_tuning */
-    J2K_BATCH_MQ_LANES = 6
+    J2K_BATCH_MQ_LANES = 6,
+    J2K_BATCH_MQ_TIERS = 7       /* read-only: 1 when the MQ coder runs the tiered warp schedule */
 };
 j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, j2k_batch** out);
 j2k_status j2k_batch_destroy(j2k_batch* b);

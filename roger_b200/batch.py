@@ -8,7 +8,6 @@ import torch
 
 from . import _lib as L
 from ._lib import check, lib
-from .codec import default_context
 
 TILE_NAMES = {0: "64x64", 1: "128x32", 2: "32x128"}
 
@@ -17,7 +16,9 @@ class BatchEncoder:
     """images: list of dicts with w, h, ncomp (1|3), kernel (53|97), levels, cb[, steps]."""
 
     def __init__(self, images, ctx=None):
-        self.ctx = ctx or default_context(0)
+        # a context of its own by default: autotune() sets the context's tier-1 schedule
+        from .codec import Context
+        self.ctx = ctx or Context(0)
         self.desc = list(images)
         n = len(self.desc)
         arr = (L.BatchImage * n)()
@@ -102,9 +103,13 @@ class BatchEncoder:
         rep = (C.c_int * 5)()
         hh = self.ctx._bind()
         check(lib().j2k_batch_autotune(self.h, reps, rep), hh)
+        tiers = C.c_int()
+        check(lib().j2k_batch_get_option(self.h, 7, C.byref(tiers)), hh)
+        mq = "state+code warp pair" if rep[3] else f"one lane per block, {rep[4]} per warp"
+        if tiers.value and not rep[3]:
+            mq += " after the tiers (longest blocks: 1 per warp, then 4 per warp)"
         return {"tile53": TILE_NAMES[rep[0]], "tile97": TILE_NAMES[rep[1]],
-                "phase_a_order": "largest-first" if rep[2] else "natural",
-                "mq": ("state+code warp pair" if rep[3] else f"one lane per block, {rep[4]} per warp")}
+                "phase_a_order": "largest-first" if rep[2] else "natural", "mq": mq}
 
     def results(self, pinned=True):
         """Every image's (descs, codeword bytes), read back in one packing pass and two copies

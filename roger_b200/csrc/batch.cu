@@ -443,6 +443,7 @@ j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
         case J2K_BATCH_PHASE_A_ORDER: *value = b->phase_a_order; break;
         case J2K_BATCH_MQ_VARIANT: *value = b->ctx->mq_variant; break;
         case J2K_BATCH_MQ_LANES: *value = b->ctx->mq_lanes; break;
+        case J2K_BATCH_MQ_TIERS: *value = b->ctx->mq_tier_lanes[0] > 0 && b->ctx->mq_tier_warps[0] > 0; break;
         default: return J2K_ERR_INVALID_ARG;
     }
     return J2K_OK;
@@ -550,20 +551,33 @@ j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report) {
         b->tile_code[f] = best_code;
         if (s == J2K_OK) s = plan_dwt(b);
     }
-    const int cand[4][2] = {{0, 8}, {0, 16}, {0, 32}, {1, 32}};
+    // MQ candidates: {variant, blocks per warp, tiered schedule on}; the tiers are the context's
+    // (by default one warp per SM with one block, two per SM with four blocks)
+    const int cand[7][3] = {{0, 8, 1}, {0, 16, 1}, {0, 32, 1}, {0, 8, 0}, {0, 16, 0}, {0, 32, 0}, {1, 32, 0}};
+    int tw[J2K_MQ_TIERS], tl[J2K_MQ_TIERS];
+    std::copy(ctx->mq_tier_warps, ctx->mq_tier_warps + J2K_MQ_TIERS, tw);
+    std::copy(ctx->mq_tier_lanes, ctx->mq_tier_lanes + J2K_MQ_TIERS, tl);
+    auto set_tiers = [&](bool on) {
+        for (int k = 0; k < J2K_MQ_TIERS; ++k) {
+            ctx->mq_tier_warps[k] = on ? tw[k] : 0;
+            ctx->mq_tier_lanes[k] = on ? tl[k] : 0;
+        }
+    };
     int best_order = 1, best_c = 0;
     float best_t = 1e30f;
     for (int ord = 0; ord < 2 && s == J2K_OK; ++ord)
-        for (int c = 0; c < 4 && s == J2K_OK; ++c) {
+        for (int c = 0; c < 7 && s == J2K_OK; ++c) {
             b->phase_a_order = ord;
             ctx->mq_variant = cand[c][0];
             ctx->mq_lanes = cand[c][1];
+            set_tiers(cand[c][2] != 0);
             s = time_stage(false, false, true, &t);
             if (s == J2K_OK && t < best_t) { best_t = t; best_order = ord; best_c = c; }
         }
     b->phase_a_order = best_order;
     ctx->mq_variant = cand[best_c][0];
     ctx->mq_lanes = cand[best_c][1];
+    set_tiers(cand[best_c][2] != 0);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->use_graph = graph;
