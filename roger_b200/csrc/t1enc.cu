@@ -639,48 +639,58 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
             next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
         }
     }
+    // 4 symbols per unrolled body over a rotating word (a 16-symbol body made the lone-block
+    // warps stall on instruction fetch)
     for (int k = 0; k < nchunks; ++k) {
         const uint4 cur = c0;
         c0 = c1;
         c1 = (k + 2 < nchunks) ? __ldcs(sp4 + k + 2) : z4;
         const int m = min(16, n - 16 * k);
-        const uint32_t w[5] = {cur.x, cur.y, cur.z, cur.w, c0.x};
+        uint32_t wa = cur.x, wb = cur.y, wc = cur.z, wd = cur.w;
+        const uint32_t we = c0.x;
+#pragma unroll 1
+        for (int q = 0; q < 4 && 4 * q < m; ++q) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            if (j < m) {
-                const uint32_t sym = (w[j >> 2] >> (8 * (j & 3))) & 0xFF;
-                const uint32_t nsym = (w[(j + 1) >> 2] >> (8 * ((j + 1) & 3))) & 0xFF;
-                const int d = sym >> 7;
-                const int ncx = min((int)(nsym & 31), 18);
-                uint32_t nent = st[ncx * kMqThreads];
-                const uint32_t qe = ent & 0xFFFF;
-                const int mps = ent >> 31;
-                const bool is_mps = d == mps;
-                const uint32_t a1 = e.A - qe;
-                const bool fast = is_mps && (a1 & 0x8000);
-                const bool addc = fast || (is_mps != (a1 < qe));
-                e.C += addc ? qe : 0u;
-                e.A = addc ? a1 : qe;
-                // state transition (not taken on the fast path)
-                const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
-                const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
-                const uint32_t upd = tab[nidx] | (nmps << 31);
-                if (!fast) {
-                    st[cx * kMqThreads] = upd;
-                    if (ncx == cx) nent = upd;
-                }
-                e.renorm(__clz(e.A) - 16);
-                cx = ncx;
-                ent = nent;
-                if (RATE) {
-                    const uint32_t done = (uint32_t)(16 * k + j + 1);
-                    while (done == next_end) {
-                        if (kp < 32) plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);
-                        ++kp;
-                        next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
+            for (int j = 0; j < 4; ++j) {
+                if (4 * q + j < m) {
+                    const uint32_t sym = (wa >> (8 * j)) & 0xFF;
+                    const uint32_t nsym = j < 3 ? (wa >> (8 * (j + 1))) & 0xFF : wb & 0xFF;
+                    const int d = sym >> 7;
+                    const int ncx = min((int)(nsym & 31), 18);
+                    uint32_t nent = st[ncx * kMqThreads];
+                    const uint32_t qe = ent & 0xFFFF;
+                    const int mps = ent >> 31;
+                    const bool is_mps = d == mps;
+                    const uint32_t a1 = e.A - qe;
+                    const bool fast = is_mps && (a1 & 0x8000);
+                    const bool addc = fast || (is_mps != (a1 < qe));
+                    e.C += addc ? qe : 0u;
+                    e.A = addc ? a1 : qe;
+                    // state transition (not taken on the fast path)
+                    const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
+                    const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
+                    const uint32_t upd = tab[nidx] | (nmps << 31);
+                    if (!fast) {
+                        st[cx * kMqThreads] = upd;
+                        if (ncx == cx) nent = upd;
+                    }
+                    e.renorm(__clz(e.A) - 16);
+                    cx = ncx;
+                    ent = nent;
+                    if (RATE) {
+                        const uint32_t done = (uint32_t)(16 * k + 4 * q + j + 1);
+                        while (done == next_end) {
+                            if (kp < 32) plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);
+                            ++kp;
+                            next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
+                        }
                     }
                 }
             }
+            wa = wb;
+            wb = wc;
+            wc = wd;
+            wd = we;
         }
     }
     int len = 0;
