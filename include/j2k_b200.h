@@ -206,7 +206,12 @@ j2k_status j2k_encoder_unmap_dwt_out(j2k_encoder* enc, void* ptr);
  * Pass descs/bytes NULL to query count and total bytes. */
 j2k_status j2k_encoder_get_codeblocks(j2k_encoder* enc, j2k_cb_desc* descs, size_t* count,
                                       uint8_t* bytes, size_t cap, size_t* used);
-/* T.800 codestream (SOC..EOC, one tile, one layer, LRCP) of the last run.  out NULL: size only. */
+/* Times the tier-1 MQ schedules (J2K_TUNE_MQ_TIER / _LANES) on the last run's coefficients and
+ * keeps the fastest in the encoder's context; the result stays that of the last run.
+ * report (optional, 4 ints): tier-0 warps, tier-1 warps, tier-1 blocks per warp, blocks per warp. */
+j2k_status j2k_encoder_autotune(j2k_encoder* enc, int reps, int* report);
+/* T.800 codestream (SOC..EOC, one tile, LRCP; one quality layer, or the layers asked for) of the
+ * last run.  out NULL: size only. */
 j2k_status j2k_encoder_get_codestream(j2k_encoder* enc, uint8_t* out, size_t cap, size_t* len);
 /* Device-side view of the last run's results (valid until the next run). */
 j2k_status j2k_encoder_device_results(j2k_encoder* enc, const j2k_cb_desc** descs,

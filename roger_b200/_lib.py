@@ -89,6 +89,7 @@ SIGS = {
     "j2k_decoder_destroy": (I, [P]),
     "j2k_decoder_run_codeblocks": (I, [P, P, P, S, I, I, S, S, P, P, I, S]),
     "j2k_decoder_run_batch": (I, [P, P, I]),
+    "j2k_encoder_autotune": (I, [P, I, P]),
     "j2k_dwt97_forward_adjoint": (I, [P, P, P, I, S, S, I]),
     "j2k_dwt97_inverse_adjoint": (I, [P, P, P, I, S, S, I]),
     "j2k_relaxed_quant_forward": (I, [P, P, P, I, S, S, I, P, C.c_uint64, P, I]),

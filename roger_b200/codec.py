@@ -280,6 +280,15 @@ class OCLEncoder(OCLEncodeDecode):
         self.w, self.h_, self.ncomp, self.levels = w, h, len(comps), levels
         return self
 
+    def autotune(self, reps=2):
+        """Times the tier-1 MQ warp schedules on the last run's coefficients and keeps the fastest
+        in this encoder's context (shared with every object on that context)."""
+        rep = (C.c_int * 4)()
+        hh = self.ctx._bind()
+        check(lib().j2k_encoder_autotune(self.h, reps, rep), hh)
+        return {"tier0_warps": rep[0], "tier1_warps": rep[1], "tier1_blocks_per_warp": rep[2],
+                "blocks_per_warp": rep[3]}
+
     def run_rgb(self, img, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None, target_bytes=0,
                 layers=None):
         """Interleaved uint8 image, (H, W, C) or (H, W); numpy (host) or CUDA tensor.

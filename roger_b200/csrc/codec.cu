@@ -183,7 +183,7 @@ static j2k_status rate_control(j2k_encoder* e) {
             continue;
         }
         size_t budget = budgets[l];
-        for (int it = 0; it < 6; ++it) {
+        for (int it = 0; it < 24; ++it) {
             std::memcpy(d.data(), dh, n * sizeof(j2k_cb_desc));
             j2k_pcrd_truncate(d.data(), n, pb, dist, w.data(), budget);
             for (size_t i = 0; i < n; ++i) {
@@ -195,13 +195,12 @@ static j2k_status rate_control(j2k_encoder* e) {
                                             e->mct != J2K_MCT_NONE, e->steps.data(), blocks, l + 1,
                                             e->lay_np.data(), e->lay_len.data());
             if (size <= budgets[l]) break;
-            const size_t excess = size - budgets[l] + 16;
-            if (budget <= excess) {
-                budget = 0;
-                if (it > 0) break;
-            } else {
-                budget -= excess;
-            }
+            // the headers of a cut differ from those of the one before: lower the codeword
+            // budget by the excess, by more on every try, until the codestream fits (with no
+            // codeword bytes left it holds headers only)
+            const size_t excess = size - budgets[l] + 16 + (size_t)it * it * 8;
+            if (budget == 0) break;
+            budget = budget > excess ? budget - excess : 0;
         }
     }
     const int32_t* fnp = e->lay_np.data() + (size_t)(L - 1) * n;
@@ -217,6 +216,8 @@ static j2k_status rate_control(j2k_encoder* e) {
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return J2K_OK;
 }
+
+static j2k_status run_tier1(j2k_encoder* e);
 
 static j2k_status encode_planes(j2k_encoder* e) {
     j2k_ctx* ctx = e->ctx;
@@ -238,6 +239,12 @@ static j2k_status encode_planes(j2k_encoder* e) {
     }
     e->have_result = true;
     if (e->dwt_only) return J2K_OK;
+    return run_tier1(e);
+}
+
+// Tier-1 of every code-block of the current coefficients (and rate control when asked for).
+static j2k_status run_tier1(j2k_encoder* e) {
+    j2k_ctx* ctx = e->ctx;
     J2K_TRY(prepare_jobs(ctx, e->hjobs, e->jobs, e->job_key, e->w, e->h, e->ncomp, e->levels, e->cbw,
                          e->cbh, &e->njobs));
     const size_t nblk = (size_t)e->cbw * e->cbh;
@@ -527,6 +534,62 @@ j2k_status j2k_encoder_get_codeblocks(j2k_encoder* e, j2k_cb_desc* descs, size_t
         }
     }
     return J2K_OK;
+}
+
+j2k_status j2k_encoder_autotune(j2k_encoder* e, int reps, int* report) {
+    if (!e) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    if (!e->have_result || e->dwt_only || e->njobs == 0)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "autotune needs the tier-1 result of a run");
+    cudaSetDevice(ctx->device);
+    reps = std::max(reps, 1);
+    // candidates: {tier-0 warps per SM, tier-1 warps per SM, tier-1 blocks per warp, blocks per
+    // warp after the tiers}; 0 warps: no tier
+    const int cand[8][4] = {{1, 2, 4, 16}, {1, 2, 4, 8}, {1, 2, 4, 32}, {1, 0, 0, 8},
+                            {1, 0, 0, 16}, {0, 0, 0, 8}, {2, 2, 4, 16}, {1, 2, 8, 16}};
+    cudaEvent_t e0, e1;
+    J2K_CUDA(ctx, cudaEventCreate(&e0));
+    J2K_CUDA(ctx, cudaEventCreate(&e1));
+    const int variant = ctx->mq_variant;
+    ctx->mq_variant = 0;
+    auto apply = [&](const int* c) {
+        for (int k = 0; k < J2K_MQ_TIERS; ++k) ctx->mq_tier_warps[k] = 0, ctx->mq_tier_lanes[k] = 0;
+        if (c[0]) ctx->mq_tier_warps[0] = c[0] * ctx->sm_count, ctx->mq_tier_lanes[0] = 1;
+        if (c[0] && c[1]) ctx->mq_tier_warps[1] = c[1] * ctx->sm_count, ctx->mq_tier_lanes[1] = c[2];
+        ctx->mq_lanes = c[3];
+    };
+    j2k_status s = J2K_OK;
+    int best = 0;
+    float best_t = 1e30f;
+    for (int c = 0; c < 8 && s == J2K_OK; ++c) {
+        apply(cand[c]);
+        float tmin = 1e30f;
+        for (int r = 0; r <= reps && s == J2K_OK; ++r) {  // the first run warms up
+            cudaEventRecord(e0, ctx->stream);
+            s = j2k_t1_encode_jobs(ctx, (const int32_t*)e->coef.p, (const j2k_cb_job*)e->jobs.p, e->njobs,
+                                   (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p, e->njobs * e->sym_cap, nullptr,
+                                   ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            if (s == J2K_OK) s = j2k_read_device_error(ctx);
+            float t = 0;
+            if (s == J2K_OK && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess && r > 0) tmin = std::min(tmin, t);
+        }
+        if (s == J2K_OK && tmin < best_t) best_t = tmin, best = c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    apply(cand[best]);
+    ctx->mq_variant = variant;
+    if (report) {
+        report[0] = ctx->mq_tier_warps[0];
+        report[1] = ctx->mq_tier_warps[1];
+        report[2] = ctx->mq_tier_lanes[1];
+        report[3] = ctx->mq_lanes;
+    }
+    // the result again, as the encoder left it (rate control included)
+    e->packed_ok = false;
+    if (s == J2K_OK) s = run_tier1(e);
+    return s;
 }
 
 j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, size_t* len) {

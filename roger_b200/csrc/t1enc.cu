@@ -974,7 +974,7 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     if (!tbuf) return J2K_ERR_OUT_OF_MEMORY;
     J2K_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, nsyms, keys_out, idx_in, idx_out,
                                                             (int)njobs, 0, 32, st));
-    if (ctx->mq_variant == 1) {
+    if (ctx->mq_variant == 1 && !(plane_bytes && dist)) {  // the rate path runs the one-lane coder
         unsigned gp = (unsigned)((njobs + 31) / 32);
         t1_mq_pair_kernel<<<gp, 64, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err);
         J2K_CUDA(ctx, cudaGetLastError());
@@ -994,17 +994,22 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     }
     warps += (left + lanes - 1) / lanes;
     unsigned gb = (unsigned)((warps + kMqThreads / 32 - 1) / (kMqThreads / 32));
-    if (plane_bytes && dist) {
-        // rate control: byte positions at every bit-plane end, and the distortion of each
-        // truncation point (the coefficients are still in place)
-        t1_mq_kernel<8, true><<<(unsigned)((njobs + 15) / 16), kMqThreads, 0, st>>>(
-            syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err, pend, plane_bytes);
+    const bool rate = plane_bytes && dist;
+    // rate control also records the byte positions at every bit-plane end, and the distortion
+    // of each truncation point (the coefficients are still in place)
+    if (rate) {
+        if (lanes == 8)
+            t1_mq_kernel<8, true><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs,
+                                                             ctx->d_err, pend, plane_bytes, sc);
+        else if (lanes == 16)
+            t1_mq_kernel<16, true><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs,
+                                                              ctx->d_err, pend, plane_bytes, sc);
+        else
+            t1_mq_kernel<32, true><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs,
+                                                              ctx->d_err, pend, plane_bytes, sc);
         J2K_CUDA(ctx, cudaGetLastError());
         t1_dist_kernel<<<(unsigned)((njobs + 1) / 2), 64, 0, st>>>(coeff, d_jobs, descs, (int)njobs, dist);
-        J2K_CUDA(ctx, cudaGetLastError());
-        return J2K_OK;
-    }
-    if (lanes == 8)
+    } else if (lanes == 8)
         t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err,
                                                    nullptr, nullptr, sc);
     else if (lanes == 16)

@@ -214,3 +214,13 @@ def test_quality_layers():
         im.tile = [type(t)(t[0], t[1], t[2], (t[3][0], 0, k) + tuple(t[3][3:]))]
         theirs = np.asarray(im).reshape(img.shape)
         assert abs(_psnr(theirs, img) - p) < 1.0
+
+
+@pytest.mark.gpu
+def test_rate_control_never_exceeds_the_budget():
+    from roger_b200 import codec as C
+    img = synth.rgb(512, 384, (75, 76, 77, 78))
+    enc = C.OCLEncoder()
+    for t in list(range(11900, 12101, 13)) + [2500, 5000, 20000, 40000]:
+        n = len(bytes(enc.run_rgb(img, levels=5, target_bytes=t).codestream()))
+        assert n <= t, (t, n)
