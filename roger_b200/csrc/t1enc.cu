@@ -650,6 +650,8 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
         const uint32_t we = c0.x;
 #pragma unroll 1
         for (int q = 0; q < 4 && 4 * q < m; ++q) {
+            // RATE: only a group that holds a bit-plane end checks symbol by symbol
+            const bool hit = RATE && next_end <= (uint32_t)(16 * k + 4 * q + 4);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (4 * q + j < m) {
@@ -677,7 +679,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
                     e.renorm(__clz(e.A) - 16);
                     cx = ncx;
                     ent = nent;
-                    if (RATE) {
+                    if (RATE && hit) {
                         const uint32_t done = (uint32_t)(16 * k + 4 * q + j + 1);
                         while (done == next_end) {
                             if (kp < 32) plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);

@@ -224,3 +224,31 @@ def test_rate_control_never_exceeds_the_budget():
     for t in list(range(11900, 12101, 13)) + [2500, 5000, 20000, 40000]:
         n = len(bytes(enc.run_rgb(img, levels=5, target_bytes=t).codestream()))
         assert n <= t, (t, n)
+
+
+@pytest.mark.gpu
+def test_cut_lengths_are_the_oracles_plane_end_lengths():
+    # every cut block keeps exactly the bytes the oracle's MQ coder had produced at the end of
+    # that bit-plane, plus the read-ahead margin: checks the rate pass's plane-end records
+    from roger_b200 import codec as C
+    img = synth.rgb(256, 192, (81, 82, 83, 84))
+    L = 4
+    enc = C.OCLEncoder()
+    full = len(enc.run_rgb(img, levels=L, cbw=32, cbh=32).codestream())
+    planes = O.planar_fwd(img, 1)
+    coef = [O.dwt53_fwd(planes[c], L) for c in range(3)]
+    checked = 0
+    for frac in (0.05, 0.2, 0.5):
+        cs = bytes(enc.run_rgb(img, levels=L, cbw=32, cbh=32, target_bytes=int(full * frac)).codestream())
+        _, descs, _ = C.read_codestream(cs)
+        for d in descs:
+            if d["npasses"] == 0:
+                continue
+            blk = coef[d["comp"]][d["y0"]:d["y0"] + d["ch"], d["x0"]:d["x0"] + d["cw"]]
+            _, info = O.t1_encode(blk, int(d["orient"]))
+            assert info["numbps"] == d["numbps"]
+            k = (int(d["npasses"]) - 1) // 3
+            assert (int(d["npasses"]) - 1) % 3 == 0
+            assert int(d["length"]) == O.truncation_length(info, k)
+            checked += 1
+    assert checked > 100
