@@ -570,7 +570,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
               const uint32_t* __restrict__ pend = nullptr, uint32_t* __restrict__ plane_bytes = nullptr,
               MqSchedule sched = MqSchedule{}) {
     __shared__ uint32_t tab[47];
-    __shared__ uint32_t cst[19 * kMqThreads];
+    __shared__ uint32_t cst[32 * kMqThreads];  // contexts 0..18 used; 32 so that a 5-bit index needs no clamp
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
         tab[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
@@ -597,7 +597,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
     const int jid = order ? (int)order[gid] : gid;
     const int t = threadIdx.x;
     uint32_t* st = cst + t;  // context k at st[k * kMqThreads]
-    for (int k = 0; k < 19; ++k) st[k * kMqThreads] = tab[0];
+    for (int k = 0; k < 32; ++k) st[k * kMqThreads] = tab[0];
     st[0] = tab[4];
     st[17 * kMqThreads] = tab[3];
     st[18 * kMqThreads] = tab[46];
@@ -623,7 +623,7 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
     const uint4 z4 = make_uint4(0, 0, 0, 0);
     uint4 c0 = nchunks > 0 ? __ldcs(sp4) : z4;
     uint4 c1 = nchunks > 1 ? __ldcs(sp4 + 1) : z4;
-    int cx = min((int)(c0.x & 31), 18);
+    int cx = (int)(c0.x & 31);
     uint32_t ent = st[cx * kMqThreads];
     // RATE bookkeeping: next cleanup pass (3 * kp) and the symbol count at which it ends
     int kp = 0, npass = 0;
@@ -639,6 +639,39 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
             next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
         }
     }
+    // one symbol: d (bit 7) coded in context cx; the next symbol's context state is loaded now
+    // and forwarded if this symbol updates the same context
+    auto step = [&](uint32_t sym, uint32_t nsym, bool hit, uint32_t done) {
+        const int d = sym >> 7;
+        const int ncx = (int)(nsym & 31);
+        uint32_t nent = st[ncx * kMqThreads];
+        const uint32_t qe = ent & 0xFFFF;
+        const int mps = ent >> 31;
+        const bool is_mps = d == mps;
+        const uint32_t a1 = e.A - qe;
+        const bool fast = is_mps && (a1 & 0x8000);
+        const bool addc = fast || (is_mps != (a1 < qe));
+        e.C += addc ? qe : 0u;
+        e.A = addc ? a1 : qe;
+        // state transition (not taken on the fast path)
+        const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
+        const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
+        const uint32_t upd = tab[nidx] | (nmps << 31);
+        if (!fast) {
+            st[cx * kMqThreads] = upd;
+            if (ncx == cx) nent = upd;
+        }
+        e.renorm(__clz(e.A) - 16);
+        cx = ncx;
+        ent = nent;
+        if (RATE && hit) {
+            while (done == next_end) {
+                if (kp < 32) plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);
+                ++kp;
+                next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
+            }
+        }
+    };
     // 4 symbols per unrolled body over a rotating word (a 16-symbol body made the lone-block
     // warps stall on instruction fetch)
     for (int k = 0; k < nchunks; ++k) {
@@ -652,42 +685,17 @@ t1_mq_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jo
         for (int q = 0; q < 4 && 4 * q < m; ++q) {
             // RATE: only a group that holds a bit-plane end checks symbol by symbol
             const bool hit = RATE && next_end <= (uint32_t)(16 * k + 4 * q + 4);
+            const uint32_t base = (uint32_t)(16 * k + 4 * q);
+            if (4 * q + 4 <= m) {  // a full group: no per-symbol bound
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (4 * q + j < m) {
-                    const uint32_t sym = (wa >> (8 * j)) & 0xFF;
-                    const uint32_t nsym = j < 3 ? (wa >> (8 * (j + 1))) & 0xFF : wb & 0xFF;
-                    const int d = sym >> 7;
-                    const int ncx = min((int)(nsym & 31), 18);
-                    uint32_t nent = st[ncx * kMqThreads];
-                    const uint32_t qe = ent & 0xFFFF;
-                    const int mps = ent >> 31;
-                    const bool is_mps = d == mps;
-                    const uint32_t a1 = e.A - qe;
-                    const bool fast = is_mps && (a1 & 0x8000);
-                    const bool addc = fast || (is_mps != (a1 < qe));
-                    e.C += addc ? qe : 0u;
-                    e.A = addc ? a1 : qe;
-                    // state transition (not taken on the fast path)
-                    const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
-                    const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
-                    const uint32_t upd = tab[nidx] | (nmps << 31);
-                    if (!fast) {
-                        st[cx * kMqThreads] = upd;
-                        if (ncx == cx) nent = upd;
-                    }
-                    e.renorm(__clz(e.A) - 16);
-                    cx = ncx;
-                    ent = nent;
-                    if (RATE && hit) {
-                        const uint32_t done = (uint32_t)(16 * k + 4 * q + j + 1);
-                        while (done == next_end) {
-                            if (kp < 32) plane_bytes[(size_t)jid * 32 + kp] = (uint32_t)(e.bp + 1);
-                            ++kp;
-                            next_end = 3 * kp < npass ? pe[3 * kp] : 0xFFFFFFFFu;
-                        }
-                    }
-                }
+                for (int j = 0; j < 4; ++j)
+                    step((wa >> (8 * j)) & 0xFF, j < 3 ? (wa >> (8 * (j + 1))) & 0xFF : wb & 0xFF, hit, base + j + 1);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (4 * q + j < m)
+                        step((wa >> (8 * j)) & 0xFF, j < 3 ? (wa >> (8 * (j + 1))) & 0xFF : wb & 0xFF, hit,
+                             base + j + 1);
             }
             wa = wb;
             wb = wc;
