@@ -272,6 +272,19 @@ typedef struct {
 j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
                                size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
                                size_t errlen);
+/* Tier-2 only: writes the codestream of code-blocks coded elsewhere (this library's encoders,
+ * j2k_codestream_read, or another tier-1), host memory, no context.  descs in job order
+ * (component, subband in QCD order, raster), codewords in `bytes` at descs[i].offset; lossless
+ * selects 5/3 (RCT for 3 components), else 9/7 (ICT) with `steps` (3*levels+1, NULL =
+ * 8*2^-level).  layers <= 1 with NULL arrays: one layer holding every block's npasses and
+ * length.  Else `layers` quality layers: after layer l block i holds layer_npasses[l*count+i]
+ * passes and the first layer_lengths[l*count+i] bytes of its codeword (non-decreasing in l, at
+ * most the descriptor's; 0 bytes when 0 passes).  out NULL: size only.  The reference writes no
+ * codestream. */
+j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, int levels, int cbw, int cbh, int lossless,
+                                const float* steps, const j2k_cb_desc* descs, size_t count, const uint8_t* bytes,
+                                size_t nbytes, int layers, const int32_t* layer_npasses,
+                                const int32_t* layer_lengths, uint8_t* out, size_t cap, size_t* len);
 /* Same, keeping only the first max_layers quality layers (0: all): each block's codeword is the
  * concatenation of its segments from those layers and npasses counts their passes, so the
  * result decodes to the image at that layer's quality. */

@@ -74,6 +74,7 @@ SIGS = {
     "j2k_codeblock_count": (S, [S, S, I, I, I]),
     "j2k_codestream_read": (I, [P, S, P, P, P, P, S, P, P, S]),
     "j2k_codestream_read_layers": (I, [P, S, I, P, P, P, P, S, P, P, S]),
+    "j2k_codestream_write": (I, [C.c_uint32, C.c_uint32, I, I, I, I, I, P, P, S, P, S, I, P, P, P, S, P]),
     "j2k_bpc_encode": (I, [P, P, S, S, S, I, I, I, P, P, S]),
     "j2k_bpc_decode": (I, [P, P, P, S, P, S, S, S, I, I, I]),
     "j2k_encoder_create": (I, [P, I, I, C.POINTER(P)]),

@@ -427,6 +427,34 @@ def read_codestream(cs, max_layers=0):
     return d, descs, data[:used.value]
 
 
+def write_codestream(w, h, ncomp, levels, descs, data, cbw=64, cbh=64, lossless=True, steps=None, layers=None):
+    """Tier-2 only (host): the codestream of code-blocks coded elsewhere.  descs/data as
+    get_codeblocks or read_codestream return them (job order).  layers: None for one layer, or
+    (npasses, lengths), two (L, count) int arrays of what each block holds after each layer."""
+    descs = np.ascontiguousarray(descs)
+    data = np.ascontiguousarray(data, np.uint8)
+    st = None if steps is None else np.ascontiguousarray(steps, np.float32)
+    nl, lp, ll = 0, None, None
+    if layers is not None:
+        lp = np.ascontiguousarray(layers[0], np.int32)
+        ll = np.ascontiguousarray(layers[1], np.int32)
+        if lp.shape != ll.shape or lp.ndim != 2 or lp.shape[1] != descs.size:
+            raise ValueError("layers: two (L, count) arrays")
+        nl = lp.shape[0]
+    args = (w, h, ncomp, levels, cbw, cbh, int(lossless), None if st is None else st.ctypes.data,
+            descs.ctypes.data, descs.size, data.ctypes.data, data.size, nl,
+            None if lp is None else lp.ctypes.data, None if ll is None else ll.ctypes.data)
+    n = C.c_size_t()
+    s = lib().j2k_codestream_write(*args, None, 0, C.byref(n))
+    if s != 0:
+        raise L.J2KError(s, "j2k_codestream_write: invalid arguments")
+    out = np.zeros(n.value, np.uint8)
+    s = lib().j2k_codestream_write(*args, out.ctypes.data, out.size, C.byref(n))
+    if s != 0:
+        raise L.J2KError(s, "j2k_codestream_write failed")
+    return out.tobytes()
+
+
 def decode_codestream(cs, ctx=None, max_layers=0):
     """Decodes a codestream on the GPU: tier-2 on the host, then tier-1, inverse DWT and inverse
     colour transform on the device.  max_layers > 0 decodes only the first quality layers.

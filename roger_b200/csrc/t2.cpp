@@ -458,6 +458,62 @@ int get_npasses(BitReader& br) {  // Table B.4
 
 }  // namespace
 
+extern "C" j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, int levels, int cbw, int cbh,
+                                           int lossless, const float* steps, const j2k_cb_desc* descs,
+                                           size_t count, const uint8_t* bytes, size_t nbytes, int layers,
+                                           const int32_t* layer_npasses, const int32_t* layer_lengths, uint8_t* out,
+                                           size_t cap, size_t* len) {
+    if (!len || (!descs && count) || (!bytes && nbytes)) return J2K_ERR_INVALID_ARG;
+    auto pow2 = [](int v) { return v >= 4 && v <= 64 && (v & (v - 1)) == 0; };
+    if (w == 0 || h == 0 || w > 65535 || h > 65535 || (ncomp != 1 && ncomp != 3) || levels < 0 || levels > 32 ||
+        !pow2(cbw) || !pow2(cbh) || cbw * cbh > 4096)
+        return J2K_ERR_INVALID_ARG;
+    if (count != j2k_build_jobs(w, h, levels, cbw, cbh, nullptr) * (size_t)ncomp) return J2K_ERR_INVALID_ARG;
+    const bool layered = layers > 1 || (layers == 1 && layer_npasses && layer_lengths);
+    if (layers < 0 || layers > 64 || (layered && (!layer_npasses || !layer_lengths))) return J2K_ERR_INVALID_ARG;
+    const int nl = layered ? layers : 1;
+    std::vector<j2k_t2_block> blocks(count);
+    for (size_t i = 0; i < count; ++i) {
+        const j2k_cb_desc& d = descs[i];
+        if (d.numbps > 31 || d.length < 0 || (d.numbps && d.npasses > 3 * d.numbps - 2) || (!d.numbps && d.npasses) ||
+            (size_t)d.offset + (size_t)d.length > nbytes)
+            return J2K_ERR_INVALID_ARG;
+        blocks[i] = j2k_t2_block{d.numbps, d.npasses, d.length, bytes ? bytes + d.offset : nullptr};
+        if (layered) {
+            int pn = 0, pl = 0;
+            for (int l = 0; l < nl; ++l) {
+                const int np = layer_npasses[(size_t)l * count + i], ln = layer_lengths[(size_t)l * count + i];
+                if (np < pn || ln < pl || np > d.npasses || ln > d.length || (np == 0 && ln != 0))
+                    return J2K_ERR_INVALID_ARG;
+                pn = np;
+                pl = ln;
+            }
+        }
+    }
+    std::vector<float> st;
+    if (!lossless) {
+        const int nb = 3 * levels + 1;
+        if (steps) {
+            st.assign(steps, steps + nb);
+        } else {
+            std::vector<j2k_band_rect> r(nb);
+            j2k_band_rects(w, h, levels, r.data());
+            st.resize(nb);
+            for (int b = 0; b < nb; ++b) st[b] = 8.0f * std::ldexp(1.0f, -r[b].level);
+        }
+        for (float v : st)
+            if (!(v > 0.0f)) return J2K_ERR_INVALID_ARG;
+    }
+    Bytes o;
+    t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless ? 1 : 0, ncomp == 3, lossless ? nullptr : st.data(), blocks,
+            true, nl, layered ? layer_npasses : nullptr, layered ? layer_lengths : nullptr);
+    *len = o.v.size();
+    if (!out) return J2K_OK;
+    if (cap < o.v.size()) return J2K_ERR_CAPACITY;
+    std::memcpy(out, o.v.data(), o.v.size());
+    return J2K_OK;
+}
+
 namespace {
 
 // Parses a codestream into stream parameters, one descriptor per code-block (job order:

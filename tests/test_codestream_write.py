@@ -1,0 +1,138 @@
+"""Host tier-2 writer (j2k_codestream_write), on the CPU: code-blocks coded by the oracle's
+tier-1 are written into codestreams.  One layer must be byte-identical to the oracle's own
+codestream; quality layers (cut at the oracle's bit-plane truncation points) must parse back
+through j2k_codestream_read_layers to exactly the passes and bytes written, decode losslessly
+in OpenJPEG when complete, and decode each prefix of layers like the oracle's decode of the same
+cuts (OpenJPEG: within 1 dB)."""
+import io
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from roger_b200 import _lib as L
+from roger_b200 import codec as C
+from roger_b200 import synth
+from roger_b200._lib import J2KError
+
+PIL = pytest.importorskip("PIL.Image")
+
+
+def _blocks(img, levels, cb):
+    """Oracle tier-1 of every code-block of the lossless transform, in job order."""
+    h, w = img.shape[:2]
+    nc = 1 if img.ndim == 2 else img.shape[2]
+    planes = O.planar_fwd(img, 1 if nc == 3 else 0)
+    descs, datas, infos, coefs = [], [], [], []
+    off = 0
+    for c in range(nc):
+        co = O.dwt53_fwd(planes[c], levels)
+        coefs.append(co)
+        for b, (x0, y0, sw, sh, o, lv) in enumerate(O.subbands(w, h, levels)):
+            if not sw or not sh:
+                continue
+            for by in range(0, sh, cb):
+                for bx in range(0, sw, cb):
+                    blk = co[y0 + by:y0 + min(by + cb, sh), x0 + bx:x0 + min(bx + cb, sw)]
+                    data, info = O.t1_encode(blk, o)
+                    d = np.zeros(1, L.CB_DESC)[0]
+                    d["offset"], d["length"], d["numbps"], d["npasses"] = off, info["length"], info["numbps"], info["npasses"]
+                    d["orient"], d["band"], d["x0"], d["y0"] = o, b, x0 + bx, y0 + by
+                    d["cw"], d["ch"], d["comp"] = blk.shape[1], blk.shape[0], c
+                    descs.append(d)
+                    datas.append(data)
+                    infos.append(info)
+                    off += len(data)
+    return np.array(descs, L.CB_DESC), np.frombuffer(b"".join(datas), np.uint8), infos, coefs
+
+
+CASES = [(96, 80, 3, 3, 32), (131, 97, 1, 4, 64), (200, 64, 3, 5, 64)]
+
+
+@pytest.mark.parametrize("w,h,nc,lv,cb", CASES)
+def test_one_layer_is_the_oracles_codestream(w, h, nc, lv, cb):
+    img = synth.gray(w, h, 91) if nc == 1 else synth.rgb(w, h, (91, 92, 93, 94))
+    descs, data, _, _ = _blocks(img, lv, cb)
+    cs = C.write_codestream(w, h, nc, lv, descs, data, cb, cb)
+    assert cs == bytes(O.encode_image(img, lv, cb, cb, True))
+
+
+def _layers(descs, infos, cuts):
+    """(L, n) passes and lengths: layer l cuts block i after bit-plane cuts[l](numbps) (None: all)."""
+    n = len(descs)
+    npl = np.zeros((len(cuts), n), np.int32)
+    lnl = np.zeros((len(cuts), n), np.int32)
+    for i, info in enumerate(infos):
+        nb = info["numbps"]
+        for l, cut in enumerate(cuts):
+            if nb == 0:
+                continue
+            k = nb - 1 if cut is None else min(cut(nb), nb - 1)
+            if k < 0:
+                continue
+            npl[l, i] = min(3 * k + 1, info["npasses"])
+            lnl[l, i] = O.truncation_length(info, k)
+    return npl, lnl
+
+
+def _oracle_decode(img_shape, lv, descs, data):
+    h, w = img_shape[:2]
+    nc = 1 if len(img_shape) == 2 else img_shape[2]
+    planes = np.zeros((nc, h, w), np.int32)
+    for d in descs:
+        if d["npasses"] == 0:
+            continue
+        blk = O.t1_decode(bytes(data[d["offset"]:d["offset"] + d["length"]]), int(d["numbps"]), int(d["npasses"]),
+                          int(d["orient"]), int(d["cw"]), int(d["ch"]))
+        planes[d["comp"], d["y0"]:d["y0"] + d["ch"], d["x0"]:d["x0"] + d["cw"]] = blk
+    rec = np.stack([O.dwt53_inv(p, lv) for p in planes])
+    return O.planar_inv(rec, 1 if nc == 3 else 0).reshape(img_shape)
+
+
+def _psnr(a, b):
+    e = a.astype(np.float64) - b.astype(np.float64)
+    return 10 * np.log10(255.0 ** 2 / max((e * e).mean(), 1e-12))
+
+
+@pytest.mark.parametrize("w,h,nc,lv,cb", CASES)
+def test_quality_layers_round_trip(w, h, nc, lv, cb):
+    img = synth.gray(w, h, 95) if nc == 1 else synth.rgb(w, h, (95, 96, 97, 98))
+    descs, data, infos, _ = _blocks(img, lv, cb)
+    cuts = [lambda nb: 0, lambda nb: nb // 2, None]
+    npl, lnl = _layers(descs, infos, cuts)
+    cs = C.write_codestream(w, h, nc, lv, descs, data, cb, cb, layers=(npl, lnl))
+    info, full, fdata = C.read_codestream(cs)
+    assert info["layers"] == 3
+    # complete stream: lossless, ours and OpenJPEG's
+    assert np.array_equal(_oracle_decode(img.shape, lv, full, fdata), img)
+    assert np.array_equal(np.asarray(PIL.open(io.BytesIO(cs))).reshape(img.shape), img)
+    last = -1.0
+    for keep in (1, 2):
+        _, d, b = C.read_codestream(cs, max_layers=keep)
+        assert np.array_equal(d["npasses"], npl[keep - 1]) and np.array_equal(d["length"], lnl[keep - 1])
+        for k in range(len(d)):
+            n = int(d["length"][k])
+            assert bytes(b[d["offset"][k]:d["offset"][k] + n]) == bytes(data[descs["offset"][k]:descs["offset"][k] + n])
+        ours = _oracle_decode(img.shape, lv, d, b)
+        p = _psnr(ours, img)
+        assert p > last
+        last = p
+        im = PIL.open(io.BytesIO(cs))
+        t = im.tile[0]
+        im.tile = [type(t)(t[0], t[1], t[2], (t[3][0], 0, keep) + tuple(t[3][3:]))]
+        theirs = np.asarray(im).reshape(img.shape)
+        assert abs(_psnr(theirs, img) - p) < 1.0
+
+
+def test_bad_arguments_are_refused():
+    img = synth.gray(64, 48, 99)
+    descs, data, infos, _ = _blocks(img, 2, 32)
+    with pytest.raises(J2KError):  # block count of another geometry
+        C.write_codestream(64, 48, 1, 3, descs, data, 32, 32)
+    bad = descs.copy()
+    bad["length"][0] = len(data) + 1
+    with pytest.raises(J2KError):  # codeword beyond the bytes
+        C.write_codestream(64, 48, 1, 2, bad, data, 32, 32)
+    npl, lnl = _layers(descs, infos, [lambda nb: nb // 2, lambda nb: 0])
+    with pytest.raises(J2KError):  # layers that shrink
+        C.write_codestream(64, 48, 1, 2, descs, data, 32, 32, layers=(npl, lnl))
