@@ -665,8 +665,9 @@ def bench_batched(n, flush):
     dec_same = all(np.array_equal(a.reshape(-1), b.reshape(-1)) for a, b in zip(outs, outs1))
     exact53 = all(np.array_equal(o.reshape(-1), im.cpu().numpy().reshape(-1))
                   for d, o, im in zip(descs, outs, imgs) if d["kernel"] == 53)
-    decode = {"path": "decode_codestreams (tier-2 per stream on the host, one upload, one tier-1 launch, "
-                      "per-image inverse DWT + colour transform, one read-back) vs decode_codestream per image",
+    decode = {"path": "decode_codestreams (tier-2 of the streams on host threads, one upload, one tier-1 "
+                      "launch, per-image inverse DWT + colour transform, one read-back) vs decode_codestream per "
+                      "image",
               "batched_ms": round(t_dec_b, 3), "batched_mpix_s": round(mpix / (t_dec_b * 1e-3), 1),
               "per_image_ms": round(t_dec_1, 3), "per_image_mpix_s": round(mpix / (t_dec_1 * 1e-3), 1),
               "speedup": round(t_dec_1 / t_dec_b, 2), "identical": bool(dec_same), "lossless_exact_53": bool(exact53)}

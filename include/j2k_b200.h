@@ -246,6 +246,11 @@ typedef struct {
     uint8_t* out;              /* host output */
 } j2k_decode_item;
 j2k_status j2k_decoder_run_batch(j2k_decoder* dec, const j2k_decode_item* items, int n);
+/* The same from codestreams: each stream's tier-2 runs on a pool of host threads (the first
+ * max_layers quality layers, 0: all), then the batched decode above; outs[k] receives stream k's
+ * pixels (interleaved uint8, w*h*ncomp bytes; j2k_codestream_info gives w, h, ncomp). */
+j2k_status j2k_decoder_run_codestreams(j2k_decoder* dec, const uint8_t* const* streams, const size_t* sizes, int n,
+                                       int max_layers, uint8_t* const* outs);
 
 /* ---- codestream reading (tier-2 decoding).  No counterpart in the reference, which writes and
  * reads no codestream.  Parses a T.800 codestream of one tile (tile-parts allowed), any number of
@@ -285,6 +290,8 @@ j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, int levels, i
                                 const float* steps, const j2k_cb_desc* descs, size_t count, const uint8_t* bytes,
                                 size_t nbytes, int layers, const int32_t* layer_npasses,
                                 const int32_t* layer_lengths, uint8_t* out, size_t cap, size_t* len);
+/* Only the main header: the stream info without parsing any packet (cheap). */
+j2k_status j2k_codestream_info(const uint8_t* cs, size_t n, j2k_stream_info* info, char* err, size_t errlen);
 /* Same, keeping only the first max_layers quality layers (0: all): each block's codeword is the
  * concatenation of its segments from those layers and npasses counts their passes, so the
  * result decodes to the image at that layer's quality. */

@@ -90,6 +90,8 @@ SIGS = {
     "j2k_decoder_destroy": (I, [P]),
     "j2k_decoder_run_codeblocks": (I, [P, P, P, S, I, I, S, S, P, P, I, S]),
     "j2k_decoder_run_batch": (I, [P, P, I]),
+    "j2k_decoder_run_codestreams": (I, [P, P, P, I, I, P]),
+    "j2k_codestream_info": (I, [P, S, P, P, S]),
     "j2k_encoder_autotune": (I, [P, I, P]),
     "j2k_dwt97_forward_adjoint": (I, [P, P, P, I, S, S, I]),
     "j2k_dwt97_inverse_adjoint": (I, [P, P, P, I, S, S, I]),

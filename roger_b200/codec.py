@@ -465,26 +465,37 @@ def decode_codestream(cs, ctx=None, max_layers=0):
                    cbh=info["cbh"], steps=None if info["lossless"] else info["steps"])
 
 
+def codestream_info(cs):
+    """The main header of a codestream (no packet is parsed): w, h, ncomp, levels, ..."""
+    buf = np.frombuffer(bytes(cs), np.uint8)
+    info = L.StreamInfo()
+    err = C.create_string_buffer(256)
+    s = lib().j2k_codestream_info(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(info), err, 256)
+    if s != 0:
+        raise L.J2KError(s, err.value.decode())
+    return dict(w=info.w, h=info.h, ncomp=info.ncomp, levels=info.levels, cbw=info.cbw, cbh=info.cbh,
+                lossless=bool(info.lossless), layers=info.layers, progression=info.progression)
+
+
 def decode_codestreams(streams, ctx=None, max_layers=0, decoder=None):
-    """Batched GPU decode of many codestreams: tier-2 of each on the host, then one upload of all
-    code-blocks, one tier-1 launch over every block of every image, the inverse DWT and colour
-    transform per image, and one read-back.  Returns a list of (H, W[, C]) uint8 arrays."""
+    """Batched GPU decode of many codestreams: tier-2 of every stream on a pool of host threads,
+    then one upload of all code-blocks, one tier-1 launch over every block of every image, the
+    inverse DWT and colour transform per image, and one read-back.  Returns a list of
+    (H, W[, C]) uint8 arrays."""
     ctx = ctx or default_context(0)
-    parsed = [read_codestream(cs, max_layers) for cs in streams]
-    items = (L.DecodeItem * len(parsed))()
-    keep, outs = [], []
-    for k, (info, descs, data) in enumerate(parsed):
+    bufs = [np.frombuffer(bytes(cs), np.uint8) for cs in streams]
+    outs = []
+    for b in bufs:
+        info = codestream_info(b)
         nc = info["ncomp"]
-        out = np.empty((info["h"], info["w"], nc) if nc > 1 else (info["h"], info["w"]), np.uint8)
-        st = np.ascontiguousarray(info["steps"], np.float32)
-        keep += [descs, data, st]
-        outs.append(out)
-        items[k] = L.DecodeItem(info["w"], info["h"], nc, int(info["lossless"]), info["levels"], info["cbw"],
-                                info["cbh"], None if info["lossless"] else st.ctypes.data, descs.ctypes.data,
-                                descs.size, data.ctypes.data, int(data.size), out.ctypes.data)
+        outs.append(np.empty((info["h"], info["w"], nc) if nc > 1 else (info["h"], info["w"]), np.uint8))
+    n = len(bufs)
+    sp = (C.c_void_p * n)(*[b.ctypes.data for b in bufs])
+    sz = (C.c_size_t * n)(*[b.size for b in bufs])
+    op = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
     dec = decoder or OCLDecoder(ctx=ctx)  # a kept decoder reuses its device buffers
     hh = dec.ctx._bind()
-    check(lib().j2k_decoder_run_batch(dec.h, items, len(parsed)), hh)
+    check(lib().j2k_decoder_run_codestreams(dec.h, sp, sz, n, int(max_layers), op), hh)
     return outs
 
 

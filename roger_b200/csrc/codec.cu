@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <thread>
 
 #include "j2k_internal.cuh"
 
@@ -754,6 +755,44 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
     J2K_TRY(j2k_read_device_error(ctx));
     for (int k = 0; k < n; ++k) std::memcpy(items[k].out, hs + out_off[k], out_off[k + 1] - out_off[k]);
     return J2K_OK;
+}
+
+j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* streams, const size_t* sizes, int n,
+                                       int max_layers, uint8_t* const* outs) {
+    if (!d || n < 0 || (n > 0 && (!streams || !sizes || !outs)) || max_layers < 0) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = d->ctx;
+    if (n == 0) return J2K_OK;
+    // tier-2 of every stream on host threads, then one batched device decode
+    std::vector<j2k_stream_info> info(n);
+    std::vector<std::vector<j2k_cb_desc>> descs(n);
+    std::vector<std::vector<uint8_t>> bytes(n);
+    std::vector<j2k_status> st(n, J2K_OK);
+    std::vector<std::string> msg(n);
+    const int nt = (int)std::min<unsigned>((unsigned)n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    auto work = [&](int t) {
+        for (int k = t; k < n; k += nt) {
+            if (!streams[k]) {
+                st[k] = J2K_ERR_INVALID_ARG;
+                msg[k] = "NULL stream";
+                continue;
+            }
+            st[k] = j2k_t2_parse_packed(streams[k], sizes[k], max_layers, &info[k], &descs[k], &bytes[k], &msg[k]);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    std::vector<j2k_decode_item> items(n);
+    for (int k = 0; k < n; ++k) {
+        if (st[k] != J2K_OK) return j2k_fail(ctx, st[k], "stream " + std::to_string(k) + ": " + msg[k]);
+        const j2k_stream_info& I = info[k];
+        if (I.precision != 8) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "stream " + std::to_string(k) + ": precision");
+        items[k] = j2k_decode_item{I.w, I.h, I.ncomp, I.lossless, I.levels, I.cbw, I.cbh,
+                                   I.lossless ? nullptr : I.steps, descs[k].data(), descs[k].size(),
+                                   bytes[k].data(), bytes[k].size(), outs[k]};
+    }
+    return j2k_decoder_run_batch(d, items.data(), n);
 }
 
 j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, const uint8_t* bytes,

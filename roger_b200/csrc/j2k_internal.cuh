@@ -177,6 +177,10 @@ struct j2k_t2_block {
 std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
                                   int lossless, int mct, const float* steps,
                                   const std::vector<j2k_t2_block>& blocks);
+// Parses a codestream (the first max_layers quality layers, 0: all) into descriptors in job order
+// and the codewords packed back to back (descs[i].offset into bytes).
+j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
+                               std::vector<j2k_cb_desc>* descs, std::vector<uint8_t>* bytes, std::string* err);
 // Size in bytes of the codestream j2k_t2_write would produce (block data is not read).
 size_t j2k_t2_size(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
                    const float* steps, const std::vector<j2k_t2_block>& blocks, int nlayers = 1,

@@ -524,7 +524,7 @@ namespace {
 // the first `max_layers` layers (0: all), segs[i] listing (offset in tile_bytes, length).
 j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
                    std::vector<j2k_cb_desc>* descs, std::vector<std::vector<std::pair<uint32_t, int>>>* segs,
-                   std::vector<uint8_t>* tile_bytes, std::string* err) {
+                   std::vector<uint8_t>* tile_bytes, std::string* err, bool header_only = false) {
     try {
         Cursor c{cs, n};
         if (c.u16() != 0xFF4F) throw ReadErr{J2K_ERR_INVALID_ARG, "no SOC marker"};
@@ -602,6 +602,7 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
             } else if (m == 0xFF53 || m == 0xFF5D || m == 0xFF5E || m == 0xFF60 || m == 0xFF61) {
                 throw ReadErr{J2K_ERR_UNSUPPORTED, "COC, QCC, RGN, PPM or PPT marker"};
             } else if (m == 0xFF90) {  // SOT
+                if (header_only) break;
                 const uint32_t isot = c.u16(), psot = c.u32();
                 c.u8();
                 c.u8();
@@ -657,6 +658,10 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
             const int o = rects[b].orient;
             const int gain = o == J2K_BAND_LL ? 0 : (o == J2K_BAND_HH ? 2 : 1);
             I.steps[b] = I.lossless ? 1.0f : std::ldexp(1.0f + mant[b] / 2048.0f, 8 + gain - eps[b]);
+        }
+        if (header_only) {
+            *info = I;
+            return J2K_OK;
         }
         // code-blocks in job order (component, band, raster) and the packets of the tile
         std::vector<size_t> first((size_t)ncomp * nb + 1);
@@ -813,6 +818,38 @@ extern "C" j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, in
         descs[i] = d[i];
     }
     return J2K_OK;
+}
+
+j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
+                               std::vector<j2k_cb_desc>* descs, std::vector<uint8_t>* bytes, std::string* err) {
+    std::vector<std::vector<std::pair<uint32_t, int>>> segs;
+    std::vector<uint8_t> tile;
+    J2K_TRY(t2_read(cs, n, max_layers, info, descs, &segs, &tile, err));
+    size_t total = 0;
+    for (const auto& x : *descs) total += (size_t)x.length;
+    bytes->resize(total + 1);
+    size_t o = 0;
+    for (size_t i = 0; i < descs->size(); ++i) {
+        (*descs)[i].offset = (uint32_t)o;
+        for (const auto& sg : segs[i]) {
+            std::memcpy(bytes->data() + o, tile.data() + sg.first, (size_t)sg.second);
+            o += (size_t)sg.second;
+        }
+    }
+    bytes->resize(o);
+    return J2K_OK;
+}
+
+extern "C" j2k_status j2k_codestream_info(const uint8_t* cs, size_t n, j2k_stream_info* info, char* err,
+                                          size_t errlen) {
+    if (!cs || !info) return J2K_ERR_INVALID_ARG;
+    std::string msg;
+    j2k_status s = t2_read(cs, n, 0, info, nullptr, nullptr, nullptr, &msg, true);
+    if (s != J2K_OK && err && errlen) {
+        std::strncpy(err, msg.c_str(), errlen - 1);
+        err[errlen - 1] = 0;
+    }
+    return s;
 }
 
 extern "C" j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,

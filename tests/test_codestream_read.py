@@ -152,3 +152,13 @@ def test_batched_decode_matches_per_image():
     # only the first layer of the layered streams
     first = C.decode_codestreams(streams[2:3], max_layers=1)[0]
     assert np.array_equal(first.reshape(-1), C.decode_codestream(streams[2], max_layers=1).reshape(-1))
+
+
+@pytest.mark.parametrize("w,h,nc,L,cb", CASES)
+def test_header_info_matches_the_full_parse(w, h, nc, L, cb):
+    img = synth.gray(w, h, 31) if nc == 1 else synth.rgb(w, h, (31, 32, 33, 34))
+    for cs in (_openjpeg(img, L, True, cb), bytes(O.encode_image(img, L, cb, cb, True)),
+               _openjpeg_layers(img, L, [30, 8, 0], "RLCP", cb)):
+        head = C.codestream_info(cs)
+        full = C.read_codestream(cs)[0]
+        assert all(head[k] == full[k] for k in head)
