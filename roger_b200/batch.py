@@ -12,6 +12,25 @@ from ._lib import check, lib
 TILE_NAMES = {0: "64x64", 1: "128x32", 2: "32x128"}
 
 
+def split_packed(first, descs, data):
+    """Per-image (descs, codeword bytes) of a packed batch result: image i owns descriptors
+    first[i]:first[i+1], whose offsets point into `data` back to back in job order.  The
+    descriptors come back as one rebased copy (offsets relative to each image's bytes) and the
+    bytes as views of `data`."""
+    first = np.asarray(first, np.int64)
+    n = len(first) - 1
+    d = np.ascontiguousarray(descs[:first[-1]]).view(np.uint8).copy().view(descs.dtype)  # a byte copy
+    counts = np.diff(first)
+    has = counts > 0
+    base = np.zeros(n, np.int64)
+    base[has] = d["offset"][first[:-1][has]]
+    end = base.copy()
+    last = first[1:][has] - 1
+    end[has] = d["offset"][last].astype(np.int64) + np.maximum(d["length"][last], 0)
+    d["offset"] -= np.repeat(base, counts).astype(d["offset"].dtype)
+    return [(d[first[i]:first[i + 1]], data[base[i]:end[i]]) for i in range(n)]
+
+
 class BatchEncoder:
     """images: list of dicts with w, h, ncomp (1|3), kernel (53|97), levels, cb[, steps]."""
 
@@ -145,15 +164,7 @@ class BatchEncoder:
                                           self._b.ctypes.data_as(C.c_void_p), self._b.size), hh)
 
     def split(self):
-        out = []
-        for i in range(len(self.desc)):
-            a, b = self._first[i], self._first[i + 1]
-            d = self._d[a:b].copy()
-            base = int(d["offset"][0]) if b > a else 0
-            end = int(d["offset"][-1] + max(int(d["length"][-1]), 0)) if b > a else 0
-            d["offset"] -= base
-            out.append((d, self._b[base:end]))
-        return out
+        return split_packed(self._first, self._d, self._b)
 
     def codeblocks(self, i):
         cnt, used = C.c_size_t(), C.c_size_t()
