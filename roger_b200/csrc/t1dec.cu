@@ -211,21 +211,20 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
         m.init(data, len);
         int pass = 0;
         const int nb = numbps, np = npasses;
-        auto sigbit = [&](int x, int y) -> int { return (int)((S.sig[y + 1] >> x) & 1); };
-        // zero-coding label | 0x100 when a neighbour is significant
-        auto zc = [&](int x, int y) -> int {
-            const uint32_t n9 = nb3(S.sig[y], x) | (nb3(S.sig[y + 1], x) << 3) | (nb3(S.sig[y + 2], x) << 6);
-            return (int)zct[n9] | ((n9 & 0x1EF) ? 0x100 : 0);
+        // a stripe column's neighbourhood, packed: bits 3r..3r+2 hold columns x-1..x+1 of block row
+        // y0-1+r (r = 0..5), from the significance (or sign) rows; stripe row k's 9-bit
+        // neighbourhood is then (W >> 3k) & 511 and its own bit 3k+4
+        auto colw = [&](const uint64_t* rows, int y0, int x) -> uint32_t {
+            uint32_t w = 0;
+            for (int r = 0; r < 6; ++r) w |= nb3(rows[y0 + r], x) << (3 * r);
+            return w;
         };
-        // sign-coding label | xor bit << 7
-        auto sc = [&](int x, int y) -> int {
-            const uint64_t r = S.sig[y + 1], rn = S.neg[y + 1];
-            uint32_t n8 = 0;
-            if (x > 0) n8 |= (uint32_t)((r >> (x - 1)) & 1) | ((uint32_t)((rn >> (x - 1)) & 1) << 1);
-            if (x < 63) n8 |= ((uint32_t)((r >> (x + 1)) & 1) << 2) | ((uint32_t)((rn >> (x + 1)) & 1) << 3);
-            n8 |= ((uint32_t)((S.sig[y] >> x) & 1) << 4) | ((uint32_t)((S.neg[y] >> x) & 1) << 5);
-            n8 |= ((uint32_t)((S.sig[y + 2] >> x) & 1) << 6) | ((uint32_t)((S.neg[y + 2] >> x) & 1) << 7);
-            return T.sc[n8];
+        // sign-coding neighbourhood of stripe row k: sigL negL sigR negR sigU negU sigD negD
+        auto n8of = [](uint32_t W, uint32_t NW, int k) -> uint32_t {
+            const int b = 3 * k;
+            return ((W >> (b + 3)) & 1) | (((NW >> (b + 3)) & 1) << 1) | (((W >> (b + 5)) & 1) << 2) |
+                   (((NW >> (b + 5)) & 1) << 3) | (((W >> (b + 1)) & 1) << 4) | (((NW >> (b + 1)) & 1) << 5) |
+                   (((W >> (b + 7)) & 1) << 6) | (((NW >> (b + 7)) & 1) << 7);
         };
         auto set_sig = [&](int x, int y, int neg, int p) {
             S.sig[y + 1] |= 1ull << x;
@@ -238,9 +237,9 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                 // significance propagation: only columns next to a significant sample can hold a
                 // decision; a column joins when its left neighbour gains a significant sample
                 for (int y0 = 0; y0 < ch; y0 += 4) {
-                    const int y1 = min(y0 + 4, ch);
+                    const int ny = min(4, ch - y0);
                     uint64_t cm = 0;
-                    for (int y = y0; y < y1; ++y) {
+                    for (int y = y0; y < y0 + ny; ++y) {
                         uint64_t nbm = S.sig[y] | S.sig[y + 1] | S.sig[y + 2];
                         nbm |= (nbm << 1) | (nbm >> 1);
                         cm |= ~S.sig[y + 1] & nbm;
@@ -249,16 +248,21 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                     while (cm) {
                         const int x = ctz64(cm);
                         cm &= cm - 1;
-                        for (int y = y0; y < y1; ++y) {
-                            if (sigbit(x, y)) continue;
-                            int z = zc(x, y);
-                            if (!(z & 0x100)) continue;
-                            int bit = m.decode(S.st, mq, z & 31);
-                            S.vis[y + 1] |= 1ull << x;
+                        uint32_t W = colw(S.sig, y0, x), NW = 0;
+                        bool nw = false;
+                        for (int k = 0; k < ny; ++k) {
+                            if ((W >> (3 * k + 4)) & 1) continue;  // significant already
+                            const uint32_t n9 = (W >> (3 * k)) & 511;
+                            if (!(n9 & 0x1EF)) continue;           // no significant neighbour
+                            const int bit = m.decode(S.st, mq, zct[n9]);
+                            S.vis[y0 + k + 1] |= 1ull << x;
                             if (bit) {
-                                int s = sc(x, y);
-                                int sg = m.decode(S.st, mq, s & 31) ^ (s >> 7);
-                                set_sig(x, y, sg, p);
+                                if (!nw) NW = colw(S.neg, y0, x), nw = true;
+                                const int sc = T.sc[n8of(W, NW, k)];
+                                const int sg = m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+                                set_sig(x, y0 + k, sg, p);
+                                W |= 1u << (3 * k + 4);
+                                NW |= (uint32_t)sg << (3 * k + 4);
                                 cm |= (2ull << x) & cols;
                             }
                         }
@@ -267,18 +271,18 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                 if (++pass >= np) break;
                 // magnitude refinement: significant samples not visited in this plane
                 for (int y0 = 0; y0 < ch; y0 += 4) {
-                    const int y1 = min(y0 + 4, ch);
+                    const int ny = min(4, ch - y0);
                     uint64_t rm = 0;
-                    for (int y = y0; y < y1; ++y) rm |= S.sig[y + 1] & ~S.vis[y + 1];
+                    for (int y = y0; y < y0 + ny; ++y) rm |= S.sig[y + 1] & ~S.vis[y + 1];
                     rm &= cols;
                     while (rm) {
                         const int x = ctz64(rm);
                         rm &= rm - 1;
-                        for (int y = y0; y < y1; ++y) {
-                            if (!sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
-                            int lab;
-                            if ((S.ref[y + 1] >> x) & 1) lab = 16;
-                            else lab = (zc(x, y) & 0x100) ? 15 : 14;
+                        const uint32_t W = colw(S.sig, y0, x);
+                        for (int k = 0; k < ny; ++k) {
+                            const int y = y0 + k;
+                            if (!((W >> (3 * k + 4)) & 1) || ((S.vis[y + 1] >> x) & 1)) continue;
+                            const int lab = ((S.ref[y + 1] >> x) & 1) ? 16 : (((W >> (3 * k)) & 0x1EF) ? 15 : 14);
                             if (m.decode(S.st, mq, lab)) blk[(size_t)y * pitch + x] |= 1 << p;
                             S.ref[y + 1] |= 1ull << x;
                         }
@@ -288,37 +292,40 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
             }
             // cleanup: every insignificant sample not visited in this plane
             for (int y0 = 0; y0 < ch; y0 += 4) {
-                const int y1 = min(y0 + 4, ch);
+                const int ny = min(4, ch - y0);
                 uint64_t um = 0;
-                for (int y = y0; y < y1; ++y) um |= ~S.sig[y + 1] & ~S.vis[y + 1];
+                for (int y = y0; y < y0 + ny; ++y) um |= ~S.sig[y + 1] & ~S.vis[y + 1];
                 um &= cols;
                 while (um) {
                     const int x = ctz64(um);
                     um &= um - 1;
-                    int start = y0;
-                    if (y0 + 3 < ch) {
-                        bool rl = true;
-                        for (int y = y0; y < y0 + 4 && rl; ++y)
-                            if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1) || (zc(x, y) & 0x100)) rl = false;
-                        if (rl) {
-                            if (!m.decode(S.st, mq, 17)) continue;
-                            int idx = m.decode(S.st, mq, 18) << 1;
-                            idx |= m.decode(S.st, mq, 18);
-                            int y = y0 + idx;
-                            int s = sc(x, y);
-                            int sg = m.decode(S.st, mq, s & 31) ^ (s >> 7);
-                            set_sig(x, y, sg, p);
-                            start = y + 1;
-                        }
+                    uint32_t W = colw(S.sig, y0, x), NW = 0, V = 0;
+                    bool nw = false;
+                    for (int k = 0; k < ny; ++k) V |= (uint32_t)((S.vis[y0 + k + 1] >> x) & 1) << k;
+                    int start = 0;
+                    if (ny == 4 && W == 0 && V == 0) {
+                        // run-length mode: four insignificant, unvisited samples, no significant
+                        // neighbour (every bit of the column's neighbourhood is zero)
+                        if (!m.decode(S.st, mq, 17)) continue;
+                        int idx = m.decode(S.st, mq, 18) << 1;
+                        idx |= m.decode(S.st, mq, 18);
+                        const int sc = T.sc[0];
+                        const int sg = m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+                        set_sig(x, y0 + idx, sg, p);
+                        W |= 1u << (3 * idx + 4);
+                        NW = (uint32_t)sg << (3 * idx + 4);  // the only significant sample around
+                        nw = true;
+                        start = idx + 1;
                     }
-                    for (int y = start; y < y1; ++y) {
-                        if (sigbit(x, y) || ((S.vis[y + 1] >> x) & 1)) continue;
-                        int z = zc(x, y);
-                        int bit = m.decode(S.st, mq, z & 31);
-                        if (bit) {
-                            int s = sc(x, y);
-                            int sg = m.decode(S.st, mq, s & 31) ^ (s >> 7);
-                            set_sig(x, y, sg, p);
+                    for (int k = start; k < ny; ++k) {
+                        if (((W >> (3 * k + 4)) & 1) || ((V >> k) & 1)) continue;
+                        if (m.decode(S.st, mq, zct[(W >> (3 * k)) & 511])) {
+                            if (!nw) NW = colw(S.neg, y0, x), nw = true;
+                            const int sc = T.sc[n8of(W, NW, k)];
+                            const int sg = m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+                            set_sig(x, y0 + k, sg, p);
+                            W |= 1u << (3 * k + 4);
+                            NW |= (uint32_t)sg << (3 * k + 4);
                         }
                     }
                 }
