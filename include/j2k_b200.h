@@ -342,6 +342,13 @@ j2k_status j2k_relaxed_quant_backward_scaled(j2k_ctx* ctx, const float* y, const
  * of them, image-major; j2k_dwt97_forward_adjoint_residual writes
  * g_img = DWT^T(g_coef) - (*scale) * alpha * sub (scale: device pointer or NULL = 1). */
 size_t j2k_dwt97_residual_partials(size_t w, size_t h, int n);
+/* The scalar of the fused rate-distortion loss from the partial sums above, in one launch:
+ * *loss = sum(sq_partials) * inv_count + lam * sum(rate_partials) (device pointers).  And the
+ * per-band sums of quantiser partials laid out (image, band, part): out[b] = sum over images and
+ * parts (nb entries), e.g. the log-step gradient of j2k_relaxed_quant_backward_scaled. */
+j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_t nrate, const float* sq_partials,
+                                 size_t nsq, double inv_count, float lam, float* loss);
+j2k_status j2k_dwt97_band_sum(j2k_ctx* ctx, const float* partials, int n, int nb, int k, float* out);
 j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float* x, float* d, int n, size_t w,
                                       size_t h, int levels, float* sq_partials);
 j2k_status j2k_dwt97_forward_adjoint_residual(j2k_ctx* ctx, const float* g_coef, const float* sub,

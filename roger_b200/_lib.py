@@ -101,6 +101,8 @@ SIGS = {
     "j2k_relaxed_quant_backward_scaled": (I, [P, P, P, P, I, S, S, I, P, C.c_uint64, P, C.c_float, P, C.c_float,
                                               P, I]),
     "j2k_dwt97_residual_partials": (S, [S, S, I]),
+    "j2k_dwt97_rd_finalize": (I, [P, P, S, P, S, C.c_double, C.c_float, P]),
+    "j2k_dwt97_band_sum": (I, [P, P, I, I, I, P]),
     "j2k_dwt97_inverse_residual": (I, [P, P, P, P, I, S, S, I, P]),
     "j2k_dwt97_forward_adjoint_residual": (I, [P, P, P, P, C.c_float, P, I, S, S, I]),
     "j2k_batch_create": (I, [P, P, I, C.POINTER(P)]),

@@ -490,7 +490,78 @@ j2k_status quant_run(j2k_ctx* ctx, bool bwd, const float* y, const float* gin, f
 
 }  // namespace
 
+namespace {
+
+// Sum of a float array by one CTA (blockDim a power of two), in a fixed order (strided per thread, then a
+// fixed tree), so repeated steps give the same bits.
+__device__ float cta_sum(const float* __restrict__ a, size_t n, float* sh) {
+    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f, v3 = 0.0f;  // four independent chains of loads
+    const size_t step = blockDim.x;
+    size_t i = threadIdx.x;
+    for (; i + 3 * step < n; i += 4 * step) {
+        v0 += a[i];
+        v1 += a[i + step];
+        v2 += a[i + 2 * step];
+        v3 += a[i + 3 * step];
+    }
+    for (; i < n; i += step) v0 += a[i];
+    sh[threadIdx.x] = (v0 + v1) + (v2 + v3);
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const float r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// loss = sum(sq) * inv_count + lam * sum(rate)
+__global__ void __launch_bounds__(1024) rd_finalize_kernel(const float* __restrict__ rate, size_t nrate,
+                                                          const float* __restrict__ sq, size_t nsq, double inv_count,
+                                                          float lam, float* __restrict__ loss) {
+    __shared__ float sh[1024];
+    const float r = cta_sum(rate, nrate, sh);
+    const float q = cta_sum(sq, nsq, sh);
+    if (threadIdx.x == 0) *loss = (float)((double)q * inv_count) + lam * r;
+}
+
+// out[b] = sum over images i and parts j of parts[(i * nb + b) * k + j]; one CTA per band
+__global__ void __launch_bounds__(256) band_sum_kernel(const float* __restrict__ parts, int n, int nb, int k,
+                                                       float* __restrict__ out) {
+    __shared__ float sh[256];
+    const int b = blockIdx.x;
+    float v = 0.0f;
+    for (int t = threadIdx.x; t < n * k; t += blockDim.x) v += parts[((size_t)(t / k) * nb + b) * k + (t % k)];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[b] = sh[0];
+}
+
+}  // namespace
+
 extern "C" {
+
+j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_t nrate, const float* sq_partials,
+                                 size_t nsq, double inv_count, float lam, float* loss) {
+    if (!ctx || !loss || (!rate_partials && nrate) || (!sq_partials && nsq)) return J2K_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    rd_finalize_kernel<<<1, 1024, 0, ctx->stream>>>(rate_partials, nrate, sq_partials, nsq, inv_count, lam, loss);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
+}
+
+j2k_status j2k_dwt97_band_sum(j2k_ctx* ctx, const float* partials, int n, int nb, int k, float* out) {
+    if (!ctx || !partials || !out || n < 1 || nb < 1 || k < 1) return J2K_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    band_sum_kernel<<<(unsigned)nb, 256, 0, ctx->stream>>>(partials, n, nb, k, out);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
+}
 
 j2k_status j2k_dwt97_forward_adjoint(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, size_t w, size_t h,
                                      int levels) {

@@ -200,12 +200,25 @@ class RDLoss(torch.autograd.Function):
     def forward(ctx, x, log_steps, levels, lam, seed):
         x = x.detach().contiguous()
         y = dwt97(x, levels)
-        yh, rate, u = relaxed_quant(y, log_steps, levels, seed, keep_noise=True)
-        d, sq = inverse_residual(yh, x, levels)
+        c, h = _ctx(y)
+        n, hh, ww = y.shape
+        nb, k = 3 * levels + 1, _parts(hh)
+        ls = log_steps.detach().float().contiguous()
+        yh, u = torch.empty_like(y), torch.empty_like(y)
+        rparts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+        check(lib().j2k_relaxed_quant_forward_noise(h, _p(y), _p(yh), _p(u), n, ww, hh, levels, _p(ls), seed,
+                                                    _p(rparts), k), h)
+        d = torch.empty_like(y)
+        sparts = torch.empty(lib().j2k_dwt97_residual_partials(ww, hh, n), device=y.device, dtype=torch.float32)
+        check(lib().j2k_dwt97_inverse_residual(h, _p(yh), _p(x), _p(d), n, ww, hh, levels, _p(sparts)), h)
         del yh
+        # the loss scalar from both sets of partial sums, in one launch
+        loss = torch.empty((), device=y.device, dtype=torch.float32)
+        check(lib().j2k_dwt97_rd_finalize(h, _p(rparts), rparts.numel(), _p(sparts), sparts.numel(),
+                                          1.0 / x.numel(), float(lam), _p(loss)), h)
         ctx.save_for_backward(y, d, u, log_steps)
         ctx.levels, ctx.lam, ctx.seed = levels, lam, seed
-        return sq / x.numel() + lam * rate.sum()
+        return loss
 
     @staticmethod
     def backward(ctx, g):
@@ -213,9 +226,18 @@ class RDLoss(torch.autograd.Function):
         g = g.detach().float().contiguous()
         alpha = 2.0 / d.numel()
         g_res = idwt97_adjoint(d, ctx.levels)
-        g_y, g_ls = relaxed_quant_backward(y, g_res, log_steps, ctx.levels, ctx.seed, ctx.lam, scale=g, alpha=alpha,
-                                           noise=u)
+        c, h = _ctx(y)
+        n, hh, ww = y.shape
+        nb, k = 3 * ctx.levels + 1, _parts(hh)
+        ls = log_steps.detach().float().contiguous()
+        g_y = torch.empty_like(y)
+        parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+        check(lib().j2k_relaxed_quant_backward_scaled(h, _p(y), _p(g_res), _p(g_y), n, ww, hh, ctx.levels, _p(ls),
+                                                      ctx.seed, _p(u), float(ctx.lam), _p(g), float(alpha), _p(parts),
+                                                      k), h)
         del g_res
+        g_ls = torch.empty(nb, device=y.device, dtype=torch.float32)  # per band, in one launch
+        check(lib().j2k_dwt97_band_sum(h, _p(parts), n, nb, k, _p(g_ls)), h)
         gx = forward_adjoint_residual(g_y, d, ctx.levels, scale=g, alpha=alpha)
         return gx, g_ls.to(log_steps.dtype), None, None, None
 
