@@ -493,7 +493,7 @@ __constant__ uint8_t c_nlps[47] = {1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 1
                                    15, 16, 17, 18, 19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29,
                                    30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
 
-constexpr int kMqThreads = 64;
+constexpr int kMqThreads = 32;  // one warp per CTA: the longest blocks' warps spread one per SM
 
 // Branch-light MQ encoder state.  The exchange and state transition are predicated so the
 // lanes of a warp (each coding a different block) stay converged; only the byte output, about
