@@ -94,6 +94,46 @@ def cpu_baseline(tile=1024, tiles=None):
                        f"wall {wall:.1f} s including input synthesis")
 
 
+def cpu_references(tile=1024, reps=2):
+    """Single-core CPU figures on one tile of the workload's kind (no GPU touched): the C oracle
+    on one core, and OpenJPEG through Pillow (an independent encoder, single-threaded as Pillow
+    drives it) for the lossless 5/3 and the irreversible 9/7 encode of the same image."""
+    import io
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from roger_b200 import synth
+    img = synth.rgb(tile, tile, (100, 101, 102, 103))
+    mpix = tile * tile / 1e6
+
+    def best(fn):
+        fn()
+        tt = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            fn()
+            tt.append(time.perf_counter() - t)
+        return min(tt)
+    out = {"single_thread_oracle": {"mpix_s": round(mpix / best(lambda: O.encode_image(img, LEVELS, CB, CB, True)), 3),
+                                    "sample": f"one {tile}x{tile} RGB image, RCT+5/3 L={LEVELS}+tier-1+tier-2"}}
+    try:
+        from PIL import Image, features
+        im = Image.fromarray(img)
+
+        def enc(lossless):
+            b = io.BytesIO()
+            im.save(b, "JPEG2000", irreversible=not lossless, mct=1, num_resolutions=LEVELS + 1,
+                    codeblock_size=(CB, CB), no_jp2=True)
+            return b
+        out["openjpeg"] = {"version": str(features.version("jpg_2000")), "threads": 1,
+                           "lossless_53_mpix_s": round(mpix / best(lambda: enc(True)), 3),
+                           "irreversible_97_mpix_s": round(mpix / best(lambda: enc(False)), 3),
+                           "sample": f"one {tile}x{tile} RGB image through Pillow, L={LEVELS}, {CB}x{CB} blocks, "
+                                     "colour transform on"}
+    except Exception as e:  # Pillow without OpenJPEG
+        out["openjpeg"] = {"unavailable": str(e)[:200]}
+    return out
+
+
 def profiled_traffic(size):
     """DRAM bytes (read + write) of one launch of the level-0 5/3 kernel over the three
     4096x4096 planes, as captured by ncu on the same launch (kept as a text summary under
@@ -242,6 +282,7 @@ def main():
     cpu_line = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu_line = cpu_baseline()  # spawned before the first GPU call
+        cpu_line.update(cpu_references())
     import numpy as np
     import torch
     from roger_b200 import codec as C
@@ -348,7 +389,8 @@ def main():
                    np.maximum(3 * descs["numbps"].astype(np.int64) - 2, 0)).sum())
     mpix = n / 1e6
     line = dict(
-        metric=METRIC, value=round(world * mpix / (ms * 1e-3), 2), unit="Mpix/s", n_gpus=world,
+        metric=METRIC, value=round(world * mpix / (ms * 1e-3), 2), unit="Mpix/s",
+        msample_s=round(3 * world * mpix / (ms * 1e-3), 2), n_gpus=world,
         steps=args.steps, warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True,
         scaling="weak", vs_baseline=None, dtype="int32", data="synthetic",
         config={"workload": WORKLOAD.replace("4096x4096", f"{size}x{size}"), "levels": LEVELS,
@@ -381,6 +423,7 @@ def main():
         line["lossless_decode"] = bench_lossless_decode(img_h, res)
         line["lossy"] = bench_lossy(img_h, img_d, flush)
         line["rate_control"] = bench_rate_control(img_d, img_h, flush)
+        line["c0"] = bench_c0(flush)
     if args.batch_images and world == 1:
         line["batched"] = bench_batched(args.batch_images, flush)
     if args.diff and world == 1:
@@ -452,6 +495,31 @@ def bench_lossy(img_h, img_d, flush, levels=6):
             "ms_per_step": round(ms, 3), "mpix_s": round(w * h / 1e6 / (ms * 1e-3), 1),
             "codeword_bytes": int(data.size if hasattr(data, "size") else len(data)),
             "psnr_db": round(psnr, 3)}
+
+
+def bench_c0(flush, size=512, levels=5):
+    """The reference's CPU-runnable case: one 512x512 gray image (synthetic, seed 0), 5/3 L=5,
+    64x64 code-blocks, resident on the device; median of 15 encodes."""
+    import torch
+    from roger_b200 import codec as C
+    from roger_b200 import synth
+    img = torch.from_numpy(synth.gray(size, size, 0)).cuda()
+    enc = C.OCLEncoder(lossy=False)
+    for _ in range(3):
+        enc.run_rgb(img, levels=levels, cbw=CB, cbh=CB)
+    tt = []
+    for _ in range(15):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        enc.run_rgb(img, levels=levels, cbw=CB, cbh=CB)
+        e.record()
+        e.synchronize()
+        tt.append(s.elapsed_time(e))
+    ms = statistics.median(tt)
+    return {"workload": f"{size}x{size} gray uint8, 5/3 L={levels}, {CB}x{CB} code-blocks (seed 0)",
+            "ms_per_step": round(ms, 4), "mpix_s": round(size * size / 1e6 / (ms * 1e-3), 1)}
 
 
 def bench_rate_control(img_d, img_h, flush, bpp=1.0):
@@ -542,9 +610,12 @@ def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
     N = n * size * size
     tr = N * 8 * sum(4.0 ** -k for k in range(levels))
     algo = 4 * tr + 8 * N + 12 * N + 12 * N
+    passes = {"dwt_forward": int(tr), "quantiser_forward": int(8 * N), "dwt_inverse_with_residual": int(tr),
+              "loss_and_gradient": int(12 * N), "dwt_inverse_adjoint": int(tr), "quantiser_backward": int(12 * N),
+              "dwt_forward_adjoint_with_residual": int(tr)}
     return {"workload": f"{n} x {size}x{size} float32, 9/7 L={levels}, relaxed quantiser, loss = MSE + 0.01*rate, "
                         "grads wrt pixels and 16 log-steps",
-            "ms_per_step": round(ms, 3), "algorithmic_bytes": int(algo),
+            "ms_per_step": round(ms, 3), "algorithmic_bytes": int(algo), "algorithmic_bytes_per_pass": passes,
             "achieved_gbs": round(algo / (ms * 1e-3) / 1e9, 1), "hbm_frac": round(algo / (ms * 1e-3) / 1e9 / hbm, 4),
             "mpix_s": round(N / 1e6 / (ms * 1e-3), 1),
             "graphed": {"path": "diff97.GraphedRDStep (the same step captured in one CUDA graph)",
