@@ -17,6 +17,10 @@ benchmark workloads but stay within a few hundred MB of device memory:
                16 x 1024x1024 float32 (forward, quantiser, inverse+residual, inverse adjoint,
                quantiser backward, forward adjoint+residual)
   diff-step    one fused rate-distortion step (5 levels, forward + backward)
+  batched      the 256-image mixed set (config 4) through the batched encoder: the first run
+               captures its launch sequence in a CUDA graph, the second replays it
+  decode       lossless decode of one 2048x2048 RGB image (tier-1 decode, inverse 5/3, inverse
+               RCT) from code-blocks already on the host
 """
 import math
 import sys
@@ -91,9 +95,29 @@ def case_diff_step():
     return run
 
 
+def case_batched():
+    from .batch import BatchEncoder
+    descs = synth.mixed_set(256)
+    imgs = [torch.from_numpy(synth.mixed_image(d)).cuda() for d in descs]
+    be = BatchEncoder([dict(w=d["w"], h=d["h"], ncomp=d["ncomp"], kernel=d["kernel"], levels=d["levels"],
+                            cb=d["cb"]) for d in descs])
+    be.encode(imgs)
+    return lambda: be.encode(None)
+
+
+def case_decode():
+    img = synth.rgb(2048, 2048, (100, 101, 102, 103))
+    enc = C.OCLEncoder(lossy=False)
+    enc.run_rgb(img, levels=6, cbw=64, cbh=64)
+    d, b = enc.get_codeblocks()
+    dec = C.OCLDecoder(lossy=False)
+    return lambda: dec.run(d, b, 2048, 2048, 3, levels=6)
+
+
 CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_dwt53(6),
          "idwt53": case_idwt53, "tier1": case_tier1, "encode": case_encode,
-         "diff-kernels": case_diff_kernels, "diff-step": case_diff_step}
+         "diff-kernels": case_diff_kernels, "diff-step": case_diff_step, "batched": case_batched,
+         "decode": case_decode}
 
 
 def main(argv):
