@@ -65,12 +65,14 @@ __device__ __forceinline__ int sc_code(int hc, int vc) {
     return lab | (x << 7);
 }
 
-__device__ __forceinline__ uint64_t dil(uint64_t m) { return m | (m << 1) | (m >> 1); }
+template <typename T>
+__device__ __forceinline__ T dil(T m) { return m | (T)(m << 1) | (T)(m >> 1); }
 
 // 4-bit window of a row mask around this lane's column pair: bit 0 = column c0-1 ...
 // bit 3 = column c0+2 (columns outside 0..63 read as 0)
-__device__ __forceinline__ uint32_t win4(uint64_t m, int c0) {
-    return (uint32_t)(c0 ? (m >> (c0 - 1)) : (m << 1)) & 0xF;
+template <typename T>
+__device__ __forceinline__ uint32_t win4(T m, int c0) {
+    return (uint32_t)(c0 ? (m >> (c0 - 1)) : (T)(m << 1)) & 0xF;
 }
 
 // warp exclusive prefix sum; returns the total in *tot
@@ -93,51 +95,22 @@ struct Lut {
     const uint8_t* s;
 };
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
-t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__ jobs,
-                  int njobs, const uint32_t* __restrict__ order, uint32_t* __restrict__ queue,
-                  uint8_t* __restrict__ syms, uint32_t* __restrict__ nsyms,
-                  uint32_t* __restrict__ pass_end, uint64_t* __restrict__ plane_scratch,
-                  j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
-    __shared__ WarpSmem smem[kWarpsPerCta];
-    __shared__ uint8_t zlut[4][256];
-    __shared__ uint8_t slut[256];
-    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
-        int o = i >> 8, b = i & 255;
-        int W = b & 1, E = (b >> 1) & 1, N = (b >> 2) & 1, S = (b >> 3) & 1;
-        int d = ((b >> 4) & 1) + ((b >> 5) & 1) + ((b >> 6) & 1) + ((b >> 7) & 1);
-        zlut[o][b] = (uint8_t)zc_label_calc(o, W + E, N + S, d);
-    }
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        int sg = i & 15, ng = i >> 4;
-        auto ct = [&](int k) { return ((sg >> k) & 1) ? (((ng >> k) & 1) ? -1 : 1) : 0; };
-        slut[i] = (uint8_t)sc_code(ct(0) + ct(1), ct(2) + ct(3));
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpSmem& S = smem[wid];
-    // persistent: each warp pulls code-blocks from the device-side queue until it is empty;
-    // its bit-plane scratch slot is reused from block to block
-    uint64_t* planes = plane_scratch + (size_t)(blockIdx.x * kWarpsPerCta + wid) * kPlaneWords;
-    for (;;) {
-    int qi = 0;
-    if (lane == 0) qi = (int)atomicAdd(queue, 1u);
-    qi = __shfl_sync(0xffffffffu, qi, 0);
-    if (qi >= njobs) break;
-    const int jid = order ? (int)order[qi] : qi;
-    const j2k_cb_job J = jobs[jid];
-    if (J.cw == 0 || J.ch == 0 || J.cw > 64 || J.ch > 64 || J.orient > 3 || J.sym_cap % 16 != 0) {
-        if (lane == 0) {
-            atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
-            nsyms[jid] = 0;
-        }
-        continue;
-    }
+// One code-block's phase A (bit-plane slicing, the three passes per plane, symbol emission).  MT is
+// the row-mask type and CPL the columns per lane: 64-bit masks and two columns per lane for blocks
+// wider than 32, 32-bit masks and one column per lane otherwise (all 32 lanes busy, half the mask
+// work per stripe).
+template <typename MT, int CPL>
+__device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, int jid, int lane,
+                                              const int32_t* __restrict__ coeff, const uint8_t* zlut,
+                                              const uint8_t* slut, uint8_t* __restrict__ syms,
+                                              uint32_t* __restrict__ nsyms, uint32_t* __restrict__ pass_end,
+                                              uint64_t* __restrict__ planes, j2k_cb_desc* __restrict__ descs,
+                                              uint32_t* __restrict__ err) {
     const int cw = J.cw, ch = J.ch;
     const size_t pitch = J.pitch;
     const int32_t* blk = coeff + J.off;
-    const uint8_t* zl = zlut[J.orient];
-    const uint64_t colmask = cw == 64 ? ~0ull : ((1ull << cw) - 1);
+    const uint8_t* zl = zlut + J.orient * 256;
+    const MT colmask = (MT)(cw >= 64 ? ~0ull : ((1ull << cw) - 1));
 
     // ---- bit-plane slicing: lane p ends up holding plane p of each row and stores it
     uint32_t mor = 0;
@@ -187,7 +160,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
             descs[jid] = d;
         }
         __syncwarp();
-        continue;
+        return;
     }
     __syncwarp();
     uint8_t* out = syms + J.sym_off;
@@ -196,9 +169,10 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
     int pos = 0, npass = 0;
     bool ovf = false;
     const int nstripes = (ch + 3) >> 2;
-    const int c0 = 2 * lane;
+    const int c0 = CPL * lane;
     const bool active = c0 < cw;
-    const uint32_t ownmask = active ? (c0 + 1 < cw ? 3u : 1u) : 0u;  // columns c0, c0+1 present
+    // columns of this lane present: c0 (and c0+1 with two columns per lane)
+    const uint32_t ownmask = active ? (CPL == 2 && c0 + 1 < cw ? 3u : 1u) : 0u;
 
     for (int p = numbps - 1; p >= 0 && !ovf; --p) {
         // current plane into shared (rows beyond ch are zero)
@@ -209,13 +183,13 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
             // ------------------------- significance propagation pass
             for (int s = 0; s < nstripes && !ovf; ++s) {
                 const int r0 = 4 * s;
-                uint64_t O[6], N[6], C[4], M[4], E[4], K[4], B[4];
+                MT O[6], N[6], C[4], M[4], E[4], K[4], B[4];
 #pragma unroll
                 for (int j = 0; j < 6; ++j) O[j] = S.sig[r0 + j];
                 bool anyk = false;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const uint64_t V = (r0 + j < ch) ? colmask : 0;
+                    const MT V = (r0 + j < ch) ? colmask : (MT)0;
                     B[j] = S.bits[(r0 + j) & 63];
                     C[j] = ~O[j + 1] & V;
                     M[j] = C[j] & B[j];
@@ -229,8 +203,8 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
                     changed = false;
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        uint64_t seeds = M[j] & (E[j] | ((N[j] | N[j + 2]) << 1) | N[j]);
-                        uint64_t nn = M[j] & (~(M[j] + seeds) | seeds);
+                        MT seeds = M[j] & (E[j] | ((N[j] | N[j + 2]) << 1) | N[j]);
+                        MT nn = M[j] & (MT)(~(MT)(M[j] + seeds) | seeds);
                         changed |= nn != N[j + 1];
                         N[j + 1] = nn;
                     }
@@ -260,7 +234,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
                 }
                 if (cnt) {
 #pragma unroll
-                    for (int k = 0; k < 2; ++k)
+                    for (int k = 0; k < CPL; ++k)
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
                             const int bitpos = 2 * j + k;
@@ -298,7 +272,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
             // ------------------------- magnitude refinement pass
             for (int s = 0; s < nstripes && !ovf; ++s) {
                 const int r0 = 4 * s;
-                uint64_t SG[6], R[4];
+                MT SG[6], R[4];
                 bool anyr = false;
 #pragma unroll
                 for (int j = 0; j < 6; ++j) SG[j] = S.sig[r0 + j];
@@ -311,7 +285,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
                 uint32_t rr = 0, rf = 0, nb = 0, bb = 0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const uint64_t nbm = dil(SG[j]) | dil(SG[j + 2]) | (SG[j + 1] << 1) | (SG[j + 1] >> 1);
+                    const MT nbm = dil(SG[j]) | dil(SG[j + 2]) | (MT)(SG[j + 1] << 1) | (MT)(SG[j + 1] >> 1);
                     rr |= ((win4(R[j], c0) >> 1) & ownmask) << (2 * j);
                     rf |= ((win4(S.ref[r0 + j + 1], c0) >> 1) & 3u) << (2 * j);
                     nb |= ((win4(nbm, c0) >> 1) & 3u) << (2 * j);
@@ -326,7 +300,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
                 }
                 if (cnt) {
 #pragma unroll
-                    for (int k = 0; k < 2; ++k)
+                    for (int k = 0; k < CPL; ++k)
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
                             const int bitpos = 2 * j + k;
@@ -349,13 +323,13 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
         for (int s = 0; s < nstripes && !ovf; ++s) {
             const int r0 = 4 * s;
             const bool full = r0 + 3 < ch;
-            uint64_t O[6], C[4], N[4];
+            MT O[6], C[4], N[4];
             bool anyc = false;
 #pragma unroll
             for (int j = 0; j < 6; ++j) O[j] = S.sig[r0 + j];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const uint64_t V = (r0 + j < ch) ? colmask : 0;
+                const MT V = (r0 + j < ch) ? colmask : (MT)0;
                 C[j] = V & ~O[j + 1] & ~S.vis[r0 + j + 1];
                 N[j] = C[j] & S.bits[(r0 + j) & 63];
                 anyc |= C[j] != 0;
@@ -377,7 +351,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
             uint32_t rlmask = 0;  // bit k: column c0+k codes in run-length mode
             int cnt = 0;
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
+            for (int k = 0; k < CPL; ++k) {
                 const uint32_t colc = (cc >> k) & 0x55;  // bits 0,2,4,6: rows 0..3
                 const uint32_t coln = (nn4 >> k) & 0x55;
                 bool rl = false;
@@ -410,7 +384,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
             }
             if (cnt) {
 #pragma unroll
-                for (int k = 0; k < 2; ++k) {
+                for (int k = 0; k < CPL; ++k) {
                     const uint32_t colc = (cc >> k) & 0x55;
                     const uint32_t coln = (nn4 >> k) & 0x55;
                     if (!colc) continue;
@@ -468,6 +442,54 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
         descs[jid] = d;
     }
     __syncwarp();
+}
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__ jobs,
+                  int njobs, const uint32_t* __restrict__ order, uint32_t* __restrict__ queue,
+                  uint8_t* __restrict__ syms, uint32_t* __restrict__ nsyms,
+                  uint32_t* __restrict__ pass_end, uint64_t* __restrict__ plane_scratch,
+                  j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+    __shared__ WarpSmem smem[kWarpsPerCta];
+    __shared__ uint8_t zlut[4][256];
+    __shared__ uint8_t slut[256];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+        int o = i >> 8, b = i & 255;
+        int W = b & 1, E = (b >> 1) & 1, N = (b >> 2) & 1, S = (b >> 3) & 1;
+        int d = ((b >> 4) & 1) + ((b >> 5) & 1) + ((b >> 6) & 1) + ((b >> 7) & 1);
+        zlut[o][b] = (uint8_t)zc_label_calc(o, W + E, N + S, d);
+    }
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        int sg = i & 15, ng = i >> 4;
+        auto ct = [&](int k) { return ((sg >> k) & 1) ? (((ng >> k) & 1) ? -1 : 1) : 0; };
+        slut[i] = (uint8_t)sc_code(ct(0) + ct(1), ct(2) + ct(3));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpSmem& S = smem[wid];
+    // persistent: each warp pulls code-blocks from the device-side queue until it is empty;
+    // its bit-plane scratch slot is reused from block to block
+    uint64_t* planes = plane_scratch + (size_t)(blockIdx.x * kWarpsPerCta + wid) * kPlaneWords;
+    for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = (int)atomicAdd(queue, 1u);
+    qi = __shfl_sync(0xffffffffu, qi, 0);
+    if (qi >= njobs) break;
+    const int jid = order ? (int)order[qi] : qi;
+    const j2k_cb_job J = jobs[jid];
+    if (J.cw == 0 || J.ch == 0 || J.cw > 64 || J.ch > 64 || J.orient > 3 || J.sym_cap % 16 != 0) {
+        if (lane == 0) {
+            atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+            nsyms[jid] = 0;
+        }
+        continue;
+    }
+    if (J.cw <= 32)
+        phase_a_block<uint32_t, 1>(S, J, jid, lane, coeff, &zlut[0][0], slut, syms, nsyms, pass_end, planes, descs,
+                                   err);
+    else
+        phase_a_block<uint64_t, 2>(S, J, jid, lane, coeff, &zlut[0][0], slut, syms, nsyms, pass_end, planes, descs,
+                                   err);
     }  // queue loop
 }
 
