@@ -649,6 +649,30 @@ j2k_status j2k_decoder_destroy(j2k_decoder* d) {
     return J2K_OK;
 }
 
+}  // extern "C"
+
+// Runs fn(k) for k = 0..n-1 on up to 16 host threads (one thread when the work is small), each
+// thread taking every nt-th item; used for the copies between callers' buffers and page-locked
+// staging, which one thread does at only a few GB/s.
+template <typename F>
+static void host_parallel(int n, size_t bytes, F fn) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = bytes < ((size_t)8 << 20) ? 1 : (int)std::min<unsigned>((unsigned)n, std::min(16u, hw));
+    if (nt <= 1) {
+        for (int k = 0; k < n; ++k) fn(k);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (int k = t; k < n; k += nt) fn(k);
+        });
+    for (int k = 0; k < n; k += nt) fn(k);
+    for (auto& th : pool) th.join();
+}
+
+extern "C" {
+
 j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, int n) {
     if (!d || (!items && n > 0) || n < 0) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = d->ctx;
@@ -702,7 +726,7 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
     if (!hs) return J2K_ERR_OUT_OF_MEMORY;
     j2k_cb_desc* hd = (j2k_cb_desc*)hs;
     uint8_t* hb = hs + align16(dbytes);
-    for (int k = 0; k < n; ++k) {
+    host_parallel(n, byte0[n], [&](int k) {
         const j2k_decode_item& it = items[k];
         for (size_t i = 0; i < it.count; ++i) {
             j2k_cb_desc q = it.descs[i];
@@ -710,7 +734,7 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
             hd[job0[k] + i] = q;
         }
         if (it.nbytes) std::memcpy(hb + byte0[k], it.bytes, it.nbytes);
-    }
+    });
     if (nbytes + 16 > 0xFFFFFFFFull) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "more than 4 GiB of codewords");
     J2K_TRY(d->descs.ensure(ctx, dbytes + 16));
     J2K_TRY(d->bytes.ensure(ctx, nbytes + 16));
@@ -753,7 +777,7 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
     // one read-back of every image's pixels
     J2K_CUDA(ctx, cudaMemcpyAsync(hs, d->out.p, out_off[n], cudaMemcpyDeviceToHost, ctx->stream));
     J2K_TRY(j2k_read_device_error(ctx));
-    for (int k = 0; k < n; ++k) std::memcpy(items[k].out, hs + out_off[k], out_off[k + 1] - out_off[k]);
+    host_parallel(n, out_off[n], [&](int k) { std::memcpy(items[k].out, hs + out_off[k], out_off[k + 1] - out_off[k]); });
     return J2K_OK;
 }
 
