@@ -68,6 +68,47 @@ std::vector<float> default_steps(size_t w, size_t h, int levels) {
     return s;
 }
 
+// Runs fn(k) for k = 0..n-1 on up to 16 host threads (one thread when the work is small), each
+// thread taking every nt-th item; used for the copies between callers' buffers and page-locked
+// staging, which one thread does at only a few GB/s.
+template <typename F>
+void host_parallel(int n, size_t bytes, F fn) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = bytes < ((size_t)8 << 20) ? 1 : (int)std::min<unsigned>((unsigned)n, std::min(16u, hw));
+    if (nt <= 1) {
+        for (int k = 0; k < n; ++k) fn(k);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (int k = t; k < n; k += nt) fn(k);
+        });
+    for (int k = 0; k < n; k += nt) fn(k);
+    for (auto& th : pool) th.join();
+}
+
+// A host copy split over up to 16 threads when it is large (one thread copies at a few GB/s).
+void parallel_copy(void* dst, const void* src, size_t bytes) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = bytes < ((size_t)8 << 20) ? 1 : (int)std::min(16u, hw);
+    const size_t chunk = (bytes + nt - 1) / nt;
+    host_parallel(nt, bytes, [&](int t) {
+        const size_t a = (size_t)t * chunk, b = std::min(bytes, a + chunk);
+        if (a < b) std::memcpy((uint8_t*)dst + a, (const uint8_t*)src + a, b - a);
+    });
+}
+
+// Host memory that the GPU can copy from or to asynchronously (page-locked or registered).
+bool page_locked(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
 
 struct j2k_encoder {
@@ -649,30 +690,6 @@ j2k_status j2k_decoder_destroy(j2k_decoder* d) {
     return J2K_OK;
 }
 
-}  // extern "C"
-
-// Runs fn(k) for k = 0..n-1 on up to 16 host threads (one thread when the work is small), each
-// thread taking every nt-th item; used for the copies between callers' buffers and page-locked
-// staging, which one thread does at only a few GB/s.
-template <typename F>
-static void host_parallel(int n, size_t bytes, F fn) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int nt = bytes < ((size_t)8 << 20) ? 1 : (int)std::min<unsigned>((unsigned)n, std::min(16u, hw));
-    if (nt <= 1) {
-        for (int k = 0; k < n; ++k) fn(k);
-        return;
-    }
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nt; ++t)
-        pool.emplace_back([&, t] {
-            for (int k = t; k < n; k += nt) fn(k);
-        });
-    for (int k = 0; k < n; k += nt) fn(k);
-    for (auto& th : pool) th.join();
-}
-
-extern "C" {
-
 j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, int n) {
     if (!d || (!items && n > 0) || n < 0) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = d->ctx;
@@ -847,6 +864,7 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
         J2K_TRY(d->descs.ensure(ctx, njobs * sizeof(j2k_cb_desc) + 16));
         J2K_TRY(d->bytes.ensure(ctx, nbytes + 16));
         J2K_CUDA(ctx, cudaMemcpyAsync(d->descs.p, descs, njobs * sizeof(j2k_cb_desc), cudaMemcpyHostToDevice, ctx->stream));
+        // (pageable uploads are left to the driver, which pipelines its own staging)
         J2K_CUDA(ctx, cudaMemcpyAsync(d->bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, ctx->stream));
         dd = (const j2k_cb_desc*)d->descs.p;
         db = (const uint8_t*)d->bytes.p;
@@ -879,8 +897,20 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
     }
     J2K_TRY(j2k_launch_planar_inv(ctx, d->planes.p, d->lossy ? J2K_F32 : J2K_I32, w, n, ncomp, mct, dst,
                                   out_pitch, w, h, ctx->stream));
-    if (!out_on_device)
-        J2K_CUDA(ctx, cudaMemcpyAsync(out, dst, out_pitch * h, cudaMemcpyDeviceToHost, ctx->stream));
+    if (!out_on_device) {
+        const size_t ob = out_pitch * h;
+        if (ob >= ((size_t)8 << 20) && !page_locked(out)) {
+            // pageable output: through the page-locked staging buffer, emptied by host threads
+            // (a pageable download is much slower than a page-locked one and a parallel copy)
+            uint8_t* hs = (uint8_t*)j2k_pinned(ctx, ob + 16);
+            if (!hs) return J2K_ERR_OUT_OF_MEMORY;
+            J2K_CUDA(ctx, cudaMemcpyAsync(hs, dst, ob, cudaMemcpyDeviceToHost, ctx->stream));
+            J2K_TRY(j2k_read_device_error(ctx));
+            parallel_copy(out, hs, ob);
+            return J2K_OK;
+        }
+        J2K_CUDA(ctx, cudaMemcpyAsync(out, dst, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     return j2k_read_device_error(ctx);
 }
 
