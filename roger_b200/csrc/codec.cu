@@ -562,12 +562,20 @@ j2k_status j2k_encoder_get_codeblocks(j2k_encoder* e, j2k_cb_desc* descs, size_t
     if (descs && *count < e->njobs) return j2k_fail(ctx, J2K_ERR_CAPACITY, "descs array too small");
     if (bytes && cap < total) return j2k_fail(ctx, J2K_ERR_CAPACITY, "bytes buffer too small");
     *count = e->njobs;
-    if (bytes) J2K_CUDA(ctx, cudaMemcpyAsync(bytes, e->packed.p, total, cudaMemcpyDeviceToHost, ctx->stream));
+    // a large pageable destination is filled through the page-locked staging buffer by host
+    // threads (a pageable download is much slower than a page-locked one)
+    uint8_t* hs = nullptr;
+    if (bytes && total >= ((size_t)8 << 20) && !page_locked(bytes)) {
+        hs = (uint8_t*)j2k_pinned(ctx, total + 16);
+        if (!hs) return J2K_ERR_OUT_OF_MEMORY;
+    }
+    if (bytes) J2K_CUDA(ctx, cudaMemcpyAsync(hs ? hs : bytes, e->packed.p, total, cudaMemcpyDeviceToHost, ctx->stream));
     if (descs) {
         J2K_CUDA(ctx, cudaMemcpyAsync(descs, e->descs.p, e->njobs * sizeof(j2k_cb_desc), cudaMemcpyDeviceToHost,
                                       ctx->stream));
     }
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hs) parallel_copy(bytes, hs, total);
     if (descs) {
         uint32_t acc = 0;
         for (size_t i = 0; i < e->njobs; ++i) {
