@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdint>
 #include <limits>
+#include <thread>
 #include <vector>
 
 #include "j2k_internal.cuh"
@@ -88,52 +89,69 @@ double j2k_band_gain(int kernel, int levels, int band) {
 
 extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
                                   const double* weight, size_t budget) {
-    // hull points of every block, flat: block i owns [first[i], first[i+1]) (scratch kept per
-    // thread between calls)
+    // hull points of every block: block i owns slots [i * 33, i * 33 + cnt[i]) (scratch kept per
+    // thread between calls); the blocks' hulls are independent and built on host threads
     static thread_local std::vector<double> HL, HD;
     static thread_local std::vector<uint8_t> HN;
-    static thread_local std::vector<size_t> first;
-    HL.clear();
-    HD.clear();
-    HN.clear();
-    first.assign(n + 1, 0);
-    double base = 0.0;  // bytes of every hull's first point (L = 0)
-    for (size_t i = 0; i < n; ++i) {
-        const j2k_cb_desc& d = descs[i];
-        const int nb = d.numbps;
-        const double w = weight[i];
-        double pl[33], pd[33];
-        int pn[33], m = 0;
-        pl[m] = 0.0, pd[m] = dist[i * 33 + 32] * w, pn[m++] = 0;
-        for (int k = 0; k < nb && k < 31; ++k) {
-            const int np = 3 * k + 1;
-            if (np > d.npasses) break;
-            pl[m] = k == nb - 1 ? (double)d.length
-                                : std::min<double>(d.length, (double)plane_bytes[i * 32 + k] + J2K_TRUNC_EXTRA);
-            pd[m] = dist[i * 33 + k] * w;
-            pn[m++] = np;
-        }
-        // lower convex hull in (L, D): slopes (D drop per byte) strictly decreasing
-        double hl[33], hd[33];
-        int hn[33], h = 0;
-        for (int q = 0; q < m; ++q) {
-            if (h && pl[q] <= hl[h - 1]) {  // no extra bytes: keep the better point
-                if (pd[q] < hd[h - 1]) hl[h - 1] = pl[q], hd[h - 1] = pd[q], hn[h - 1] = pn[q];
-                continue;
+    static thread_local std::vector<int> cnt;
+    HL.resize(n * 33);
+    HD.resize(n * 33);
+    HN.resize(n * 33);
+    cnt.assign(n, 0);
+    double* const hlp = HL.data();
+    double* const hdp = HD.data();
+    uint8_t* const hnp = HN.data();
+    int* const cntp = cnt.data();
+    auto hulls = [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; ++i) {
+            const j2k_cb_desc& d = descs[i];
+            const int nb = d.numbps;
+            const double w = weight[i];
+            double pl[33], pd[33];
+            int pn[33], m = 0;
+            pl[m] = 0.0, pd[m] = dist[i * 33 + 32] * w, pn[m++] = 0;
+            for (int k = 0; k < nb && k < 31; ++k) {
+                const int np = 3 * k + 1;
+                if (np > d.npasses) break;
+                pl[m] = k == nb - 1 ? (double)d.length
+                                    : std::min<double>(d.length, (double)plane_bytes[i * 32 + k] + J2K_TRUNC_EXTRA);
+                pd[m] = dist[i * 33 + k] * w;
+                pn[m++] = np;
             }
-            if (h && pd[q] >= hd[h - 1]) continue;  // no improvement
-            // drop the last hull point while the new point's slope is not below its slope
-            // (cross-multiplied: both byte differences are positive)
-            while (h >= 2 && (hd[h - 1] - pd[q]) * (hl[h - 1] - hl[h - 2]) >=
-                                 (hd[h - 2] - hd[h - 1]) * (pl[q] - hl[h - 1]))
-                --h;
-            hl[h] = pl[q], hd[h] = pd[q], hn[h++] = pn[q];
+            // lower convex hull in (L, D): slopes (D drop per byte) strictly decreasing
+            double* hl = hlp + i * 33;
+            double* hd = hdp + i * 33;
+            uint8_t* hn = hnp + i * 33;
+            int h = 0;
+            for (int q = 0; q < m; ++q) {
+                if (h && pl[q] <= hl[h - 1]) {  // no extra bytes: keep the better point
+                    if (pd[q] < hd[h - 1]) hl[h - 1] = pl[q], hd[h - 1] = pd[q], hn[h - 1] = (uint8_t)pn[q];
+                    continue;
+                }
+                if (h && pd[q] >= hd[h - 1]) continue;  // no improvement
+                // drop the last hull point while the new point's slope is not below its slope
+                // (cross-multiplied: both byte differences are positive)
+                while (h >= 2 && (hd[h - 1] - pd[q]) * (hl[h - 1] - hl[h - 2]) >=
+                                     (hd[h - 2] - hd[h - 1]) * (pl[q] - hl[h - 1]))
+                    --h;
+                hl[h] = pl[q], hd[h] = pd[q], hn[h++] = (uint8_t)pn[q];
+            }
+            cntp[i] = h;
         }
-        first[i] = HL.size();
-        base += hl[0];
-        for (int q = 0; q < h; ++q) HL.push_back(hl[q]), HD.push_back(hd[q]), HN.push_back((uint8_t)hn[q]);
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = n < 4096 ? 1 : std::min<size_t>(std::min(16u, hw), n / 1024);
+    if (nt <= 1) {
+        hulls(0, n);
+    } else {
+        std::vector<std::thread> pool;
+        const size_t per = (n + nt - 1) / nt;
+        for (size_t t = 1; t < nt; ++t) pool.emplace_back(hulls, std::min(n, t * per), std::min(n, (t + 1) * per));
+        hulls(0, std::min(n, per));
+        for (auto& th : pool) th.join();
     }
-    first[n] = HL.size();
+    double base = 0.0;  // bytes of every hull's first point (L = 0)
+    for (size_t i = 0; i < n; ++i) base += HL[i * 33];
     // every hull segment (slope, extra bytes); a block's segments have decreasing slopes, so
     // keeping the segments of slope above a threshold keeps a prefix of every hull
     struct Seg {
@@ -143,7 +161,7 @@ extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* 
     seg.clear();
     double all = base;
     for (size_t i = 0; i < n; ++i)
-        for (size_t q = first[i] + 1; q < first[i + 1]; ++q) {
+        for (size_t q = i * 33 + 1; q < i * 33 + (size_t)cnt[i]; ++q) {
             const double dl = HL[q] - HL[q - 1];
             seg.push_back({(HD[q - 1] - HD[q]) / dl, dl});
             all += dl;
@@ -180,8 +198,9 @@ extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* 
         }
     }
     for (size_t i = 0; i < n; ++i) {
-        size_t q = first[i];
-        while (q + 1 < first[i + 1] && (HD[q] - HD[q + 1]) / (HL[q + 1] - HL[q]) > thr) ++q;
+        size_t q = i * 33;
+        const size_t qe = i * 33 + (size_t)cnt[i];
+        while (q + 1 < qe && (HD[q] - HD[q + 1]) / (HL[q + 1] - HL[q]) > thr) ++q;
         descs[i].npasses = HN[q];
         descs[i].length = HN[q] ? (int32_t)HL[q] : 0;
     }

@@ -141,15 +141,15 @@ def _pcrd_reference(desc, pb, dist, w, budget, extra=4):
     return out
 
 
-@pytest.mark.parametrize("seed", [1, 2, 3])
-def test_pcrd_selection_matches_sorted_threshold(seed):
+@pytest.mark.parametrize("seed,n", [(1, 700), (2, 700), (3, 6000)])
+def test_pcrd_selection_matches_sorted_threshold(seed, n):
+    """n = 6000 builds the blocks' hulls on several host threads (4096 blocks and more)."""
     import ctypes as C
     from roger_b200 import _lib
     f = C.CDLL(_lib.LIB_PATH).j2k_pcrd_truncate
     f.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
     f.restype = None
     rng = np.random.default_rng(seed)
-    n = 700
     desc = np.zeros(n, _lib.CB_DESC)
     pb = np.zeros((n, 32), np.uint32)
     dist = np.zeros((n, 33))
