@@ -204,6 +204,10 @@ static j2k_status rate_control(j2k_encoder* e) {
         if (e->lossy) gain[b] *= (double)e->steps[b] * e->steps[b];
     }
     for (size_t i = 0; i < n; ++i) w[i] = gain[e->hjobs[i].band];
+    // the blocks' hulls do not depend on the budget: built once for every layer and try
+    static thread_local j2k_pcrd_hulls hulls;
+    j2k_pcrd_hulls& hull = hulls;
+    hull.build(dh, n, pb, dist, w.data());
     std::vector<j2k_cb_desc> d(n);
     std::vector<j2k_t2_block> blocks(n);
     for (size_t i = 0; i < n; ++i) blocks[i] = j2k_t2_block{dh[i].numbps, 0, 0, nullptr};
@@ -226,13 +230,10 @@ static j2k_status rate_control(j2k_encoder* e) {
         }
         size_t budget = budgets[l];
         for (int it = 0; it < 24; ++it) {
-            std::memcpy(d.data(), dh, n * sizeof(j2k_cb_desc));
-            j2k_pcrd_truncate(d.data(), n, pb, dist, w.data(), budget);
-            for (size_t i = 0; i < n; ++i) {
-                np[i] = d[i].npasses;
-                ln[i] = d[i].length;
-                if (pnp && np[i] < pnp[i]) np[i] = pnp[i], ln[i] = pln[i];
-            }
+            hull.cut(hull.threshold(budget), np, ln);
+            if (pnp)
+                for (size_t i = 0; i < n; ++i)
+                    if (np[i] < pnp[i]) np[i] = pnp[i], ln[i] = pln[i];
             const size_t size = j2k_t2_size(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy,
                                             e->mct != J2K_MCT_NONE, e->steps.data(), blocks, l + 1,
                                             e->lay_np.data(), e->lay_len.data());

@@ -400,7 +400,7 @@ j2k_status fwd_adj_run(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, s
                        const SynExtra* ex) {
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
-    int ws[20], hs[20];
+    int ws[20] = {}, hs[20] = {};
     ws[0] = (int)w;
     hs[0] = (int)h;
     for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
@@ -583,7 +583,7 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
     J2K_TRY(check_common(ctx, g_img, g_coef, n, w, h, levels));
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
-    int ws[20], hs[20];
+    int ws[20] = {}, hs[20] = {};
     ws[0] = (int)w;
     hs[0] = (int)h;
     for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }

@@ -164,6 +164,27 @@ double j2k_band_gain(int kernel, int levels, int band);
 // as low as the convex hulls allow.  Writes descs[i].npasses and descs[i].length.
 extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
                                   const double* weight, size_t budget);
+// The same choice split in three, for callers that try several budgets on one set of blocks:
+// build() makes every block's lower convex hull (the budget plays no part), threshold(budget)
+// finds the slope below which hull segments are dropped, cut(thr) writes each block's kept
+// passes and length.  j2k_pcrd_truncate = build + threshold + cut.
+struct j2k_pcrd_hulls {
+    struct Seg {
+        uint64_t key;  // slope (weighted error drop per byte) as the bits of a positive double
+        double dl;     // extra bytes
+    };
+    size_t n = 0, nseg = 0;
+    std::vector<double> L, D;    // block i's hull points in slots [i * 33, i * 33 + cnt[i])
+    std::vector<uint8_t> N;      // passes kept at each hull point
+    std::vector<uint64_t> S;     // slot q > 0: slope key of the segment from point q - 1 to q
+    std::vector<int> cnt;
+    std::vector<Seg> cand;       // selection scratch
+    double base = 0.0, all = 0.0;  // bytes at every hull's first point; at every last point
+    void build(const j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
+               const double* weight);
+    double threshold(size_t budget);
+    void cut(double thr, int32_t* npasses, int32_t* length) const;
+};
 constexpr int J2K_TRUNC_EXTRA = 4;  // bytes kept beyond those produced at a plane end
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,

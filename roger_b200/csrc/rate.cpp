@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <limits>
 #include <thread>
 #include <vector>
@@ -87,22 +88,26 @@ double j2k_band_gain(int kernel, int levels, int band) {
     return o == 0 ? gh * gl : (o == 1 ? gl * gh : gh * gh);
 }
 
-extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
-                                  const double* weight, size_t budget) {
-    // hull points of every block: block i owns slots [i * 33, i * 33 + cnt[i]) (scratch kept per
-    // thread between calls); the blocks' hulls are independent and built on host threads
-    static thread_local std::vector<double> HL, HD;
-    static thread_local std::vector<uint8_t> HN;
-    static thread_local std::vector<int> cnt;
-    HL.resize(n * 33);
-    HD.resize(n * 33);
-    HN.resize(n * 33);
+void j2k_pcrd_hulls::build(const j2k_cb_desc* descs, size_t nblocks, const uint32_t* plane_bytes,
+                           const double* dist, const double* weight) {
+    n = nblocks;
+    L.resize(n * 33);
+    D.resize(n * 33);
+    N.resize(n * 33);
+    S.resize(n * 33);
     cnt.assign(n, 0);
-    double* const hlp = HL.data();
-    double* const hdp = HD.data();
-    uint8_t* const hnp = HN.data();
+    double* const hlp = L.data();
+    double* const hdp = D.data();
+    uint8_t* const hnp = N.data();
+    uint64_t* const hsp = S.data();
     int* const cntp = cnt.data();
-    auto hulls = [&](size_t i0, size_t i1) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = n < 4096 ? 1 : std::min<size_t>(std::min(16u, hw), n / 1024);
+    std::vector<double> part_base(nt, 0.0), part_all(nt, 0.0);
+    std::vector<size_t> part_ns(nt, 0);
+    auto hulls = [=, &part_base, &part_all, &part_ns](size_t t, size_t i0, size_t i1) {
+        double sb = 0.0, sa = 0.0;
+        size_t ns = 0;
         for (size_t i = i0; i < i1; ++i) {
             const j2k_cb_desc& d = descs[i];
             const int nb = d.numbps;
@@ -137,71 +142,127 @@ extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* 
                 hl[h] = pl[q], hd[h] = pd[q], hn[h++] = (uint8_t)pn[q];
             }
             cntp[i] = h;
+            // slopes of the hull segments as ordered keys: positive doubles order as their bits
+            uint64_t* hs = hsp + i * 33;
+            for (int q = 1; q < h; ++q) {
+                const double sl = (hd[q - 1] - hd[q]) / (hl[q] - hl[q - 1]);
+                std::memcpy(&hs[q], &sl, 8);
+            }
+            sb += hl[0];
+            sa += hl[h - 1];
+            ns += (size_t)(h - 1);
         }
+        part_base[t] = sb, part_all[t] = sa, part_ns[t] = ns;
     };
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t nt = n < 4096 ? 1 : std::min<size_t>(std::min(16u, hw), n / 1024);
     if (nt <= 1) {
-        hulls(0, n);
+        hulls(0, 0, n);
     } else {
         std::vector<std::thread> pool;
         const size_t per = (n + nt - 1) / nt;
-        for (size_t t = 1; t < nt; ++t) pool.emplace_back(hulls, std::min(n, t * per), std::min(n, (t + 1) * per));
-        hulls(0, std::min(n, per));
+        for (size_t t = 1; t < nt; ++t)
+            pool.emplace_back(hulls, t, std::min(n, t * per), std::min(n, (t + 1) * per));
+        hulls(0, 0, std::min(n, per));
         for (auto& th : pool) th.join();
     }
-    double base = 0.0;  // bytes of every hull's first point (L = 0)
-    for (size_t i = 0; i < n; ++i) base += HL[i * 33];
-    // every hull segment (slope, extra bytes); a block's segments have decreasing slopes, so
-    // keeping the segments of slope above a threshold keeps a prefix of every hull
-    struct Seg {
-        double s, dl;
-    };
-    static thread_local std::vector<Seg> seg;
-    seg.clear();
-    double all = base;
-    for (size_t i = 0; i < n; ++i)
-        for (size_t q = i * 33 + 1; q < i * 33 + (size_t)cnt[i]; ++q) {
-            const double dl = HL[q] - HL[q - 1];
-            seg.push_back({(HD[q - 1] - HD[q]) / dl, dl});
-            all += dl;
-        }
-    // Threshold: in the order of decreasing slope, the slope of the first segment that no longer
-    // fits the budget; segments of that slope or less are dropped (ties together).  Found by a
-    // weighted quickselect, linear in the number of segments on average.
-    double thr = -1.0;  // keep everything
-    if (all > (double)budget) {
-        double room = (double)budget - base;
-        size_t a = 0, b = seg.size();
-        uint64_t rng = 0x9E3779B97F4A7C15ull;
-        thr = std::numeric_limits<double>::infinity();
-        while (a < b) {
-            rng ^= rng << 13, rng ^= rng >> 7, rng ^= rng << 17;
-            const double piv = seg[a + rng % (b - a)].s;
-            // [a, g): slope > piv, [g, e): slope == piv, [e, b): slope < piv
-            auto g = std::partition(seg.begin() + a, seg.begin() + b, [piv](const Seg& x) { return x.s > piv; });
-            auto e = std::partition(g, seg.begin() + b, [piv](const Seg& x) { return x.s == piv; });
-            double sg = 0.0, se = 0.0;
-            for (auto it = seg.begin() + a; it != g; ++it) sg += it->dl;
-            if (sg > room) {
-                b = (size_t)(g - seg.begin());
-                continue;
-            }
-            room -= sg;
-            for (auto it = g; it != e; ++it) se += it->dl;
-            if (se > room) {
-                thr = piv;
-                break;
-            }
-            room -= se;
-            a = (size_t)(e - seg.begin());
-        }
-    }
+    // byte counts are whole numbers, so these sums are exact in any order
+    base = all = 0.0;
+    nseg = 0;
+    for (size_t t = 0; t < nt; ++t) base += part_base[t], all += part_all[t], nseg += part_ns[t];
+}
+
+double j2k_pcrd_hulls::threshold(size_t budget) {
+    // In the order of decreasing slope, the slope of the first segment that no longer fits the
+    // budget; segments of that slope or less are dropped (ties together): the slope v with
+    // bytes(slope > v) <= room < bytes(slope >= v).  Found by a radix selection on the slopes'
+    // bits, 11 bits per pass from the top: each pass sums the candidates' extra bytes per digit,
+    // keeps the candidates of the digit where the running sum from the top passes the room, and
+    // takes the bytes of the digits above it off the room.  Byte counts are whole numbers, so
+    // every sum is exact and the result does not depend on the order of the segments.
+    if (all <= (double)budget) return -1.0;  // keep everything
+    double room = (double)budget - base;
+    if (room < 0.0 || nseg == 0) return std::numeric_limits<double>::infinity();
+    constexpr int kBits = 11, kBins = 1 << kBits;
+    double hist[kBins];
+    // first pass over every hull segment, in place (a negative slope cannot occur: hull points'
+    // distortions strictly decrease); the sign bit is 0, so digit 0 is bits 62..52
+    std::memset(hist, 0, sizeof(hist));
+    const double* hl = L.data();
+    const uint64_t* hs = S.data();
     for (size_t i = 0; i < n; ++i) {
-        size_t q = i * 33;
-        const size_t qe = i * 33 + (size_t)cnt[i];
-        while (q + 1 < qe && (HD[q] - HD[q + 1]) / (HL[q + 1] - HL[q]) > thr) ++q;
-        descs[i].npasses = HN[q];
-        descs[i].length = HN[q] ? (int32_t)HL[q] : 0;
+        const size_t b0 = i * 33;
+        for (int q = 1; q < cnt[i]; ++q) hist[(hs[b0 + q] >> 52) & (kBins - 1)] += hl[b0 + q] - hl[b0 + q - 1];
     }
+    auto pick = [&](const double* hh) {
+        double above = 0.0;
+        for (int b = kBins - 1; b >= 0; --b) {
+            if (above + hh[b] > room) {
+                room -= above;
+                return b;
+            }
+            above += hh[b];
+        }
+        return -1;  // cannot happen: the candidates' bytes exceed the room
+    };
+    int dig = pick(hist);
+    if (dig < 0) return std::numeric_limits<double>::infinity();
+    uint64_t prefix = (uint64_t)dig << 52;
+    int shift = 52;  // bits below the digits fixed so far
+    cand.clear();
+    for (size_t i = 0; i < n; ++i) {
+        const size_t b0 = i * 33;
+        for (int q = 1; q < cnt[i]; ++q)
+            if ((hs[b0 + q] >> 52) == (uint64_t)dig) cand.push_back(Seg{hs[b0 + q], hl[b0 + q] - hl[b0 + q - 1]});
+    }
+    while (shift > 0) {
+        const int bits = std::min(kBits, shift);
+        shift -= bits;
+        const uint64_t mask = ((uint64_t)1 << bits) - 1;
+        std::memset(hist, 0, sizeof(hist));
+        for (const Seg& c : cand) hist[(c.key >> shift) & mask] += c.dl;
+        double above = 0.0;
+        int b = (int)mask;
+        for (; b >= 0; --b) {
+            if (above + hist[b] > room) break;
+            above += hist[b];
+        }
+        if (b < 0) return std::numeric_limits<double>::infinity();
+        room -= above;
+        prefix |= (uint64_t)b << shift;
+        size_t k = 0;
+        for (const Seg& c : cand)
+            if (((c.key >> shift) & mask) == (uint64_t)b) cand[k++] = c;
+        cand.resize(k);
+    }
+    double thr;
+    std::memcpy(&thr, &prefix, 8);
+    return thr;
+}
+
+void j2k_pcrd_hulls::cut(double thr, int32_t* npasses, int32_t* length) const {
+    const double* hl = L.data();
+    const uint64_t* hs = S.data();
+    const uint8_t* hn = N.data();
+    uint64_t tk;  // slopes compare as their bits; a threshold of -1 keeps every segment
+    std::memcpy(&tk, &thr, 8);
+    const bool all_kept = thr < 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        const size_t b0 = i * 33;
+        int q = 0;
+        while (q + 1 < cnt[i] && (all_kept || hs[b0 + q + 1] > tk)) ++q;
+        npasses[i] = hn[b0 + q];
+        length[i] = hn[b0 + q] ? (int32_t)hl[b0 + q] : 0;
+    }
+}
+
+extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
+                                  const double* weight, size_t budget) {
+    static thread_local j2k_pcrd_hulls hulls;  // scratch kept per thread between calls
+    static thread_local std::vector<int32_t> np, len;
+    j2k_pcrd_hulls& h = hulls;
+    h.build(descs, n, plane_bytes, dist, weight);
+    const double thr = h.threshold(budget);
+    np.resize(n);
+    len.resize(n);
+    h.cut(thr, np.data(), len.data());
+    for (size_t i = 0; i < n; ++i) descs[i].npasses = (uint8_t)np[i], descs[i].length = len[i];
 }

@@ -179,6 +179,39 @@ def test_pcrd_selection_matches_sorted_threshold(seed, n):
         assert int(d2["length"].sum()) <= min(budget, full)
 
 
+def test_pcrd_ties_drop_together():
+    """Thousands of identical blocks give hull segments of equal slope; a budget that falls inside
+    such a group drops the whole group, as the sorted restatement does (threaded hull build)."""
+    import ctypes as C
+    from roger_b200 import _lib
+    f = C.CDLL(_lib.LIB_PATH).j2k_pcrd_truncate
+    f.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
+    f.restype = None
+    n = 5000
+    desc = np.zeros(n, _lib.CB_DESC)
+    pb = np.zeros((n, 32), np.uint32)
+    dist = np.zeros((n, 33))
+    kinds = [(5, [40, 90, 200, 420, 800], [6e5, 2e5, 5e4, 9e3, 0.0], 1e6),
+             (3, [10, 60, 300], [3e5, 4e4, 0.0], 8e5)]
+    for i in range(n):
+        nb, cum, d, d0 = kinds[i % 3 == 0]
+        desc[i]["numbps"] = nb
+        desc[i]["npasses"] = 3 * nb - 2
+        desc[i]["length"] = cum[-1] + 3
+        pb[i, :nb] = cum
+        dist[i, 32] = d0
+        dist[i, :nb] = d
+    w = np.where(np.arange(n) % 2 == 0, 1.0, 2.0)  # two bands: ties within each
+    full = int(desc["length"].sum())
+    for frac in (0.01, 0.1, 0.25, 0.5, 0.75, 0.99):
+        budget = int(full * frac)
+        d2 = desc.copy()
+        f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget)
+        ref = _pcrd_reference(desc, pb, dist, w, budget)
+        assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == ref
+        assert int(d2["length"].sum()) <= budget
+
+
 @pytest.mark.gpu
 def test_quality_layers():
     from PIL import Image
