@@ -1,6 +1,7 @@
 // Tier-2: T.800 codestream assembly on the host (Annex A markers, Annex B packets).
 // One tile, one quality layer, LRCP progression, one precinct per resolution, code-blocks of
 // one codeword segment each (all passes included).  The reference has no tier-2 at all.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -32,8 +33,24 @@ struct BitWriter {
             nb = 0;
         }
     }
+    // the n low bits of v, most significant first (n <= 32), a byte's worth at a time
     void bits(uint32_t v, int n) {
-        for (int i = n - 1; i >= 0; --i) bit((v >> i) & 1);
+        while (n > 0) {
+            const int take = std::min(room - nb, n);
+            n -= take;
+            acc = (acc << take) | ((v >> n) & ((1u << take) - 1));
+            nb += take;
+            if (nb == room) {
+                out.u8(acc);
+                room = (acc == 0xFF) ? 7 : 8;
+                acc = 0;
+                nb = 0;
+            }
+        }
+    }
+    void zeros(int n) {
+        for (; n > 24; n -= 24) bits(0, 24);
+        bits(0, n);
     }
     void flush() {
         bool last_ff;
@@ -96,29 +113,27 @@ struct TagTree {
         for (int l = nlev - 1; l >= 0; --l) {
             int n = path[l];
             if (lo > low[n]) low[n] = lo; else lo = low[n];
-            while (lo < threshold) {
-                if (lo >= val[n]) {
-                    if (!known[n]) {
-                        bw.bit(1);
-                        known[n] = 1;
-                    }
-                    break;
+            // a 0 for every step from lo up to the node's value (or the threshold), then a 1
+            // once the value is reached below the threshold, if not sent before
+            if (lo < threshold) {
+                const int v = val[n];
+                if (v > lo) {
+                    const int stop = std::min(v, threshold);
+                    bw.zeros(stop - lo);
+                    lo = stop;
                 }
-                bw.bit(0);
-                ++lo;
+                if (lo < threshold && !known[n]) {
+                    bw.bit(1);
+                    known[n] = 1;
+                }
             }
             low[n] = lo;
         }
     }
 };
 
-int floorlog2(long v) {
-    int l = -1;
-    while (v) {
-        v >>= 1;
-        ++l;
-    }
-    return l;
+int floorlog2(long v) {  // -1 for 0
+    return v > 0 ? 63 - __builtin_clzl((unsigned long)v) : -1;
 }
 
 void put_npasses(BitWriter& bw, int n) {  // Table B.4
@@ -294,8 +309,7 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
                             int bits = floorlog2(seg) + 1;
                             int avail = lblock[k] + floorlog2(newp);
                             int inc = bits > avail ? bits - avail : 0;
-                            for (int t = 0; t < inc; ++t) bw.bit(1);
-                            bw.bit(0);
+                            bw.bits(((1u << inc) - 1) << 1, inc + 1);  // inc ones, then a zero
                             lblock[k] += inc;
                             bw.bits((uint32_t)seg, lblock[k] + floorlog2(newp));
                         }
