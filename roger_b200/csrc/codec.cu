@@ -131,6 +131,7 @@ struct j2k_encoder {
     std::vector<size_t> layer_budget;
     std::vector<int32_t> lay_np, lay_len;
     DevBuf rate_pb, rate_dist;
+    j2k_pcrd_hulls pcrd;  // the blocks' convex hulls of the last rate-controlled encode
     void* mapped = nullptr;
 };
 
@@ -205,8 +206,7 @@ static j2k_status rate_control(j2k_encoder* e) {
     }
     for (size_t i = 0; i < n; ++i) w[i] = gain[e->hjobs[i].band];
     // the blocks' hulls do not depend on the budget: built once for every layer and try
-    static thread_local j2k_pcrd_hulls hulls;
-    j2k_pcrd_hulls& hull = hulls;
+    j2k_pcrd_hulls& hull = e->pcrd;
     hull.build(dh, n, pb, dist, w.data());
     std::vector<j2k_cb_desc> d(n);
     std::vector<j2k_t2_block> blocks(n);
