@@ -35,6 +35,7 @@ typedef int j2k_status;
 #define J2K_ERR_CAPACITY (-5)     /* an output buffer was too small; nothing past it was written */
 #define J2K_ERR_UNSUPPORTED (-6)
 #define J2K_ERR_TIMEOUT (-7)      /* a bounded device-side wait gave up */
+#define J2K_ERR_HOST (-8)         /* a host-side failure other than memory (a host thread could not start) */
 
 enum { J2K_U8 = 0, J2K_I16 = 1, J2K_I32 = 2, J2K_F32 = 3 };
 enum { J2K_MCT_NONE = 0, J2K_MCT_RCT = 1, J2K_MCT_ICT = 2 };

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libj2kb200.so")
 J2K_OK = 0
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -4: "device-reported error", -5: "output capacity exceeded", -6: "unsupported",
-          -7: "device wait timed out"}
+          -7: "device wait timed out", -8: "host error"}
 U8, I16, I32, F32 = 0, 1, 2, 3
 MCT_NONE, MCT_RCT, MCT_ICT = 0, 1, 2
 ORDER_T800, ORDER_REF = 0, 1

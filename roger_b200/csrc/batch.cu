@@ -357,6 +357,7 @@ static j2k_status run_once(j2k_batch* b) {
 extern "C" {
 
 j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, j2k_batch** out) {
+    J2K_API_BEGIN
     if (!ctx || !out || !images || n <= 0) return J2K_ERR_INVALID_ARG;
     *out = nullptr;
     j2k_batch* b = new (std::nothrow) j2k_batch();
@@ -391,9 +392,11 @@ j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, 
     }
     *out = b;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_destroy(j2k_batch* b) {
+    J2K_API_BEGIN
     if (!b) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(b->ctx->device);
     cudaStreamSynchronize(b->ctx->stream);
@@ -404,9 +407,11 @@ j2k_status j2k_batch_destroy(j2k_batch* b) {
         x->release();
     delete b;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_input(j2k_batch* b, uint8_t** device_buffer, size_t* offsets) {
+    J2K_API_BEGIN
     if (!b) return J2K_ERR_INVALID_ARG;
     if (device_buffer) *device_buffer = (uint8_t*)b->in.p;
     if (offsets) {
@@ -414,9 +419,11 @@ j2k_status j2k_batch_input(j2k_batch* b, uint8_t** device_buffer, size_t* offset
         offsets[b->img.size()] = b->in_bytes;
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value) {
+    J2K_API_BEGIN
     if (!b) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     switch (key) {
@@ -432,9 +439,11 @@ j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value) {
     }
     drop_graph(b);
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
+    J2K_API_BEGIN
     if (!b || !value) return J2K_ERR_INVALID_ARG;
     switch (key) {
         case J2K_BATCH_USE_GRAPH: *value = b->use_graph; break;
@@ -447,9 +456,11 @@ j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
         default: return J2K_ERR_INVALID_ARG;
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_upload(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
+    J2K_API_BEGIN
     if (!b || !pixels) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
@@ -461,9 +472,11 @@ j2k_status j2k_batch_upload(j2k_batch* b, const uint8_t* const* pixels, int on_d
                                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_encode_async(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
+    J2K_API_BEGIN
     if (!b) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
@@ -474,6 +487,7 @@ j2k_status j2k_batch_encode_async(j2k_batch* b, const uint8_t* const* pixels, in
     J2K_TRY(run_once(b));
     b->pending = true;
     return J2K_OK;
+    J2K_API_END
 }
 
 }  // extern "C"
@@ -503,13 +517,16 @@ static j2k_status batch_finish(j2k_batch* b) {
 extern "C" {
 
 j2k_status j2k_batch_encode(j2k_batch* b, const uint8_t* const* pixels, int on_device) {
+    J2K_API_BEGIN
     J2K_TRY(j2k_batch_encode_async(b, pixels, on_device));
     return batch_finish(b);
+    J2K_API_END
 }
 
 // Times each candidate on this batch (CUDA events around the stage it affects) and keeps the
 // fastest: DWT tile shape per filter, then phase-A order, then the MQ schedule.
 j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report) {
+    J2K_API_BEGIN
     if (!b) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
@@ -589,10 +606,12 @@ j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report) {
         report[4] = ctx->mq_lanes;
     }
     return s;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_get_codeblocks(j2k_batch* b, int image, j2k_cb_desc* descs, size_t* count,
                                     uint8_t* bytes, size_t cap, size_t* used) {
+    J2K_API_BEGIN
     if (!b || !count || image < 0 || image >= (int)b->img.size()) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     J2K_TRY(batch_finish(b));
@@ -622,9 +641,11 @@ j2k_status j2k_batch_get_codeblocks(j2k_batch* b, int image, j2k_cb_desc* descs,
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (descs) std::memcpy(descs, d.data(), im.njobs * sizeof(j2k_cb_desc));
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_get_codestream(j2k_batch* b, int image, uint8_t* out, size_t cap, size_t* len) {
+    J2K_API_BEGIN
     if (!b || !len) return J2K_ERR_INVALID_ARG;
     size_t count = 0, total = 0;
     J2K_TRY(j2k_batch_get_codeblocks(b, image, nullptr, &count, nullptr, 0, &total));
@@ -641,6 +662,7 @@ j2k_status j2k_batch_get_codestream(j2k_batch* b, int image, uint8_t* out, size_
     if (cap < cs.size()) return j2k_fail(b->ctx, J2K_ERR_CAPACITY, "codestream buffer too small");
     std::memcpy(out, cs.data(), cs.size());
     return J2K_OK;
+    J2K_API_END
 }
 
 }  // extern "C"
@@ -649,6 +671,7 @@ j2k_status j2k_batch_get_codestream(j2k_batch* b, int image, uint8_t* out, size_
 extern "C" {
 
 j2k_status j2k_batch_pack(j2k_batch* b, size_t* total) {
+    J2K_API_BEGIN
     if (!b || !total) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     cudaSetDevice(ctx->device);
@@ -677,9 +700,11 @@ j2k_status j2k_batch_pack(j2k_batch* b, size_t* total) {
     b->packed_total = tot;
     *total = tot;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_read_packed(j2k_batch* b, j2k_cb_desc* descs, uint8_t* bytes, size_t cap) {
+    J2K_API_BEGIN
     if (!b || !descs || !bytes) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = b->ctx;
     if (cap < b->packed_total) return j2k_fail(ctx, J2K_ERR_CAPACITY, "bytes buffer smaller than the packed total");
@@ -689,13 +714,16 @@ j2k_status j2k_batch_read_packed(j2k_batch* b, j2k_cb_desc* descs, uint8_t* byte
     if (b->packed_total)
         J2K_CUDA(ctx, cudaMemcpyAsync(bytes, b->packed.p, b->packed_total, cudaMemcpyDeviceToHost, ctx->stream));
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_batch_image_jobs(j2k_batch* b, size_t* first) {
+    J2K_API_BEGIN
     if (!b || !first) return J2K_ERR_INVALID_ARG;
     for (size_t i = 0; i < b->img.size(); ++i) first[i] = b->img[i].job0;
     first[b->img.size()] = b->hjobs.size();
     return J2K_OK;
+    J2K_API_END
 }
 
 }  // extern "C"

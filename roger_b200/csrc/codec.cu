@@ -79,13 +79,9 @@ void host_parallel(int n, size_t bytes, F fn) {
         for (int k = 0; k < n; ++k) fn(k);
         return;
     }
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nt; ++t)
-        pool.emplace_back([&, t] {
-            for (int k = t; k < n; k += nt) fn(k);
-        });
-    for (int k = 0; k < n; k += nt) fn(k);
-    for (auto& th : pool) th.join();
+    j2k_run_threads(nt, [&](int t) {
+        for (int k = t; k < n; k += nt) fn(k);
+    });
 }
 
 // A host copy split over up to 16 threads when it is large (one thread copies at a few GB/s).
@@ -360,6 +356,7 @@ extern "C" {
 j2k_status j2k_bpc_encode(j2k_ctx* ctx, const int32_t* coeff, size_t pitch, size_t w, size_t h,
                           int levels, int cbw, int cbh, j2k_cb_desc* descs, uint8_t* bytes,
                           size_t cap_per_block) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     if (!coeff || !descs || !bytes || pitch < w || w == 0 || h == 0 || w > 65535 || h > 65535)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_encode: bad pointer/size/pitch");
@@ -388,11 +385,13 @@ j2k_status j2k_bpc_encode(j2k_ctx* ctx, const int32_t* coeff, size_t pitch, size
         return s;
     }
     return j2k_fail(ctx, J2K_ERR_CAPACITY, "tier-1 symbol capacity kept overflowing");
+    J2K_API_END
 }
 
 j2k_status j2k_bpc_decode(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                           size_t count, int32_t* coeff, size_t pitch, size_t w, size_t h,
                           int levels, int cbw, int cbh) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     if (!coeff || !descs || !bytes || pitch < w || w == 0 || h == 0 || w > 65535 || h > 65535)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bpc_decode: bad pointer/size/pitch");
@@ -409,9 +408,11 @@ j2k_status j2k_bpc_decode(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t*
     J2K_TRY(j2k_clear_device_error(ctx));
     J2K_TRY(j2k_t1_decode_jobs(ctx, descs, bytes, dj, jobs.size(), coeff, ctx->stream));
     return j2k_read_device_error(ctx);
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_encoder** out) {
+    J2K_API_BEGIN
     if (!ctx || !out) return J2K_ERR_INVALID_ARG;
     j2k_encoder* e = new (std::nothrow) j2k_encoder();
     if (!e) return J2K_ERR_OUT_OF_MEMORY;
@@ -420,9 +421,11 @@ j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_
     e->dwt_only = output_dwt_only ? 1 : 0;
     *out = e;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_destroy(j2k_encoder* e) {
+    J2K_API_BEGIN
     if (!e) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(e->ctx->device);
     cudaStreamSynchronize(e->ctx->stream);
@@ -432,6 +435,7 @@ j2k_status j2k_encoder_destroy(j2k_encoder* e) {
     if (e->mapped) cudaFreeHost(e->mapped);
     delete e;
     return J2K_OK;
+    J2K_API_END
 }
 
 static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const j2k_enc_params* p) {
@@ -481,6 +485,7 @@ static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const
 j2k_status j2k_encoder_run_interleaved(j2k_encoder* e, const uint8_t* pixels, int on_device,
                                        size_t pitch, int ncomp, size_t w, size_t h,
                                        const j2k_enc_params* p) {
+    J2K_API_BEGIN
     if (!e) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = e->ctx;
     if (!pixels) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "pixels is NULL");
@@ -497,10 +502,12 @@ j2k_status j2k_encoder_run_interleaved(j2k_encoder* e, const uint8_t* pixels, in
     J2K_TRY(j2k_launch_planar_fwd(ctx, src, pitch, ncomp, e->mct, e->lossy ? J2K_F32 : J2K_I32, e->planes.p,
                                   w, w * h, w, h, ctx->stream));
     return encode_planes(e);
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_run(j2k_encoder* e, const void* const* comps, int ncomp, int dtype, size_t w,
                            size_t h, size_t levels, size_t precision, const j2k_enc_params* p) {
+    J2K_API_BEGIN
     if (!e) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = e->ctx;
     if (!comps) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "components is NULL");
@@ -523,9 +530,11 @@ j2k_status j2k_encoder_run(j2k_encoder* e, const void* const* comps, int ncomp, 
     }
     if (e->mct != J2K_MCT_NONE) J2K_TRY(j2k_launch_mct_planes(ctx, e->planes.p, pd, n, n, e->mct, ctx->stream));
     return encode_planes(e);
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_map_dwt_out(j2k_encoder* e, void** ptr, size_t* pitch_bytes) {
+    J2K_API_BEGIN
     if (!e || !ptr) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = e->ctx;
     if (!e->have_result) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no encoder run yet");
@@ -536,19 +545,23 @@ j2k_status j2k_encoder_map_dwt_out(j2k_encoder* e, void** ptr, size_t* pitch_byt
     *ptr = e->mapped;
     if (pitch_bytes) *pitch_bytes = e->w * 4;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_unmap_dwt_out(j2k_encoder* e, void* ptr) {
+    J2K_API_BEGIN
     if (!e) return J2K_ERR_INVALID_ARG;
     if (ptr && ptr == e->mapped) {
         cudaFreeHost(e->mapped);
         e->mapped = nullptr;
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_get_codeblocks(j2k_encoder* e, j2k_cb_desc* descs, size_t* count,
                                       uint8_t* bytes, size_t cap, size_t* used) {
+    J2K_API_BEGIN
     if (!e || !count) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = e->ctx;
     if (!e->have_result || e->dwt_only) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no tier-1 result");
@@ -585,9 +598,11 @@ j2k_status j2k_encoder_get_codeblocks(j2k_encoder* e, j2k_cb_desc* descs, size_t
         }
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_autotune(j2k_encoder* e, int reps, int* report) {
+    J2K_API_BEGIN
     if (!e) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = e->ctx;
     if (!e->have_result || e->dwt_only || e->njobs == 0)
@@ -641,9 +656,11 @@ j2k_status j2k_encoder_autotune(j2k_encoder* e, int reps, int* report) {
     e->packed_ok = false;
     if (s == J2K_OK) s = run_tier1(e);
     return s;
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, size_t* len) {
+    J2K_API_BEGIN
     if (!e || !len) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = e->ctx;
     size_t count = 0, total = 0;
@@ -667,10 +684,12 @@ j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, 
     if (cap < cs.size()) return j2k_fail(ctx, J2K_ERR_CAPACITY, "codestream buffer too small");
     std::memcpy(out, cs.data(), cs.size());
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_encoder_device_results(j2k_encoder* e, const j2k_cb_desc** descs, const uint8_t** bytes,
                                       size_t* count, size_t* cap_per_block) {
+    J2K_API_BEGIN
     if (!e) return J2K_ERR_INVALID_ARG;
     if (!e->have_result || e->dwt_only) return j2k_fail(e->ctx, J2K_ERR_INVALID_ARG, "no tier-1 result");
     if (descs) *descs = (const j2k_cb_desc*)e->descs.p;
@@ -678,9 +697,11 @@ j2k_status j2k_encoder_device_results(j2k_encoder* e, const j2k_cb_desc** descs,
     if (count) *count = e->njobs;
     if (cap_per_block) *cap_per_block = e->cap;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_decoder_create(j2k_ctx* ctx, int lossy, j2k_decoder** out) {
+    J2K_API_BEGIN
     if (!ctx || !out) return J2K_ERR_INVALID_ARG;
     j2k_decoder* d = new (std::nothrow) j2k_decoder();
     if (!d) return J2K_ERR_OUT_OF_MEMORY;
@@ -688,18 +709,22 @@ j2k_status j2k_decoder_create(j2k_ctx* ctx, int lossy, j2k_decoder** out) {
     d->lossy = lossy ? 1 : 0;
     *out = d;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_decoder_destroy(j2k_decoder* d) {
+    J2K_API_BEGIN
     if (!d) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(d->ctx->device);
     cudaStreamSynchronize(d->ctx->stream);
     for (DevBuf* b : {&d->descs, &d->bytes, &d->coef, &d->planes, &d->out, &d->jobs}) b->release();
     delete d;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, int n) {
+    J2K_API_BEGIN
     if (!d || (!items && n > 0) || n < 0) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = d->ctx;
     if (n == 0) return J2K_OK;
@@ -805,10 +830,12 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
     J2K_TRY(j2k_read_device_error(ctx));
     host_parallel(n, out_off[n], [&](int k) { std::memcpy(items[k].out, hs + out_off[k], out_off[k + 1] - out_off[k]); });
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* streams, const size_t* sizes, int n,
                                        int max_layers, uint8_t* const* outs) {
+    J2K_API_BEGIN
     if (!d || n < 0 || (n > 0 && (!streams || !sizes || !outs)) || max_layers < 0) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = d->ctx;
     if (n == 0) return J2K_OK;
@@ -826,13 +853,15 @@ j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* str
                 msg[k] = "NULL stream";
                 continue;
             }
-            st[k] = j2k_t2_parse_packed(streams[k], sizes[k], max_layers, &info[k], &descs[k], &bytes[k], &msg[k]);
+            try {
+                st[k] = j2k_t2_parse_packed(streams[k], sizes[k], max_layers, &info[k], &descs[k], &bytes[k],
+                                            &msg[k]);
+            } catch (...) {  // a host allocation failed
+                st[k] = J2K_ERR_OUT_OF_MEMORY;
+            }
         }
     };
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto& th : pool) th.join();
+    j2k_run_threads(nt, work);
     std::vector<j2k_decode_item> items(n);
     for (int k = 0; k < n; ++k) {
         if (st[k] != J2K_OK) return j2k_fail(ctx, st[k], "stream " + std::to_string(k) + ": " + msg[k]);
@@ -843,12 +872,14 @@ j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* str
                                    bytes[k].data(), bytes[k].size(), outs[k]};
     }
     return j2k_decoder_run_batch(d, items.data(), n);
+    J2K_API_END
 }
 
 j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, const uint8_t* bytes,
                                       size_t nbytes, int on_device, int ncomp, size_t w, size_t h,
                                       const j2k_enc_params* p, uint8_t* out, int out_on_device,
                                       size_t out_pitch) {
+    J2K_API_BEGIN
     if (!d) return J2K_ERR_INVALID_ARG;
     j2k_ctx* ctx = d->ctx;
     if (!descs || !bytes || !out) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "NULL pointer");
@@ -921,6 +952,7 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
         J2K_CUDA(ctx, cudaMemcpyAsync(out, dst, ob, cudaMemcpyDeviceToHost, ctx->stream));
     }
     return j2k_read_device_error(ctx);
+    J2K_API_END
 }
 
 }  // extern "C"

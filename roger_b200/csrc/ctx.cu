@@ -167,11 +167,13 @@ const char* j2k_status_string(j2k_status s) {
         case J2K_ERR_CAPACITY: return "output capacity exceeded";
         case J2K_ERR_UNSUPPORTED: return "unsupported";
         case J2K_ERR_TIMEOUT: return "device wait timed out";
+        case J2K_ERR_HOST: return "host error";
         default: return "unknown status";
     }
 }
 
 j2k_status j2k_ctx_create(int device, j2k_ctx** out) {
+    J2K_API_BEGIN
     if (!out) return J2K_ERR_INVALID_ARG;
     *out = nullptr;
     j2k_ctx* c = new (std::nothrow) j2k_ctx();
@@ -198,9 +200,11 @@ j2k_status j2k_ctx_create(int device, j2k_ctx** out) {
     c->mq_lanes = 16;
     *out = c;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_ctx_destroy(j2k_ctx* ctx) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
@@ -211,29 +215,37 @@ j2k_status j2k_ctx_destroy(j2k_ctx* ctx) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_ctx_set_stream(j2k_ctx* ctx, void* s) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     ctx->stream = (cudaStream_t)s;  // NULL is the CUDA legacy default stream
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_ctx_use_own_stream(j2k_ctx* ctx) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     ctx->stream = ctx->own_stream;
     return J2K_OK;
+    J2K_API_END
 }
 
 void* j2k_ctx_stream(j2k_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 j2k_status j2k_stream_sync(j2k_ctx* ctx) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     if (key == J2K_TUNE_MQ_LANES) {
         if (value != 8 && value != 16 && value != 32)
@@ -269,6 +281,7 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         return J2K_OK;
     }
     return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown tuning key");
+    J2K_API_END
 }
 
 const char* j2k_last_error(const j2k_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
@@ -281,6 +294,7 @@ size_t j2k_codeblock_count(size_t w, size_t h, int levels, int cbw, int cbh) {
 j2k_status j2k_rgb_to_planar(j2k_ctx* ctx, const uint8_t* in, size_t in_pitch, int ncomp, int mct,
                              int out_dtype, void* planes, size_t plane_pitch, size_t plane_stride,
                              size_t w, size_t h) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     if (!in || !planes || ncomp < 1 || ncomp > 4 || w == 0 || h == 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "rgb_to_planar: bad pointer/ncomp/size");
@@ -294,11 +308,13 @@ j2k_status j2k_rgb_to_planar(j2k_ctx* ctx, const uint8_t* in, size_t in_pitch, i
     cudaSetDevice(ctx->device);
     return j2k_launch_planar_fwd(ctx, in, in_pitch, ncomp, mct, out_dtype, planes, plane_pitch,
                                  plane_stride, w, h, ctx->stream);
+    J2K_API_END
 }
 
 j2k_status j2k_planar_to_rgb(j2k_ctx* ctx, const void* planes, int in_dtype, size_t plane_pitch,
                              size_t plane_stride, int ncomp, int mct, uint8_t* out,
                              size_t out_pitch, size_t w, size_t h) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     if (!out || !planes || ncomp < 1 || ncomp > 4 || w == 0 || h == 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "planar_to_rgb: bad pointer/ncomp/size");
@@ -311,6 +327,7 @@ j2k_status j2k_planar_to_rgb(j2k_ctx* ctx, const void* planes, int in_dtype, siz
     cudaSetDevice(ctx->device);
     return j2k_launch_planar_inv(ctx, planes, in_dtype, plane_pitch, plane_stride, ncomp, mct, out,
                                  out_pitch, w, h, ctx->stream);
+    J2K_API_END
 }
 
 static j2k_status check_dwt_args(j2k_ctx* ctx, int kernel, int order, const void* in,
@@ -332,6 +349,7 @@ static j2k_status check_dwt_args(j2k_ctx* ctx, int kernel, int order, const void
 j2k_status j2k_dwt_forward(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
                            const float* steps) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     J2K_TRY(check_dwt_args(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels));
     if (kernel == J2K_W53 && steps)
@@ -343,11 +361,13 @@ j2k_status j2k_dwt_forward(j2k_ctx* ctx, int kernel, int order, const void* in, 
     if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
     return j2k_dwt_fwd_impl(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps,
                             ll0, ll1, j2k_dwt_tile{64, 64}, ctx->stream);
+    J2K_API_END
 }
 
 j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                            void* out, size_t out_pitch, size_t w, size_t h, int levels,
                            const float* steps) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     J2K_TRY(check_dwt_args(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels));
     if (kernel == J2K_W53 && steps)
@@ -359,6 +379,7 @@ j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, 
     if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
     return j2k_dwt_inv_impl(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps,
                             ll0, ll1, j2k_dwt_tile{64, 64}, ctx->stream);
+    J2K_API_END
 }
 
 }  // extern "C"
@@ -366,6 +387,7 @@ j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, 
 extern "C" j2k_status j2k_dwt_forward_batch(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                                             size_t in_stride, void* out, size_t out_pitch, size_t out_stride,
                                             int n, size_t w, size_t h, int levels, const float* steps) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     J2K_TRY(check_dwt_args(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels));
     if (n <= 0 || n > 65535 || in_stride < in_pitch * h || out_stride < out_pitch * h)
@@ -379,11 +401,13 @@ extern "C" j2k_status j2k_dwt_forward_batch(j2k_ctx* ctx, int kernel, int order,
     if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
     return j2k_dwt_fwd_impl(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps, ll0, ll1,
                             j2k_dwt_tile{64, 64}, ctx->stream, n, in_stride, out_stride);
+    J2K_API_END
 }
 
 extern "C" j2k_status j2k_dwt_inverse_batch(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                                             size_t in_stride, void* out, size_t out_pitch, size_t out_stride,
                                             int n, size_t w, size_t h, int levels, const float* steps) {
+    J2K_API_BEGIN
     if (!ctx) return J2K_ERR_INVALID_ARG;
     J2K_TRY(check_dwt_args(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels));
     if (n <= 0 || n > 65535 || in_stride < in_pitch * h || out_stride < out_pitch * h)
@@ -397,4 +421,5 @@ extern "C" j2k_status j2k_dwt_inverse_batch(j2k_ctx* ctx, int kernel, int order,
     if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
     return j2k_dwt_inv_impl(ctx, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps, ll0, ll1,
                             j2k_dwt_tile{64, 64}, ctx->stream, n, in_stride, out_stride);
+    J2K_API_END
 }

@@ -548,38 +548,47 @@ extern "C" {
 
 j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_t nrate, const float* sq_partials,
                                  size_t nsq, double inv_count, float lam, float* loss) {
+    J2K_API_BEGIN
     if (!ctx || !loss || (!rate_partials && nrate) || (!sq_partials && nsq)) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     rd_finalize_kernel<<<1, 1024, 0, ctx->stream>>>(rate_partials, nrate, sq_partials, nsq, inv_count, lam, loss);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_dwt97_band_sum(j2k_ctx* ctx, const float* partials, int n, int nb, int k, float* out) {
+    J2K_API_BEGIN
     if (!ctx || !partials || !out || n < 1 || nb < 1 || k < 1) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     band_sum_kernel<<<(unsigned)nb, 256, 0, ctx->stream>>>(partials, n, nb, k, out);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_dwt97_forward_adjoint(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, size_t w, size_t h,
                                      int levels) {
+    J2K_API_BEGIN
     J2K_TRY(check_common(ctx, g_coef, g_img, n, w, h, levels));
     return fwd_adj_run(ctx, g_coef, g_img, n, w, h, levels, nullptr);
+    J2K_API_END
 }
 
 j2k_status j2k_dwt97_forward_adjoint_residual(j2k_ctx* ctx, const float* g_coef, const float* sub,
                                               const float* scale, float alpha, float* g_img, int n, size_t w,
                                               size_t h, int levels) {
+    J2K_API_BEGIN
     J2K_TRY(check_common(ctx, g_coef, g_img, n, w, h, levels));
     if (!sub) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "forward adjoint residual: sub is NULL");
     const SynExtra ex{sub, w, w * h, scale, alpha, nullptr};
     return fwd_adj_run(ctx, g_coef, g_img, n, w, h, levels, &ex);
+    J2K_API_END
 }
 
 j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_coef, int n, size_t w, size_t h,
                                      int levels) {
+    J2K_API_BEGIN
     J2K_TRY(check_common(ctx, g_img, g_coef, n, w, h, levels));
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
@@ -622,6 +631,7 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
         iz = llz;
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 size_t j2k_dwt97_residual_partials(size_t w, size_t h, int n) {
@@ -630,6 +640,7 @@ size_t j2k_dwt97_residual_partials(size_t w, size_t h, int n) {
 
 j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float* x, float* d, int n, size_t w,
                                       size_t h, int levels, float* sq_partials) {
+    J2K_API_BEGIN
     J2K_TRY(check_common(ctx, y, d, n, w, h, levels));
     if (!x || !sq_partials) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "inverse residual: NULL x or partials");
     cudaSetDevice(ctx->device);
@@ -670,36 +681,45 @@ j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float*
                                                                      ZStride{plane, plane, llz}, vec, ex);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_relaxed_quant_forward(j2k_ctx* ctx, const float* y, float* y_hat, int n, size_t w, size_t h,
                                      int levels, const float* log_steps, uint64_t seed, float* rate_partials,
                                      int parts_per_band) {
+    J2K_API_BEGIN
     return quant_run(ctx, false, y, nullptr, y_hat, n, w, h, levels, log_steps, seed, 0.0f, nullptr, 1.0f,
                      rate_partials, parts_per_band, nullptr);
+    J2K_API_END
 }
 
 j2k_status j2k_relaxed_quant_forward_noise(j2k_ctx* ctx, const float* y, float* y_hat, float* noise, int n, size_t w,
                                            size_t h, int levels, const float* log_steps, uint64_t seed,
                                            float* rate_partials, int parts_per_band) {
+    J2K_API_BEGIN
     if (!noise) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "relaxed quantiser: noise buffer is NULL");
     return quant_run(ctx, false, y, nullptr, y_hat, n, w, h, levels, log_steps, seed, 0.0f, nullptr, 1.0f,
                      rate_partials, parts_per_band, noise);
+    J2K_API_END
 }
 
 j2k_status j2k_relaxed_quant_backward(j2k_ctx* ctx, const float* y, const float* g_yhat, float* g_y, int n,
                                       size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
                                       float lam, float* g_logstep_partials, int parts_per_band) {
+    J2K_API_BEGIN
     return quant_run(ctx, true, y, g_yhat, g_y, n, w, h, levels, log_steps, seed, lam, nullptr, 1.0f,
                      g_logstep_partials, parts_per_band, nullptr);
+    J2K_API_END
 }
 
 j2k_status j2k_relaxed_quant_backward_scaled(j2k_ctx* ctx, const float* y, const float* g_in, float* g_y, int n,
                                              size_t w, size_t h, int levels, const float* log_steps, uint64_t seed,
                                              const float* noise, float lam, const float* scale, float alpha,
                                              float* g_logstep_partials, int parts_per_band) {
+    J2K_API_BEGIN
     return quant_run(ctx, true, y, g_in, g_y, n, w, h, levels, log_steps, seed, lam, scale, alpha,
                      g_logstep_partials, parts_per_band, const_cast<float*>(noise));
+    J2K_API_END
 }
 
 }  // extern "C"

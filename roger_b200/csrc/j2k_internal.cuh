@@ -3,10 +3,50 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <exception>
+#include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "j2k_b200.h"
+
+// Every entry point of the C ABI runs its body between J2K_API_BEGIN and J2K_API_END, so that no
+// C++ exception crosses the ABI: a failed host allocation returns J2K_ERR_OUT_OF_MEMORY, any
+// other exception J2K_ERR_HOST.
+#define J2K_API_BEGIN try {
+#define J2K_API_END                          \
+    }                                        \
+    catch (const std::bad_alloc&) {          \
+        return J2K_ERR_OUT_OF_MEMORY;        \
+    }                                        \
+    catch (...) {                            \
+        return J2K_ERR_HOST;                 \
+    }
+
+// Runs fn(t) for t in [0, nt): t = 0 and every t whose host thread cannot be started run on the
+// calling thread, the rest on their own threads.  Every started thread is joined before this
+// returns, also when fn throws on the calling thread (the exception is then rethrown).  fn must
+// not throw on the other threads.
+template <class F>
+void j2k_run_threads(int nt, F fn) {
+    std::vector<std::thread> pool;
+    std::exception_ptr err;
+    int t = 1;
+    try {
+        pool.reserve(nt > 1 ? (size_t)nt - 1 : 0);
+        for (; t < nt; ++t) pool.emplace_back(fn, t);
+    } catch (...) {  // no more threads: the remaining shares run here
+    }
+    try {
+        fn(0);
+        for (; t < nt; ++t) fn(t);
+    } catch (...) {
+        err = std::current_exception();
+    }
+    for (auto& th : pool) th.join();
+    if (err) std::rethrow_exception(err);
+}
 
 // Device error word values (written by kernels, read back by the host; kernels never trap).
 enum : uint32_t {
@@ -162,8 +202,8 @@ double j2k_band_gain(int kernel, int levels, int band);
 // weight w = band gain (* step^2 when lossy)), picks npasses in {0, 1, 4, ..., 3nb-2} and the
 // kept length so that the total kept bytes stay within budget and the weighted distortion is
 // as low as the convex hulls allow.  Writes descs[i].npasses and descs[i].length.
-extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
-                                  const double* weight, size_t budget);
+extern "C" j2k_status j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes,
+                                        const double* dist, const double* weight, size_t budget);
 // The same choice split in three, for callers that try several budgets on one set of blocks:
 // build() makes every block's lower convex hull (the budget plays no part), threshold(budget)
 // finds the slope below which hull segments are dropped, cut(thr) writes each block's kept

@@ -45,6 +45,7 @@ j2k_status scratch_address(int device, void** out) {
 extern "C" j2k_status j2k_dwt_forward_noalloc(void* cuda_stream, int kernel, int order, const void* in,
                                               size_t in_pitch, void* out, size_t out_pitch, size_t w,
                                               size_t h, int levels, const float* steps) {
+    J2K_API_BEGIN
     if (!in || !out || w == 0 || h == 0 || in_pitch < w || out_pitch < w) return J2K_ERR_INVALID_ARG;
     if (kernel != J2K_W53 && kernel != J2K_W97) return J2K_ERR_INVALID_ARG;
     if (order != J2K_ORDER_T800 && order != J2K_ORDER_REF) return J2K_ERR_INVALID_ARG;
@@ -64,4 +65,5 @@ extern "C" j2k_status j2k_dwt_forward_noalloc(void* cuda_stream, int kernel, int
     if (((need0 * 4 + 255) & ~(size_t)255) / 4 + need1 > kNoallocElems) ll1 = (char*)base + need0 * 4;
     return j2k_dwt_fwd_impl(nullptr, kernel, order, in, in_pitch, out, out_pitch, w, h, levels, steps, ll0, ll1,
                             j2k_dwt_tile{64, 64}, (cudaStream_t)cuda_stream);
+    J2K_API_END
 }

@@ -154,16 +154,8 @@ void j2k_pcrd_hulls::build(const j2k_cb_desc* descs, size_t nblocks, const uint3
         }
         part_base[t] = sb, part_all[t] = sa, part_ns[t] = ns;
     };
-    if (nt <= 1) {
-        hulls(0, 0, n);
-    } else {
-        std::vector<std::thread> pool;
-        const size_t per = (n + nt - 1) / nt;
-        for (size_t t = 1; t < nt; ++t)
-            pool.emplace_back(hulls, t, std::min(n, t * per), std::min(n, (t + 1) * per));
-        hulls(0, 0, std::min(n, per));
-        for (auto& th : pool) th.join();
-    }
+    const size_t per = (n + nt - 1) / nt;
+    j2k_run_threads((int)nt, [&](int t) { hulls(t, std::min(n, t * per), std::min(n, (t + 1) * per)); });
     // byte counts are whole numbers, so these sums are exact in any order
     base = all = 0.0;
     nseg = 0;
@@ -254,8 +246,10 @@ void j2k_pcrd_hulls::cut(double thr, int32_t* npasses, int32_t* length) const {
     }
 }
 
-extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes, const double* dist,
-                                  const double* weight, size_t budget) {
+extern "C" j2k_status j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* plane_bytes,
+                                        const double* dist, const double* weight, size_t budget) {
+    J2K_API_BEGIN
+    if (n && (!descs || !plane_bytes || !dist || !weight)) return J2K_ERR_INVALID_ARG;
     static thread_local j2k_pcrd_hulls hulls;  // scratch kept per thread between calls
     static thread_local std::vector<int32_t> np, len;
     j2k_pcrd_hulls& h = hulls;
@@ -265,4 +259,6 @@ extern "C" void j2k_pcrd_truncate(j2k_cb_desc* descs, size_t n, const uint32_t* 
     len.resize(n);
     h.cut(thr, np.data(), len.data());
     for (size_t i = 0; i < n; ++i) descs[i].npasses = (uint8_t)np[i], descs[i].length = len[i];
+    return J2K_OK;
+    J2K_API_END
 }

@@ -391,12 +391,11 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
     DecSmem S;
     for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
     for (int k = 0; k < 19; ++k) S.st[k] = 0;
-    static DecTables T;
-    static bool built = false;
-    if (!built) {
-        for (int i = 0; i < 4 * 512; ++i) fill_tables_entry(T, i);
-        built = true;
-    }
+    static const DecTables T = [] {  // built once, thread-safely
+        DecTables t{};
+        for (int i = 0; i < 4 * 512; ++i) fill_tables_entry(t, i);
+        return t;
+    }();
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x) out[(size_t)y * pitch + x] = 0;
     if (numbps > 0 && npasses > 0) decode_block(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);

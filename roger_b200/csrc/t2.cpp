@@ -287,7 +287,7 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
                 bw.bit(1);
                 for (int q = 0; q < bcount; ++q) {
                     int b = b0 + q;
-                    if (!(ncbx[b] * ncby[b])) continue;
+                    if (ncbx[b] == 0 || ncby[b] == 0) continue;
                     size_t f = first[(size_t)c * nb + b];
                     TagTree& ti = incl[(size_t)c * nb + b];
                     TagTree& tz = zbp[(size_t)c * nb + b];
@@ -435,6 +435,7 @@ struct TagTreeDec {
     }
     // value of leaf (x, y) if it is below `threshold`, else `threshold`
     int decode(BitReader& br, int x, int y, int threshold) {
+        const int leaf = y * lw[0] + x;  // level 0 starts at offset 0
         int path[40];
         for (int l = 0; l < nlev; ++l) {
             path[l] = off[l] + y * lw[l] + x;
@@ -455,7 +456,6 @@ struct TagTreeDec {
             }
             lo = low[q];
         }
-        const int leaf = path[0];
         return (known[leaf] && val[leaf] < threshold) ? val[leaf] : threshold;
     }
 };
@@ -477,6 +477,7 @@ extern "C" j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, in
                                            size_t count, const uint8_t* bytes, size_t nbytes, int layers,
                                            const int32_t* layer_npasses, const int32_t* layer_lengths, uint8_t* out,
                                            size_t cap, size_t* len) {
+    J2K_API_BEGIN
     if (!len || (!descs && count) || (!bytes && nbytes)) return J2K_ERR_INVALID_ARG;
     auto pow2 = [](int v) { return v >= 4 && v <= 64 && (v & (v - 1)) == 0; };
     if (w == 0 || h == 0 || w > 65535 || h > 65535 || (ncomp != 1 && ncomp != 3) || levels < 0 || levels > 32 ||
@@ -526,6 +527,7 @@ extern "C" j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, in
     if (cap < o.v.size()) return J2K_ERR_CAPACITY;
     std::memcpy(out, o.v.data(), o.v.size());
     return J2K_OK;
+    J2K_API_END
 }
 
 namespace {
@@ -803,6 +805,7 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
 extern "C" j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
                                                  j2k_cb_desc* descs, size_t* count, uint8_t* bytes, size_t cap,
                                                  size_t* used, char* err, size_t errlen) {
+    J2K_API_BEGIN
     if (!cs || !info || !count || !used || max_layers < 0) return J2K_ERR_INVALID_ARG;
     std::vector<j2k_cb_desc> d;
     std::vector<std::vector<std::pair<uint32_t, int>>> segs;
@@ -832,6 +835,7 @@ extern "C" j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, in
         descs[i] = d[i];
     }
     return J2K_OK;
+    J2K_API_END
 }
 
 j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
@@ -856,6 +860,7 @@ j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_
 
 extern "C" j2k_status j2k_codestream_info(const uint8_t* cs, size_t n, j2k_stream_info* info, char* err,
                                           size_t errlen) {
+    J2K_API_BEGIN
     if (!cs || !info) return J2K_ERR_INVALID_ARG;
     std::string msg;
     j2k_status s = t2_read(cs, n, 0, info, nullptr, nullptr, nullptr, &msg, true);
@@ -864,10 +869,13 @@ extern "C" j2k_status j2k_codestream_info(const uint8_t* cs, size_t n, j2k_strea
         err[errlen - 1] = 0;
     }
     return s;
+    J2K_API_END
 }
 
 extern "C" j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
                                           size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
                                           size_t errlen) {
+    J2K_API_BEGIN
     return j2k_codestream_read_layers(cs, n, 0, info, descs, count, bytes, cap, used, err, errlen);
+    J2K_API_END
 }

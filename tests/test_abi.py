@@ -36,6 +36,27 @@ def test_version_and_status_strings():
     L = _lib.lib()
     assert L.j2k_version() >= 1
     assert L.j2k_status_string(-5) == b"output capacity exceeded"
+    # the Python table of statuses says what the library says
+    for code, text in _lib.STATUS.items():
+        assert L.j2k_status_string(code).decode() == text, code
+    assert L.j2k_status_string(-99) == b"unknown status"
+
+
+def test_every_status_entry_point_is_guarded():
+    """No C++ exception crosses the C ABI: every j2k_status function the public header declares
+    runs its body between J2K_API_BEGIN and J2K_API_END (one-line bodies aside)."""
+    import glob
+    names = set(re.findall(r"j2k_status\s+(j2k_\w+)\s*\(", open(os.path.join(ROOT, "include", "j2k_b200.h")).read()))
+    found = {}
+    for f in glob.glob(os.path.join(ROOT, "roger_b200", "csrc", "*.c[up]*")):
+        src = open(f).read()
+        for m in re.finditer(r'^(?:extern "C" )?j2k_status (j2k_\w+)\([^{;]*\{(.*?)^\}', src, re.M | re.S):
+            if m.group(1) in names:
+                found[m.group(1)] = m.group(2)
+    assert names == set(found), sorted(names ^ set(found))
+    for name, body in found.items():
+        lines = [l for l in body.strip().splitlines() if l.strip()]
+        assert lines[0].strip() == "J2K_API_BEGIN" and lines[-1].strip() == "J2K_API_END", name
 
 
 @pytest.mark.parametrize("w,h,L,cb", [(512, 512, 5, 64), (4096, 4096, 6, 64), (33, 17, 2, 32),

@@ -148,7 +148,7 @@ def test_pcrd_selection_matches_sorted_threshold(seed, n):
     from roger_b200 import _lib
     f = C.CDLL(_lib.LIB_PATH).j2k_pcrd_truncate
     f.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
-    f.restype = None
+    f.restype = C.c_int
     rng = np.random.default_rng(seed)
     desc = np.zeros(n, _lib.CB_DESC)
     pb = np.zeros((n, 32), np.uint32)
@@ -173,7 +173,7 @@ def test_pcrd_selection_matches_sorted_threshold(seed, n):
     for frac in (0.0, 0.05, 0.3, 0.8, 1.2):
         budget = int(full * frac)
         d2 = desc.copy()
-        f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget)
+        assert f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget) == 0
         ref = _pcrd_reference(desc, pb, dist, w, budget)
         assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == ref
         assert int(d2["length"].sum()) <= min(budget, full)
@@ -186,7 +186,7 @@ def test_pcrd_ties_drop_together():
     from roger_b200 import _lib
     f = C.CDLL(_lib.LIB_PATH).j2k_pcrd_truncate
     f.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
-    f.restype = None
+    f.restype = C.c_int
     n = 5000
     desc = np.zeros(n, _lib.CB_DESC)
     pb = np.zeros((n, 32), np.uint32)
@@ -206,7 +206,7 @@ def test_pcrd_ties_drop_together():
     for frac in (0.01, 0.1, 0.25, 0.5, 0.75, 0.99):
         budget = int(full * frac)
         d2 = desc.copy()
-        f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget)
+        assert f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget) == 0
         ref = _pcrd_reference(desc, pb, dist, w, budget)
         assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == ref
         assert int(d2["length"].sum()) <= budget
