@@ -2,6 +2,7 @@
 // One tile, one quality layer, LRCP progression, one precinct per resolution, code-blocks of
 // one codeword segment each (all passes included).  The reference has no tier-2 at all.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -269,58 +270,94 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
             zbp.emplace_back(std::max(ncbx[b], 1), std::max(ncby[b], 1), lz);
         }
     std::vector<int> lblock(nblk, 3);
-    for (int l = 0; l < nlayers; ++l)
-        for (int r = 0; r <= levels; ++r)
-            for (int c = 0; c < ncomp; ++c) {
-                int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
-                int bcount = r == 0 ? 1 : 3;
-                bool any = false;
-                for (int q = 0; q < bcount; ++q)
-                    for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
-                        any |= NP(l, i) > NP(l - 1, i);
-                BitWriter bw(o);
-                if (!any) {
-                    bw.bit(0);
-                    bw.flush();
-                    continue;
+    // packet (layer l, resolution r, component c): its header, then (with bodies) its codeword
+    // segments.  Within a layer the packets touch disjoint bands, tag trees and blocks.
+    auto packet = [&](Bytes& out, int l, int r, int c) {
+        int b0 = r == 0 ? 0 : 1 + 3 * (r - 1);  // resolution r holds level L-r+1
+        int bcount = r == 0 ? 1 : 3;
+        bool any = false;
+        for (int q = 0; q < bcount; ++q)
+            for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
+                any |= NP(l, i) > NP(l - 1, i);
+        BitWriter bw(out);
+        if (!any) {
+            bw.bit(0);
+            bw.flush();
+            return;
+        }
+        bw.bit(1);
+        for (int q = 0; q < bcount; ++q) {
+            int b = b0 + q;
+            if (ncbx[b] == 0 || ncby[b] == 0) continue;
+            size_t f = first[(size_t)c * nb + b];
+            TagTree& ti = incl[(size_t)c * nb + b];
+            TagTree& tz = zbp[(size_t)c * nb + b];
+            for (int j = 0; j < ncby[b]; ++j)
+                for (int i = 0; i < ncbx[b]; ++i) {
+                    const size_t k = f + (size_t)j * ncbx[b] + i;
+                    const int prev = NP(l - 1, k), cur = NP(l, k);
+                    if (prev == 0) {  // not included before: inclusion tag tree up to layer l
+                        ti.encode(bw, i, j, l + 1);
+                        if (cur == 0) continue;
+                        tz.encode(bw, i, j, 0x7FFFFFF);
+                    } else {
+                        bw.bit(cur > prev);
+                        if (cur == prev) continue;
+                    }
+                    const int newp = cur - prev;
+                    const int seg = LEN(l, k) - LEN(l - 1, k);
+                    put_npasses(bw, newp);
+                    int bits = floorlog2(seg) + 1;
+                    int avail = lblock[k] + floorlog2(newp);
+                    int inc = bits > avail ? bits - avail : 0;
+                    bw.bits(((1u << inc) - 1) << 1, inc + 1);  // inc ones, then a zero
+                    lblock[k] += inc;
+                    bw.bits((uint32_t)seg, lblock[k] + floorlog2(newp));
                 }
-                bw.bit(1);
-                for (int q = 0; q < bcount; ++q) {
-                    int b = b0 + q;
-                    if (ncbx[b] == 0 || ncby[b] == 0) continue;
-                    size_t f = first[(size_t)c * nb + b];
-                    TagTree& ti = incl[(size_t)c * nb + b];
-                    TagTree& tz = zbp[(size_t)c * nb + b];
-                    for (int j = 0; j < ncby[b]; ++j)
-                        for (int i = 0; i < ncbx[b]; ++i) {
-                            const size_t k = f + (size_t)j * ncbx[b] + i;
-                            const int prev = NP(l - 1, k), cur = NP(l, k);
-                            if (prev == 0) {  // not included before: inclusion tag tree up to layer l
-                                ti.encode(bw, i, j, l + 1);
-                                if (cur == 0) continue;
-                                tz.encode(bw, i, j, 0x7FFFFFF);
-                            } else {
-                                bw.bit(cur > prev);
-                                if (cur == prev) continue;
-                            }
-                            const int newp = cur - prev;
-                            const int seg = LEN(l, k) - LEN(l - 1, k);
-                            put_npasses(bw, newp);
-                            int bits = floorlog2(seg) + 1;
-                            int avail = lblock[k] + floorlog2(newp);
-                            int inc = bits > avail ? bits - avail : 0;
-                            bw.bits(((1u << inc) - 1) << 1, inc + 1);  // inc ones, then a zero
-                            lblock[k] += inc;
-                            bw.bits((uint32_t)seg, lblock[k] + floorlog2(newp));
-                        }
+        }
+        bw.flush();
+        if (bodies)
+            for (int q = 0; q < bcount; ++q)
+                for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
+                    if (NP(l, i) > NP(l - 1, i))
+                        out.v.insert(out.v.end(), blocks[i].data + LEN(l - 1, i), blocks[i].data + LEN(l, i));
+    };
+    // many blocks: a layer's packets on host threads (largest first, taken from a shared
+    // counter) into their own buffers, appended in LRCP order
+    const int npk = (levels + 1) * ncomp;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = nblk < 4096 ? 1 : (int)std::min<unsigned>(std::min(16u, hw), (unsigned)npk);
+    std::vector<Bytes> pk(nt > 1 ? npk : 0);
+    std::vector<int> order(npk);
+    for (int i = 0; i < npk; ++i) order[i] = i;
+    auto blocks_of = [&](int i) {  // packet i = r * ncomp + c
+        const int r = i / ncomp, c = i % ncomp;
+        const int b0 = r == 0 ? 0 : 1 + 3 * (r - 1), bcount = r == 0 ? 1 : 3;
+        return first[(size_t)c * nb + b0 + bcount] - first[(size_t)c * nb + b0];
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return blocks_of(a) > blocks_of(b); });
+    for (int l = 0; l < nlayers; ++l) {
+        if (nt <= 1) {
+            for (int r = 0; r <= levels; ++r)
+                for (int c = 0; c < ncomp; ++c) packet(o, l, r, c);
+            continue;
+        }
+        std::atomic<int> next{0};
+        std::atomic<bool> failed{false};
+        j2k_run_threads(nt, [&](int) {
+            for (int i; (i = next.fetch_add(1)) < npk;) {
+                const int p = order[i];
+                pk[p].v.clear();
+                try {
+                    packet(pk[p], l, p / ncomp, p % ncomp);
+                } catch (...) {  // a host allocation failed: reported after the join
+                    failed = true;
                 }
-                bw.flush();
-                if (bodies)
-                    for (int q = 0; q < bcount; ++q)
-                        for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
-                            if (NP(l, i) > NP(l - 1, i))
-                                o.v.insert(o.v.end(), blocks[i].data + LEN(l - 1, i), blocks[i].data + LEN(l, i));
             }
+        });
+        if (failed) throw std::bad_alloc();
+        for (int p = 0; p < npk; ++p) o.v.insert(o.v.end(), pk[p].v.begin(), pk[p].v.end());
+    }
     const size_t extra = bodies ? 0 : body;
     uint32_t psot = (uint32_t)(o.v.size() + extra - sot);
     o.v[sot + 6] = (uint8_t)(psot >> 24);

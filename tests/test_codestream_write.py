@@ -46,7 +46,10 @@ def _blocks(img, levels, cb):
     return np.array(descs, L.CB_DESC), np.frombuffer(b"".join(datas), np.uint8), infos, coefs
 
 
-CASES = [(96, 80, 3, 3, 32), (131, 97, 1, 4, 64), (200, 64, 3, 5, 64)]
+# the last two have 4096 code-blocks or more, so the writer builds each layer's packets on host
+# threads
+CASES = [(96, 80, 3, 3, 32), (131, 97, 1, 4, 64), (200, 64, 3, 5, 64), (512, 512, 1, 5, 8),
+         (384, 384, 3, 4, 8)]
 
 
 @pytest.mark.parametrize("w,h,nc,lv,cb", CASES)
