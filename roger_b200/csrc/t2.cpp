@@ -623,8 +623,10 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
                 layers = (int)c.u16();
                 mct = (int)c.u8();
                 levels = (int)c.u8();
-                cbw = 1 << ((int)c.u8() + 2);
-                cbh = 1 << ((int)c.u8() + 2);
+                const int xcb = (int)c.u8(), ycb = (int)c.u8();  // exponents - 2 (A.6.1)
+                if (xcb > 8 || ycb > 8) throw ReadErr{J2K_ERR_INVALID_ARG, "code-block size exponent"};
+                cbw = 1 << (xcb + 2);
+                cbh = 1 << (ycb + 2);
                 sty = (int)c.u8();
                 xform = (int)c.u8();
                 if (scod & 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "user-defined precincts"};

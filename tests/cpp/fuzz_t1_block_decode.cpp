@@ -1,0 +1,42 @@
+// Random-input fuzzer for the tier-1 block decoder, through its host entry point
+// j2k_t1_decode_block_host, which runs the same __host__ __device__ decode_block as the device
+// kernel.  Built with AddressSanitizer and UBSan together with t1dec.cu itself.  Each block gets
+// a random size (1..64 a side, at most 4096 samples), orientation, bit-plane count, a pass count
+// the kernel's descriptor check admits (0..3*numbps) and a codeword of random, all-0xFF or
+// sparse bytes held in a buffer of exactly its length, so that any read past the codeword's end
+// is a sanitizer report.  Prints "decoded N" and exits 0.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <vector>
+
+extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
+                                        int cw, int ch, int32_t* out, size_t pitch);
+
+int main(int argc, char** argv) {
+    const int iters = argc > 1 ? std::atoi(argv[1]) : 1000;
+    std::mt19937_64 rng(12345);
+    const int sizes[] = {4, 8, 16, 32, 64};
+    int decoded = 0;
+    for (int it = 0; it < iters; ++it) {
+        const int cw = (rng() % 3 == 0) ? 1 + (int)(rng() % 64) : sizes[rng() % 5];
+        const int ch = (rng() % 3 == 0) ? 1 + (int)(rng() % 64) : sizes[rng() % 5];
+        if (cw * ch > 4096) continue;
+        const int numbps = (int)(rng() % 32);
+        const int npasses = numbps ? (int)(rng() % (3 * numbps + 1)) : 0;
+        const int len = (rng() % 4 == 0) ? (int)(rng() % 8) : (int)(rng() % 6000);
+        std::vector<uint8_t> data(len);
+        const int mode = (int)(rng() % 3);
+        for (auto& b : data) b = mode == 0 ? (uint8_t)rng() : mode == 1 ? 0xFF : (uint8_t)(rng() & 0x8F);
+        std::vector<int32_t> out((size_t)ch * cw);
+        if (j2k_t1_decode_block_host(len ? data.data() : nullptr, len, numbps, npasses, (int)(rng() % 4), cw, ch,
+                                     out.data(), (size_t)cw) != 0) {
+            std::printf("refused block %d\n", it);
+            return 1;
+        }
+        ++decoded;
+    }
+    std::printf("decoded %d\n", decoded);
+    return 0;
+}
