@@ -1140,6 +1140,10 @@ long or_encode_image(const uint8_t* img, size_t w, size_t h, int ncomp, const or
             int e2 = ex - 1;                  /* step = 2^e2 * (1 + mu/2048) */
             eps[b] = Rb - e2;
             mant[b] = (int)lrintf((fr * 2.0f - 1.0f) * 2048.0f);
+            if (mant[b] == 2048) { /* the 11-bit mantissa rounded up: next power of two */
+                mant[b] = 0;
+                eps[b] -= 1;
+            }
         }
         int need = maxbps[b] - eps[b] + 1;
         if (need > G) G = need;

@@ -377,8 +377,15 @@ j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, 
             std::vector<j2k_band_rect> r(3 * d.levels + 1);
             j2k_band_rects(d.w, d.h, d.levels, r.data());
             im.steps.resize(r.size());
-            for (size_t q = 0; q < r.size(); ++q)
+            for (size_t q = 0; q < r.size(); ++q) {
                 im.steps[q] = d.steps ? d.steps[q] : 8.0f * std::ldexp(1.0f, -r[q].level);
+                int ex, mt;
+                if (!j2k_qcd_step(im.steps[q], (int)q, &ex, &mt)) {
+                    delete b;
+                    return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "batch image " + std::to_string(i) +
+                                                                   ": a quantiser step is not positive or out of the QCD range");
+                }
+            }
         }
         im.d.steps = nullptr;
         b->img.push_back(im);

@@ -471,8 +471,12 @@ static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const
     if (e->lossy) {
         if (p && p->steps) e->steps.assign(p->steps, p->steps + 3 * levels + 1);
         else e->steps = default_steps(w, h, levels);
-        for (float s : e->steps)
-            if (!(s > 0.0f)) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "quantiser steps must be > 0");
+        for (int b = 0; b < (int)e->steps.size(); ++b) {
+            int ex, mt;
+            if (!j2k_qcd_step(e->steps[b], b, &ex, &mt))
+                return j2k_fail(ctx, J2K_ERR_INVALID_ARG,
+                                "quantiser step " + std::to_string(b) + " is not positive or out of the QCD range");
+        }
     } else {
         e->steps.clear();
     }

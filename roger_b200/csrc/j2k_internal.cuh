@@ -230,6 +230,13 @@ j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
                               cudaStream_t st);
 
+// Expounded quantisation (T.800 A.6.4, E.1.1) for 8-bit samples: step = 2^(Rb - eps) *
+// (1 + mant / 2^11), Rb = 8 + the gain of QCD band `band` (0 for LL, 1 for HL and LH, 2 for HH).
+// Writes the 5-bit exponent and the 11-bit mantissa of `step`, the mantissa rounded to nearest (a
+// carry out of it moves to the exponent); false when the step is not a positive finite number or
+// its exponent falls outside 0..31.
+bool j2k_qcd_step(float step, int band, int* eps, int* mant);
+
 // host tier-2 writer
 struct j2k_t2_block {
     int numbps, npasses, length;

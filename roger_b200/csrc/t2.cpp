@@ -149,6 +149,23 @@ void put_npasses(BitWriter& bw, int n) {  // Table B.4
 
 namespace {
 
+bool j2k_qcd_step_impl(float step, int band, int* eps, int* mant) {
+    if (!(step > 0.0f) || !std::isfinite(step)) return false;
+    const int gain = band == 0 ? 0 : ((band - 1) % 3 == 2 ? 2 : 1);
+    int ex;
+    const float fr = std::frexp(step, &ex);  // step = fr * 2^ex, fr in [0.5, 1)
+    int e = 8 + gain - (ex - 1);
+    int m = (int)std::lrint((fr * 2.0f - 1.0f) * 2048.0f);
+    if (m == 2048) {  // rounded up to the next power of two
+        m = 0;
+        e -= 1;
+    }
+    if (e < 0 || e > 31) return false;
+    *eps = e;
+    *mant = m;
+    return true;
+}
+
 // Writes the codestream into `o`; without bodies only the markers and packet headers are
 // written and the returned size still counts every block's codeword bytes.  nlayers quality
 // layers: after layer l block i has cum_np[l * n + i] passes and cum_len[l * n + i] bytes of its
@@ -198,11 +215,9 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
         if (lossless) {
             eps[b] = Rb + (mct ? 1 : 0);
             mant[b] = 0;
-        } else {
-            int ex;
-            float fr = std::frexp(steps[b], &ex);
-            eps[b] = Rb - (ex - 1);
-            mant[b] = (int)std::lrint((fr * 2.0f - 1.0f) * 2048.0f);
+        } else if (!j2k_qcd_step(steps[b], b, &eps[b], &mant[b])) {  // callers refuse such steps
+            eps[b] = 31;
+            mant[b] = 0;
         }
         G = std::max(G, maxbps[b] - eps[b] + 1);
     }
@@ -369,6 +384,8 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
 }
 
 }  // namespace
+
+bool j2k_qcd_step(float step, int band, int* eps, int* mant) { return j2k_qcd_step_impl(step, band, eps, mant); }
 
 // blocks: component-major, then subbands in QCD order, then raster order within each subband
 // (exactly the order of j2k_build_jobs).
@@ -553,8 +570,10 @@ extern "C" j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, in
             st.resize(nb);
             for (int b = 0; b < nb; ++b) st[b] = 8.0f * std::ldexp(1.0f, -r[b].level);
         }
-        for (float v : st)
-            if (!(v > 0.0f)) return J2K_ERR_INVALID_ARG;
+        for (int b = 0; b < (int)st.size(); ++b) {
+            int e, m;
+            if (!j2k_qcd_step(st[b], b, &e, &m)) return J2K_ERR_INVALID_ARG;
+        }
     }
     Bytes o;
     t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless ? 1 : 0, ncomp == 3, lossless ? nullptr : st.data(), blocks,

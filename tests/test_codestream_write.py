@@ -139,3 +139,35 @@ def test_bad_arguments_are_refused():
     npl, lnl = _layers(descs, infos, [lambda nb: nb // 2, lambda nb: 0])
     with pytest.raises(J2KError):  # layers that shrink
         C.write_codestream(64, 48, 1, 2, descs, data, 32, 32, layers=(npl, lnl))
+
+
+def test_quantiser_steps_round_trip_through_qcd():
+    """Expounded steps: 5-bit exponent, 11-bit mantissa.  A step just below a power of two rounds
+    up to it (the mantissa's carry goes to the exponent); every step comes back from the QCD
+    within half a mantissa unit, and steps the QCD cannot hold are refused."""
+    import math
+    w = h = 64
+    lv = 2
+    n = int(L.lib().j2k_codeblock_count(w, h, lv, 32, 32))
+    descs = np.zeros(n, L.CB_DESC)  # empty blocks: only the main header matters here
+    data = np.zeros(1, np.uint8)
+    steps = np.array([0.99999, 1.9999, 0.5, 3.0e-4, 7.5, 0.7, 100.0], np.float32)
+    cs = C.write_codestream(w, h, 1, lv, descs, data, 32, 32, lossless=False, steps=steps)
+    back = C.read_codestream(cs)[0]["steps"]
+    for want, got in zip(steps, back):
+        assert abs(float(got) - float(want)) <= float(want) * 2.0 ** -11, (want, got)
+    assert float(back[0]) == 1.0 and float(back[1]) == 2.0  # carried into the exponent
+    for bad in (0.0, -1.0, float("nan"), float("inf"), 1.0e-9, 1.0e6):
+        st = steps.copy()
+        st[3] = bad
+        with pytest.raises(J2KError):
+            C.write_codestream(w, h, 1, lv, descs, data, 32, 32, lossless=False, steps=st)
+    # the oracle's writer encodes the same steps identically (the QCD's SPqcd fields; the guard
+    # bits before them depend on the blocks)
+    def spqcd(stream):
+        i = stream.find(b"\xff\x5c")
+        return stream[i + 5:i + 2 + int.from_bytes(stream[i + 2:i + 4], "big")]
+    img = synth.gray(w, h, 3)
+    assert spqcd(bytes(O.encode_image(img, lv, 32, 32, False, steps=steps))) == spqcd(cs)
+    assert len(spqcd(cs)) == 2 * steps.size
+
