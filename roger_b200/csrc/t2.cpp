@@ -575,6 +575,19 @@ extern "C" j2k_status j2k_codestream_write(uint32_t w, uint32_t h, int ncomp, in
             if (!j2k_qcd_step(st[b], b, &e, &m)) return J2K_ERR_INVALID_ARG;
         }
     }
+    // a block's bit-planes must fit its band's exponent and at most 7 guard bits (the zero
+    // bit-plane count Mb - numbps is not negative, Mb = guard + eps - 1)
+    {
+        std::vector<j2k_cb_job> jobs;
+        for (int c = 0; c < ncomp; ++c) j2k_build_jobs(w, h, levels, cbw, cbh, &jobs, c);
+        for (size_t i = 0; i < count; ++i) {
+            const int b = jobs[i].band;
+            const int gain = b == 0 ? 0 : ((b - 1) % 3 == 2 ? 2 : 1);
+            int e = 8 + gain + (ncomp == 3 ? 1 : 0), m;
+            if (!lossless) j2k_qcd_step(st[b], b, &e, &m);
+            if (descs[i].numbps > e + 6) return J2K_ERR_INVALID_ARG;
+        }
+    }
     Bytes o;
     t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless ? 1 : 0, ncomp == 3, lossless ? nullptr : st.data(), blocks,
             true, nl, layered ? layer_npasses : nullptr, layered ? layer_lengths : nullptr);

@@ -171,3 +171,18 @@ def test_quantiser_steps_round_trip_through_qcd():
     assert spqcd(bytes(O.encode_image(img, lv, 32, 32, False, steps=steps))) == spqcd(cs)
     assert len(spqcd(cs)) == 2 * steps.size
 
+
+def test_bit_planes_beyond_the_guard_bits_are_refused():
+    """A block may not have more magnitude bit-planes than its band's exponent plus 6 (7 guard
+    bits at most), or its zero bit-plane count would be negative."""
+    w = h = 64
+    lv = 2
+    n = int(L.lib().j2k_codeblock_count(w, h, lv, 32, 32))
+    descs = np.zeros(n, L.CB_DESC)
+    data = np.zeros(1, np.uint8)
+    descs[0]["numbps"] = 8 + 6  # LL band of a gray image: eps = 8
+    C.write_codestream(w, h, 1, lv, descs, data, 32, 32)
+    descs[0]["numbps"] = 8 + 7
+    with pytest.raises(J2KError):
+        C.write_codestream(w, h, 1, lv, descs, data, 32, 32)
+
