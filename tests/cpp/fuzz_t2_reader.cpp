@@ -3,8 +3,12 @@
 // on the command line is truncated or has bytes overwritten, set to 0xFF or deleted; every
 // mutant must be refused with a status or parse into descriptors whose codeword ranges lie
 // inside the returned bytes.  Headers that claim more than 2^20 code-blocks are only sized.
-// Prints "parsed P refused R huge H" and exits 0; a sanitizer report or a bad descriptor ends
-// it with a non-zero status.
+// Every parsed mutant is also written back as one layer by j2k_codestream_write (which may
+// refuse blocks the writer does not produce, e.g. a cut inside a bit-plane); a written stream
+// must read back to the same blocks and codeword bytes.
+// Prints "parsed P refused R huge H rewritten W" and exits 0; a sanitizer report, a bad
+// descriptor or a round trip that differs ends it with a non-zero status.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -21,7 +25,7 @@ int main(int argc, char** argv) {
         return 2;
     }
     const int iters = std::atoi(argv[1]);
-    size_t parsed = 0, refused = 0, huge = 0;
+    size_t parsed = 0, refused = 0, huge = 0, rewritten = 0;
     for (int s = 2; s < argc; ++s) {
         std::ifstream f(argv[s], std::ios::binary);
         const std::vector<uint8_t> cs((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
@@ -75,8 +79,43 @@ int main(int argc, char** argv) {
                     return 1;
                 }
             ++parsed;
+            // write the parsed blocks back (one layer) and read them again
+            size_t wl = 0;
+            const float* st = info.lossless ? nullptr : info.steps;
+            if (j2k_codestream_write(info.w, info.h, info.ncomp, info.levels, info.cbw, info.cbh, info.lossless, st,
+                                     d.data(), cnt, b.data(), used, 1, nullptr, nullptr, nullptr, 0, &wl) != J2K_OK)
+                continue;
+            std::vector<uint8_t> w2(wl);
+            if (j2k_codestream_write(info.w, info.h, info.ncomp, info.levels, info.cbw, info.cbh, info.lossless, st,
+                                     d.data(), cnt, b.data(), used, 1, nullptr, nullptr, w2.data(), w2.size(),
+                                     &wl) != J2K_OK) {
+                std::printf("second write of mutant %d of %s failed\n", it, argv[s]);
+                return 1;
+            }
+            j2k_stream_info i2;
+            size_t c2 = 0, u2 = 0;
+            if (j2k_codestream_read_layers(w2.data(), wl, 0, &i2, nullptr, &c2, nullptr, 0, &u2, err, sizeof err) !=
+                    J2K_OK || c2 != cnt || u2 != used) {
+                std::printf("written stream of mutant %d of %s does not read back: %s\n", it, argv[s], err);
+                return 1;
+            }
+            std::vector<j2k_cb_desc> d2(c2 + 1);
+            std::vector<uint8_t> b2(u2 + 1);
+            if (j2k_codestream_read_layers(w2.data(), wl, 0, &i2, d2.data(), &c2, b2.data(), b2.size(), &u2, err,
+                                           sizeof err) != J2K_OK) {
+                std::printf("written stream of mutant %d of %s does not read back: %s\n", it, argv[s], err);
+                return 1;
+            }
+            for (size_t i = 0; i < cnt; ++i)
+                if (d2[i].numbps != d[i].numbps || d2[i].npasses != d[i].npasses || d2[i].length != d[i].length ||
+                    !std::equal(b.begin() + d[i].offset, b.begin() + d[i].offset + d[i].length,
+                                b2.begin() + d2[i].offset)) {
+                    std::printf("block %zu of mutant %d of %s differs after the round trip\n", i, it, argv[s]);
+                    return 1;
+                }
+            ++rewritten;
         }
     }
-    std::printf("parsed %zu refused %zu huge %zu\n", parsed, refused, huge);
+    std::printf("parsed %zu refused %zu huge %zu rewritten %zu\n", parsed, refused, huge, rewritten);
     return 0;
 }

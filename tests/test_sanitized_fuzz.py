@@ -59,8 +59,8 @@ def test_t2_reader_under_sanitizers(tmp_path):
     exe = _link(tmp_path, "fuzz_t2_reader",
                 [os.path.join(ROOT, "tests", "cpp", "fuzz_t2_reader.cpp"), os.path.join(CSRC, "t2.cpp")])
     out = _run([exe, "3000"] + paths, env=ENV, timeout=600)
-    parsed, refused = int(out.split()[1]), int(out.split()[3])
-    assert parsed > 0 and refused > 0, out
+    parsed, refused, rewritten = int(out.split()[1]), int(out.split()[3]), int(out.split()[7])
+    assert parsed > 0 and refused > 0 and rewritten > 0, out
 
 
 def test_t1_block_decoder_under_sanitizers(tmp_path):
