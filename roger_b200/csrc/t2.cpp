@@ -294,12 +294,20 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
         for (int q = 0; q < bcount; ++q)
             for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
                 any |= NP(l, i) > NP(l - 1, i);
-        BitWriter bw(out);
         if (!any) {
+            BitWriter bw(out);
             bw.bit(0);
             bw.flush();
             return;
         }
+        if (bodies) {  // room for the header (a few bytes a block) and the segments
+            size_t need = 64;
+            for (int q = 0; q < bcount; ++q)
+                for (size_t i = first[(size_t)c * nb + b0 + q]; i < first[(size_t)c * nb + b0 + q + 1]; ++i)
+                    need += 16 + (size_t)(LEN(l, i) - LEN(l - 1, i));
+            out.v.reserve(out.v.size() + need);
+        }
+        BitWriter bw(out);
         bw.bit(1);
         for (int q = 0; q < bcount; ++q) {
             int b = b0 + q;
@@ -371,7 +379,22 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
             }
         });
         if (failed) throw std::bad_alloc();
-        for (int p = 0; p < npk; ++p) o.v.insert(o.v.end(), pk[p].v.begin(), pk[p].v.end());
+        // append the packets in order; with codeword bytes (over 4 MB) each packet is copied by
+        // one of the threads
+        std::vector<size_t> at(npk + 1, o.v.size());
+        for (int p = 0; p < npk; ++p) at[p + 1] = at[p] + pk[p].v.size();
+        if (at[npk] - at[0] < ((size_t)4 << 20)) {
+            for (int p = 0; p < npk; ++p) o.v.insert(o.v.end(), pk[p].v.begin(), pk[p].v.end());
+            continue;
+        }
+        o.v.resize(at[npk]);
+        next = 0;
+        j2k_run_threads(nt, [&](int) {
+            for (int i; (i = next.fetch_add(1)) < npk;) {
+                const int p = order[i];
+                if (!pk[p].v.empty()) std::memcpy(o.v.data() + at[p], pk[p].v.data(), pk[p].v.size());
+            }
+        });
     }
     const size_t extra = bodies ? 0 : body;
     uint32_t psot = (uint32_t)(o.v.size() + extra - sot);
