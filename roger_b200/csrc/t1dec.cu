@@ -387,7 +387,9 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
 // Host execution of the device decoder logic for one block (used by the test suite).
 extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
                                         int cw, int ch, int32_t* out, size_t pitch) {
-    if (cw < 1 || ch < 1 || cw > 64 || ch > 64 || orient < 0 || orient > 3 || numbps > 31) return -1;
+    if (cw < 1 || ch < 1 || cw > 64 || ch > 64 || orient < 0 || orient > 3 || numbps < 0 || numbps > 31 ||
+        npasses < 0 || npasses > 3 * numbps || len < 0 || (len > 0 && !data) || !out || pitch < (size_t)cw)
+        return -1;  // the checks the kernel makes of a descriptor, and the host buffers
     DecSmem S;
     for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
     for (int k = 0; k < 19; ++k) S.st[k] = 0;
