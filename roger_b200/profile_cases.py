@@ -21,6 +21,8 @@ benchmark workloads but stay within a few hundred MB of device memory:
                captures its launch sequence in a CUDA graph, the second replays it
   decode       lossless decode of one 2048x2048 RGB image (tier-1 decode, inverse 5/3, inverse
                RCT) from code-blocks already on the host
+  rate         one lossless 4096x4096 RGB encode cut to 1 bit per pixel by PCRD-opt (tier-1
+               rate path, distortion pass, host PCRD and header sizing, descriptor update)
 """
 import math
 import sys
@@ -114,10 +116,16 @@ def case_decode():
     return lambda: dec.run(d, b, 2048, 2048, 3, levels=6)
 
 
+def case_rate():
+    img = _rgb()
+    enc = C.OCLEncoder(lossy=False)
+    return lambda: enc.run_rgb(img, levels=6, cbw=64, cbh=64, target_bytes=4096 * 4096 // 8)
+
+
 CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_dwt53(6),
          "idwt53": case_idwt53, "tier1": case_tier1, "encode": case_encode,
          "diff-kernels": case_diff_kernels, "diff-step": case_diff_step, "batched": case_batched,
-         "decode": case_decode}
+         "decode": case_decode, "rate": case_rate}
 
 
 def main(argv):
