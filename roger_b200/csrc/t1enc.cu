@@ -915,56 +915,57 @@ __global__ void iota_kernel(uint32_t* v, int n) {
 
 // Squared reconstruction error of every code-block when decoded down to bit-plane k only
 // (dist[job * 33 + k]; magnitudes below the last decoded plane at the middle of their interval)
-// and with nothing decoded (dist[job * 33 + 32]).  One warp per block; exact 64-bit integer sums
-// in a fixed order, so the truncation choices built on them are deterministic.  A sample of
-// magnitude m with top bit b contributes m^2 to every plane above b (bucketed, prefix-summed at
-// the end) and its exact midpoint error to the planes at and below b.
-__global__ void __launch_bounds__(64)
+// and with nothing decoded (dist[job * 33 + 32]).  One warp per block, kDistWarps blocks per CTA.
+// Each lane keeps one exact 64-bit sum per plane p in registers: a sample of magnitude m with
+// top bit b adds its midpoint error at the planes p <= b and m^2 at the planes above b; the
+// lanes' sums are then added by shuffles.  Integer sums, so the result (and the truncation
+// choices built on it) does not depend on the order of the additions.
+constexpr int kDistWarps = 4;
+__global__ void __launch_bounds__(kDistWarps * 32)
 t1_dist_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__ jobs,
                const j2k_cb_desc* __restrict__ descs, int njobs, double* __restrict__ dist) {
-    __shared__ unsigned long long acc[2][32][33], bucket[2][32][33];  // [warp][plane or bit][lane]
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int jid = blockIdx.x * 2 + w;
+    const int lane = threadIdx.x & 31;
+    const int jid = blockIdx.x * kDistWarps + (threadIdx.x >> 5);
     if (jid >= njobs) return;
     const j2k_cb_job J = jobs[jid];
-    const int nb = min((int)descs[jid].numbps, 31);
-    for (int k = 0; k < 32; ++k) acc[w][k][lane] = bucket[w][k][lane] = 0ull;
+    const int nb = min((int)descs[jid].numbps, 31);  // the same for the whole warp
+    unsigned long long acc[31], total = 0;
+#pragma unroll
+    for (int p = 0; p < 31; ++p) acc[p] = 0;
     if (J.cw <= 64 && J.ch <= 64) {
         for (int y = 0; y < J.ch; ++y) {
             const int32_t* row = coeff + J.off + (size_t)y * J.pitch;
             for (int x = lane; x < J.cw; x += 32) {
                 const int32_t v = row[x];
                 const uint32_t m = v < 0 ? (uint32_t)(-(int64_t)v) : (uint32_t)v;
-                if (!m) continue;
-                const int b = 31 - __clz(m);
-                bucket[w][b][lane] += (unsigned long long)m * m;
-                for (int p = min(b, nb - 1); p >= 0; --p) {
-                    const uint32_t hi = (m >> p) << p;
-                    const int64_t e = (int64_t)m - (int64_t)(hi + ((1u << p) >> 1));
-                    acc[w][nb - 1 - p][lane] += (unsigned long long)(e * e);
+                const int b = 31 - __clz(m);  // -1 for m = 0, which adds nothing
+                const unsigned long long m2 = (unsigned long long)m * m;
+                total += m2;
+#pragma unroll
+                for (int p = 0; p < 31; ++p) {
+                    if (p >= nb) break;
+                    // m - (m truncated to plane p + half its interval); |e| < 2^30
+                    const int e = (int)(m & ((1u << p) - 1u)) - (int)((1u << p) >> 1);
+                    acc[p] += p <= b ? (unsigned long long)((long long)e * e) : m2;
                 }
             }
         }
     }
-    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < 31; ++p) {
+        if (p >= nb) break;
+        unsigned long long s = acc[p];
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        acc[p] = s;
+    }
+    for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
     if (lane == 0) {
-        unsigned long long bsum[32], total = 0;
-        for (int b = 0; b < 32; ++b) {
-            unsigned long long s2 = 0;
-            for (int l = 0; l < 32; ++l) s2 += bucket[w][b][l];
-            bsum[b] = s2;
-            total += s2;
-        }
         double* d = dist + (size_t)jid * 33;
-        for (int k = 0; k < 32; ++k) {
-            unsigned long long s2 = 0;
-            if (k < nb) {
-                for (int l = 0; l < 32; ++l) s2 += acc[w][k][l];
-                const int p = nb - 1 - k;
-                for (int b = 0; b < p && b < 32; ++b) s2 += bsum[b];  // samples still below plane p
-            }
-            d[k] = (double)s2;
-        }
+        // plane p is the last decoded one after k = nb - 1 - p planes
+#pragma unroll
+        for (int p = 0; p < 31; ++p)
+            if (p < nb) d[nb - 1 - p] = (double)acc[p];
+        for (int k = nb; k < 32; ++k) d[k] = 0.0;
         d[32] = (double)total;
     }
 }
@@ -1040,7 +1041,8 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
             t1_mq_kernel<32, true><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs,
                                                               ctx->d_err, pend, plane_bytes, sc);
         J2K_CUDA(ctx, cudaGetLastError());
-        t1_dist_kernel<<<(unsigned)((njobs + 1) / 2), 64, 0, st>>>(coeff, d_jobs, descs, (int)njobs, dist);
+        t1_dist_kernel<<<(unsigned)((njobs + kDistWarps - 1) / kDistWarps), kDistWarps * 32, 0, st>>>(
+            coeff, d_jobs, descs, (int)njobs, dist);
     } else if (lanes == 8)
         t1_mq_kernel<8><<<gb, kMqThreads, 0, st>>>(syms, d_jobs, nsyms, idx_out, (int)njobs, bytes, descs, ctx->d_err,
                                                    nullptr, nullptr, sc);
