@@ -1,5 +1,6 @@
 // Rate control: post-compression rate-distortion optimised truncation (PCRD-opt) of the
-// code-blocks to a byte budget, single quality layer.  No counterpart in the reference.
+// code-blocks to a byte budget (each quality layer of a layered stream is one such cut, at its
+// cumulative budget).  No counterpart in the reference.
 //
 // Truncation points of a block are the ends of its bit-planes (after each cleanup pass:
 // npasses = 1, 4, 7, ..., 3nb-2) and "nothing" (npasses = 0).  At the end of bit-plane k the
@@ -10,8 +11,10 @@
 // of the subband's synthesis basis (and the step squared for quantised coefficients), so that
 // blocks of different bands compare in image units.  Each block's points are reduced to their
 // lower convex hull; over all hull segments in order of decreasing slope, those before the first
-// one that no longer fits the budget are kept (a threshold on the slope, found by a weighted
-// selection), so that every block keeps a prefix of its hull.
+// one that no longer fits the budget are kept (a threshold on the slope, found by a radix
+// selection over the slopes' bits weighted by their bytes), so that every block keeps a prefix
+// of its hull.  The hulls do not depend on the budget: j2k_pcrd_hulls builds them once for every
+// budget a caller tries.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>

@@ -1,6 +1,7 @@
-// Tier-2: T.800 codestream assembly on the host (Annex A markers, Annex B packets).
-// One tile, one quality layer, LRCP progression, one precinct per resolution, code-blocks of
-// one codeword segment each (all passes included).  The reference has no tier-2 at all.
+// Tier-2: T.800 codestream assembly and parsing on the host (Annex A markers, Annex B packets).
+// Writer: one tile, LRCP progression, one precinct per resolution, one or more quality layers,
+// each block's codeword one segment (the default code-block style).  Reader: the same subset,
+// LRCP or RLCP, any number of layers.  The reference has no tier-2 at all.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
