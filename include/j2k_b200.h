@@ -172,7 +172,9 @@ typedef struct {
     int levels;        /* decomposition levels */
     int cbw, cbh;      /* code-block size (default 64x64) */
     int order;         /* J2K_ORDER_* (default T800) */
-    const float* steps;/* lossy: 3*levels+1 steps; NULL = 8*2^-level */
+    const float* steps;/* lossy: 3*levels+1 steps; NULL = 8*2^-level.  Each must fit the QCD's
+                          5-bit exponent (about 2^(g-23) <= step < 2^(g+9), g = 0 for LL, 1 for
+                          HL/LH, 2 for HH); others are refused with J2K_ERR_INVALID_ARG */
     size_t target_bytes; /* 0: every coding pass kept; else the codestream is cut to at most this many
                             bytes by rate-distortion optimised truncation of the code-blocks (PCRD-opt:
                             bit-plane truncation points, one quality layer).  No counterpart in the
