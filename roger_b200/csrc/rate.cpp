@@ -123,6 +123,9 @@ void j2k_pcrd_hulls::build(const j2k_cb_desc* descs, size_t nblocks, const uint3
                 if (np > d.npasses) break;
                 pl[m] = k == nb - 1 ? (double)d.length
                                     : std::min<double>(d.length, (double)plane_bytes[i * 32 + k] + J2K_TRUNC_EXTRA);
+                // a later cut never keeps fewer bytes (the coder's output only grows); held for
+                // any input, so that the kept lengths add up along every hull
+                pl[m] = std::max(pl[m], pl[m - 1]);
                 pd[m] = dist[i * 33 + k] * w;
                 pn[m++] = np;
             }

@@ -106,6 +106,7 @@ def _pcrd_reference(desc, pb, dist, w, budget, extra=4):
             if np_ > npas:
                 break
             L = float(ln) if k == nb - 1 else min(float(ln), float(pb[i, k]) + extra)
+            L = max(L, pts[-1][0])  # a later cut never keeps fewer bytes
             pts.append((L, dist[i, k] * w[i], np_))
         h = []
         for p in pts:
@@ -210,6 +211,34 @@ def test_pcrd_ties_drop_together():
         ref = _pcrd_reference(desc, pb, dist, w, budget)
         assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == ref
         assert int(d2["length"].sum()) <= budget
+
+
+def test_pcrd_holds_the_budget_for_any_plane_positions():
+    """Plane-end byte positions that do not increase (never produced by the coder) are held
+    non-decreasing, so the cut still fits the budget and matches the restatement."""
+    import ctypes as C
+    from roger_b200 import _lib
+    f = C.CDLL(_lib.LIB_PATH).j2k_pcrd_truncate
+    f.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
+    f.restype = C.c_int
+    rng = np.random.default_rng(11)
+    n = 500
+    desc = np.zeros(n, _lib.CB_DESC)
+    nb = rng.integers(1, 12, n)
+    desc["numbps"] = nb
+    desc["npasses"] = 3 * nb - 2
+    desc["length"] = rng.integers(100, 3000, n)
+    pb = rng.integers(0, 3000, (n, 32)).astype(np.uint32)  # in no particular order
+    dist = np.sort(rng.exponential(1e6, (n, 33)), axis=1)[:, ::-1]
+    dist = np.ascontiguousarray(np.concatenate([dist[:, 1:], dist[:, :1]], axis=1))  # [32]: nothing decoded
+    w = rng.uniform(0.5, 2.0, n)
+    full = int(desc["length"].sum())
+    for frac in (0.05, 0.2, 0.5, 0.9):
+        budget = int(full * frac)
+        d2 = desc.copy()
+        assert f(d2.ctypes.data, n, pb.ctypes.data, dist.ctypes.data, w.ctypes.data, budget) == 0
+        assert int(d2["length"].sum()) <= budget
+        assert [(int(a), int(b)) for a, b in zip(d2["npasses"], d2["length"])] == _pcrd_reference(desc, pb, dist, w, budget)
 
 
 @pytest.mark.gpu

@@ -1,8 +1,9 @@
-"""Sanitizer fuzzing on the CPU (no kernel is launched).  The host tier-2 reader (t2.cpp) and the
-tier-1 block decoder (t1dec.cu, whose decode_block is the device kernel's own code, run through
-its host entry point) are compiled with AddressSanitizer and UBSan into the drivers under
-tests/cpp/, and fed mutated codestreams and random codewords: no out-of-bounds access, no
-undefined behaviour, every mutant refused with a status or parsed consistently."""
+"""Sanitizer fuzzing on the CPU (no kernel is launched).  The host tier-2 reader and writer
+(t2.cpp), the tier-1 block decoder (t1dec.cu, whose decode_block is the device kernel's own code,
+run through its host entry point) and PCRD-opt (rate.cpp) are compiled with AddressSanitizer and
+UBSan into the drivers under tests/cpp/, and fed mutated codestreams, random codewords and random
+block sets: no out-of-bounds access, no undefined behaviour, every mutant refused with a status
+or parsed consistently, every cut within its budget."""
 import os
 import shutil
 import subprocess
@@ -72,3 +73,12 @@ def test_t1_block_decoder_under_sanitizers(tmp_path):
     exe = _link(tmp_path, "fuzz_t1_block_decode", [os.path.join(ROOT, "tests", "cpp", "fuzz_t1_block_decode.cpp"), obj])
     out = _run([exe, "20000"], env=ENV, timeout=600)
     assert int(out.split()[1]) > 15000, out
+
+
+def test_pcrd_under_sanitizers(tmp_path):
+    """PCRD-opt (rate.cpp) on random block sets, up to 9000 blocks: every cut keeps whole passes
+    within the codeword and fits the budget, whatever the plane-end positions and distortions."""
+    exe = _link(tmp_path, "fuzz_pcrd", [os.path.join(ROOT, "tests", "cpp", "fuzz_pcrd.cpp"), os.path.join(CSRC, "rate.cpp")])
+    out = _run([exe, "200"], env=ENV, timeout=600)
+    assert int(out.split()[1]) == 1200, out
+
