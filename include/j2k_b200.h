@@ -118,7 +118,8 @@ j2k_status j2k_dwt_inverse(j2k_ctx* ctx, int kernel, int order, const void* in, 
  * (2048x2048 at most for square images); larger images return J2K_ERR_CAPACITY.  Arguments
  * and output are those of j2k_dwt_forward, launched on `cuda_stream` (NULL = legacy default
  * stream).  The first call on a device looks up the array's device address; make that first
- * call before any stream capture.  All calls share the one array (its contents persist from
+ * call before any stream capture.  The address is kept per device and CUDA context, so the
+ * first call after a cudaDeviceReset (which creates a new context) looks it up again.  All calls share the one array (its contents persist from
  * the previous call and nothing needs clearing), so calls whose execution overlaps on the GPU
  * race: order them on one stream or synchronise between them.  Errors are returned as
  * statuses only (there is no context to hold a message). */

@@ -9,7 +9,7 @@ __version__ = "0.1.0"
 
 def __getattr__(name):
     # the torch-backed API is imported lazily so that `import roger_b200` stays cheap
-    if name in ("codec", "synth", "diff97", "batch", "autotune"):
+    if name in ("codec", "synth", "diff97", "batch", "shard"):
         import importlib
         return importlib.import_module(f"{__name__}.{name}")
     raise AttributeError(name)

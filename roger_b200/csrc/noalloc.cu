@@ -8,6 +8,8 @@
 // j2k_dwt_forward_noalloc serves them: the intermediate LL bands live in the file-scope array
 // below, reserved once in every process that loads the library and held until exit, so the
 // call allocates nothing and needs no context.  The caller still passes input and output.
+#include <cudaTypedefs.h>
+
 #include <mutex>
 
 #include "j2k_internal.cuh"
@@ -22,21 +24,67 @@ static __device__ __align__(256) uint32_t g_dwt_scratch[kNoallocElems];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+
+// The array's device address per device, and the id of the CUDA context it was looked up in.
+// A cudaDeviceReset destroys the context and unloads the module; the next context gets a new
+// id (context ids are unique for the life of the process), so the address is looked up again.
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    void* ptr;
+};
+ScratchSlot g_slot[kMaxDevices] = {};
+
+// Driver entry points for the current context's id, resolved once through the runtime (no link
+// dependency on libcuda).  When they are unavailable the address is looked up on every call.
+PFN_cuCtxGetCurrent_v4000 g_get_current = nullptr;
+PFN_cuCtxGetId_v12000 g_get_id = nullptr;
+bool g_resolved = false;
+
+void resolve_entry_points() {
+    if (g_resolved) return;
+    g_resolved = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_get_current = (PFN_cuCtxGetCurrent_v4000)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_get_id = (PFN_cuCtxGetId_v12000)f;
+    if (!g_get_current || !g_get_id) g_get_current = nullptr, g_get_id = nullptr;
+}
+
+// Id of the current context, 0 when there is none yet or it cannot be read.
+unsigned long long current_ctx_id() {
+    if (!g_get_current) return 0;
+    CUcontext c = nullptr;
+    if (g_get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    unsigned long long id = 0;
+    if (g_get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Device address of g_dwt_scratch on `device` (which is current).  In host code the array's
-// name is only a host-side stand-in, so the address must come from cudaGetSymbolAddress, once
-// per device.
+// name is only a host-side stand-in, so the address must come from cudaGetSymbolAddress: once
+// per device and context (the first call on a device, and again after a device reset).
 j2k_status scratch_address(int device, void** out) {
     if (device < 0 || device >= kMaxDevices) return J2K_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_dwt_scratch);
-        if (e != cudaSuccess || !p) return J2K_ERR_CUDA;
-        g_scratch_ptr[device] = p;
+    resolve_entry_points();
+    ScratchSlot& s = g_slot[device];
+    unsigned long long id = current_ctx_id();
+    if (id != 0 && s.ptr && s.ctx_id == id) {
+        *out = s.ptr;
+        return J2K_OK;
     }
-    *out = g_scratch_ptr[device];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_dwt_scratch);  // loads the module in this context
+    if (e != cudaSuccess || !p) return J2K_ERR_CUDA;
+    if (id == 0) id = current_ctx_id();  // the lookup made the device's context current
+    s.ctx_id = id;
+    s.ptr = id != 0 ? p : nullptr;  // without a context id, look it up again next time
+    *out = p;
     return J2K_OK;
 }
 
@@ -47,6 +95,7 @@ extern "C" j2k_status j2k_dwt_forward_noalloc(void* cuda_stream, int kernel, int
                                               size_t h, int levels, const float* steps) {
     J2K_API_BEGIN
     if (!in || !out || w == 0 || h == 0 || in_pitch < w || out_pitch < w) return J2K_ERR_INVALID_ARG;
+    if (w > 0x7FFFFFFF || h > 0x7FFFFFFF) return J2K_ERR_INVALID_ARG;
     if (kernel != J2K_W53 && kernel != J2K_W97) return J2K_ERR_INVALID_ARG;
     if (order != J2K_ORDER_T800 && order != J2K_ORDER_REF) return J2K_ERR_INVALID_ARG;
     if (levels < 0 || levels > 32 || (kernel == J2K_W53 && steps)) return J2K_ERR_INVALID_ARG;

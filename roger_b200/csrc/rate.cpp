@@ -136,7 +136,9 @@ void j2k_pcrd_hulls::build(const j2k_cb_desc* descs, size_t nblocks, const uint3
             int h = 0;
             for (int q = 0; q < m; ++q) {
                 if (h && pl[q] <= hl[h - 1]) {  // no extra bytes: keep the better point
-                    if (pd[q] < hd[h - 1]) hl[h - 1] = pl[q], hd[h - 1] = pd[q], hn[h - 1] = (uint8_t)pn[q];
+                    // (never in place of the empty cut: coded passes need bytes, so a cut of
+                    // passes with no bytes, which only a malformed input gives, is skipped)
+                    if (h > 1 && pd[q] < hd[h - 1]) hl[h - 1] = pl[q], hd[h - 1] = pd[q], hn[h - 1] = (uint8_t)pn[q];
                     continue;
                 }
                 if (h && pd[q] >= hd[h - 1]) continue;  // no improvement

@@ -662,6 +662,9 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
                 const uint32_t tx0 = c.u32(), ty0 = c.u32();
                 ncomp = (int)c.u16();
                 if (x0 || y0 || tx0 || ty0) throw ReadErr{J2K_ERR_UNSUPPORTED, "image or tile offsets"};
+                // code-block positions are kept in 16 bits, as the writer's limit
+                if (xs == 0 || ys == 0 || xs > 65535 || ys > 65535)
+                    throw ReadErr{J2K_ERR_UNSUPPORTED, "image width or height outside 1..65535"};
                 if (tw < xs || th < ys) throw ReadErr{J2K_ERR_UNSUPPORTED, "more than one tile"};
                 if (ncomp != 1 && ncomp != 3) throw ReadErr{J2K_ERR_UNSUPPORTED, "component count other than 1 or 3"};
                 for (int k = 0; k < ncomp; ++k) {

@@ -31,6 +31,10 @@ int main(int argc, char** argv) {
             d[i].length = (int32_t)(rng() % 5000);
             full += (size_t)d[i].length;
             for (int k = 0; k < 32; ++k) pb[i * 32 + k] = (uint32_t)(rng() % 6000);
+            if (rng() % 16 == 0) {  // coded passes with no bytes (a codeword of length 0)
+                d[i].length = 0;
+                for (int k = 0; k < 32; ++k) pb[i * 32 + k] = 0;
+            }
             for (int k = 0; k < 33; ++k) dist[i * 33 + k] = (rng() % 4 == 0) ? 0.0 : (double)(rng() % 1000000);
             w[i] = (rng() % 8 == 0) ? 0.0 : 0.1 + (double)(rng() % 100) / 10.0;
         }
@@ -45,7 +49,7 @@ int main(int argc, char** argv) {
             for (size_t i = 0; i < n; ++i) {
                 const int np = c[i].npasses;
                 if (np > d[i].npasses || (np && np % 3 != 1) || c[i].length < 0 || c[i].length > d[i].length ||
-                    (np == 0 && c[i].length != 0)) {
+                    (np == 0 && c[i].length != 0) || (np != 0 && c[i].length == 0)) {
                     std::printf("set %d block %zu: bad cut (%d passes, %d bytes)\n", t, i, np, c[i].length);
                     return 1;
                 }

@@ -90,6 +90,21 @@ def test_unsupported_streams_are_rejected_with_a_reason():
         C.read_codestream(b"\x00\x01\x02")
 
 
+def test_sizes_beyond_16_bits_are_refused():
+    """Code-block positions are kept in 16 bits (the writer's limit too), so a SIZ width or
+    height above 65535, or of 0, is refused instead of decoding to wrapped positions."""
+    cs = bytearray(O.encode_image(synth.gray(64, 48, 0), 2, 32, 32, True))
+    siz = cs.index(b"\xff\x51")
+    for w, h in [(70000, 48), (64, 65536), (0, 48), (1 << 31, 1 << 31)]:
+        bad = bytearray(cs)
+        bad[siz + 6:siz + 10] = w.to_bytes(4, "big")    # Xsiz
+        bad[siz + 10:siz + 14] = h.to_bytes(4, "big")   # Ysiz
+        bad[siz + 22:siz + 26] = w.to_bytes(4, "big")   # XTsiz (one tile)
+        bad[siz + 26:siz + 30] = h.to_bytes(4, "big")   # YTsiz
+        with pytest.raises(J2KError, match="65535"):
+            C.read_codestream(bytes(bad))
+
+
 def _openjpeg_layers(img, levels, rates, prog="LRCP", cb=64):
     buf = io.BytesIO()
     kw = dict(irreversible=False, num_resolutions=levels + 1, codeblock_size=(cb, cb), progression=prog,
