@@ -380,7 +380,13 @@ enum {
     J2K_BATCH_PHASE_A_ORDER = 4, /* 1: context modelling takes the largest code-blocks first */
     J2K_BATCH_MQ_VARIANT = 5,    /* read-only here; set with j2k_ctx_set_tuning */
     J2K_BATCH_MQ_LANES = 6,
-    J2K_BATCH_MQ_TIERS = 7       /* read-only: 1 when the MQ coder runs the tiered warp schedule */
+    J2K_BATCH_MQ_TIERS = 7,      /* read-only: 1 when the MQ coder runs the tiered warp schedule */
+    J2K_BATCH_GRAPH_KERNELS = 8, /* read-only: kernel launches of one replay of the captured
+                                    sequence, this library's own (library sort/scan kernels are
+                                    not counted); 0 before the first graph encode */
+    J2K_BATCH_STAGES = 9         /* stages an encode runs, for timing them apart: 1 planar split,
+                                    2 DWT, 4 tier-1 (default 7, all).  Without 4 the encode leaves
+                                    no code-blocks to read */
 };
 j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, j2k_batch** out);
 j2k_status j2k_batch_destroy(j2k_batch* b);

@@ -450,13 +450,18 @@ static void mq_reset_states(uint8_t* st, uint8_t* mps) {
     st[CX_UNI] = 46;
 }
 
-static void mqe_init(mqe_t* e, uint8_t* out, int cap) {
+/* INITENC (C.2.8) of a codeword segment starting at `out`; the context states are kept */
+static void mqe_start(mqe_t* e, uint8_t* out, int cap) {
     e->A = 0x8000;
     e->C = 0;
     e->CT = 12;
     e->bp = -1;
     e->out = out;
     e->cap = cap;
+}
+
+static void mqe_init(mqe_t* e, uint8_t* out, int cap) {
+    mqe_start(e, out, cap);
     e->ovf = 0;
     e->nsyms = 0;
     mq_reset_states(e->st, e->mps);
@@ -546,6 +551,74 @@ static int mqe_flush(mqe_t* e) {
     return len;
 }
 
+/* Raw (bypass) segments, T.800 D.6: decisions written as bits, most significant bit of each
+ * byte first; a byte that follows 0xFF carries 7 bits (its top bit is a stuffed 0).  At the
+ * end of a segment the bits of a partial byte are padded with 0s, and a last byte of 0xFF is
+ * dropped (a decoder reads 0xFF past the end of a segment, as the MQ decoder does). */
+typedef struct {
+    uint8_t* out;
+    int cap, pos, ovf;
+    uint32_t c;
+    int ct, lastff;
+} rawe_t;
+
+static void rawe_start(rawe_t* r, uint8_t* out, int cap) {
+    r->out = out;
+    r->cap = cap;
+    r->pos = 0;
+    r->ovf = 0;
+    r->c = 0;
+    r->ct = 8;
+    r->lastff = 0;
+}
+
+static void rawe_byte(rawe_t* r, uint8_t b) {
+    if (r->pos < r->cap) r->out[r->pos] = b; else r->ovf = 1;
+    r->pos++;
+    r->lastff = b == 0xFF;
+    r->ct = r->lastff ? 7 : 8;
+    r->c = 0;
+}
+
+static void rawe_put(rawe_t* r, int bit) {
+    r->c = (r->c << 1) | (uint32_t)(bit & 1);
+    if (--r->ct == 0) rawe_byte(r, (uint8_t)r->c);
+}
+
+static int rawe_flush(rawe_t* r) {
+    if (r->ct < (r->lastff ? 7 : 8)) rawe_byte(r, (uint8_t)(r->c << r->ct));
+    int len = r->pos;
+    if (len > 0 && len <= r->cap && r->out[len - 1] == 0xFF) len--;
+    return len;
+}
+
+typedef struct {
+    const uint8_t* data;
+    int len, pos, ct, lastff;
+    uint32_t c;
+} rawd_t;
+
+static void rawd_start(rawd_t* r, const uint8_t* data, int len) {
+    r->data = data;
+    r->len = len;
+    r->pos = 0;
+    r->ct = 0;
+    r->lastff = 0;
+    r->c = 0;
+}
+
+static int rawd_get(rawd_t* r) {
+    if (r->ct == 0) {
+        uint8_t b = r->pos < r->len ? r->data[r->pos] : 0xFF;
+        r->pos++;
+        r->ct = r->lastff ? 7 : 8;
+        r->lastff = b == 0xFF;
+        r->c = b;
+    }
+    r->ct--;
+    return (int)((r->c >> r->ct) & 1);
+}
+
 typedef struct {
     const uint8_t* data;
     int len, bp;
@@ -573,7 +646,8 @@ static void mqd_bytein(mqd_t* d) {
     }
 }
 
-static void mqd_init(mqd_t* d, const uint8_t* data, int len) {
+/* INITDEC (C.3.5) on a codeword segment; the context states are kept */
+static void mqd_start(mqd_t* d, const uint8_t* data, int len) {
     d->data = data;
     d->len = len;
     d->bp = 0;
@@ -582,6 +656,10 @@ static void mqd_init(mqd_t* d, const uint8_t* data, int len) {
     d->C <<= 7;
     d->CT -= 7;
     d->A = 0x8000;
+}
+
+static void mqd_init(mqd_t* d, const uint8_t* data, int len) {
+    mqd_start(d, data, len);
     mq_reset_states(d->st, d->mps);
 }
 
@@ -710,8 +788,64 @@ static int t1_alloc(t1st_t* t, int cw, int ch) {
     return t->f != NULL;
 }
 
-int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient, uint8_t* out,
-                 int cap, uint8_t* syms, int sym_cap, or_t1_info* info) {
+/* ---- code-block styles (T.800 Table A.19, D.6): which passes are raw-coded, and after which
+ * passes the codeword is terminated (a new codeword segment starts with the next pass). */
+int or_t1_pass_raw(int style, int pass) {
+    return (style & OR_STYLE_BYPASS) && pass >= 10 && pass % 3 != 0;
+}
+
+int or_t1_pass_terminated(int style, int pass, int npasses) {
+    if (pass >= npasses - 1 || (style & OR_STYLE_TERMALL)) return 1;
+    return or_t1_pass_raw(style, pass) != or_t1_pass_raw(style, pass + 1);
+}
+
+/* Tier-1 coder of one code-block: MQ or raw per pass, segments terminated per the style. */
+typedef struct {
+    mqe_t e;
+    rawe_t r;
+    int style, raw, open;
+    uint8_t* out;
+    int cap, base, ovf;
+} t1e_t;
+
+static void t1e_bit(t1e_t* E, int cx, int d) {
+    if (E->raw) rawe_put(&E->r, d); else mqe_encode(&E->e, cx, d);
+}
+
+/* sign of a newly significant sample: MQ codes it XOR the context's bit, raw codes it as is */
+static void t1e_sign(t1e_t* E, int cx, int xb, int neg) {
+    if (E->raw) rawe_put(&E->r, neg); else mqe_encode(&E->e, cx, neg ^ xb);
+}
+
+static void t1e_begin(t1e_t* E, int pass) {
+    if (pass > 0 && (E->style & OR_STYLE_RESET)) mq_reset_states(E->e.st, E->e.mps);
+    E->raw = or_t1_pass_raw(E->style, pass);
+    if (!E->open) {
+        if (E->raw) rawe_start(&E->r, E->out + E->base, E->cap - E->base);
+        else mqe_start(&E->e, E->out + E->base, E->cap - E->base);
+        E->open = 1;
+    }
+}
+
+/* bytes of the codeword so far (exact once the segment is terminated) */
+static int t1e_end(t1e_t* E, int pass, int npasses) {
+    if (or_t1_pass_terminated(E->style, pass, npasses)) {
+        int len;
+        if (E->raw) {
+            len = rawe_flush(&E->r);
+            E->ovf |= E->r.ovf;
+        } else {
+            len = mqe_flush(&E->e);
+        }
+        E->base += len;
+        E->open = 0;
+        return E->base;
+    }
+    return E->base + (E->raw ? E->r.pos : E->e.bp + 1);
+}
+
+static int t1_encode_core(const int32_t* coeff, size_t pitch, int cw, int ch, int orient, int style, uint8_t* out,
+                          int cap, uint8_t* syms, int sym_cap, or_t1_info* info, int* pass_end) {
     t1st_t t;
     if (!t1_alloc(&t, cw, ch)) return -1;
     uint32_t* mag = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)cw * ch);
@@ -726,15 +860,24 @@ int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient,
         }
     int nbps = 0;
     while (nbps < 32 && (mx >> nbps)) nbps++;
-    mqe_t e;
-    mqe_init(&e, out, cap);
-    e.syms = syms;
-    e.sym_cap = sym_cap;
-    int npasses = 0;
+    const int total = nbps ? 3 * nbps - 2 : 0;
+    t1e_t E;
+    mqe_init(&E.e, out, cap);
+    E.e.syms = syms;
+    E.e.sym_cap = sym_cap;
+    E.style = style;
+    E.raw = 0;
+    E.open = 0;
+    E.out = out;
+    E.cap = cap;
+    E.base = 0;
+    E.ovf = 0;
+    int npasses = 0, len = 0;
     for (int p = nbps - 1; p >= 0; --p) {
         int first = (p == nbps - 1);
         if (!first) {
             /* significance propagation pass */
+            t1e_begin(&E, npasses);
             for (int y0 = 0; y0 < ch; y0 += 4)
                 for (int x = 0; x < cw; ++x)
                     for (int y = y0; y < y0 + 4 && y < ch; ++y) {
@@ -744,27 +887,34 @@ int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient,
                         nbr_counts(&t, x, y, &h, &v, &d);
                         if (h + v + d == 0) continue;
                         int bit = (mag[y * cw + x] >> p) & 1;
-                        mqe_encode(&e, zc_label(orient, h, v, d), bit);
+                        t1e_bit(&E, zc_label(orient, h, v, d), bit);
                         FLAG(&t, x, y) |= F_VIS;
                         if (bit) {
                             int xb;
                             int cx = sc_label(&t, x, y, &xb);
-                            mqe_encode(&e, cx, ((FLAG(&t, x, y) & F_NEG) ? 1 : 0) ^ xb);
+                            t1e_sign(&E, cx, xb, (FLAG(&t, x, y) & F_NEG) ? 1 : 0);
                             FLAG(&t, x, y) |= F_SIG;
                         }
                     }
+            len = t1e_end(&E, npasses, total);
+            if (pass_end) pass_end[npasses] = len;
+            npasses++;
             /* magnitude refinement pass */
+            t1e_begin(&E, npasses);
             for (int y0 = 0; y0 < ch; y0 += 4)
                 for (int x = 0; x < cw; ++x)
                     for (int y = y0; y < y0 + 4 && y < ch; ++y) {
                         uint8_t f = FLAG(&t, x, y);
                         if (!(f & F_SIG) || (f & F_VIS)) continue;
-                        mqe_encode(&e, mr_label(&t, x, y), (mag[y * cw + x] >> p) & 1);
+                        t1e_bit(&E, mr_label(&t, x, y), (mag[y * cw + x] >> p) & 1);
                         FLAG(&t, x, y) |= F_REF;
                     }
-            npasses += 2;
+            len = t1e_end(&E, npasses, total);
+            if (pass_end) pass_end[npasses] = len;
+            npasses++;
         }
-        /* cleanup pass */
+        /* cleanup pass (never raw-coded) */
+        t1e_begin(&E, npasses);
         for (int y0 = 0; y0 < ch; y0 += 4)
             for (int x = 0; x < cw; ++x) {
                 int start = y0;
@@ -780,13 +930,13 @@ int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient,
                         int idx = -1;
                         for (int k = 0; k < 4; ++k)
                             if ((mag[(y0 + k) * cw + x] >> p) & 1) { idx = k; break; }
-                        mqe_encode(&e, CX_RL, idx >= 0);
+                        t1e_bit(&E, CX_RL, idx >= 0);
                         if (idx < 0) continue;
-                        mqe_encode(&e, CX_UNI, (idx >> 1) & 1);
-                        mqe_encode(&e, CX_UNI, idx & 1);
+                        t1e_bit(&E, CX_UNI, (idx >> 1) & 1);
+                        t1e_bit(&E, CX_UNI, idx & 1);
                         int y = y0 + idx, xb;
                         int cx = sc_label(&t, x, y, &xb);
-                        mqe_encode(&e, cx, ((FLAG(&t, x, y) & F_NEG) ? 1 : 0) ^ xb);
+                        t1e_sign(&E, cx, xb, (FLAG(&t, x, y) & F_NEG) ? 1 : 0);
                         FLAG(&t, x, y) |= F_SIG;
                         start = y + 1;
                     }
@@ -797,47 +947,97 @@ int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient,
                     int h, v, d;
                     nbr_counts(&t, x, y, &h, &v, &d);
                     int bit = (mag[y * cw + x] >> p) & 1;
-                    mqe_encode(&e, zc_label(orient, h, v, d), bit);
+                    t1e_bit(&E, zc_label(orient, h, v, d), bit);
                     if (bit) {
                         int xb;
                         int cx = sc_label(&t, x, y, &xb);
-                        mqe_encode(&e, cx, ((FLAG(&t, x, y) & F_NEG) ? 1 : 0) ^ xb);
+                        t1e_sign(&E, cx, xb, (FLAG(&t, x, y) & F_NEG) ? 1 : 0);
                         FLAG(&t, x, y) |= F_SIG;
                     }
                 }
             }
+        if (info && nbps - 1 - p < 32) info->plane_bytes[nbps - 1 - p] = E.base + E.e.bp + 1;
+        len = t1e_end(&E, npasses, total);
+        if (pass_end) pass_end[npasses] = len;
         npasses += 1;
-        if (info && nbps - 1 - p < 32) info->plane_bytes[nbps - 1 - p] = e.bp + 1;
         for (int y = 0; y < ch; ++y)
             for (int x = 0; x < cw; ++x) FLAG(&t, x, y) &= (uint8_t)~F_VIS;
     }
-    int len = nbps ? mqe_flush(&e) : 0;
+    len = nbps ? E.base : 0;
     free(mag);
     free(t.f);
     if (info) {
         info->numbps = nbps;
         info->npasses = npasses;
         info->length = len;
-        info->nsyms = e.nsyms;
+        info->nsyms = E.e.nsyms;
     }
-    if (e.ovf || (syms && e.nsyms > sym_cap)) return -1;
+    if (E.e.ovf || E.ovf || (syms && E.e.nsyms > sym_cap)) return -1;
     return len;
 }
 
-int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orient,
-                 int32_t* coeff, size_t pitch, int cw, int ch) {
+int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient, uint8_t* out,
+                 int cap, uint8_t* syms, int sym_cap, or_t1_info* info) {
+    return t1_encode_core(coeff, pitch, cw, ch, orient, 0, out, cap, syms, sym_cap, info, NULL);
+}
+
+int or_t1_encode_styled(const int32_t* coeff, size_t pitch, int cw, int ch, int orient, int style, uint8_t* out,
+                        int cap, or_t1_info* info, int* pass_end) {
+    return t1_encode_core(coeff, pitch, cw, ch, orient, style, out, cap, NULL, 0, info, pass_end);
+}
+
+/* Tier-1 decoder of one code-block: segments located by the pass ends, MQ or raw per pass. */
+typedef struct {
+    mqd_t d;
+    rawd_t r;
+    int style, raw, npasses;
+    const uint8_t* data;
+    int len;
+    const int* pass_end;
+} t1d_t;
+
+static int t1d_bit(t1d_t* D, int cx) { return D->raw ? rawd_get(&D->r) : mqd_decode(&D->d, cx); }
+
+static int t1d_sign(t1d_t* D, int cx, int xb) { return D->raw ? rawd_get(&D->r) : (mqd_decode(&D->d, cx) ^ xb); }
+
+static void t1d_begin(t1d_t* D, int pass) {
+    if (pass > 0 && (D->style & OR_STYLE_RESET)) mq_reset_states(D->d.st, D->d.mps);
+    D->raw = or_t1_pass_raw(D->style, pass);
+    if (pass == 0 || or_t1_pass_terminated(D->style, pass - 1, D->npasses)) {
+        /* a new segment: from the end of the previous one to the end of its last pass */
+        int b0 = pass == 0 ? 0 : (D->pass_end ? D->pass_end[pass - 1] : 0);
+        int q = pass;
+        while (!or_t1_pass_terminated(D->style, q, D->npasses)) q++;
+        int b1 = D->pass_end ? D->pass_end[q] : D->len;
+        if (b0 < 0) b0 = 0;
+        if (b1 > D->len) b1 = D->len;
+        if (b1 < b0) b1 = b0;
+        if (D->raw) rawd_start(&D->r, D->data + b0, b1 - b0);
+        else mqd_start(&D->d, D->data + b0, b1 - b0);
+    }
+}
+
+static int t1_decode_core(const uint8_t* data, int len, const int* pass_end, int numbps, int npasses, int orient,
+                          int style, int32_t* coeff, size_t pitch, int cw, int ch) {
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x) coeff[(size_t)y * pitch + x] = 0;
     if (numbps == 0 || npasses == 0) return 0;
     t1st_t t;
     if (!t1_alloc(&t, cw, ch)) return -1;
     uint32_t* mag = (uint32_t*)calloc((size_t)cw * ch, sizeof(uint32_t));
-    mqd_t d;
-    mqd_init(&d, data, len);
+    t1d_t D;
+    D.style = style;
+    D.npasses = npasses;
+    D.data = data;
+    D.len = len;
+    D.pass_end = pass_end;
+    D.raw = 0;
+    mq_reset_states(D.d.st, D.d.mps);
     int pass = 0;
     for (int p = numbps - 1; p >= 0 && pass < npasses; --p) {
         int first = (p == numbps - 1);
         if (!first) {
+            t1d_begin(&D, pass);
             for (int y0 = 0; y0 < ch; y0 += 4)
                 for (int x = 0; x < cw; ++x)
                     for (int y = y0; y < y0 + 4 && y < ch; ++y) {
@@ -846,28 +1046,30 @@ int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orie
                         int h, v, dd;
                         nbr_counts(&t, x, y, &h, &v, &dd);
                         if (h + v + dd == 0) continue;
-                        int bit = mqd_decode(&d, zc_label(orient, h, v, dd));
+                        int bit = t1d_bit(&D, zc_label(orient, h, v, dd));
                         FLAG(&t, x, y) |= F_VIS;
                         if (bit) {
                             int xb;
                             int cx = sc_label(&t, x, y, &xb);
-                            int s = mqd_decode(&d, cx) ^ xb;
+                            int s = t1d_sign(&D, cx, xb);
                             FLAG(&t, x, y) |= (uint8_t)(F_SIG | (s ? F_NEG : 0));
                             mag[y * cw + x] |= 1u << p;
                         }
                     }
             if (++pass >= npasses) break;
+            t1d_begin(&D, pass);
             for (int y0 = 0; y0 < ch; y0 += 4)
                 for (int x = 0; x < cw; ++x)
                     for (int y = y0; y < y0 + 4 && y < ch; ++y) {
                         uint8_t f = FLAG(&t, x, y);
                         if (!(f & F_SIG) || (f & F_VIS)) continue;
-                        int bit = mqd_decode(&d, mr_label(&t, x, y));
+                        int bit = t1d_bit(&D, mr_label(&t, x, y));
                         if (bit) mag[y * cw + x] |= 1u << p;
                         FLAG(&t, x, y) |= F_REF;
                     }
             if (++pass >= npasses) break;
         }
+        t1d_begin(&D, pass);
         for (int y0 = 0; y0 < ch; y0 += 4)
             for (int x = 0; x < cw; ++x) {
                 int start = y0;
@@ -880,12 +1082,12 @@ int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orie
                         if ((f & (F_SIG | F_VIS)) || h + v + dd) rl = 0;
                     }
                     if (rl) {
-                        if (!mqd_decode(&d, CX_RL)) continue;
-                        int idx = mqd_decode(&d, CX_UNI) << 1;
-                        idx |= mqd_decode(&d, CX_UNI);
+                        if (!t1d_bit(&D, CX_RL)) continue;
+                        int idx = t1d_bit(&D, CX_UNI) << 1;
+                        idx |= t1d_bit(&D, CX_UNI);
                         int y = y0 + idx, xb;
                         int cx = sc_label(&t, x, y, &xb);
-                        int s = mqd_decode(&d, cx) ^ xb;
+                        int s = t1d_sign(&D, cx, xb);
                         FLAG(&t, x, y) |= (uint8_t)(F_SIG | (s ? F_NEG : 0));
                         mag[y * cw + x] |= 1u << p;
                         start = y + 1;
@@ -896,11 +1098,11 @@ int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orie
                     if (f & (F_SIG | F_VIS)) continue;
                     int h, v, dd;
                     nbr_counts(&t, x, y, &h, &v, &dd);
-                    int bit = mqd_decode(&d, zc_label(orient, h, v, dd));
+                    int bit = t1d_bit(&D, zc_label(orient, h, v, dd));
                     if (bit) {
                         int xb;
                         int cx = sc_label(&t, x, y, &xb);
-                        int s = mqd_decode(&d, cx) ^ xb;
+                        int s = t1d_sign(&D, cx, xb);
                         FLAG(&t, x, y) |= (uint8_t)(F_SIG | (s ? F_NEG : 0));
                         mag[y * cw + x] |= 1u << p;
                     }
@@ -926,6 +1128,16 @@ int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orie
     free(mag);
     free(t.f);
     return 0;
+}
+
+int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orient,
+                 int32_t* coeff, size_t pitch, int cw, int ch) {
+    return t1_decode_core(data, len, NULL, numbps, npasses, orient, 0, coeff, pitch, cw, ch);
+}
+
+int or_t1_decode_styled(const uint8_t* data, int len, const int* pass_end, int numbps, int npasses, int orient,
+                        int style, int32_t* coeff, size_t pitch, int cw, int ch) {
+    return t1_decode_core(data, len, pass_end, numbps, npasses, orient, style, coeff, pitch, cw, ch);
 }
 
 /* ============================================================================================
@@ -1058,6 +1270,7 @@ static int floorlog2(long v) { int l = -1; while (v) { v >>= 1; l++; } return l;
 typedef struct {
     int x0, y0, cw, ch;
     or_t1_info info;
+    int pass_end[96];
     uint8_t* data;
 } cb_t;
 
@@ -1116,13 +1329,28 @@ long or_encode_image(const uint8_t* img, size_t w, size_t h, int ncomp, const or
                     cb->y0 = j * p->cbh;
                     cb->cw = (int)((bd->sw - cb->x0) < (size_t)p->cbw ? bd->sw - cb->x0 : (size_t)p->cbw);
                     cb->ch = (int)((bd->sh - cb->y0) < (size_t)p->cbh ? bd->sh - cb->y0 : (size_t)p->cbh);
-                    int ccap = cb->cw * cb->ch * 5 + 64;
+                    int ccap = cb->cw * cb->ch * 5 + 64 + 4 * 96;
                     cb->data = (uint8_t*)malloc((size_t)ccap);
                     const int32_t* src = coef + c * N + (bd->y0 + cb->y0) * w + bd->x0 + cb->x0;
-                    or_t1_encode(src, w, cb->cw, cb->ch, bd->orient, cb->data, ccap, NULL, 0, &cb->info);
+                    t1_encode_core(src, w, cb->cw, cb->ch, bd->orient, p->style, cb->data, ccap, NULL, 0, &cb->info,
+                                   cb->pass_end);
                     if (cb->info.numbps > maxbps[b]) maxbps[b] = cb->info.numbps;
                 }
         }
+    if (p->tier1_only) {
+        long total = 0;
+        for (int i = 0; i < nb * ncomp; ++i) {
+            band_t* bd = &bands[i];
+            for (int k = 0; k < bd->ncbx * bd->ncby; ++k) {
+                total += bd->cbs[k].info.length;
+                free(bd->cbs[k].data);
+            }
+            free(bd->cbs);
+        }
+        free(bands);
+        free(coef);
+        return total;
+    }
     /* quantisation exponents (eps_b) and guard bits */
     int eps[3 * 32 + 1], mant[3 * 32 + 1], G = 2;
     for (int b = 0; b < nb; ++b) {
@@ -1169,7 +1397,7 @@ long or_encode_image(const uint8_t* img, size_t w, size_t h, int ncomp, const or
     bput(&o, (uint8_t)L);
     bput(&o, (uint8_t)(floorlog2(p->cbw) - 2));
     bput(&o, (uint8_t)(floorlog2(p->cbh) - 2));
-    bput(&o, 0);
+    bput(&o, (uint8_t)p->style);            /* code-block style */
     bput(&o, p->lossless ? 1 : 0);
     bput16(&o, 0xFF5C);                      /* QCD */
     if (p->lossless) {
@@ -1228,14 +1456,29 @@ long or_encode_image(const uint8_t* img, size_t w, size_t h, int ncomp, const or
                         if (cb->info.npasses == 0) continue;
                         tt_encode(&tz, &bw, i, j, 0x7FFFFFF);
                         put_npasses(&bw, cb->info.npasses);
-                        int lblock = 3;
-                        int bits = floorlog2(cb->info.length) + 1;
-                        int avail = lblock + floorlog2(cb->info.npasses);
-                        int inc = bits > avail ? bits - avail : 0;
+                        /* one codeword segment per terminated pass (B.10.7.2): each length in
+                         * Lblock + floor(log2(passes of the segment)) bits, Lblock raised once
+                         * so that every length fits */
+                        int lblock = 3, nseg = 0, seg_np[96], seg_len[96], prev = 0, np0 = 0;
+                        for (int q = 0; q < cb->info.npasses; ++q)
+                            if (or_t1_pass_terminated(p->style, q, cb->info.npasses)) {
+                                seg_np[nseg] = q + 1 - np0;
+                                seg_len[nseg] = cb->pass_end[q] - prev;
+                                prev = cb->pass_end[q];
+                                np0 = q + 1;
+                                nseg++;
+                            }
+                        int inc = 0;
+                        for (int q = 0; q < nseg; ++q) {
+                            int bits = floorlog2(seg_len[q]) + 1;
+                            int avail = lblock + floorlog2(seg_np[q]);
+                            if (bits - avail > inc) inc = bits - avail;
+                        }
                         for (int q = 0; q < inc; ++q) bw_put(&bw, 1);
                         bw_put(&bw, 0);
                         lblock += inc;
-                        bw_putn(&bw, (uint32_t)cb->info.length, lblock + floorlog2(cb->info.npasses));
+                        for (int q = 0; q < nseg; ++q)
+                            bw_putn(&bw, (uint32_t)seg_len[q], lblock + floorlog2(seg_np[q]));
                     }
                 tt_free(&ti);
                 tt_free(&tz);

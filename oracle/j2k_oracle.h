@@ -120,6 +120,24 @@ int or_t1_encode(const int32_t* coeff, size_t pitch, int cw, int ch, int orient,
 int or_t1_decode(const uint8_t* data, int len, int numbps, int npasses, int orient,
                  int32_t* coeff, size_t pitch, int cw, int ch);
 
+/* Code-block styles (T.800 Table A.19, COD SPcod byte): selective arithmetic-coding bypass
+ * (the significance-propagation and refinement passes from the fifth bit-plane on are written
+ * as raw bits, D.6), context reset at every pass boundary, and termination of the codeword
+ * after every pass.  Each terminated segment starts afresh (MQ INITENC, or a new raw byte). */
+enum { OR_STYLE_BYPASS = 1, OR_STYLE_RESET = 2, OR_STYLE_TERMALL = 4 };
+/* 1 when pass `pass` (0 = the first cleanup pass) is raw-coded under `style` */
+int or_t1_pass_raw(int style, int pass);
+/* 1 when the codeword is terminated after pass `pass` of a block coded in `npasses` passes */
+int or_t1_pass_terminated(int style, int pass, int npasses);
+/* or_t1_encode with a code-block style; pass_end (optional, 96 entries) receives, per pass,
+ * the codeword bytes when the pass ended (exact where the pass is terminated). */
+int or_t1_encode_styled(const int32_t* coeff, size_t pitch, int cw, int ch, int orient, int style, uint8_t* out,
+                        int cap, or_t1_info* info, int* pass_end);
+/* Decodes a block coded with `style`; the codeword segments are located by pass_end (the
+ * encoder's pass ends, exact at terminated passes; NULL for one segment of `len` bytes). */
+int or_t1_decode_styled(const uint8_t* data, int len, const int* pass_end, int numbps, int npasses, int orient,
+                        int style, int32_t* coeff, size_t pitch, int cw, int ch);
+
 /* ---- whole-image encode (tier-1 + tier-2) --------------------------------------------------- */
 typedef struct {
     int levels;
@@ -127,9 +145,13 @@ typedef struct {
     int lossless;          /* 1: RCT + 5/3, 0: ICT + 9/7 + quantiser */
     int order;             /* OR_ORDER_* for the 5/3 path */
     const float* steps;    /* 3L+1 quantiser steps (lossy); NULL = 8*2^-level */
+    int tier1_only;        /* 1: stop after tier-1 (no codestream written; out may be NULL) */
+    int style;             /* code-block style, OR_STYLE_* bits (0: none) */
 } or_enc_params;
 /* Encodes an interleaved uint8 image (ncomp 1 or 3) into a raw J2K codestream.  Returns the
- * codestream length, or -1 when `cap` is too small. */
+ * codestream length, or -1 when `cap` is too small.  With p->tier1_only the image is coded up
+ * to the code-blocks' codewords only (planar, colour transform, DWT, quantiser, tier-1) and the
+ * return value is the sum of the codeword lengths. */
 long or_encode_image(const uint8_t* img, size_t w, size_t h, int ncomp, const or_enc_params* p,
                      uint8_t* out, long cap);
 

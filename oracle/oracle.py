@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 ORDER_T800, ORDER_REF = 0, 1
+STYLE_BYPASS, STYLE_RESET, STYLE_TERMALL = 1, 2, 4
 MCT_NONE, MCT_RCT, MCT_ICT = 0, 1, 2
 LL, HL, LH, HH = 0, 1, 2, 3
 
@@ -48,6 +49,10 @@ def lib():
             "or_dequantize_f32": [P, S, P, S, S, S, I, P],
             "or_t1_encode": [P, S, I, I, I, P, I, P, I, P],
             "or_t1_decode": [P, I, I, I, I, P, S, I, I],
+            "or_t1_encode_styled": [P, S, I, I, I, I, P, I, P, P],
+            "or_t1_decode_styled": [P, I, P, I, I, I, I, P, S, I, I],
+            "or_t1_pass_raw": [I, I],
+            "or_t1_pass_terminated": [I, I, I],
             "or_encode_image": [P, S, S, I, P, P, C.c_long],
             "or_philox_uniform": [C.c_uint64, C.c_uint64],
             "or_rd_noise": [C.c_uint64, S, S, S],
@@ -59,6 +64,10 @@ def lib():
             f.argtypes = args
         L.or_t1_encode.restype = I
         L.or_t1_decode.restype = I
+        L.or_t1_encode_styled.restype = I
+        L.or_t1_decode_styled.restype = I
+        L.or_t1_pass_raw.restype = I
+        L.or_t1_pass_terminated.restype = I
         L.or_subband_rect.restype = I
         L.or_encode_image.restype = C.c_long
         L.or_philox_uniform.restype = D
@@ -79,7 +88,7 @@ class T1Info(C.Structure):
 
 class EncParams(C.Structure):
     _fields_ = [("levels", C.c_int), ("cbw", C.c_int), ("cbh", C.c_int), ("lossless", C.c_int),
-                ("order", C.c_int), ("steps", C.c_void_p)]
+                ("order", C.c_int), ("steps", C.c_void_p), ("tier1_only", C.c_int), ("style", C.c_int)]
 
 
 def planar_fwd(img, mct, as_float=False):
@@ -197,6 +206,40 @@ def t1_encode(block, orient, want_symbols=False):
     return out[:n].tobytes(), d
 
 
+def t1_encode_styled(block, orient, style):
+    """Encodes one code-block with a code-block style.  Returns (bytes, info dict, pass_end
+    list: codeword bytes at the end of each pass, exact where the pass is terminated)."""
+    block = np.ascontiguousarray(block, np.int32)
+    ch, cw = block.shape
+    cap = cw * ch * 8 + 1024
+    out = np.empty(cap, np.uint8)
+    info = T1Info()
+    pe = np.zeros(96, np.int32)
+    n = lib().or_t1_encode_styled(_p(block), cw, cw, ch, orient, style, _p(out), cap, C.byref(info), _p(pe))
+    if n < 0:
+        raise RuntimeError("oracle t1 encode overflow")
+    d = dict(numbps=info.numbps, npasses=info.npasses, length=info.length, nsyms=info.nsyms)
+    return out[:n].tobytes(), d, [int(v) for v in pe[:info.npasses]]
+
+
+def t1_decode_styled(data, pass_end, numbps, npasses, orient, cw, ch, style):
+    buf = np.frombuffer(bytes(data) + b"\0", np.uint8).copy()
+    pe = np.ascontiguousarray(np.asarray(pass_end, np.int32)) if pass_end is not None else None
+    out = np.empty((ch, cw), np.int32)
+    r = lib().or_t1_decode_styled(_p(buf), len(data), _p(pe), numbps, npasses, orient, style, _p(out), cw, cw, ch)
+    if r != 0:
+        raise RuntimeError("oracle t1 decode failed")
+    return out
+
+
+def pass_raw(style, p):
+    return bool(lib().or_t1_pass_raw(style, p))
+
+
+def pass_terminated(style, p, npasses):
+    return bool(lib().or_t1_pass_terminated(style, p, npasses))
+
+
 def t1_decode(data, numbps, npasses, orient, cw, ch):
     buf = np.frombuffer(bytes(data) + b"\0", np.uint8).copy()
     out = np.empty((ch, cw), np.int32)
@@ -206,14 +249,30 @@ def t1_decode(data, numbps, npasses, orient, cw, ch):
     return out
 
 
-def encode_image(img, levels, cbw=64, cbh=64, lossless=True, order=ORDER_T800, steps=None):
-    """Whole-image oracle encoder -> raw J2K codestream bytes."""
+def encode_tier1(img, levels, cbw=64, cbh=64, lossless=True, order=ORDER_T800, steps=None, style=0):
+    """Whole-image oracle encode up to the code-blocks' codewords (planar, colour transform,
+    DWT, quantiser, tier-1; no tier-2) -> the sum of the codeword lengths."""
     img = np.ascontiguousarray(img, np.uint8)
     if img.ndim == 2:
         img = img[:, :, None]
     h, w, nc = img.shape
     st = None if steps is None else np.ascontiguousarray(steps, np.float32)
-    par = EncParams(levels, cbw, cbh, int(lossless), order, st.ctypes.data if st is not None else None)
+    par = EncParams(levels, cbw, cbh, int(lossless), order, st.ctypes.data if st is not None else None, 1, style)
+    n = lib().or_encode_image(_p(img), w, h, nc, C.byref(par), None, 0)
+    if n < 0:
+        raise RuntimeError("oracle tier-1 encode failed")
+    return int(n)
+
+
+def encode_image(img, levels, cbw=64, cbh=64, lossless=True, order=ORDER_T800, steps=None, style=0):
+    """Whole-image oracle encoder -> raw J2K codestream bytes (style: code-block style bits,
+    STYLE_*)."""
+    img = np.ascontiguousarray(img, np.uint8)
+    if img.ndim == 2:
+        img = img[:, :, None]
+    h, w, nc = img.shape
+    st = None if steps is None else np.ascontiguousarray(steps, np.float32)
+    par = EncParams(levels, cbw, cbh, int(lossless), order, st.ctypes.data if st is not None else None, 0, style)
     cap = w * h * nc * 4 + 65536
     out = np.empty(cap, np.uint8)
     n = lib().or_encode_image(_p(img), w, h, nc, C.byref(par), _p(out), cap)

@@ -118,6 +118,11 @@ class BatchEncoder:
     def set_option(self, key, value):
         check(lib().j2k_batch_set_option(self.h, key, value), self.ctx.h)
 
+    def get_option(self, key):
+        v = C.c_int()
+        check(lib().j2k_batch_get_option(self.h, key, C.byref(v)), self.ctx.h)
+        return v.value
+
     def autotune(self, reps=2):
         rep = (C.c_int * 5)()
         hh = self.ctx._bind()

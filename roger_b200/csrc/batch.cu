@@ -83,6 +83,7 @@ struct j2k_batch {
     int tile_code[2] = {0, 0};
     int phase_a_order = 1;  // 1: largest blocks first, 0: natural order
     bool use_graph = true;
+    int stages = 7;  // J2K_BATCH_STAGES: 1 planar, 2 DWT, 4 tier-1
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;  // capture stream (the caller's may be the legacy stream)
@@ -321,12 +322,33 @@ static j2k_status enqueue(j2k_batch* b, bool do_planar, bool do_dwt, bool do_t1)
     return J2K_OK;
 }
 
+// Kernel nodes of a captured graph whose kernels are this library's (CUB's sort and scan
+// kernels, which the tier-1 order uses, are left out); -1 when the graph cannot be read.
+static int count_own_kernel_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return -1;
+    int count = 0;
+    for (size_t i = 0; i < n; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        if (cudaGraphKernelNodeGetParams(nodes[i], &kp) != cudaSuccess) continue;
+        const char* name = nullptr;
+        if (cudaFuncGetName(&name, kp.func) != cudaSuccess || !name) continue;
+        if (std::strstr(name, "cub") != nullptr) continue;
+        ++count;
+    }
+    return count;
+}
+
 static j2k_status run_once(j2k_batch* b) {
     j2k_ctx* ctx = b->ctx;
     if (b->use_graph) {
         if (!b->gexec) {
             // warm every launch path once outside capture (lazy module loading, scratch sizing)
-            J2K_TRY(enqueue(b, true, true, true));
+            J2K_TRY(enqueue(b, b->stages & 1, b->stages & 2, b->stages & 4));
             J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
             if (!b->cap_stream) J2K_CUDA(ctx, cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
             cudaStream_t caller = ctx->stream;
@@ -336,7 +358,7 @@ static j2k_status run_once(j2k_batch* b) {
                 ctx->stream = caller;
                 J2K_CUDA(ctx, eb);
             }
-            j2k_status s = enqueue(b, true, true, true);
+            j2k_status s = enqueue(b, b->stages & 1, b->stages & 2, b->stages & 4);
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
             ctx->stream = caller;
@@ -351,7 +373,7 @@ static j2k_status run_once(j2k_batch* b) {
         J2K_CUDA(ctx, cudaGraphLaunch(b->gexec, ctx->stream));
         return J2K_OK;
     }
-    return enqueue(b, true, true, true);
+    return enqueue(b, b->stages & 1, b->stages & 2, b->stages & 4);
 }
 
 extern "C" {
@@ -442,6 +464,10 @@ j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value) {
             J2K_TRY(plan_dwt(b));
             break;
         case J2K_BATCH_PHASE_A_ORDER: b->phase_a_order = value != 0; break;
+        case J2K_BATCH_STAGES:
+            if (value < 1 || value > 7) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "stage mask must be 1..7");
+            b->stages = value;
+            break;
         default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "unknown batch option");
     }
     drop_graph(b);
@@ -460,6 +486,8 @@ j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
         case J2K_BATCH_MQ_VARIANT: *value = b->ctx->mq_variant; break;
         case J2K_BATCH_MQ_LANES: *value = b->ctx->mq_lanes; break;
         case J2K_BATCH_MQ_TIERS: *value = b->ctx->mq_tier_lanes[0] > 0 && b->ctx->mq_tier_warps[0] > 0; break;
+        case J2K_BATCH_GRAPH_KERNELS: *value = b->graph ? count_own_kernel_nodes(b->graph) : 0; break;
+        case J2K_BATCH_STAGES: *value = b->stages; break;
         default: return J2K_ERR_INVALID_ARG;
     }
     return J2K_OK;
@@ -508,7 +536,7 @@ static j2k_status batch_finish(j2k_batch* b) {
     for (int attempt = 0; attempt < 6; ++attempt) {
         j2k_status s = j2k_read_device_error(ctx);
         if (s == J2K_OK) {
-            b->have_result = true;
+            b->have_result = (b->stages & 4) != 0;  // code-blocks exist only when tier-1 ran
             return J2K_OK;
         }
         if (s != J2K_ERR_CAPACITY) return s;

@@ -1,4 +1,4 @@
-"""Sharding a set of images across GPUs (one process per GPU).
+"""Sharding a set of images across GPUs (one process per GPU), and the multi-GPU set encoder.
 
 Images, their tiles and their code-blocks are independent, so a multi-GPU encode needs no
 exchange on the data path: each rank encodes its own share and writes its own codestreams.
@@ -72,3 +72,46 @@ def gather_counts(local_indices, local_counts, n_total, group=None):
         v[torch.as_tensor(local_indices, device=dev)] = torch.as_tensor(local_counts, dtype=torch.int64, device=dev)
     dist.all_reduce(v, op=dist.ReduceOp.SUM, group=group)
     return v.cpu().numpy()
+
+
+def _gpu_encode_share(descs, images):
+    """Encodes one rank's images with one batched encoder on the current CUDA device (one
+    launch sequence for the whole share) and returns each image's codestream."""
+    import torch
+    from .batch import BatchEncoder
+    from .codec import Context
+    if not descs:
+        return []
+    be = BatchEncoder([dict(w=d["w"], h=d["h"], ncomp=d["ncomp"], kernel=d["kernel"], levels=d["levels"],
+                            cb=d["cb"], steps=d.get("steps")) for d in descs],
+                      ctx=Context(torch.cuda.current_device()))
+    be.encode(images)
+    return [be.codestream(i) for i in range(len(descs))]
+
+
+def encode_set(descs, load_image, rank=0, world=1, encode_share=None, group=None, blocks_weight=4096):
+    """Multi-GPU encoder of an image set: this rank encodes its LPT share of `descs` and the
+    codestream sizes of every image are gathered to every rank.
+
+    descs: one dict per image (w, h, ncomp, kernel, levels, cb[, steps]).
+    load_image(i): image i as (h, w[, 3]) uint8 (numpy or CUDA tensor); called only for this
+        rank's own images, so no rank holds the whole set.
+    encode_share(share_descs, share_images): list of codestreams (bytes), one per image; by
+        default one batched encode on this rank's GPU.
+    Returns (indices of this rank's images, their codestreams, int64 array of every image's
+    codestream bytes).  With world > 1 the byte-count gather is the one collective (an
+    all-reduce over `group`); the encode itself exchanges nothing.  The reference encodes one
+    image at a time on one in-order queue (src/OCLUtil.cpp:505-516)."""
+    idx = shard(descs, rank, world, blocks_weight)
+    mine = [descs[i] for i in idx]
+    images = [load_image(i) for i in idx]
+    streams = (encode_share or _gpu_encode_share)(mine, images)
+    if len(streams) != len(idx):
+        raise RuntimeError("encode_share returned a codestream count unlike its share")
+    sizes = [len(s) for s in streams]
+    if world > 1:
+        counts = gather_counts(idx, sizes, len(descs), group)
+    else:
+        counts = np.zeros(len(descs), np.int64)
+        counts[idx] = sizes
+    return idx, streams, counts

@@ -186,3 +186,52 @@ def test_philox_known_answers_and_noise_layout():
         c, o = (C.c_uint32 * 4)(ctr & 0xffffffff, ctr >> 32, 0, 0), (C.c_uint32 * 4)()
         L.or_philox4x32(seed & 0xffffffff, seed >> 32, c, o)
         assert O.rd_noise(seed, w, x, y) == (o[x % 4] >> 8) / 16777216.0 - 0.5
+
+
+STYLES = [0, O.STYLE_BYPASS, O.STYLE_RESET, O.STYLE_TERMALL, O.STYLE_RESET | O.STYLE_TERMALL,
+          O.STYLE_BYPASS | O.STYLE_TERMALL, O.STYLE_BYPASS | O.STYLE_RESET,
+          O.STYLE_BYPASS | O.STYLE_RESET | O.STYLE_TERMALL]
+
+
+def test_style_pass_rules():
+    """Raw passes: SPP and MRP from the fifth bit-plane on (pass 10 on) under bypass; the
+    codeword ends after every pass under termination, else where bypass switches between raw
+    and MQ coding, and always after the last pass (T.800 D.6, Table A.19)."""
+    assert [p for p in range(20) if O.pass_raw(O.STYLE_BYPASS, p)] == [10, 11, 13, 14, 16, 17, 19]
+    assert not any(O.pass_raw(O.STYLE_RESET | O.STYLE_TERMALL, p) for p in range(40))
+    assert [p for p in range(16) if O.pass_terminated(O.STYLE_BYPASS, p, 16)] == [9, 11, 12, 14, 15]
+    assert [p for p in range(16) if O.pass_terminated(0, p, 16)] == [15]
+    assert all(O.pass_terminated(O.STYLE_TERMALL, p, 16) for p in range(16))
+
+
+@pytest.mark.parametrize("style", STYLES)
+def test_styled_blocks_round_trip(style):
+    """Every style: the styled encoder's codeword decodes back to the block (segments located
+    by the pass ends), and style 0 gives the plain encoder's codeword."""
+    rng = np.random.default_rng(style + 11)
+    for cw, ch, orient in [(64, 64, 0), (32, 32, 3), (17, 5, 1), (4, 4, 2), (1, 1, 0), (64, 3, 1), (8, 64, 2)]:
+        blk = rng.integers(-5000, 5000, (ch, cw)).astype(np.int32)
+        blk[rng.random((ch, cw)) < 0.6] = 0
+        data, info, pe = O.t1_encode_styled(blk, orient, style)
+        assert pe[-1] == len(data) if info["npasses"] else len(data) == 0
+        back = O.t1_decode_styled(data, pe, info["numbps"], info["npasses"], orient, cw, ch, style)
+        assert np.array_equal(back, blk), (cw, ch)
+        if style == 0:
+            assert data == O.t1_encode(blk, orient)[0]
+
+
+@pytest.mark.parametrize("style", STYLES[1:])
+def test_openjpeg_decodes_styled_oracle_codestreams(style):
+    """An independent decoder (OpenJPEG through Pillow) decodes the styled codestreams: lossless
+    exactly, lossy to the same pixels as the unstyled stream."""
+    from PIL import Image
+    for w, h, nc, lossless, L, cb in [(200, 131, 3, True, 4, 32), (256, 256, 3, False, 5, 64),
+                                      (67, 45, 1, False, 3, 16), (97, 200, 1, True, 5, 64)]:
+        img = synth.gray(w, h, 3) if nc == 1 else synth.rgb(w, h, (5, 6, 7, 8))
+        cs = O.encode_image(img, L, cb, cb, lossless, style=style)
+        dec = np.array(Image.open(io.BytesIO(cs))).reshape(img.shape)
+        ref = np.array(Image.open(io.BytesIO(O.encode_image(img, L, cb, cb, lossless)))).reshape(img.shape)
+        assert np.array_equal(dec, ref)
+        if lossless:
+            assert np.array_equal(dec, img)
+        assert cs[cs.index(b"\xff\x52") + 12] == style  # COD code-block style byte
