@@ -491,6 +491,9 @@ def main():
         line["c1"] = c1
         img_h = c1.pop("_img_h")
         line["lossless_decode"] = bench_lossless_decode(img_h, c1.pop("_res"))
+        st = c1["stages_ms"]
+        c1["styles"] = bench_styles(img_h, flush, st["planar_rct"] + st["dwt_all_levels_3comp"], c1["ms_per_step"],
+                                    c1["tier1"]["codeword_bytes"])
         if world == 1:
             line["lossy"] = bench_lossy(img_h, flush)
             line["rate_control"] = bench_rate_control(img_h, flush)
@@ -506,6 +509,35 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def bench_styles(img_h, flush, front_ms, plain_ms, plain_bytes):
+    """The 4096x4096 lossless encode in the code-block styles that let tier-1 code the passes
+    of a block in parallel (context reset + termination after every pass, and that with the
+    arithmetic-coding bypass of the low planes' refinement and propagation passes): encode time,
+    tier-1 time (encode minus the planar + DWT stages) and the codewords' size against the
+    default style."""
+    import torch
+    from roger_b200 import codec as C
+    img_d = torch.from_numpy(img_h).cuda()
+    out = {}
+    for name, style in (("reset_termall", 6), ("bypass_reset_termall", 7)):
+        enc = C.OCLEncoder(lossy=False)
+
+        def step():
+            enc.run_rgb(img_d, levels=C1_LEVELS, cbw=C1_CB, cbh=C1_CB, cblk_style=style)
+        for _ in range(3):
+            step()
+        ms = ev_median(step, flush, 7)
+        _, data = enc.get_codeblocks()
+        nb = int(data.size)
+        out[name] = {"cblk_style": style, "ms_per_step": round(ms, 4),
+                     "mpix_s": round(img_h.shape[0] * img_h.shape[1] / 1e6 / (ms * 1e-3), 1),
+                     "tier1_ms": round(ms - front_ms, 4), "codeword_bytes": nb,
+                     "size_vs_default": round(nb / plain_bytes, 4)}
+    out["default"] = {"ms_per_step": round(plain_ms, 4), "tier1_ms": round(plain_ms - front_ms, 4),
+                      "codeword_bytes": int(plain_bytes)}
+    return out
 
 
 def bench_per_image(be, descs, imgs, flush, ms_batched, mpix):

@@ -67,6 +67,8 @@ enum {
     J2K_TUNE_DWT_PIPE = 4,    /* 1: that kernel streams bands with cp.async double buffering (default 0) */
     J2K_TUNE_DWT_REG = 5,     /* 1 (default): that kernel loads its columns straight into registers;
                                  0: it stages the strip in shared memory with cp.async */
+    J2K_TUNE_DWT_TMA = 7,     /* 1: that kernel is the TMA-staged form (persistent CTAs, each strip brought in
+                                 by one tensor copy, two stages deep) */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of
@@ -139,6 +141,18 @@ j2k_status j2k_dwt_inverse_batch(j2k_ctx* ctx, int kernel, int order, const void
 /* ---- EBCOT tier-1: replaces OCLBPC<T>::run (src/OCLBPC.cpp:38-50) and src/CL/oclbpc.cl:279-746.
  * Code-blocks partition every subband of a Mallat plane (w x h, `levels`) on a cbw x cbh grid
  * anchored at the subband origin, subbands in QCD order, blocks in raster order. */
+/* Code-block styles (T.800 Table A.19, the COD code-block style byte), no counterpart in the
+ * reference.  BYPASS: the significance-propagation and refinement passes from the fifth
+ * bit-plane on are written as raw bits (T.800 D.6).  RESET: the context states start afresh at
+ * every pass.  TERMALL: the codeword is terminated after every pass.  With RESET and TERMALL
+ * together every pass is an independent codeword segment, which the encoder codes one lane per
+ * pass instead of one lane per code-block.  A styled block's codeword is the concatenation of
+ * its segments; its pass ends (codeword bytes when each pass ended, exact at terminated passes,
+ * J2K_PASS_STRIDE entries per block) locate them. */
+#define J2K_CBLK_BYPASS 1
+#define J2K_CBLK_RESET 2
+#define J2K_CBLK_TERMALL 4
+#define J2K_PASS_STRIDE 92
 typedef struct {
     uint32_t offset;   /* byte offset of this block's codeword in the bytes buffer */
     int32_t length;    /* codeword bytes (0 for an all-zero block) */
@@ -184,6 +198,13 @@ typedef struct {
                             codestream for layers 0..l (non-decreasing; 0 in the last place keeps
                             every pass: a lossless final layer); target_bytes is then unused */
     const size_t* layer_bytes;
+    int cblk_style;      /* J2K_CBLK_* bits (0: none).  Encoding: the code-blocks are coded in that
+                            style (rate control and layers are not combined with a style); the
+                            pass ends come from j2k_encoder_get_pass_ends.  Decoding: the style
+                            the code-blocks were coded in */
+    const uint32_t* pass_ends; /* decoding with a style: the blocks' pass ends, J2K_PASS_STRIDE
+                                  per block in descriptor order, in the memory the descriptors
+                                  are in */
 } j2k_enc_params;
 
 j2k_status j2k_encoder_create(j2k_ctx* ctx, int lossy, int output_dwt_only, j2k_encoder** out);
@@ -217,6 +238,11 @@ j2k_status j2k_encoder_autotune(j2k_encoder* enc, int reps, int* report);
 /* T.800 codestream (SOC..EOC, one tile, LRCP; one quality layer, or the layers asked for) of the
  * last run.  out NULL: size only. */
 j2k_status j2k_encoder_get_codestream(j2k_encoder* enc, uint8_t* out, size_t cap, size_t* len);
+/* Pass ends of the last styled encode (j2k_enc_params.cblk_style != 0): for every code-block in
+ * job order J2K_PASS_STRIDE entries, entry p the codeword bytes when pass p ended (exact where
+ * the style terminates the codeword after pass p; entries past the block's npasses are 0).
+ * ends NULL: *count = the number of entries only.  No reference counterpart. */
+j2k_status j2k_encoder_get_pass_ends(j2k_encoder* enc, uint32_t* ends, size_t cap, size_t* count);
 /* Device-side view of the last run's results (valid until the next run). */
 j2k_status j2k_encoder_device_results(j2k_encoder* enc, const j2k_cb_desc** descs,
                                       const uint8_t** bytes, size_t* count,
@@ -248,6 +274,8 @@ typedef struct {
     const uint8_t* bytes;      /* codewords, descs[i].offset into it */
     size_t nbytes;
     uint8_t* out;              /* host output */
+    int cblk_style;            /* code-block style of the blocks (J2K_CBLK_*) */
+    const uint32_t* pass_ends; /* with a style: J2K_PASS_STRIDE pass ends per block (host) */
 } j2k_decode_item;
 j2k_status j2k_decoder_run_batch(j2k_decoder* dec, const j2k_decode_item* items, int n);
 /* The same from codestreams: each stream's tier-2 runs on a pool of host threads (the first
@@ -258,7 +286,8 @@ j2k_status j2k_decoder_run_codestreams(j2k_decoder* dec, const uint8_t* const* s
 
 /* ---- codestream reading (tier-2 decoding).  No counterpart in the reference, which writes and
  * reads no codestream.  Parses a T.800 codestream of one tile (tile-parts allowed), any number of
- * quality layers, LRCP or RLCP progression, one precinct per resolution, the default code-block style,
+ * quality layers, LRCP or RLCP progression, one precinct per resolution, the default code-block style
+ * or the bypass / reset / per-pass termination styles (see j2k_codestream_pass_ends),
  * reversible (5/3) or irreversible (9/7) transform with no, derived or expounded quantisation,
  * 1 or 3 (with colour transform) 8-bit components: the subset this library writes and the one
  * OpenJPEG writes by default.  SOP/EPH markers are skipped.  Other streams return
@@ -277,6 +306,7 @@ typedef struct {
     int precision;     /* bits per component sample */
     int layers, progression;
     float steps[J2K_MAX_BANDS];  /* per-subband quantiser steps in QCD order (1 when lossless) */
+    int cblk_style;              /* J2K_CBLK_* bits of the code-block style */
 } j2k_stream_info;
 j2k_status j2k_codestream_read(const uint8_t* cs, size_t n, j2k_stream_info* info, j2k_cb_desc* descs,
                                size_t* count, uint8_t* bytes, size_t cap, size_t* used, char* err,
@@ -302,6 +332,13 @@ j2k_status j2k_codestream_info(const uint8_t* cs, size_t n, j2k_stream_info* inf
 j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
                                       j2k_cb_desc* descs, size_t* count, uint8_t* bytes, size_t cap,
                                       size_t* used, char* err, size_t errlen);
+/* The pass ends of the blocks j2k_codestream_read_layers returns (same stream, same max_layers):
+ * J2K_PASS_STRIDE entries per block in job order, for decoding a styled stream
+ * (j2k_enc_params.pass_ends); for an unstyled stream every entry is the block's codeword length.
+ * ends NULL: *count only.  Streams with the bypass, reset, per-pass or predictable termination
+ * styles are read; vertically causal contexts and segmentation symbols are refused. */
+j2k_status j2k_codestream_pass_ends(const uint8_t* cs, size_t n, int max_layers, uint32_t* ends, size_t cap,
+                                    size_t* count, char* err, size_t errlen);
 
 /* ---- differentiable 9/7 (no counterpart in the reference).  n images of w x h float32,
  * planes back to back (pitch w, plane stride w*h), device pointers, T.800 order.  Used with

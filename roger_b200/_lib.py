@@ -30,7 +30,12 @@ assert CB_DESC.itemsize == 24
 class EncParams(C.Structure):
     _fields_ = [("levels", C.c_int), ("cbw", C.c_int), ("cbh", C.c_int), ("order", C.c_int),
                 ("steps", C.c_void_p), ("target_bytes", C.c_size_t), ("layers", C.c_int),
-                ("layer_bytes", C.c_void_p)]
+                ("layer_bytes", C.c_void_p), ("cblk_style", C.c_int), ("pass_ends", C.c_void_p)]
+
+
+# code-block styles (T.800 Table A.19) and the pass-end stride per code-block
+CBLK_BYPASS, CBLK_RESET, CBLK_TERMALL = 1, 2, 4
+PASS_STRIDE = 92
 
 
 J2K_MAX_BANDS = 97
@@ -40,7 +45,7 @@ class StreamInfo(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("ncomp", C.c_int), ("levels", C.c_int), ("cbw", C.c_int),
                 ("cbh", C.c_int), ("lossless", C.c_int), ("mct", C.c_int), ("guard", C.c_int),
                 ("precision", C.c_int), ("layers", C.c_int), ("progression", C.c_int),
-                ("steps", C.c_float * J2K_MAX_BANDS)]
+                ("steps", C.c_float * J2K_MAX_BANDS), ("cblk_style", C.c_int)]
 
 
 class J2KError(RuntimeError):
@@ -85,6 +90,8 @@ SIGS = {
     "j2k_encoder_unmap_dwt_out": (I, [P, P]),
     "j2k_encoder_get_codeblocks": (I, [P, P, C.POINTER(S), P, S, C.POINTER(S)]),
     "j2k_encoder_get_codestream": (I, [P, P, S, C.POINTER(S)]),
+    "j2k_encoder_get_pass_ends": (I, [P, P, S, C.POINTER(S)]),
+    "j2k_codestream_pass_ends": (I, [P, S, I, P, S, C.POINTER(S), P, S]),
     "j2k_encoder_device_results": (I, [P, C.POINTER(P), C.POINTER(P), C.POINTER(S), C.POINTER(S)]),
     "j2k_decoder_create": (I, [P, I, C.POINTER(P)]),
     "j2k_decoder_destroy": (I, [P]),
@@ -131,7 +138,7 @@ class DecodeItem(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("ncomp", C.c_int), ("lossless", C.c_int),
                 ("levels", C.c_int), ("cbw", C.c_int), ("cbh", C.c_int), ("steps", C.c_void_p),
                 ("descs", C.c_void_p), ("count", C.c_size_t), ("bytes", C.c_void_p), ("nbytes", C.c_size_t),
-                ("out", C.c_void_p)]
+                ("out", C.c_void_p), ("cblk_style", C.c_int), ("pass_ends", C.c_void_p)]
 
 
 def exported_symbols():

@@ -18,7 +18,7 @@ __all__ = ["Context", "rgb_to_planar", "planar_to_rgb", "dwt_forward", "dwt_inve
            "codeblock_count", "bpc_encode", "bpc_decode", "OCLEncoder", "OCLDecoder",
            "OCLDWTForward", "OCLDWTRev", "OCLRGBtoPlanar", "OCLBPC", "default_steps", "read_codestream",
            "decode_codestream",
-           "subband_rects", "J2KError"]
+           "read_pass_ends", "subband_rects", "J2KError"]
 
 
 def _ptr(t):
@@ -222,14 +222,19 @@ def bpc_decode(descs, data, w, h, levels, cbw=64, cbh=64, ctx=None, out=None):
 # Reference-shaped classes
 # ---------------------------------------------------------------------------------------------
 
-def _params(levels, cbw, cbh, order, steps, target_bytes=0, layers=None):
+def _params(levels, cbw, cbh, order, steps, target_bytes=0, layers=None, cblk_style=0, pass_ends=None):
     keep, sp = _steps_arg(steps, levels) if steps is not None else (None, None)
     nl, lp = 0, None
     if layers is not None and len(layers) > 1:
         lb = np.ascontiguousarray(np.asarray(layers, np.uint64))
         keep = (keep, lb)
         nl, lp = len(lb), lb.ctypes.data
-    p = L.EncParams(levels, cbw, cbh, order, sp, int(target_bytes), nl, lp)
+    pe = None
+    if pass_ends is not None:
+        pea = np.ascontiguousarray(pass_ends, np.uint32)
+        keep = (keep, pea)
+        pe = pea.ctypes.data
+    p = L.EncParams(levels, cbw, cbh, order, sp, int(target_bytes), nl, lp, int(cblk_style), pe)
     return p, keep
 
 
@@ -290,12 +295,14 @@ class OCLEncoder(OCLEncodeDecode):
                 "blocks_per_warp": rep[3]}
 
     def run_rgb(self, img, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None, target_bytes=0,
-                layers=None):
+                layers=None, cblk_style=0):
         """Interleaved uint8 image, (H, W, C) or (H, W); numpy (host) or CUDA tensor.
         target_bytes > 0 cuts the codestream to at most that many bytes (PCRD-opt rate control:
         bit-plane truncation points of every code-block chosen on their rate-distortion hulls).
         layers: cumulative codestream byte budgets of quality layers 0, 1, ... (non-decreasing;
-        a last entry of 0 keeps every pass, a lossless final layer for 5/3)."""
+        a last entry of 0 keeps every pass, a lossless final layer for 5/3).  cblk_style:
+        code-block style bits (CBLK_BYPASS | CBLK_RESET | CBLK_TERMALL; not with rate control);
+        with RESET and TERMALL the passes of a block are coded in parallel."""
         if isinstance(img, torch.Tensor) and img.is_cuda:
             t = img.contiguous()
             ptr, on_dev = t.data_ptr(), 1
@@ -308,13 +315,25 @@ class OCLEncoder(OCLEncodeDecode):
             hgt, wid = a.shape[0], a.shape[1]
             nc = 1 if a.ndim == 2 else a.shape[2]
             keep_img = a
-        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes, layers)
+        p, keep = _params(levels, cbw, cbh, order, steps, target_bytes, layers, cblk_style)
         hh = self.ctx._bind()
         check(lib().j2k_encoder_run_interleaved(self.h, C.c_void_p(ptr), on_dev, wid * nc, nc, wid, hgt,
                                                 C.byref(p)), hh)
         del keep_img
         self.w, self.h_, self.ncomp, self.levels = wid, hgt, nc, levels
+        self.cblk_style = int(cblk_style)
         return self
+
+    def get_pass_ends(self):
+        """Pass ends of the last styled run: (count, PASS_STRIDE) uint32, row i for code-block i
+        (job order), entry p the codeword bytes when pass p ended (exact where the style
+        terminates the codeword after it)."""
+        n = C.c_size_t()
+        check(lib().j2k_encoder_get_pass_ends(self.h, None, 0, C.byref(n)), self.ctx.h)
+        out = np.zeros(n.value, np.uint32)
+        check(lib().j2k_encoder_get_pass_ends(self.h, out.ctypes.data_as(C.c_void_p), out.size, C.byref(n)),
+              self.ctx.h)
+        return out.reshape(-1, L.PASS_STRIDE)
 
     def map_dwt_out(self):
         """Host copy of the coefficient planes: (ncomp, H, W) int32 (float32 for lossy DWT-only)."""
@@ -383,12 +402,17 @@ class OCLDecoder(OCLEncodeDecode):
         except Exception:
             pass
 
-    def run(self, descs, data, w, h, ncomp, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None):
-        """descs/data as returned by OCLEncoder.get_codeblocks (host).  Returns (H, W, C) uint8."""
+    def run(self, descs, data, w, h, ncomp, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None,
+            cblk_style=0, pass_ends=None):
+        """descs/data as returned by OCLEncoder.get_codeblocks (host).  Returns (H, W, C) uint8.
+        Blocks coded with a code-block style need cblk_style and their pass ends
+        (OCLEncoder.get_pass_ends, read_pass_ends)."""
         descs = np.ascontiguousarray(descs)
         data = np.ascontiguousarray(data, np.uint8)
         out = np.zeros((h, w, ncomp), np.uint8)
-        p, keep = _params(levels, cbw, cbh, order, steps)
+        if cblk_style and pass_ends is None:
+            raise ValueError("a styled decode needs the pass ends")
+        p, keep = _params(levels, cbw, cbh, order, steps, cblk_style=cblk_style, pass_ends=pass_ends)
         hh = self.ctx._bind()
         check(lib().j2k_decoder_run_codeblocks(self.h, descs.ctypes.data_as(C.c_void_p),
                                                data.ctypes.data_as(C.c_void_p), data.size, 0, ncomp,
@@ -422,9 +446,27 @@ def read_codestream(cs, max_layers=0):
     nb = 3 * info.levels + 1
     d = dict(w=info.w, h=info.h, ncomp=info.ncomp, levels=info.levels, cbw=info.cbw, cbh=info.cbh,
              lossless=bool(info.lossless), mct=info.mct, guard=info.guard, precision=info.precision,
-             layers=info.layers, progression=info.progression,
+             layers=info.layers, progression=info.progression, cblk_style=info.cblk_style,
              steps=np.array(info.steps[:nb], np.float32))
     return d, descs, data[:used.value]
+
+
+def read_pass_ends(cs, max_layers=0):
+    """Pass ends of the blocks read_codestream returns: (count, PASS_STRIDE) uint32 (for a
+    styled stream's decode; an unstyled stream gives each block's codeword length)."""
+    buf = np.frombuffer(bytes(cs), np.uint8)
+    n = C.c_size_t()
+    err = C.create_string_buffer(256)
+    s = lib().j2k_codestream_pass_ends(buf.ctypes.data_as(C.c_void_p), buf.size, int(max_layers), None, 0,
+                                       C.byref(n), err, 256)
+    if s != 0:
+        raise L.J2KError(s, err.value.decode())
+    out = np.zeros(n.value, np.uint32)
+    s = lib().j2k_codestream_pass_ends(buf.ctypes.data_as(C.c_void_p), buf.size, int(max_layers),
+                                       out.ctypes.data_as(C.c_void_p), out.size, C.byref(n), err, 256)
+    if s != 0:
+        raise L.J2KError(s, err.value.decode())
+    return out.reshape(-1, L.PASS_STRIDE)
 
 
 def write_codestream(w, h, ncomp, levels, descs, data, cbw=64, cbh=64, lossless=True, steps=None, layers=None):
@@ -460,9 +502,11 @@ def decode_codestream(cs, ctx=None, max_layers=0):
     colour transform on the device.  max_layers > 0 decodes only the first quality layers.
     Returns (H, W, C) uint8."""
     info, descs, data = read_codestream(cs, max_layers)
+    pe = read_pass_ends(cs, max_layers) if info["cblk_style"] else None
     dec = OCLDecoder(ctx=ctx, lossy=not info["lossless"])
     return dec.run(descs, data, info["w"], info["h"], info["ncomp"], levels=info["levels"], cbw=info["cbw"],
-                   cbh=info["cbh"], steps=None if info["lossless"] else info["steps"])
+                   cbh=info["cbh"], steps=None if info["lossless"] else info["steps"],
+                   cblk_style=info["cblk_style"], pass_ends=pe)
 
 
 def codestream_info(cs):

@@ -122,6 +122,8 @@ struct j2k_encoder {
     bool packed_ok = false;  // the packed codewords of the current result are on the device
     size_t packed_total = 0;
     size_t target_bytes = 0;  // rate control: codestream budget (0 = keep every pass)
+    int style = 0;            // code-block style of the last run (J2K_CBLK_*)
+    DevBuf pass_ends;         // styled runs: J2K_PASS_STRIDE pass ends per job
     // quality layers: cumulative codestream budgets (0 in the last place: every pass), and per
     // layer l and block i the passes / codeword bytes kept after that layer (lay_*[l * n + i])
     std::vector<size_t> layer_budget;
@@ -134,7 +136,7 @@ struct j2k_encoder {
 struct j2k_decoder {
     j2k_ctx* ctx = nullptr;
     int lossy = 0;
-    DevBuf descs, bytes, coef, planes, out, jobs;
+    DevBuf descs, bytes, coef, planes, out, jobs, pass_ends, job_style;
     std::vector<j2k_cb_job> hjobs;
     size_t job_key[6] = {0, 0, 0, 0, 0, 0};
 };
@@ -170,6 +172,8 @@ static j2k_status check_params(j2k_ctx* ctx, const j2k_enc_params* p, size_t w, 
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "bad order");
     if (w == 0 || h == 0 || w > 65535 || h > 65535)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "image size must be in 1..65535");
+    if (p && (p->cblk_style < 0 || p->cblk_style > 7))
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "code-block style: BYPASS, RESET and TERMALL bits only");
     return J2K_OK;
 }
 
@@ -306,14 +310,20 @@ static j2k_status run_tier1(j2k_encoder* e) {
             pb = (uint32_t*)e->rate_pb.p;
             dist = (double*)e->rate_dist.p;
         }
+        uint32_t* pe = nullptr;
+        if (e->style) {
+            J2K_TRY(e->pass_ends.ensure(ctx, e->njobs * J2K_PASS_STRIDE * 4 + 16));
+            pe = (uint32_t*)e->pass_ends.p;
+        }
         J2K_TRY(j2k_t1_encode_jobs(ctx, (const int32_t*)e->coef.p, (const j2k_cb_job*)e->jobs.p,
                                    e->njobs, (j2k_cb_desc*)e->descs.p, (uint8_t*)e->bytes.p,
-                                   e->njobs * e->sym_cap, nullptr, ctx->stream, pb, dist));
+                                   e->njobs * e->sym_cap, nullptr, ctx->stream, pb, dist, e->style, pe));
         j2k_status s = j2k_read_device_error(ctx);
         if (s == J2K_OK) return (e->target_bytes || !e->layer_budget.empty()) ? rate_control(e) : J2K_OK;
         if (s != J2K_ERR_CAPACITY) return s;
         // grow whichever capacity overflowed and retry
         if (ctx->err.find("symbol") != std::string::npos) e->sym_cap = align16(e->sym_cap * 2);
+        else if (ctx->err.find("segment") != std::string::npos) ctx->t1_seg_factor *= 2;
         else e->cap = align16(e->cap * 2);
     }
     return j2k_fail(ctx, J2K_ERR_CAPACITY, "tier-1 capacities kept overflowing");
@@ -445,6 +455,9 @@ static j2k_status setup_run(j2k_encoder* e, int ncomp, size_t w, size_t h, const
     if (ncomp != 1 && ncomp != 3)
         return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "encoder supports 1 or 3 components");
     e->target_bytes = p ? p->target_bytes : 0;
+    e->style = p ? p->cblk_style : 0;
+    if (e->style && (e->target_bytes || (p && p->layers > 1)))
+        return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "rate control and layers are not combined with a code-block style");
     e->layer_budget.clear();
     e->lay_np.clear();
     e->lay_len.clear();
@@ -672,9 +685,16 @@ j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, 
     std::vector<j2k_cb_desc> d(count);
     std::vector<uint8_t> b(total + 1);
     J2K_TRY(j2k_encoder_get_codeblocks(e, d.data(), &count, b.data(), b.size(), &total));
+    std::vector<uint32_t> pe;
+    if (e->style) {  // the segments of styled blocks are located by their pass ends
+        pe.resize(count * J2K_PASS_STRIDE);
+        J2K_CUDA(ctx, cudaMemcpyAsync(pe.data(), e->pass_ends.p, pe.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     std::vector<j2k_t2_block> blocks(count);
     for (size_t i = 0; i < count; ++i)
-        blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, b.data() + d[i].offset};
+        blocks[i] = j2k_t2_block{d[i].numbps, d[i].npasses, d[i].length, b.data() + d[i].offset,
+                                 e->style ? pe.data() + i * J2K_PASS_STRIDE : nullptr};
     const int L = (int)(e->lay_np.size() / std::max<size_t>(count, 1));
     std::vector<uint8_t> cs =
         L > 1 && e->lay_np.size() == (size_t)L * count
@@ -682,11 +702,27 @@ j2k_status j2k_encoder_get_codestream(j2k_encoder* e, uint8_t* out, size_t cap, 
                                   e->mct != J2K_MCT_NONE, e->steps.data(), blocks, L, e->lay_np.data(),
                                   e->lay_len.data())
             : j2k_t2_write(e->w, e->h, e->ncomp, e->levels, e->cbw, e->cbh, !e->lossy, e->mct != J2K_MCT_NONE,
-                           e->steps.data(), blocks);
+                           e->steps.data(), blocks, e->style);
     *len = cs.size();
     if (!out) return J2K_OK;
     if (cap < cs.size()) return j2k_fail(ctx, J2K_ERR_CAPACITY, "codestream buffer too small");
     std::memcpy(out, cs.data(), cs.size());
+    return J2K_OK;
+    J2K_API_END
+}
+
+j2k_status j2k_encoder_get_pass_ends(j2k_encoder* e, uint32_t* ends, size_t cap, size_t* count) {
+    J2K_API_BEGIN
+    if (!e || !count) return J2K_ERR_INVALID_ARG;
+    j2k_ctx* ctx = e->ctx;
+    if (!e->have_result || e->dwt_only || !e->style)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "no styled tier-1 result");
+    *count = e->njobs * J2K_PASS_STRIDE;
+    if (!ends) return J2K_OK;
+    if (cap < *count) return j2k_fail(ctx, J2K_ERR_CAPACITY, "pass-end buffer too small");
+    cudaSetDevice(ctx->device);
+    J2K_CUDA(ctx, cudaMemcpyAsync(ends, e->pass_ends.p, *count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return J2K_OK;
     J2K_API_END
 }
@@ -721,7 +757,8 @@ j2k_status j2k_decoder_destroy(j2k_decoder* d) {
     if (!d) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(d->ctx->device);
     cudaStreamSynchronize(d->ctx->stream);
-    for (DevBuf* b : {&d->descs, &d->bytes, &d->coef, &d->planes, &d->out, &d->jobs}) b->release();
+    for (DevBuf* b : {&d->descs, &d->bytes, &d->coef, &d->planes, &d->out, &d->jobs, &d->pass_ends, &d->job_style})
+        b->release();
     delete d;
     return J2K_OK;
     J2K_API_END
@@ -738,6 +775,7 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
     std::vector<size_t> coef_off(n), out_off(n + 1, 0), job0(n + 1, 0), byte0(n + 1, 0);
     std::vector<int> lv(n), cbw(n), cbh(n);
     size_t coef_total = 0, desc_total = 0, max_ll0 = 16, max_ll1 = 16;
+    bool any_style = false;
     for (int k = 0; k < n; ++k) {
         const j2k_decode_item& it = items[k];
         if (!it.descs || (!it.bytes && it.nbytes) || !it.out)
@@ -759,6 +797,9 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
         if (it.count != job0[k + 1] - job0[k])
             return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "item " + std::to_string(k) + ": descriptor count does not "
                                                       "match the image's code-blocks");
+        if (it.cblk_style < 0 || it.cblk_style > 7 || (it.cblk_style && !it.pass_ends))
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "item " + std::to_string(k) + ": bad code-block style or "
+                                                      "no pass ends");
         for (size_t i = 0; i < it.count; ++i) {
             const j2k_cb_desc& q = it.descs[i];
             if (q.length < 0 || (size_t)q.offset + (size_t)q.length > it.nbytes || q.numbps > 31 ||
@@ -766,6 +807,7 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
                 return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "item " + std::to_string(k) + ": code-block descriptor " +
                                                               std::to_string(i) + " is out of range");
         }
+        any_style |= it.cblk_style != 0;
         coef_total += (size_t)it.w * it.h * it.ncomp;
         byte0[k + 1] = byte0[k] + it.nbytes;
         out_off[k + 1] = out_off[k] + (size_t)it.w * it.h * it.ncomp;
@@ -804,9 +846,36 @@ j2k_status j2k_decoder_run_batch(j2k_decoder* d, const j2k_decode_item* items, i
     J2K_CUDA(ctx, cudaMemcpyAsync(d->jobs.p, jobs.data(), jobs.size() * sizeof(j2k_cb_job), cudaMemcpyHostToDevice,
                                   ctx->stream));
     J2K_TRY(j2k_clear_device_error(ctx));
+    const uint32_t* dpe = nullptr;
+    const uint8_t* djs = nullptr;
+    if (any_style) {
+        // a style per job, and pass ends for every job (an unstyled block: one segment of its
+        // whole codeword, the end of its last pass)
+        const size_t nj = jobs.size();
+        std::vector<uint32_t> pe(nj * J2K_PASS_STRIDE, 0);
+        std::vector<uint8_t> js(nj, 0);
+        for (int k = 0; k < n; ++k) {
+            const j2k_decode_item& it = items[k];
+            for (size_t i = 0; i < it.count; ++i) {
+                uint32_t* row = pe.data() + (job0[k] + i) * J2K_PASS_STRIDE;
+                js[job0[k] + i] = (uint8_t)it.cblk_style;
+                if (it.cblk_style) std::memcpy(row, it.pass_ends + i * J2K_PASS_STRIDE, J2K_PASS_STRIDE * 4);
+                else
+                    for (int q = 0; q < J2K_PASS_STRIDE; ++q) row[q] = (uint32_t)std::max(it.descs[i].length, 0);
+            }
+        }
+        J2K_TRY(d->pass_ends.ensure(ctx, pe.size() * 4 + 16));
+        J2K_TRY(d->job_style.ensure(ctx, nj + 16));
+        J2K_CUDA(ctx, cudaMemcpyAsync(d->pass_ends.p, pe.data(), pe.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        J2K_CUDA(ctx, cudaMemcpyAsync(d->job_style.p, js.data(), nj, cudaMemcpyHostToDevice, ctx->stream));
+        J2K_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the host vectors go out of scope
+        dpe = (const uint32_t*)d->pass_ends.p;
+        djs = (const uint8_t*)d->job_style.p;
+    }
     // tier-1 of every block of every image in one launch
     J2K_TRY(j2k_t1_decode_jobs(ctx, (const j2k_cb_desc*)d->descs.p, (const uint8_t*)d->bytes.p,
-                               (const j2k_cb_job*)d->jobs.p, jobs.size(), (int32_t*)d->coef.p, ctx->stream));
+                               (const j2k_cb_job*)d->jobs.p, jobs.size(), (int32_t*)d->coef.p, ctx->stream, 0, dpe,
+                               djs));
     void* ll0 = j2k_scratch(ctx, SCR_LL0, max_ll0);
     void* ll1 = j2k_scratch(ctx, SCR_LL1, max_ll1);
     if (!ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
@@ -847,6 +916,7 @@ j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* str
     std::vector<j2k_stream_info> info(n);
     std::vector<std::vector<j2k_cb_desc>> descs(n);
     std::vector<std::vector<uint8_t>> bytes(n);
+    std::vector<std::vector<uint32_t>> ends(n);
     std::vector<j2k_status> st(n, J2K_OK);
     std::vector<std::string> msg(n);
     const int nt = (int)std::min<unsigned>((unsigned)n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
@@ -859,7 +929,7 @@ j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* str
             }
             try {
                 st[k] = j2k_t2_parse_packed(streams[k], sizes[k], max_layers, &info[k], &descs[k], &bytes[k],
-                                            &msg[k]);
+                                            &msg[k], &ends[k]);
             } catch (...) {  // a host allocation failed
                 st[k] = J2K_ERR_OUT_OF_MEMORY;
             }
@@ -873,7 +943,8 @@ j2k_status j2k_decoder_run_codestreams(j2k_decoder* d, const uint8_t* const* str
         if (I.precision != 8) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "stream " + std::to_string(k) + ": precision");
         items[k] = j2k_decode_item{I.w, I.h, I.ncomp, I.lossless, I.levels, I.cbw, I.cbh,
                                    I.lossless ? nullptr : I.steps, descs[k].data(), descs[k].size(),
-                                   bytes[k].data(), bytes[k].size(), outs[k]};
+                                   bytes[k].data(), bytes[k].size(), outs[k], I.cblk_style,
+                                   I.cblk_style ? ends[k].data() : nullptr};
     }
     return j2k_decoder_run_batch(d, items.data(), n);
     J2K_API_END
@@ -896,6 +967,15 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
     J2K_TRY(prepare_jobs(ctx, d->hjobs, d->jobs, d->job_key, w, h, ncomp, levels, cbw, cbh, &njobs));
     const j2k_cb_desc* dd = descs;
     const uint8_t* db = bytes;
+    const int style = p ? p->cblk_style : 0;
+    const uint32_t* dpe = style ? p->pass_ends : nullptr;
+    if (style && !dpe) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "a styled decode needs the pass ends");
+    if (style && !on_device) {
+        J2K_TRY(d->pass_ends.ensure(ctx, njobs * J2K_PASS_STRIDE * 4 + 16));
+        J2K_CUDA(ctx, cudaMemcpyAsync(d->pass_ends.p, dpe, njobs * J2K_PASS_STRIDE * 4, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        dpe = (const uint32_t*)d->pass_ends.p;
+    }
     if (!on_device) {
         // host descriptors are validated before any kernel reads through them
         for (size_t i = 0; i < njobs; ++i) {
@@ -917,7 +997,8 @@ j2k_status j2k_decoder_run_codeblocks(j2k_decoder* d, const j2k_cb_desc* descs, 
     J2K_TRY(d->coef.ensure(ctx, n * 4 * ncomp));
     J2K_TRY(d->planes.ensure(ctx, n * 4 * ncomp));
     J2K_TRY(j2k_clear_device_error(ctx));
-    J2K_TRY(j2k_t1_decode_jobs(ctx, dd, db, (const j2k_cb_job*)d->jobs.p, njobs, (int32_t*)d->coef.p, ctx->stream));
+    J2K_TRY(j2k_t1_decode_jobs(ctx, dd, db, (const j2k_cb_job*)d->jobs.p, njobs, (int32_t*)d->coef.p, ctx->stream,
+                               style, dpe));
     std::vector<float> steps;
     if (d->lossy) {
         if (p && p->steps) steps.assign(p->steps, p->steps + 3 * levels + 1);

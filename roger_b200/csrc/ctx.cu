@@ -81,6 +81,8 @@ j2k_status j2k_read_device_error(j2k_ctx* ctx) {
             return j2k_fail(ctx, J2K_ERR_TIMEOUT, "bounded device wait expired");
         case J2K_DEVERR_PLANES:
             return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "more than 31 magnitude bit-planes");
+        case J2K_DEVERR_SEG_CAPACITY:
+            return j2k_fail(ctx, J2K_ERR_CAPACITY, "a coding-pass segment outgrew its slot");
         default: return j2k_fail(ctx, J2K_ERR_DEVICE, "device error word " + std::to_string(v));
     }
 }
@@ -270,6 +272,10 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
     }
     if (key == J2K_TUNE_DWT_REG) {
         ctx->dwt_reg = value != 0;
+        return J2K_OK;
+    }
+    if (key == J2K_TUNE_DWT_TMA) {
+        ctx->dwt_tma = value != 0;
         return J2K_OK;
     }
     if (key == J2K_TUNE_MQ_TIER) {

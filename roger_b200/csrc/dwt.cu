@@ -19,6 +19,9 @@
 // HBM roofline per level: read c*n + write c*n bytes (c = 4), n = samples of the level.
 #include <algorithm>
 
+#include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's entry points)
+#include <cudaTypedefs.h>
+
 #include "lift.cuh"
 
 namespace {
@@ -208,75 +211,17 @@ dwt_fwd_batched(const j2k_dwt_level_desc* __restrict__ descs, const uint32_t* __
 //   * subbands are written straight from registers (8-byte vectors when aligned).
 // Same arithmetic, operation order and rounding as dwt_fwd_level, so the outputs are identical.
 
-// REG: each thread loads its column of the strip straight from global memory into registers
-// (coalesced 4-byte loads, all NY in flight at once), so the strip is never staged in shared
-// memory; only the FTH vertically lifted rows go through shared memory to the horizontal pass.
-template <int KERN, typename TD, bool QUANT, bool QLL, int FTH, bool REG>
-__global__ void __launch_bounds__(256, REG ? (FTH == 16 ? 6 : 4) : ((KERN == 53 && FTH == 16) ? 8 : 6))
-dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
-             typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
-             Steps4 st, int vec_out, ZStride z) {
+// Step 3 of the fast forward level: horizontal lifting of the FTH vertically lifted rows held in
+// shared memory (strip row r at s[r - RO]), 8 samples per lane (tile columns 8*lane ..
+// 8*lane+7), and the writes of the four subbands (dead-zone indices when QUANT) straight from
+// registers.  Shared by the register-load and the TMA-staged forms of the level kernel.
+template <int KERN, typename TD, bool QUANT, bool QLL, int FTH, int RO>
+__device__ __forceinline__ void fwd_fast_rows(typename KT<KERN>::T (*s)[FNX], int x0, int y0, int w, int h,
+                                              typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch,
+                                              TD* __restrict__ dst, size_t dpitch, Steps4 st, int vec_out) {
     using T = typename KT<KERN>::T;
-    src += blockIdx.z * z.src;
-    dst += blockIdx.z * z.dst;
-    ll_dst += blockIdx.z * z.ll;
-    constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
-    constexpr int SR = REG ? FTH : NY, RO = REG ? HV : 0;  // shared rows; strip row r at s[r - RO]
-    __shared__ __align__(16) T s[SR][FNX];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
-    const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * FTH;
-    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
-    T c[NY];
-    if constexpr (REG) {
-        // 1. column t of the strip, rows y0-HV .. y0+FTH+HV-1 (mirrored at the image edges)
-        const bool inner_y = (y0 - HV >= 0) && (y0 + FTH + HV <= h);
-        const int gx = x0 - 4 + t;
-        const T* colp = src + (inner_x ? gx : mirror(gx, w));
-#pragma unroll
-        for (int r = 0; r < NY; ++r) {
-            const int gy = inner_y ? y0 - HV + r : mirror(y0 - HV + r, h);
-            c[r] = __ldg(colp + (size_t)gy * spitch);
-        }
-    } else {
-        // 1. load the strip: every copy of the CTA in flight at once (cp.async, no register staging)
-        for (int r = warp; r < NY; r += 8) {
-            const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
-#pragma unroll
-            for (int q2 = 0; q2 < 2; ++q2) {
-                const int q = lane + 32 * q2;
-                const int gx = x0 - 4 + 4 * q;
-                if (inner_x) {
-                    cp_async16(&s[r][4 * q], row + gx);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) cp_async4(&s[r][4 * q + k], row + mirror(gx + k, w));
-                }
-            }
-        }
-        cp_async_wait_all();
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < NY; ++r) c[r] = s[r][t];
-        __syncthreads();
-    }
-    // 2. vertical lifting of column t in registers
-    if (h > 1) {
-#pragma unroll
-        for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
-            const int par = 1 - (k & 1);
-#pragma unroll
-            for (int r = k + 1; r < NY - k - 1; ++r)
-                if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
-        }
-    }
-#pragma unroll
-    for (int r = HV; r < HV + FTH; ++r) {
-        T v = c[r];
-        if (KERN == 97 && h > 1) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
-        s[r - RO][t] = v;
-    }
-    __syncthreads();
-    // 3. horizontal lifting per row, 8 samples per lane (tile columns 8*lane .. 8*lane+7)
+    constexpr int HV = KT<KERN>::H;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
     const bool doh = w > 1;
 #pragma unroll
@@ -353,6 +298,201 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
                 }
             }
         }
+    }
+}
+
+// REG: each thread loads its column of the strip straight from global memory into registers
+// (coalesced 4-byte loads, all NY in flight at once), so the strip is never staged in shared
+// memory; only the FTH vertically lifted rows go through shared memory to the horizontal pass.
+template <int KERN, typename TD, bool QUANT, bool QLL, int FTH, bool REG>
+__global__ void __launch_bounds__(256, REG ? (FTH == 16 ? 6 : 4) : ((KERN == 53 && FTH == 16) ? 8 : 6))
+dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w, int h,
+             typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
+             Steps4 st, int vec_out, ZStride z) {
+    using T = typename KT<KERN>::T;
+    griddep_launch_dependents();
+    griddep_wait();  // a level launched as a dependent reads the previous level's LL band
+    src += blockIdx.z * z.src;
+    dst += blockIdx.z * z.dst;
+    ll_dst += blockIdx.z * z.ll;
+    constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
+    constexpr int SR = REG ? FTH : NY, RO = REG ? HV : 0;  // shared rows; strip row r at s[r - RO]
+    __shared__ __align__(16) T s[SR][FNX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
+    const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * FTH;
+    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
+    T c[NY];
+    if constexpr (REG) {
+        // 1. column t of the strip, rows y0-HV .. y0+FTH+HV-1 (mirrored at the image edges)
+        const bool inner_y = (y0 - HV >= 0) && (y0 + FTH + HV <= h);
+        const int gx = x0 - 4 + t;
+        const T* colp = src + (inner_x ? gx : mirror(gx, w));
+#pragma unroll
+        for (int r = 0; r < NY; ++r) {
+            const int gy = inner_y ? y0 - HV + r : mirror(y0 - HV + r, h);
+            c[r] = __ldg(colp + (size_t)gy * spitch);
+        }
+    } else {
+        // 1. load the strip: every copy of the CTA in flight at once (cp.async, no register staging)
+        for (int r = warp; r < NY; r += 8) {
+            const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
+#pragma unroll
+            for (int q2 = 0; q2 < 2; ++q2) {
+                const int q = lane + 32 * q2;
+                const int gx = x0 - 4 + 4 * q;
+                if (inner_x) {
+                    cp_async16(&s[r][4 * q], row + gx);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) cp_async4(&s[r][4 * q + k], row + mirror(gx + k, w));
+                }
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NY; ++r) c[r] = s[r][t];
+        __syncthreads();
+    }
+    // 2. vertical lifting of column t in registers
+    if (h > 1) {
+#pragma unroll
+        for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+            const int par = 1 - (k & 1);
+#pragma unroll
+            for (int r = k + 1; r < NY - k - 1; ++r)
+                if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
+        }
+    }
+#pragma unroll
+    for (int r = HV; r < HV + FTH; ++r) {
+        T v = c[r];
+        if (KERN == 97 && h > 1) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
+        s[r - RO][t] = v;
+    }
+    __syncthreads();
+    // 3. horizontal lifting and the subband writes
+    fwd_fast_rows<KERN, TD, QUANT, QLL, FTH, RO>(s, x0, y0, w, h, ll_dst, llpitch, dst, dpitch, st, vec_out);
+}
+
+// ---- TMA-staged forward level -----------------------------------------------------------------
+// Persistent CTAs walk the tiles (248 output columns x 16 rows of one plane) in a fixed order.
+// A tile's strip (256 columns x 16 + 2*HV rows, halo included) comes into shared memory by one
+// tensor copy (cp.async.bulk.tensor, TMA) that one thread issues, two stages deep: the next
+// tile's copy is in flight while the current tile is lifted.  Strip samples outside the plane
+// arrive as zeros and are never used: every thread reads its column through the mirror map
+// (whole-sample symmetric extension), and the mirrored sample of every row and column an output
+// depends on lies inside the strip.  Vertical lifting then runs per column in registers and the
+// horizontal pass is fwd_fast_rows, as in dwt_fwd_fast, so the outputs are identical.  No
+// multicast: each copy reads this GPU's plane into this CTA's shared memory.
+constexpr int kTmaTh = 16;
+
+template <int KERN>
+struct TmaStrip {
+    static constexpr int NY = kTmaTh + 2 * KT<KERN>::H;
+    static constexpr int BYTES = NY * FNX * 4;
+    static constexpr int SMEM = 2 * BYTES + kTmaTh * FNX * 4;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <int KERN, typename TD, bool QUANT, bool QLL>
+__global__ void __launch_bounds__(256)
+dwt_fwd_tma(const __grid_constant__ CUtensorMap tmap, int w, int h, int nz, int tiles_x, int tiles_y,
+            typename KT<KERN>::T* __restrict__ ll_dst, size_t llpitch, TD* __restrict__ dst, size_t dpitch,
+            Steps4 st, int vec_out, ZStride z, uint32_t* __restrict__ err) {
+    using T = typename KT<KERN>::T;
+    constexpr int HV = KT<KERN>::H, NY = TmaStrip<KERN>::NY;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    T(*stg)[NY][FNX] = reinterpret_cast<T(*)[NY][FNX]>(dsm);                             // [2][NY][FNX]
+    T(*s)[FNX] = reinterpret_cast<T(*)[FNX]>(dsm + 2 * TmaStrip<KERN>::BYTES);             // [16][FNX]
+    __shared__ __align__(8) uint64_t bar[2];
+    const int t = threadIdx.x;
+    const int ntiles = tiles_x * tiles_y * nz;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    griddep_launch_dependents();
+    griddep_wait();  // a level launched as a dependent reads the previous level's LL band
+    auto issue = [&](int tile, int stage) {
+        const int tx = tile % tiles_x, rest = tile / tiles_x;
+        const int ty = rest % tiles_y, tz = rest / tiles_y;
+        const int x = tx * FTW - 4, y = ty * kTmaTh - HV;  // x a multiple of 4: 16-byte aligned
+        const uint32_t b = smem_u32(&bar[stage]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
+                     "r"((uint32_t)TmaStrip<KERN>::BYTES)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+            "[%5];" ::"r"(smem_u32(&stg[stage][0][0])),
+            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(x), "r"(y), "r"(tz), "r"(b)
+            : "memory");
+    };
+    if (t == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int stage = it & 1;
+        if (t == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
+        // this tile's strip: wait on its barrier's phase (bounded; a copy that never lands
+        // sets the timeout error and the CTA leaves)
+        auto wait_bar = [&](int sg, uint32_t par) -> bool {
+            const uint32_t b = smem_u32(&bar[sg]);
+            uint32_t ok = 0;
+            for (int spin = 0; spin < (1 << 22) && !ok; ++spin)
+                asm volatile(
+                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                    : "=r"(ok)
+                    : "r"(b), "r"(par)
+                    : "memory");
+            return ok != 0;
+        };
+        if (__syncthreads_or(!wait_bar(stage, (uint32_t)(it >> 1) & 1u))) {
+            // the whole CTA leaves together; first the copy of the next tile, if one was
+            // issued, is waited for (bounded), so that nothing lands after the CTA is gone
+            if (t == 0) {
+                atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_TIMEOUT);
+                if (tile + (int)gridDim.x < ntiles) wait_bar(stage ^ 1, (uint32_t)((it + 1) >> 1) & 1u);
+            }
+            return;
+        }
+        const int tx = tile % tiles_x, rest = tile / tiles_x;
+        const int ty = rest % tiles_y, tz = rest / tiles_y;
+        const int x0 = tx * FTW, y0 = ty * kTmaTh;
+        // 1. column t of the strip, through the mirror map at the plane's edges
+        int sx = mirror(x0 - 4 + t, w) - (x0 - 4);
+        sx = min(max(sx, 0), FNX - 1);  // columns no output depends on: any sample
+        const bool inner_y = (y0 - HV >= 0) && (y0 + kTmaTh + HV <= h);
+        T c[NY];
+#pragma unroll
+        for (int r = 0; r < NY; ++r) {
+            int sy = r;
+            if (!inner_y) sy = min(max(mirror(y0 - HV + r, h) - (y0 - HV), 0), NY - 1);
+            c[r] = stg[stage][sy][sx];
+        }
+        __syncthreads();  // the stage is free for the copy after next, and s for this tile
+        // 2. vertical lifting of column t in registers
+        if (h > 1) {
+#pragma unroll
+            for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+                const int par = 1 - (k & 1);
+#pragma unroll
+                for (int r = k + 1; r < NY - k - 1; ++r)
+                    if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
+            }
+        }
+#pragma unroll
+        for (int r = HV; r < HV + kTmaTh; ++r) {
+            T v = c[r];
+            if (KERN == 97 && h > 1) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
+            s[r - HV][t] = v;
+        }
+        __syncthreads();
+        // 3. horizontal lifting and the subband writes
+        fwd_fast_rows<KERN, TD, QUANT, QLL, kTmaTh, HV>(s, x0, y0, w, h, ll_dst + tz * z.ll, llpitch,
+                                                        dst + tz * z.dst, dpitch, st, vec_out);
     }
 }
 
@@ -585,6 +725,64 @@ __global__ void copy_plane_deq(const TI* __restrict__ in, size_t ip, TO* __restr
     else out[(size_t)y * op + x] = (TO)v;
 }
 
+// cuTensorMapEncodeTiled through the runtime (no link dependency on the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+        return (PFN_cuTensorMapEncodeTiled_v12000)f;
+    }();
+    return fn;
+}
+
+// One forward level by the TMA-staged kernel: n planes of w x h at src (pitch and plane stride
+// in elements, both multiples of 4 so that rows and planes start on 16-byte boundaries).
+template <int KERN, typename TD, bool QUANT, bool QLL>
+static j2k_status launch_fwd_tma(j2k_ctx* ctx, const void* src, size_t spitch, size_t src_z, int w, int h, int n,
+                                 typename KT<KERN>::T* lld, size_t llp, TD* out, size_t out_pitch, Steps4 st, int vec,
+                                 ZStride zs, cudaStream_t stream, bool pdl) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "no tensor-map encoder in this driver");
+    CUtensorMap tm;
+    const cuuint64_t dims[3] = {(cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {(cuuint64_t)spitch * 4, (cuuint64_t)(n > 1 ? src_z : spitch * h) * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)FNX, (cuuint32_t)TmaStrip<KERN>::NY, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(&tm, KERN == 53 ? CU_TENSOR_MAP_DATA_TYPE_INT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                           const_cast<void*>(src), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return j2k_fail(ctx, J2K_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    auto kern = dwt_fwd_tma<KERN, TD, QUANT, QLL>;
+    constexpr int smem = TmaStrip<KERN>::SMEM;
+    static int per_sm = 0;  // resident CTAs per SM of this instantiation (set once)
+    if (per_sm == 0) {
+        J2K_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int v = 0;
+        J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, 256, smem));
+        per_sm = std::max(v, 1);
+    }
+    const int tiles_x = (w + FTW - 1) / FTW, tiles_y = (h + kTmaTh - 1) / kTmaTh;
+    const long ntiles = (long)tiles_x * tiles_y * n;
+    const int grid = (int)std::min<long>(ntiles, (long)per_sm * ctx->sm_count);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    J2K_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, tm, w, h, n, tiles_x, tiles_y, lld, llp, out, out_pitch, st, vec, zs,
+                                     ctx->d_err));
+    return J2K_OK;
+}
+
 template <int KERN, int ORDER, int TW, int TH>
 j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, size_t out_pitch,
                       int w, int h, int levels, const float* steps, void* ll0, void* ll1,
@@ -650,7 +848,21 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
                 src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, vec, zs);                        \
         }                                                                                                \
     } while (0)
-            if (ctx && ctx->dwt_pipe && n == 1) {
+            const bool tma_ok = ctx && ctx->dwt_tma && (n == 1 || (src_z & 3) == 0) && cw >= 16;
+            if (tma_ok) {
+                const bool pdl = k > 0;
+                if (quant && last)
+                    J2K_TRY((launch_fwd_tma<KERN, int32_t, true, true>(ctx, src, spitch, src_z, cw, chh, n, lld, llp,
+                                                                      (int32_t*)out, out_pitch, st, vec, zs, stream,
+                                                                      pdl)));
+                else if (quant)
+                    J2K_TRY((launch_fwd_tma<KERN, int32_t, true, false>(ctx, src, spitch, src_z, cw, chh, n, lld, llp,
+                                                                       (int32_t*)out, out_pitch, st, vec, zs, stream,
+                                                                       pdl)));
+                else
+                    J2K_TRY((launch_fwd_tma<KERN, T, false, false>(ctx, src, spitch, src_z, cw, chh, n, lld, llp,
+                                                                  (T*)out, out_pitch, st, vec, zs, stream, pdl)));
+            } else if (ctx && ctx->dwt_pipe && n == 1) {
                 const int bands = (chh + 16 - 1) / 16;
                 const int tx = (cw + FTW - 1) / FTW;
                 const int want = std::max(1, (ctx->sm_count * 4 + tx - 1) / tx);
@@ -669,7 +881,27 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
             } else if (ctx && !ctx->dwt_reg) {
                 if (fth == 16) FAST(16, false); else FAST(32, false);
             } else {
-                if (fth == 16) FAST(16, true); else FAST(32, true);
+                // the default path: every level after the first is a programmatic dependent of
+                // the one before, so its launch overlaps the previous level's last CTAs
+                const bool pdl = k > 0;
+                const dim3 b(256);
+                cudaError_t le;
+                if (quant && last)
+                    le = fth == 16 ? launch_pdl(dwt_fwd_fast<KERN, int32_t, true, true, 16, true>, fg, b, stream, pdl,
+                                                src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs)
+                                   : launch_pdl(dwt_fwd_fast<KERN, int32_t, true, true, 32, true>, fg, b, stream, pdl,
+                                                src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs);
+                else if (quant)
+                    le = fth == 16 ? launch_pdl(dwt_fwd_fast<KERN, int32_t, true, false, 16, true>, fg, b, stream, pdl,
+                                                src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs)
+                                   : launch_pdl(dwt_fwd_fast<KERN, int32_t, true, false, 32, true>, fg, b, stream, pdl,
+                                                src, spitch, cw, chh, lld, llp, (int32_t*)out, out_pitch, st, vec, zs);
+                else
+                    le = fth == 16 ? launch_pdl(dwt_fwd_fast<KERN, T, false, false, 16, true>, fg, b, stream, pdl,
+                                                src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, vec, zs)
+                                   : launch_pdl(dwt_fwd_fast<KERN, T, false, false, 32, true>, fg, b, stream, pdl,
+                                                src, spitch, cw, chh, lld, llp, (T*)out, out_pitch, st, vec, zs);
+                J2K_CUDA(ctx, le);
             }
 #undef FAST
         } else if (quant) {

@@ -56,9 +56,10 @@ enum : uint32_t {
     J2K_DEVERR_BAD_JOB = 3,       // malformed code-block descriptor
     J2K_DEVERR_TIMEOUT = 4,       // bounded wait expired
     J2K_DEVERR_PLANES = 5,        // more magnitude bit-planes than the coder supports
+    J2K_DEVERR_SEG_CAPACITY = 6,  // a coding-pass segment outgrew its slot (code-block styles)
 };
 
-constexpr int J2K_SCRATCH_SLOTS = 9;
+constexpr int J2K_SCRATCH_SLOTS = 11;
 
 constexpr int J2K_MQ_TIERS = 4;
 
@@ -81,11 +82,13 @@ struct j2k_ctx {
     // MQ schedule: tiers of warps with fewer blocks each for the longest blocks (lanes 0 ends)
     int mq_tier_warps[4] = {0, 0, 0, 0}, mq_tier_lanes[4] = {1, 0, 0, 0};  // tier 0: sm_count warps
     int dwt_reg = 1;             // fast forward DWT: columns loaded straight into registers (0: cp.async strip)
+    int t1_seg_factor = 1;       // styled tier-1: pass-segment slot bytes per symbol (grown on overflow)
+    int dwt_tma = 0;             // fast forward DWT: strips staged by TMA tensor copies (persistent CTAs)
 };
 
 // scratch slot ids
 enum { SCR_LL0 = 0, SCR_LL1 = 1, SCR_JOBS = 2, SCR_SYMS = 3, SCR_T1STATE = 4, SCR_MISC = 5,
-       SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8 };
+       SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8, SCR_UNITS = 9, SCR_SEGS = 10 };
 
 j2k_status j2k_fail(j2k_ctx* ctx, j2k_status s, const std::string& msg);
 j2k_status j2k_cuda_check(j2k_ctx* ctx, cudaError_t e, const char* what);
@@ -188,10 +191,22 @@ j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in,
 // plane_bytes (njobs x 32) and dist (njobs x 33), both device, optional: when given, the MQ coder
 // records the bytes produced at every bit-plane end and the distortion of every truncation point
 // is computed (rate control).
+// style: code-block style bits (J2K_CBLK_*; 0 = none).  With a style, pass_ends (device,
+// J2K_PASS_STRIDE entries per job) receives each pass's end in codeword bytes (exact where the
+// pass is terminated); rate control (plane_bytes, dist) is not combined with a style.
 j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_job* d_jobs, size_t njobs,
                               j2k_cb_desc* descs, uint8_t* bytes, size_t sym_bytes,
                               const uint32_t* d_order, cudaStream_t st, uint32_t* plane_bytes = nullptr,
-                              double* dist = nullptr);
+                              double* dist = nullptr, int style = 0, uint32_t* pass_ends = nullptr);
+// Code-block style rules (T.800 Table A.19, D.6), host and device: pass `p` (0 = the first
+// cleanup pass) is raw-coded, and the codeword is terminated after pass p of npasses.
+__host__ __device__ __forceinline__ bool j2k_pass_raw(int style, int p) {
+    return (style & J2K_CBLK_BYPASS) && p >= 10 && p % 3 != 0;
+}
+__host__ __device__ __forceinline__ bool j2k_pass_terminated(int style, int p, int npasses) {
+    if (p >= npasses - 1 || (style & J2K_CBLK_TERMALL)) return true;
+    return j2k_pass_raw(style, p) != j2k_pass_raw(style, p + 1);
+}
 
 // ---- rate control (PCRD-opt, rate.cpp) -----------------------------------------------------
 // Squared-norm gain of the synthesis basis of subband b (QCD order) for the 5/3 or 9/7 inverse
@@ -226,9 +241,13 @@ struct j2k_pcrd_hulls {
     void cut(double thr, int32_t* npasses, int32_t* length) const;
 };
 constexpr int J2K_TRUNC_EXTRA = 4;  // bytes kept beyond those produced at a plane end
+// style / pass_ends (device, J2K_PASS_STRIDE per job) locate the codeword segments of styled
+// blocks; style 0 decodes one segment of descs[i].length bytes.  job_style (device, one byte per
+// job, optional) gives each job its own style (pass ends then needed for every job).
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
-                              cudaStream_t st);
+                              cudaStream_t st, int style = 0, const uint32_t* pass_ends = nullptr,
+                              const uint8_t* job_style = nullptr);
 
 // Expounded quantisation (T.800 A.6.4, E.1.1) for 8-bit samples: step = 2^(Rb - eps) *
 // (1 + mant / 2^11), Rb = 8 + the gain of QCD band `band` (0 for LL, 1 for HL and LH, 2 for HH).
@@ -241,14 +260,18 @@ bool j2k_qcd_step(float step, int band, int* eps, int* mant);
 struct j2k_t2_block {
     int numbps, npasses, length;
     const uint8_t* data;
+    const uint32_t* pass_end = nullptr;  // styled blocks: J2K_PASS_STRIDE pass ends
 };
+// style: the code-block style written in COD; styled blocks' segments (one per terminated pass)
+// get a length each in the packet headers.
 std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
                                   int lossless, int mct, const float* steps,
-                                  const std::vector<j2k_t2_block>& blocks);
+                                  const std::vector<j2k_t2_block>& blocks, int style = 0);
 // Parses a codestream (the first max_layers quality layers, 0: all) into descriptors in job order
 // and the codewords packed back to back (descs[i].offset into bytes).
 j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
-                               std::vector<j2k_cb_desc>* descs, std::vector<uint8_t>* bytes, std::string* err);
+                               std::vector<j2k_cb_desc>* descs, std::vector<uint8_t>* bytes, std::string* err,
+                               std::vector<uint32_t>* pass_ends = nullptr);
 // Size in bytes of the codestream j2k_t2_write would produce (block data is not read).
 size_t j2k_t2_size(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
                    const float* steps, const std::vector<j2k_t2_block>& blocks, int nlayers = 1,

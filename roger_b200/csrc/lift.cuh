@@ -89,6 +89,32 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Programmatic dependent launch (sm_90+): a level kernel lets the next level's grid be launched
+// while its own CTAs still run, and waits for the previous level's grid (its writes visible)
+// before it reads that level's output.  Both are no-ops for a kernel launched without the
+// programmatic-serialisation attribute.
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+// Launches k<<<g, b, 0, s>>>(args...); with pdl, as a programmatic dependent of the previous
+// kernel on the stream (cudaLaunchAttributeProgrammaticStreamSerialization).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 g, dim3 b, cudaStream_t s, bool pdl, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // ---- transposed 9/7 steps -----------------------------------------------------------------------
 // A forward step updates parity p: x_i += c (x_m(i-1) + x_m(i+1)), m = symmetric mirror.  Its
 // transpose updates the other parity with the same coefficient from the neighbours weighted by

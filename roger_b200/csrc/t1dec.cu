@@ -197,18 +197,81 @@ __host__ __device__ __forceinline__ uint32_t nb3(uint64_t m, int x) {
     return (uint32_t)(x > 0 ? (m >> (x - 1)) & 7 : (m << 1) & 7);
 }
 
+// Raw (bypass) segment reader, T.800 D.6: bits most significant first; a byte after 0xFF holds
+// 7 bits (its top bit is a stuffed 0); past the end of the segment 0xFF is read.
+struct RawD {
+    const uint8_t* data;
+    int len, pos, ct;
+    uint32_t c;
+    bool lastff;
+    __host__ __device__ void init(const uint8_t* d, int n) {
+        data = d;
+        len = n;
+        pos = 0;
+        ct = 0;
+        c = 0;
+        lastff = false;
+    }
+    __host__ __device__ int bit() {
+        if (ct == 0) {
+            const uint32_t b = pos < len ? data[pos] : 0xFFu;
+            ++pos;
+            ct = lastff ? 7 : 8;
+            lastff = b == 0xFF;
+            c = b;
+        }
+        --ct;
+        return (int)((c >> ct) & 1);
+    }
+};
+
 // Serial decode of one code-block into magnitudes (blk, pre-zeroed) and sign/state masks in S.
-// Host-callable so that the exact device logic can be checked on the CPU.
+// Host-callable so that the exact device logic can be checked on the CPU.  STYLED: the block was
+// coded with code-block style `style` (contexts reset per pass, a new codeword segment after
+// every terminated pass, located by the pass ends `pe`; raw-coded passes read as bits).
+template <bool STYLED = false>
 __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint8_t* data, int len, int numbps,
-                                      int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch) {
+                                      int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch,
+                                      int style = 0, const uint32_t* pe = nullptr) {
         const uint8_t* zct = T.zc[orient];
         const uint32_t* mq = T.mq;
 
-        S.st[0] = 4 << 1;
-        S.st[17] = 3 << 1;
-        S.st[18] = 46 << 1;
+        auto reset_states = [&]() {
+            for (int k = 0; k < 19; ++k) S.st[k] = 0;
+            S.st[0] = 4 << 1;
+            S.st[17] = 3 << 1;
+            S.st[18] = 46 << 1;
+        };
+        reset_states();
         Mqd m;
-        m.init(data, len);
+        RawD rd;
+        bool raw = false;
+        if (!STYLED) m.init(data, len);
+        // the start of pass q of a styled block: context reset, and a new segment after a
+        // terminated pass
+        auto begin = [&](int q) {
+            if (!STYLED) return;
+            if (q > 0 && (style & J2K_CBLK_RESET)) reset_states();
+            raw = j2k_pass_raw(style, q);
+            if (q == 0 || j2k_pass_terminated(style, q - 1, npasses)) {
+                int e = q;
+                while (!j2k_pass_terminated(style, e, npasses)) ++e;
+                int b0 = q ? (int)min(pe[q - 1], (uint32_t)len) : 0;
+                int b1 = (int)min(pe[e], (uint32_t)len);
+                if (b1 < b0) b1 = b0;
+                if (raw) rd.init(data + b0, b1 - b0);
+                else m.init(data + b0, b1 - b0);
+            }
+        };
+        // one decision in context cx, and one sign in sign context sc (label | xor << 7)
+        auto dec = [&](int cx) -> int {
+            if (STYLED && raw) return rd.bit();
+            return m.decode(S.st, mq, cx);
+        };
+        auto dsign = [&](int sc) -> int {
+            if (STYLED && raw) return rd.bit();
+            return m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+        };
         int pass = 0;
         const int nb = numbps, np = npasses;
         // a stripe column's neighbourhood, packed: bits 3r..3r+2 hold columns x-1..x+1 of block row
@@ -236,6 +299,7 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
             if (p != nb - 1) {
                 // significance propagation: only columns next to a significant sample can hold a
                 // decision; a column joins when its left neighbour gains a significant sample
+                begin(pass);
                 for (int y0 = 0; y0 < ch; y0 += 4) {
                     const int ny = min(4, ch - y0);
                     uint64_t cm = 0;
@@ -254,12 +318,12 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                             if ((W >> (3 * k + 4)) & 1) continue;  // significant already
                             const uint32_t n9 = (W >> (3 * k)) & 511;
                             if (!(n9 & 0x1EF)) continue;           // no significant neighbour
-                            const int bit = m.decode(S.st, mq, zct[n9]);
+                            const int bit = dec(zct[n9]);
                             S.vis[y0 + k + 1] |= 1ull << x;
                             if (bit) {
                                 if (!nw) NW = colw(S.neg, y0, x), nw = true;
                                 const int sc = T.sc[n8of(W, NW, k)];
-                                const int sg = m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+                                const int sg = dsign(sc);
                                 set_sig(x, y0 + k, sg, p);
                                 W |= 1u << (3 * k + 4);
                                 NW |= (uint32_t)sg << (3 * k + 4);
@@ -270,6 +334,7 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                 }
                 if (++pass >= np) break;
                 // magnitude refinement: significant samples not visited in this plane
+                begin(pass);
                 for (int y0 = 0; y0 < ch; y0 += 4) {
                     const int ny = min(4, ch - y0);
                     uint64_t rm = 0;
@@ -283,7 +348,7 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                             const int y = y0 + k;
                             if (!((W >> (3 * k + 4)) & 1) || ((S.vis[y + 1] >> x) & 1)) continue;
                             const int lab = ((S.ref[y + 1] >> x) & 1) ? 16 : (((W >> (3 * k)) & 0x1EF) ? 15 : 14);
-                            if (m.decode(S.st, mq, lab)) blk[(size_t)y * pitch + x] |= 1 << p;
+                            if (dec(lab)) blk[(size_t)y * pitch + x] |= 1 << p;
                             S.ref[y + 1] |= 1ull << x;
                         }
                     }
@@ -291,6 +356,7 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                 if (++pass >= np) break;
             }
             // cleanup: every insignificant sample not visited in this plane
+            begin(pass);
             for (int y0 = 0; y0 < ch; y0 += 4) {
                 const int ny = min(4, ch - y0);
                 uint64_t um = 0;
@@ -306,11 +372,11 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                     if (ny == 4 && W == 0 && V == 0) {
                         // run-length mode: four insignificant, unvisited samples, no significant
                         // neighbour (every bit of the column's neighbourhood is zero)
-                        if (!m.decode(S.st, mq, 17)) continue;
-                        int idx = m.decode(S.st, mq, 18) << 1;
-                        idx |= m.decode(S.st, mq, 18);
+                        if (!dec(17)) continue;
+                        int idx = dec(18) << 1;
+                        idx |= dec(18);
                         const int sc = T.sc[0];
-                        const int sg = m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+                        const int sg = dsign(sc);
                         set_sig(x, y0 + idx, sg, p);
                         W |= 1u << (3 * idx + 4);
                         NW = (uint32_t)sg << (3 * idx + 4);  // the only significant sample around
@@ -319,10 +385,10 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                     }
                     for (int k = start; k < ny; ++k) {
                         if (((W >> (3 * k + 4)) & 1) || ((V >> k) & 1)) continue;
-                        if (m.decode(S.st, mq, zct[(W >> (3 * k)) & 511])) {
+                        if (dec(zct[(W >> (3 * k)) & 511])) {
                             if (!nw) NW = colw(S.neg, y0, x), nw = true;
                             const int sc = T.sc[n8of(W, NW, k)];
-                            const int sg = m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+                            const int sg = dsign(sc);
                             set_sig(x, y0 + k, sg, p);
                             W |= 1u << (3 * k + 4);
                             NW |= (uint32_t)sg << (3 * k + 4);
@@ -335,10 +401,12 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
         }
 }
 
+template <bool STYLED>
 __global__ void __launch_bounds__(kWarps * 32)
 t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
                  const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
-                 uint32_t* __restrict__ err) {
+                 uint32_t* __restrict__ err, int style, const uint32_t* __restrict__ pass_ends,
+                 const uint8_t* __restrict__ job_style) {
     __shared__ DecSmem smem[kWarps];
     __shared__ DecTables tabs;
     for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
@@ -350,8 +418,9 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
     const j2k_cb_job J = jobs[jid];
     const j2k_cb_desc D = descs[jid];
     const int cw = J.cw, ch = J.ch, orient = J.orient;
+    // (a styled block's passes index its pass ends: at most 3 * 31 - 2 of them)
     if (cw == 0 || ch == 0 || cw > 64 || ch > 64 || orient > 3 || D.numbps > 31 ||
-        D.npasses > 3 * D.numbps || D.length < 0) {
+        D.npasses > 3 * D.numbps || D.length < 0 || (STYLED && D.npasses > J2K_PASS_STRIDE - 1)) {
         if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
         return;
     }
@@ -363,8 +432,9 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
     if (lane < 19) S.st[lane] = 0;
     __syncwarp();
     if (lane == 0 && D.numbps > 0 && D.npasses > 0)
-        decode_block(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch,
-                     blk, pitch);
+        decode_block<STYLED>(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch, blk, pitch,
+                             job_style ? (int)job_style[jid] : style,
+                             STYLED ? pass_ends + (size_t)jid * J2K_PASS_STRIDE : nullptr);
     __syncwarp();
     // a block cut at the end of a bit-plane above the last one (rate control): significant
     // magnitudes are reconstructed at the middle of the interval their undecoded bits leave
@@ -409,10 +479,17 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
 
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
-                              cudaStream_t st) {
+                              cudaStream_t st, int style, const uint32_t* pass_ends, const uint8_t* job_style) {
     if (njobs == 0) return J2K_OK;
+    if ((style || job_style) && !pass_ends)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "a styled decode needs the pass ends");
     unsigned g = (unsigned)((njobs + kWarps - 1) / kWarps);
-    t1_decode_kernel<<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err);
+    if (style || job_style)
+        t1_decode_kernel<true><<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, style,
+                                                          pass_ends, job_style);
+    else
+        t1_decode_kernel<false><<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, 0,
+                                                           nullptr, nullptr);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }

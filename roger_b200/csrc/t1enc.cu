@@ -17,7 +17,8 @@
 //     forms the ZC/SC/MR/RL labels for stripe columns 2l and 2l+1 in parallel, and a warp
 //     prefix sum places the symbols in scan order.
 // The output is the exact (context, decision) sequence of the serial coder, one byte per
-// symbol (label in bits 0-4, decision in bit 7).
+// symbol (label in bits 0-4, decision in bit 7; sign symbols also carry their context's XOR
+// bit in bit 5, so that a raw-coded pass can recover the sign itself).
 //
 // Phase B — one lane per code-block runs the MQ encoder over its symbol stream (T.800 C.2,
 // FLUSH of C.2.9, trailing 0xFF dropped); codeword bytes are written as aligned 32-bit words.
@@ -253,7 +254,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                                 const uint32_t ng4 = (nw & 1) | ((nw >> 1) & 2) | ((nu & 2) << 1) | ((nd & 2) << 2);
                                 const int sc = slut[sg4 | (ng4 << 4)];
                                 const int sgn = (ng[j + 1] >> (k + 1)) & 1;
-                                out[off++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                                out[off++] = (uint8_t)((sc & 31) | ((sc >> 7) << 5) | ((sgn ^ (sc >> 7)) << 7));
                             }
                         }
                 }
@@ -398,7 +399,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                         // sign of the first significant sample: its four neighbours are insignificant
                         const int sgn = (ng[first + 1] >> (k + 1)) & 1;
                         const int sc = slut[0];
-                        out[off++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                        out[off++] = (uint8_t)((sc & 31) | ((sc >> 7) << 5) | ((sgn ^ (sc >> 7)) << 7));
                         jstart = first + 1;
                     }
 #pragma unroll
@@ -416,7 +417,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                             const uint32_t ng4 = (nw & 1) | ((nw >> 1) & 2) | ((nu & 2) << 1) | ((nd & 2) << 2);
                             const int sc = slut[(zi & 15) | (ng4 << 4)];
                             const int sgn = (ng[j + 1] >> (k + 1)) & 1;
-                            out[off++] = (uint8_t)((sc & 31) | ((sgn ^ (sc >> 7)) << 7));
+                            out[off++] = (uint8_t)((sc & 31) | ((sc >> 7) << 5) | ((sgn ^ (sc >> 7)) << 7));
                         }
                     }
                 }
@@ -908,6 +909,224 @@ t1_mq_pair_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict
     }
 }
 
+// ---- code-block styles: coding units --------------------------------------------------------
+//
+// With a code-block style the MQ coder works on units: a run of passes coded serially by one
+// lane (context states carried from pass to pass, reset where the style says so, the codeword
+// terminated after the passes the style terminates, raw-coded passes written as bits).  When
+// the style has both RESET and TERMALL every pass starts from fresh states and a fresh coder,
+// so each pass is a unit of its own and the passes of a block code in parallel lanes; otherwise
+// a block is one unit.  Unit k of job j is slot j * J2K_PASS_STRIDE + k.  A unit writes its
+// segments into a slot of its own (its symbols' range of the symbol buffer, times a factor,
+// plus 16 bytes per pass), and a compaction pass then puts each block's units back to back.
+
+__host__ __device__ __forceinline__ bool units_per_pass(int style) {
+    return (style & (J2K_CBLK_RESET | J2K_CBLK_TERMALL)) == (J2K_CBLK_RESET | J2K_CBLK_TERMALL);
+}
+
+// slot byte offset of the unit that starts at symbol s0 and pass p0 of job j (symbol stream of
+// job j at sym_off): slots follow the symbols, so consecutive units never overlap
+__device__ __forceinline__ uint64_t seg_slot(uint64_t sym_off, uint32_t s0, int j, int p0, int fac) {
+    return (uint64_t)fac * ((sym_off + s0 + 3) & ~(uint64_t)3) + 16ull * ((uint64_t)j * J2K_PASS_STRIDE + p0);
+}
+
+// sort keys: symbols of each unit + 1 (0 for slots without a unit); values: slot ids
+__global__ void t1_unit_keys_kernel(const j2k_cb_desc* __restrict__ descs, const uint32_t* __restrict__ pend,
+                                    int njobs, int style, uint32_t* __restrict__ keys, uint32_t* __restrict__ ids) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= njobs * J2K_PASS_STRIDE) return;
+    const int j = i / J2K_PASS_STRIDE, k = i % J2K_PASS_STRIDE;
+    const int np = descs[j].npasses;
+    const uint32_t* pe = pend + (size_t)j * J2K_PASS_STRIDE;
+    uint32_t key = 0;
+    if (units_per_pass(style)) {
+        if (k < np) key = pe[k] - (k ? pe[k - 1] : 0u) + 1u;
+    } else if (k == 0 && np > 0) {
+        key = pe[np - 1] + 1u;
+    }
+    keys[i] = key;
+    ids[i] = (uint32_t)i;
+}
+
+// One lane per unit, units longest first.  ulen[slot] receives the unit's bytes; ends[j *
+// stride + p] the unit-relative codeword bytes when pass p ended.
+__global__ void __launch_bounds__(128)
+t1_mq_units_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jobs,
+                   const j2k_cb_desc* __restrict__ descs, const uint32_t* __restrict__ pend,
+                   const uint32_t* __restrict__ order, const uint32_t* __restrict__ keys, int nslots, int style,
+                   int fac, uint8_t* __restrict__ segs, uint32_t* __restrict__ ulen, uint32_t* __restrict__ ends,
+                   uint32_t* __restrict__ err) {
+    __shared__ uint32_t tab[47];
+    __shared__ uint32_t cst[32 * 128];
+    for (int i = threadIdx.x; i < 47; i += blockDim.x)
+        tab[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
+                 ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
+    __syncthreads();
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= nslots || keys[gid] == 0) return;  // keys are sorted: the empty slots come last
+    const int u = (int)order[gid];
+    const int j = u / J2K_PASS_STRIDE, k = u % J2K_PASS_STRIDE;
+    const j2k_cb_job J = jobs[j];
+    const int np = descs[j].npasses;
+    const bool per_pass = units_per_pass(style);
+    const int p0 = per_pass ? k : 0, p1 = per_pass ? k + 1 : np;
+    const uint32_t* pe = pend + (size_t)j * J2K_PASS_STRIDE;
+    uint32_t* eo = ends + (size_t)j * J2K_PASS_STRIDE;
+    const uint32_t s0 = p0 ? pe[p0 - 1] : 0u, s1 = pe[p1 - 1];
+    if (s1 > J.sym_cap || s0 > s1) {
+        atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+        return;
+    }
+    const uint64_t base = seg_slot(J.sym_off, s0, j, p0, fac);
+    const uint64_t lim = seg_slot(J.sym_off, s1, j, p1, fac);
+    uint32_t* st = cst + threadIdx.x;  // context c at st[c * 128]
+    auto reset_states = [&]() {
+        for (int c = 0; c < 32; ++c) st[c * 128] = tab[0];
+        st[0] = tab[4];
+        st[17 * 128] = tab[3];
+        st[18 * 128] = tab[46];
+    };
+    reset_states();
+    MqEnc e;
+    e.out = reinterpret_cast<uint32_t*>(segs + base);
+    e.cap = (int)(lim - base);
+    e.wacc = 0;
+    e.wn = 0;
+    e.wbase = 0;
+    e.ovf = false;
+    // raw coder: bits of the byte being filled, bits left in it, the last completed byte (held
+    // back one byte so that a final 0xFF can be dropped)
+    uint32_t rc = 0;
+    int rct = 8, rpend = -1;
+    bool rlastff = false, raw = false;
+    auto raw_complete = [&](uint32_t b) {
+        if (rpend >= 0) e.push((uint32_t)rpend);
+        rpend = (int)b;
+        rlastff = b == 0xFF;
+        rct = rlastff ? 7 : 8;
+        rc = 0;
+    };
+    const uint8_t* sp = syms + J.sym_off;
+    for (int p = p0; p < p1; ++p) {
+        if (p > p0 && (style & J2K_CBLK_RESET)) reset_states();
+        raw = j2k_pass_raw(style, p);
+        if (p == p0 || j2k_pass_terminated(style, p - 1, np)) {  // a new segment
+            if (raw) {
+                rc = 0;
+                rct = 8;
+                rpend = -1;
+                rlastff = false;
+            } else {
+                e.A = 0x8000;
+                e.C = 0;
+                e.B = 0;
+                e.CT = 12;
+                e.bp = -1;
+            }
+        }
+        const uint32_t a = p ? pe[p - 1] : 0u, b = pe[p];
+        uint32_t word = 0;
+        for (uint32_t i = a; i < b; ++i) {
+            if (i == a || (i & 3) == 0) word = __ldcs(reinterpret_cast<const uint32_t*>(sp + (i & ~3u)));
+            const uint32_t sym = (word >> (8 * (i & 3))) & 0xFF;
+            if (raw) {
+                const uint32_t lab = sym & 31;
+                const uint32_t bit = ((sym >> 7) ^ ((lab >= 9 && lab <= 13) ? (sym >> 5) : 0u)) & 1u;
+                rc = (rc << 1) | bit;
+                if (--rct == 0) raw_complete(rc & 0xFF);
+            } else {
+                const int cx = (int)(sym & 31);
+                const int d = (int)(sym >> 7);
+                const uint32_t ent = st[cx * 128];
+                const uint32_t qe = ent & 0xFFFF;
+                const int mps = (int)(ent >> 31);
+                const bool is_mps = d == mps;
+                const uint32_t a1 = e.A - qe;
+                const bool fast = is_mps && (a1 & 0x8000);
+                const bool addc = fast || (is_mps != (a1 < qe));
+                e.C += addc ? qe : 0u;
+                e.A = addc ? a1 : qe;
+                if (!fast) {
+                    const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
+                    const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
+                    st[cx * 128] = tab[nidx] | (nmps << 31);
+                }
+                e.renorm(__clz(e.A) - 16);
+            }
+        }
+        if (j2k_pass_terminated(style, p, np)) {
+            if (raw) {
+                if (rct < (rlastff ? 7 : 8)) raw_complete((rc << rct) & 0xFF);
+                if (rpend >= 0 && rpend != 0xFF) e.push((uint32_t)rpend);
+                rpend = -1;
+            } else {  // FLUSH (T.800 C.2.9); a last byte of 0xFF is dropped
+                const uint32_t tempc = e.C + e.A;
+                e.C |= 0xFFFF;
+                if (e.C >= tempc) e.C -= 0x8000;
+                e.C <<= e.CT;
+                e.byteout();
+                e.C <<= e.CT;
+                e.byteout();
+                if (e.B != 0xFF) e.push(e.B);
+            }
+            eo[p] = (uint32_t)(e.wbase + e.wn);
+        } else {
+            eo[p] = (uint32_t)(e.wbase + e.wn) + (raw ? (rpend >= 0) : (uint32_t)(e.bp + 1 > 0));
+        }
+    }
+    // the last partial word
+    uint8_t* bb = segs + base;
+    for (int q = 0; q < e.wn; ++q) {
+        if (e.wbase + q < e.cap) bb[e.wbase + q] = (uint8_t)(e.wacc >> (8 * q));
+        else e.ovf = true;
+    }
+    if (e.ovf) {
+        atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_SEG_CAPACITY);
+        ulen[u] = 0;
+        return;
+    }
+    ulen[u] = (uint32_t)(e.wbase + e.wn);
+}
+
+// One warp per code-block: its units' segments back to back into the block's codeword, the
+// pass ends made block-relative, and the descriptor's length.
+__global__ void t1_units_compact_kernel(const j2k_cb_job* __restrict__ jobs, j2k_cb_desc* __restrict__ descs,
+                                        const uint32_t* __restrict__ pend, int njobs, int style, int fac,
+                                        const uint8_t* __restrict__ segs, const uint32_t* __restrict__ ulen,
+                                        uint32_t* __restrict__ ends, uint8_t* __restrict__ bytes,
+                                        uint32_t* __restrict__ err) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (j >= njobs) return;
+    const j2k_cb_job J = jobs[j];
+    const int np = descs[j].npasses;
+    const bool per_pass = units_per_pass(style);
+    const int nu = np == 0 ? 0 : (per_pass ? np : 1);
+    const uint32_t* pe = pend + (size_t)j * J2K_PASS_STRIDE;
+    uint32_t* eo = ends + (size_t)j * J2K_PASS_STRIDE;
+    uint32_t run = 0;  // bytes of the units before this round of 32
+    uint8_t* dst = bytes + J.out_off;
+    for (int k0 = 0; k0 < nu; k0 += 32) {
+        const int k = k0 + lane;
+        const uint32_t len = k < nu ? ulen[(size_t)j * J2K_PASS_STRIDE + k] : 0u;
+        int tot;
+        const uint32_t off = run + (uint32_t)warp_excl((int)len, lane, &tot);
+        if (k < nu) {
+            if (off + len > J.out_cap) {
+                atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_OUT_CAPACITY);
+            } else {
+                const int p0 = per_pass ? k : 0, p1 = per_pass ? k + 1 : np;
+                const uint32_t s0 = p0 ? pe[p0 - 1] : 0u;
+                const uint8_t* src = segs + seg_slot(J.sym_off, s0, j, p0, fac);
+                for (uint32_t q = 0; q < len; ++q) dst[off + q] = src[q];
+                for (int p = p0; p < p1; ++p) eo[p] += off;
+            }
+        }
+        run += (uint32_t)tot;
+    }
+    for (int p = np + lane; p < J2K_PASS_STRIDE; p += 32) eo[p] = 0;
+    if (lane == 0) descs[j].length = run <= J.out_cap ? (int32_t)run : 0;
+}
+
 __global__ void iota_kernel(uint32_t* v, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = (uint32_t)i;
@@ -972,10 +1191,52 @@ t1_dist_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__
 
 }  // namespace
 
+// Phase B of a styled encode: units keyed and sorted longest first, coded one lane each, then
+// compacted into the blocks' codewords.
+static j2k_status encode_styled_units(j2k_ctx* ctx, const j2k_cb_job* d_jobs, size_t njobs, j2k_cb_desc* descs,
+                                      uint8_t* bytes, size_t sym_bytes, const uint8_t* syms, const uint32_t* pend,
+                                      int style, uint32_t* pass_ends, cudaStream_t st) {
+    const size_t nslots = njobs * J2K_PASS_STRIDE;
+    if (nslots > 0x7FFFFFFF) return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "too many code-blocks for a styled encode");
+    uint32_t* ub = (uint32_t*)j2k_scratch(ctx, SCR_UNITS, (nslots * (pass_ends ? 5 : 6) + 64) * 4);
+    if (!ub) return J2K_ERR_OUT_OF_MEMORY;
+    uint32_t* keys_in = ub;
+    uint32_t* keys_out = keys_in + nslots;
+    uint32_t* ids_in = keys_out + nslots;
+    uint32_t* ids_out = ids_in + nslots;
+    uint32_t* ulen = ids_out + nslots;
+    uint32_t* ends = pass_ends ? pass_ends : ulen + nslots;
+    const int fac = std::max(1, ctx->t1_seg_factor);
+    // slots end by fac * (sym_bytes + 3) + 16 * nslots (seg_slot of the last unit's end)
+    uint8_t* segs = (uint8_t*)j2k_scratch(ctx, SCR_SEGS, (size_t)fac * (sym_bytes + 64) + 16 * nslots + 64);
+    if (!segs) return J2K_ERR_OUT_OF_MEMORY;
+    const unsigned g = (unsigned)((nslots + 255) / 256);
+    t1_unit_keys_kernel<<<g, 256, 0, st>>>(descs, pend, (int)njobs, style, keys_in, ids_in);
+    J2K_CUDA(ctx, cudaGetLastError());
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, keys_in, keys_out, ids_in, ids_out, (int)nslots, 0, 32,
+                                              st);
+    void* tbuf = j2k_scratch(ctx, SCR_MISC, tmp + 16);
+    if (!tbuf) return J2K_ERR_OUT_OF_MEMORY;
+    J2K_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, keys_in, keys_out, ids_in, ids_out,
+                                                            (int)nslots, 0, 32, st));
+    t1_mq_units_kernel<<<(unsigned)((nslots + 127) / 128), 128, 0, st>>>(syms, d_jobs, descs, pend, ids_out, keys_out,
+                                                                         (int)nslots, style, fac, segs, ulen, ends,
+                                                                         ctx->d_err);
+    J2K_CUDA(ctx, cudaGetLastError());
+    t1_units_compact_kernel<<<(unsigned)((njobs * 32 + 255) / 256), 256, 0, st>>>(
+        d_jobs, descs, pend, (int)njobs, style, fac, segs, ulen, ends, bytes, ctx->d_err);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
+}
+
 j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_job* d_jobs, size_t njobs,
                               j2k_cb_desc* descs, uint8_t* bytes, size_t sym_bytes,
-                              const uint32_t* d_order, cudaStream_t st, uint32_t* plane_bytes, double* dist) {
+                              const uint32_t* d_order, cudaStream_t st, uint32_t* plane_bytes, double* dist,
+                              int style, uint32_t* pass_ends) {
     if (njobs == 0) return J2K_OK;
+    if (style && (plane_bytes || dist))
+        return j2k_fail(ctx, J2K_ERR_UNSUPPORTED, "rate control with a code-block style");
     if (((uintptr_t)bytes & 15) != 0)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "t1: bytes buffer must be 16-byte aligned");
     uint8_t* syms = (uint8_t*)j2k_scratch(ctx, SCR_SYMS, sym_bytes + 64);
@@ -999,6 +1260,8 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     t1_symbols_kernel<<<(unsigned)ctas, kWarpsPerCta * 32, 0, st>>>(coeff, d_jobs, (int)njobs, d_order, queue, syms,
                                                                    nsyms, pend, planes, descs, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
+    if (style)
+        return encode_styled_units(ctx, d_jobs, njobs, descs, bytes, sym_bytes, syms, pend, style, pass_ends, st);
     // longest-first order for the MQ lanes
     iota_kernel<<<(unsigned)((njobs + 255) / 256), 256, 0, st>>>(idx_in, (int)njobs);
     size_t tmp = 0;

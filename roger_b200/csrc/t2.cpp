@@ -174,7 +174,7 @@ bool j2k_qcd_step_impl(float step, int band, int* eps, int* mant) {
 // blocks[i] says.
 size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int cbh, int lossless, int mct,
                const float* steps, const std::vector<j2k_t2_block>& blocks, bool bodies, int nlayers = 1,
-               const int32_t* cum_np = nullptr, const int32_t* cum_len = nullptr) {
+               const int32_t* cum_np = nullptr, const int32_t* cum_len = nullptr, int style = 0) {
     const size_t nblk = blocks.size();
     if (!cum_np || !cum_len) nlayers = 1;
     // passes / bytes of block i after layer l (l = -1: nothing)
@@ -243,7 +243,7 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
     o.u8((uint32_t)levels);
     o.u8((uint32_t)(floorlog2(cbw) - 2));
     o.u8((uint32_t)(floorlog2(cbh) - 2));
-    o.u8(0);
+    o.u8((uint32_t)style);  // code-block style
     o.u8(lossless ? 1 : 0);
     o.u16(0xFF5C);  // QCD
     if (lossless) {
@@ -329,14 +329,35 @@ size_t t2_emit(Bytes& o, size_t w, size_t h, int ncomp, int levels, int cbw, int
                         if (cur == prev) continue;
                     }
                     const int newp = cur - prev;
-                    const int seg = LEN(l, k) - LEN(l - 1, k);
                     put_npasses(bw, newp);
-                    int bits = floorlog2(seg) + 1;
-                    int avail = lblock[k] + floorlog2(newp);
-                    int inc = bits > avail ? bits - avail : 0;
+                    // the new passes as pieces of codeword segments (B.10.7.2): one piece per
+                    // segment the style terminates within them, and the rest; each piece's
+                    // length in Lblock + floor(log2(its passes)) bits, Lblock raised once so
+                    // that every length fits
+                    int pnp[J2K_PASS_STRIDE + 1], plen[J2K_PASS_STRIDE + 1], npc = 0;
+                    if (style) {
+                        const j2k_t2_block& B = blocks[k];
+                        int at = LEN(l - 1, k), start = prev;
+                        for (int q = prev; q < cur; ++q) {
+                            const bool term = j2k_pass_terminated(style, q, B.npasses);
+                            if (!term && q != cur - 1) continue;
+                            const int end = term && B.pass_end ? (int)B.pass_end[q] : LEN(l, k);
+                            pnp[npc] = q + 1 - start;
+                            plen[npc++] = end - at;
+                            at = end;
+                            start = q + 1;
+                        }
+                    } else {
+                        pnp[0] = newp;
+                        plen[0] = LEN(l, k) - LEN(l - 1, k);
+                        npc = 1;
+                    }
+                    int inc = 0;
+                    for (int q = 0; q < npc; ++q)
+                        inc = std::max(inc, floorlog2(plen[q]) + 1 - (lblock[k] + floorlog2(pnp[q])));
                     bw.bits(((1u << inc) - 1) << 1, inc + 1);  // inc ones, then a zero
                     lblock[k] += inc;
-                    bw.bits((uint32_t)seg, lblock[k] + floorlog2(newp));
+                    for (int q = 0; q < npc; ++q) bw.bits((uint32_t)plen[q], lblock[k] + floorlog2(pnp[q]));
                 }
         }
         bw.flush();
@@ -415,9 +436,9 @@ bool j2k_qcd_step(float step, int band, int* eps, int* mant) { return j2k_qcd_st
 // (exactly the order of j2k_build_jobs).
 std::vector<uint8_t> j2k_t2_write(size_t w, size_t h, int ncomp, int levels, int cbw, int cbh,
                                   int lossless, int mct, const float* steps,
-                                  const std::vector<j2k_t2_block>& blocks) {
+                                  const std::vector<j2k_t2_block>& blocks, int style) {
     Bytes o;
-    t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, true);
+    t2_emit(o, w, h, ncomp, levels, cbw, cbh, lossless, mct, steps, blocks, true, 1, nullptr, nullptr, style);
     return std::move(o.v);
 }
 
@@ -633,7 +654,8 @@ namespace {
 // the first `max_layers` layers (0: all), segs[i] listing (offset in tile_bytes, length).
 j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
                    std::vector<j2k_cb_desc>* descs, std::vector<std::vector<std::pair<uint32_t, int>>>* segs,
-                   std::vector<uint8_t>* tile_bytes, std::string* err, bool header_only = false) {
+                   std::vector<uint8_t>* tile_bytes, std::string* err, bool header_only = false,
+                   std::vector<uint32_t>* pass_ends = nullptr) {
     try {
         Cursor c{cs, n};
         if (c.u16() != 0xFF4F) throw ReadErr{J2K_ERR_INVALID_ARG, "no SOC marker"};
@@ -691,7 +713,12 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
                 if (scod & 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "user-defined precincts"};
                 if (layers < 1) throw ReadErr{J2K_ERR_INVALID_ARG, "no quality layer"};
                 if (prog != 0 && prog != 1) throw ReadErr{J2K_ERR_UNSUPPORTED, "progression other than LRCP/RLCP"};
-                if (sty != 0) throw ReadErr{J2K_ERR_UNSUPPORTED, "code-block style options (bypass, reset, ...)"};
+                // bypass, reset, per-pass termination and predictable termination (which needs
+                // nothing of a decoder) are read; vertically causal contexts and segmentation
+                // symbols are not
+                if (sty & 0x08) throw ReadErr{J2K_ERR_UNSUPPORTED, "vertically causal code-block contexts"};
+                if (sty & 0x20) throw ReadErr{J2K_ERR_UNSUPPORTED, "code-block segmentation symbols"};
+                if (sty & ~0x3F) throw ReadErr{J2K_ERR_INVALID_ARG, "code-block style"};
                 if (levels > 32 || cbw > 64 || cbh > 64 || cbw * cbh > 4096)
                     throw ReadErr{J2K_ERR_UNSUPPORTED, "code-block size or decomposition levels"};
             } else if (m == 0xFF5C) {  // QCD
@@ -766,6 +793,8 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
         I.guard = guard;
         I.layers = layers;
         I.progression = prog;
+        I.cblk_style = sty & (J2K_CBLK_BYPASS | J2K_CBLK_RESET | J2K_CBLK_TERMALL);
+        const int style = I.cblk_style;
         std::vector<j2k_band_rect> rects(nb);
         j2k_band_rects(I.w, I.h, levels, rects.data());
         for (int b = 0; b < nb && b < J2K_MAX_BANDS; ++b) {
@@ -814,6 +843,7 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
                 zbp.emplace_back(std::max(ncbx[b], 1), std::max(ncby[b], 1));
             }
         std::vector<int> lblock(k, 3), tot_np(k, 0);
+        if (pass_ends) pass_ends->assign(style ? k * J2K_PASS_STRIDE : 0, 0u);
         std::vector<uint8_t> included(k, 0);  // 0, or the block's bit-plane count once included
         const int keep = max_layers > 0 ? std::min(max_layers, layers) : layers;
         size_t pos = 0;
@@ -853,12 +883,30 @@ j2k_status t2_read(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info*
                             }
                             const int np = get_npasses(br);
                             while (br.bit()) ++lblock[idx];
-                            const int lbits = lblock[idx] + floorlog2(np);
-                            if (lbits > 31) throw ReadErr{J2K_ERR_INVALID_ARG, "code-block length field too long"};
-                            const int len = (int)br.bits(lbits);
+                            const int p0 = tot_np[idx];
                             tot_np[idx] += np;
                             if (tot_np[idx] > 3 * included[idx] - 2)
                                 throw ReadErr{J2K_ERR_INVALID_ARG, "more passes than bit-planes allow"};
+                            // the new passes as pieces of codeword segments (B.10.7.2): a piece
+                            // ends where the style terminates the codeword, and at the last new
+                            // pass; each has a length of Lblock + floor(log2(its passes)) bits
+                            int64_t acc = 0;
+                            int start = p0;
+                            for (int q = p0; q < p0 + np; ++q) {
+                                const bool term = style && q + 1 < 3 * included[idx] - 2 &&
+                                                  j2k_pass_terminated(style, q, q + 2);
+                                if (!term && q != p0 + np - 1) continue;
+                                const int lbits = lblock[idx] + floorlog2(q + 1 - start);
+                                if (lbits > 31)
+                                    throw ReadErr{J2K_ERR_INVALID_ARG, "code-block length field too long"};
+                                acc += (int64_t)br.bits(lbits);
+                                if (acc + d.length > 0x7FFFFFFF)
+                                    throw ReadErr{J2K_ERR_INVALID_ARG, "code-block length"};
+                                if (pass_ends && style && l < keep)
+                                    (*pass_ends)[idx * J2K_PASS_STRIDE + q] = (uint32_t)(d.length + acc);
+                                start = q + 1;
+                            }
+                            const int len = (int)acc;
                             if (l < keep) {
                                 d.numbps = included[idx];
                                 d.npasses = (uint8_t)(d.npasses + np);
@@ -937,10 +985,11 @@ extern "C" j2k_status j2k_codestream_read_layers(const uint8_t* cs, size_t n, in
 }
 
 j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_stream_info* info,
-                               std::vector<j2k_cb_desc>* descs, std::vector<uint8_t>* bytes, std::string* err) {
+                               std::vector<j2k_cb_desc>* descs, std::vector<uint8_t>* bytes, std::string* err,
+                               std::vector<uint32_t>* pass_ends) {
     std::vector<std::vector<std::pair<uint32_t, int>>> segs;
     std::vector<uint8_t> tile;
-    J2K_TRY(t2_read(cs, n, max_layers, info, descs, &segs, &tile, err));
+    J2K_TRY(t2_read(cs, n, max_layers, info, descs, &segs, &tile, err, false, pass_ends));
     size_t total = 0;
     for (const auto& x : *descs) total += (size_t)x.length;
     bytes->resize(total + 1);
@@ -954,6 +1003,37 @@ j2k_status j2k_t2_parse_packed(const uint8_t* cs, size_t n, int max_layers, j2k_
     }
     bytes->resize(o);
     return J2K_OK;
+}
+
+extern "C" j2k_status j2k_codestream_pass_ends(const uint8_t* cs, size_t n, int max_layers, uint32_t* ends,
+                                               size_t cap, size_t* count, char* err, size_t errlen) {
+    J2K_API_BEGIN
+    if (!cs || !count || max_layers < 0) return J2K_ERR_INVALID_ARG;
+    j2k_stream_info info{};
+    std::vector<j2k_cb_desc> d;
+    std::vector<std::vector<std::pair<uint32_t, int>>> segs;
+    std::vector<uint8_t> tile;
+    std::vector<uint32_t> pe;
+    std::string msg;
+    j2k_status s = t2_read(cs, n, max_layers, &info, &d, &segs, &tile, &msg, false, &pe);
+    if (s != J2K_OK) {
+        if (err && errlen) {
+            std::strncpy(err, msg.c_str(), errlen - 1);
+            err[errlen - 1] = 0;
+        }
+        return s;
+    }
+    *count = d.size() * J2K_PASS_STRIDE;
+    if (!ends) return J2K_OK;
+    if (cap < *count) return J2K_ERR_CAPACITY;
+    if (pe.empty()) {  // no style: one segment per block, its whole codeword
+        for (size_t i = 0; i < d.size(); ++i)
+            for (int q = 0; q < J2K_PASS_STRIDE; ++q) ends[i * J2K_PASS_STRIDE + q] = (uint32_t)d[i].length;
+    } else {
+        std::memcpy(ends, pe.data(), pe.size() * 4);
+    }
+    return J2K_OK;
+    J2K_API_END
 }
 
 extern "C" j2k_status j2k_codestream_info(const uint8_t* cs, size_t n, j2k_stream_info* info, char* err,

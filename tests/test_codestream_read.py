@@ -177,3 +177,47 @@ def test_header_info_matches_the_full_parse(w, h, nc, L, cb):
         head = C.codestream_info(cs)
         full = C.read_codestream(cs)[0]
         assert all(head[k] == full[k] for k in head)
+
+
+@pytest.mark.parametrize("style", [1, 2, 4, 5, 6, 7])
+@pytest.mark.parametrize("w,h,nc,L,cb,lossless", [(200, 131, 3, 4, 32, True), (97, 64, 1, 5, 16, True),
+                                                  (128, 96, 3, 3, 64, False)])
+def test_styled_oracle_codestreams_parse_and_decode(style, w, h, nc, L, cb, lossless):
+    """Streams in the bypass / reset / per-pass termination styles: the reader gives the
+    style and each block's pass ends, and the oracle's styled block decoder, fed those segments,
+    rebuilds the coefficients, hence the image (lossless) or OpenJPEG's decode (lossy)."""
+    img = synth.gray(w, h, 3) if nc == 1 else synth.rgb(w, h, (5, 6, 7, 8))
+    cs = O.encode_image(img, L, cb, cb, lossless, style=style)
+    info, descs, data = C.read_codestream(cs)
+    assert info["cblk_style"] == style
+    pe = C.read_pass_ends(cs)
+    assert pe.shape == (len(descs), 92)
+    planes = np.zeros((nc, h, w), np.int32)
+    for d, ends in zip(descs, pe):
+        if d["npasses"] == 0:
+            continue
+        seg = bytes(data[d["offset"]:d["offset"] + d["length"]])
+        assert ends[d["npasses"] - 1] == d["length"]
+        blk = O.t1_decode_styled(seg, ends[:d["npasses"]], int(d["numbps"]), int(d["npasses"]), int(d["orient"]),
+                                 int(d["cw"]), int(d["ch"]), style)
+        planes[d["comp"], d["y0"]:d["y0"] + d["ch"], d["x0"]:d["x0"] + d["cw"]] = blk
+    if lossless:
+        rec = np.stack([O.dwt53_inv(p, L) for p in planes])
+        out = O.planar_inv(rec, 1 if nc == 3 else 0)
+        assert np.array_equal(out.reshape(img.shape), img)
+    else:
+        st = info["steps"]
+        rec = np.stack([O.dwt97_inv(O.dequantize(p, L, st), L) for p in planes])
+        out = O.planar_inv(rec, 2).reshape(img.shape)
+        ref = np.array(PIL.open(io.BytesIO(cs))).reshape(img.shape)
+        assert np.abs(out.astype(int) - ref.astype(int)).max() <= 1
+
+
+def test_unsupported_code_block_styles_are_refused():
+    cs = bytearray(O.encode_image(synth.gray(64, 48, 0), 2, 32, 32, True))
+    cod = cs.index(b"\xff\x52")
+    for sty, word in [(0x08, "causal"), (0x20, "segmentation")]:
+        bad = bytearray(cs)
+        bad[cod + 12] = sty
+        with pytest.raises(J2KError, match=word):
+            C.read_codestream(bytes(bad))
