@@ -477,6 +477,33 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
     return 0;
 }
 
+// The same for a block coded with a code-block style, its segments located by pass_ends
+// (J2K_PASS_STRIDE entries; values past len are clamped to it, as the kernel does).
+extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, const uint32_t* pass_ends, int numbps,
+                                               int npasses, int orient, int style, int cw, int ch, int32_t* out,
+                                               size_t pitch) {
+    if (cw < 1 || ch < 1 || cw > 64 || ch > 64 || orient < 0 || orient > 3 || numbps < 0 || numbps > 31 ||
+        npasses < 0 || npasses > 3 * numbps || npasses > J2K_PASS_STRIDE - 1 || len < 0 || (len > 0 && !data) ||
+        !out || pitch < (size_t)cw || !pass_ends || style < 0 || style > 7)
+        return -1;
+    DecSmem S;
+    for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
+    for (int k = 0; k < 19; ++k) S.st[k] = 0;
+    static const DecTables T = [] {
+        DecTables t{};
+        for (int i = 0; i < 4 * 512; ++i) fill_tables_entry(t, i);
+        return t;
+    }();
+    for (int y = 0; y < ch; ++y)
+        for (int x = 0; x < cw; ++x) out[(size_t)y * pitch + x] = 0;
+    if (numbps > 0 && npasses > 0)
+        decode_block<true>(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch, style, pass_ends);
+    for (int y = 0; y < ch; ++y)
+        for (int x = 0; x < cw; ++x)
+            if ((S.neg[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
+    return 0;
+}
+
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
                               cudaStream_t st, int style, const uint32_t* pass_ends, const uint8_t* job_style) {

@@ -190,61 +190,95 @@ class RelaxedQuant(torch.autograd.Function):
         return gy, gls.to(log_steps.dtype), None, None
 
 
+def _rd_forward(x, log_steps, levels, lam, seed):
+    """The forward of the fused loss: y = DWT(x), the quantiser keeping its noise u, the residual
+    d = IDWT(y_hat) - x fused into the last inverse level, and the loss scalar from the partial
+    sums.  Returns (loss, y, d, u)."""
+    x = x.detach().contiguous()
+    y = dwt97(x, levels)
+    c, h = _ctx(y)
+    n, hh, ww = y.shape
+    nb, k = 3 * levels + 1, _parts(hh)
+    ls = log_steps.detach().float().contiguous()
+    yh, u = torch.empty_like(y), torch.empty_like(y)
+    rparts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+    check(lib().j2k_relaxed_quant_forward_noise(h, _p(y), _p(yh), _p(u), n, ww, hh, levels, _p(ls), seed,
+                                                _p(rparts), k), h)
+    d = torch.empty_like(y)
+    sparts = torch.empty(lib().j2k_dwt97_residual_partials(ww, hh, n), device=y.device, dtype=torch.float32)
+    check(lib().j2k_dwt97_inverse_residual(h, _p(yh), _p(x), _p(d), n, ww, hh, levels, _p(sparts)), h)
+    del yh
+    # the loss scalar from both sets of partial sums, in one launch
+    loss = torch.empty((), device=y.device, dtype=torch.float32)
+    check(lib().j2k_dwt97_rd_finalize(h, _p(rparts), rparts.numel(), _p(sparts), sparts.numel(),
+                                      1.0 / x.numel(), float(lam), _p(loss)), h)
+    return loss, y, d, u
+
+
+def _rd_backward(y, d, u, log_steps, g, levels, lam, seed):
+    """The backward of the fused loss for output gradient g (0-dim, read on the device): inverse
+    adjoint of the residual, quantiser backward (scaled by 2/N and g), per-band log-step
+    gradient in one launch, forward adjoint with the -2/N residual fused in.  Returns (dL/dx,
+    dL/dlog_steps)."""
+    g = g.detach().float().contiguous()
+    alpha = 2.0 / d.numel()
+    g_res = idwt97_adjoint(d, levels)
+    c, h = _ctx(y)
+    n, hh, ww = y.shape
+    nb, k = 3 * levels + 1, _parts(hh)
+    ls = log_steps.detach().float().contiguous()
+    g_y = torch.empty_like(y)
+    parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
+    check(lib().j2k_relaxed_quant_backward_scaled(h, _p(y), _p(g_res), _p(g_y), n, ww, hh, levels, _p(ls), seed,
+                                                  _p(u), float(lam), _p(g), float(alpha), _p(parts), k), h)
+    del g_res
+    g_ls = torch.empty(nb, device=y.device, dtype=torch.float32)  # per band, in one launch
+    check(lib().j2k_dwt97_band_sum(h, _p(parts), n, nb, k, _p(g_ls)), h)
+    gx = forward_adjoint_residual(g_y, d, levels, scale=g, alpha=alpha)
+    return gx, g_ls
+
+
 class RDLoss(torch.autograd.Function):
     """Fused rate-distortion loss of a (N, H, W) float32 batch (one 0-dim CUDA tensor).
     Forward: DWT, quantiser, inverse with the residual fused in.  Backward: inverse adjoint of
     the residual, quantiser backward (scaled by 2/N and the output gradient on the device),
-    forward adjoint with the -2/N residual fused in."""
+    forward adjoint with the -2/N residual fused in.
+
+    checkpoint=True keeps nothing of the forward for the backward but the input: the lifting
+    outputs of every level (the coefficients y), the quantiser's noise and the residual are
+    recomputed in the backward from x (one more forward DWT, quantiser and inverse).  Between
+    the two passes the step then holds x alone instead of x, y, u and d, which is what lets a
+    batch, or one image, that does not fit four times over run at all; the gradients are
+    identical to the stored form's (the recomputation is the same deterministic kernels, the
+    noise the same Philox counters)."""
 
     @staticmethod
-    def forward(ctx, x, log_steps, levels, lam, seed):
-        x = x.detach().contiguous()
-        y = dwt97(x, levels)
-        c, h = _ctx(y)
-        n, hh, ww = y.shape
-        nb, k = 3 * levels + 1, _parts(hh)
-        ls = log_steps.detach().float().contiguous()
-        yh, u = torch.empty_like(y), torch.empty_like(y)
-        rparts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
-        check(lib().j2k_relaxed_quant_forward_noise(h, _p(y), _p(yh), _p(u), n, ww, hh, levels, _p(ls), seed,
-                                                    _p(rparts), k), h)
-        d = torch.empty_like(y)
-        sparts = torch.empty(lib().j2k_dwt97_residual_partials(ww, hh, n), device=y.device, dtype=torch.float32)
-        check(lib().j2k_dwt97_inverse_residual(h, _p(yh), _p(x), _p(d), n, ww, hh, levels, _p(sparts)), h)
-        del yh
-        # the loss scalar from both sets of partial sums, in one launch
-        loss = torch.empty((), device=y.device, dtype=torch.float32)
-        check(lib().j2k_dwt97_rd_finalize(h, _p(rparts), rparts.numel(), _p(sparts), sparts.numel(),
-                                          1.0 / x.numel(), float(lam), _p(loss)), h)
-        ctx.save_for_backward(y, d, u, log_steps)
-        ctx.levels, ctx.lam, ctx.seed = levels, lam, seed
+    def forward(ctx, x, log_steps, levels, lam, seed, checkpoint=False):
+        loss, y, d, u = _rd_forward(x, log_steps, levels, lam, seed)
+        if checkpoint:
+            del y, d, u
+            ctx.save_for_backward(x, log_steps)
+        else:
+            ctx.save_for_backward(y, d, u, log_steps)
+        ctx.levels, ctx.lam, ctx.seed, ctx.checkpoint = levels, lam, seed, checkpoint
         return loss
 
     @staticmethod
     def backward(ctx, g):
-        y, d, u, log_steps = ctx.saved_tensors
-        g = g.detach().float().contiguous()
-        alpha = 2.0 / d.numel()
-        g_res = idwt97_adjoint(d, ctx.levels)
-        c, h = _ctx(y)
-        n, hh, ww = y.shape
-        nb, k = 3 * ctx.levels + 1, _parts(hh)
-        ls = log_steps.detach().float().contiguous()
-        g_y = torch.empty_like(y)
-        parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
-        check(lib().j2k_relaxed_quant_backward_scaled(h, _p(y), _p(g_res), _p(g_y), n, ww, hh, ctx.levels, _p(ls),
-                                                      ctx.seed, _p(u), float(ctx.lam), _p(g), float(alpha), _p(parts),
-                                                      k), h)
-        del g_res
-        g_ls = torch.empty(nb, device=y.device, dtype=torch.float32)  # per band, in one launch
-        check(lib().j2k_dwt97_band_sum(h, _p(parts), n, nb, k, _p(g_ls)), h)
-        gx = forward_adjoint_residual(g_y, d, ctx.levels, scale=g, alpha=alpha)
-        return gx, g_ls.to(log_steps.dtype), None, None, None
+        if ctx.checkpoint:
+            x, log_steps = ctx.saved_tensors
+            _, y, d, u = _rd_forward(x, log_steps, ctx.levels, ctx.lam, ctx.seed)
+        else:
+            y, d, u, log_steps = ctx.saved_tensors
+        gx, g_ls = _rd_backward(y, d, u, log_steps, g, ctx.levels, ctx.lam, ctx.seed)
+        return gx, g_ls.to(log_steps.dtype), None, None, None, None
 
 
-def rd_loss(x, log_steps, levels=5, lam=0.01, seed=0):
-    """Rate-distortion loss of a (N, H, W) float32 batch; differentiable in x and log_steps."""
-    return RDLoss.apply(x, log_steps, levels, lam, seed)
+def rd_loss(x, log_steps, levels=5, lam=0.01, seed=0, checkpoint=False):
+    """Rate-distortion loss of a (N, H, W) float32 batch; differentiable in x and log_steps.
+    checkpoint=True recomputes the forward's intermediates in the backward instead of keeping
+    them (see RDLoss)."""
+    return RDLoss.apply(x, log_steps, levels, lam, seed, checkpoint)
 
 
 def rd_loss_composed(x, log_steps, levels=5, lam=0.01, seed=0):

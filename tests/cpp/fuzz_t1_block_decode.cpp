@@ -4,7 +4,8 @@
 // a random size (1..64 a side, at most 4096 samples), orientation, bit-plane count, a pass count
 // the kernel's descriptor check admits (0..3*numbps) and a codeword of random, all-0xFF or
 // sparse bytes held in a buffer of exactly its length, so that any read past the codeword's end
-// is a sanitizer report.  Prints "decoded N" and exits 0.
+// is a sanitizer report.  Every other block is decoded as coded in a random code-block style
+// with random pass ends (j2k_t1_decode_block_styled_host).  Prints "decoded N" and exits 0.
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -13,6 +14,9 @@
 
 extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
                                         int cw, int ch, int32_t* out, size_t pitch);
+extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, const uint32_t* pass_ends, int numbps,
+                                               int npasses, int orient, int style, int cw, int ch, int32_t* out,
+                                               size_t pitch);
 
 int main(int argc, char** argv) {
     const int iters = argc > 1 ? std::atoi(argv[1]) : 1000;
@@ -30,8 +34,23 @@ int main(int argc, char** argv) {
         const int mode = (int)(rng() % 3);
         for (auto& b : data) b = mode == 0 ? (uint8_t)rng() : mode == 1 ? 0xFF : (uint8_t)(rng() & 0x8F);
         std::vector<int32_t> out((size_t)ch * cw);
-        if (j2k_t1_decode_block_host(len ? data.data() : nullptr, len, numbps, npasses, (int)(rng() % 4), cw, ch,
-                                     out.data(), (size_t)cw) != 0) {
+        if (it % 2 == 1 && npasses <= 91) {
+            // a code-block style, with pass ends that need not make sense (out of order, past
+            // the codeword, zero)
+            std::vector<uint32_t> pe(92);
+            uint32_t at = 0;
+            for (auto& e : pe) {
+                const int k = (int)(rng() % 8);
+                e = k == 0 ? (uint32_t)rng() : k == 1 ? 0u : (at += (uint32_t)(rng() % 200));
+            }
+            if (j2k_t1_decode_block_styled_host(len ? data.data() : nullptr, len, pe.data(), numbps, npasses,
+                                                (int)(rng() % 4), 1 + (int)(rng() % 7), cw, ch, out.data(),
+                                                (size_t)cw) != 0) {
+                std::printf("refused styled block %d\n", it);
+                return 1;
+            }
+        } else if (j2k_t1_decode_block_host(len ? data.data() : nullptr, len, numbps, npasses, (int)(rng() % 4), cw,
+                                            ch, out.data(), (size_t)cw) != 0) {
             std::printf("refused block %d\n", it);
             return 1;
         }

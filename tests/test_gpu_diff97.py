@@ -182,3 +182,51 @@ def test_graphed_step_matches_eager_step(D):
         ref.backward()
         assert loss == ref.item()
         assert torch.equal(x.grad, xe.grad) and torch.equal(ls.grad, le.grad)
+
+
+def test_checkpointed_step_matches_stored_step_and_fd64(D):
+    """checkpoint=True (the forward keeps only x; the backward recomputes the coefficients,
+    the noise and the residual) gives the stored form's loss and gradients exactly, holds less
+    memory between the passes, and matches FP64 finite differences on the config's crop."""
+    L, lam, seed = 5, 0.01, 200
+    xs = torch.from_numpy(synth.float_batch(3, 256, 192, 70)).cuda()
+    ls0 = torch.full((3 * L + 1,), math.log(1 / 64.0), device="cuda")
+    res = []
+    for ck in (False, True):
+        x = xs.clone().requires_grad_(True)
+        ls = ls0.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        base = torch.cuda.memory_allocated()
+        loss = D.rd_loss(x, ls, L, lam, seed, checkpoint=ck)
+        held = torch.cuda.memory_allocated() - base  # kept for the backward
+        loss.backward()
+        res.append((loss.item(), x.grad.clone(), ls.grad.clone(), held))
+    assert res[0][0] == res[1][0]
+    assert torch.equal(res[0][1], res[1][1]) and torch.equal(res[0][2], res[1][2])
+    plane = xs.numel() * 4
+    assert res[0][3] >= 3 * plane and res[1][3] < plane  # y, d and u kept, against none
+    # FD64 on the 64x64 crop of config 3, checkpointed
+    x = _crop()
+    lsn = np.full(3 * L + 1, math.log(1 / 64.0))
+    xt = torch.from_numpy(x.astype(np.float32))[None].cuda().requires_grad_(True)
+    lt = torch.from_numpy(lsn.astype(np.float32)).cuda().requires_grad_(True)
+    D.rd_loss(xt, lt, L, lam, seed, checkpoint=True).backward()
+    gx = xt.grad[0].cpu().double().numpy()
+    gl = lt.grad.cpu().double().numpy()
+    h = 1e-6
+    _, ref_gx, _ = O.rd_loss(x, L, lsn, lam, seed)
+    scale_x = np.abs(ref_gx).max()
+    rng = np.random.default_rng(5)
+    for _ in range(12):
+        i, j = rng.integers(0, 64, 2)
+        xp, xm = x.copy(), x.copy()
+        xp[i, j] += h
+        xm[i, j] -= h
+        fd = (O.rd_loss(xp, L, lsn, lam, seed, False) - O.rd_loss(xm, L, lsn, lam, seed, False)) / (2 * h)
+        assert abs(gx[i, j] - fd) <= GRAD_TOL * max(abs(fd), 0.05 * scale_x)
+    for b in range(0, len(lsn), 3):
+        lp, lm = lsn.copy(), lsn.copy()
+        lp[b] += h
+        lm[b] -= h
+        fd = (O.rd_loss(x, L, lp, lam, seed, False) - O.rd_loss(x, L, lm, lam, seed, False)) / (2 * h)
+        assert abs(gl[b] - fd) <= GRAD_TOL * max(abs(fd), 1e-3)

@@ -46,7 +46,9 @@ def test_t2_reader_under_sanitizers(tmp_path):
     PIL = pytest.importorskip("PIL.Image")
     import io
     seeds = [bytes(O.encode_image(synth.rgb(96, 80, (5, 6, 7, 8)), 3, 32, 32, True)),
-             bytes(O.encode_image(synth.gray(131, 97, 9), 4, 64, 64, True))]
+             bytes(O.encode_image(synth.gray(131, 97, 9), 4, 64, 64, True)),
+             bytes(O.encode_image(synth.gray(90, 70, 3), 3, 16, 16, True, style=O.STYLE_BYPASS | O.STYLE_TERMALL)),
+             bytes(O.encode_image(synth.rgb(64, 64, (1, 2, 3, 4)), 3, 32, 32, False, style=7))]
     buf = io.BytesIO()
     PIL.fromarray(synth.rgb(72, 56, (11, 12, 13, 14))).save(
         buf, "JPEG2000", irreversible=False, mct=1, num_resolutions=4, codeblock_size=(16, 16), progression="RLCP",
