@@ -391,7 +391,7 @@ template <int KERN>
 struct TmaStrip {
     static constexpr int NY = kTmaTh + 2 * KT<KERN>::H;
     static constexpr int BYTES = NY * FNX * 4;
-    static constexpr int SMEM = 2 * BYTES + kTmaTh * FNX * 4;
+    static constexpr int SMEM = 2 * BYTES + kTmaTh * FNX * 4 + 16;  // two strips, the rows, two barriers
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -406,7 +406,7 @@ dwt_fwd_tma(const __grid_constant__ CUtensorMap tmap, int w, int h, int nz, int 
     extern __shared__ __align__(128) unsigned char dsm[];
     T(*stg)[NY][FNX] = reinterpret_cast<T(*)[NY][FNX]>(dsm);                             // [2][NY][FNX]
     T(*s)[FNX] = reinterpret_cast<T(*)[FNX]>(dsm + 2 * TmaStrip<KERN>::BYTES);             // [16][FNX]
-    __shared__ __align__(8) uint64_t bar[2];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + 2 * TmaStrip<KERN>::BYTES + kTmaTh * FNX * 4);  // [2]
     const int t = threadIdx.x;
     const int ntiles = tiles_x * tiles_y * nz;
     if (t == 0) {
