@@ -382,16 +382,18 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
 // tile's copy is in flight while the current tile is lifted.  Strip samples outside the plane
 // arrive as zeros and are never used: every thread reads its column through the mirror map
 // (whole-sample symmetric extension), and the mirrored sample of every row and column an output
-// depends on lies inside the strip.  Vertical lifting then runs per column in registers and the
-// horizontal pass is fwd_fast_rows, as in dwt_fwd_fast, so the outputs are identical.  No
-// multicast: each copy reads this GPU's plane into this CTA's shared memory.
+// depends on lies inside the strip.  Vertical lifting then runs per column in registers, the
+// lifted rows go back into the strip in place, and the horizontal pass is fwd_fast_rows on the
+// strip, as in dwt_fwd_fast, so the outputs are identical.  Shared memory is the two strips
+// alone (40 KB for 5/3, 48 KB for 9/7).  No multicast: each copy reads this GPU's plane into this
+// CTA's shared memory.
 constexpr int kTmaTh = 16;
 
 template <int KERN>
 struct TmaStrip {
     static constexpr int NY = kTmaTh + 2 * KT<KERN>::H;
     static constexpr int BYTES = NY * FNX * 4;
-    static constexpr int SMEM = 2 * BYTES + kTmaTh * FNX * 4 + 16;  // two strips, the rows, two barriers
+    static constexpr int SMEM = 2 * BYTES + 16;  // two strips, two barriers
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -405,8 +407,7 @@ dwt_fwd_tma(const __grid_constant__ CUtensorMap tmap, int w, int h, int nz, int 
     constexpr int HV = KT<KERN>::H, NY = TmaStrip<KERN>::NY;
     extern __shared__ __align__(128) unsigned char dsm[];
     T(*stg)[NY][FNX] = reinterpret_cast<T(*)[NY][FNX]>(dsm);                             // [2][NY][FNX]
-    T(*s)[FNX] = reinterpret_cast<T(*)[FNX]>(dsm + 2 * TmaStrip<KERN>::BYTES);             // [16][FNX]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + 2 * TmaStrip<KERN>::BYTES + kTmaTh * FNX * 4);  // [2]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + 2 * TmaStrip<KERN>::BYTES);  // [2]
     const int t = threadIdx.x;
     const int ntiles = tiles_x * tiles_y * nz;
     if (t == 0) {
@@ -472,7 +473,7 @@ dwt_fwd_tma(const __grid_constant__ CUtensorMap tmap, int w, int h, int nz, int 
             if (!inner_y) sy = min(max(mirror(y0 - HV + r, h) - (y0 - HV), 0), NY - 1);
             c[r] = stg[stage][sy][sx];
         }
-        __syncthreads();  // the stage is free for the copy after next, and s for this tile
+        __syncthreads();  // every column read (mirrored reads cross columns) before any write-back
         // 2. vertical lifting of column t in registers
         if (h > 1) {
 #pragma unroll
@@ -487,12 +488,13 @@ dwt_fwd_tma(const __grid_constant__ CUtensorMap tmap, int w, int h, int nz, int 
         for (int r = HV; r < HV + kTmaTh; ++r) {
             T v = c[r];
             if (KERN == 97 && h > 1) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
-            s[r - HV][t] = v;
+            stg[stage][r][t] = v;  // the lifted rows go back into the strip, in place
         }
         __syncthreads();
-        // 3. horizontal lifting and the subband writes
-        fwd_fast_rows<KERN, TD, QUANT, QLL, kTmaTh, HV>(s, x0, y0, w, h, ll_dst + tz * z.ll, llpitch,
-                                                        dst + tz * z.dst, dpitch, st, vec_out);
+        // 3. horizontal lifting and the subband writes, from the strip's rows HV .. HV+15
+        fwd_fast_rows<KERN, TD, QUANT, QLL, kTmaTh, 0>(stg[stage], x0, y0, w, h, ll_dst + tz * z.ll, llpitch,
+                                                       dst + tz * z.dst, dpitch, st, vec_out);
+        __syncthreads();  // the strip is free for the copy issued at the top of the next tile
     }
 }
 

@@ -23,6 +23,10 @@ benchmark workloads but stay within a few hundred MB of device memory:
                RCT) from code-blocks already on the host
   rate         one lossless 4096x4096 RGB encode cut to 1 bit per pixel by PCRD-opt (tier-1
                rate path, distortion pass, host PCRD and header sizing, descriptor update)
+  dwt53-tma    as dwt53, with the TMA-staged level kernel (tuning key J2K_TUNE_DWT_TMA)
+  dwt53-all-tma  as dwt53-all, with the TMA-staged level kernel
+  encode-styled  the lossless 4096x4096 RGB encode with code-block style RESET | TERMALL (every
+               pass of a block coded in its own lane)
 """
 import math
 import sys
@@ -46,6 +50,22 @@ def case_dwt53(levels=1):
     planes = C.rgb_to_planar(_rgb(), 1)
     out = torch.empty_like(planes)
     return lambda: C.dwt_forward(planes, levels, out=out)
+
+
+def _tma(on):
+    from ._lib import lib
+    lib().j2k_ctx_set_tuning(C.default_context(0).h, 7, 1 if on else 0)
+
+
+def case_dwt53_tma(levels=1):
+    _tma(True)
+    return case_dwt53(levels)
+
+
+def case_encode_styled():
+    img = _rgb()
+    enc = C.OCLEncoder(lossy=False)
+    return lambda: enc.run_rgb(img, levels=6, cbw=64, cbh=64, cblk_style=6)
 
 
 def case_idwt53():
@@ -125,7 +145,8 @@ def case_rate():
 CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_dwt53(6),
          "idwt53": case_idwt53, "tier1": case_tier1, "encode": case_encode,
          "diff-kernels": case_diff_kernels, "diff-step": case_diff_step, "batched": case_batched,
-         "decode": case_decode, "rate": case_rate}
+         "decode": case_decode, "rate": case_rate, "dwt53-tma": case_dwt53_tma,
+         "dwt53-all-tma": lambda: case_dwt53_tma(6), "encode-styled": case_encode_styled}
 
 
 def main(argv):
