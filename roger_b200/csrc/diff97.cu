@@ -272,6 +272,8 @@ relaxed_quant_k(const float* __restrict__ y, const float* __restrict__ gin, floa
     extern __shared__ float acc[];  // [band][256]
     __shared__ float stp[49], rstp[49];
     __shared__ int wlim[17], hlim[17];
+    griddep_launch_dependents();
+    griddep_wait();  // launched as a dependent: the previous kernel's writes are visible from here
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5, img = blockIdx.y;
     const int L = lv.L, nb = 3 * L + 1;
     for (int b = 0; b < nb; ++b) acc[b * 256 + t] = 0.0f;
@@ -432,12 +434,11 @@ j2k_status fwd_adj_run(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, s
             const dim3 fg((ws[k] + FTW - 1) / FTW, (hs[k] + STH - 1) / STH, n);
             const ZStride zs{plane, oz, llz};
             if (fused)
-                dwt_syn_fast<97, 1, float, false, false, 2><<<fg, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k],
-                                                                                 out, op, Steps4{}, zs, vec, *ex);
+                J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 1, float, false, false, 2>, fg, dim3(256), st, true, g_coef, w,
+                                         ll, llp, ws[k], hs[k], out, op, Steps4{}, zs, vec, *ex));
             else
-                dwt_syn_fast<97, 1, float, false, false, 0><<<fg, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k],
-                                                                                 out, op, Steps4{}, zs, vec,
-                                                                                 SynExtra{});
+                J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 1, float, false, false, 0>, fg, dim3(256), st, true, g_coef, w,
+                                         ll, llp, ws[k], hs[k], out, op, Steps4{}, zs, vec, SynExtra{}));
         } else {
             dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
             fwd_adj_level<<<g, 256, 0, st>>>(g_coef, w, ll, llp, ws[k], hs[k], out, op, plane, llz, oz);
@@ -472,9 +473,9 @@ j2k_status quant_run(j2k_ctx* ctx, bool bwd, const float* y, const float* gin, f
         if (smem > 48 * 1024)                                                                                  \
             J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<B_, N_>,                                        \
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));       \
-        relaxed_quant_k<B_, N_><<<g, 256, smem, ctx->stream>>>(y, gin, out, (int)w, (int)h, plane, lv,         \
-                                                              log_steps, seed, lam, gscale, alpha, partials,   \
-                                                              rows, vec, noise);                               \
+        J2K_CUDA(ctx, launch_pdl_smem(relaxed_quant_k<B_, N_>, g, dim3(256), smem, ctx->stream, true, y, gin, out, \
+                                      (int)w, (int)h, plane, lv, log_steps, seed, lam, gscale, alpha, partials,    \
+                                      rows, vec, noise));                                                          \
     } while (0)
     if (bwd) {
         if (noise) RQ_LAUNCH(true, true);
@@ -521,6 +522,8 @@ __global__ void __launch_bounds__(1024) rd_finalize_kernel(const float* __restri
                                                           const float* __restrict__ sq, size_t nsq, double inv_count,
                                                           float lam, float* __restrict__ loss) {
     __shared__ float sh[1024];
+    griddep_launch_dependents();
+    griddep_wait();
     const float r = cta_sum(rate, nrate, sh);
     const float q = cta_sum(sq, nsq, sh);
     if (threadIdx.x == 0) *loss = (float)((double)q * inv_count) + lam * r;
@@ -530,6 +533,8 @@ __global__ void __launch_bounds__(1024) rd_finalize_kernel(const float* __restri
 __global__ void __launch_bounds__(256) band_sum_kernel(const float* __restrict__ parts, int n, int nb, int k,
                                                        float* __restrict__ out) {
     __shared__ float sh[256];
+    griddep_launch_dependents();
+    griddep_wait();
     const int b = blockIdx.x;
     float v = 0.0f;
     for (int t = threadIdx.x; t < n * k; t += blockDim.x) v += parts[((size_t)(t / k) * nb + b) * k + (t % k)];
@@ -551,7 +556,8 @@ j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_
     J2K_API_BEGIN
     if (!ctx || !loss || (!rate_partials && nrate) || (!sq_partials && nsq)) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    rd_finalize_kernel<<<1, 1024, 0, ctx->stream>>>(rate_partials, nrate, sq_partials, nsq, inv_count, lam, loss);
+    J2K_CUDA(ctx, launch_pdl(rd_finalize_kernel, dim3(1), dim3(1024), ctx->stream, true, rate_partials, nrate,
+                             sq_partials, nsq, inv_count, lam, loss));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
     J2K_API_END
@@ -561,7 +567,8 @@ j2k_status j2k_dwt97_band_sum(j2k_ctx* ctx, const float* partials, int n, int nb
     J2K_API_BEGIN
     if (!ctx || !partials || !out || n < 1 || nb < 1 || k < 1) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    band_sum_kernel<<<(unsigned)nb, 256, 0, ctx->stream>>>(partials, n, nb, k, out);
+    J2K_CUDA(ctx, launch_pdl(band_sum_kernel, dim3((unsigned)nb), dim3(256), ctx->stream, true, partials, n, nb, k,
+                             out));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
     J2K_API_END
@@ -619,8 +626,8 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
             const int vout = (((uintptr_t)g_coef & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) &&
                              (((uintptr_t)ll & 7) == 0) && ((llp & 1) == 0) && ((llz & 1) == 0);
             const dim3 fg((ws[k] + FTW - 1) / FTW, (hs[k] + STH - 1) / STH, n);
-            iadj_ana_fast<<<fg, 256, 0, st>>>(in, ip, ws[k], hs[k], g_coef, w, ll, llp, ZStride{iz, plane, llz}, vin,
-                                              vout);
+            J2K_CUDA(ctx, launch_pdl(iadj_ana_fast, fg, dim3(256), st, true, in, ip, ws[k], hs[k], g_coef, w, ll, llp,
+                                     ZStride{iz, plane, llz}, vin, vout));
         } else {
             dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
             inv_adj_level<<<g, 256, 0, st>>>(in, ip, ws[k], hs[k], g_coef, w, ll, llp, iz, plane, llz);
@@ -677,8 +684,8 @@ j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float*
     const int vec = (((uintptr_t)y & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) && (((uintptr_t)ll & 7) == 0) &&
                     ((llp & 1) == 0) && ((llz & 1) == 0) && ((wl & 1) == 0);
     const SynExtra ex{x, w, plane, nullptr, 1.0f, sq_partials};
-    dwt_syn_fast<97, 0, float, false, false, 1><<<fg, 256, 0, st>>>(y, w, ll, llp, (int)w, (int)h, d, w, Steps4{},
-                                                                     ZStride{plane, plane, llz}, vec, ex);
+    J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 0, float, false, false, 1>, fg, dim3(256), st, true, y, w, ll, llp,
+                             (int)w, (int)h, d, w, Steps4{}, ZStride{plane, plane, llz}, vec, ex));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
     J2K_API_END

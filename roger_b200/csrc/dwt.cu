@@ -973,17 +973,22 @@ j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
                             ((wl & 1) == 0);
             const dim3 fg((cw + FTW - 1) / FTW, (chh + STH - 1) / STH, n);
             const SynExtra ex{};
+            // every synthesis kernel waits for its predecessor's grid first, so each one is
+            // launched as a programmatic dependent (its launch overlaps the predecessor's tail)
+            const dim3 b(256);
+            cudaError_t le;
             if (deq) {
                 if (k == levels - 1)
-                    dwt_syn_fast<KERN, 0, int32_t, true, true, 0><<<fg, 256, 0, stream>>>(
-                        (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
+                    le = launch_pdl(dwt_syn_fast<KERN, 0, int32_t, true, true, 0>, fg, b, stream, true,
+                                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
                 else
-                    dwt_syn_fast<KERN, 0, int32_t, true, false, 0><<<fg, 256, 0, stream>>>(
-                        (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
+                    le = launch_pdl(dwt_syn_fast<KERN, 0, int32_t, true, false, 0>, fg, b, stream, true,
+                                    (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
             } else {
-                dwt_syn_fast<KERN, 0, T, false, false, 0><<<fg, 256, 0, stream>>>(
-                    (const T*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
+                le = launch_pdl(dwt_syn_fast<KERN, 0, T, false, false, 0>, fg, b, stream, true, (const T*)in,
+                                in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
             }
+            J2K_CUDA(ctx, le);
         } else if (deq) {
             if (k == levels - 1)
                 dwt_inv_level<KERN, ORDER, TW, TH, int32_t, true, true><<<grid, 256, 0, stream>>>(

@@ -101,11 +101,12 @@ __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wa
 // Launches k<<<g, b, 0, s>>>(args...); with pdl, as a programmatic dependent of the previous
 // kernel on the stream (cudaLaunchAttributeProgrammaticStreamSerialization).
 template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*k)(KArgs...), dim3 g, dim3 b, cudaStream_t s, bool pdl, Args... args) {
+cudaError_t launch_pdl_smem(void (*k)(KArgs...), dim3 g, dim3 b, size_t smem, cudaStream_t s, bool pdl,
+                            Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = g;
     cfg.blockDim = b;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -113,6 +114,10 @@ cudaError_t launch_pdl(void (*k)(KArgs...), dim3 g, dim3 b, cudaStream_t s, bool
     cfg.attrs = pdl ? at : nullptr;
     cfg.numAttrs = pdl ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, k, args...);
+}
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 g, dim3 b, cudaStream_t s, bool pdl, Args... args) {
+    return launch_pdl_smem(k, g, b, 0, s, pdl, args...);
 }
 
 // ---- transposed 9/7 steps -----------------------------------------------------------------------
@@ -282,6 +287,8 @@ dwt_syn_fast(const TS* __restrict__ src, size_t spitch, const typename KT<KERN>:
     using T = typename KT<KERN>::T;
     constexpr int HV = KT<KERN>::H, NY = STH + 2 * HV;
     __shared__ __align__(16) T s[NY][FNX];
+    griddep_launch_dependents();
+    griddep_wait();  // launched as a dependent: the previous kernel's writes are visible from here
     src += blockIdx.z * z.src;
     ll_src += blockIdx.z * z.ll;
     out += blockIdx.z * z.dst;
@@ -426,6 +433,8 @@ iadj_ana_fast(const float* __restrict__ gin, size_t ipitch, int w, int h, float*
               float* __restrict__ gll, size_t llpitch, ZStride z, int vec_in, int vec_out) {
     constexpr int HV = 4, NY = STH + 2 * HV;
     __shared__ __align__(16) float s[STH][FNX];  // the vertically lifted rows y0 .. y0+STH-1
+    griddep_launch_dependents();
+    griddep_wait();  // launched as a dependent: the previous kernel's writes are visible from here
     gin += blockIdx.z * z.src;
     gdst += blockIdx.z * z.dst;
     gll += blockIdx.z * z.ll;
