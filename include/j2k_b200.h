@@ -412,7 +412,8 @@ typedef struct {
 typedef struct j2k_batch j2k_batch;
 enum {
     J2K_BATCH_USE_GRAPH = 1,     /* 1 (default): capture the launch sequence once, replay it */
-    J2K_BATCH_TILE53 = 2,        /* DWT tile shape of 5/3 images: 0 64x64, 1 128x32, 2 32x128 */
+    J2K_BATCH_TILE53 = 2,        /* DWT tile shape of 5/3 images: 0 64x64, 1 128x32, 2 32x128 (shared-memory
+                                    tiles), 3 (default) 248x16 register lifting */
     J2K_BATCH_TILE97 = 3,        /* same for 9/7 images */
     J2K_BATCH_PHASE_A_ORDER = 4, /* 1: context modelling takes the largest code-blocks first */
     J2K_BATCH_MQ_VARIANT = 5,    /* read-only here; set with j2k_ctx_set_tuning */

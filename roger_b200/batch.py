@@ -9,7 +9,7 @@ import torch
 from . import _lib as L
 from ._lib import check, lib
 
-TILE_NAMES = {0: "64x64", 1: "128x32", 2: "32x128"}
+TILE_NAMES = {0: "64x64", 1: "128x32", 2: "32x128", 3: "248x16 register lifting"}
 
 
 def split_packed(first, descs, data):

@@ -61,8 +61,11 @@ struct ImgPlan {
     size_t job0 = 0, njobs = 0;
 };
 
+// tile shapes of the batched forward DWT: 0-2 the shared-memory tile kernel, 3 the
+// register-lifting kernel (248 output columns x 16 rows, the form the per-image path uses)
 j2k_dwt_tile tile_of(int code) {
-    return code == 1 ? j2k_dwt_tile{128, 32} : (code == 2 ? j2k_dwt_tile{32, 128} : j2k_dwt_tile{64, 64});
+    return code == 1 ? j2k_dwt_tile{128, 32}
+                     : (code == 2 ? j2k_dwt_tile{32, 128} : (code == 3 ? j2k_dwt_tile{248, 16} : j2k_dwt_tile{64, 64}));
 }
 
 }  // namespace
@@ -80,7 +83,7 @@ struct j2k_batch {
     size_t out_bytes = 0, sym_bytes = 0;
     double out_factor = 2.0, sym_factor = 20.0;  // capacity per sample (grown on overflow)
     // tuning
-    int tile_code[2] = {0, 0};
+    int tile_code[2] = {3, 3};
     int phase_a_order = 1;  // 1: largest blocks first, 0: natural order
     bool use_graph = true;
     int stages = 7;  // J2K_BATCH_STAGES: 1 planar, 2 DWT, 4 tier-1
@@ -250,6 +253,9 @@ static j2k_status plan_dwt(j2k_batch* b) {
                         d.s_hh = im.steps[bt + 2];
                         d.flags = 1 | (last ? 2 : 0);
                     }
+                    if ((((uintptr_t)d.dst & 7) == 0) && ((d.dpitch & 1) == 0) && (((uintptr_t)d.ll_dst & 7) == 0) &&
+                        ((d.llpitch & 1) == 0))
+                        d.flags |= 4;  // 8-byte vector stores of sample pairs
                     d.tiles_x = (d.w + t.tw - 1) / t.tw;
                     const int ty = (d.h + t.th - 1) / t.th;
                     d.tile0 = (uint32_t)(owners.size() - b->lowner_first[f][k]);  // launch-relative
@@ -459,7 +465,7 @@ j2k_status j2k_batch_set_option(j2k_batch* b, int key, int value) {
         case J2K_BATCH_USE_GRAPH: b->use_graph = value != 0; break;
         case J2K_BATCH_TILE53:
         case J2K_BATCH_TILE97:
-            if (value < 0 || value > 2) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tile code must be 0, 1 or 2");
+            if (value < 0 || value > 3) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tile code must be 0, 1, 2 or 3");
             b->tile_code[key == J2K_BATCH_TILE97] = value;
             J2K_TRY(plan_dwt(b));
             break;
@@ -594,7 +600,7 @@ j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report) {
     for (int f = 0; f < 2 && s == J2K_OK; ++f) {
         int best_code = 0;
         float best_t = 1e30f;
-        for (int code = 0; code < 3 && s == J2K_OK; ++code) {
+        for (int code = 0; code < 4 && s == J2K_OK; ++code) {
             b->tile_code[f] = code;
             s = plan_dwt(b);
             if (s == J2K_OK) s = time_stage(false, true, false, &t);

@@ -301,6 +301,51 @@ __device__ __forceinline__ void fwd_fast_rows(typename KT<KERN>::T (*s)[FNX], in
     }
 }
 
+// One 248 x FTH output tile of a forward level in the register-load form: each thread loads its
+// column of the strip (columns x0-4 .. x0+251, rows y0-HV .. y0+FTH+HV-1, mirrored at the image
+// edges) straight into registers, lifts it vertically there, and the FTH lifted rows go through
+// s (FTH x FNX) to the horizontal pass and the subband writes (fwd_fast_rows).
+template <int KERN, typename TD, bool QUANT, bool QLL, int FTH>
+__device__ __forceinline__ void fwd_fast_tile_reg(typename KT<KERN>::T (*s)[FNX],
+                                                  const typename KT<KERN>::T* __restrict__ src, size_t spitch,
+                                                  int w, int h, typename KT<KERN>::T* __restrict__ ll_dst,
+                                                  size_t llpitch, TD* __restrict__ dst, size_t dpitch, Steps4 st,
+                                                  int vec_out, int x0, int y0) {
+    using T = typename KT<KERN>::T;
+    constexpr int HV = KT<KERN>::H, NY = FTH + 2 * HV;
+    const int t = threadIdx.x;
+    const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
+    const bool inner_y = (y0 - HV >= 0) && (y0 + FTH + HV <= h);
+    T c[NY];
+    // 1. column t of the strip
+    const int gx = x0 - 4 + t;
+    const T* colp = src + (inner_x ? gx : mirror(gx, w));
+#pragma unroll
+    for (int r = 0; r < NY; ++r) {
+        const int gy = inner_y ? y0 - HV + r : mirror(y0 - HV + r, h);
+        c[r] = __ldg(colp + (size_t)gy * spitch);
+    }
+    // 2. vertical lifting of column t in registers
+    if (h > 1) {
+#pragma unroll
+        for (int k = 0; k < KT<KERN>::NSTEP; ++k) {
+            const int par = 1 - (k & 1);
+#pragma unroll
+            for (int r = k + 1; r < NY - k - 1; ++r)
+                if ((r & 1) == par) c[r] = KT<KERN>::op(false, k, c[r], c[r - 1], c[r + 1]);
+        }
+    }
+#pragma unroll
+    for (int r = HV; r < HV + FTH; ++r) {
+        T v = c[r];
+        if (KERN == 97 && h > 1) v = (T)__fmul_rn((float)v, (r & 1) ? KMUL : KDIV);
+        s[r - HV][t] = v;
+    }
+    __syncthreads();
+    // 3. horizontal lifting and the subband writes
+    fwd_fast_rows<KERN, TD, QUANT, QLL, FTH, HV>(s, x0, y0, w, h, ll_dst, llpitch, dst, dpitch, st, vec_out);
+}
+
 // REG: each thread loads its column of the strip straight from global memory into registers
 // (coalesced 4-byte loads, all NY in flight at once), so the strip is never staged in shared
 // memory; only the FTH vertically lifted rows go through shared memory to the horizontal pass.
@@ -320,19 +365,14 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
     __shared__ __align__(16) T s[SR][FNX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, t = threadIdx.x;
     const int x0 = blockIdx.x * FTW, y0 = blockIdx.y * FTH;
+    if constexpr (REG) {
+        fwd_fast_tile_reg<KERN, TD, QUANT, QLL, FTH>(s, src, spitch, w, h, ll_dst, llpitch, dst, dpitch, st,
+                                                     vec_out, x0, y0);
+        return;
+    }
     const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
     T c[NY];
-    if constexpr (REG) {
-        // 1. column t of the strip, rows y0-HV .. y0+FTH+HV-1 (mirrored at the image edges)
-        const bool inner_y = (y0 - HV >= 0) && (y0 + FTH + HV <= h);
-        const int gx = x0 - 4 + t;
-        const T* colp = src + (inner_x ? gx : mirror(gx, w));
-#pragma unroll
-        for (int r = 0; r < NY; ++r) {
-            const int gy = inner_y ? y0 - HV + r : mirror(y0 - HV + r, h);
-            c[r] = __ldg(colp + (size_t)gy * spitch);
-        }
-    } else {
+    {
         // 1. load the strip: every copy of the CTA in flight at once (cp.async, no register staging)
         for (int r = warp; r < NY; r += 8) {
             const T* row = src + (size_t)mirror(y0 - HV + r, h) * spitch;
@@ -373,6 +413,60 @@ dwt_fwd_fast(const typename KT<KERN>::T* __restrict__ src, size_t spitch, int w,
     __syncthreads();
     // 3. horizontal lifting and the subband writes
     fwd_fast_rows<KERN, TD, QUANT, QLL, FTH, RO>(s, x0, y0, w, h, ll_dst, llpitch, dst, dpitch, st, vec_out);
+}
+
+// The batched level in the register-lifting form (T.800 order): CTA b takes tile b - d.tile0 of
+// its image's level (248 output columns x 16 rows, tiles row-major), and runs the same tile as
+// dwt_fwd_fast.  A level narrower than 8 or lower than 2 samples takes the shared-memory tile
+// instead (fwd_tile, 64 x 16 sub-tiles over the CTA's 248 x 16 region).  The descriptor's flags:
+// 1 quantise the details (9/7), 2 last level (LL quantised into dst), 4 8-byte vector stores.
+constexpr int kBatchFastTh = 16;
+
+template <int KERN>
+__global__ void __launch_bounds__(256, 6)
+dwt_fwd_batched_fast(const j2k_dwt_level_desc* __restrict__ descs, const uint32_t* __restrict__ owner) {
+    using T = typename KT<KERN>::T;
+    __shared__ __align__(16) T s[kBatchFastTh][FNX];
+    griddep_launch_dependents();
+    griddep_wait();  // a level launched as a dependent reads the previous level's LL band
+    const j2k_dwt_level_desc d = descs[owner[blockIdx.x]];
+    const int t = (int)(blockIdx.x - d.tile0);
+    const int x0 = (t % d.tiles_x) * FTW, y0 = (t / d.tiles_x) * kBatchFastTh;
+    const Steps4 st{d.s_ll, d.s_hl, d.s_lh, d.s_hh};
+    const int vec = (d.flags >> 2) & 1;
+    const T* src = (const T*)d.src;
+    T* lld = (T*)d.ll_dst;
+    if (d.w < 8 || d.h < 2) {
+        using G = Tile<KERN, 64, kBatchFastTh>;
+        T* ts = reinterpret_cast<T*>(&s[0][0]);
+        static_assert(G::NY * G::S <= kBatchFastTh * FNX, "fallback tile must fit the shared rows");
+        for (int sx = x0; sx < x0 + FTW && sx < d.w; sx += 64) {
+            if (KERN == 97 && (d.flags & 1)) {
+                if (d.flags & 2)
+                    fwd_tile<KERN, J2K_ORDER_T800, 64, kBatchFastTh, int32_t, true, true>(
+                        ts, src, d.spitch, d.w, d.h, lld, d.llpitch, (int32_t*)d.dst, d.dpitch, st, sx, y0);
+                else
+                    fwd_tile<KERN, J2K_ORDER_T800, 64, kBatchFastTh, int32_t, true, false>(
+                        ts, src, d.spitch, d.w, d.h, lld, d.llpitch, (int32_t*)d.dst, d.dpitch, st, sx, y0);
+            } else {
+                fwd_tile<KERN, J2K_ORDER_T800, 64, kBatchFastTh, T, false, false>(
+                    ts, src, d.spitch, d.w, d.h, lld, d.llpitch, (T*)d.dst, d.dpitch, st, sx, y0);
+            }
+            __syncthreads();
+        }
+        return;
+    }
+    if (KERN == 97 && (d.flags & 1)) {
+        if (d.flags & 2)
+            fwd_fast_tile_reg<KERN, int32_t, true, true, kBatchFastTh>(s, src, d.spitch, d.w, d.h, lld, d.llpitch,
+                                                                      (int32_t*)d.dst, d.dpitch, st, vec, x0, y0);
+        else
+            fwd_fast_tile_reg<KERN, int32_t, true, false, kBatchFastTh>(s, src, d.spitch, d.w, d.h, lld, d.llpitch,
+                                                                       (int32_t*)d.dst, d.dpitch, st, vec, x0, y0);
+    } else {
+        fwd_fast_tile_reg<KERN, T, false, false, kBatchFastTh>(s, src, d.spitch, d.w, d.h, lld, d.llpitch, (T*)d.dst,
+                                                              d.dpitch, st, vec, x0, y0);
+    }
 }
 
 // ---- TMA-staged forward level -----------------------------------------------------------------
@@ -1054,6 +1148,14 @@ j2k_status j2k_dwt_fwd_batched_launch(j2k_ctx* ctx, int kernel, int order, j2k_d
                                       const j2k_dwt_level_desc* d_descs, const uint32_t* d_owner,
                                       unsigned ntiles, cudaStream_t st) {
     if (ntiles == 0) return J2K_OK;
+    if (tile.tw == FTW && tile.th == kBatchFastTh && order == J2K_ORDER_T800) {
+        // the register-lifting form, launched as a programmatic dependent of the previous level
+        if (kernel == J2K_W53)
+            J2K_CUDA(ctx, launch_pdl(dwt_fwd_batched_fast<53>, dim3(ntiles), dim3(256), st, true, d_descs, d_owner));
+        else
+            J2K_CUDA(ctx, launch_pdl(dwt_fwd_batched_fast<97>, dim3(ntiles), dim3(256), st, true, d_descs, d_owner));
+        return J2K_OK;
+    }
 #define BL(K, O, TW_, TH_) dwt_fwd_batched<K, O, TW_, TH_><<<ntiles, 256, 0, st>>>(d_descs, d_owner)
 #define BL_ORDER(K, TW_, TH_)                          \
     do {                                               \

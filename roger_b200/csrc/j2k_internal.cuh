@@ -168,7 +168,8 @@ struct j2k_dwt_level_desc {
     size_t spitch, llpitch, dpitch;
     int w, h;
     float s_ll, s_hl, s_lh, s_hh;  // quantiser steps (9/7)
-    int flags;          // 1: quantise details (9/7), 2: this is the last level (LL quantised into dst)
+    int flags;          // 1: quantise details (9/7), 2: this is the last level (LL quantised into dst),
+                        // 4: dst and ll_dst take 8-byte vector stores
     int tiles_x;
     uint32_t tile0;     // first flattened tile index of this image
 };
