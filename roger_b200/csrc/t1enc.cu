@@ -106,7 +106,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                                               const uint8_t* slut, uint8_t* __restrict__ syms,
                                               uint32_t* __restrict__ nsyms, uint32_t* __restrict__ pass_end,
                                               uint64_t* __restrict__ planes, j2k_cb_desc* __restrict__ descs,
-                                              uint32_t* __restrict__ err) {
+                                              uint32_t* __restrict__ err, int pad) {
     const int cw = J.cw, ch = J.ch;
     const size_t pitch = J.pitch;
     const int32_t* blk = coeff + J.off;
@@ -270,6 +270,10 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
             }
             if (lane == 0) pend[npass] = (uint32_t)pos;
             ++npass;
+            if (pad) {  // the next pass starts on a 16-byte boundary (a coding unit of its own)
+                pos = (pos + 15) & ~15;
+                ovf |= pos > cap;
+            }
             // ------------------------- magnitude refinement pass
             for (int s = 0; s < nstripes && !ovf; ++s) {
                 const int r0 = 4 * s;
@@ -319,6 +323,10 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
             }
             if (lane == 0) pend[npass] = (uint32_t)pos;
             ++npass;
+            if (pad) {  // the next pass starts on a 16-byte boundary (a coding unit of its own)
+                pos = (pos + 15) & ~15;
+                ovf |= pos > cap;
+            }
         }
         // ------------------------- cleanup pass
         for (int s = 0; s < nstripes && !ovf; ++s) {
@@ -431,6 +439,10 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
         }
         if (lane == 0) pend[npass] = (uint32_t)pos;
         ++npass;
+        if (pad) {
+            pos = (pos + 15) & ~15;
+            ovf |= pos > cap;
+        }
         for (int r = lane; r < kRows + 2; r += 32) S.vis[r] = 0;
         __syncwarp();
     }
@@ -450,7 +462,7 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
                   int njobs, const uint32_t* __restrict__ order, uint32_t* __restrict__ queue,
                   uint8_t* __restrict__ syms, uint32_t* __restrict__ nsyms,
                   uint32_t* __restrict__ pass_end, uint64_t* __restrict__ plane_scratch,
-                  j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err) {
+                  j2k_cb_desc* __restrict__ descs, uint32_t* __restrict__ err, int pad) {
     __shared__ WarpSmem smem[kWarpsPerCta];
     __shared__ uint8_t zlut[4][256];
     __shared__ uint8_t slut[256];
@@ -487,10 +499,10 @@ t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restric
     }
     if (J.cw <= 32)
         phase_a_block<uint32_t, 1>(S, J, jid, lane, coeff, &zlut[0][0], slut, syms, nsyms, pass_end, planes, descs,
-                                   err);
+                                   err, pad);
     else
         phase_a_block<uint64_t, 2>(S, J, jid, lane, coeff, &zlut[0][0], slut, syms, nsyms, pass_end, planes, descs,
-                                   err);
+                                   err, pad);
     }  // queue loop
 }
 
@@ -930,6 +942,13 @@ __device__ __forceinline__ uint64_t seg_slot(uint64_t sym_off, uint32_t s0, int 
     return (uint64_t)fac * ((sym_off + s0 + 3) & ~(uint64_t)3) + 16ull * ((uint64_t)j * J2K_PASS_STRIDE + p0);
 }
 
+// first symbol of pass p of a job whose pass ends are pe: with per-pass units every pass's
+// symbols start on a 16-byte boundary (phase A pads them)
+__device__ __forceinline__ uint32_t pass_start(const uint32_t* pe, int p, bool per_pass) {
+    if (p == 0) return 0u;
+    return per_pass ? (pe[p - 1] + 15u) & ~15u : pe[p - 1];
+}
+
 // sort keys: symbols of each unit + 1 (0 for slots without a unit); values: slot ids
 __global__ void t1_unit_keys_kernel(const j2k_cb_desc* __restrict__ descs, const uint32_t* __restrict__ pend,
                                     int njobs, int style, uint32_t* __restrict__ keys, uint32_t* __restrict__ ids) {
@@ -940,7 +959,8 @@ __global__ void t1_unit_keys_kernel(const j2k_cb_desc* __restrict__ descs, const
     const uint32_t* pe = pend + (size_t)j * J2K_PASS_STRIDE;
     uint32_t key = 0;
     if (units_per_pass(style)) {
-        if (k < np) key = pe[k] - (k ? pe[k - 1] : 0u) + 1u;
+        // raw passes sort after the MQ ones (bit 31), so that a warp's lanes code alike passes
+        if (k < np) key = (pe[k] - pass_start(pe, k, true) + 1u) | (j2k_pass_raw(style, k) ? 0u : 0x80000000u);
     } else if (k == 0 && np > 0) {
         key = pe[np - 1] + 1u;
     }
@@ -1088,6 +1108,167 @@ t1_mq_units_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restric
     ulen[u] = (uint32_t)(e.wbase + e.wn);
 }
 
+// Per-pass units (RESET | TERMALL: every pass a codeword segment that starts from fresh context
+// states and a fresh coder): one lane per pass, passes longest first, the MQ passes before the
+// raw ones.  An MQ pass runs the same loop as t1_mq_kernel (16-byte symbol chunks two in flight,
+// four symbols per unrolled body, the next context's state loaded one symbol ahead and
+// forwarded), from its 16-byte aligned start, and ends with the FLUSH of T.800 C.2.9 (a last
+// 0xFF dropped), however few symbols it has; a raw pass writes its decisions as bits (T.800
+// D.6: a byte after 0xFF holds 7, the partial last byte padded with 0s, a last 0xFF dropped).
+// Unit bytes go to the pass's slot; ulen / ends as t1_mq_units_kernel.
+constexpr int kPassThreads = 128;
+
+__global__ void __launch_bounds__(kPassThreads)
+t1_mq_pass_kernel(const uint8_t* __restrict__ syms, const j2k_cb_job* __restrict__ jobs,
+                  const j2k_cb_desc* __restrict__ descs, const uint32_t* __restrict__ pend,
+                  const uint32_t* __restrict__ order, const uint32_t* __restrict__ keys, int nslots, int style,
+                  int fac, uint8_t* __restrict__ segs, uint32_t* __restrict__ ulen, uint32_t* __restrict__ ends,
+                  uint32_t* __restrict__ err) {
+    __shared__ uint32_t tab[47];
+    __shared__ uint32_t cst[32 * kPassThreads];  // 32 contexts per lane: a 5-bit index needs no clamp
+    for (int i = threadIdx.x; i < 47; i += blockDim.x)
+        tab[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
+                 ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
+    __syncthreads();
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= nslots || keys[gid] == 0) return;  // keys are sorted: the empty slots come last
+    const int u = (int)order[gid];
+    const int j = u / J2K_PASS_STRIDE, p = u % J2K_PASS_STRIDE;
+    const j2k_cb_job J = jobs[j];
+    const uint32_t* pe = pend + (size_t)j * J2K_PASS_STRIDE;
+    const uint32_t s0 = pass_start(pe, p, true), s1 = pe[p];
+    const uint32_t snext = (s1 + 15u) & ~15u;  // where the next pass's symbols (and slot) start
+    if (s1 > J.sym_cap || s0 > s1) {
+        atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+        return;
+    }
+    const int n = (int)(s1 - s0);
+    const uint64_t base = seg_slot(J.sym_off, s0, j, p, fac);
+    const uint64_t lim = seg_slot(J.sym_off, snext, j, p + 1, fac);
+    MqEnc e;
+    e.A = 0x8000;
+    e.C = 0;
+    e.B = 0;
+    e.CT = 12;
+    e.bp = -1;
+    e.out = reinterpret_cast<uint32_t*>(segs + base);
+    e.cap = (int)(lim - base);
+    e.wacc = 0;
+    e.wn = 0;
+    e.wbase = 0;
+    e.ovf = false;
+    const uint4* sp4 = reinterpret_cast<const uint4*>(syms + J.sym_off + s0);
+    const int nchunks = (n + 15) >> 4;
+    const uint4 z4 = make_uint4(0, 0, 0, 0);
+    uint4 c0 = nchunks > 0 ? __ldcs(sp4) : z4;
+    uint4 c1 = nchunks > 1 ? __ldcs(sp4 + 1) : z4;
+    if (j2k_pass_raw(style, p)) {
+        uint32_t rc = 0;
+        int rct = 8, rpend = -1;
+        bool rlastff = false;
+        auto complete = [&](uint32_t b) {
+            if (rpend >= 0) e.push((uint32_t)rpend);
+            rpend = (int)b;
+            rlastff = b == 0xFF;
+            rct = rlastff ? 7 : 8;
+            rc = 0;
+        };
+        for (int k = 0; k < nchunks; ++k) {
+            const uint4 cur = c0;
+            c0 = c1;
+            c1 = (k + 2 < nchunks) ? __ldcs(sp4 + k + 2) : z4;
+            const uint32_t wv[4] = {cur.x, cur.y, cur.z, cur.w};
+            const int m = min(16, n - 16 * k);
+            for (int i = 0; i < m; ++i) {
+                const uint32_t sym = (wv[i >> 2] >> (8 * (i & 3))) & 0xFF;
+                const uint32_t lab = sym & 31;
+                const uint32_t bit = ((sym >> 7) ^ ((lab >= 9 && lab <= 13) ? (sym >> 5) : 0u)) & 1u;
+                rc = (rc << 1) | bit;
+                if (--rct == 0) complete(rc & 0xFF);
+            }
+        }
+        if (rct < (rlastff ? 7 : 8)) complete((rc << rct) & 0xFF);
+        if (rpend >= 0 && rpend != 0xFF) e.push((uint32_t)rpend);
+    } else {
+        uint32_t* st = cst + threadIdx.x;  // context c at st[c * kPassThreads]
+        for (int c = 0; c < 32; ++c) st[c * kPassThreads] = tab[0];
+        st[0] = tab[4];
+        st[17 * kPassThreads] = tab[3];
+        st[18 * kPassThreads] = tab[46];
+        int cx = (int)(c0.x & 31);
+        uint32_t ent = st[cx * kPassThreads];
+        auto step = [&](uint32_t sym, uint32_t nsym) {
+            const int d = sym >> 7;
+            const int ncx = (int)(nsym & 31);
+            uint32_t nent = st[ncx * kPassThreads];
+            const uint32_t qe = ent & 0xFFFF;
+            const int mps = ent >> 31;
+            const bool is_mps = d == mps;
+            const uint32_t a1 = e.A - qe;
+            const bool fast = is_mps && (a1 & 0x8000);
+            const bool addc = fast || (is_mps != (a1 < qe));
+            e.C += addc ? qe : 0u;
+            e.A = addc ? a1 : qe;
+            const int nidx = is_mps ? (ent >> 16) & 63 : (ent >> 22) & 63;
+            const uint32_t nmps = (uint32_t)(mps ^ (!is_mps & (int)((ent >> 28) & 1)));
+            const uint32_t upd = tab[nidx] | (nmps << 31);
+            if (!fast) {
+                st[cx * kPassThreads] = upd;
+                if (ncx == cx) nent = upd;
+            }
+            e.renorm(__clz(e.A) - 16);
+            cx = ncx;
+            ent = nent;
+        };
+        for (int k = 0; k < nchunks; ++k) {
+            const uint4 cur = c0;
+            c0 = c1;
+            c1 = (k + 2 < nchunks) ? __ldcs(sp4 + k + 2) : z4;
+            const int m = min(16, n - 16 * k);
+            uint32_t wa = cur.x, wb = cur.y, wc = cur.z, wd = cur.w;
+            const uint32_t we = c0.x;
+#pragma unroll 1
+            for (int q = 0; q < 4 && 4 * q < m; ++q) {
+                if (4 * q + 4 <= m) {
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj)
+                        step((wa >> (8 * jj)) & 0xFF, jj < 3 ? (wa >> (8 * (jj + 1))) & 0xFF : wb & 0xFF);
+                } else {
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj)
+                        if (4 * q + jj < m) step((wa >> (8 * jj)) & 0xFF, jj < 3 ? (wa >> (8 * (jj + 1))) & 0xFF : wb & 0xFF);
+                }
+                wa = wb;
+                wb = wc;
+                wc = wd;
+                wd = we;
+            }
+        }
+        // FLUSH (T.800 C.2.9); a last byte of 0xFF is dropped
+        const uint32_t tempc = e.C + e.A;
+        e.C |= 0xFFFF;
+        if (e.C >= tempc) e.C -= 0x8000;
+        e.C <<= e.CT;
+        e.byteout();
+        e.C <<= e.CT;
+        e.byteout();
+        if (e.B != 0xFF) e.push(e.B);
+    }
+    uint8_t* bb = segs + base;
+    for (int q = 0; q < e.wn; ++q) {
+        if (e.wbase + q < e.cap) bb[e.wbase + q] = (uint8_t)(e.wacc >> (8 * q));
+        else e.ovf = true;
+    }
+    if (e.ovf) {
+        atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_SEG_CAPACITY);
+        ulen[u] = 0;
+        return;
+    }
+    const uint32_t len = (uint32_t)(e.wbase + e.wn);
+    ulen[u] = len;
+    ends[(size_t)j * J2K_PASS_STRIDE + p] = len;
+}
+
 // One warp per code-block: its units' segments back to back into the block's codeword, the
 // pass ends made block-relative, and the descriptor's length.
 __global__ void t1_units_compact_kernel(const j2k_cb_job* __restrict__ jobs, j2k_cb_desc* __restrict__ descs,
@@ -1115,11 +1296,19 @@ __global__ void t1_units_compact_kernel(const j2k_cb_job* __restrict__ jobs, j2k
                 atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_OUT_CAPACITY);
             } else {
                 const int p0 = per_pass ? k : 0, p1 = per_pass ? k + 1 : np;
-                const uint32_t s0 = p0 ? pe[p0 - 1] : 0u;
-                const uint8_t* src = segs + seg_slot(J.sym_off, s0, j, p0, fac);
-                for (uint32_t q = 0; q < len; ++q) dst[off + q] = src[q];
                 for (int p = p0; p < p1; ++p) eo[p] += off;
             }
+        }
+        // the round's units copied one after another, each by the whole warp
+        const bool ok = k < nu && off + len <= J.out_cap;
+        const unsigned okm = __ballot_sync(0xffffffffu, ok);
+        for (int q = 0; q < 32; ++q) {
+            if (!((okm >> q) & 1u)) continue;
+            const uint32_t ql = __shfl_sync(0xffffffffu, len, q), qo = __shfl_sync(0xffffffffu, off, q);
+            const int kq = k0 + q;
+            const int p0 = per_pass ? kq : 0;
+            const uint8_t* src = segs + seg_slot(J.sym_off, pass_start(pe, p0, per_pass), j, p0, fac);
+            for (uint32_t b = (uint32_t)lane; b < ql; b += 32) dst[qo + b] = src[b];
         }
         run += (uint32_t)tot;
     }
@@ -1220,9 +1409,13 @@ static j2k_status encode_styled_units(j2k_ctx* ctx, const j2k_cb_job* d_jobs, si
     if (!tbuf) return J2K_ERR_OUT_OF_MEMORY;
     J2K_CUDA(ctx, cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, keys_in, keys_out, ids_in, ids_out,
                                                             (int)nslots, 0, 32, st));
-    t1_mq_units_kernel<<<(unsigned)((nslots + 127) / 128), 128, 0, st>>>(syms, d_jobs, descs, pend, ids_out, keys_out,
-                                                                         (int)nslots, style, fac, segs, ulen, ends,
-                                                                         ctx->d_err);
+    if (units_per_pass(style))
+        t1_mq_pass_kernel<<<(unsigned)((nslots + kPassThreads - 1) / kPassThreads), kPassThreads, 0, st>>>(
+            syms, d_jobs, descs, pend, ids_out, keys_out, (int)nslots, style, fac, segs, ulen, ends, ctx->d_err);
+    else
+        t1_mq_units_kernel<<<(unsigned)((nslots + 127) / 128), 128, 0, st>>>(syms, d_jobs, descs, pend, ids_out,
+                                                                             keys_out, (int)nslots, style, fac, segs,
+                                                                             ulen, ends, ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     t1_units_compact_kernel<<<(unsigned)((njobs * 32 + 255) / 256), 256, 0, st>>>(
         d_jobs, descs, pend, (int)njobs, style, fac, segs, ulen, ends, bytes, ctx->d_err);
@@ -1257,8 +1450,10 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     uint32_t* idx_in = keys_out + njobs;
     uint32_t* idx_out = idx_in + njobs;
     J2K_CUDA(ctx, cudaMemsetAsync(queue, 0, 4, st));
+    // with per-pass coding units (RESET | TERMALL) every pass's symbols start 16-byte aligned
+    const int pad = (style & (J2K_CBLK_RESET | J2K_CBLK_TERMALL)) == (J2K_CBLK_RESET | J2K_CBLK_TERMALL) ? 1 : 0;
     t1_symbols_kernel<<<(unsigned)ctas, kWarpsPerCta * 32, 0, st>>>(coeff, d_jobs, (int)njobs, d_order, queue, syms,
-                                                                   nsyms, pend, planes, descs, ctx->d_err);
+                                                                   nsyms, pend, planes, descs, ctx->d_err, pad);
     J2K_CUDA(ctx, cudaGetLastError());
     if (style)
         return encode_styled_units(ctx, d_jobs, njobs, descs, bytes, sym_bytes, syms, pend, style, pass_ends, st);
