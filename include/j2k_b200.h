@@ -69,6 +69,8 @@ enum {
                                  0: it stages the strip in shared memory with cp.async */
     J2K_TUNE_DWT_TMA = 7,     /* 1: that kernel is the TMA-staged form (persistent CTAs, each strip brought in
                                  by one tensor copy, two stages deep) */
+    J2K_TUNE_T1A_CTAS = 8,    /* tier-1 context modelling: resident CTAs per SM its registers are cut for,
+                                 2 (default, no spills) or 3 */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of

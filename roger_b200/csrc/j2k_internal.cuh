@@ -84,6 +84,7 @@ struct j2k_ctx {
     int dwt_reg = 1;             // fast forward DWT: columns loaded straight into registers (0: cp.async strip)
     int t1_seg_factor = 1;       // styled tier-1: pass-segment slot bytes per symbol (grown on overflow)
     int dwt_tma = 0;             // fast forward DWT: strips staged by TMA tensor copies (persistent CTAs)
+    int t1a_ctas = 2;            // tier-1 phase A: resident CTAs per SM its registers are cut for (2 or 3)
 };
 
 // scratch slot ids

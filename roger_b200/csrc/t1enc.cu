@@ -457,7 +457,10 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
+// MINB: resident CTAs per SM the register budget is cut for (2: no spills; 3: a few spilled
+// registers, more warps to hide the ALU chains)
+template <int MINB>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, MINB)
 t1_symbols_kernel(const int32_t* __restrict__ coeff, const j2k_cb_job* __restrict__ jobs,
                   int njobs, const uint32_t* __restrict__ order, uint32_t* __restrict__ queue,
                   uint8_t* __restrict__ syms, uint32_t* __restrict__ nsyms,
@@ -1435,7 +1438,11 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     uint8_t* syms = (uint8_t*)j2k_scratch(ctx, SCR_SYMS, sym_bytes + 64);
     // persistent phase A: one bit-plane slot per resident warp
     int per_sm = 0;
-    J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_symbols_kernel, kWarpsPerCta * 32, 0));
+    const bool occ3 = ctx->t1a_ctas == 3;
+    if (occ3)
+        J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_symbols_kernel<3>, kWarpsPerCta * 32, 0));
+    else
+        J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_symbols_kernel<2>, kWarpsPerCta * 32, 0));
     per_sm = std::max(per_sm, 1);
     const size_t ctas = std::min<size_t>((njobs + kWarpsPerCta - 1) / kWarpsPerCta, (size_t)per_sm * ctx->sm_count);
     uint64_t* planes = (uint64_t*)j2k_scratch(ctx, SCR_PLANES, ctas * kWarpsPerCta * kPlaneWords * 8 + 64);
@@ -1452,8 +1459,14 @@ j2k_status j2k_t1_encode_jobs(j2k_ctx* ctx, const int32_t* coeff, const j2k_cb_j
     J2K_CUDA(ctx, cudaMemsetAsync(queue, 0, 4, st));
     // with per-pass coding units (RESET | TERMALL) every pass's symbols start 16-byte aligned
     const int pad = (style & (J2K_CBLK_RESET | J2K_CBLK_TERMALL)) == (J2K_CBLK_RESET | J2K_CBLK_TERMALL) ? 1 : 0;
-    t1_symbols_kernel<<<(unsigned)ctas, kWarpsPerCta * 32, 0, st>>>(coeff, d_jobs, (int)njobs, d_order, queue, syms,
-                                                                   nsyms, pend, planes, descs, ctx->d_err, pad);
+    if (occ3)
+        t1_symbols_kernel<3><<<(unsigned)ctas, kWarpsPerCta * 32, 0, st>>>(coeff, d_jobs, (int)njobs, d_order, queue,
+                                                                          syms, nsyms, pend, planes, descs, ctx->d_err,
+                                                                          pad);
+    else
+        t1_symbols_kernel<2><<<(unsigned)ctas, kWarpsPerCta * 32, 0, st>>>(coeff, d_jobs, (int)njobs, d_order, queue,
+                                                                          syms, nsyms, pend, planes, descs, ctx->d_err,
+                                                                          pad);
     J2K_CUDA(ctx, cudaGetLastError());
     if (style)
         return encode_styled_units(ctx, d_jobs, njobs, descs, bytes, sym_bytes, syms, pend, style, pass_ends, st);
