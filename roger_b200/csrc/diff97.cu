@@ -434,10 +434,10 @@ j2k_status fwd_adj_run(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, s
             const dim3 fg((ws[k] + FTW - 1) / FTW, (hs[k] + STH - 1) / STH, n);
             const ZStride zs{plane, oz, llz};
             if (fused)
-                J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 1, float, false, false, 2>, fg, dim3(256), st, true, g_coef, w,
+                J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 1, float, false, false, 2>, fg, dim3(256), st, false, g_coef, w,
                                          ll, llp, ws[k], hs[k], out, op, Steps4{}, zs, vec, *ex));
             else
-                J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 1, float, false, false, 0>, fg, dim3(256), st, true, g_coef, w,
+                J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 1, float, false, false, 0>, fg, dim3(256), st, false, g_coef, w,
                                          ll, llp, ws[k], hs[k], out, op, Steps4{}, zs, vec, SynExtra{}));
         } else {
             dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
@@ -473,7 +473,7 @@ j2k_status quant_run(j2k_ctx* ctx, bool bwd, const float* y, const float* gin, f
         if (smem > 48 * 1024)                                                                                  \
             J2K_CUDA(ctx, cudaFuncSetAttribute(relaxed_quant_k<B_, N_>,                                        \
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));       \
-        J2K_CUDA(ctx, launch_pdl_smem(relaxed_quant_k<B_, N_>, g, dim3(256), smem, ctx->stream, true, y, gin, out, \
+        J2K_CUDA(ctx, launch_pdl_smem(relaxed_quant_k<B_, N_>, g, dim3(256), smem, ctx->stream, false, y, gin, out, \
                                       (int)w, (int)h, plane, lv, log_steps, seed, lam, gscale, alpha, partials,    \
                                       rows, vec, noise));                                                          \
     } while (0)
@@ -556,7 +556,7 @@ j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_
     J2K_API_BEGIN
     if (!ctx || !loss || (!rate_partials && nrate) || (!sq_partials && nsq)) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    J2K_CUDA(ctx, launch_pdl(rd_finalize_kernel, dim3(1), dim3(1024), ctx->stream, true, rate_partials, nrate,
+    J2K_CUDA(ctx, launch_pdl(rd_finalize_kernel, dim3(1), dim3(1024), ctx->stream, false, rate_partials, nrate,
                              sq_partials, nsq, inv_count, lam, loss));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
@@ -567,7 +567,7 @@ j2k_status j2k_dwt97_band_sum(j2k_ctx* ctx, const float* partials, int n, int nb
     J2K_API_BEGIN
     if (!ctx || !partials || !out || n < 1 || nb < 1 || k < 1) return J2K_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
-    J2K_CUDA(ctx, launch_pdl(band_sum_kernel, dim3((unsigned)nb), dim3(256), ctx->stream, true, partials, n, nb, k,
+    J2K_CUDA(ctx, launch_pdl(band_sum_kernel, dim3((unsigned)nb), dim3(256), ctx->stream, false, partials, n, nb, k,
                              out));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
@@ -626,7 +626,7 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
             const int vout = (((uintptr_t)g_coef & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) &&
                              (((uintptr_t)ll & 7) == 0) && ((llp & 1) == 0) && ((llz & 1) == 0);
             const dim3 fg((ws[k] + FTW - 1) / FTW, (hs[k] + STH - 1) / STH, n);
-            J2K_CUDA(ctx, launch_pdl(iadj_ana_fast, fg, dim3(256), st, true, in, ip, ws[k], hs[k], g_coef, w, ll, llp,
+            J2K_CUDA(ctx, launch_pdl(iadj_ana_fast, fg, dim3(256), st, false, in, ip, ws[k], hs[k], g_coef, w, ll, llp,
                                      ZStride{iz, plane, llz}, vin, vout));
         } else {
             dim3 g((ws[k] + TW - 1) / TW, (hs[k] + TH - 1) / TH, n);
@@ -684,7 +684,7 @@ j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float*
     const int vec = (((uintptr_t)y & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) && (((uintptr_t)ll & 7) == 0) &&
                     ((llp & 1) == 0) && ((llz & 1) == 0) && ((wl & 1) == 0);
     const SynExtra ex{x, w, plane, nullptr, 1.0f, sq_partials};
-    J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 0, float, false, false, 1>, fg, dim3(256), st, true, y, w, ll, llp,
+    J2K_CUDA(ctx, launch_pdl(dwt_syn_fast<97, 0, float, false, false, 1>, fg, dim3(256), st, false, y, w, ll, llp,
                              (int)w, (int)h, d, w, Steps4{}, ZStride{plane, plane, llz}, vec, ex));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;

@@ -115,7 +115,7 @@ __device__ __forceinline__ void fwd_tile(typename KT<KERN>::T* s, const typename
     for (int e = threadIdx.x; e < G::NX * G::NY; e += blockDim.x) {
         int r = e / G::NX, c = e % G::NX;
         int gy = mirror(y0 - H + r, h), gx = mirror(x0 - H + c, w);
-        s[r * G::S + c] = src[(size_t)gy * spitch + gx];
+        s[r * G::S + c] = __ldcg(src + (size_t)gy * spitch + gx);  // L2 only, as fwd_fast_tile_reg
     }
     __syncthreads();
     const bool dov = h > 1, doh = w > 1;
@@ -317,13 +317,15 @@ __device__ __forceinline__ void fwd_fast_tile_reg(typename KT<KERN>::T (*s)[FNX]
     const bool inner_x = (x0 - 4 >= 0) && (x0 + 252 <= w);
     const bool inner_y = (y0 - HV >= 0) && (y0 + FTH + HV <= h);
     T c[NY];
-    // 1. column t of the strip
+    // 1. column t of the strip.  Loads cached in L2 only: a level launched as a programmatic
+    // dependent may start while the previous level still runs on the same SMs, so lines of
+    // its input buffer that an earlier level read could still sit in an SM's L1
     const int gx = x0 - 4 + t;
     const T* colp = src + (inner_x ? gx : mirror(gx, w));
 #pragma unroll
     for (int r = 0; r < NY; ++r) {
         const int gy = inner_y ? y0 - HV + r : mirror(y0 - HV + r, h);
-        c[r] = __ldg(colp + (size_t)gy * spitch);
+        c[r] = __ldcg(colp + (size_t)gy * spitch);
     }
     // 2. vertical lifting of column t in registers
     if (h > 1) {
@@ -1067,19 +1069,19 @@ j2k_status inv_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
                             ((wl & 1) == 0);
             const dim3 fg((cw + FTW - 1) / FTW, (chh + STH - 1) / STH, n);
             const SynExtra ex{};
-            // every synthesis kernel waits for its predecessor's grid first, so each one is
-            // launched as a programmatic dependent (its launch overlaps the predecessor's tail)
+            // (not programmatic dependents: these kernels read their input through the read-only
+            // cache, which the previous level writes)
             const dim3 b(256);
             cudaError_t le;
             if (deq) {
                 if (k == levels - 1)
-                    le = launch_pdl(dwt_syn_fast<KERN, 0, int32_t, true, true, 0>, fg, b, stream, true,
+                    le = launch_pdl(dwt_syn_fast<KERN, 0, int32_t, true, true, 0>, fg, b, stream, false,
                                     (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
                 else
-                    le = launch_pdl(dwt_syn_fast<KERN, 0, int32_t, true, false, 0>, fg, b, stream, true,
+                    le = launch_pdl(dwt_syn_fast<KERN, 0, int32_t, true, false, 0>, fg, b, stream, false,
                                     (const int32_t*)in, in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
             } else {
-                le = launch_pdl(dwt_syn_fast<KERN, 0, T, false, false, 0>, fg, b, stream, true, (const T*)in,
+                le = launch_pdl(dwt_syn_fast<KERN, 0, T, false, false, 0>, fg, b, stream, false, (const T*)in,
                                 in_pitch, lls, llp, cw, chh, o, op, st, zs, vec, ex);
             }
             J2K_CUDA(ctx, le);
