@@ -424,9 +424,11 @@ enum {
     J2K_BATCH_GRAPH_KERNELS = 8, /* read-only: kernel launches of one replay of the captured
                                     sequence, this library's own (library sort/scan kernels are
                                     not counted); 0 before the first graph encode */
-    J2K_BATCH_STAGES = 9         /* stages an encode runs, for timing them apart: 1 planar split,
+    J2K_BATCH_STAGES = 9,        /* stages an encode runs, for timing them apart: 1 planar split,
                                     2 DWT, 4 tier-1 (default 7, all).  Without 4 the encode leaves
                                     no code-blocks to read */
+    J2K_BATCH_T1A_CTAS = 10      /* read-only: the context modelling's resident CTAs per SM that
+                                    the autotuner kept (J2K_TUNE_T1A_CTAS) */
 };
 j2k_status j2k_batch_create(j2k_ctx* ctx, const j2k_batch_image* images, int n, j2k_batch** out);
 j2k_status j2k_batch_destroy(j2k_batch* b);

@@ -133,7 +133,8 @@ class BatchEncoder:
         if tiers.value and not rep[3]:
             mq += " after the tiers (longest blocks: 1 per warp, then 4 per warp)"
         return {"tile53": TILE_NAMES[rep[0]], "tile97": TILE_NAMES[rep[1]],
-                "phase_a_order": "largest-first" if rep[2] else "natural", "mq": mq}
+                "phase_a_order": "largest-first" if rep[2] else "natural", "mq": mq,
+                "phase_a_ctas_per_sm": self.get_option(10)}
 
     def results(self, pinned=True):
         """Every image's (descs, codeword bytes), read back in one packing pass and two copies

@@ -494,6 +494,7 @@ j2k_status j2k_batch_get_option(j2k_batch* b, int key, int* value) {
         case J2K_BATCH_MQ_TIERS: *value = b->ctx->mq_tier_lanes[0] > 0 && b->ctx->mq_tier_warps[0] > 0; break;
         case J2K_BATCH_GRAPH_KERNELS: *value = b->graph ? count_own_kernel_nodes(b->graph) : 0; break;
         case J2K_BATCH_STAGES: *value = b->stages; break;
+        case J2K_BATCH_T1A_CTAS: *value = b->ctx->t1a_ctas; break;
         default: return J2K_ERR_INVALID_ARG;
     }
     return J2K_OK;
@@ -636,6 +637,20 @@ j2k_status j2k_batch_autotune(j2k_batch* b, int reps, int* report) {
     ctx->mq_variant = cand[best_c][0];
     ctx->mq_lanes = cand[best_c][1];
     set_tiers(cand[best_c][2] != 0);
+    // phase A's register budget: 2 or 3 resident CTAs per SM
+    {
+        int best_occ = ctx->t1a_ctas;
+        float occ_t = best_t;
+        for (int occ = 2; occ <= 3 && s == J2K_OK; ++occ) {
+            if (occ == best_occ) continue;
+            const int keep = ctx->t1a_ctas;
+            ctx->t1a_ctas = occ;
+            s = time_stage(false, false, true, &t);
+            if (s == J2K_OK && t < occ_t) occ_t = t, best_occ = occ;
+            ctx->t1a_ctas = keep;
+        }
+        ctx->t1a_ctas = best_occ;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->use_graph = graph;
