@@ -71,6 +71,8 @@ enum {
                                  by one tensor copy, two stages deep) */
     J2K_TUNE_T1A_CTAS = 8,    /* tier-1 context modelling: resident CTAs per SM its registers are cut for,
                                  2 (default, no spills) or 3 */
+    J2K_TUNE_DWT_TAIL = 9,    /* 1: the forward DWT's deep levels (at most two tiles per resident CTA) run in
+                                 one cooperative launch with grid barriers between levels */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of

@@ -471,6 +471,88 @@ dwt_fwd_batched_fast(const j2k_dwt_level_desc* __restrict__ descs, const uint32_
     }
 }
 
+// ---- fused deep levels ---------------------------------------------------------------------------
+// The deep levels of a forward transform are under one wave each (config 1's levels 3-5: 96 to 24
+// CTAs), so each costs a tile's latency plus a launch.  dwt_fwd_tail runs levels k0 .. k1-1 in one
+// cooperative launch: every CTA takes tiles of a level in turn (the register-lifting tile of
+// dwt_fwd_fast), then all CTAs meet at a grid barrier before the next level reads the LL band
+// they wrote.  The barrier is an arrival counter and a generation word in global memory; a CTA
+// waits for the generation with a bounded spin and, when the bound runs out, sets the timeout
+// error and leaves.  Loads are L2-only (fwd_fast_tile_reg), so no SM reads a stale L1 line of
+// the band the level before wrote.
+constexpr int kTailLevels = 8;
+struct TailLevel {
+    const void* src;
+    void* lld;
+    size_t spitch, llp, src_z, ll_z;
+    int w, h, tiles_x, tiles_y, vec, last;
+    Steps4 st;
+};
+struct TailPlan {
+    TailLevel lv[kTailLevels];
+    int nlev, nz;
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All CTAs of the (co-resident) grid; false when the wait for the others gave up.
+__device__ __forceinline__ bool tail_barrier(uint32_t* bar, uint32_t gen) {
+    __syncthreads();
+    int ok = 1;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&bar[0], 1u) + 1u;
+        if (arrived == gridDim.x) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            int spin = 0;
+            while (ld_acquire_u32(&bar[1]) < gen && spin < (1 << 22)) ++spin;
+            ok = spin < (1 << 22);
+        }
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+template <int KERN, bool QUANT>
+__global__ void __launch_bounds__(256, 4)
+dwt_fwd_tail(const TailPlan plan, void* __restrict__ dst, size_t dpitch, size_t dst_z, uint32_t* __restrict__ bar,
+             uint32_t* __restrict__ err) {
+    using T = typename KT<KERN>::T;
+    __shared__ __align__(16) T s[16][FNX];
+    for (int li = 0; li < plan.nlev; ++li) {
+        const TailLevel& L = plan.lv[li];
+        const int per = L.tiles_x * L.tiles_y, ntiles = per * plan.nz;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            const int tz = tile / per, r = tile % per;
+            const int x0 = (r % L.tiles_x) * FTW, y0 = (r / L.tiles_x) * 16;
+            const T* src = (const T*)L.src + tz * L.src_z;
+            T* lld = (T*)L.lld + tz * L.ll_z;
+            if (QUANT && L.last)
+                fwd_fast_tile_reg<KERN, int32_t, true, true, 16>(s, src, L.spitch, L.w, L.h, lld, L.llp,
+                                                                 (int32_t*)dst + tz * dst_z, dpitch, L.st, L.vec, x0,
+                                                                 y0);
+            else if (QUANT)
+                fwd_fast_tile_reg<KERN, int32_t, true, false, 16>(s, src, L.spitch, L.w, L.h, lld, L.llp,
+                                                                  (int32_t*)dst + tz * dst_z, dpitch, L.st, L.vec, x0,
+                                                                  y0);
+            else
+                fwd_fast_tile_reg<KERN, T, false, false, 16>(s, src, L.spitch, L.w, L.h, lld, L.llp,
+                                                             (T*)dst + tz * dst_z, dpitch, L.st, L.vec, x0, y0);
+            __syncthreads();  // s is reused by the next tile
+        }
+        if (li + 1 < plan.nlev && !tail_barrier(bar, (uint32_t)li + 1u)) {
+            if (threadIdx.x == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_TIMEOUT);
+            return;
+        }
+    }
+}
+
 // ---- TMA-staged forward level -----------------------------------------------------------------
 // Persistent CTAs walk the tiles (248 output columns x 16 rows of one plane) in a fixed order.
 // A tile's strip (256 columns x 16 + 2*HV rows, halo included) comes into shared memory by one
@@ -881,6 +963,84 @@ static j2k_status launch_fwd_tma(j2k_ctx* ctx, const void* src, size_t spitch, s
     return J2K_OK;
 }
 
+// Levels k .. of the transform whose level-k input is cw x chh (n planes) by one cooperative
+// dwt_fwd_tail launch, when they are few tiles: from the first level with at most two tiles per
+// resident CTA, through the last level at least 8 x 2 samples.  *used = the levels it covered
+// (0: none, the caller launches level k itself).
+template <int KERN>
+static j2k_status fwd_tail_launch(j2k_ctx* ctx, int k, int levels, int cw, int chh, int n,
+                                  const typename KT<KERN>::T* src, size_t spitch, size_t src_z, void* out,
+                                  size_t out_pitch, size_t out_z, const float* steps, void* ll0, void* ll1,
+                                  size_t z0, size_t z1, cudaStream_t stream, int* used) {
+    using T = typename KT<KERN>::T;
+    *used = 0;
+    const bool quant = (KERN == 97) && steps != nullptr;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int v = 0;
+        J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                          &v, quant ? dwt_fwd_tail<KERN, true> : dwt_fwd_tail<KERN, false>, 256, 0));
+        per_sm = std::max(v, 1);
+    }
+    const long cap = (long)per_sm * ctx->sm_count;
+    const long tiles_k = (long)((cw + FTW - 1) / FTW) * ((chh + 15) / 16) * n;
+    if (tiles_k > 2 * cap) return J2K_OK;  // a full-size level: its own launch
+    TailPlan plan{};
+    plan.nz = n;
+    int w = cw, h = chh;
+    const T* s = src;
+    size_t sp = spitch, sz = src_z;
+    long maxt = 0;
+    for (int q = k; q < levels && plan.nlev < kTailLevels; ++q) {
+        if (w < 8 || h < 2) break;
+        const bool last = q == levels - 1;
+        TailLevel& L = plan.lv[plan.nlev];
+        L.src = s;
+        L.spitch = sp;
+        L.src_z = sz;
+        L.w = w;
+        L.h = h;
+        if (last) {
+            L.lld = out;
+            L.llp = out_pitch;
+            L.ll_z = out_z;
+        } else {
+            L.lld = q % 2 == 0 ? ll0 : ll1;
+            L.llp = (size_t)((w + 1) / 2);
+            L.ll_z = q % 2 == 0 ? z0 : z1;
+        }
+        L.last = last;
+        L.tiles_x = (w + FTW - 1) / FTW;
+        L.tiles_y = (h + 15) / 16;
+        L.vec = (((uintptr_t)out & 7) == 0) && ((out_pitch & 1) == 0) && (((uintptr_t)L.lld & 7) == 0) &&
+                ((L.llp & 1) == 0);
+        const int bt = 1 + 3 * (levels - (q + 1));
+        L.st = quant ? Steps4{steps[0], steps[bt], steps[bt + 1], steps[bt + 2]} : Steps4{1.f, 1.f, 1.f, 1.f};
+        maxt = std::max(maxt, (long)L.tiles_x * L.tiles_y * n);
+        ++plan.nlev;
+        s = (const T*)L.lld;
+        sp = L.llp;
+        sz = L.ll_z;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+        if (last) break;
+    }
+    if (plan.nlev < 2) return J2K_OK;  // one level gains nothing
+    uint32_t* bar = (uint32_t*)j2k_scratch(ctx, SCR_BARRIER, 64);
+    if (!bar) return J2K_ERR_OUT_OF_MEMORY;
+    J2K_CUDA(ctx, cudaMemsetAsync(bar, 0, 8, stream));
+    const int grid = (int)std::min<long>(maxt, cap);
+    void* args[] = {(void*)&plan, (void*)&out, (void*)&out_pitch, (void*)&out_z, (void*)&bar, (void*)&ctx->d_err};
+    if (quant)
+        J2K_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)dwt_fwd_tail<KERN, true>, dim3(grid), dim3(256), args, 0,
+                                                  stream));
+    else
+        J2K_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)dwt_fwd_tail<KERN, false>, dim3(grid), dim3(256), args,
+                                                  0, stream));
+    *used = plan.nlev;
+    return J2K_OK;
+}
+
 template <int KERN, int ORDER, int TW, int TH>
 j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, size_t out_pitch,
                       int w, int h, int levels, const float* steps, void* ll0, void* ll1,
@@ -906,6 +1066,22 @@ j2k_status fwd_levels(j2k_ctx* ctx, const void* in, size_t in_pitch, void* out, 
     size_t src_z = in_z;
     for (int k = 0; k < levels; ++k) {
         bool last = (k == levels - 1);
+        if (ctx && ctx->dwt_tail && ORDER == J2K_ORDER_T800 && ctx->dwt_fast_th == 16 && k >= 1 && !ctx->dwt_tma) {
+            int used = 0;
+            J2K_TRY((fwd_tail_launch<KERN>(ctx, k, levels, cw, chh, n, src, spitch, src_z, out, out_pitch, out_z,
+                                           steps, ll0, ll1, z0, z1, stream, &used)));
+            if (used > 0) {
+                for (int q = 0; q < used; ++q) {
+                    src = (const T*)((k + q) % 2 == 0 ? ll0 : ll1);
+                    spitch = (size_t)((cw + 1) / 2);
+                    src_z = (k + q) % 2 == 0 ? z0 : z1;
+                    cw = (cw + 1) / 2;
+                    chh = (chh + 1) / 2;
+                }
+                k += used - 1;
+                continue;
+            }
+        }
         dim3 grid((cw + TW - 1) / TW, (chh + TH - 1) / TH, n);
         T* lld;
         size_t llp, ll_z;

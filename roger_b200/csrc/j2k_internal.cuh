@@ -59,7 +59,7 @@ enum : uint32_t {
     J2K_DEVERR_SEG_CAPACITY = 6,  // a coding-pass segment outgrew its slot (code-block styles)
 };
 
-constexpr int J2K_SCRATCH_SLOTS = 11;
+constexpr int J2K_SCRATCH_SLOTS = 12;
 
 constexpr int J2K_MQ_TIERS = 4;
 
@@ -85,11 +85,12 @@ struct j2k_ctx {
     int t1_seg_factor = 1;       // styled tier-1: pass-segment slot bytes per symbol (grown on overflow)
     int dwt_tma = 0;             // fast forward DWT: strips staged by TMA tensor copies (persistent CTAs)
     int t1a_ctas = 2;            // tier-1 phase A: resident CTAs per SM its registers are cut for (2 or 3)
+    int dwt_tail = 0;            // forward DWT: deep levels fused into one cooperative launch
 };
 
 // scratch slot ids
 enum { SCR_LL0 = 0, SCR_LL1 = 1, SCR_JOBS = 2, SCR_SYMS = 3, SCR_T1STATE = 4, SCR_MISC = 5,
-       SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8, SCR_UNITS = 9, SCR_SEGS = 10 };
+       SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8, SCR_UNITS = 9, SCR_SEGS = 10, SCR_BARRIER = 11 };
 
 j2k_status j2k_fail(j2k_ctx* ctx, j2k_status s, const std::string& msg);
 j2k_status j2k_cuda_check(j2k_ctx* ctx, cudaError_t e, const char* what);
