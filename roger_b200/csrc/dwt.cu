@@ -975,7 +975,8 @@ static j2k_status fwd_tail_launch(j2k_ctx* ctx, int k, int levels, int cw, int c
     using T = typename KT<KERN>::T;
     *used = 0;
     const bool quant = (KERN == 97) && steps != nullptr;
-    static int per_sm = 0;
+    static int per_sm_q = 0, per_sm_f = 0;  // resident CTAs per SM of each instantiation (set once)
+    int& per_sm = quant ? per_sm_q : per_sm_f;
     if (per_sm == 0) {
         int v = 0;
         J2K_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
