@@ -282,6 +282,12 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->dwt_tail = value != 0;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_T1D_LANES) {
+        if (value != 0 && value != 8 && value != 16 && value != 32)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder blocks per warp must be 0, 8, 16 or 32");
+        ctx->t1d_lanes = value;
+        return J2K_OK;
+    }
     if (key == J2K_TUNE_T1A_CTAS) {
         if (value != 2 && value != 3) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "phase-A CTAs per SM must be 2 or 3");
         ctx->t1a_ctas = value;

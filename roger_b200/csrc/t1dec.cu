@@ -1,11 +1,18 @@
 // EBCOT tier-1 decoder (T.800 Annex D context modelling + Annex C.3 MQ decoder).
 //
 // The reference has no decoder for this stage (src/OCLDecoder.cpp:35-38 runs only the "reverse"
-// DWT).  Decoding is serial per code-block (every context depends on the bits decoded before
-// it), so one warp takes one block: lane 0 runs the MQ decoder and the context logic on 64-bit
-// row masks of significance / sign / refined / visited in shared memory, the whole warp clears
-// the output region first and applies the signs at the end.  Magnitude bits are accumulated in
-// the output plane itself (each block owns its region).
+// DWT).  Decoding is serial per code-block: every context depends on the bits decoded before it.
+// The default kernel runs one code-block per LANE: a warp decodes 8, 16 or 32 blocks side by side,
+// each lane with its own MQ registers and its own 64-bit row masks of significance / sign /
+// refined / visited in shared memory (interleaved by lane, so that the warp's accesses to any rows
+// fall in distinct banks).  Lanes that take the same branch of the pass / stripe / column loops
+// issue together; the decoder is bound by the latency of each decision's dependent chain, not by
+// instruction issue, so a warp instruction that serves many blocks is what makes it fast.  The
+// warp clears its blocks' output regions first and applies the signs at the end, cooperatively;
+// magnitude bits go to the output plane by fire-and-forget atomic ORs (each block owns its region).
+// The older form, one warp per block with lane 0 decoding, stays as a tuning choice.
+#include <atomic>
+
 #include "j2k_internal.cuh"
 
 namespace {
@@ -100,10 +107,35 @@ __host__ __device__ __forceinline__ int clz32(uint32_t v) {
 #endif
 }
 
+// Decoder state of one code-block: rows of 64-bit masks (row r + 1 holds block row r; rows 0
+// and 65 are the zero border) and the 19 MQ context states.
 struct DecSmem {
-    uint64_t sig[66], neg[66], ref[66], vis[66];
-    uint8_t st[19];
+    uint64_t sig_[66], neg_[66], ref_[66], vis_[66];
+    uint8_t st_[19];
+    __host__ __device__ uint64_t& sig(int r) { return sig_[r]; }
+    __host__ __device__ uint64_t& neg(int r) { return neg_[r]; }
+    __host__ __device__ uint64_t& ref(int r) { return ref_[r]; }
+    __host__ __device__ uint64_t& vis(int r) { return vis_[r]; }
+    __host__ __device__ uint8_t& st(int k) { return st_[k]; }
 };
+
+// The same state for the lanes of a warp that decode L blocks side by side: word (a, r, lane) of
+// mask array a at base[(a * 66 + r) * L + lane], context state k at stb[k * L + lane].
+template <int L>
+struct LaneState {
+    uint64_t* base;
+    uint8_t* stb;
+    int lane;
+    __device__ uint64_t& sig(int r) { return base[(0 * 66 + r) * L + lane]; }
+    __device__ uint64_t& neg(int r) { return base[(1 * 66 + r) * L + lane]; }
+    __device__ uint64_t& ref(int r) { return base[(2 * 66 + r) * L + lane]; }
+    __device__ uint64_t& vis(int r) { return base[(3 * 66 + r) * L + lane]; }
+    __device__ uint8_t& st(int k) { return stb[k * L + lane]; }
+};
+template <int L>
+__host__ __device__ constexpr size_t lane_state_bytes() {  // one warp's share: the masks, then the context states
+    return (size_t)4 * 66 * L * 8 + (((size_t)19 * L + 15) & ~(size_t)15);
+}
 
 struct Mqd {
     const uint8_t* data;
@@ -149,8 +181,8 @@ struct Mqd {
             sh -= k;
         }
     }
-    __host__ __device__ int decode(uint8_t* st, const uint32_t* mq, int cx) {
-        const uint32_t sv = st[cx];
+    __host__ __device__ int decode(uint8_t& st, const uint32_t* mq) {
+        const uint32_t sv = st;
         const uint32_t e = mq[sv >> 1];
         const uint32_t qe = e & 0xFFFF;
         const int mps = sv & 1;
@@ -179,7 +211,7 @@ struct Mqd {
             }
             A = qe;
         }
-        st[cx] = (uint8_t)((nidx << 1) | nm);
+        st = (uint8_t)((nidx << 1) | nm);
         renorm();
         return D;
     }
@@ -225,22 +257,24 @@ struct RawD {
     }
 };
 
-// Serial decode of one code-block into magnitudes (blk, pre-zeroed) and sign/state masks in S.
-// Host-callable so that the exact device logic can be checked on the CPU.  STYLED: the block was
-// coded with code-block style `style` (contexts reset per pass, a new codeword segment after
-// every terminated pass, located by the pass ends `pe`; raw-coded passes read as bits).
-template <bool STYLED = false>
-__host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint8_t* data, int len, int numbps,
+// Serial decode of one code-block into magnitudes (blk, pre-zeroed) and sign/state masks in S
+// (a DecSmem, or a LaneState of a block decoded beside others in the same warp).  Host-callable
+// so that the exact device logic can be checked on the CPU.  STYLED: the block was coded with
+// code-block style `style` (contexts reset per pass, a new codeword segment after every
+// terminated pass, located by the pass ends `pe`; raw-coded passes read as bits).  RED: magnitude
+// bits are set by atomic ORs whose result is not read (device only).
+template <bool STYLED = false, bool RED = false, class State>
+__host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_t* data, int len, int numbps,
                                       int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch,
                                       int style = 0, const uint32_t* pe = nullptr) {
         const uint8_t* zct = T.zc[orient];
         const uint32_t* mq = T.mq;
 
         auto reset_states = [&]() {
-            for (int k = 0; k < 19; ++k) S.st[k] = 0;
-            S.st[0] = 4 << 1;
-            S.st[17] = 3 << 1;
-            S.st[18] = 46 << 1;
+            for (int k = 0; k < 19; ++k) S.st(k) = 0;
+            S.st(0) = 4 << 1;
+            S.st(17) = 3 << 1;
+            S.st(18) = 46 << 1;
         };
         reset_states();
         Mqd m;
@@ -266,21 +300,30 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
         // one decision in context cx, and one sign in sign context sc (label | xor << 7)
         auto dec = [&](int cx) -> int {
             if (STYLED && raw) return rd.bit();
-            return m.decode(S.st, mq, cx);
+            return m.decode(S.st(cx), mq);
         };
         auto dsign = [&](int sc) -> int {
             if (STYLED && raw) return rd.bit();
-            return m.decode(S.st, mq, sc & 31) ^ (sc >> 7);
+            return m.decode(S.st(sc & 31), mq) ^ (sc >> 7);
         };
         int pass = 0;
         const int nb = numbps, np = npasses;
         // a stripe column's neighbourhood, packed: bits 3r..3r+2 hold columns x-1..x+1 of block row
         // y0-1+r (r = 0..5), from the significance (or sign) rows; stripe row k's 9-bit
         // neighbourhood is then (W >> 3k) & 511 and its own bit 3k+4
-        auto colw = [&](const uint64_t* rows, int y0, int x) -> uint32_t {
+        auto colw = [&](bool negs, int y0, int x) -> uint32_t {
             uint32_t w = 0;
-            for (int r = 0; r < 6; ++r) w |= nb3(rows[y0 + r], x) << (3 * r);
+            for (int r = 0; r < 6; ++r) w |= nb3(negs ? S.neg(y0 + r) : S.sig(y0 + r), x) << (3 * r);
             return w;
+        };
+        auto add_bit = [&](int x, int y, int p) {
+#ifdef __CUDA_ARCH__
+            if (RED) {
+                atomicOr(reinterpret_cast<unsigned int*>(blk + (size_t)y * pitch + x), 1u << p);
+                return;
+            }
+#endif
+            blk[(size_t)y * pitch + x] |= 1 << p;
         };
         // sign-coding neighbourhood of stripe row k: sigL negL sigR negR sigU negU sigD negD
         auto n8of = [](uint32_t W, uint32_t NW, int k) -> uint32_t {
@@ -290,9 +333,9 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                    (((W >> (b + 7)) & 1) << 6) | (((NW >> (b + 7)) & 1) << 7);
         };
         auto set_sig = [&](int x, int y, int neg, int p) {
-            S.sig[y + 1] |= 1ull << x;
-            if (neg) S.neg[y + 1] |= 1ull << x;
-            blk[(size_t)y * pitch + x] |= 1 << p;
+            S.sig(y + 1) |= 1ull << x;
+            if (neg) S.neg(y + 1) |= 1ull << x;
+            add_bit(x, y, p);
         };
         const uint64_t cols = cw >= 64 ? ~0ull : ((1ull << cw) - 1);
         for (int p = nb - 1; p >= 0 && pass < np; --p) {
@@ -304,24 +347,25 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                     const int ny = min(4, ch - y0);
                     uint64_t cm = 0;
                     for (int y = y0; y < y0 + ny; ++y) {
-                        uint64_t nbm = S.sig[y] | S.sig[y + 1] | S.sig[y + 2];
+                        const uint64_t own = S.sig(y + 1);
+                        uint64_t nbm = S.sig(y) | own | S.sig(y + 2);
                         nbm |= (nbm << 1) | (nbm >> 1);
-                        cm |= ~S.sig[y + 1] & nbm;
+                        cm |= ~own & nbm;
                     }
                     cm &= cols;
                     while (cm) {
                         const int x = ctz64(cm);
                         cm &= cm - 1;
-                        uint32_t W = colw(S.sig, y0, x), NW = 0;
+                        uint32_t W = colw(false, y0, x), NW = 0;
                         bool nw = false;
                         for (int k = 0; k < ny; ++k) {
                             if ((W >> (3 * k + 4)) & 1) continue;  // significant already
                             const uint32_t n9 = (W >> (3 * k)) & 511;
                             if (!(n9 & 0x1EF)) continue;           // no significant neighbour
                             const int bit = dec(zct[n9]);
-                            S.vis[y0 + k + 1] |= 1ull << x;
+                            S.vis(y0 + k + 1) |= 1ull << x;
                             if (bit) {
-                                if (!nw) NW = colw(S.neg, y0, x), nw = true;
+                                if (!nw) NW = colw(true, y0, x), nw = true;
                                 const int sc = T.sc[n8of(W, NW, k)];
                                 const int sg = dsign(sc);
                                 set_sig(x, y0 + k, sg, p);
@@ -338,18 +382,18 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                 for (int y0 = 0; y0 < ch; y0 += 4) {
                     const int ny = min(4, ch - y0);
                     uint64_t rm = 0;
-                    for (int y = y0; y < y0 + ny; ++y) rm |= S.sig[y + 1] & ~S.vis[y + 1];
+                    for (int y = y0; y < y0 + ny; ++y) rm |= S.sig(y + 1) & ~S.vis(y + 1);
                     rm &= cols;
                     while (rm) {
                         const int x = ctz64(rm);
                         rm &= rm - 1;
-                        const uint32_t W = colw(S.sig, y0, x);
+                        const uint32_t W = colw(false, y0, x);
                         for (int k = 0; k < ny; ++k) {
                             const int y = y0 + k;
-                            if (!((W >> (3 * k + 4)) & 1) || ((S.vis[y + 1] >> x) & 1)) continue;
-                            const int lab = ((S.ref[y + 1] >> x) & 1) ? 16 : (((W >> (3 * k)) & 0x1EF) ? 15 : 14);
-                            if (dec(lab)) blk[(size_t)y * pitch + x] |= 1 << p;
-                            S.ref[y + 1] |= 1ull << x;
+                            if (!((W >> (3 * k + 4)) & 1) || ((S.vis(y + 1) >> x) & 1)) continue;
+                            const int lab = ((S.ref(y + 1) >> x) & 1) ? 16 : (((W >> (3 * k)) & 0x1EF) ? 15 : 14);
+                            if (dec(lab)) add_bit(x, y, p);
+                            S.ref(y + 1) |= 1ull << x;
                         }
                     }
                 }
@@ -360,14 +404,14 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
             for (int y0 = 0; y0 < ch; y0 += 4) {
                 const int ny = min(4, ch - y0);
                 uint64_t um = 0;
-                for (int y = y0; y < y0 + ny; ++y) um |= ~S.sig[y + 1] & ~S.vis[y + 1];
+                for (int y = y0; y < y0 + ny; ++y) um |= ~S.sig(y + 1) & ~S.vis(y + 1);
                 um &= cols;
                 while (um) {
                     const int x = ctz64(um);
                     um &= um - 1;
-                    uint32_t W = colw(S.sig, y0, x), NW = 0, V = 0;
+                    uint32_t W = colw(false, y0, x), NW = 0, V = 0;
                     bool nw = false;
-                    for (int k = 0; k < ny; ++k) V |= (uint32_t)((S.vis[y0 + k + 1] >> x) & 1) << k;
+                    for (int k = 0; k < ny; ++k) V |= (uint32_t)((S.vis(y0 + k + 1) >> x) & 1) << k;
                     int start = 0;
                     if (ny == 4 && W == 0 && V == 0) {
                         // run-length mode: four insignificant, unvisited samples, no significant
@@ -386,7 +430,7 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                     for (int k = start; k < ny; ++k) {
                         if (((W >> (3 * k + 4)) & 1) || ((V >> k) & 1)) continue;
                         if (dec(zct[(W >> (3 * k)) & 511])) {
-                            if (!nw) NW = colw(S.neg, y0, x), nw = true;
+                            if (!nw) NW = colw(true, y0, x), nw = true;
                             const int sc = T.sc[n8of(W, NW, k)];
                             const int sg = dsign(sc);
                             set_sig(x, y0 + k, sg, p);
@@ -397,8 +441,24 @@ __host__ __device__ void decode_block(DecSmem& S, const DecTables& T, const uint
                 }
             }
             ++pass;
-            for (int r = 0; r < 66; ++r) S.vis[r] = 0;
+            for (int r = 0; r < 66; ++r) S.vis(r) = 0;
         }
+}
+
+// the checks a decoder kernel makes of a job before touching its region
+__device__ __forceinline__ bool dec_job_ok(const j2k_cb_job& J, const j2k_cb_desc& D, bool styled) {
+    return !(J.cw == 0 || J.ch == 0 || J.cw > 64 || J.ch > 64 || J.orient > 3 || D.numbps > 31 ||
+             D.npasses > 3 * D.numbps || D.length < 0 || (styled && D.npasses > J2K_PASS_STRIDE - 1));
+}
+
+// magnitude offset of a block cut at the end of a bit-plane above the last one (rate control):
+// significant magnitudes are reconstructed at the middle of the interval their undecoded bits leave
+__host__ __device__ __forceinline__ int32_t cut_half(int numbps, int npasses) {
+    if (npasses < 3 * numbps - 2 && (npasses - 1) % 3 == 0) {
+        const int plast = numbps - 1 - (npasses - 1) / 3;
+        return plast > 0 ? 1 << (plast - 1) : 0;
+    }
+    return 0;
 }
 
 template <bool STYLED>
@@ -419,8 +479,7 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
     const j2k_cb_desc D = descs[jid];
     const int cw = J.cw, ch = J.ch, orient = J.orient;
     // (a styled block's passes index its pass ends: at most 3 * 31 - 2 of them)
-    if (cw == 0 || ch == 0 || cw > 64 || ch > 64 || orient > 3 || D.numbps > 31 ||
-        D.npasses > 3 * D.numbps || D.length < 0 || (STYLED && D.npasses > J2K_PASS_STRIDE - 1)) {
+    if (!dec_job_ok(J, D, STYLED)) {
         if (lane == 0) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
         return;
     }
@@ -428,28 +487,98 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
     int32_t* blk = coeff + J.off;
     for (int r = 0; r < ch; ++r)
         for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
-    for (int r = lane; r < 66; r += 32) { S.sig[r] = 0; S.neg[r] = 0; S.ref[r] = 0; S.vis[r] = 0; }
-    if (lane < 19) S.st[lane] = 0;
+    for (int r = lane; r < 66; r += 32) { S.sig_[r] = 0; S.neg_[r] = 0; S.ref_[r] = 0; S.vis_[r] = 0; }
+    if (lane < 19) S.st_[lane] = 0;
     __syncwarp();
     if (lane == 0 && D.numbps > 0 && D.npasses > 0)
         decode_block<STYLED>(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, orient, cw, ch, blk, pitch,
                              job_style ? (int)job_style[jid] : style,
                              STYLED ? pass_ends + (size_t)jid * J2K_PASS_STRIDE : nullptr);
     __syncwarp();
-    // a block cut at the end of a bit-plane above the last one (rate control): significant
-    // magnitudes are reconstructed at the middle of the interval their undecoded bits leave
-    int32_t half = 0;
-    if (D.npasses < 3 * D.numbps - 2 && (D.npasses - 1) % 3 == 0) {
-        const int plast = D.numbps - 1 - (D.npasses - 1) / 3;
-        half = plast > 0 ? 1 << (plast - 1) : 0;
-    }
+    const int32_t half = cut_half(D.numbps, D.npasses);
     for (int r = 0; r < ch; ++r)
         for (int x = lane; x < cw; x += 32) {
             int32_t v = blk[(size_t)r * pitch + x];
-            if ((S.sig[r + 1] >> x) & 1) v += half;
-            if ((S.neg[r + 1] >> x) & 1) v = -v;
+            if ((S.sig_[r + 1] >> x) & 1) v += half;
+            if ((S.neg_[r + 1] >> x) & 1) v = -v;
             blk[(size_t)r * pitch + x] = v;
         }
+}
+
+
+constexpr size_t kTablesBytes = (sizeof(DecTables) + 15) & ~(size_t)15;
+constexpr int kLaneCtaBlocks = 32;  // code-blocks per CTA of the lane-per-block decoder
+
+template <int L>
+__host__ __device__ constexpr size_t lanes_smem_bytes() {
+    return kTablesBytes + (size_t)(kLaneCtaBlocks / L) * lane_state_bytes<L>();
+}
+
+// One code-block per lane: a CTA takes 32 consecutive jobs in 32 / L warps of L (lanes 0..L-1 of
+// a warp decode, one block each); every lane of the warp helps clear its blocks' regions first
+// and apply the signs at the end.  Dynamic shared memory: the tables, then each warp's
+// LaneState<L> area.
+template <bool STYLED, int L>
+__global__ void __launch_bounds__(32 * (kLaneCtaBlocks / L))
+t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
+                       const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
+                       uint32_t* __restrict__ err, int style, const uint32_t* __restrict__ pass_ends,
+                       const uint8_t* __restrict__ job_style) {
+    extern __shared__ __align__(16) uint8_t dsm[];
+    DecTables& tabs = *reinterpret_cast<DecTables*>(dsm);
+    for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int j0 = blockIdx.x * kLaneCtaBlocks + wid * L;
+    if (j0 >= njobs) return;
+    const int nb = min(L, njobs - j0);
+    uint8_t* wsm = dsm + kTablesBytes + (size_t)wid * lane_state_bytes<L>();
+    uint64_t* base = reinterpret_cast<uint64_t*>(wsm);
+    uint8_t* stb = wsm + (size_t)4 * 66 * L * 8;
+    j2k_cb_job J{};
+    j2k_cb_desc D{};
+    bool ok = false;
+    if (lane < nb) {
+        J = jobs[j0 + lane];
+        D = descs[j0 + lane];
+        ok = dec_job_ok(J, D, STYLED);
+        if (!ok) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+    }
+    const unsigned okmask = __ballot_sync(~0u, ok);
+    for (int i = lane; i < 4 * 66 * L; i += 32) base[i] = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (!((okmask >> b) & 1)) continue;
+        const int cw = __shfl_sync(~0u, (int)J.cw, b), ch = __shfl_sync(~0u, (int)J.ch, b);
+        const size_t pitch = __shfl_sync(~0u, J.pitch, b);
+        int32_t* blk = coeff + __shfl_sync(~0u, (unsigned long long)J.off, b);
+        for (int r = 0; r < ch; ++r)
+            for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
+    }
+    __syncwarp();
+    if (ok && D.numbps > 0 && D.npasses > 0) {
+        LaneState<L> S{base, stb, lane};
+        decode_block<STYLED, true>(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, J.orient, J.cw, J.ch,
+                                   coeff + J.off, J.pitch, job_style ? (int)job_style[j0 + lane] : style,
+                                   STYLED ? pass_ends + (size_t)(j0 + lane) * J2K_PASS_STRIDE : nullptr);
+    }
+    __syncwarp();
+    const int32_t my_half = ok ? cut_half(D.numbps, D.npasses) : 0;
+    for (int b = 0; b < nb; ++b) {
+        if (!((okmask >> b) & 1)) continue;
+        const int cw = __shfl_sync(~0u, (int)J.cw, b), ch = __shfl_sync(~0u, (int)J.ch, b);
+        const size_t pitch = __shfl_sync(~0u, J.pitch, b);
+        int32_t* blk = coeff + __shfl_sync(~0u, (unsigned long long)J.off, b);
+        const int32_t half = __shfl_sync(~0u, my_half, b);
+        for (int r = 0; r < ch; ++r) {
+            const uint64_t sg = base[(0 * 66 + r + 1) * L + b], ng = base[(1 * 66 + r + 1) * L + b];
+            for (int x = lane; x < cw; x += 32) {
+                int32_t v = __ldcg(blk + (size_t)r * pitch + x);
+                if ((sg >> x) & 1) v += half;
+                if ((ng >> x) & 1) v = -v;
+                blk[(size_t)r * pitch + x] = v;
+            }
+        }
+    }
 }
 
 }  // namespace
@@ -461,8 +590,8 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
         npasses < 0 || npasses > 3 * numbps || len < 0 || (len > 0 && !data) || !out || pitch < (size_t)cw)
         return -1;  // the checks the kernel makes of a descriptor, and the host buffers
     DecSmem S;
-    for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
-    for (int k = 0; k < 19; ++k) S.st[k] = 0;
+    for (int r = 0; r < 66; ++r) S.sig_[r] = S.neg_[r] = S.ref_[r] = S.vis_[r] = 0;
+    for (int k = 0; k < 19; ++k) S.st_[k] = 0;
     static const DecTables T = [] {  // built once, thread-safely
         DecTables t{};
         for (int i = 0; i < 4 * 512; ++i) fill_tables_entry(t, i);
@@ -473,7 +602,7 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
     if (numbps > 0 && npasses > 0) decode_block(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x)
-            if ((S.neg[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
+            if ((S.neg_[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
     return 0;
 }
 
@@ -487,8 +616,8 @@ extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, con
         !out || pitch < (size_t)cw || !pass_ends || style < 0 || style > 7)
         return -1;
     DecSmem S;
-    for (int r = 0; r < 66; ++r) S.sig[r] = S.neg[r] = S.ref[r] = S.vis[r] = 0;
-    for (int k = 0; k < 19; ++k) S.st[k] = 0;
+    for (int r = 0; r < 66; ++r) S.sig_[r] = S.neg_[r] = S.ref_[r] = S.vis_[r] = 0;
+    for (int k = 0; k < 19; ++k) S.st_[k] = 0;
     static const DecTables T = [] {
         DecTables t{};
         for (int i = 0; i < 4 * 512; ++i) fill_tables_entry(t, i);
@@ -500,8 +629,26 @@ extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, con
         decode_block<true>(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch, style, pass_ends);
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x)
-            if ((S.neg[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
+            if ((S.neg_[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
     return 0;
+}
+
+template <bool STYLED, int L>
+static j2k_status launch_lanes(j2k_ctx* ctx, unsigned grid, cudaStream_t st, const j2k_cb_desc* descs,
+                               const uint8_t* bytes, const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
+                               int style, const uint32_t* pass_ends, const uint8_t* job_style) {
+    constexpr size_t smem = lanes_smem_bytes<L>();
+    static std::atomic<uint64_t> attr_set{0};  // devices whose attribute is set, per instantiation
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    if (!(attr_set.load() & bit)) {
+        J2K_CUDA(ctx, cudaFuncSetAttribute(t1_decode_lanes_kernel<STYLED, L>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set.fetch_or(bit);
+    }
+    t1_decode_lanes_kernel<STYLED, L><<<grid, 32 * (kLaneCtaBlocks / L), smem, st>>>(
+        descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, style, pass_ends, job_style);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
 }
 
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
@@ -510,13 +657,27 @@ j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint
     if (njobs == 0) return J2K_OK;
     if ((style || job_style) && !pass_ends)
         return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "a styled decode needs the pass ends");
-    unsigned g = (unsigned)((njobs + kWarps - 1) / kWarps);
-    if (style || job_style)
-        t1_decode_kernel<true><<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, style,
-                                                          pass_ends, job_style);
-    else
-        t1_decode_kernel<false><<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, 0,
-                                                           nullptr, nullptr);
-    J2K_CUDA(ctx, cudaGetLastError());
-    return J2K_OK;
+    const bool styled = style || job_style;
+    const int L = ctx->t1d_lanes;
+    if (L == 0) {  // one warp per block, lane 0 decoding
+        const unsigned g = (unsigned)((njobs + kWarps - 1) / kWarps);
+        if (styled)
+            t1_decode_kernel<true><<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err,
+                                                              style, pass_ends, job_style);
+        else
+            t1_decode_kernel<false><<<g, kWarps * 32, 0, st>>>(descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err,
+                                                               0, nullptr, nullptr);
+        J2K_CUDA(ctx, cudaGetLastError());
+        return J2K_OK;
+    }
+    const unsigned g = (unsigned)((njobs + kLaneCtaBlocks - 1) / kLaneCtaBlocks);
+    switch ((styled ? 100 : 0) + L) {
+    case 8: return launch_lanes<false, 8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 16: return launch_lanes<false, 16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 32: return launch_lanes<false, 32>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 108: return launch_lanes<true, 8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 116: return launch_lanes<true, 16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 132: return launch_lanes<true, 32>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder: blocks per warp must be 0, 8, 16 or 32");
+    }
 }
