@@ -288,6 +288,10 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->t1d_lanes = value;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_T1D_STEPS) {
+        ctx->t1d_steps = value != 0;
+        return J2K_OK;
+    }
     if (key == J2K_TUNE_T1A_CTAS) {
         if (value != 2 && value != 3) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "phase-A CTAs per SM must be 2 or 3");
         ctx->t1a_ctas = value;

@@ -229,6 +229,16 @@ __host__ __device__ __forceinline__ uint32_t nb3(uint64_t m, int x) {
     return (uint32_t)(x > 0 ? (m >> (x - 1)) & 7 : (m << 1) & 7);
 }
 
+// sign-coding neighbourhood of stripe row k of a column whose significance / sign neighbourhoods
+// are W / NW (bits 3r..3r+2: columns x-1..x+1 of window row r): sigL negL sigR negR sigU negU
+// sigD negD
+__host__ __device__ __forceinline__ uint32_t sign_nbhd(uint32_t W, uint32_t NW, int k) {
+    const int b = 3 * k;
+    return ((W >> (b + 3)) & 1) | (((NW >> (b + 3)) & 1) << 1) | (((W >> (b + 5)) & 1) << 2) |
+           (((NW >> (b + 5)) & 1) << 3) | (((W >> (b + 1)) & 1) << 4) | (((NW >> (b + 1)) & 1) << 5) |
+           (((W >> (b + 7)) & 1) << 6) | (((NW >> (b + 7)) & 1) << 7);
+}
+
 // Raw (bypass) segment reader, T.800 D.6: bits most significant first; a byte after 0xFF holds
 // 7 bits (its top bit is a stuffed 0); past the end of the segment 0xFF is read.
 struct RawD {
@@ -325,13 +335,7 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
 #endif
             blk[(size_t)y * pitch + x] |= 1 << p;
         };
-        // sign-coding neighbourhood of stripe row k: sigL negL sigR negR sigU negU sigD negD
-        auto n8of = [](uint32_t W, uint32_t NW, int k) -> uint32_t {
-            const int b = 3 * k;
-            return ((W >> (b + 3)) & 1) | (((NW >> (b + 3)) & 1) << 1) | (((W >> (b + 5)) & 1) << 2) |
-                   (((NW >> (b + 5)) & 1) << 3) | (((W >> (b + 1)) & 1) << 4) | (((NW >> (b + 1)) & 1) << 5) |
-                   (((W >> (b + 7)) & 1) << 6) | (((NW >> (b + 7)) & 1) << 7);
-        };
+        auto n8of = [](uint32_t W, uint32_t NW, int k) { return sign_nbhd(W, NW, k); };
         auto set_sig = [&](int x, int y, int neg, int p) {
             S.sig(y + 1) |= 1ull << x;
             if (neg) S.neg(y + 1) |= 1ull << x;
@@ -581,9 +585,261 @@ t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     }
 }
 
+
+// symbol kinds, pass kinds and pending symbols of decode_block_steps
+enum : int { kSymZC = 0, kSymSign = 1, kSymMR = 2, kSymRL = 3, kSymUni = 4 };
+enum : int { kPassCU = 0, kPassSP = 1, kPassMR = 2 };
+enum : int { kPendNone = 0, kPendSign = 1, kPendUni1 = 2, kPendUni2 = 3 };
+
+// The same decode as decode_block (unstyled blocks), written as a loop of one symbol per step:
+// (1) advance the cursor (pass, stripe, column, row) to the next sample that codes a symbol in its
+// pass, or take the pending sign / run-length index symbol, (2) decode that one symbol -- the MQ
+// decoder's only call site -- and (3) apply it.  Lanes of a warp that decode different blocks
+// with it stay together on the decoding step whatever pass or column each is in.  The scan
+// order, contexts and pass rules are T.800 D.3-D.5 (significance propagation, magnitude
+// refinement and cleanup passes, stripes of four rows scanned column by column, the cleanup
+// pass's run-length mode).  Host-callable, for the tests.
+template <bool RED = false, class State>
+__host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, const uint8_t* data, int len, int numbps,
+                                            int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch) {
+    auto add_bit = [&](int x, int y, int p) {
+#ifdef __CUDA_ARCH__
+        if (RED) {
+            atomicOr(reinterpret_cast<unsigned int*>(blk + (size_t)y * pitch + x), 1u << p);
+            return;
+        }
+#endif
+        blk[(size_t)y * pitch + x] |= 1 << p;
+    };
+    const uint8_t* zct = tabs.zc[orient];
+    const uint32_t* mq = tabs.mq;
+    const int np = npasses;
+    const uint64_t cols = cw >= 64 ? ~0ull : ((1ull << cw) - 1);
+    for (int c = 0; c < 19; ++c) S.st(c) = 0;
+    S.st(0) = 4 << 1;
+    S.st(17) = 3 << 1;
+    S.st(18) = 46 << 1;
+    Mqd m;
+    m.init(data, len);
+    // cursor
+    int pass = 0, ptype = kPassCU, p = numbps - 1, y0 = 0, x = 0, k = 4, ny = min(4, ch);
+    int pending = kPendNone, idx = 0;
+    bool colstart = false, nwv = false;
+    uint32_t W = 0, NW = 0, V = 0, R = 0;
+    uint64_t cm = 0;
+    // candidate columns of the stripe at y0 in the current pass
+    auto stripe_setup = [&]() {
+        ny = min(4, ch - y0);
+        uint64_t c = 0;
+        for (int r = 0; r < ny; ++r) {
+            const uint64_t own = S.sig(y0 + r + 1);
+            if (ptype == kPassSP) {
+                uint64_t nbm = S.sig(y0 + r) | own | S.sig(y0 + r + 2);
+                nbm |= (nbm << 1) | (nbm >> 1);
+                c |= ~own & nbm;
+            } else {
+                const uint64_t vis = S.vis(y0 + r + 1);
+                c |= (ptype == kPassMR ? own : ~own) & ~vis;
+            }
+        }
+        cm = c & cols;
+    };
+    auto colw = [&](bool negs) -> uint32_t {
+        uint32_t w = 0;
+        for (int r = 0; r < 6; ++r) w |= nb3(negs ? S.neg(y0 + r) : S.sig(y0 + r), x) << (3 * r);
+        return w;
+    };
+    stripe_setup();
+    // rows of the current column, from row k on, that code a symbol in this pass
+    auto cand_rows = [&]() -> uint32_t {
+        const uint32_t s4 = ((W >> 4) & 1) | ((W >> 6) & 2) | ((W >> 8) & 4) | ((W >> 10) & 8);
+        uint32_t rows;
+        if (ptype == kPassSP) {
+            uint32_t n4 = 0;
+            for (int r = 0; r < 4; ++r) n4 |= (uint32_t)(((W >> (3 * r)) & 0x1EF) != 0) << r;
+            rows = ~s4 & n4;
+        } else {
+            rows = (ptype == kPassMR ? s4 : ~s4) & ~V;
+        }
+        return rows & ((1u << ny) - 1) & (0xFu << k);
+    };
+    for (;;) {
+        int kind = kSymUni;
+        if (pending == kPendSign) {
+            kind = kSymSign;
+        } else if (pending == kPendNone) {
+            bool done = false;
+            for (;;) {
+                if (k < 4) {
+                    if (ptype == kPassCU && colstart && ny == 4 && W == 0 && V == 0) {
+                        kind = kSymRL;  // run-length mode: no significant sample around the column
+                        break;
+                    }
+                    const uint32_t rows = cand_rows();
+                    if (rows) {
+                        k = ctz64(rows);
+                        kind = ptype == kPassMR ? kSymMR : kSymZC;
+                        break;
+                    }
+                    k = 4;
+                }
+                if (cm) {  // next column of the stripe that holds a candidate
+                    x = ctz64(cm);
+                    cm &= cm - 1;
+                    W = colw(false);
+                    nwv = false;
+                    V = 0;
+                    R = 0;
+                    if (ptype != kPassSP)
+                        for (int r = 0; r < ny; ++r) V |= (uint32_t)((S.vis(y0 + r + 1) >> x) & 1) << r;
+                    if (ptype == kPassMR)
+                        for (int r = 0; r < ny; ++r) R |= (uint32_t)((S.ref(y0 + r + 1) >> x) & 1) << r;
+                    k = 0;
+                    colstart = true;
+                    continue;
+                }
+                if (y0 + 4 < ch) {  // next stripe
+                    y0 += 4;
+                    stripe_setup();
+                    continue;
+                }
+                // end of the pass
+                if (ptype == kPassCU)
+                    for (int r = 0; r < 66; ++r) S.vis(r) = 0;
+                if (++pass >= np || (ptype == kPassCU && p == 0)) {  // (the last plane's cleanup ends it)
+                    done = true;
+                    break;
+                }
+                if (ptype == kPassCU) {
+                    --p;
+                    ptype = kPassSP;
+                } else {
+                    ptype = ptype == kPassSP ? kPassMR : kPassCU;
+                }
+                y0 = 0;
+                stripe_setup();
+            }
+            if (done) break;
+        }
+        // the symbol's context (sign symbols: label | xor bit << 7)
+        int cx, xr = 0;
+        if (kind == kSymZC) {
+            cx = zct[(W >> (3 * k)) & 511];
+        } else if (kind == kSymMR) {
+            cx = ((R >> k) & 1) ? 16 : (((W >> (3 * k)) & 0x1EF) ? 15 : 14);
+        } else if (kind == kSymSign) {
+            if (!nwv && W) {  // (with no significant neighbour the signs around do not matter)
+                NW = colw(true);
+                nwv = true;
+            }
+            const int sc = tabs.sc[sign_nbhd(W, NW, k)];
+            cx = sc & 31;
+            xr = sc >> 7;
+        } else {
+            cx = kind == kSymRL ? 17 : 18;
+        }
+        const int d = m.decode(S.st(cx), mq) ^ xr;
+        if (kind == kSymZC) {
+            if (ptype == kPassSP) S.vis(y0 + k + 1) |= 1ull << x;
+            if (d) pending = kPendSign;
+            else ++k;
+            colstart = false;
+        } else if (kind == kSymSign) {
+            const int y = y0 + k;
+            S.sig(y + 1) |= 1ull << x;
+            if (d) S.neg(y + 1) |= 1ull << x;
+            add_bit(x, y, p);
+            W |= 1u << (3 * k + 4);
+            NW |= (uint32_t)d << (3 * k + 4);
+            if (ptype == kPassSP) cm |= (2ull << x) & cols;
+            pending = kPendNone;
+            ++k;
+        } else if (kind == kSymMR) {
+            const int y = y0 + k;
+            if (d) add_bit(x, y, p);
+            S.ref(y + 1) |= 1ull << x;
+            ++k;
+        } else if (kind == kSymRL) {
+            colstart = false;
+            if (d) pending = kPendUni1;
+            else k = 4;
+        } else if (pending == kPendUni1) {
+            idx = d << 1;
+            pending = kPendUni2;
+        } else {
+            k = idx | d;
+            pending = kPendSign;
+        }
+    }
+}
+
+// One code-block per lane, each decoded by decode_block_steps.
+
+template <int L>
+__global__ void __launch_bounds__(32 * (kLaneCtaBlocks / L))
+t1_decode_steps_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
+                       const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
+                       uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) uint8_t dsm[];
+    DecTables& tabs = *reinterpret_cast<DecTables*>(dsm);
+    for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int j0 = blockIdx.x * kLaneCtaBlocks + wid * L;
+    if (j0 >= njobs) return;
+    const int nb = min(L, njobs - j0);
+    uint8_t* wsm = dsm + kTablesBytes + (size_t)wid * lane_state_bytes<L>();
+    uint64_t* base = reinterpret_cast<uint64_t*>(wsm);
+    uint8_t* stb = wsm + (size_t)4 * 66 * L * 8;
+    j2k_cb_job J{};
+    j2k_cb_desc D{};
+    bool ok = false;
+    if (lane < nb) {
+        J = jobs[j0 + lane];
+        D = descs[j0 + lane];
+        ok = dec_job_ok(J, D, false);
+        if (!ok) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
+    }
+    const unsigned okmask = __ballot_sync(~0u, ok);
+    for (int i = lane; i < 4 * 66 * L; i += 32) base[i] = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (!((okmask >> b) & 1)) continue;
+        const int cw = __shfl_sync(~0u, (int)J.cw, b), ch = __shfl_sync(~0u, (int)J.ch, b);
+        const size_t pitch = __shfl_sync(~0u, J.pitch, b);
+        int32_t* blk = coeff + __shfl_sync(~0u, (unsigned long long)J.off, b);
+        for (int r = 0; r < ch; ++r)
+            for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
+    }
+    __syncwarp();
+    if (ok && D.numbps > 0 && D.npasses > 0) {
+        LaneState<L> S{base, stb, lane};
+        decode_block_steps<true>(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, J.orient, J.cw, J.ch,
+                                 coeff + J.off, J.pitch);
+    }
+    __syncwarp();
+    const int32_t my_half = ok ? cut_half(D.numbps, D.npasses) : 0;
+    for (int b = 0; b < nb; ++b) {
+        if (!((okmask >> b) & 1)) continue;
+        const int cw = __shfl_sync(~0u, (int)J.cw, b), ch = __shfl_sync(~0u, (int)J.ch, b);
+        const size_t pitch = __shfl_sync(~0u, J.pitch, b);
+        int32_t* blk = coeff + __shfl_sync(~0u, (unsigned long long)J.off, b);
+        const int32_t half = __shfl_sync(~0u, my_half, b);
+        for (int r = 0; r < ch; ++r) {
+            const uint64_t sg = base[(0 * 66 + r + 1) * L + b], ng = base[(1 * 66 + r + 1) * L + b];
+            for (int x = lane; x < cw; x += 32) {
+                int32_t v = __ldcg(blk + (size_t)r * pitch + x);
+                if ((sg >> x) & 1) v += half;
+                if ((ng >> x) & 1) v = -v;
+                blk[(size_t)r * pitch + x] = v;
+            }
+        }
+    }
+}
+
 }  // namespace
 
-// Host execution of the device decoder logic for one block (used by the test suite).
+// Host execution of the device decoder logic for one block (used by the test suite): the
+// one-symbol-per-step loop that the default decoder kernel runs for unstyled blocks.
 extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
                                         int cw, int ch, int32_t* out, size_t pitch) {
     if (cw < 1 || ch < 1 || cw > 64 || ch > 64 || orient < 0 || orient > 3 || numbps < 0 || numbps > 31 ||
@@ -599,7 +855,7 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
     }();
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x) out[(size_t)y * pitch + x] = 0;
-    if (numbps > 0 && npasses > 0) decode_block(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
+    if (numbps > 0 && npasses > 0) decode_block_steps(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x)
             if ((S.neg_[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
@@ -651,6 +907,23 @@ static j2k_status launch_lanes(j2k_ctx* ctx, unsigned grid, cudaStream_t st, con
     return J2K_OK;
 }
 
+template <int L>
+static j2k_status launch_steps(j2k_ctx* ctx, unsigned grid, cudaStream_t st, const j2k_cb_desc* descs,
+                               const uint8_t* bytes, const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff) {
+    constexpr size_t smem = lanes_smem_bytes<L>();
+    static std::atomic<uint64_t> attr_set{0};
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    if (!(attr_set.load() & bit)) {
+        J2K_CUDA(ctx, cudaFuncSetAttribute(t1_decode_steps_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        attr_set.fetch_or(bit);
+    }
+    t1_decode_steps_kernel<L><<<grid, 32 * (kLaneCtaBlocks / L), smem, st>>>(descs, bytes, d_jobs, (int)njobs, coeff,
+                                                                            ctx->d_err);
+    J2K_CUDA(ctx, cudaGetLastError());
+    return J2K_OK;
+}
+
 j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint8_t* bytes,
                               const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
                               cudaStream_t st, int style, const uint32_t* pass_ends, const uint8_t* job_style) {
@@ -671,6 +944,14 @@ j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint
         return J2K_OK;
     }
     const unsigned g = (unsigned)((njobs + kLaneCtaBlocks - 1) / kLaneCtaBlocks);
+    if (!styled && ctx->t1d_steps) {
+        switch (L) {
+        case 8: return launch_steps<8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff);
+        case 16: return launch_steps<16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff);
+        case 32: return launch_steps<32>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff);
+        default: break;
+        }
+    }
     switch ((styled ? 100 : 0) + L) {
     case 8: return launch_lanes<false, 8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
     case 16: return launch_lanes<false, 16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);

@@ -1,6 +1,6 @@
 // Random-input fuzzer for the tier-1 block decoder, through its host entry point
-// j2k_t1_decode_block_host, which runs the same __host__ __device__ decode_block as the device
-// kernel.  Built with AddressSanitizer and UBSan together with t1dec.cu itself.  Each block gets
+// j2k_t1_decode_block_host, which runs the same __host__ __device__ decode_block_steps as the
+// default device kernel.  Built with AddressSanitizer and UBSan together with t1dec.cu itself.  Each block gets
 // a random size (1..64 a side, at most 4096 samples), orientation, bit-plane count, a pass count
 // the kernel's descriptor check admits (0..3*numbps) and a codeword of random, all-0xFF or
 // sparse bytes held in a buffer of exactly its length, so that any read past the codeword's end

@@ -104,3 +104,30 @@ def test_device_decoder_logic_runs_on_host(cw, ch, orient):
     out = np.zeros_like(blk)
     assert f(buf.ctypes.data, len(data), info["numbps"], info["npasses"], orient, cw, ch, out.ctypes.data, cw) == 0
     assert np.array_equal(out, blk)
+
+
+@pytest.mark.parametrize("cw,ch,orient", [(64, 64, 0), (64, 64, 3), (33, 17, 1), (64, 3, 2), (5, 64, 0)])
+def test_device_decoder_logic_on_truncated_passes(cw, ch, orient):
+    """The same host run of the device decoder on every pass count of oracle-encoded blocks
+    (rate-control cuts end a block after any pass), against the oracle's decoder; the oracle puts
+    a block cut at a plane end at the middle of its interval, the device routine leaves that to
+    the kernel's sign pass."""
+    import ctypes as C
+    from oracle import oracle as O
+    from roger_b200 import _lib
+    f = C.CDLL(_lib.LIB_PATH).j2k_t1_decode_block_host
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
+    rng = np.random.default_rng(cw * 11 + ch * 3 + orient)
+    blk = (rng.laplace(0, 40, (ch, cw)) * (rng.random((ch, cw)) < 0.7)).astype(np.int32)
+    data, info = O.t1_encode(blk, orient)
+    nb, full = info["numbps"], info["npasses"]
+    buf = np.frombuffer(data + b"\0", np.uint8).copy()
+    for npasses in range(1, full + 1):
+        out = np.zeros_like(blk)
+        assert f(buf.ctypes.data, len(data), nb, npasses, orient, cw, ch, out.ctypes.data, cw) == 0
+        half = 0
+        if npasses < 3 * nb - 2 and (npasses - 1) % 3 == 0:
+            plast = nb - 1 - (npasses - 1) // 3
+            half = 1 << (plast - 1) if plast > 0 else 0
+        got = np.where(out != 0, np.sign(out) * (np.abs(out) + half), 0)
+        assert np.array_equal(got, O.t1_decode(data, nb, npasses, orient, cw, ch)), npasses
