@@ -403,13 +403,19 @@ class OCLDecoder(OCLEncodeDecode):
             pass
 
     def run(self, descs, data, w, h, ncomp, levels=5, cbw=64, cbh=64, order=L.ORDER_T800, steps=None,
-            cblk_style=0, pass_ends=None):
-        """descs/data as returned by OCLEncoder.get_codeblocks (host).  Returns (H, W, C) uint8.
-        Blocks coded with a code-block style need cblk_style and their pass ends
-        (OCLEncoder.get_pass_ends, read_pass_ends)."""
+            cblk_style=0, pass_ends=None, out=None):
+        """descs/data as returned by OCLEncoder.get_codeblocks (host).  Returns (H, W, C) uint8:
+        `out` when given (a C-contiguous (H, W, C) uint8 host array, e.g. page-locked memory,
+        which the pixels are copied into directly), else a new array.  Blocks coded with a
+        code-block style need cblk_style and their pass ends (OCLEncoder.get_pass_ends,
+        read_pass_ends)."""
         descs = np.ascontiguousarray(descs)
         data = np.ascontiguousarray(data, np.uint8)
-        out = np.zeros((h, w, ncomp), np.uint8)
+        if out is None:
+            out = np.zeros((h, w, ncomp), np.uint8)
+        elif (out.dtype != np.uint8 or out.shape != (h, w, ncomp) or not out.flags["C_CONTIGUOUS"]
+              or not out.flags["WRITEABLE"]):
+            raise ValueError(f"out must be a writeable C-contiguous uint8 array of shape {(h, w, ncomp)}")
         if cblk_style and pass_ends is None:
             raise ValueError("a styled decode needs the pass ends")
         p, keep = _params(levels, cbw, cbh, order, steps, cblk_style=cblk_style, pass_ends=pass_ends)

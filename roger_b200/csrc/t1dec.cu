@@ -601,7 +601,8 @@ enum : int { kPendNone = 0, kPendSign = 1, kPendUni1 = 2, kPendUni2 = 3 };
 // pass's run-length mode).  Host-callable, for the tests.
 template <bool RED = false, class State>
 __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, const uint8_t* data, int len, int numbps,
-                                            int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch) {
+                                            int npasses, int orient, int cw, int ch, int32_t* blk, size_t pitch,
+                                            bool active = true) {
     auto add_bit = [&](int x, int y, int p) {
 #ifdef __CUDA_ARCH__
         if (RED) {
@@ -611,16 +612,18 @@ __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, con
 #endif
         blk[(size_t)y * pitch + x] |= 1 << p;
     };
-    const uint8_t* zct = tabs.zc[orient];
+    const uint8_t* zct = tabs.zc[orient & 3];
     const uint32_t* mq = tabs.mq;
     const int np = npasses;
     const uint64_t cols = cw >= 64 ? ~0ull : ((1ull << cw) - 1);
-    for (int c = 0; c < 19; ++c) S.st(c) = 0;
-    S.st(0) = 4 << 1;
-    S.st(17) = 3 << 1;
-    S.st(18) = 46 << 1;
     Mqd m;
-    m.init(data, len);
+    if (active) {
+        for (int c = 0; c < 19; ++c) S.st(c) = 0;
+        S.st(0) = 4 << 1;
+        S.st(17) = 3 << 1;
+        S.st(18) = 46 << 1;
+        m.init(data, len);
+    }
     // cursor
     int pass = 0, ptype = kPassCU, p = numbps - 1, y0 = 0, x = 0, k = 4, ny = min(4, ch);
     int pending = kPendNone, idx = 0;
@@ -649,7 +652,7 @@ __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, con
         for (int r = 0; r < 6; ++r) w |= nb3(negs ? S.neg(y0 + r) : S.sig(y0 + r), x) << (3 * r);
         return w;
     };
-    stripe_setup();
+    if (active) stripe_setup();
     // rows of the current column, from row k on, that code a symbol in this pass
     auto cand_rows = [&]() -> uint32_t {
         const uint32_t s4 = ((W >> 4) & 1) | ((W >> 6) & 2) | ((W >> 8) & 4) | ((W >> 10) & 8);
@@ -663,7 +666,15 @@ __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, con
         }
         return rows & ((1u << ny) - 1) & (0xFu << k);
     };
-    for (;;) {
+    // On the device every lane of the warp runs this loop (lanes without a block, or done with
+    // theirs, inactive), and the vote at the top of each step brings the lanes back together
+    // before the next symbol, however their searches diverged.
+#ifdef __CUDA_ARCH__
+    while (__any_sync(0xffffffffu, active)) {
+        if (!active) continue;
+#else
+    while (active) {
+#endif
         int kind = kSymUni;
         if (pending == kPendSign) {
             kind = kSymSign;
@@ -719,7 +730,10 @@ __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, con
                 y0 = 0;
                 stripe_setup();
             }
-            if (done) break;
+            if (done) {
+                active = false;
+                continue;
+            }
         }
         // the symbol's context (sign symbols: label | xor bit << 7)
         int cx, xr = 0;
@@ -811,10 +825,11 @@ t1_decode_steps_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
             for (int x = lane; x < cw; x += 32) blk[(size_t)r * pitch + x] = 0;
     }
     __syncwarp();
-    if (ok && D.numbps > 0 && D.npasses > 0) {
-        LaneState<L> S{base, stb, lane};
+    {  // every lane of the warp takes part in the step loop, whether or not it has a block
+        LaneState<L> S{base, stb, lane < L ? lane : 0};
+        const bool act = ok && D.numbps > 0 && D.npasses > 0;
         decode_block_steps<true>(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, J.orient, J.cw, J.ch,
-                                 coeff + J.off, J.pitch);
+                                 coeff + J.off, J.pitch, act);
     }
     __syncwarp();
     const int32_t my_half = ok ? cut_half(D.numbps, D.npasses) : 0;
