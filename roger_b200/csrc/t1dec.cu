@@ -511,11 +511,16 @@ t1_decode_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restric
 
 
 constexpr size_t kTablesBytes = (sizeof(DecTables) + 15) & ~(size_t)15;
-constexpr int kLaneCtaBlocks = 32;  // code-blocks per CTA of the lane-per-block decoder
+// warps per CTA of the lane-per-block decoders for L blocks per warp: 32 blocks per CTA for
+// L >= 8, four warps for smaller L (so that a CTA's shared-memory state stays near 70 KB or less)
+template <int L>
+__host__ __device__ constexpr int cta_warps() {
+    return L >= 8 ? 32 / L : 4;
+}
 
 template <int L>
 __host__ __device__ constexpr size_t lanes_smem_bytes() {
-    return kTablesBytes + (size_t)(kLaneCtaBlocks / L) * lane_state_bytes<L>();
+    return kTablesBytes + (size_t)cta_warps<L>() * lane_state_bytes<L>();
 }
 
 // One code-block per lane: a CTA takes 32 consecutive jobs in 32 / L warps of L (lanes 0..L-1 of
@@ -523,7 +528,7 @@ __host__ __device__ constexpr size_t lanes_smem_bytes() {
 // and apply the signs at the end.  Dynamic shared memory: the tables, then each warp's
 // LaneState<L> area.
 template <bool STYLED, int L>
-__global__ void __launch_bounds__(32 * (kLaneCtaBlocks / L))
+__global__ void __launch_bounds__(32 * cta_warps<L>())
 t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
                        const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
                        uint32_t* __restrict__ err, int style, const uint32_t* __restrict__ pass_ends,
@@ -533,7 +538,7 @@ t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int j0 = blockIdx.x * kLaneCtaBlocks + wid * L;
+    const int j0 = (blockIdx.x * cta_warps<L>() + wid) * L;
     if (j0 >= njobs) return;
     const int nb = min(L, njobs - j0);
     uint8_t* wsm = dsm + kTablesBytes + (size_t)wid * lane_state_bytes<L>();
@@ -790,7 +795,7 @@ __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, con
 // One code-block per lane, each decoded by decode_block_steps.
 
 template <int L>
-__global__ void __launch_bounds__(32 * (kLaneCtaBlocks / L))
+__global__ void __launch_bounds__(32 * cta_warps<L>())
 t1_decode_steps_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
                        const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
                        uint32_t* __restrict__ err) {
@@ -799,7 +804,7 @@ t1_decode_steps_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int j0 = blockIdx.x * kLaneCtaBlocks + wid * L;
+    const int j0 = (blockIdx.x * cta_warps<L>() + wid) * L;
     if (j0 >= njobs) return;
     const int nb = min(L, njobs - j0);
     uint8_t* wsm = dsm + kTablesBytes + (size_t)wid * lane_state_bytes<L>();
@@ -905,10 +910,11 @@ extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, con
 }
 
 template <bool STYLED, int L>
-static j2k_status launch_lanes(j2k_ctx* ctx, unsigned grid, cudaStream_t st, const j2k_cb_desc* descs,
+static j2k_status launch_lanes(j2k_ctx* ctx, cudaStream_t st, const j2k_cb_desc* descs,
                                const uint8_t* bytes, const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
                                int style, const uint32_t* pass_ends, const uint8_t* job_style) {
     constexpr size_t smem = lanes_smem_bytes<L>();
+    const unsigned grid = (unsigned)((njobs + L * cta_warps<L>() - 1) / (L * cta_warps<L>()));
     static std::atomic<uint64_t> attr_set{0};  // devices whose attribute is set, per instantiation
     const uint64_t bit = 1ull << (ctx->device & 63);
     if (!(attr_set.load() & bit)) {
@@ -916,16 +922,17 @@ static j2k_status launch_lanes(j2k_ctx* ctx, unsigned grid, cudaStream_t st, con
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set.fetch_or(bit);
     }
-    t1_decode_lanes_kernel<STYLED, L><<<grid, 32 * (kLaneCtaBlocks / L), smem, st>>>(
+    t1_decode_lanes_kernel<STYLED, L><<<grid, 32 * cta_warps<L>(), smem, st>>>(
         descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, style, pass_ends, job_style);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
 }
 
 template <int L>
-static j2k_status launch_steps(j2k_ctx* ctx, unsigned grid, cudaStream_t st, const j2k_cb_desc* descs,
+static j2k_status launch_steps(j2k_ctx* ctx, cudaStream_t st, const j2k_cb_desc* descs,
                                const uint8_t* bytes, const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff) {
     constexpr size_t smem = lanes_smem_bytes<L>();
+    const unsigned grid = (unsigned)((njobs + L * cta_warps<L>() - 1) / (L * cta_warps<L>()));
     static std::atomic<uint64_t> attr_set{0};
     const uint64_t bit = 1ull << (ctx->device & 63);
     if (!(attr_set.load() & bit)) {
@@ -933,7 +940,7 @@ static j2k_status launch_steps(j2k_ctx* ctx, unsigned grid, cudaStream_t st, con
                                            (int)smem));
         attr_set.fetch_or(bit);
     }
-    t1_decode_steps_kernel<L><<<grid, 32 * (kLaneCtaBlocks / L), smem, st>>>(descs, bytes, d_jobs, (int)njobs, coeff,
+    t1_decode_steps_kernel<L><<<grid, 32 * cta_warps<L>(), smem, st>>>(descs, bytes, d_jobs, (int)njobs, coeff,
                                                                             ctx->d_err);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
@@ -958,22 +965,25 @@ j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint
         J2K_CUDA(ctx, cudaGetLastError());
         return J2K_OK;
     }
-    const unsigned g = (unsigned)((njobs + kLaneCtaBlocks - 1) / kLaneCtaBlocks);
     if (!styled && ctx->t1d_steps) {
         switch (L) {
-        case 8: return launch_steps<8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff);
-        case 16: return launch_steps<16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff);
-        case 32: return launch_steps<32>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff);
+        case 8: return launch_steps<8>(ctx, st, descs, bytes, d_jobs, njobs, coeff);
+        case 16: return launch_steps<16>(ctx, st, descs, bytes, d_jobs, njobs, coeff);
+        case 32: return launch_steps<32>(ctx, st, descs, bytes, d_jobs, njobs, coeff);
         default: break;
         }
     }
     switch ((styled ? 100 : 0) + L) {
-    case 8: return launch_lanes<false, 8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 16: return launch_lanes<false, 16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 32: return launch_lanes<false, 32>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 108: return launch_lanes<true, 8>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 116: return launch_lanes<true, 16>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 132: return launch_lanes<true, 32>(ctx, g, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder: blocks per warp must be 0, 8, 16 or 32");
+    case 2: return launch_lanes<false, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 4: return launch_lanes<false, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 8: return launch_lanes<false, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 16: return launch_lanes<false, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 32: return launch_lanes<false, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 102: return launch_lanes<true, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 104: return launch_lanes<true, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 108: return launch_lanes<true, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 116: return launch_lanes<true, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 132: return launch_lanes<true, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder: blocks per warp must be 0, 2, 4, 8, 16 or 32");
     }
 }
