@@ -74,10 +74,13 @@ enum {
     J2K_TUNE_DWT_TAIL = 9,    /* 1: the forward DWT's deep levels (at most two tiles per resident CTA) run in
                                  one cooperative launch with grid barriers between levels */
     J2K_TUNE_T1D_LANES = 10,  /* tier-1 decoder: code-blocks decoded side by side in one warp, one per lane
-                                 (2, 4, 8 default, 16, 32); 0: one warp per block, lane 0 decoding */
+                                 (2, 4 default, 8, 16, 32); 0: one warp per block, lane 0 decoding */
     J2K_TUNE_T1D_STEPS = 11,  /* 1: with 8, 16 or 32 lanes, unstyled blocks are decoded in a loop of one
                                  symbol per step (one MQ decoding site); 0 (default): in the pass /
                                  stripe / column loops */
+    J2K_TUNE_PLANAR = 12,     /* interleaved-to-planar split of contiguous images: 0 (default) 16 pixels per
+                                 thread stored at the end; 1: stored every 4 pixels; 2: as 1, two groups
+                                 of 16 pixels per thread with all their loads issued first */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of

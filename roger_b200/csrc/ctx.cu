@@ -288,6 +288,11 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->t1d_lanes = value;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_PLANAR) {
+        if (value < 0 || value > 2) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "planar form must be 0, 1 or 2");
+        ctx->planar_form = value;
+        return J2K_OK;
+    }
     if (key == J2K_TUNE_T1D_STEPS) {
         ctx->t1d_steps = value != 0;
         return J2K_OK;
