@@ -79,8 +79,8 @@ enum {
                                  symbol per step (one MQ decoding site); 0 (default): in the pass /
                                  stripe / column loops */
     J2K_TUNE_PLANAR = 12,     /* interleaved-to-planar split of contiguous images: 0 (default) 16 pixels per
-                                 thread stored at the end; 1: stored every 4 pixels; 2: as 1, two groups
-                                 of 16 pixels per thread with all their loads issued first */
+                                 thread; 1 / 2: 4 pixels per thread and step, a warp's stores contiguous,
+                                 4 / 8 steps per thread with all their loads issued first */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of

@@ -101,66 +101,63 @@ __global__ void __launch_bounds__(256) planar_fwd_vec16(const uint8_t* __restric
     }
 }
 
-// The same flat path with G groups of 16 pixels per thread (groups g0 + 256 j of the CTA's
-// 256 G): every group's 16 NC input bytes are requested (16-byte streaming loads) before any is
-// used, so G times as many loads are in flight per thread, and each 4 pixels are transformed and
-// stored at once (one 16-byte streaming store per plane), so few registers hold outputs.
-template <int NC, typename TO, int G>
-__global__ void __launch_bounds__(256) planar_fwd_grp(const uint8_t* __restrict__ in, int mct,
-                                                      TO* __restrict__ planes, size_t stride, size_t ngroups) {
-    const size_t g0 = (size_t)blockIdx.x * (256 * G) + threadIdx.x;
-    uint4 raw[G][NC];
+// The same flat path, 4 pixels per thread and step (their 4 NC bytes are NC aligned 32-bit
+// words): consecutive threads take consecutive 4-pixel groups, so each plane's store of a warp
+// is one contiguous 512-byte run of 16-byte streaming stores, and the loads of a warp cover
+// 128 NC contiguous bytes.  Each thread takes U groups (groups g0 + 256 j of the CTA's 256 U),
+// all of whose words are requested before any is used.
+template <int NC, typename TO, int U>
+__global__ void __launch_bounds__(256) planar_fwd_c4(const uint8_t* __restrict__ in, int mct,
+                                                     TO* __restrict__ planes, size_t stride, size_t ngroups) {
+    const size_t g0 = (size_t)blockIdx.x * (256 * U) + threadIdx.x;
+    const uint32_t* in32 = reinterpret_cast<const uint32_t*>(in);
+    uint32_t raw[U][NC];
 #pragma unroll
-    for (int j = 0; j < G; ++j) {
+    for (int j = 0; j < U; ++j) {
         const size_t g = g0 + (size_t)j * 256;
         if (g < ngroups) {
-            const uint4* src = reinterpret_cast<const uint4*>(in + g * 16 * NC);
 #pragma unroll
-            for (int i = 0; i < NC; ++i) raw[j][i] = __ldcs(src + i);
+            for (int i = 0; i < NC; ++i) raw[j][i] = __ldcs(in32 + g * NC + i);
         }
     }
 #pragma unroll
-    for (int j = 0; j < G; ++j) {
+    for (int j = 0; j < U; ++j) {
         const size_t g = g0 + (size_t)j * 256;
         if (g >= ngroups) break;
         const uint8_t* px = reinterpret_cast<const uint8_t*>(raw[j]);
+        TO o[NC][4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            TO o[NC][4];
+        for (int p = 0; p < 4; ++p) {
+            const uint8_t* q = px + p * NC;
+            bool done = false;
+            if constexpr (NC >= 3) {
+                if (mct == J2K_MCT_RCT) {
+                    const int r = (int)q[0] - 128, gg = (int)q[1] - 128, b = (int)q[2] - 128;
+                    o[0][p] = (TO)((r + 2 * gg + b) >> 2);
+                    o[1][p] = (TO)(b - gg);
+                    o[2][p] = (TO)(r - gg);
 #pragma unroll
-            for (int p = 0; p < 4; ++p) {
-                const uint8_t* q = px + (4 * k + p) * NC;
-                bool done = false;
-                if constexpr (NC >= 3) {
-                    if (mct == J2K_MCT_RCT) {
-                        const int r = (int)q[0] - 128, gg = (int)q[1] - 128, b = (int)q[2] - 128;
-                        o[0][p] = (TO)((r + 2 * gg + b) >> 2);
-                        o[1][p] = (TO)(b - gg);
-                        o[2][p] = (TO)(r - gg);
+                    for (int c = 3; c < NC; ++c) o[c][p] = (TO)((int)q[c] - 128);
+                    done = true;
+                } else if (mct == J2K_MCT_ICT) {
+                    const float r = (float)((int)q[0] - 128), gg = (float)((int)q[1] - 128),
+                                b = (float)((int)q[2] - 128);
+                    o[0][p] = (TO)dot3(YR, r, YG, gg, YB, b);
+                    o[1][p] = (TO)dot3(BR, r, BG, gg, BB, b);
+                    o[2][p] = (TO)dot3(RR, r, RG, gg, RB, b);
 #pragma unroll
-                        for (int c = 3; c < NC; ++c) o[c][p] = (TO)((int)q[c] - 128);
-                        done = true;
-                    } else if (mct == J2K_MCT_ICT) {
-                        const float r = (float)((int)q[0] - 128), gg = (float)((int)q[1] - 128),
-                                    b = (float)((int)q[2] - 128);
-                        o[0][p] = (TO)dot3(YR, r, YG, gg, YB, b);
-                        o[1][p] = (TO)dot3(BR, r, BG, gg, BB, b);
-                        o[2][p] = (TO)dot3(RR, r, RG, gg, RB, b);
-#pragma unroll
-                        for (int c = 3; c < NC; ++c) o[c][p] = (TO)((int)q[c] - 128);
-                        done = true;
-                    }
-                }
-                if (!done) {
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) o[c][p] = (TO)((int)q[c] - 128);
+                    for (int c = 3; c < NC; ++c) o[c][p] = (TO)((int)q[c] - 128);
+                    done = true;
                 }
             }
+            if (!done) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                __stcs(reinterpret_cast<uint4*>(planes + c * stride + g * 16 + 4 * k),
-                       *reinterpret_cast<const uint4*>(o[c]));
+                for (int c = 0; c < NC; ++c) o[c][p] = (TO)((int)q[c] - 128);
+            }
         }
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            __stcs(reinterpret_cast<uint4*>(planes + c * stride + g * 4), *reinterpret_cast<const uint4*>(o[c]));
     }
 }
 
@@ -272,17 +269,18 @@ j2k_status j2k_launch_planar_fwd(j2k_ctx* ctx, const uint8_t* in, size_t in_pitc
                 (ncomp == 1 || ncomp == 3 || ncomp == 4);
     if (flat) {
         size_t groups = n / 16;
-        const int form = ctx->planar_form;  // 0: 16 pixels per thread, stored at the end; 1, 2: G groups
-        const int G = form == 2 ? 2 : 1;
-        unsigned blocks = (unsigned)((groups + 256 * G - 1) / (256 * G));
+        const int form = ctx->planar_form;  // 0: 16 pixels per thread; 1, 2: 4 pixels per step, U = 4 or 8
+        const size_t g4 = n / 4;
+        const int U = form == 2 ? 8 : 4;
+        unsigned blocks = form == 0 ? (unsigned)((groups + 255) / 256) : (unsigned)((g4 + 256 * U - 1) / (256 * U));
 #define PF(NC, T)                                                                                   \
     do {                                                                                            \
         if (form == 0)                                                                              \
             planar_fwd_vec16<NC, T><<<blocks, 256, 0, st>>>(in, mct, (T*)planes, plane_stride, groups); \
         else if (form == 1)                                                                         \
-            planar_fwd_grp<NC, T, 1><<<blocks, 256, 0, st>>>(in, mct, (T*)planes, plane_stride, groups); \
+            planar_fwd_c4<NC, T, 4><<<blocks, 256, 0, st>>>(in, mct, (T*)planes, plane_stride, g4);    \
         else                                                                                        \
-            planar_fwd_grp<NC, T, 2><<<blocks, 256, 0, st>>>(in, mct, (T*)planes, plane_stride, groups); \
+            planar_fwd_c4<NC, T, 8><<<blocks, 256, 0, st>>>(in, mct, (T*)planes, plane_stride, g4);    \
     } while (0)
         if (out_dtype == J2K_I32) {
             if (ncomp == 1) PF(1, int32_t); else if (ncomp == 3) PF(3, int32_t); else PF(4, int32_t);
