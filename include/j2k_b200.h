@@ -78,8 +78,8 @@ enum {
     J2K_TUNE_T1D_STEPS = 11,  /* 1: with 8, 16 or 32 lanes, unstyled blocks are decoded in a loop of one
                                  symbol per step (one MQ decoding site); 0 (default): in the pass /
                                  stripe / column loops */
-    J2K_TUNE_PLANAR = 12,     /* interleaved-to-planar split of contiguous images: 0 (default) 16 pixels per
-                                 thread; 1 / 2: 4 pixels per thread and step, a warp's stores contiguous,
+    J2K_TUNE_PLANAR = 12,     /* interleaved-to-planar split of contiguous images: 0: 16 pixels per thread;
+                                 1 (default) / 2: 4 pixels per thread and step, a warp's stores contiguous,
                                  4 / 8 steps per thread with all their loads issued first */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with

@@ -88,7 +88,7 @@ struct j2k_ctx {
     int dwt_tail = 0;            // forward DWT: deep levels fused into one cooperative launch
     int t1d_lanes = 4;           // tier-1 decoder: code-blocks per warp (2, 4, 8, 16, 32), 0 = one warp per block
     int t1d_steps = 0;           // tier-1 decoder: unstyled blocks by the one-symbol-per-step loop
-    int planar_form = 0;         // planar split: 0 16 pixels per thread, 1 / 2 groups stored every 4 pixels
+    int planar_form = 1;         // planar split: 0 16 pixels per thread; 1 / 2: 4 pixels per thread and step
 };
 
 // scratch slot ids

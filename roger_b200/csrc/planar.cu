@@ -360,9 +360,11 @@ j2k_status j2k_launch_mct_planes(j2k_ctx* ctx, void* planes, int dtype, size_t s
 }
 
 // ---- batched planar split: one launch for many images ------------------------------------------
-// Each CTA converts a chunk of 4096 pixels of one image (256 threads x 16 pixels); chunks of all
-// images are listed in `work` as (image, first pixel).  Full 16-pixel groups use 16-byte loads
-// and stores (image inputs start 16-byte aligned, planes on 16-element boundaries).
+// Each CTA converts a chunk of 4096 pixels of one image; chunks of all images are listed in `work`
+// as (image, first pixel).  A thread takes 4 pixels in each of 4 steps (pixels first + 1024 j +
+// 4 t .. + 3), so each plane's store of a warp is one contiguous run of 16-byte streaming stores
+// and the loads are aligned 32-bit words (image inputs start 16-byte aligned, planes on
+// 16-element boundaries); a last group of fewer than 4 pixels goes pixel by pixel.
 namespace {
 template <typename TO>
 __global__ void __launch_bounds__(256) planar_fwd_batched(const j2k_batch_planar_desc* __restrict__ descs,
@@ -371,56 +373,62 @@ __global__ void __launch_bounds__(256) planar_fwd_batched(const j2k_batch_planar
                                                           TO* __restrict__ plane_base) {
     const uint2 wk = work[blockIdx.x];
     const j2k_batch_planar_desc d = descs[wk.x];
-    const size_t p0 = (size_t)wk.y + (size_t)threadIdx.x * 16;
-    if (p0 >= d.n) return;
     const uint8_t* in = in_base + d.in_off;
     TO* out = plane_base + d.plane_off;
     const int nc = d.ncomp;
-    if (p0 + 16 <= d.n && nc == 3) {
-        uint8_t px[48];
-        const uint4* src = reinterpret_cast<const uint4*>(in + p0 * 3);
+    uint32_t raw[4][3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) *reinterpret_cast<uint4*>(px + 16 * i) = __ldcs(src + i);
-        TO o[3][16];
+    for (int j = 0; j < 4; ++j) {
+        const size_t p = (size_t)wk.y + (size_t)j * 1024 + (size_t)threadIdx.x * 4;
+        if (p + 4 > d.n) continue;
+        if (nc == 3) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(in + p * 3);
 #pragma unroll
-        for (int p = 0; p < 16; ++p) {
-            const uint8_t* q = px + 3 * p;
-            if (d.mct == J2K_MCT_RCT) {
-                int r = (int)q[0] - 128, g = (int)q[1] - 128, b = (int)q[2] - 128;
-                o[0][p] = (TO)((r + 2 * g + b) >> 2);
-                o[1][p] = (TO)(b - g);
-                o[2][p] = (TO)(r - g);
-            } else if (d.mct == J2K_MCT_ICT) {
-                float r = (float)((int)q[0] - 128), g = (float)((int)q[1] - 128), b = (float)((int)q[2] - 128);
-                o[0][p] = (TO)dot3(YR, r, YG, g, YB, b);
-                o[1][p] = (TO)dot3(BR, r, BG, g, BB, b);
-                o[2][p] = (TO)dot3(RR, r, RG, g, RB, b);
-            } else {
+            for (int i = 0; i < 3; ++i) raw[j][i] = __ldcs(src + i);
+        } else if (nc == 1) {
+            raw[j][0] = __ldcs(reinterpret_cast<const uint32_t*>(in + p));
+        }
+    }
 #pragma unroll
-                for (int c = 0; c < 3; ++c) o[c][p] = (TO)((int)q[c] - 128);
+    for (int j = 0; j < 4; ++j) {
+        const size_t p = (size_t)wk.y + (size_t)j * 1024 + (size_t)threadIdx.x * 4;
+        if (p >= d.n) break;
+        if (p + 4 <= d.n && nc == 3) {
+            const uint8_t* px = reinterpret_cast<const uint8_t*>(raw[j]);
+            TO o[3][4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint8_t* q = px + 3 * k;
+                if (d.mct == J2K_MCT_RCT) {
+                    const int r = (int)q[0] - 128, g = (int)q[1] - 128, b = (int)q[2] - 128;
+                    o[0][k] = (TO)((r + 2 * g + b) >> 2);
+                    o[1][k] = (TO)(b - g);
+                    o[2][k] = (TO)(r - g);
+                } else if (d.mct == J2K_MCT_ICT) {
+                    const float r = (float)((int)q[0] - 128), g = (float)((int)q[1] - 128),
+                                b = (float)((int)q[2] - 128);
+                    o[0][k] = (TO)dot3(YR, r, YG, g, YB, b);
+                    o[1][k] = (TO)dot3(BR, r, BG, g, BB, b);
+                    o[2][k] = (TO)dot3(RR, r, RG, g, RB, b);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) o[c][k] = (TO)((int)q[c] - 128);
+                }
             }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                __stcs(reinterpret_cast<uint4*>(out + c * d.stride + p), *reinterpret_cast<const uint4*>(o[c]));
+        } else if (p + 4 <= d.n && nc == 1) {
+            const uint8_t* px = reinterpret_cast<const uint8_t*>(raw[j]);
+            TO o[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) o[k] = (TO)((int)px[k] - 128);
+            __stcs(reinterpret_cast<uint4*>(out + p), *reinterpret_cast<const uint4*>(o));
+        } else {
+            const size_t pe = min(p + 4, d.n);
+            for (size_t q = p; q < pe; ++q) fwd_pixel<TO>(in + q * nc, nc, d.mct, out, q, d.stride);
         }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            uint4* dst = reinterpret_cast<uint4*>(out + c * d.stride + p0);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) __stcs(dst + k, *reinterpret_cast<const uint4*>(&o[c][4 * k]));
-        }
-        return;
     }
-    if (p0 + 16 <= d.n && nc == 1) {
-        uint8_t px[16];
-        *reinterpret_cast<uint4*>(px) = __ldcs(reinterpret_cast<const uint4*>(in + p0));
-        TO o[16];
-#pragma unroll
-        for (int p = 0; p < 16; ++p) o[p] = (TO)((int)px[p] - 128);
-        uint4* dst = reinterpret_cast<uint4*>(out + p0);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) __stcs(dst + k, *reinterpret_cast<const uint4*>(&o[4 * k]));
-        return;
-    }
-    const size_t pe = min(p0 + 16, d.n);
-    for (size_t p = p0; p < pe; ++p) fwd_pixel<TO>(in + p * nc, nc, d.mct, out, p, d.stride);
 }
 }  // namespace
 
