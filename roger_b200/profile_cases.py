@@ -24,6 +24,7 @@ benchmark workloads but stay within a few hundred MB of device memory:
   decode-steps / decode-lanes / decode-warp  the same with the tier-1 decoder forced to one
                symbol per step with 32 blocks per warp, to the pass / stripe / column loops with
                8 blocks per warp, or to one warp per block
+  decode-4096  the decode case on the 4096x4096 RGB image (12288 code-blocks), default decoder
   rate         one lossless 4096x4096 RGB encode cut to 1 bit per pixel by PCRD-opt (tier-1
                rate path, distortion pass, host PCRD and header sizing, descriptor update)
   dwt53-tma    as dwt53, with the TMA-staged level kernel (tuning key J2K_TUNE_DWT_TMA)
@@ -131,8 +132,8 @@ def case_batched():
     return lambda: be.encode(None)
 
 
-def case_decode(lanes=None, steps=None):
-    img = synth.rgb(2048, 2048, (100, 101, 102, 103))
+def case_decode(lanes=None, steps=None, size=2048):
+    img = synth.rgb(size, size, (100, 101, 102, 103))
     enc = C.OCLEncoder(lossy=False)
     enc.run_rgb(img, levels=6, cbw=64, cbh=64)
     d, b = enc.get_codeblocks()
@@ -141,7 +142,7 @@ def case_decode(lanes=None, steps=None):
         C.check(lib().j2k_ctx_set_tuning(dec.ctx.h, 10, lanes), dec.ctx.h)  # J2K_TUNE_T1D_LANES
     if steps is not None:
         C.check(lib().j2k_ctx_set_tuning(dec.ctx.h, 11, steps), dec.ctx.h)  # J2K_TUNE_T1D_STEPS
-    return lambda: dec.run(d, b, 2048, 2048, 3, levels=6)
+    return lambda: dec.run(d, b, size, size, 3, levels=6)
 
 
 def case_rate():
@@ -155,7 +156,7 @@ CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_d
          "diff-kernels": case_diff_kernels, "diff-step": case_diff_step, "batched": case_batched,
          "decode": case_decode,
          "decode-steps": lambda: case_decode(32, 1), "decode-lanes": lambda: case_decode(8, 0),
-         "decode-warp": lambda: case_decode(0, 0), "rate": case_rate, "dwt53-tma": case_dwt53_tma,
+         "decode-warp": lambda: case_decode(0, 0), "decode-4096": lambda: case_decode(size=4096), "rate": case_rate, "dwt53-tma": case_dwt53_tma,
          "dwt53-all-tma": lambda: case_dwt53_tma(6), "encode-styled": case_encode_styled}
 
 
