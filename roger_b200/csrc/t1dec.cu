@@ -321,10 +321,32 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
         // a stripe column's neighbourhood, packed: bits 3r..3r+2 hold columns x-1..x+1 of block row
         // y0-1+r (r = 0..5), from the significance (or sign) rows; stripe row k's 9-bit
         // neighbourhood is then (W >> 3k) & 511 and its own bit 3k+4
-        auto colw = [&](bool negs, int y0, int x) -> uint32_t {
+        auto colw = [&](int y0, int x) -> uint32_t {
             uint32_t w = 0;
-            for (int r = 0; r < 6; ++r) w |= nb3(negs ? S.neg(y0 + r) : S.sig(y0 + r), x) << (3 * r);
+#ifdef __CUDA_ARCH__
+            if (x > 0) {  // bits x-1..x+1 of each row: one funnel shift of its two halves
+                const int s5 = (x - 1) & 31;
+                const bool hiw = x - 1 >= 32;
+                for (int r = 0; r < 6; ++r) {
+                    const uint64_t m = S.sig(y0 + r);
+                    const uint32_t lo = (uint32_t)m, hi = (uint32_t)(m >> 32);
+                    const uint32_t t = hiw ? (hi >> s5) : __funnelshift_r(lo, hi, s5);
+                    w |= (t & 7u) << (3 * r);
+                }
+                return w;
+            }
+#endif
+            for (int r = 0; r < 6; ++r) w |= nb3(S.sig(y0 + r), x) << (3 * r);
             return w;
+        };
+        // the sign bits sign_nbhd reads for stripe row k of column x (left and right in its row,
+        // above and below), from the sign rows as they are now
+        auto negnb = [&](int y0, int x, int k) -> uint32_t {
+            const uint64_t nu = S.neg(y0 + k), no = S.neg(y0 + k + 1), nd = S.neg(y0 + k + 2);
+            const uint32_t l = x > 0 ? (uint32_t)(no >> (x - 1)) & 1u : 0u;
+            const uint32_t r = x < 63 ? (uint32_t)(no >> (x + 1)) & 1u : 0u;
+            return (((uint32_t)(nu >> x) & 1u) << (3 * k + 1)) | (l << (3 * k + 3)) | (r << (3 * k + 5)) |
+                   (((uint32_t)(nd >> x) & 1u) << (3 * k + 7));
         };
         auto add_bit = [&](int x, int y, int p) {
 #ifdef __CUDA_ARCH__
@@ -360,8 +382,7 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                     while (cm) {
                         const int x = ctz64(cm);
                         cm &= cm - 1;
-                        uint32_t W = colw(false, y0, x), NW = 0;
-                        bool nw = false;
+                        uint32_t W = colw(y0, x);
                         for (int k = 0; k < ny; ++k) {
                             if ((W >> (3 * k + 4)) & 1) continue;  // significant already
                             const uint32_t n9 = (W >> (3 * k)) & 511;
@@ -369,12 +390,10 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                             const int bit = dec(zct[n9]);
                             S.vis(y0 + k + 1) |= 1ull << x;
                             if (bit) {
-                                if (!nw) NW = colw(true, y0, x), nw = true;
-                                const int sc = T.sc[n8of(W, NW, k)];
+                                const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                                 const int sg = dsign(sc);
                                 set_sig(x, y0 + k, sg, p);
                                 W |= 1u << (3 * k + 4);
-                                NW |= (uint32_t)sg << (3 * k + 4);
                                 cm |= (2ull << x) & cols;
                             }
                         }
@@ -385,19 +404,30 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                 begin(pass);
                 for (int y0 = 0; y0 < ch; y0 += 4) {
                     const int ny = min(4, ch - y0);
+                    // per stripe row k, as masks over the columns (this pass changes none of
+                    // them): the samples to refine (significant, not visited in this plane), the
+                    // ones refined before (label 16), and the ones with a significant neighbour
+                    // (label 15, else 14)
+                    uint64_t mr[4] = {0, 0, 0, 0}, rf[4] = {0, 0, 0, 0}, nbs[4] = {0, 0, 0, 0};
                     uint64_t rm = 0;
-                    for (int y = y0; y < y0 + ny; ++y) rm |= S.sig(y + 1) & ~S.vis(y + 1);
-                    rm &= cols;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (k >= ny) break;
+                        const uint64_t own = S.sig(y0 + k + 1), v3 = S.sig(y0 + k) | S.sig(y0 + k + 2);
+                        mr[k] = own & ~S.vis(y0 + k + 1) & cols;
+                        rf[k] = S.ref(y0 + k + 1);
+                        nbs[k] = v3 | (v3 << 1) | (v3 >> 1) | (own << 1) | (own >> 1);
+                        rm |= mr[k];
+                    }
                     while (rm) {
                         const int x = ctz64(rm);
                         rm &= rm - 1;
-                        const uint32_t W = colw(false, y0, x);
-                        for (int k = 0; k < ny; ++k) {
-                            const int y = y0 + k;
-                            if (!((W >> (3 * k + 4)) & 1) || ((S.vis(y + 1) >> x) & 1)) continue;
-                            const int lab = ((S.ref(y + 1) >> x) & 1) ? 16 : (((W >> (3 * k)) & 0x1EF) ? 15 : 14);
-                            if (dec(lab)) add_bit(x, y, p);
-                            S.ref(y + 1) |= 1ull << x;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (!((mr[k] >> x) & 1)) continue;
+                            const int lab = ((rf[k] >> x) & 1) ? 16 : (((nbs[k] >> x) & 1) ? 15 : 14);
+                            if (dec(lab)) add_bit(x, y0 + k, p);
+                            S.ref(y0 + k + 1) |= 1ull << x;
                         }
                     }
                 }
@@ -413,8 +443,7 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                 while (um) {
                     const int x = ctz64(um);
                     um &= um - 1;
-                    uint32_t W = colw(false, y0, x), NW = 0, V = 0;
-                    bool nw = false;
+                    uint32_t W = colw(y0, x), V = 0;
                     for (int k = 0; k < ny; ++k) V |= (uint32_t)((S.vis(y0 + k + 1) >> x) & 1) << k;
                     int start = 0;
                     if (ny == 4 && W == 0 && V == 0) {
@@ -427,19 +456,15 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                         const int sg = dsign(sc);
                         set_sig(x, y0 + idx, sg, p);
                         W |= 1u << (3 * idx + 4);
-                        NW = (uint32_t)sg << (3 * idx + 4);  // the only significant sample around
-                        nw = true;
                         start = idx + 1;
                     }
                     for (int k = start; k < ny; ++k) {
                         if (((W >> (3 * k + 4)) & 1) || ((V >> k) & 1)) continue;
                         if (dec(zct[(W >> (3 * k)) & 511])) {
-                            if (!nw) NW = colw(true, y0, x), nw = true;
-                            const int sc = T.sc[n8of(W, NW, k)];
+                            const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                             const int sg = dsign(sc);
                             set_sig(x, y0 + k, sg, p);
                             W |= 1u << (3 * k + 4);
-                            NW |= (uint32_t)sg << (3 * k + 4);
                         }
                     }
                 }
@@ -858,10 +883,11 @@ t1_decode_steps_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
 
 }  // namespace
 
-// Host execution of the device decoder logic for one block (used by the test suite): the
-// one-symbol-per-step loop that the default decoder kernel runs for unstyled blocks.
-extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
-                                        int cw, int ch, int32_t* out, size_t pitch) {
+// Host execution of the device decoder logic for one block (used by the test suite): the pass /
+// stripe / column loops that the default decoder kernel runs in each lane, or (steps != 0) the
+// one-symbol-per-step loop of J2K_TUNE_T1D_STEPS.
+static int decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient, int cw, int ch,
+                             int32_t* out, size_t pitch, bool steps) {
     if (cw < 1 || ch < 1 || cw > 64 || ch > 64 || orient < 0 || orient > 3 || numbps < 0 || numbps > 31 ||
         npasses < 0 || npasses > 3 * numbps || len < 0 || (len > 0 && !data) || !out || pitch < (size_t)cw)
         return -1;  // the checks the kernel makes of a descriptor, and the host buffers
@@ -875,11 +901,24 @@ extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps
     }();
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x) out[(size_t)y * pitch + x] = 0;
-    if (numbps > 0 && npasses > 0) decode_block_steps(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
+    if (numbps > 0 && npasses > 0) {
+        if (steps) decode_block_steps(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
+        else decode_block(S, T, data, len, numbps, npasses, orient, cw, ch, out, pitch);
+    }
     for (int y = 0; y < ch; ++y)
         for (int x = 0; x < cw; ++x)
             if ((S.neg_[y + 1] >> x) & 1) out[(size_t)y * pitch + x] = -out[(size_t)y * pitch + x];
     return 0;
+}
+
+extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
+                                        int cw, int ch, int32_t* out, size_t pitch) {
+    return decode_block_host(data, len, numbps, npasses, orient, cw, ch, out, pitch, false);
+}
+
+extern "C" int j2k_t1_decode_block_steps_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
+                                              int cw, int ch, int32_t* out, size_t pitch) {
+    return decode_block_host(data, len, numbps, npasses, orient, cw, ch, out, pitch, true);
 }
 
 // The same for a block coded with a code-block style, its segments located by pass_ends

@@ -5,7 +5,8 @@
 // the kernel's descriptor check admits (0..3*numbps) and a codeword of random, all-0xFF or
 // sparse bytes held in a buffer of exactly its length, so that any read past the codeword's end
 // is a sanitizer report.  Every other block is decoded as coded in a random code-block style
-// with random pass ends (j2k_t1_decode_block_styled_host).  Prints "decoded N" and exits 0.
+// with random pass ends (j2k_t1_decode_block_styled_host); the others by both unstyled forms,
+// which must give the same output.  Prints "decoded N" and exits 0.
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -14,6 +15,8 @@
 
 extern "C" int j2k_t1_decode_block_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
                                         int cw, int ch, int32_t* out, size_t pitch);
+extern "C" int j2k_t1_decode_block_steps_host(const uint8_t* data, int len, int numbps, int npasses, int orient,
+                                              int cw, int ch, int32_t* out, size_t pitch);
 extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, const uint32_t* pass_ends, int numbps,
                                                int npasses, int orient, int style, int cw, int ch, int32_t* out,
                                                size_t pitch);
@@ -49,10 +52,22 @@ int main(int argc, char** argv) {
                 std::printf("refused styled block %d\n", it);
                 return 1;
             }
-        } else if (j2k_t1_decode_block_host(len ? data.data() : nullptr, len, numbps, npasses, (int)(rng() % 4), cw,
-                                            ch, out.data(), (size_t)cw) != 0) {
-            std::printf("refused block %d\n", it);
-            return 1;
+        } else {
+            // the default per-lane loops and the one-symbol-per-step loop on the same block must
+            // agree, bit for bit, whatever the bytes
+            const int orient = (int)(rng() % 4);
+            std::vector<int32_t> out2((size_t)ch * cw);
+            if (j2k_t1_decode_block_host(len ? data.data() : nullptr, len, numbps, npasses, orient, cw, ch, out.data(),
+                                         (size_t)cw) != 0 ||
+                j2k_t1_decode_block_steps_host(len ? data.data() : nullptr, len, numbps, npasses, orient, cw, ch,
+                                               out2.data(), (size_t)cw) != 0) {
+                std::printf("refused block %d\n", it);
+                return 1;
+            }
+            if (out != out2) {
+                std::printf("decoder forms differ on block %d\n", it);
+                return 1;
+            }
         }
         ++decoded;
     }

@@ -87,15 +87,17 @@ def test_python_mirror_subbands_match_oracle():
         assert np.array_equal(default_steps(w, h, L), O.default_steps(w, h, L))
 
 
+@pytest.mark.parametrize("form", ["j2k_t1_decode_block_host", "j2k_t1_decode_block_steps_host"])
 @pytest.mark.parametrize("cw,ch,orient", [(64, 64, 0), (64, 64, 1), (64, 64, 2), (64, 64, 3), (64, 4, 0),
                                           (64, 1, 3), (33, 17, 1), (8, 64, 2), (1, 1, 0)])
-def test_device_decoder_logic_runs_on_host(cw, ch, orient):
-    """The tier-1 decoder's per-block routine is __host__ __device__; run it on the CPU against
-    oracle-encoded blocks (no kernel launch)."""
+def test_device_decoder_logic_runs_on_host(cw, ch, orient, form):
+    """The tier-1 decoder's per-block routines (the default pass / stripe / column loops and the
+    one-symbol-per-step loop) are __host__ __device__; run them on the CPU against oracle-encoded
+    blocks (no kernel launch)."""
     import ctypes as C
     from oracle import oracle as O
     from roger_b200 import _lib
-    f = C.CDLL(_lib.LIB_PATH).j2k_t1_decode_block_host
+    f = getattr(C.CDLL(_lib.LIB_PATH), form)
     f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
     rng = np.random.default_rng(cw * 7 + ch + orient)
     blk = rng.laplace(0, 25, (ch, cw)).astype(np.int32)
@@ -106,8 +108,9 @@ def test_device_decoder_logic_runs_on_host(cw, ch, orient):
     assert np.array_equal(out, blk)
 
 
+@pytest.mark.parametrize("form", ["j2k_t1_decode_block_host", "j2k_t1_decode_block_steps_host"])
 @pytest.mark.parametrize("cw,ch,orient", [(64, 64, 0), (64, 64, 3), (33, 17, 1), (64, 3, 2), (5, 64, 0)])
-def test_device_decoder_logic_on_truncated_passes(cw, ch, orient):
+def test_device_decoder_logic_on_truncated_passes(cw, ch, orient, form):
     """The same host run of the device decoder on every pass count of oracle-encoded blocks
     (rate-control cuts end a block after any pass), against the oracle's decoder; the oracle puts
     a block cut at a plane end at the middle of its interval, the device routine leaves that to
@@ -115,7 +118,7 @@ def test_device_decoder_logic_on_truncated_passes(cw, ch, orient):
     import ctypes as C
     from oracle import oracle as O
     from roger_b200 import _lib
-    f = C.CDLL(_lib.LIB_PATH).j2k_t1_decode_block_host
+    f = getattr(C.CDLL(_lib.LIB_PATH), form)
     f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
     rng = np.random.default_rng(cw * 11 + ch * 3 + orient)
     blk = (rng.laplace(0, 40, (ch, cw)) * (rng.random((ch, cw)) < 0.7)).astype(np.int32)
