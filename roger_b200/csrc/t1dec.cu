@@ -379,16 +379,19 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                         cm |= ~own & nbm;
                     }
                     cm &= cols;
+                    uint64_t vacc[4] = {0, 0, 0, 0};  // this stripe's visits, stored once at its end
                     while (cm) {
                         const int x = ctz64(cm);
                         cm &= cm - 1;
                         uint32_t W = colw(y0, x);
-                        for (int k = 0; k < ny; ++k) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (k >= ny) break;
                             if ((W >> (3 * k + 4)) & 1) continue;  // significant already
                             const uint32_t n9 = (W >> (3 * k)) & 511;
                             if (!(n9 & 0x1EF)) continue;           // no significant neighbour
                             const int bit = dec(zct[n9]);
-                            S.vis(y0 + k + 1) |= 1ull << x;
+                            vacc[k] |= 1ull << x;
                             if (bit) {
                                 const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                                 const int sg = dsign(sc);
@@ -398,6 +401,9 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                             }
                         }
                     }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k < ny) S.vis(y0 + k + 1) |= vacc[k];
                 }
                 if (++pass >= np) break;
                 // magnitude refinement: significant samples not visited in this plane
@@ -427,9 +433,12 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                             if (!((mr[k] >> x) & 1)) continue;
                             const int lab = ((rf[k] >> x) & 1) ? 16 : (((nbs[k] >> x) & 1) ? 15 : 14);
                             if (dec(lab)) add_bit(x, y0 + k, p);
-                            S.ref(y0 + k + 1) |= 1ull << x;
                         }
                     }
+                    // every sample of mr was refined in this pass
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k < ny) S.ref(y0 + k + 1) = rf[k] | mr[k];
                 }
                 if (++pass >= np) break;
             }
@@ -437,16 +446,25 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
             begin(pass);
             for (int y0 = 0; y0 < ch; y0 += 4) {
                 const int ny = min(4, ch - y0);
+                // per stripe row k: the samples this pass codes (insignificant, not visited in
+                // this plane); a sample that becomes significant here is the one being coded, so
+                // the masks hold for the whole pass
+                uint64_t un[4] = {0, 0, 0, 0};
                 uint64_t um = 0;
-                for (int y = y0; y < y0 + ny; ++y) um |= ~S.sig(y + 1) & ~S.vis(y + 1);
-                um &= cols;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= ny) break;
+                    un[k] = ~S.sig(y0 + k + 1) & ~S.vis(y0 + k + 1) & cols;
+                    um |= un[k];
+                }
                 while (um) {
                     const int x = ctz64(um);
                     um &= um - 1;
-                    uint32_t W = colw(y0, x), V = 0;
-                    for (int k = 0; k < ny; ++k) V |= (uint32_t)((S.vis(y0 + k + 1) >> x) & 1) << k;
+                    uint32_t W = colw(y0, x), U = 0;  // U: rows of the column to code
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) U |= (uint32_t)((un[k] >> x) & 1) << k;
                     int start = 0;
-                    if (ny == 4 && W == 0 && V == 0) {
+                    if (ny == 4 && W == 0 && U == 15) {
                         // run-length mode: four insignificant, unvisited samples, no significant
                         // neighbour (every bit of the column's neighbourhood is zero)
                         if (!dec(17)) continue;
@@ -459,7 +477,7 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                         start = idx + 1;
                     }
                     for (int k = start; k < ny; ++k) {
-                        if (((W >> (3 * k + 4)) & 1) || ((V >> k) & 1)) continue;
+                        if (!((U >> k) & 1)) continue;
                         if (dec(zct[(W >> (3 * k)) & 511])) {
                             const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                             const int sg = dsign(sc);
