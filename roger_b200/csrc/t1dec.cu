@@ -321,24 +321,22 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
         // a stripe column's neighbourhood, packed: bits 3r..3r+2 hold columns x-1..x+1 of block row
         // y0-1+r (r = 0..5), from the significance (or sign) rows; stripe row k's 9-bit
         // neighbourhood is then (W >> 3k) & 511 and its own bit 3k+4
-        // from the stripe's six significance rows R (block rows y0-1 .. y0+4), held in registers
-        auto colw = [&](const uint64_t* R, int x) -> uint32_t {
+        auto colw = [&](int y0, int x) -> uint32_t {
             uint32_t w = 0;
 #ifdef __CUDA_ARCH__
             if (x > 0) {  // bits x-1..x+1 of each row: one funnel shift of its two halves
                 const int s5 = (x - 1) & 31;
                 const bool hiw = x - 1 >= 32;
-#pragma unroll
                 for (int r = 0; r < 6; ++r) {
-                    const uint32_t lo = (uint32_t)R[r], hi = (uint32_t)(R[r] >> 32);
+                    const uint64_t m = S.sig(y0 + r);
+                    const uint32_t lo = (uint32_t)m, hi = (uint32_t)(m >> 32);
                     const uint32_t t = hiw ? (hi >> s5) : __funnelshift_r(lo, hi, s5);
                     w |= (t & 7u) << (3 * r);
                 }
                 return w;
             }
 #endif
-#pragma unroll
-            for (int r = 0; r < 6; ++r) w |= nb3(R[r], x) << (3 * r);
+            for (int r = 0; r < 6; ++r) w |= nb3(S.sig(y0 + r), x) << (3 * r);
             return w;
         };
         // the sign bits sign_nbhd reads for stripe row k of column x (left and right in its row,
@@ -373,23 +371,19 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                 begin(pass);
                 for (int y0 = 0; y0 < ch; y0 += 4) {
                     const int ny = min(4, ch - y0);
-                    uint64_t R[6];  // the stripe's significance rows, kept up to date below
-#pragma unroll
-                    for (int r = 0; r < 6; ++r) R[r] = S.sig(y0 + r);
                     uint64_t cm = 0;
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (k >= ny) break;
-                        uint64_t nbm = R[k] | R[k + 1] | R[k + 2];
+                    for (int y = y0; y < y0 + ny; ++y) {
+                        const uint64_t own = S.sig(y + 1);
+                        uint64_t nbm = S.sig(y) | own | S.sig(y + 2);
                         nbm |= (nbm << 1) | (nbm >> 1);
-                        cm |= ~R[k + 1] & nbm;
+                        cm |= ~own & nbm;
                     }
                     cm &= cols;
                     uint64_t vacc[4] = {0, 0, 0, 0};  // this stripe's visits, stored once at its end
                     while (cm) {
                         const int x = ctz64(cm);
                         cm &= cm - 1;
-                        uint32_t W = colw(R, x);
+                        uint32_t W = colw(y0, x);
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
                             if (k >= ny) break;
@@ -402,7 +396,6 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                                 const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                                 const int sg = dsign(sc);
                                 set_sig(x, y0 + k, sg, p);
-                                R[k + 1] |= 1ull << x;
                                 W |= 1u << (3 * k + 4);
                                 cm |= (2ull << x) & cols;
                             }
@@ -456,21 +449,18 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                 // per stripe row k: the samples this pass codes (insignificant, not visited in
                 // this plane); a sample that becomes significant here is the one being coded, so
                 // the masks hold for the whole pass
-                uint64_t R[6];  // the stripe's significance rows, kept up to date below
-#pragma unroll
-                for (int r = 0; r < 6; ++r) R[r] = S.sig(y0 + r);
                 uint64_t un[4] = {0, 0, 0, 0};
                 uint64_t um = 0;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (k >= ny) break;
-                    un[k] = ~R[k + 1] & ~S.vis(y0 + k + 1) & cols;
+                    un[k] = ~S.sig(y0 + k + 1) & ~S.vis(y0 + k + 1) & cols;
                     um |= un[k];
                 }
                 while (um) {
                     const int x = ctz64(um);
                     um &= um - 1;
-                    uint32_t W = colw(R, x), U = 0;  // U: rows of the column to code
+                    uint32_t W = colw(y0, x), U = 0;  // U: rows of the column to code
 #pragma unroll
                     for (int k = 0; k < 4; ++k) U |= (uint32_t)((un[k] >> x) & 1) << k;
                     int start = 0;
@@ -483,20 +473,15 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                         const int sc = T.sc[0];
                         const int sg = dsign(sc);
                         set_sig(x, y0 + idx, sg, p);
-#pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            if (r == idx) R[r + 1] |= 1ull << x;
                         W |= 1u << (3 * idx + 4);
                         start = idx + 1;
                     }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (k < start || k >= ny || !((U >> k) & 1)) continue;
+                    for (int k = start; k < ny; ++k) {
+                        if (!((U >> k) & 1)) continue;
                         if (dec(zct[(W >> (3 * k)) & 511])) {
                             const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                             const int sg = dsign(sc);
                             set_sig(x, y0 + k, sg, p);
-                            R[k + 1] |= 1ull << x;
                             W |= 1u << (3 * k + 4);
                         }
                     }
