@@ -71,8 +71,11 @@ enum {
                                  by one tensor copy, two stages deep) */
     J2K_TUNE_T1A_CTAS = 8,    /* tier-1 context modelling: resident CTAs per SM its registers are cut for,
                                  2 (default, no spills) or 3 */
-    J2K_TUNE_DWT_TAIL = 9,    /* 1: the forward DWT's deep levels (at most two tiles per resident CTA) run in
-                                 one cooperative launch with grid barriers between levels */
+    J2K_TUNE_DWT_TAIL = 9,    /* the forward DWT's deep levels in one launch.  1: those with at most two tiles
+                                 per resident CTA, one cooperative launch with grid barriers between
+                                 levels; 2, 3, 4, 5: from the first level with at most 96, 32, 96, 320
+                                 tiles per plane, one thread-block cluster of 16, 16, 8, 16 CTAs per
+                                 plane with the cluster barrier between levels.  0 (default): off */
     J2K_TUNE_T1D_LANES = 10,  /* tier-1 decoder: code-blocks decoded side by side in one warp, one per lane
                                  (2, 4 default, 8, 16, 32); 0: one warp per block, lane 0 decoding */
     J2K_TUNE_T1D_STEPS = 11,  /* 1: with 8, 16 or 32 lanes, unstyled blocks are decoded in a loop of one

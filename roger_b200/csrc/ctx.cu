@@ -279,7 +279,8 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         return J2K_OK;
     }
     if (key == J2K_TUNE_DWT_TAIL) {
-        ctx->dwt_tail = value != 0;
+        if (value < 0 || value > 5) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "DWT tail form must be 0..5");
+        ctx->dwt_tail = value;
         return J2K_OK;
     }
     if (key == J2K_TUNE_T1D_LANES) {

@@ -553,6 +553,52 @@ dwt_fwd_tail(const TailPlan plan, void* __restrict__ dst, size_t dpitch, size_t 
     }
 }
 
+// The same deep levels with one thread-block cluster per plane (cluster size = gridDim.x, plane =
+// blockIdx.z): CTA r of a cluster takes tiles r, r + gridDim.x, ... of its plane's level, and the
+// cluster's hardware barrier (arrive.release / wait.acquire at cluster scope, after a fence) sits
+// between levels, so no global counter is spun on.  Every CTA of a cluster runs every level and
+// every barrier (the plan is a kernel parameter and there is no early exit), and the CTAs of a
+// cluster are scheduled together, so each barrier is reached by all of them.
+__device__ __forceinline__ void cluster_barrier_rel_acq() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <int KERN, bool QUANT>
+__global__ void __launch_bounds__(256)
+dwt_fwd_ctail(const TailPlan plan, void* __restrict__ dst, size_t dpitch, size_t dst_z) {
+    using T = typename KT<KERN>::T;
+    __shared__ __align__(16) T s[16][FNX];
+    griddep_launch_dependents();
+    griddep_wait();  // launched as a dependent: the level before has finished and its LL is visible
+    const int tz = blockIdx.z, cs = (int)gridDim.x;
+    for (int li = 0; li < plan.nlev; ++li) {
+        const TailLevel& L = plan.lv[li];
+        const int per = L.tiles_x * L.tiles_y;
+        const T* src = (const T*)L.src + tz * L.src_z;
+        T* lld = (T*)L.lld + tz * L.ll_z;
+        for (int r = (int)blockIdx.x; r < per; r += cs) {
+            const int x0 = (r % L.tiles_x) * FTW, y0 = (r / L.tiles_x) * 16;
+            if (QUANT && L.last)
+                fwd_fast_tile_reg<KERN, int32_t, true, true, 16>(s, src, L.spitch, L.w, L.h, lld, L.llp,
+                                                                 (int32_t*)dst + tz * dst_z, dpitch, L.st, L.vec, x0,
+                                                                 y0);
+            else if (QUANT)
+                fwd_fast_tile_reg<KERN, int32_t, true, false, 16>(s, src, L.spitch, L.w, L.h, lld, L.llp,
+                                                                  (int32_t*)dst + tz * dst_z, dpitch, L.st, L.vec, x0,
+                                                                  y0);
+            else
+                fwd_fast_tile_reg<KERN, T, false, false, 16>(s, src, L.spitch, L.w, L.h, lld, L.llp,
+                                                             (T*)dst + tz * dst_z, dpitch, L.st, L.vec, x0, y0);
+            __syncthreads();  // s is reused by the next tile
+        }
+        if (li + 1 < plan.nlev) {
+            __threadfence();
+            __syncthreads();
+            cluster_barrier_rel_acq();
+        }
+    }
+}
+
 // ---- TMA-staged forward level -----------------------------------------------------------------
 // Persistent CTAs walk the tiles (248 output columns x 16 rows of one plane) in a fixed order.
 // A tile's strip (256 columns x 16 + 2*HV rows, halo included) comes into shared memory by one
@@ -985,7 +1031,15 @@ static j2k_status fwd_tail_launch(j2k_ctx* ctx, int k, int levels, int cw, int c
     }
     const long cap = (long)per_sm * ctx->sm_count;
     const long tiles_k = (long)((cw + FTW - 1) / FTW) * ((chh + 15) / 16) * n;
-    if (tiles_k > 2 * cap) return J2K_OK;  // a full-size level: its own launch
+    // form 1: cooperative launch over the GPU; 2..5: one cluster per plane (size 16, 16, 8, 16)
+    // from the first level with at most 96, 32, 96, 320 tiles per plane
+    const int form = ctx->dwt_tail;
+    static const int kCs[6] = {0, 0, 16, 16, 8, 16}, kThr[6] = {0, 0, 96, 32, 96, 320};
+    if (form >= 2) {
+        if (tiles_k > (long)kThr[form] * n) return J2K_OK;
+    } else if (tiles_k > 2 * cap) {
+        return J2K_OK;  // a full-size level: its own launch
+    }
     TailPlan plan{};
     plan.nz = n;
     int w = cw, h = chh;
@@ -1027,6 +1081,30 @@ static j2k_status fwd_tail_launch(j2k_ctx* ctx, int k, int levels, int cw, int c
         if (last) break;
     }
     if (plan.nlev < 2) return J2K_OK;  // one level gains nothing
+    if (form >= 2) {
+        const int cs = kCs[form];
+        auto kern = quant ? dwt_fwd_ctail<KERN, true> : dwt_fwd_ctail<KERN, false>;
+        if (cs > 8) J2K_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cs, 1, n);
+        cfg.blockDim = dim3(256);
+        cfg.stream = stream;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 2;
+        int clusters = 0;
+        J2K_CUDA(ctx, cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
+        if (clusters < 1) return J2K_OK;  // no room for a cluster of this size: level by level
+        J2K_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, plan, out, out_pitch, out_z));
+        *used = plan.nlev;
+        return J2K_OK;
+    }
     uint32_t* bar = (uint32_t*)j2k_scratch(ctx, SCR_BARRIER, 64);
     if (!bar) return J2K_ERR_OUT_OF_MEMORY;
     J2K_CUDA(ctx, cudaMemsetAsync(bar, 0, 8, stream));

@@ -85,7 +85,7 @@ struct j2k_ctx {
     int t1_seg_factor = 1;       // styled tier-1: pass-segment slot bytes per symbol (grown on overflow)
     int dwt_tma = 0;             // fast forward DWT: strips staged by TMA tensor copies (persistent CTAs)
     int t1a_ctas = 2;            // tier-1 phase A: resident CTAs per SM its registers are cut for (2 or 3)
-    int dwt_tail = 0;            // forward DWT: deep levels fused into one cooperative launch
+    int dwt_tail = 0;            // forward DWT: deep levels in one launch (1 cooperative, 2..5 clusters)
     int t1d_lanes = 4;           // tier-1 decoder: code-blocks per warp (2, 4, 8, 16, 32), 0 = one warp per block
     int t1d_steps = 0;           // tier-1 decoder: unstyled blocks by the one-symbol-per-step loop
     int planar_form = 1;         // planar split: 0 16 pixels per thread; 1 / 2: 4 pixels per thread and step
