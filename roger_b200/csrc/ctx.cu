@@ -284,8 +284,10 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         return J2K_OK;
     }
     if (key == J2K_TUNE_T1D_LANES) {
-        if (value != 0 && value != 2 && value != 4 && value != 8 && value != 16 && value != 32)
-            return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder blocks per warp must be 0, 2, 4, 8, 16 or 32");
+        if (value != 0 && value != 2 && value != 3 && value != 4 && value != 6 && value != 8 && value != 16 &&
+            value != 32)
+            return j2k_fail(ctx, J2K_ERR_INVALID_ARG,
+                            "tier-1 decoder blocks per warp must be 0, 2, 3, 4, 6, 8, 16 or 32");
         ctx->t1d_lanes = value;
         return J2K_OK;
     }

@@ -1032,15 +1032,19 @@ j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint
     }
     switch ((styled ? 100 : 0) + L) {
     case 2: return launch_lanes<false, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 3: return launch_lanes<false, 3>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
     case 4: return launch_lanes<false, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
+    case 6: return launch_lanes<false, 6>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
     case 8: return launch_lanes<false, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
     case 16: return launch_lanes<false, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
     case 32: return launch_lanes<false, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
     case 102: return launch_lanes<true, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 103: return launch_lanes<true, 3>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 106: return launch_lanes<true, 6>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
     case 104: return launch_lanes<true, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
     case 108: return launch_lanes<true, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
     case 116: return launch_lanes<true, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
     case 132: return launch_lanes<true, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder: blocks per warp must be 0, 2, 4, 8, 16 or 32");
+    default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder: blocks per warp must be 0, 2, 3, 4, 6, 8, 16 or 32");
     }
 }
