@@ -73,8 +73,7 @@ __host__ __device__ __forceinline__ int zc_label_calc(int orient, int h, int v, 
 //              (bits 0-2: row above, columns x-1..x+1; 3-5: own row; 6-8: row below; the
 //              sample's own bit 4 is ignored; a significant neighbour is n9 & 0x1EF != 0)
 //   sc[n8]:    sign-coding label | xor bit << 7 for n8 = sigL negL sigR negR sigU negU sigD negD
-//   mq[i]:     Qe | NMPS << 17 | NLPS << 23 | SWITCH << 29 of probability state i (Table C.2): a
-//              context's state word is this entry | MPS << 16, so one load gives all a decision needs
+//   mq[i]:     Qe | NMPS << 16 | NLPS << 22 | SWITCH << 28 of probability state i (Table C.2)
 struct DecTables {
     uint8_t zc[4][512];
     uint8_t sc[256];
@@ -96,8 +95,8 @@ __host__ __device__ inline void fill_tables_entry(DecTables& T, int i) {
         T.sc[i] = (uint8_t)((hc == 0 ? (vc ? 10 : 9) : 12 + vc) | (xr << 7));
     }
     if (i < 47)
-        T.mq[i] = (uint32_t)QE(i) | ((uint32_t)NMPS(i) << 17) | ((uint32_t)NLPS(i) << 23) |
-                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 29);
+        T.mq[i] = (uint32_t)QE(i) | ((uint32_t)NMPS(i) << 16) | ((uint32_t)NLPS(i) << 22) |
+                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
 }
 
 __host__ __device__ __forceinline__ int clz32(uint32_t v) {
@@ -112,12 +111,12 @@ __host__ __device__ __forceinline__ int clz32(uint32_t v) {
 // and 65 are the zero border) and the 19 MQ context states.
 struct DecSmem {
     uint64_t sig_[66], neg_[66], ref_[66], vis_[66];
-    uint32_t st_[19];
+    uint8_t st_[19];
     __host__ __device__ uint64_t& sig(int r) { return sig_[r]; }
     __host__ __device__ uint64_t& neg(int r) { return neg_[r]; }
     __host__ __device__ uint64_t& ref(int r) { return ref_[r]; }
     __host__ __device__ uint64_t& vis(int r) { return vis_[r]; }
-    __host__ __device__ uint32_t& st(int k) { return st_[k]; }
+    __host__ __device__ uint8_t& st(int k) { return st_[k]; }
 };
 
 // The same state for the lanes of a warp that decode L blocks side by side: word (a, r, lane) of
@@ -125,17 +124,17 @@ struct DecSmem {
 template <int L>
 struct LaneState {
     uint64_t* base;
-    uint32_t* stb;
+    uint8_t* stb;
     int lane;
     __device__ uint64_t& sig(int r) { return base[(0 * 66 + r) * L + lane]; }
     __device__ uint64_t& neg(int r) { return base[(1 * 66 + r) * L + lane]; }
     __device__ uint64_t& ref(int r) { return base[(2 * 66 + r) * L + lane]; }
     __device__ uint64_t& vis(int r) { return base[(3 * 66 + r) * L + lane]; }
-    __device__ uint32_t& st(int k) { return stb[k * L + lane]; }
+    __device__ uint8_t& st(int k) { return stb[k * L + lane]; }
 };
 template <int L>
 __host__ __device__ constexpr size_t lane_state_bytes() {  // one warp's share: the masks, then the context states
-    return (size_t)4 * 66 * L * 8 + (((size_t)19 * L * 4 + 15) & ~(size_t)15);
+    return (size_t)4 * 66 * L * 8 + (((size_t)19 * L + 15) & ~(size_t)15);
 }
 
 struct Mqd {
@@ -182,26 +181,39 @@ struct Mqd {
             sh -= k;
         }
     }
-    // one decision with the context whose state word is st (table entry | MPS << 16)
-    __host__ __device__ int decode(uint32_t& st, const uint32_t* mq) {
-        const uint32_t e = st;
+    __host__ __device__ int decode(uint8_t& st, const uint32_t* mq) {
+        const uint32_t sv = st;
+        const uint32_t e = mq[sv >> 1];
         const uint32_t qe = e & 0xFFFF;
-        const int mps = (int)(e >> 16) & 1;
+        const int mps = sv & 1;
         A -= qe;
-        int lps;
+        int D, nm = mps;
+        uint32_t nidx;
         if ((C >> 16) >= qe) {
             C -= qe << 16;
             if (A & 0x8000) return mps;  // MPS, no renormalisation
-            lps = A < qe;                // conditional exchange
+            if (A < qe) {                // conditional exchange: LPS
+                D = 1 - mps;
+                nm ^= (int)(e >> 28);
+                nidx = (e >> 22) & 63;
+            } else {
+                D = mps;
+                nidx = (e >> 16) & 63;
+            }
         } else {
-            lps = !(A < qe);
+            if (A < qe) {  // conditional exchange: MPS
+                D = mps;
+                nidx = (e >> 16) & 63;
+            } else {
+                D = 1 - mps;
+                nm ^= (int)(e >> 28);
+                nidx = (e >> 22) & 63;
+            }
             A = qe;
         }
-        const uint32_t nidx = lps ? (e >> 23) & 63 : (e >> 17) & 63;
-        const uint32_t nm = (uint32_t)mps ^ ((uint32_t)lps & (e >> 29));
-        st = mq[nidx] | (nm << 16);
+        st = (uint8_t)((nidx << 1) | nm);
         renorm();
-        return mps ^ lps;
+        return D;
     }
 };
 
@@ -269,10 +281,10 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
         const uint32_t* mq = T.mq;
 
         auto reset_states = [&]() {
-            for (int k = 0; k < 19; ++k) S.st(k) = mq[0];
-            S.st(0) = mq[4];
-            S.st(17) = mq[3];
-            S.st(18) = mq[46];
+            for (int k = 0; k < 19; ++k) S.st(k) = 0;
+            S.st(0) = 4 << 1;
+            S.st(17) = 3 << 1;
+            S.st(18) = 46 << 1;
         };
         reset_states();
         Mqd m;
@@ -574,7 +586,7 @@ t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     const int nb = min(L, njobs - j0);
     uint8_t* wsm = dsm + kTablesBytes + (size_t)wid * lane_state_bytes<L>();
     uint64_t* base = reinterpret_cast<uint64_t*>(wsm);
-    uint32_t* stb = reinterpret_cast<uint32_t*>(wsm + (size_t)4 * 66 * L * 8);
+    uint8_t* stb = wsm + (size_t)4 * 66 * L * 8;
     j2k_cb_job J{};
     j2k_cb_desc D{};
     bool ok = false;
@@ -654,10 +666,10 @@ __host__ __device__ void decode_block_steps(State& S, const DecTables& tabs, con
     const uint64_t cols = cw >= 64 ? ~0ull : ((1ull << cw) - 1);
     Mqd m;
     if (active) {
-        for (int c = 0; c < 19; ++c) S.st(c) = mq[0];
-        S.st(0) = mq[4];
-        S.st(17) = mq[3];
-        S.st(18) = mq[46];
+        for (int c = 0; c < 19; ++c) S.st(c) = 0;
+        S.st(0) = 4 << 1;
+        S.st(17) = 3 << 1;
+        S.st(18) = 46 << 1;
         m.init(data, len);
     }
     // cursor
@@ -840,7 +852,7 @@ t1_decode_steps_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     const int nb = min(L, njobs - j0);
     uint8_t* wsm = dsm + kTablesBytes + (size_t)wid * lane_state_bytes<L>();
     uint64_t* base = reinterpret_cast<uint64_t*>(wsm);
-    uint32_t* stb = reinterpret_cast<uint32_t*>(wsm + (size_t)4 * 66 * L * 8);
+    uint8_t* stb = wsm + (size_t)4 * 66 * L * 8;
     j2k_cb_job J{};
     j2k_cb_desc D{};
     bool ok = false;
