@@ -41,6 +41,34 @@ def encode_job(job):
     return O.encode_image(img, levels, cb, cb, lossless)
 
 
+def reconstruct_job(desc):
+    """The oracle's decode of a lossy (9/7) mixed-set image, as its encoder codes it (colour
+    transform ICT for RGB, default steps): the quantised indices dequantised at the interval
+    midpoint, the inverse 9/7 and the inverse colour transform -> (H, W[, C]) uint8."""
+    if _ROOT not in sys.path:
+        sys.path.insert(0, _ROOT)
+    import numpy as np
+    from oracle import oracle as O
+    from roger_b200 import synth
+    img = synth.mixed_image(desc)
+    L = desc["levels"]
+    mct = O.MCT_ICT if desc["ncomp"] == 3 else O.MCT_NONE
+    planes = O.planar_fwd(img, mct, as_float=True)
+    st = O.default_steps(desc["w"], desc["h"], L)
+    rec = O.planar_inv(np.stack([O.dwt97_inv(O.dequantize(O.quantize(O.dwt97_fwd(p, L), L, st), L, st), L)
+                                 for p in planes]), mct)
+    return rec if desc["ncomp"] == 3 else rec[:, :, 0]
+
+
+def reconstruct_many(descs, processes=None):
+    """reconstruct_job of every descriptor, in order, on a spawned pool of host processes."""
+    procs = max(1, min(processes or os.cpu_count() or 1, len(descs)))
+    if procs == 1:
+        return [reconstruct_job(d) for d in descs]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(reconstruct_job, descs, chunksize=1)
+
+
 def encode_many(jobs, processes=None):
     """Oracle codestreams of `jobs`, in order, computed on `processes` host processes (default:
     every core)."""

@@ -8,7 +8,8 @@ The other parity tests run at 512x512 and below.  These run the workloads themse
     codestream equal to the oracle's, and the decode equal to the oracle's reconstruction;
   * the 256-image mixed set (log-uniform sizes in [64, 2048], 5/3 and 9/7, gray and RGB, 3-5
     levels, 32x32 and 64x64 code-blocks) through the batched encoder: every image's codestream
-    equal to the oracle's;
+    equal to the oracle's; and through the batched decoder: 5/3 images exact, 9/7 images equal
+    to the oracle's reconstruction;
   * 16 x 1024x1024 float32, 9/7 with 5 levels: forward and inverse bit-identical to the FP32
     oracle, the error per subband against the FP64 oracle, and one rate-distortion step's loss
     and gradients against the FP64 oracle's.
@@ -95,6 +96,22 @@ def test_c4_mixed_set_batched_codestreams_equal_oracle(oracle_streams):
     # the largest and the odd-sized images are in the set
     assert max(max(d["w"], d["h"]) for d in descs) >= 1500
     assert sum(1 for d in descs if d["w"] % 2 or d["h"] % 2) >= 64
+
+
+def test_c4_mixed_set_batched_decode(C, oracle_streams):
+    """The 256 codestreams decoded in one batched call (tier-2 on host threads, one tier-1
+    launch over every block of every image): 5/3 images exactly the input, 9/7 images equal to
+    the oracle's reconstruction (midpoint dequantisation, inverse 9/7, inverse ICT)."""
+    descs = oracle_streams["mixed_descs"]
+    outs = C.decode_codestreams(oracle_streams["mixed"])
+    lossy = [d for d in descs if d["kernel"] == 97]
+    recon = dict(zip((d["index"] for d in lossy), P.reconstruct_many(lossy)))
+    bad = []
+    for d, out in zip(descs, outs):
+        ref = synth.mixed_image(d) if d["kernel"] == 53 else recon[d["index"]]
+        if not np.array_equal(out.reshape(ref.shape), ref):
+            bad.append(d)
+    assert not bad, f"{len(bad)} of {len(descs)} images differ, first {bad[0]}"
 
 
 @pytest.fixture(scope="module")
