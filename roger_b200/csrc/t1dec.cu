@@ -383,15 +383,13 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                     while (cm) {
                         const int x = ctz64(cm);
                         cm &= cm - 1;
-                        uint32_t W = colw(y0, x);
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            if (k >= ny) break;
+                        uint32_t W = colw(y0, x), vb = 0;
+                        for (int k = 0; k < ny; ++k) {  // one decoding site: not unrolled
                             if ((W >> (3 * k + 4)) & 1) continue;  // significant already
                             const uint32_t n9 = (W >> (3 * k)) & 511;
                             if (!(n9 & 0x1EF)) continue;           // no significant neighbour
                             const int bit = dec(zct[n9]);
-                            vacc[k] |= 1ull << x;
+                            vb |= 1u << k;
                             if (bit) {
                                 const int sc = T.sc[n8of(W, negnb(y0, x, k), k)];
                                 const int sg = dsign(sc);
@@ -400,6 +398,8 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                                 cm |= (2ull << x) & cols;
                             }
                         }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) vacc[k] |= (uint64_t)((vb >> k) & 1) << x;
                     }
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
@@ -428,10 +428,17 @@ __host__ __device__ void decode_block(State& S, const DecTables& T, const uint8_
                     while (rm) {
                         const int x = ctz64(rm);
                         rm &= rm - 1;
+                        uint32_t mb = 0, rb = 0, nbb = 0;  // the column's rows, as 4-bit masks
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
-                            if (!((mr[k] >> x) & 1)) continue;
-                            const int lab = ((rf[k] >> x) & 1) ? 16 : (((nbs[k] >> x) & 1) ? 15 : 14);
+                            mb |= (uint32_t)((mr[k] >> x) & 1) << k;
+                            rb |= (uint32_t)((rf[k] >> x) & 1) << k;
+                            nbb |= (uint32_t)((nbs[k] >> x) & 1) << k;
+                        }
+                        while (mb) {  // one decoding site
+                            const int k = ctz64(mb);
+                            mb &= mb - 1;
+                            const int lab = ((rb >> k) & 1) ? 16 : (((nbb >> k) & 1) ? 15 : 14);
                             if (dec(lab)) add_bit(x, y0 + k, p);
                         }
                     }
