@@ -818,8 +818,12 @@ def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
     """One rate-distortion training step of the differentiable 9/7 path on 16 x 1024^2 float32
     images (seeds 200..215, /255): forward DWT, relaxed quantiser, inverse DWT, MSE + 0.01 *
     rate, and the backward through the adjoint kernels, for pixels and 16 log-steps.
-    Compulsory traffic: 4 transforms of N*8*sum_k 4^-k bytes, quantiser forward 8N, loss and
-    its gradient 12N, quantiser backward 12N (N = samples)."""
+    Algorithmic traffic of the fused step (every level of this config runs as band kernels, the
+    quantiser inside them), N samples of 4 bytes, S = N * sum_{k<L} 4^-k, Nl = N * 4^-(L-1):
+    forward with the quantiser (input, y and u of the details, LL): 4 (2.75 S + 0.25 Nl);
+    inverse with y_hat formed on load and the residual: 4 (2.75 S + 0.25 Nl + N);
+    transpose of the inverse with the quantiser backward (reads y and u): 4 (3.5 S + 0.5 Nl);
+    transpose of the forward with the residual term: 4 (2 S + N)."""
     import math
     import numpy as np
     import torch
@@ -864,11 +868,13 @@ def bench_diff97(flush, hbm, n=16, size=1024, levels=5):
         tg.append(s.elapsed_time(e))
     ms_graph = statistics.median(tg)
     N = n * size * size
-    tr = N * 8 * sum(4.0 ** -k for k in range(levels))
-    algo = 4 * tr + 8 * N + 12 * N + 12 * N
-    passes = {"dwt_forward": int(tr), "quantiser_forward": int(8 * N), "dwt_inverse_with_residual": int(tr),
-              "loss_and_gradient": int(12 * N), "dwt_inverse_adjoint": int(tr), "quantiser_backward": int(12 * N),
-              "dwt_forward_adjoint_with_residual": int(tr)}
+    S = N * sum(4.0 ** -k for k in range(levels))
+    Nl = N * 4.0 ** -(levels - 1)
+    passes = {"dwt_forward_with_quantiser": int(4 * (2.75 * S + 0.25 * Nl)),
+              "dwt_inverse_with_residual": int(4 * (2.75 * S + 0.25 * Nl + N)),
+              "dwt_inverse_adjoint_with_quantiser_backward": int(4 * (3.5 * S + 0.5 * Nl)),
+              "dwt_forward_adjoint_with_residual": int(4 * (2 * S + N))}
+    algo = sum(passes.values())
     return {"workload": f"{n} x {size}x{size} float32, 9/7 L={levels}, relaxed quantiser, loss = MSE + 0.01*rate, "
                         "grads wrt pixels and 16 log-steps",
             "ms_per_step": round(ms, 3), "algorithmic_bytes": int(algo), "algorithmic_bytes_per_pass": passes,

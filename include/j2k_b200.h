@@ -84,6 +84,9 @@ enum {
     J2K_TUNE_PLANAR = 12,     /* interleaved-to-planar split of contiguous images: 0: 16 pixels per thread;
                                  1 (default) / 2: 4 pixels per thread and step, a warp's stores contiguous,
                                  4 / 8 steps per thread with all their loads issued first */
+    J2K_TUNE_DWT97_ROWS = 13, /* differentiable 9/7 (j2k_dwt97_*): 1 (default) runs every level whose width is
+                                 a power of two in 64..1024 as bands of 16 full rows (a warp per row in
+                                 registers, no halo columns); 0: the 248 x 16 strip kernels */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of
@@ -407,6 +410,25 @@ j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_
 j2k_status j2k_dwt97_band_sum(j2k_ctx* ctx, const float* partials, int n, int nb, int k, float* out);
 j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float* x, float* d, int n, size_t w,
                                       size_t h, int levels, float* sq_partials);
+/* The fused rate-distortion step of config 3 (no counterpart in the reference) in two calls.
+ * j2k_dwt97_rd_forward: y = DWT(x) with the relaxed quantiser run as each level writes its bands
+ * (y and its noise u written; rate partial sums), then the inverse of y_hat = (y/step + u)*step,
+ * formed as the bands are loaded, with d = IDWT(y_hat) - x and the partial sums of d^2
+ * (j2k_dwt97_residual_partials of them).  rate_partials: n x (3L+1) x j2k_dwt97_rd_parts floats,
+ * laid out (image, band, part); j2k_dwt97_rd_finalize turns both sets into the loss.
+ * j2k_dwt97_rd_backward: for the loss's gradient (*scale) (device pointer, NULL = 1) and
+ * alpha = 2 / (n w h): g_y = dL/dy (the transpose of the inverse with the quantiser backward in
+ * its band writes) and g_x = DWT^T(g_y) - (*scale) alpha d; log-step partial sums in the same
+ * layout, for j2k_dwt97_band_sum.  y, u and d are the forward's outputs.  When every level's width
+ * is a power of two in 64..1024 (J2K_TUNE_DWT97_ROWS on) both run as band kernels; otherwise as
+ * the separate passes above.  y, u, d, g_y, g_x: n*w*h floats each. */
+size_t j2k_dwt97_rd_parts(j2k_ctx* ctx, size_t w, size_t h, int levels);
+j2k_status j2k_dwt97_rd_forward(j2k_ctx* ctx, const float* x, float* y, float* u, float* d, int n, size_t w,
+                                size_t h, int levels, const float* log_steps, uint64_t seed, float* rate_partials,
+                                float* sq_partials);
+j2k_status j2k_dwt97_rd_backward(j2k_ctx* ctx, const float* y, const float* u, const float* d, const float* log_steps,
+                                 float lam, const float* scale, float alpha, float* g_y, float* g_x, int n, size_t w,
+                                 size_t h, int levels, float* ls_partials);
 j2k_status j2k_dwt97_forward_adjoint_residual(j2k_ctx* ctx, const float* g_coef, const float* sub,
                                               const float* scale, float alpha, float* g_img, int n, size_t w,
                                               size_t h, int levels);

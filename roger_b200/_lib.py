@@ -112,6 +112,9 @@ SIGS = {
     "j2k_dwt97_band_sum": (I, [P, P, I, I, I, P]),
     "j2k_dwt97_inverse_residual": (I, [P, P, P, P, I, S, S, I, P]),
     "j2k_dwt97_forward_adjoint_residual": (I, [P, P, P, P, C.c_float, P, I, S, S, I]),
+    "j2k_dwt97_rd_parts": (S, [P, S, S, I]),
+    "j2k_dwt97_rd_forward": (I, [P, P, P, P, P, I, S, S, I, P, C.c_uint64, P, P]),
+    "j2k_dwt97_rd_backward": (I, [P, P, P, P, P, C.c_float, P, C.c_float, P, P, I, S, S, I, P]),
     "j2k_batch_create": (I, [P, P, I, C.POINTER(P)]),
     "j2k_batch_destroy": (I, [P]),
     "j2k_batch_pack": (I, [P, C.POINTER(S)]),

@@ -19,6 +19,7 @@
 // Relaxed quantiser (value domain): t = y/step + u, y_hat = t*step, rate = log2(1+|t|),
 // u ~ U[-1/2, 1/2) from Philox4x32-10 keyed by (seed, image) and counted by the sample's
 // position in its Mallat plane (the oracle draws the same stream).
+#include <atomic>
 #include <cmath>
 
 #include "lift.cuh"
@@ -256,6 +257,8 @@ __device__ __forceinline__ int band_of(int dx, int dy, int L) {
     return 1 + 3 * (L - (m + 1)) + o;
 }
 
+#include "rowband.cuh"
+
 // Relaxed quantiser over whole Mallat planes.  grid (parts, images); CTA p takes rows
 // [p*rows, (p+1)*rows) of its image, thread i the 4-sample groups i, i+256, ... of each row.
 // Noise: one Philox4x32-10 call per group (key seed + image, counter y*ceil(w/4) + x/4), word
@@ -388,6 +391,111 @@ Levels make_levels(int w, int h, int levels) {
     return lv;
 }
 
+// ---- row-band level launches ------------------------------------------------------------------
+static_assert(RB_BH == STH, "the band kernels keep the strip kernels' 16-row partial-sum layout");
+
+bool rb_width_ok(int w) { return w == 64 || w == 128 || w == 256 || w == 512 || w == 1024; }
+bool rb_level_ok(const j2k_ctx* ctx, int w, int h) { return ctx->dwt97_rows && rb_width_ok(w) && h >= 2; }
+// how many levels, finest first, the band kernels take (widths halve, so they are a prefix)
+int rb_levels(const j2k_ctx* ctx, const int* ws, const int* hs, int levels) {
+    int k = 0;
+    while (k < levels && rb_level_ok(ctx, ws[k], hs[k])) ++k;
+    return k;
+}
+
+// Each kernel opts in to its dynamic shared memory once per device (with its static arrays the
+// total can pass 48 KB even when the dynamic part does not).
+template <typename K>
+cudaError_t rb_optin(K* k, size_t smem, std::atomic<uint32_t>& mask, int dev) {
+    const uint32_t bit = 1u << (dev & 31);
+    if (mask.load() & bit) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) mask.fetch_or(bit);
+    return e;
+}
+
+template <int MODE, int SPL, int QB>
+cudaError_t rb_ana_go(j2k_ctx* ctx, int h, int n, bool pdl, const float* in, size_t ip, size_t iz, float* dst,
+                      size_t dp, size_t dz, float* lld, size_t llp, size_t llz, int last, const RbQ& q) {
+    static std::atomic<uint32_t> optin{0};
+    const size_t smem = (size_t)RB_BH * RB<SPL>::W * sizeof(float);
+    const cudaError_t e = rb_optin(rb_ana<MODE, SPL, QB>, smem, optin, ctx->device);
+    if (e != cudaSuccess) return e;
+    const dim3 g((unsigned)((h + RB_BH - 1) / RB_BH), (unsigned)n);
+    return launch_pdl_smem(rb_ana<MODE, SPL, QB>, g, dim3(RB<SPL>::NT), smem, ctx->stream, pdl, in, ip, iz, h, dst,
+                           dp, dz, lld, llp, llz, last, q);
+}
+
+// One analysis-shape level of width w (rb_width_ok) and height h over n images.
+template <int MODE, int QB>
+j2k_status rb_ana_level(j2k_ctx* ctx, int w, int h, int n, bool pdl, const float* in, size_t ip, size_t iz,
+                        float* dst, size_t dp, size_t dz, float* lld, size_t llp, size_t llz, int last,
+                        const RbQ& q) {
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (w) {
+        case 64: e = rb_ana_go<MODE, 2, QB>(ctx, h, n, pdl, in, ip, iz, dst, dp, dz, lld, llp, llz, last, q); break;
+        case 128: e = rb_ana_go<MODE, 4, QB>(ctx, h, n, pdl, in, ip, iz, dst, dp, dz, lld, llp, llz, last, q); break;
+        case 256: e = rb_ana_go<MODE, 8, QB>(ctx, h, n, pdl, in, ip, iz, dst, dp, dz, lld, llp, llz, last, q); break;
+        case 512: e = rb_ana_go<MODE, 16, QB>(ctx, h, n, pdl, in, ip, iz, dst, dp, dz, lld, llp, llz, last, q); break;
+        case 1024: e = rb_ana_go<MODE, 32, QB>(ctx, h, n, pdl, in, ip, iz, dst, dp, dz, lld, llp, llz, last, q); break;
+        default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "band kernels: level width not a power of two in 64..1024");
+    }
+    J2K_CUDA(ctx, e);
+    return J2K_OK;
+}
+
+template <int MODE, int SPL, bool LQ, int EXTRA>
+cudaError_t rb_syn_go(j2k_ctx* ctx, int h, int n, bool pdl, const float* src, size_t sp, size_t sz,
+                      const float* lls, size_t llp, size_t llz, float* out, size_t op, size_t oz,
+                      const SynExtra& ex, const RbQ& q, int deepest) {
+    static std::atomic<uint32_t> optin{0};
+    const size_t smem = (size_t)(RB_BH + 2 * RB_HV) * RB<SPL>::W * sizeof(float);
+    const cudaError_t e = rb_optin(rb_syn<MODE, SPL, LQ, EXTRA>, smem, optin, ctx->device);
+    if (e != cudaSuccess) return e;
+    const dim3 g((unsigned)((h + RB_BH - 1) / RB_BH), (unsigned)n);
+    return launch_pdl_smem(rb_syn<MODE, SPL, LQ, EXTRA>, g, dim3(RB<SPL>::NT), smem, ctx->stream, pdl, src, sp, sz,
+                           lls, llp, llz, h, out, op, oz, ex, q, deepest);
+}
+
+// One synthesis-shape level of width w (rb_width_ok) and height h over n images.
+template <int MODE, bool LQ, int EXTRA>
+j2k_status rb_syn_level(j2k_ctx* ctx, int w, int h, int n, bool pdl, const float* src, size_t sp, size_t sz,
+                        const float* lls, size_t llp, size_t llz, float* out, size_t op, size_t oz,
+                        const SynExtra& ex, const RbQ& q, int deepest) {
+    cudaError_t e = cudaErrorInvalidValue;
+#define RB_SYN(SPL_) rb_syn_go<MODE, SPL_, LQ, EXTRA>(ctx, h, n, pdl, src, sp, sz, lls, llp, llz, out, op, oz, ex, q, deepest)
+    switch (w) {
+        case 64: e = RB_SYN(2); break;
+        case 128: e = RB_SYN(4); break;
+        case 256: e = RB_SYN(8); break;
+        case 512: e = RB_SYN(16); break;
+        case 1024: e = RB_SYN(32); break;
+        default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "band kernels: level width not a power of two in 64..1024");
+    }
+#undef RB_SYN
+    J2K_CUDA(ctx, e);
+    return J2K_OK;
+}
+
+// the quantiser operands of level k (partials, steps and planes as the call needs them)
+RbQ rb_q(const float* log_steps, uint64_t seed, const float* u, const float* y, float lam, const float* gscale,
+         float alpha, float* part, int kp, int levels, int k, size_t w) {
+    RbQ q{};
+    q.log_steps = log_steps;
+    q.seed = seed;
+    q.u = const_cast<float*>(u);
+    q.y = y;
+    q.lam = lam;
+    q.gscale = gscale;
+    q.alpha = alpha;
+    q.part = part;
+    q.kp = kp;
+    q.levels = levels;
+    q.level = k;
+    q.groups = (int)((w + 3) / 4);
+    return q;
+}
+
 j2k_status check_common(j2k_ctx* ctx, const void* a, const void* b, int n, size_t w, size_t h, int levels) {
     if (!ctx) return J2K_ERR_INVALID_ARG;
     if (!a || !b || n <= 0 || n > 65535 || w == 0 || h == 0 || w > 65535 || h > 65535 || levels < 0 ||
@@ -427,7 +535,16 @@ j2k_status fwd_adj_run(j2k_ctx* ctx, const float* g_coef, float* g_img, int n, s
         float* out = k == 0 ? g_img : ((levels - 1 - k) % 2 == 0 ? s0 : s1);
         const size_t op = k == 0 ? w : (size_t)ws[k], oz = k == 0 ? plane : zlev;
         const bool fused = k == 0 && ex;
-        if (ws[k] >= 8 && hs[k] >= 2) {
+        if (rb_level_ok(ctx, ws[k], hs[k])) {
+            const bool pdl = k < levels - 1;  // every launch of the chain but the first
+            const RbQ q = rb_q(nullptr, 0, nullptr, nullptr, 0.0f, nullptr, 1.0f, nullptr, 0, levels, k, w);
+            if (fused)
+                J2K_TRY((rb_syn_level<1, false, 2>(ctx, ws[k], hs[k], n, pdl, g_coef, w, plane, ll, llp, llz, out, op, oz,
+                                                    *ex, q, 0)));
+            else
+                J2K_TRY((rb_syn_level<1, false, 0>(ctx, ws[k], hs[k], n, pdl, g_coef, w, plane, ll, llp, llz, out, op, oz,
+                                                    SynExtra{}, q, 0)));
+        } else if (ws[k] >= 8 && hs[k] >= 2) {
             const int wl = (ws[k] + 1) / 2;
             const int vec = (((uintptr_t)g_coef & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) &&
                             (((uintptr_t)ll & 7) == 0) && ((llp & 1) == 0) && ((llz & 1) == 0) && ((wl & 1) == 0);
@@ -549,6 +666,76 @@ __global__ void __launch_bounds__(256) band_sum_kernel(const float* __restrict__
 
 }  // namespace
 
+namespace {
+
+// Inverse 9/7 of the Mallat planes y with the residual d = IDWT(y) - x fused into level 0, for
+// planes whose finest kr >= 1 levels the band kernels take; the deeper levels, if any, run as one
+// strip-kernel transform of the planes' top-left corner.  lq (kr == levels only): y holds the
+// coefficients with their noise q.u, every band entering as y_hat.  pdl: the first launch is a
+// programmatic dependent too.
+j2k_status inv_residual_rb(j2k_ctx* ctx, const float* y, const float* x, float* d, int n, size_t w, size_t h,
+                           int levels, float* sq_partials, const RbQ* lq, bool pdl) {
+    cudaStream_t st = ctx->stream;
+    const size_t plane = w * h;
+    int ws[20] = {}, hs[20] = {};
+    ws[0] = (int)w;
+    hs[0] = (int)h;
+    for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
+    const int kr = rb_levels(ctx, ws, hs, levels);
+    if (kr < 1 || (lq && kr < levels)) return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "band inverse: level shapes");
+    float *bufA = nullptr, *bufB = nullptr;
+    if (levels > 1) {
+        const size_t z1 = (size_t)ws[1] * hs[1] * (size_t)n * 4 + 64;
+        bufA = (float*)j2k_scratch(ctx, SCR_RES, z1);
+        bufB = (float*)j2k_scratch(ctx, SCR_LL1, z1);
+        if (!bufA || !bufB) return J2K_ERR_OUT_OF_MEMORY;
+    }
+    const float* ll = y;
+    size_t llp = w, llz = plane;
+    if (kr < levels) {
+        // levels kr .. L-1: the top-left ws[kr] x hs[kr] of each plane is their own Mallat plane
+        void* a = j2k_scratch(ctx, SCR_LL0, (size_t)ws[kr + 1] * hs[kr + 1] * (size_t)n * 4 + 64);
+        if (!a) return J2K_ERR_OUT_OF_MEMORY;
+        const size_t zk = (size_t)ws[kr] * hs[kr];
+        J2K_TRY(j2k_dwt_inv_impl(ctx, J2K_W97, J2K_ORDER_T800, y, w, bufA, ws[kr], ws[kr], hs[kr], levels - kr, nullptr,
+                                 a, bufB, j2k_dwt_tile{64, 64}, st, n, plane, zk));
+        ll = bufA;
+        llp = (size_t)ws[kr];
+        llz = zk;
+        pdl = true;
+    }
+    for (int k = kr - 1; k >= 0; --k) {
+        const int deepest = k == levels - 1;
+        RbQ q = lq ? *lq : rb_q(nullptr, 0, nullptr, nullptr, 0.0f, nullptr, 1.0f, nullptr, 0, levels, k, w);
+        q.level = k;
+        if (k == 0) {
+            const SynExtra ex{x, w, plane, nullptr, 1.0f, sq_partials, (int)((w + FTW - 1) / FTW)};
+            if (lq)
+                J2K_TRY((rb_syn_level<0, true, 1>(ctx, ws[0], hs[0], n, pdl, y, w, plane, ll, llp, llz, d, w, plane, ex, q,
+                                                   deepest)));
+            else
+                J2K_TRY((rb_syn_level<0, false, 1>(ctx, ws[0], hs[0], n, pdl, y, w, plane, ll, llp, llz, d, w, plane, ex,
+                                                    q, deepest)));
+        } else {
+            float* out = ll == bufA ? bufB : bufA;
+            const size_t op = (size_t)ws[k], oz = (size_t)ws[k] * hs[k];
+            if (lq)
+                J2K_TRY((rb_syn_level<0, true, 0>(ctx, ws[k], hs[k], n, pdl, y, w, plane, ll, llp, llz, out, op, oz,
+                                                   SynExtra{}, q, deepest)));
+            else
+                J2K_TRY((rb_syn_level<0, false, 0>(ctx, ws[k], hs[k], n, pdl, y, w, plane, ll, llp, llz, out, op, oz,
+                                                    SynExtra{}, q, deepest)));
+            ll = out;
+            llp = op;
+            llz = oz;
+        }
+        pdl = true;
+    }
+    return J2K_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 j2k_status j2k_dwt97_rd_finalize(j2k_ctx* ctx, const float* rate_partials, size_t nrate, const float* sq_partials,
@@ -621,7 +808,10 @@ j2k_status j2k_dwt97_inverse_adjoint(j2k_ctx* ctx, const float* g_img, float* g_
         const bool last = k == levels - 1;
         float* ll = last ? g_coef : (k % 2 == 0 ? s0 : s1);
         const size_t llp = last ? w : (size_t)ws[k + 1], llz = last ? plane : zlev;
-        if (ws[k] >= 8 && hs[k] >= 2) {
+        if (rb_level_ok(ctx, ws[k], hs[k])) {
+            const RbQ q = rb_q(nullptr, 0, nullptr, nullptr, 0.0f, nullptr, 1.0f, nullptr, 0, levels, k, w);
+            J2K_TRY((rb_ana_level<2, 0>(ctx, ws[k], hs[k], n, k > 0, in, ip, iz, g_coef, w, plane, ll, llp, llz, 0, q)));
+        } else if (ws[k] >= 8 && hs[k] >= 2) {
             const int vin = (((uintptr_t)in & 15) == 0) && ((ip & 3) == 0) && ((iz & 3) == 0);
             const int vout = (((uintptr_t)g_coef & 7) == 0) && ((w & 1) == 0) && ((plane & 1) == 0) &&
                              (((uintptr_t)ll & 7) == 0) && ((llp & 1) == 0) && ((llz & 1) == 0);
@@ -662,6 +852,14 @@ j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float*
         J2K_CUDA(ctx, cudaGetLastError());
         return J2K_OK;
     }
+    {
+        int ws[20] = {}, hs[20] = {};
+        ws[0] = (int)w;
+        hs[0] = (int)h;
+        for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
+        if (rb_levels(ctx, ws, hs, levels) >= 1)
+            return inv_residual_rb(ctx, y, x, d, n, w, h, levels, sq_partials, nullptr, false);
+    }
     // levels L..2 reconstruct LL_1 (the top-left ceil(w/2) x ceil(h/2) of each Mallat plane is
     // itself the Mallat plane of LL_1's (L-1)-level transform) into scratch; level 1 runs fused
     const size_t w1 = (w + 1) / 2, h1 = (h + 1) / 2;
@@ -688,6 +886,116 @@ j2k_status j2k_dwt97_inverse_residual(j2k_ctx* ctx, const float* y, const float*
                              (int)w, (int)h, d, w, Steps4{}, ZStride{plane, plane, llz}, vec, ex));
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
+    J2K_API_END
+}
+
+// The fused step runs when the band kernels take every level.
+static bool rd_fused(const j2k_ctx* ctx, size_t w, size_t h, int levels, int* ws, int* hs) {
+    ws[0] = (int)w;
+    hs[0] = (int)h;
+    for (int k = 1; k <= levels; ++k) { ws[k] = (ws[k - 1] + 1) / 2; hs[k] = (hs[k - 1] + 1) / 2; }
+    return levels >= 1 && rb_levels(ctx, ws, hs, levels) == levels;
+}
+
+size_t j2k_dwt97_rd_parts(j2k_ctx* ctx, size_t w, size_t h, int levels) {
+    if (!ctx || w == 0 || h == 0 || w > 65535 || h > 65535 || levels < 0 || levels > 16) return 0;
+    int ws[20] = {}, hs[20] = {};
+    if (rd_fused(ctx, w, h, levels, ws, hs)) return (h + RB_BH - 1) / RB_BH;
+    return h < 64 ? h : 64;  // the quantiser kernels' row ranges
+}
+
+j2k_status j2k_dwt97_rd_forward(j2k_ctx* ctx, const float* x, float* y, float* u, float* d, int n, size_t w,
+                                size_t h, int levels, const float* log_steps, uint64_t seed, float* rate_partials,
+                                float* sq_partials) {
+    J2K_API_BEGIN
+    J2K_TRY(check_common(ctx, x, y, n, w, h, levels));
+    if (!u || !d || !log_steps || !rate_partials || !sq_partials)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "rd forward: NULL noise, residual, log steps or partials");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t plane = w * h;
+    const int nb = 3 * levels + 1;
+    int ws[20] = {}, hs[20] = {};
+    const int kp = (int)j2k_dwt97_rd_parts(ctx, w, h, levels);
+    if (!rd_fused(ctx, w, h, levels, ws, hs)) {
+        // the separate passes: forward DWT, quantiser keeping its noise (y_hat in scratch), inverse
+        // with the residual
+        float* yh = (float*)j2k_scratch(ctx, SCR_PLANE, plane * (size_t)n * 4 + 64);
+        if (!yh) return J2K_ERR_OUT_OF_MEMORY;
+        J2K_TRY(j2k_dwt_forward_batch(ctx, J2K_W97, J2K_ORDER_T800, x, w, plane, y, w, plane, n, w, h, levels, nullptr));
+        J2K_TRY(quant_run(ctx, false, y, nullptr, yh, n, w, h, levels, log_steps, seed, 0.0f, nullptr, 1.0f,
+                          rate_partials, kp, u));
+        return j2k_dwt97_inverse_residual(ctx, yh, x, d, n, w, h, levels, sq_partials);
+    }
+    // forward levels with the quantiser in their band writes (y and u; rate partials), every
+    // level after the first a programmatic dependent of the one before
+    J2K_CUDA(ctx, cudaMemsetAsync(rate_partials, 0, (size_t)n * nb * kp * sizeof(float), st));
+    const size_t zlev = (size_t)ws[1] * hs[1];
+    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, zlev * n * 4 + 64);
+    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, zlev * n * 4 + 64);
+    if (!s0 || !s1) return J2K_ERR_OUT_OF_MEMORY;
+    const float* in = x;
+    size_t ip = w, iz = plane;
+    for (int k = 0; k < levels; ++k) {
+        const int last = k == levels - 1;
+        float* lld = last ? y : (k % 2 == 0 ? s0 : s1);
+        const size_t llp = last ? w : (size_t)ws[k + 1], llz = last ? plane : zlev;
+        const RbQ q = rb_q(log_steps, seed, u, nullptr, 0.0f, nullptr, 1.0f, rate_partials, kp, levels, k, w);
+        J2K_TRY((rb_ana_level<3, 1>(ctx, ws[k], hs[k], n, k > 0, in, ip, iz, y, w, plane, lld, llp, llz, last, q)));
+        in = lld;
+        ip = llp;
+        iz = llz;
+    }
+    // inverse of y_hat = (y / step + u) * step, formed as the bands are loaded, residual at level 0
+    const RbQ q = rb_q(log_steps, seed, u, nullptr, 0.0f, nullptr, 1.0f, nullptr, 0, levels, 0, w);
+    return inv_residual_rb(ctx, y, x, d, n, w, h, levels, sq_partials, &q, true);
+    J2K_API_END
+}
+
+j2k_status j2k_dwt97_rd_backward(j2k_ctx* ctx, const float* y, const float* u, const float* d, const float* log_steps,
+                                 float lam, const float* scale, float alpha, float* g_y, float* g_x, int n, size_t w,
+                                 size_t h, int levels, float* ls_partials) {
+    J2K_API_BEGIN
+    J2K_TRY(check_common(ctx, y, g_x, n, w, h, levels));
+    if (!u || !d || !log_steps || !g_y || !ls_partials)
+        return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "rd backward: NULL noise, residual, log steps or buffers");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const size_t plane = w * h;
+    const int nb = 3 * levels + 1;
+    int ws[20] = {}, hs[20] = {};
+    const int kp = (int)j2k_dwt97_rd_parts(ctx, w, h, levels);
+    const SynExtra ex{d, w, plane, scale, alpha, nullptr, 0};
+    if (!rd_fused(ctx, w, h, levels, ws, hs)) {
+        // the separate passes: inverse adjoint of d (into scratch), quantiser backward into g_y,
+        // forward adjoint with the residual term
+        float* gr = (float*)j2k_scratch(ctx, SCR_PLANE, plane * (size_t)n * 4 + 64);
+        if (!gr) return J2K_ERR_OUT_OF_MEMORY;
+        J2K_TRY(j2k_dwt97_inverse_adjoint(ctx, d, gr, n, w, h, levels));
+        J2K_TRY(quant_run(ctx, true, y, gr, g_y, n, w, h, levels, log_steps, 0, lam, scale, alpha, ls_partials, kp,
+                          const_cast<float*>(u)));
+        return fwd_adj_run(ctx, g_y, g_x, n, w, h, levels, &ex);
+    }
+    // transpose of the inverse, level by level, with the quantiser backward in the band writes
+    J2K_CUDA(ctx, cudaMemsetAsync(ls_partials, 0, (size_t)n * nb * kp * sizeof(float), st));
+    const size_t zlev = (size_t)ws[1] * hs[1];
+    float* s0 = (float*)j2k_scratch(ctx, SCR_LL0, zlev * n * 4 + 64);
+    float* s1 = (float*)j2k_scratch(ctx, SCR_LL1, zlev * n * 4 + 64);
+    if (!s0 || !s1) return J2K_ERR_OUT_OF_MEMORY;
+    const float* in = d;
+    size_t ip = w, iz = plane;
+    for (int k = 0; k < levels; ++k) {
+        const int last = k == levels - 1;
+        float* lld = last ? g_y : (k % 2 == 0 ? s0 : s1);
+        const size_t llp = last ? w : (size_t)ws[k + 1], llz = last ? plane : zlev;
+        const RbQ q = rb_q(log_steps, 0, u, y, lam, scale, alpha, ls_partials, kp, levels, k, w);
+        J2K_TRY((rb_ana_level<2, 2>(ctx, ws[k], hs[k], n, k > 0, in, ip, iz, g_y, w, plane, lld, llp, llz, last, q)));
+        in = lld;
+        ip = llp;
+        iz = llz;
+    }
+    // transpose of the forward, with the -scale * alpha * d term at level 0
+    return fwd_adj_run(ctx, g_y, g_x, n, w, h, levels, &ex);
     J2K_API_END
 }
 

@@ -277,6 +277,7 @@ struct SynExtra {
     const float* scale;
     float alpha;
     float* part;
+    int part_stride;  // row-band kernels: slots per CTA (the sum, then zeros; 0 counts as 1)
 };
 
 template <int KERN, int MODE, typename TS, bool DEQ, bool DEQLL, int EXTRA>

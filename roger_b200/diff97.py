@@ -9,8 +9,11 @@ device memory and the stream; every pass runs in libj2kb200's kernels.  The fuse
 planes per image for its backward: the quantiser input y, its noise u (so the backward does not
 regenerate it) and the residual d = IDWT(y_hat) - x (the reconstruction itself is never stored;
 the residual pass is fused into the last inverse level, and the "- 2/N d" term of the pixel
-gradient into the last forward-adjoint level).  The backward reads its output gradient on the
-device, so a step never synchronises with the host.
+gradient into the last forward-adjoint level).  Where every level's width is a power of two in
+64..1024, the quantiser runs inside the transforms: its forward as the forward levels write their
+bands, y_hat as the inverse loads them (never stored), its backward as the transpose of the
+inverse writes its bands.  The backward reads its output gradient on the device, so a step never
+synchronises with the host.
 """
 import ctypes as C
 
@@ -191,50 +194,46 @@ class RelaxedQuant(torch.autograd.Function):
 
 
 def _rd_forward(x, log_steps, levels, lam, seed):
-    """The forward of the fused loss: y = DWT(x), the quantiser keeping its noise u, the residual
-    d = IDWT(y_hat) - x fused into the last inverse level, and the loss scalar from the partial
-    sums.  Returns (loss, y, d, u)."""
+    """The forward of the fused loss (j2k_dwt97_rd_forward): y = DWT(x) with the quantiser's
+    noise u drawn as each level writes its bands, the residual d = IDWT(y_hat) - x with y_hat
+    formed as the inverse loads the bands, and the loss scalar from the partial sums.  Returns
+    (loss, y, d, u)."""
     x = x.detach().contiguous()
-    y = dwt97(x, levels)
-    c, h = _ctx(y)
-    n, hh, ww = y.shape
-    nb, k = 3 * levels + 1, _parts(hh)
+    c, h = _ctx(x)
+    n, hh, ww = x.shape
+    nb, kp = 3 * levels + 1, lib().j2k_dwt97_rd_parts(h, ww, hh, levels)
     ls = log_steps.detach().float().contiguous()
-    yh, u = torch.empty_like(y), torch.empty_like(y)
-    rparts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
-    check(lib().j2k_relaxed_quant_forward_noise(h, _p(y), _p(yh), _p(u), n, ww, hh, levels, _p(ls), seed,
-                                                _p(rparts), k), h)
-    d = torch.empty_like(y)
-    sparts = torch.empty(lib().j2k_dwt97_residual_partials(ww, hh, n), device=y.device, dtype=torch.float32)
-    check(lib().j2k_dwt97_inverse_residual(h, _p(yh), _p(x), _p(d), n, ww, hh, levels, _p(sparts)), h)
-    del yh
+    y, u, d = torch.empty_like(x), torch.empty_like(x), torch.empty_like(x)
+    rparts = torch.empty(n * nb * kp, device=x.device, dtype=torch.float32)
+    sparts = torch.empty(lib().j2k_dwt97_residual_partials(ww, hh, n), device=x.device, dtype=torch.float32)
+    check(lib().j2k_dwt97_rd_forward(h, _p(x), _p(y), _p(u), _p(d), n, ww, hh, levels, _p(ls), seed, _p(rparts),
+                                     _p(sparts)), h)
     # the loss scalar from both sets of partial sums, in one launch
-    loss = torch.empty((), device=y.device, dtype=torch.float32)
+    loss = torch.empty((), device=x.device, dtype=torch.float32)
     check(lib().j2k_dwt97_rd_finalize(h, _p(rparts), rparts.numel(), _p(sparts), sparts.numel(),
                                       1.0 / x.numel(), float(lam), _p(loss)), h)
     return loss, y, d, u
 
 
 def _rd_backward(y, d, u, log_steps, g, levels, lam, seed):
-    """The backward of the fused loss for output gradient g (0-dim, read on the device): inverse
-    adjoint of the residual, quantiser backward (scaled by 2/N and g), per-band log-step
-    gradient in one launch, forward adjoint with the -2/N residual fused in.  Returns (dL/dx,
-    dL/dlog_steps)."""
+    """The backward of the fused loss for output gradient g (0-dim, read on the device),
+    j2k_dwt97_rd_backward: the transpose of the inverse applied to the residual with the
+    quantiser backward (scaled by 2/N and g) in its band writes, then the transpose of the
+    forward with the -2/N residual term; the per-band log-step gradient in one launch.
+    Returns (dL/dx, dL/dlog_steps)."""
+    del seed  # the backward reads the forward's noise u
     g = g.detach().float().contiguous()
-    alpha = 2.0 / d.numel()
-    g_res = idwt97_adjoint(d, levels)
     c, h = _ctx(y)
     n, hh, ww = y.shape
-    nb, k = 3 * levels + 1, _parts(hh)
+    nb, kp = 3 * levels + 1, lib().j2k_dwt97_rd_parts(h, ww, hh, levels)
     ls = log_steps.detach().float().contiguous()
-    g_y = torch.empty_like(y)
-    parts = torch.empty(n * nb * k, device=y.device, dtype=torch.float32)
-    check(lib().j2k_relaxed_quant_backward_scaled(h, _p(y), _p(g_res), _p(g_y), n, ww, hh, levels, _p(ls), seed,
-                                                  _p(u), float(lam), _p(g), float(alpha), _p(parts), k), h)
-    del g_res
+    g_y, gx = torch.empty_like(y), torch.empty_like(y)
+    parts = torch.empty(n * nb * kp, device=y.device, dtype=torch.float32)
+    check(lib().j2k_dwt97_rd_backward(h, _p(y), _p(u), _p(d), _p(ls), float(lam), _p(g), 2.0 / d.numel(), _p(g_y),
+                                      _p(gx), n, ww, hh, levels, _p(parts)), h)
+    del g_y
     g_ls = torch.empty(nb, device=y.device, dtype=torch.float32)  # per band, in one launch
-    check(lib().j2k_dwt97_band_sum(h, _p(parts), n, nb, k, _p(g_ls)), h)
-    gx = forward_adjoint_residual(g_y, d, levels, scale=g, alpha=alpha)
+    check(lib().j2k_dwt97_band_sum(h, _p(parts), n, nb, kp, _p(g_ls)), h)
     return gx, g_ls
 
 

@@ -230,3 +230,68 @@ def test_checkpointed_step_matches_stored_step_and_fd64(D):
         lm[b] -= h
         fd = (O.rd_loss(x, L, lp, lam, seed, False) - O.rd_loss(x, L, lm, lam, seed, False)) / (2 * h)
         assert abs(gl[b] - fd) <= GRAD_TOL * max(abs(fd), 1e-3)
+
+
+# ---- band kernels (levels 64..1024 wide as full-row bands) against the strip kernels ----------
+
+def _rows(on):
+    """Switch the default context between the band kernels (on) and the strip kernels."""
+    from roger_b200._lib import lib
+    from roger_b200.codec import default_context
+    assert lib().j2k_ctx_set_tuning(default_context(0).h, 13, 1 if on else 0) == 0
+
+
+def _both(fn):
+    _rows(False)
+    try:
+        a = fn()
+    finally:
+        _rows(True)
+    return a, fn()
+
+
+BAND_SHAPES = [(2, 1024, 64, 5), (2, 512, 96, 4), (1, 256, 37, 3), (3, 64, 40, 1), (1, 128, 2, 1),
+               (1, 1024, 80, 6), (2, 256, 256, 3)]
+
+
+@pytest.mark.parametrize("n,w,h,L", BAND_SHAPES)
+def test_band_kernels_bit_identical_to_strip_kernels(D, n, w, h, L):
+    """Both adjoints and the inverse with its residual, per level through the band kernels where
+    the level width allows (1024 x 80 at L=6: the 32-wide level runs as a strip-kernel
+    sub-transform), equal the strip kernels bit for bit; the residual's partial sums add up to
+    the same total."""
+    g = torch.from_numpy(np.random.default_rng(w + h + L).normal(size=(n, h, w)).astype(np.float32)).cuda()
+    x = torch.from_numpy(np.random.default_rng(7 * w + h).normal(size=(n, h, w)).astype(np.float32)).cuda()
+    fa0, fa1 = _both(lambda: D.dwt97_adjoint(g, L))
+    ia0, ia1 = _both(lambda: D.idwt97_adjoint(g, L))
+    assert torch.equal(fa0, fa1)
+    assert torch.equal(ia0, ia1)
+    (d0, s0), (d1, s1) = _both(lambda: D.inverse_residual(g, x, L))
+    assert torch.equal(d0, d1)
+    assert abs(s0.item() - s1.item()) <= 1e-5 * abs(s0.item())
+    gsc = torch.tensor(1.7, device="cuda")
+    r0, r1 = _both(lambda: D.forward_adjoint_residual(g, x, L, scale=gsc, alpha=0.3))
+    assert torch.equal(r0, r1)
+
+
+@pytest.mark.parametrize("n,w,h,L", [(2, 1024, 64, 5), (1, 512, 50, 4), (2, 128, 128, 2), (1, 64, 64, 1),
+                                     (1, 1024, 80, 6)])
+def test_fused_rd_step_matches_separate_passes(D, n, w, h, L):
+    """The fused step (quantiser inside the band kernels) against the separate passes of the strip
+    kernels: y, u, d and dL/dx bit for bit (the same operations per sample), the loss and the
+    log-step gradient to 1e-5 (their partial sums are added in another order)."""
+    lam, seed = 0.01, 11
+    x = torch.from_numpy(np.stack([synth.gray(w, h, 300 + i) for i in range(n)]).astype(np.float32) / 255).cuda()
+    ls = torch.full((3 * L + 1,), math.log(1 / 64.0), device="cuda")
+    ls += torch.linspace(-0.3, 0.3, 3 * L + 1, device="cuda")
+
+    def step():
+        loss, y, d, u = D._rd_forward(x, ls, L, lam, seed)
+        gx, gl = D._rd_backward(y, d, u, ls, torch.tensor(1.5, device="cuda"), L, lam, seed)
+        return [t.clone() for t in (loss, y, d, u, gx, gl)]
+
+    a, b = _both(step)
+    for i in (1, 2, 3, 4):
+        assert torch.equal(a[i], b[i]), i
+    assert abs(a[0].item() - b[0].item()) <= 1e-5 * abs(a[0].item())
+    assert torch.allclose(a[5], b[5], rtol=1e-5, atol=1e-7 * a[5].abs().max().item())
