@@ -268,7 +268,7 @@ constexpr int RB_BH = 16;  // rows per band
 // positions in dst, its LL to lld (last: lld is dst itself and the LL is a band of the plane,
 // which the QB epilogue then covers too).  Dynamic shared memory: BH rows of W floats.
 template <int MODE, int SPL, int QB>
-__global__ void __launch_bounds__(RB<SPL>::NT, (QB == 2 && SPL >= 16) ? 2 : 3)
+__global__ void __launch_bounds__(RB<SPL>::NT, SPL >= 32 ? (QB == 2 ? 2 : 3) : (SPL == 16 ? (QB == 2 ? 2 : 3) : 4))
 rb_ana(const float* __restrict__ in, size_t ipitch, size_t iz, int h, float* __restrict__ dst, size_t dpitch,
        size_t dz, float* __restrict__ lld, size_t llpitch, size_t llz, int last, RbQ q) {
     using G = RB<SPL>;
@@ -410,7 +410,7 @@ rb_ana(const float* __restrict__ in, size_t ipitch, size_t iz, int h, float* __r
 // of out^2 to ex.part[image * bands + band]; 2 out = result - (*scale) * alpha * sub.
 // Dynamic shared memory: BH + 8 rows of W floats.
 template <int MODE, int SPL, bool LQ, int EXTRA>
-__global__ void __launch_bounds__(RB<SPL>::NT, 2)
+__global__ void __launch_bounds__(RB<SPL>::NT, SPL >= 32 ? 2 : (SPL == 16 ? 3 : 4))
 rb_syn(const float* __restrict__ src, size_t spitch, size_t sz, const float* __restrict__ lls, size_t llpitch,
        size_t llz, int h, float* __restrict__ out, size_t opitch, size_t oz, SynExtra ex, RbQ q, int deepest) {
     using G = RB<SPL>;
