@@ -77,6 +77,11 @@ def test_invalid_arguments_are_rejected_without_a_device():
     assert L.j2k_codeblock_count(64, 64, 3, 3, 64) == 0     # not a power of two
     assert L.j2k_codeblock_count(64, 64, 3, 128, 64) == 0   # too wide
     assert L.j2k_ctx_destroy(None) == -1
+    # the fused rate-distortion step: no context, no partial slots and no launch
+    assert L.j2k_dwt97_rd_parts(None, 1024, 1024, 5) == 0
+    assert L.j2k_dwt97_rd_forward(None, None, None, None, None, 1, 64, 64, 1, None, 0, None, None) == -1
+    assert L.j2k_dwt97_rd_backward(None, None, None, None, None, 0.0, None, 1.0, None, None, 1, 64, 64, 1,
+                                   None) == -1
 
 
 def test_python_mirror_subbands_match_oracle():
