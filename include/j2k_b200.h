@@ -87,6 +87,9 @@ enum {
     J2K_TUNE_DWT97_ROWS = 13, /* differentiable 9/7 (j2k_dwt97_*): 1 (default) runs every level whose width is
                                  a power of two in 64..1024 as bands of 16 full rows (a warp per row in
                                  registers, no halo columns); 0: the 248 x 16 strip kernels */
+    J2K_TUNE_T1D_ORDER = 14,  /* tier-1 decoder with blocks side by side in a warp: 1 (default) gives the
+                                 warps their blocks sorted by codeword length, longest first (the blocks
+                                 of a warp then take about as long); 0: list order */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of

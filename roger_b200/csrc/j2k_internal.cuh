@@ -59,7 +59,7 @@ enum : uint32_t {
     J2K_DEVERR_SEG_CAPACITY = 6,  // a coding-pass segment outgrew its slot (code-block styles)
 };
 
-constexpr int J2K_SCRATCH_SLOTS = 13;
+constexpr int J2K_SCRATCH_SLOTS = 14;
 
 constexpr int J2K_MQ_TIERS = 4;
 
@@ -90,12 +90,13 @@ struct j2k_ctx {
     int t1d_steps = 0;           // tier-1 decoder: unstyled blocks by the one-symbol-per-step loop
     int planar_form = 1;         // planar split: 0 16 pixels per thread; 1 / 2: 4 pixels per thread and step
     int dwt97_rows = 1;          // differentiable 9/7: levels 64..1024 wide (powers of two) as full-row bands
+    int t1d_order = 1;           // tier-1 decoder: blocks to lanes by codeword length, longest first
 };
 
 // scratch slot ids
 enum { SCR_LL0 = 0, SCR_LL1 = 1, SCR_JOBS = 2, SCR_SYMS = 3, SCR_T1STATE = 4, SCR_MISC = 5,
        SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8, SCR_UNITS = 9, SCR_SEGS = 10, SCR_BARRIER = 11,
-       SCR_PLANE = 12 };
+       SCR_PLANE = 12, SCR_DECORD = 13 };
 
 j2k_status j2k_fail(j2k_ctx* ctx, j2k_status s, const std::string& msg);
 j2k_status j2k_cuda_check(j2k_ctx* ctx, cudaError_t e, const char* what);

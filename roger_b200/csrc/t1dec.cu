@@ -13,6 +13,8 @@
 // The older form, one warp per block with lane 0 decoding, stays as a tuning choice.
 #include <atomic>
 
+#include <cub/cub.cuh>
+
 #include "j2k_internal.cuh"
 
 namespace {
@@ -573,8 +575,9 @@ __host__ __device__ constexpr size_t lanes_smem_bytes() {
     return kTablesBytes + (size_t)cta_warps<L>() * lane_state_bytes<L>();
 }
 
-// One code-block per lane: a CTA takes 32 consecutive jobs in 32 / L warps of L (lanes 0..L-1 of
-// a warp decode, one block each); every lane of the warp helps clear its blocks' regions first
+// One code-block per lane: a CTA takes 32 consecutive jobs (of `order` when given: the jobs
+// sorted by codeword length, longest first, so that the blocks sharing a warp take about as long
+// and the longest start first) in 32 / L warps of L (lanes 0..L-1 of a warp decode, one block each); every lane of the warp helps clear its blocks' regions first
 // and apply the signs at the end.  Dynamic shared memory: the tables, then each warp's
 // LaneState<L> area.
 template <bool STYLED, int L>
@@ -582,7 +585,7 @@ __global__ void __launch_bounds__(32 * cta_warps<L>())
 t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __restrict__ bytes,
                        const j2k_cb_job* __restrict__ jobs, int njobs, int32_t* __restrict__ coeff,
                        uint32_t* __restrict__ err, int style, const uint32_t* __restrict__ pass_ends,
-                       const uint8_t* __restrict__ job_style) {
+                       const uint8_t* __restrict__ job_style, const uint32_t* __restrict__ order) {
     extern __shared__ __align__(16) uint8_t dsm[];
     DecTables& tabs = *reinterpret_cast<DecTables*>(dsm);
     for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) fill_tables_entry(tabs, i);
@@ -597,9 +600,11 @@ t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     j2k_cb_job J{};
     j2k_cb_desc D{};
     bool ok = false;
+    // this lane's job: position j0 + lane of the order (longest codewords first), or of the list
+    const int jid = lane < nb ? (order ? (int)order[j0 + lane] : j0 + lane) : 0;
     if (lane < nb) {
-        J = jobs[j0 + lane];
-        D = descs[j0 + lane];
+        J = jobs[jid];
+        D = descs[jid];
         ok = dec_job_ok(J, D, STYLED);
         if (!ok) atomicCAS(err, 0u, (uint32_t)J2K_DEVERR_BAD_JOB);
     }
@@ -617,8 +622,8 @@ t1_decode_lanes_kernel(const j2k_cb_desc* __restrict__ descs, const uint8_t* __r
     if (ok && D.numbps > 0 && D.npasses > 0) {
         LaneState<L> S{base, stb, lane};
         decode_block<STYLED, true>(S, tabs, bytes + D.offset, D.length, D.numbps, D.npasses, J.orient, J.cw, J.ch,
-                                   coeff + J.off, J.pitch, job_style ? (int)job_style[j0 + lane] : style,
-                                   STYLED ? pass_ends + (size_t)(j0 + lane) * J2K_PASS_STRIDE : nullptr);
+                                   coeff + J.off, J.pitch, job_style ? (int)job_style[jid] : style,
+                                   STYLED ? pass_ends + (size_t)jid * J2K_PASS_STRIDE : nullptr);
     }
     __syncwarp();
     const int32_t my_half = ok ? cut_half(D.numbps, D.npasses) : 0;
@@ -976,7 +981,8 @@ extern "C" int j2k_t1_decode_block_styled_host(const uint8_t* data, int len, con
 template <bool STYLED, int L>
 static j2k_status launch_lanes(j2k_ctx* ctx, cudaStream_t st, const j2k_cb_desc* descs,
                                const uint8_t* bytes, const j2k_cb_job* d_jobs, size_t njobs, int32_t* coeff,
-                               int style, const uint32_t* pass_ends, const uint8_t* job_style) {
+                               int style, const uint32_t* pass_ends, const uint8_t* job_style,
+                               const uint32_t* order) {
     constexpr size_t smem = lanes_smem_bytes<L>();
     const unsigned grid = (unsigned)((njobs + L * cta_warps<L>() - 1) / (L * cta_warps<L>()));
     static std::atomic<uint64_t> attr_set{0};  // devices whose attribute is set, per instantiation
@@ -987,9 +993,40 @@ static j2k_status launch_lanes(j2k_ctx* ctx, cudaStream_t st, const j2k_cb_desc*
         attr_set.fetch_or(bit);
     }
     t1_decode_lanes_kernel<STYLED, L><<<grid, 32 * cta_warps<L>(), smem, st>>>(
-        descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, style, pass_ends, job_style);
+        descs, bytes, d_jobs, (int)njobs, coeff, ctx->d_err, style, pass_ends, job_style, order);
     J2K_CUDA(ctx, cudaGetLastError());
     return J2K_OK;
+}
+
+// keys[i] = codeword length of job i, ids[i] = i
+__global__ void t1d_order_keys(const j2k_cb_desc* __restrict__ descs, int n, uint32_t* __restrict__ keys,
+                               uint32_t* __restrict__ ids) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t len = descs[i].length;
+    keys[i] = len > 0 ? (uint32_t)len : 0u;
+    ids[i] = (uint32_t)i;
+}
+
+// The jobs sorted by codeword length, longest first (a stable radix sort: equal lengths keep
+// their list order), in scratch; nullptr with the error set when scratch runs out.
+static const uint32_t* decode_order(j2k_ctx* ctx, cudaStream_t st, const j2k_cb_desc* descs, size_t njobs) {
+    const int n = (int)njobs;
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (const uint32_t*)nullptr, (uint32_t*)nullptr, n, 0, 32, st);
+    const size_t words = 4 * njobs + 64;
+    uint32_t* w = (uint32_t*)j2k_scratch(ctx, SCR_DECORD, words * 4 + tmp + 64);
+    if (!w) return nullptr;
+    uint32_t *keys_in = w, *keys_out = w + njobs, *ids_in = w + 2 * njobs, *ids_out = w + 3 * njobs;
+    void* temp = w + words;
+    t1d_order_keys<<<(unsigned)((njobs + 255) / 256), 256, 0, st>>>(descs, n, keys_in, ids_in);
+    if (j2k_cuda_check(ctx, cudaGetLastError(), "decode order keys") != J2K_OK) return nullptr;
+    if (j2k_cuda_check(ctx, cub::DeviceRadixSort::SortPairsDescending(temp, tmp, keys_in, keys_out, ids_in, ids_out,
+                                                                      n, 0, 32, st),
+                       "decode order sort") != J2K_OK)
+        return nullptr;
+    return ids_out;
 }
 
 template <int L>
@@ -1037,21 +1074,26 @@ j2k_status j2k_t1_decode_jobs(j2k_ctx* ctx, const j2k_cb_desc* descs, const uint
         default: break;
         }
     }
+    const uint32_t* ord = nullptr;
+    if (ctx->t1d_order && njobs > (size_t)L) {
+        ord = decode_order(ctx, st, descs, njobs);
+        if (!ord) return J2K_ERR_OUT_OF_MEMORY;
+    }
     switch ((styled ? 100 : 0) + L) {
-    case 2: return launch_lanes<false, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 3: return launch_lanes<false, 3>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 4: return launch_lanes<false, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 6: return launch_lanes<false, 6>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 8: return launch_lanes<false, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 16: return launch_lanes<false, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 32: return launch_lanes<false, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr);
-    case 102: return launch_lanes<true, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 103: return launch_lanes<true, 3>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 106: return launch_lanes<true, 6>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 104: return launch_lanes<true, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 108: return launch_lanes<true, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 116: return launch_lanes<true, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
-    case 132: return launch_lanes<true, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style);
+    case 2: return launch_lanes<false, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 3: return launch_lanes<false, 3>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 4: return launch_lanes<false, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 6: return launch_lanes<false, 6>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 8: return launch_lanes<false, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 16: return launch_lanes<false, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 32: return launch_lanes<false, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, 0, nullptr, nullptr, ord);
+    case 102: return launch_lanes<true, 2>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
+    case 103: return launch_lanes<true, 3>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
+    case 106: return launch_lanes<true, 6>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
+    case 104: return launch_lanes<true, 4>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
+    case 108: return launch_lanes<true, 8>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
+    case 116: return launch_lanes<true, 16>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
+    case 132: return launch_lanes<true, 32>(ctx, st, descs, bytes, d_jobs, njobs, coeff, style, pass_ends, job_style, ord);
     default: return j2k_fail(ctx, J2K_ERR_INVALID_ARG, "tier-1 decoder: blocks per warp must be 0, 2, 3, 4, 6, 8, 16 or 32");
     }
 }

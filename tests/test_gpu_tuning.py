@@ -44,3 +44,27 @@ def test_encoder_autotune_keeps_the_result():
     assert len(cut) <= 12000
     enc.autotune(reps=1)
     assert bytes(enc.codestream()) == cut
+
+
+@pytest.mark.parametrize("lanes", [2, 4, 8, 32])
+def test_decoder_block_order_gives_the_same_image(lanes):
+    """The tier-1 decoder's block-to-lane order (longest codewords first, J2K_TUNE_T1D_ORDER 1, or
+    list order, 0) decodes every block the same: lossless round trips stay exact and the lossy
+    decode is identical either way, unstyled and with the bypass / reset / per-pass styles."""
+    img = synth.rgb(520, 300, (81, 82, 83, 84))
+    for lossy, style in ((False, 0), (True, 0), (False, 7)):
+        enc = C.OCLEncoder(ctx=C.Context(0), lossy=lossy)
+        enc.run_rgb(img, levels=4, cbw=32, cbh=32, cblk_style=style)
+        d, b = enc.get_codeblocks()
+        pe = enc.get_pass_ends() if style else None
+        outs = []
+        for order in (0, 1):
+            ctx = C.Context(0)
+            assert lib().j2k_ctx_set_tuning(ctx.h, 10, lanes) == 0
+            assert lib().j2k_ctx_set_tuning(ctx.h, 14, order) == 0
+            dec = C.OCLDecoder(ctx=ctx, lossy=lossy)
+            kw = {"cblk_style": style, "pass_ends": pe} if style else {}
+            outs.append(np.array(dec.run(np.array(d), np.array(b), 520, 300, 3, levels=4, cbw=32, cbh=32, **kw)))
+        assert np.array_equal(outs[0], outs[1])
+        if not lossy:
+            assert np.array_equal(outs[1], img)
