@@ -200,15 +200,19 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                 if (!anyk) continue;  // no candidate has a significant neighbour: nothing coded
                 N[0] = N[5] = 0;
                 N[1] = N[2] = N[3] = N[4] = 0;
-                for (bool changed = true; changed;) {
-                    changed = false;
+                if ((M[0] | M[1] | M[2] | M[3]) != 0) {  // else no sample becomes significant
+                    // Sweeps top to bottom (each row from the row above as just computed); a row's
+                    // fill is stable unless the row below, computed after it, seeds one of its
+                    // samples outside the runs already filled (row 3's lower neighbour is the next
+                    // stripe, not yet coded: always zero).  The fixpoint is the least one either way.
+                    do {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        MT seeds = M[j] & (E[j] | ((N[j] | N[j + 2]) << 1) | N[j]);
-                        MT nn = M[j] & (MT)(~(MT)(M[j] + seeds) | seeds);
-                        changed |= nn != N[j + 1];
-                        N[j + 1] = nn;
-                    }
+                        for (int j = 0; j < 4; ++j) {
+                            MT seeds = M[j] & (E[j] | ((N[j] | N[j + 2]) << 1) | N[j]);
+                            N[j + 1] = M[j] & (MT)(~(MT)(M[j] + seeds) | seeds);
+                        }
+                    } while (((M[0] & (MT)(N[2] << 1) & ~N[1]) | (M[1] & (MT)(N[3] << 1) & ~N[2]) |
+                              (M[2] & (MT)(N[4] << 1) & ~N[3])) != 0);
                 }
 #pragma unroll
                 for (int j = 0; j < 4; ++j) K[j] = C[j] & (E[j] | ((N[j] | N[j + 1] | N[j + 2]) << 1) | N[j]);
