@@ -194,10 +194,11 @@ def _profile_values(name, keys):
     return got if len(got) == len(keys) else None
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) of one launch of the level-0 5/3 kernel over the three 4096x4096
-    planes, from the ncu capture of that launch; None when the summary is absent."""
-    v = _profile_values("dwt_fwd_fast_53_level0_3x4096.txt", ["dram_bytes_per_launch"])
+def profiled_traffic(name="dwt_fwd_fast_53_level0_3x4096.txt"):
+    """DRAM bytes (read + write) of one launch of a level-0 5/3 kernel on the 4096x4096 RGB image
+    (by default the one over the three planes), from the ncu capture of that launch; None when the
+    summary is absent."""
+    v = _profile_values(name, ["dram_bytes_per_launch"])
     return v["dram_bytes_per_launch"] if v else None
 
 
@@ -575,7 +576,8 @@ def bench_per_image(be, descs, imgs, flush, ms_batched, mpix):
 def bench_c1(flush, hbm, peak_src, clocks):
     """The reference's own workload size: one 4096x4096 RGB lossless encode (RCT + 5/3 L=6 +
     tier-1, 64x64 code-blocks), resident and end to end, with its stages; the level-0 DWT launch
-    over the three planes is the HBM roofline kernel."""
+    over the three planes is the HBM roofline kernel.  Beside it, the encoder's other front end:
+    the first DWT level reading the interleaved pixels itself (J2K_TUNE_DWT_PX)."""
     import numpy as np
     import torch
     from roger_b200 import codec as C
@@ -619,10 +621,20 @@ def bench_c1(flush, hbm, peak_src, clocks):
     t_planar = ev_time(lambda i: C.rgb_to_planar(imgs4[i % 4], 1), inner=8)
     t_dwt_l0 = ev_time(lambda i: C.dwt_forward(planes, 1, out=coef), inner=8)
     t_dwt = ev_time(lambda i: C.dwt_forward(planes, C1_LEVELS, out=coef), inner=4)
+    # the other front end: the DWT from the pixels (coefficients only, no tier-1)
+    from roger_b200._lib import lib
+    ctx_px = C.Context(0)
+    lib().j2k_ctx_set_tuning(ctx_px.h, 15, 1)
+    enc_px = C.OCLEncoder(ctx=ctx_px, lossy=False, output_dwt=True)
+    t_px_l0 = ev_time(lambda i: enc_px.run_rgb(imgs4[i % 4], levels=1), inner=8)
+    t_px = ev_time(lambda i: enc_px.run_rgb(imgs4[i % 4], levels=C1_LEVELS), inner=4)
     n = size * size
     lvl_bytes = sum(n * 8 * 4.0 ** -k for k in range(C1_LEVELS)) * 3
     l0_bytes = 3 * n * 8
+    px_l0_bytes = 3 * n + 3 * n * 4  # RGB bytes in, three int32 planes of subbands out
+    px_bytes = px_l0_bytes + sum(n * 8 * 4.0 ** -k for k in range(1, C1_LEVELS)) * 3
     achieved = l0_bytes / (t_dwt_l0 * 1e-3) / 1e9
+    px_gbs = px_l0_bytes / (t_px_l0 * 1e-3) / 1e9
     descs = res[0]
     samples = int((descs["cw"].astype(np.int64) * descs["ch"] *
                    np.maximum(3 * descs["numbps"].astype(np.int64) - 2, 0)).sum())
@@ -642,6 +654,15 @@ def bench_c1(flush, hbm, peak_src, clocks):
                   "workload": "the c1 section's image (4096x4096 RGB, RCT planes)"},
         stages_ms={"planar_rct": round(t_planar, 4), "dwt_all_levels_3comp": round(t_dwt, 4),
                    "dwt_level0_3comp": round(t_dwt_l0, 4), "tier1_all_blocks_derived": round(t1_ms, 4)},
+        dwt_from_pixels={"note": "J2K_TUNE_DWT_PX 1: level 0 reads the RGB pixels (level shift and RCT inside its "
+                                 "loads), the int32 planes are never written; same coefficients, off by default",
+                         "kernel": "dwt_fwd_fast_px<53, 3, RCT> (one launch, a CTA per tile and component)",
+                         "level0_ms": round(t_px_l0, 4), "all_levels_ms": round(t_px, 4),
+                         "planar_path_front_ms": round(t_planar + t_dwt, 4),
+                         "algorithmic_bytes_level0": px_l0_bytes, "level0_gbs": round(px_gbs, 1),
+                         "level0_frac": round(px_gbs / hbm, 4),
+                         "all_levels_gbs": round(px_bytes / (t_px * 1e-3) / 1e9, 1),
+                         "level0_traffic": profiled_traffic("dwt_fwd_fast_px_53_rgb_4096.txt")},
         dwt_all_levels_gbs=round(lvl_bytes / (t_dwt * 1e-3) / 1e9, 1),
         dwt_all_levels_frac=round(lvl_bytes / (t_dwt * 1e-3) / 1e9 / hbm, 4),
         planar_gbs=round(n * 15 / (t_planar * 1e-3) / 1e9, 1),

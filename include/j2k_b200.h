@@ -90,6 +90,12 @@ enum {
     J2K_TUNE_T1D_ORDER = 14,  /* tier-1 decoder with blocks side by side in a warp: 1 (default) gives the
                                  warps their blocks sorted by codeword length, longest first (the blocks
                                  of a warp then take about as long); 0: list order */
+    J2K_TUNE_DWT_PX = 15,     /* encoder of interleaved 8-bit pixels (j2k_encoder_run_interleaved), 1 or 3
+                                 components, T.800 order: 1 runs the level shift and colour transform
+                                 inside the first DWT level's loads, so the component planes are never
+                                 written (a third of the DRAM bytes, but more instructions in a level
+                                 kernel that is issue-bound: slower on B200); 0 (default): a planar
+                                 split first, then the DWT of the planes.  Same coefficients either way */
     J2K_TUNE_MQ_TIER = 6      /* MQ kernel schedule: value = tier << 24 | lanes << 20 | warps.  The
                                  blocks, longest first, go to up to 4 tiers of `warps` warps with
                                  `lanes` blocks each (lanes 0 ends the list), then to warps of

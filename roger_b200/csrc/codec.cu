@@ -285,6 +285,45 @@ static j2k_status encode_planes(j2k_encoder* e) {
     return run_tier1(e);
 }
 
+// The first DWT level reads the interleaved pixels itself (the level shift and colour transform
+// inside its loads) when J2K_TUNE_DWT_PX asks for it and the level takes the register-lifting tile
+// in the T.800 order.
+static bool pixels_to_dwt(const j2k_encoder* e) {
+    const j2k_ctx* ctx = e->ctx;
+    const int order = e->lossy ? J2K_ORDER_T800 : e->order;
+    return ctx->dwt_px && order == J2K_ORDER_T800 && e->levels >= 1 && ctx->dwt_fast_th == 16 && ctx->dwt_reg &&
+           !ctx->dwt_tma && !ctx->dwt_pipe &&
+           j2k_dwt_fwd_px_ok(e->lossy ? J2K_W97 : J2K_W53, e->ncomp, e->mct, e->w, e->h);
+}
+
+// Encode from device pixels: level 0 of every component straight from the pixels (their LL
+// bands to a scratch buffer), then the remaining levels of all components in one call with the
+// components side by side (gridDim.z), then tier-1.  The same coefficients as the planar split
+// followed by encode_planes.
+static j2k_status encode_pixels(j2k_encoder* e, const uint8_t* px, size_t pitch) {
+    j2k_ctx* ctx = e->ctx;
+    const size_t n = e->w * e->h;
+    const int nc = e->ncomp;
+    const bool quant = e->lossy && !e->dwt_only;
+    const int kern = e->lossy ? J2K_W97 : J2K_W53;
+    J2K_TRY(e->coef.ensure(ctx, n * 4 * nc));
+    const size_t w1 = (e->w + 1) / 2, h1 = (e->h + 1) / 2, w2 = (w1 + 1) / 2, h2 = (h1 + 1) / 2;
+    const size_t w3 = (w2 + 1) / 2, h3 = (h2 + 1) / 2;
+    void* llpx = j2k_scratch(ctx, SCR_LLPX, w1 * h1 * 4 * nc);
+    void* ll0 = j2k_scratch(ctx, SCR_LL0, w2 * h2 * 4 * nc);
+    void* ll1 = j2k_scratch(ctx, SCR_LL1, w3 * h3 * 4 * nc);
+    if (!llpx || !ll0 || !ll1) return J2K_ERR_OUT_OF_MEMORY;
+    const float* steps = quant ? e->steps.data() : nullptr;
+    J2K_TRY(j2k_dwt_fwd_px_launch(ctx, kern, nc, e->mct, px, pitch, e->w, e->h, e->levels, steps, llpx, w1, w1 * h1,
+                                  e->coef.p, e->w, n, ctx->stream));
+    if (e->levels > 1)
+        J2K_TRY(j2k_dwt_fwd_impl(ctx, kern, J2K_ORDER_T800, llpx, w1, e->coef.p, e->w, w1, h1, e->levels - 1, steps,
+                                 ll0, ll1, j2k_dwt_tile{64, 64}, ctx->stream, nc, w1 * h1, n));
+    e->have_result = true;
+    if (e->dwt_only) return J2K_OK;
+    return run_tier1(e);
+}
+
 // Tier-1 of every code-block of the current coefficients (and rate control when asked for).
 static j2k_status run_tier1(j2k_encoder* e) {
     j2k_ctx* ctx = e->ctx;
@@ -516,6 +555,7 @@ j2k_status j2k_encoder_run_interleaved(j2k_encoder* e, const uint8_t* pixels, in
         J2K_CUDA(ctx, cudaMemcpyAsync(e->in.p, pixels, pitch * h, cudaMemcpyHostToDevice, ctx->stream));
         src = (const uint8_t*)e->in.p;
     }
+    if (pixels_to_dwt(e)) return encode_pixels(e, src, pitch);
     J2K_TRY(j2k_launch_planar_fwd(ctx, src, pitch, ncomp, e->mct, e->lossy ? J2K_F32 : J2K_I32, e->planes.p,
                                   w, w * h, w, h, ctx->stream));
     return encode_planes(e);

@@ -296,6 +296,10 @@ j2k_status j2k_ctx_set_tuning(j2k_ctx* ctx, int key, int value) {
         ctx->planar_form = value;
         return J2K_OK;
     }
+    if (key == J2K_TUNE_DWT_PX) {
+        ctx->dwt_px = value != 0;
+        return J2K_OK;
+    }
     if (key == J2K_TUNE_T1D_ORDER) {
         ctx->t1d_order = value != 0;
         return J2K_OK;

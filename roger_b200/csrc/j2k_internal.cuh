@@ -59,7 +59,7 @@ enum : uint32_t {
     J2K_DEVERR_SEG_CAPACITY = 6,  // a coding-pass segment outgrew its slot (code-block styles)
 };
 
-constexpr int J2K_SCRATCH_SLOTS = 14;
+constexpr int J2K_SCRATCH_SLOTS = 15;
 
 constexpr int J2K_MQ_TIERS = 4;
 
@@ -91,12 +91,13 @@ struct j2k_ctx {
     int planar_form = 1;         // planar split: 0 16 pixels per thread; 1 / 2: 4 pixels per thread and step
     int dwt97_rows = 1;          // differentiable 9/7: levels 64..1024 wide (powers of two) as full-row bands
     int t1d_order = 1;           // tier-1 decoder: blocks to lanes by codeword length, longest first
+    int dwt_px = 0;              // encoder: first DWT level read straight from interleaved pixels
 };
 
 // scratch slot ids
 enum { SCR_LL0 = 0, SCR_LL1 = 1, SCR_JOBS = 2, SCR_SYMS = 3, SCR_T1STATE = 4, SCR_MISC = 5,
        SCR_PLANES = 6, SCR_MISC2 = 7, SCR_RES = 8, SCR_UNITS = 9, SCR_SEGS = 10, SCR_BARRIER = 11,
-       SCR_PLANE = 12, SCR_DECORD = 13 };
+       SCR_PLANE = 12, SCR_DECORD = 13, SCR_LLPX = 14 };
 
 j2k_status j2k_fail(j2k_ctx* ctx, j2k_status s, const std::string& msg);
 j2k_status j2k_cuda_check(j2k_ctx* ctx, cudaError_t e, const char* what);
@@ -190,6 +191,14 @@ j2k_status j2k_dwt_fwd_impl(j2k_ctx* ctx, int kernel, int order, const void* in,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,
                             cudaStream_t st, int n = 1, size_t in_z = 0, size_t out_z = 0);
+// Level 0 of ncomp (1 or 3) components read straight from interleaved 8-bit pixels, the colour
+// transform (mct) inside the level's loads; T.800 order.  Component c's subbands go to
+// out + c * out_z (Mallat positions), its LL band to ll + c * ll_z, or into out when levels == 1
+// (quantised when steps are given).  _ok tells whether a shape and transform pair is supported.
+bool j2k_dwt_fwd_px_ok(int kernel, int ncomp, int mct, size_t w, size_t h);
+j2k_status j2k_dwt_fwd_px_launch(j2k_ctx* ctx, int kernel, int ncomp, int mct, const uint8_t* px, size_t pitch,
+                                 size_t w, size_t h, int levels, const float* steps, void* ll, size_t llpitch,
+                                 size_t ll_z, void* out, size_t out_pitch, size_t out_z, cudaStream_t stream);
 j2k_status j2k_dwt_inv_impl(j2k_ctx* ctx, int kernel, int order, const void* in, size_t in_pitch,
                             void* out, size_t out_pitch, size_t w, size_t h, int levels,
                             const float* steps, void* ll0, void* ll1, j2k_dwt_tile tile,

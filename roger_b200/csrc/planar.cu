@@ -7,17 +7,9 @@
 // HBM-bound: algorithmic bytes per pixel = ncomp (uint8 in) + 4*ncomp (planes out).  The fast
 // kernel moves 16 pixels per thread with 16-byte loads and stores.
 #include "j2k_internal.cuh"
+#include "mct.cuh"
 
 namespace {
-
-constexpr float YR = 0.299f, YG = 0.587f, YB = 0.114f;
-constexpr float BR = -0.16875f, BG = -0.33126f, BB = 0.5f;
-constexpr float RR = 0.5f, RG = -0.41869f, RB = -0.08131f;
-constexpr float IRV = 1.402f, IGU = -0.34413f, IGV = -0.71414f, IBU = 1.772f;
-
-__device__ __forceinline__ float dot3(float a, float x, float b, float y, float c, float z) {
-    return __fadd_rn(__fadd_rn(__fmul_rn(a, x), __fmul_rn(b, y)), __fmul_rn(c, z));
-}
 
 // one pixel, generic path
 template <typename TO>

@@ -10,6 +10,9 @@ benchmark workloads but stay within a few hundred MB of device memory:
   planar       4096x4096 RGB uint8 -> 3 int32 planes with RCT (1 launch)
   dwt53        level-0 5/3 forward of the three 4096x4096 int32 RCT planes (1 launch per run)
   dwt53-all    6-level 5/3 forward of the same planes
+  dwt-px       the encoder's level-0 5/3 forward straight from the 4096x4096 RGB uint8 pixels (tuning
+               key J2K_TUNE_DWT_PX; RCT inside the loads, the three components in one launch;
+               coefficients only)
   idwt53       level-0 5/3 inverse of the same plane
   tier1        EBCOT tier-1 of one 4096x4096 RCT component (6 levels, 4096 64x64 blocks)
   encode       one whole lossless 4096x4096 RGB encode (planar, 3 x 6 DWT levels, tier-1)
@@ -55,6 +58,14 @@ def case_dwt53(levels=1):
     planes = C.rgb_to_planar(_rgb(), 1)
     out = torch.empty_like(planes)
     return lambda: C.dwt_forward(planes, levels, out=out)
+
+
+def case_dwt_px(levels=1):
+    img = _rgb()
+    ctx = C.Context(0)
+    lib().j2k_ctx_set_tuning(ctx.h, 15, 1)  # J2K_TUNE_DWT_PX: level 0 from the pixels
+    enc = C.OCLEncoder(ctx=ctx, lossy=False, output_dwt=True)
+    return lambda: enc.run_rgb(img, levels=levels)
 
 
 def _tma(on):
@@ -151,7 +162,7 @@ def case_rate():
     return lambda: enc.run_rgb(img, levels=6, cbw=64, cbh=64, target_bytes=4096 * 4096 // 8)
 
 
-CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_dwt53(6),
+CASES = {"planar": case_planar, "dwt53": case_dwt53, "dwt53-all": lambda: case_dwt53(6), "dwt-px": case_dwt_px,
          "idwt53": case_idwt53, "tier1": case_tier1, "encode": case_encode,
          "diff-kernels": case_diff_kernels, "diff-step": case_diff_step, "batched": case_batched,
          "decode": case_decode,
