@@ -294,7 +294,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                 uint32_t rr = 0, rf = 0, nb = 0, bb = 0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const MT nbm = dil(SG[j]) | dil(SG[j + 2]) | (MT)(SG[j + 1] << 1) | (MT)(SG[j + 1] >> 1);
+                    const MT nbm = dil((MT)(SG[j] | SG[j + 2])) | (MT)(SG[j + 1] << 1) | (MT)(SG[j + 1] >> 1);
                     rr |= ((win4(R[j], c0) >> 1) & ownmask) << (2 * j);
                     rf |= ((win4(S.ref[r0 + j + 1], c0) >> 1) & 3u) << (2 * j);
                     nb |= ((win4(nbm, c0) >> 1) & 3u) << (2 * j);
