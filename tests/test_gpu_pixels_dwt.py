@@ -65,3 +65,25 @@ def test_pixel_level_on_device_input_and_pitch():
     a = C.OCLEncoder(ctx=_ctx(1)).run_rgb(img, levels=5).get_codeblocks()
     b = C.OCLEncoder(ctx=_ctx(1)).run_rgb(torch.from_numpy(img).cuda(), levels=5).get_codeblocks()
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("kernel_dtype", ["int32", "float32"])
+def test_dwt_batch_with_odd_plane_strides(kernel_dtype):
+    """A batch of planes whose plane stride is odd (even row pitch) transforms like each plane on
+    its own: the level kernels keep 8-byte stores and 16-byte copies for batches whose every plane
+    stays aligned for them."""
+    import torch
+    n, h, w, levels = 3, 157, 300, 4
+    pitch, stride = w, w * h + 1
+    rng = np.random.default_rng(5)
+    src = rng.integers(-128, 128, size=(n, h, w)).astype(np.int32)
+    dt = torch.int32 if kernel_dtype == "int32" else torch.float32
+    flat_in = torch.zeros(n * stride, dtype=dt, device="cuda")
+    flat_out = torch.zeros(n * stride, dtype=dt, device="cuda")
+    planes = torch.as_strided(flat_in, (n, h, w), (stride, pitch, 1))
+    planes.copy_(torch.from_numpy(src).to(dt))
+    out = torch.as_strided(flat_out, (n, h, w), (stride, pitch, 1))
+    C.dwt_forward(planes, levels, out=out)
+    for i in range(n):
+        one = C.dwt_forward(planes[i].clone(), levels)  # a fresh, aligned plane
+        assert torch.equal(out[i].contiguous().view(torch.int32), one.view(torch.int32))
