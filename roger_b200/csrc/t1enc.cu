@@ -194,7 +194,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                     B[j] = S.bits[(r0 + j) & 63];
                     C[j] = ~O[j + 1] & V;
                     M[j] = C[j] & B[j];
-                    E[j] = C[j] & (dil(O[j]) | dil(O[j + 1]) | dil(O[j + 2]));
+                    E[j] = C[j] & dil((MT)(O[j] | O[j + 1] | O[j + 2]));  // dilation distributes over OR
                     anyk |= E[j] != 0;
                 }
                 if (!anyk) continue;  // no candidate has a significant neighbour: nothing coded
