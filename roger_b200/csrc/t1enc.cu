@@ -191,13 +191,16 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const MT V = (r0 + j < ch) ? colmask : (MT)0;
-                    B[j] = S.bits[(r0 + j) & 63];
                     C[j] = ~O[j + 1] & V;
-                    M[j] = C[j] & B[j];
                     E[j] = C[j] & dil((MT)(O[j] | O[j + 1] | O[j + 2]));  // dilation distributes over OR
                     anyk |= E[j] != 0;
                 }
                 if (!anyk) continue;  // no candidate has a significant neighbour: nothing coded
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    B[j] = S.bits[(r0 + j) & 63];
+                    M[j] = C[j] & B[j];
+                }
                 N[0] = N[5] = 0;
                 N[1] = N[2] = N[3] = N[4] = 0;
                 if ((M[0] | M[1] | M[2] | M[3]) != 0) {  // else no sample becomes significant
@@ -217,7 +220,7 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
 #pragma unroll
                 for (int j = 0; j < 4; ++j) K[j] = C[j] & (E[j] | ((N[j] | N[j + 1] | N[j + 2]) << 1) | N[j]);
                 // per-lane windows
-                uint32_t a[6], o[6], ng[6], kk = 0, nn4 = 0, bb = 0;
+                uint32_t a[6], o[6], ng[6], kk = 0, bb = 0;
 #pragma unroll
                 for (int j = 0; j < 6; ++j) {
                     o[j] = win4(O[j], c0);
@@ -227,9 +230,10 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     kk |= ((win4(K[j], c0) >> 1) & ownmask) << (2 * j);
-                    nn4 |= ((win4(N[j + 1], c0) >> 1) & ownmask) << (2 * j);
                     bb |= ((win4(B[j], c0) >> 1) & 3u) << (2 * j);
                 }
+                // the newly significant samples are the coded ones whose bit is 1 (N = K & B)
+                const uint32_t nn4 = kk & bb;
                 int cnt = __popc(kk) + __popc(nn4);
                 int tot;
                 int off = pos + warp_excl(cnt, lane, &tot);
