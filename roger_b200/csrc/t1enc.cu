@@ -76,6 +76,13 @@ __device__ __forceinline__ uint32_t win4(T m, int c0) {
     return (uint32_t)(c0 ? (m >> (c0 - 1)) : (T)(m << 1)) & 0xF;
 }
 
+// the lane's own columns c0 and c0+1 of a row mask (bit 0 = column c0; columns past the mask
+// read as 0): bits 1-2 of win4 without its left-edge case
+template <typename T>
+__device__ __forceinline__ uint32_t own2(T m, int c0) {
+    return (uint32_t)(m >> c0) & 3u;
+}
+
 // warp exclusive prefix sum; returns the total in *tot
 __device__ __forceinline__ int warp_excl(int v, int lane, int* tot) {
     int inc = v;
@@ -229,8 +236,8 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
                 }
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    kk |= ((win4(K[j], c0) >> 1) & ownmask) << (2 * j);
-                    bb |= ((win4(B[j], c0) >> 1) & 3u) << (2 * j);
+                    kk |= (own2(K[j], c0) & ownmask) << (2 * j);
+                    bb |= own2(B[j], c0) << (2 * j);
                 }
                 // the newly significant samples are the coded ones whose bit is 1 (N = K & B)
                 const uint32_t nn4 = kk & bb;
@@ -299,10 +306,10 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const MT nbm = dil((MT)(SG[j] | SG[j + 2])) | (MT)(SG[j + 1] << 1) | (MT)(SG[j + 1] >> 1);
-                    rr |= ((win4(R[j], c0) >> 1) & ownmask) << (2 * j);
-                    rf |= ((win4(S.ref[r0 + j + 1], c0) >> 1) & 3u) << (2 * j);
-                    nb |= ((win4(nbm, c0) >> 1) & 3u) << (2 * j);
-                    bb |= ((win4(S.bits[(r0 + j) & 63], c0) >> 1) & 3u) << (2 * j);
+                    rr |= (own2(R[j], c0) & ownmask) << (2 * j);
+                    rf |= own2(S.ref[r0 + j + 1], c0) << (2 * j);
+                    nb |= own2(nbm, c0) << (2 * j);
+                    bb |= own2(S.bits[(r0 + j) & 63], c0) << (2 * j);
                 }
                 const int cnt = __popc(rr);
                 int tot;
@@ -361,8 +368,8 @@ __device__ __forceinline__ void phase_a_block(WarpSmem& S, const j2k_cb_job& J, 
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                cc |= ((win4(C[j], c0) >> 1) & ownmask) << (2 * j);
-                nn4 |= ((win4(N[j], c0) >> 1) & ownmask) << (2 * j);
+                cc |= (own2(C[j], c0) & ownmask) << (2 * j);
+                nn4 |= (own2(N[j], c0) & ownmask) << (2 * j);
             }
             // per column: run-length mode?  (full stripe, 4 candidates, no significant neighbour)
             uint32_t rlmask = 0;  // bit k: column c0+k codes in run-length mode
